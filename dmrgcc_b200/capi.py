@@ -1,0 +1,321 @@
+"""ctypes binding of the libdmrg_b200 C ABI (include/dmrg_b200.h).
+
+The library is the product: every numeric call here goes to the sm_100a
+kernels.  There is no CPU fallback; loading fails loudly when the shared
+library has not been built (python -m dmrgcc_b200.build).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Sequence
+
+import numpy as np
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "lib", "libdmrg_b200.so")
+
+DMRG_PREC_FP64 = 0
+DMRG_PREC_BF16X3 = 1
+
+_lib: C.CDLL | None = None
+
+
+class DmrgError(RuntimeError):
+    def __init__(self, code: int, where: str):
+        msg = lib().dmrg_last_error().decode()
+        super().__init__(f"{where} failed ({code}): {msg}")
+        self.code = code
+
+
+class Blocks(C.Structure):
+    """dmrg_blocks_t."""
+
+    _fields_ = [("nblocks", C.c_int), ("left", C.POINTER(C.c_int)), ("right", C.POINTER(C.c_int)),
+                ("rows", C.POINTER(C.c_int)), ("cols", C.POINTER(C.c_int))]
+
+
+_I = C.POINTER(C.c_int)
+_D = C.POINTER(C.c_double)
+_I64 = C.POINTER(C.c_int64)
+_VP = C.c_void_p
+
+_SIGS = {
+    "dmrg_version": (C.c_char_p, []),
+    "dmrg_last_error": (C.c_char_p, []),
+    "dmrg_ctx_create": (C.c_int, [C.c_int, C.POINTER(_VP)]),
+    "dmrg_ctx_destroy": (C.c_int, [_VP]),
+    "dmrg_ctx_set_stream": (C.c_int, [_VP, _VP]),
+    "dmrg_ctx_stream": (_VP, [_VP]),
+    "dmrg_ctx_sync": (C.c_int, [_VP]),
+    "dmrg_malloc": (C.c_int, [_VP, C.c_size_t, C.POINTER(_VP)]),
+    "dmrg_free": (C.c_int, [_VP, _VP]),
+    "dmrg_memcpy_h2d": (C.c_int, [_VP, _VP, _VP, C.c_size_t]),
+    "dmrg_memcpy_d2h": (C.c_int, [_VP, _VP, _VP, C.c_size_t]),
+    "dmrg_memset": (C.c_int, [_VP, _VP, C.c_int, C.c_size_t]),
+    "dmrg_fill_uniform": (C.c_int, [_VP, _VP, C.c_int64, C.c_uint64, C.c_int64]),
+    "dmrg_fp64_peak": (C.c_int, [_VP, C.c_int, C.c_int, _D]),
+    "dmrg_heff_create": (C.c_int, [_VP, C.c_int, C.c_int, _I, C.POINTER(Blocks), C.c_int, C.c_int, C.c_int, _D,
+                                   C.POINTER(Blocks), C.POINTER(Blocks), C.c_int, C.POINTER(_VP)]),
+    "dmrg_heff_destroy": (C.c_int, [_VP]),
+    "dmrg_heff_sizes": (C.c_int, [_VP, _I64, _I64, _I64]),
+    "dmrg_heff_flops": (C.c_int, [_VP, _D, _D]),
+    "dmrg_heff_set_env": (C.c_int, [_VP, _VP, _VP]),
+    "dmrg_heff_apply": (C.c_int, [_VP, _VP, _VP, C.c_int]),
+    "dmrg_heff_apply_host": (C.c_int, [_VP, _VP, _VP, C.c_int]),
+    "dmrg_heff_profile": (C.c_int, [_VP, _VP, _VP, _D, _D]),
+    "dmrg_env_create": (C.c_int, [_VP, C.c_int, C.c_int, C.c_int, _I, C.POINTER(Blocks), C.c_int, C.c_int, C.c_int,
+                                  _D, C.POINTER(Blocks), C.c_int, C.POINTER(_VP)]),
+    "dmrg_env_destroy": (C.c_int, [_VP]),
+    "dmrg_env_out_info": (C.c_int, [_VP, _I, _I64]),
+    "dmrg_env_out_blocks": (C.c_int, [_VP, C.c_int, C.c_int, _I, _I, _I, _I, _I]),
+    "dmrg_env_flops": (C.c_int, [_VP, _D, _D]),
+    "dmrg_env_apply": (C.c_int, [_VP, _VP, _VP, _VP]),
+}
+
+
+def declared_symbols() -> list[str]:
+    """Every entry point bound here (all of include/dmrg_b200.h)."""
+    return sorted(_SIGS)
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m dmrgcc_b200.build`")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGS.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(rc: int, where: str) -> None:
+    if rc != 0:
+        raise DmrgError(rc, where)
+
+
+def _iptr(a: np.ndarray):
+    return a.ctypes.data_as(_I)
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(_D)
+
+
+class BlockSpec:
+    """Shape of one block list (the sector indices and sizes of a RealMatrixBlock)."""
+
+    def __init__(self, left: Sequence[int], right: Sequence[int], rows: Sequence[int], cols: Sequence[int]):
+        self.left = np.ascontiguousarray(left, dtype=np.int32)
+        self.right = np.ascontiguousarray(right, dtype=np.int32)
+        self.rows = np.ascontiguousarray(rows, dtype=np.int32)
+        self.cols = np.ascontiguousarray(cols, dtype=np.int32)
+
+    @property
+    def size(self) -> int:
+        return int(np.sum(self.rows.astype(np.int64) * self.cols.astype(np.int64)))
+
+    def c(self) -> Blocks:
+        return Blocks(len(self.left), _iptr(self.left), _iptr(self.right), _iptr(self.rows), _iptr(self.cols))
+
+
+def _blocks_array(specs: Sequence[BlockSpec]):
+    arr = (Blocks * max(len(specs), 1))()
+    for i, s in enumerate(specs):
+        arr[i] = s.c()
+    return arr
+
+
+class Context:
+    def __init__(self, device: int = 0):
+        h = _VP()
+        check(lib().dmrg_ctx_create(device, C.byref(h)), "dmrg_ctx_create")
+        self.h = h
+
+    def close(self) -> None:
+        if self.h:
+            lib().dmrg_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream_ptr: int | None) -> None:
+        check(lib().dmrg_ctx_set_stream(self.h, stream_ptr), "dmrg_ctx_set_stream")
+
+    @property
+    def stream(self) -> int:
+        return lib().dmrg_ctx_stream(self.h) or 0
+
+    def sync(self) -> None:
+        check(lib().dmrg_ctx_sync(self.h), "dmrg_ctx_sync")
+
+    def fp64_peak(self, mode: int = 0, iters: int = 20000) -> float:
+        """Measured FP64 TFLOP/s (mode 0: DMMA, 1: DFMA)."""
+        t = C.c_double()
+        check(lib().dmrg_fp64_peak(self.h, mode, iters, C.byref(t)), "dmrg_fp64_peak")
+        return t.value
+
+
+class DeviceArray:
+    """A float64 device buffer allocated through the C ABI."""
+
+    def __init__(self, ctx: Context, n: int):
+        self.ctx, self.n = ctx, int(n)
+        p = _VP()
+        check(lib().dmrg_malloc(ctx.h, max(self.n, 1) * 8, C.byref(p)), "dmrg_malloc")
+        self.ptr = p.value
+
+    @classmethod
+    def from_host(cls, ctx: Context, a: np.ndarray) -> "DeviceArray":
+        a = np.ascontiguousarray(a, dtype=np.float64).ravel()
+        d = cls(ctx, a.size)
+        d.upload(a)
+        return d
+
+    def upload(self, a: np.ndarray) -> None:
+        a = np.ascontiguousarray(a, dtype=np.float64).ravel()
+        assert a.size == self.n
+        check(lib().dmrg_memcpy_h2d(self.ctx.h, self.ptr, a.ctypes.data, a.nbytes), "dmrg_memcpy_h2d")
+
+    def download(self) -> np.ndarray:
+        out = np.empty(self.n, dtype=np.float64)
+        check(lib().dmrg_memcpy_d2h(self.ctx.h, out.ctypes.data, self.ptr, out.nbytes), "dmrg_memcpy_d2h")
+        return out
+
+    def fill_uniform(self, seed: int, start: int = 0) -> None:
+        check(lib().dmrg_fill_uniform(self.ctx.h, self.ptr, self.n, seed, start), "dmrg_fill_uniform")
+
+    def zero(self) -> None:
+        check(lib().dmrg_memset(self.ctx.h, self.ptr, 0, self.n * 8), "dmrg_memset")
+
+    def free(self) -> None:
+        if self.ptr:
+            lib().dmrg_free(self.ctx.h, self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class SiteProblem:
+    """Block structure of one site: sectors, ket blocks, MPO tensor."""
+
+    def __init__(self, nl: int, nr: int, phys: np.ndarray, ket: BlockSpec, W: np.ndarray):
+        self.nl, self.nr = int(nl), int(nr)
+        self.phys = np.ascontiguousarray(phys, dtype=np.int32).reshape(-1)
+        assert self.phys.size == self.nl * self.nr
+        self.ket = ket
+        self.W = np.ascontiguousarray(W, dtype=np.float64)
+        self.lb, self.rb, self.d = self.W.shape[0], self.W.shape[1], self.W.shape[2]
+
+
+class Heff:
+    """H_eff*psi operator (MultiplyEffectHamilton)."""
+
+    def __init__(self, ctx: Context, site: SiteProblem, L: Sequence[BlockSpec], R: Sequence[BlockSpec],
+                 precision: int = DMRG_PREC_FP64):
+        self.ctx, self.site = ctx, site
+        self._L, self._R = _blocks_array(L), _blocks_array(R)
+        kb = site.ket.c()
+        h = _VP()
+        check(lib().dmrg_heff_create(ctx.h, site.nl, site.nr, _iptr(site.phys), C.byref(kb), site.d, site.lb,
+                                     site.rb, _dptr(site.W), self._L, self._R, precision, C.byref(h)),
+              "dmrg_heff_create")
+        self.h = h
+        a, b, c = C.c_int64(), C.c_int64(), C.c_int64()
+        check(lib().dmrg_heff_sizes(h, C.byref(a), C.byref(b), C.byref(c)), "dmrg_heff_sizes")
+        self.psi_dim, self.l_size, self.r_size = a.value, b.value, c.value
+
+    def flops(self) -> tuple[float, float]:
+        a, e = C.c_double(), C.c_double()
+        check(lib().dmrg_heff_flops(self.h, C.byref(a), C.byref(e)), "dmrg_heff_flops")
+        return a.value, e.value
+
+    def set_env(self, L_dev: DeviceArray, R_dev: DeviceArray) -> None:
+        self._env_refs = (L_dev, R_dev)
+        check(lib().dmrg_heff_set_env(self.h, L_dev.ptr, R_dev.ptr), "dmrg_heff_set_env")
+
+    def apply(self, psi: DeviceArray, out: DeviceArray, accumulate: bool = False) -> None:
+        check(lib().dmrg_heff_apply(self.h, psi.ptr, out.ptr, int(accumulate)), "dmrg_heff_apply")
+
+    def apply_ptr(self, psi_ptr: int, out_ptr: int, accumulate: bool = False) -> None:
+        check(lib().dmrg_heff_apply(self.h, psi_ptr, out_ptr, int(accumulate)), "dmrg_heff_apply")
+
+    def profile(self, psi: DeviceArray, out: DeviceArray) -> tuple[float, float]:
+        """Durations (ms) of the two grouped launches of one accumulating apply."""
+        a, b = C.c_double(), C.c_double()
+        check(lib().dmrg_heff_profile(self.h, psi.ptr, out.ptr, C.byref(a), C.byref(b)), "dmrg_heff_profile")
+        return a.value, b.value
+
+    def apply_host(self, psi: np.ndarray, out: np.ndarray, accumulate: bool = False) -> None:
+        check(lib().dmrg_heff_apply_host(self.h, psi.ctypes.data, out.ctypes.data, int(accumulate)),
+              "dmrg_heff_apply_host")
+
+    def close(self) -> None:
+        if self.h:
+            lib().dmrg_heff_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Env:
+    """Environment update (Left/RightComputeTensorContraction)."""
+
+    def __init__(self, ctx: Context, side: int, site: SiteProblem, env_in: Sequence[BlockSpec],
+                 precision: int = DMRG_PREC_FP64):
+        self.ctx, self.site, self.side = ctx, site, side
+        self._in = _blocks_array(env_in)
+        kb = site.ket.c()
+        h = _VP()
+        check(lib().dmrg_env_create(ctx.h, side, site.nl, site.nr, _iptr(site.phys), C.byref(kb), site.d, site.lb,
+                                    site.rb, _dptr(site.W), self._in, precision, C.byref(h)), "dmrg_env_create")
+        self.h = h
+        bond, size = C.c_int(), C.c_int64()
+        check(lib().dmrg_env_out_info(h, C.byref(bond), C.byref(size)), "dmrg_env_out_info")
+        self.out_bond, self.out_size = bond.value, size.value
+
+    def out_blocks(self) -> list[BlockSpec]:
+        res = []
+        for o in range(self.out_bond):
+            n = C.c_int()
+            check(lib().dmrg_env_out_blocks(self.h, o, 0, C.byref(n), None, None, None, None), "env_out_blocks")
+            arrs = [np.zeros(max(n.value, 1), dtype=np.int32) for _ in range(4)]
+            check(lib().dmrg_env_out_blocks(self.h, o, max(n.value, 1), C.byref(n), *[_iptr(a) for a in arrs]),
+                  "env_out_blocks")
+            res.append(BlockSpec(*[a[:n.value] for a in arrs]))
+        return res
+
+    def flops(self) -> tuple[float, float]:
+        a, e = C.c_double(), C.c_double()
+        check(lib().dmrg_env_flops(self.h, C.byref(a), C.byref(e)), "dmrg_env_flops")
+        return a.value, e.value
+
+    def apply(self, ket: DeviceArray, env_in: DeviceArray, env_out: DeviceArray) -> None:
+        check(lib().dmrg_env_apply(self.h, ket.ptr, env_in.ptr, env_out.ptr), "dmrg_env_apply")
+
+    def close(self) -> None:
+        if self.h:
+            lib().dmrg_env_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,141 @@
+// Context, error reporting and memory entry points of the C ABI.
+#include <cstring>
+
+#include "blocksparse.h"
+#include "common.cuh"
+
+namespace dmrg {
+
+static thread_local std::string g_last_error = "no error";
+
+int set_error(int code, const char* fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return code;
+}
+
+int build_site_desc(SiteDesc& s, int nl, int nr, const int* phys, const dmrg_blocks_t* ket, int d, int lb, int rb,
+                    const double* W) {
+    if (nl <= 0 || nr <= 0 || !phys || !ket || d <= 0 || lb <= 0 || rb <= 0 || !W)
+        return set_error(DMRG_E_ARG, "invalid site description (nl=%d nr=%d d=%d lb=%d rb=%d)", nl, nr, d, lb, rb);
+    s.nl = nl;
+    s.nr = nr;
+    s.d = d;
+    s.lb = lb;
+    s.rb = rb;
+    s.phys.assign(phys, phys + (size_t)nl * nr);
+    s.W.assign(W, W + (size_t)lb * rb * d * d);
+    if (!s.ket.assign(*ket)) return set_error(DMRG_E_ARG, "invalid ket block list");
+    for (int k = 0; k < s.ket.count(); ++k) {
+        int l = s.ket.left[k], r = s.ket.right[k];
+        if (l < 0 || l >= nl || r < 0 || r >= nr)
+            return set_error(DMRG_E_ARG, "ket block %d has sectors (%d,%d) outside %dx%d", k, l, r, nl, nr);
+        int p = s.p(l, r);
+        if (p < 0 || p >= d)
+            return set_error(DMRG_E_ARG, "ket block %d (%d,%d) has physics index %d", k, l, r, p);
+    }
+    return DMRG_OK;
+}
+
+}  // namespace dmrg
+
+using namespace dmrg;
+
+extern "C" {
+
+const char* dmrg_version(void) { return "dmrg_b200 0.1 (sm_100a)"; }
+
+const char* dmrg_last_error(void) { return g_last_error.c_str(); }
+
+int dmrg_ctx_create(int device, dmrg_ctx_t* out) {
+    if (!out) return set_error(DMRG_E_ARG, "null output pointer");
+    *out = nullptr;
+    int n = 0;
+    DMRG_CUDA_TRY(cudaGetDeviceCount(&n));
+    if (device < 0 || device >= n) return set_error(DMRG_E_ARG, "device %d out of range (%d devices)", device, n);
+    DMRG_CUDA_TRY(cudaSetDevice(device));
+    auto* c = new dmrg_ctx_s();
+    c->device = device;
+    cudaError_t e = cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete c;
+        return set_error(DMRG_E_CUDA, "cudaStreamCreate: %s", cudaGetErrorString(e));
+    }
+    c->stream = c->own_stream;
+    cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
+    e = cudaMalloc(&c->d_status, sizeof(int) * 16);
+    if (e != cudaSuccess) {
+        cudaStreamDestroy(c->own_stream);
+        delete c;
+        return set_error(DMRG_E_NOMEM, "cudaMalloc status: %s", cudaGetErrorString(e));
+    }
+    cudaMemset(c->d_status, 0, sizeof(int) * 16);
+    *out = c;
+    return DMRG_OK;
+}
+
+int dmrg_ctx_destroy(dmrg_ctx_t ctx) {
+    if (!ctx) return DMRG_OK;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    cudaFree(ctx->d_status);
+    cudaStreamDestroy(ctx->own_stream);
+    delete ctx;
+    return DMRG_OK;
+}
+
+int dmrg_ctx_set_stream(dmrg_ctx_t ctx, void* stream) {
+    if (!ctx) return set_error(DMRG_E_ARG, "null context");
+    ctx->stream = stream ? (cudaStream_t)stream : ctx->own_stream;
+    return DMRG_OK;
+}
+
+void* dmrg_ctx_stream(dmrg_ctx_t ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+int dmrg_ctx_sync(dmrg_ctx_t ctx) {
+    if (!ctx) return set_error(DMRG_E_ARG, "null context");
+    DMRG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    return DMRG_OK;
+}
+
+int dmrg_malloc(dmrg_ctx_t ctx, size_t bytes, void** dev) {
+    if (!ctx || !dev) return set_error(DMRG_E_ARG, "null argument");
+    cudaError_t e = cudaMalloc(dev, bytes ? bytes : 1);
+    if (e != cudaSuccess) return set_error(DMRG_E_NOMEM, "cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e));
+    return DMRG_OK;
+}
+
+int dmrg_free(dmrg_ctx_t ctx, void* dev) {
+    (void)ctx;
+    if (dev) DMRG_CUDA_TRY(cudaFree(dev));
+    return DMRG_OK;
+}
+
+int dmrg_memcpy_h2d(dmrg_ctx_t ctx, void* dst, const void* src, size_t bytes) {
+    if (!ctx) return set_error(DMRG_E_ARG, "null context");
+    if (bytes == 0) return DMRG_OK;
+    DMRG_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    DMRG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    return DMRG_OK;
+}
+
+int dmrg_memcpy_d2h(dmrg_ctx_t ctx, void* dst, const void* src, size_t bytes) {
+    if (!ctx) return set_error(DMRG_E_ARG, "null context");
+    if (bytes == 0) return DMRG_OK;
+    DMRG_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    DMRG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    return DMRG_OK;
+}
+
+int dmrg_memset(dmrg_ctx_t ctx, void* dev, int value, size_t bytes) {
+    if (!ctx) return set_error(DMRG_E_ARG, "null context");
+    if (bytes == 0) return DMRG_OK;
+    DMRG_CUDA_TRY(cudaMemsetAsync(dev, value, bytes, ctx->stream));
+    return DMRG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,83 @@
+// Grouped multi-term block GEMM: the one contraction engine behind H_eff*psi,
+// the environment updates and the merge.
+//
+// A launch processes a list of output blocks ("groups").  Group g owns a
+// row-major m x n block C_g at C + c_off (leading dimension ldc) and a range of
+// terms [t0, t1); each term contributes scale * op(A_t) @ op(B_t) with A_t at
+// A + a_off (m x k, or k x m when TA) and B_t at B + b_off (k x n, or n x k when
+// TB).  All terms of a group are summed in registers by the CTA that owns the
+// output tile, so no atomics are needed and the summation order is fixed.
+// Work items ("tiles") are (group, m0, n0) output tiles, sorted by cost.
+#pragma once
+
+#include <cstdint>
+
+#include "common.cuh"
+
+namespace dmrg {
+
+struct GemmTerm {
+    int64_t a_off;
+    int64_t b_off;
+    int lda;
+    int ldb;
+    int k;
+    int pad_;
+    double scale;
+};
+
+struct GemmGroup {
+    int64_t c_off;
+    int ldc;
+    int m;
+    int n;
+    int t0;
+    int t1;
+    int pad_;
+};
+
+struct GemmTile {
+    int group;
+    int m0;
+    int n0;
+    int cost;  // k-steps, used for ordering only
+};
+
+// Host-side schedule of one launch.
+struct GemmSchedule {
+    std::vector<GemmTerm> terms;
+    std::vector<GemmGroup> groups;
+    std::vector<GemmTile> tiles;
+    bool ta = false, tb = false;
+    double flops = 0.0;  // 2*m*n*k summed over terms
+    // device copies
+    DeviceBuffer d_terms, d_groups, d_tiles;
+
+    void reset() {
+        terms.clear();
+        groups.clear();
+        tiles.clear();
+        ta = tb = false;
+        flops = 0.0;
+    }
+    int add_group(int64_t c_off, int ldc, int m, int n) {
+        GemmGroup g{c_off, ldc, m, n, (int)terms.size(), (int)terms.size(), 0};
+        groups.push_back(g);
+        return (int)groups.size() - 1;
+    }
+    // Terms must be appended to the most recently added group.
+    void add_term(int64_t a_off, int lda, int64_t b_off, int ldb, int k, double scale) {
+        GemmGroup& g = groups.back();
+        terms.push_back(GemmTerm{a_off, b_off, lda, ldb, k, 0, scale});
+        g.t1 = (int)terms.size();
+        flops += 2.0 * g.m * g.n * (double)k;
+    }
+    // Builds the tile list (tile_m x tile_n tiles, heaviest first) and uploads.
+    int finalize(int tile_m, int tile_n, int tile_k, cudaStream_t stream);
+};
+
+// C (+)= sum of terms for every tile of `s`.  A, B, C are the base pointers.
+int launch_gemm_f64(const GemmSchedule& s, const double* A, const double* B, double* C,
+                    bool accumulate, cudaStream_t stream);
+
+}  // namespace dmrg

@@ -1,0 +1,196 @@
+// FP64 grouped multi-term block GEMM on the FP64 tensor path (DMMA,
+// mma.sync.m8n8k4.f64).  tcgen05 has no f64 kind, so this is the sm_100a FP64
+// contraction engine.
+//
+// CTA: 128 threads (2x2 warps), 64x64 output tile, k-step 16, two shared-memory
+// stages filled by 8-byte cp.async (block leading dimensions are arbitrary, so
+// neither 16-byte vector loads nor TMA tensor maps apply to the raw blocks).
+// Each warp owns a 32x32 sub-tile = 4x4 DMMA tiles, 32 FP64 accumulators per
+// thread.  Shared tiles are stored in the operand's global orientation with a
+// 4-double row pad, which makes every fragment read conflict-free.
+#include <algorithm>
+#include <numeric>
+
+#include "gemm.cuh"
+
+namespace dmrg {
+namespace {
+
+constexpr int BM = 64, BK = 16, NT = 128;  // tile N is also 64 (2 warps x 32)
+constexpr int SA = BK + 4;            // stride of a [64][16] tile
+constexpr int SB = BM + 4;            // stride of a [16][64] tile
+constexpr int STAGE = BM * SA;        // 1280 >= BK * SB = 1088
+
+__device__ __forceinline__ void cp_async8(double* smem, const double* gmem, bool valid) {
+    unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    int src_size = valid ? 8 : 0;
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(src_size)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+__device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
+template <bool TA, bool TB>
+__device__ __forceinline__ void load_stage(double* As, double* Bs, const double* __restrict__ A,
+                                           const double* __restrict__ B, const GemmTerm& t, int k0,
+                                           int m0, int n0, int m, int n, int tid) {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const int idx = tid + NT * i;
+        const int r = TA ? (idx & 63) : (idx >> 4);
+        const int c = TA ? (idx >> 6) : (idx & 15);
+        const bool v = (m0 + r < m) && (k0 + c < t.k);
+        const int64_t off = TA ? (int64_t)(k0 + c) * t.lda + (m0 + r) : (int64_t)(m0 + r) * t.lda + (k0 + c);
+        cp_async8(TA ? (As + c * SB + r) : (As + r * SA + c), v ? (A + t.a_off + off) : A, v);
+    }
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const int idx = tid + NT * i;
+        const int nn = TB ? (idx >> 4) : (idx & 63);
+        const int c = TB ? (idx & 15) : (idx >> 6);
+        const bool v = (n0 + nn < n) && (k0 + c < t.k);
+        const int64_t off = TB ? (int64_t)(n0 + nn) * t.ldb + (k0 + c) : (int64_t)(k0 + c) * t.ldb + (n0 + nn);
+        cp_async8(TB ? (Bs + nn * SA + c) : (Bs + c * SB + nn), v ? (B + t.b_off + off) : B, v);
+    }
+}
+
+template <bool TA, bool TB>
+__device__ __forceinline__ void compute_stage(const double* As, const double* Bs, double (&acc)[4][4][2],
+                                              double scale, int wm, int wn, int lane) {
+    const int fr = lane >> 2, fc = lane & 3;
+#pragma unroll
+    for (int kk = 0; kk < BK; kk += 4) {
+        double a[4], b[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int row = wm * 32 + i * 8 + fr, col = kk + fc;
+            a[i] = (TA ? As[col * SB + row] : As[row * SA + col]) * scale;
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int kr = kk + fc, nc = wn * 32 + j * 8 + fr;
+            b[j] = TB ? Bs[nc * SA + kr] : Bs[kr * SB + nc];
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) dmma_8x8x4(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+    }
+}
+
+template <bool TA, bool TB>
+__global__ void __launch_bounds__(NT) gemm_f64_kernel(const double* __restrict__ A, const double* __restrict__ B,
+                                                      double* __restrict__ C, const GemmTerm* __restrict__ terms,
+                                                      const GemmGroup* __restrict__ groups,
+                                                      const GemmTile* __restrict__ tiles, int accumulate) {
+    __shared__ __align__(16) double smA[2][STAGE];
+    __shared__ __align__(16) double smB[2][STAGE];
+    const GemmTile tile = tiles[blockIdx.x];
+    const GemmGroup g = groups[tile.group];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, wm = warp >> 1, wn = warp & 1;
+
+    double acc[4][4][2];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+
+    int t = g.t0;
+    if (t < g.t1) {
+        GemmTerm cur = terms[t];
+        int k0 = 0, stage = 0;
+        double sc_cur = cur.scale;
+        load_stage<TA, TB>(smA[0], smB[0], A, B, cur, 0, tile.m0, tile.n0, g.m, g.n, tid);
+        cp_async_commit();
+        for (;;) {
+            int nk0 = k0 + BK, nt = t;
+            GemmTerm nxt = cur;
+            if (nk0 >= cur.k) {
+                nt = t + 1;
+                nk0 = 0;
+                if (nt < g.t1) nxt = terms[nt];
+            }
+            const bool has_next = nt < g.t1;
+            double sc_nxt = nxt.scale;
+            if (has_next) {
+                load_stage<TA, TB>(smA[stage ^ 1], smB[stage ^ 1], A, B, nxt, nk0, tile.m0, tile.n0, g.m, g.n,
+                                   tid);
+                cp_async_commit();
+                cp_async_wait<1>();
+            } else {
+                cp_async_wait<0>();
+            }
+            __syncthreads();
+            compute_stage<TA, TB>(smA[stage], smB[stage], acc, sc_cur, wm, wn, lane);
+            __syncthreads();
+            if (!has_next) break;
+            stage ^= 1;
+            t = nt;
+            k0 = nk0;
+            cur = nxt;
+            sc_cur = sc_nxt;
+        }
+    }
+
+    const int fr = lane >> 2, fc = lane & 3;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int row = tile.m0 + wm * 32 + i * 8 + fr;
+        if (row >= g.m) continue;
+        double* crow = C + g.c_off + (int64_t)row * g.ldc;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+                const int col = tile.n0 + wn * 32 + j * 8 + fc * 2 + e;
+                if (col < g.n) crow[col] = accumulate ? crow[col] + acc[i][j][e] : acc[i][j][e];
+            }
+        }
+    }
+}
+
+}  // namespace
+
+int GemmSchedule::finalize(int tile_m, int tile_n, int tile_k, cudaStream_t stream) {
+    tiles.clear();
+    for (int gi = 0; gi < (int)groups.size(); ++gi) {
+        const GemmGroup& g = groups[gi];
+        if (g.m <= 0 || g.n <= 0) continue;
+        int ksteps = 0;
+        for (int t = g.t0; t < g.t1; ++t) ksteps += (terms[t].k + tile_k - 1) / tile_k;
+        for (int m0 = 0; m0 < g.m; m0 += tile_m)
+            for (int n0 = 0; n0 < g.n; n0 += tile_n) tiles.push_back(GemmTile{gi, m0, n0, ksteps});
+    }
+    std::stable_sort(tiles.begin(), tiles.end(), [](const GemmTile& a, const GemmTile& b) { return a.cost > b.cost; });
+    DMRG_TRY(upload(d_terms, terms, stream));
+    DMRG_TRY(upload(d_groups, groups, stream));
+    DMRG_TRY(upload(d_tiles, tiles, stream));
+    return DMRG_OK;
+}
+
+int launch_gemm_f64(const GemmSchedule& s, const double* A, const double* B, double* C, bool accumulate,
+                    cudaStream_t stream) {
+    if (s.tiles.empty()) return DMRG_OK;
+    const int n = (int)s.tiles.size();
+    const auto* tr = s.d_terms.as<GemmTerm>();
+    const auto* gr = s.d_groups.as<GemmGroup>();
+    const auto* tl = s.d_tiles.as<GemmTile>();
+    const int acc = accumulate ? 1 : 0;
+    if (!s.ta && !s.tb) gemm_f64_kernel<false, false><<<n, NT, 0, stream>>>(A, B, C, tr, gr, tl, acc);
+    else if (s.ta && !s.tb) gemm_f64_kernel<true, false><<<n, NT, 0, stream>>>(A, B, C, tr, gr, tl, acc);
+    else if (!s.ta && s.tb) gemm_f64_kernel<false, true><<<n, NT, 0, stream>>>(A, B, C, tr, gr, tl, acc);
+    else gemm_f64_kernel<true, true><<<n, NT, 0, stream>>>(A, B, C, tr, gr, tl, acc);
+    DMRG_CUDA_TRY(cudaGetLastError());
+    return DMRG_OK;
+}
+
+}  // namespace dmrg

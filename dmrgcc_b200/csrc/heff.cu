@@ -1,0 +1,253 @@
+// a1: block-sparse H_eff * psi.
+//
+// The reference (RealTensorContraction::MultiplyEffectHamilton,
+// src/dmrg/realdmrg/real_tensor_contraction.cc:1223-1291) walks
+//   o2 -> R block (l -> j) -> K block (k, l) with RightCheckZero(o2, p(k,l))
+//      -> T = K(k,l) R[o2](l,j)
+//      -> psi block (i, j) -> o1 with W[o1][o2](p(i,j), p(k,l)) != 0 and L[o1](i,k)
+//      -> out(i,j) += W * L[o1](i,k) T
+// issuing one MKL dgemm per product.  Here the same walk is done once per site,
+// on the host, to build two grouped launches:
+//   stage A: every T needed by at least one term, one group each (C = scratch);
+//   stage B: one group per output block (i, j) holding all of its
+//            (W, L block, T) terms, summed in registers by the tile owner.
+#include <algorithm>
+
+#include "blocksparse.h"
+#include "gemm.cuh"
+
+using namespace dmrg;
+
+struct dmrg_heff_s {
+    dmrg_ctx_t ctx = nullptr;
+    int precision = DMRG_PREC_FP64;
+    SiteDesc site;
+    EnvDesc L, R;
+    GemmSchedule sa, sb;  // A: psi x R -> T ; B: L x T -> out
+    DeviceBuffer T;
+    int64_t t_size = 0;
+    const double* L_dev = nullptr;
+    const double* R_dev = nullptr;
+    double flops_alg = 0, flops_exec = 0;
+    DeviceBuffer io_psi, io_out;  // staging for dmrg_heff_apply_host
+};
+
+namespace {
+
+int build_heff(dmrg_heff_s& h) {
+    const SiteDesc& s = h.site;
+    const BlockListDesc& ket = s.ket;
+    auto same_right = ket.by_sector(1, s.nr);
+    // Validate environment sector indices.
+    for (int o = 0; o < s.lb; ++o)
+        for (int q = 0; q < h.L.o[o].count(); ++q)
+            if (h.L.o[o].left[q] < 0 || h.L.o[o].left[q] >= s.nl || h.L.o[o].right[q] < 0 ||
+                h.L.o[o].right[q] >= s.nl)
+                return set_error(DMRG_E_ARG, "L[%d] block %d has sectors outside %d", o, q, s.nl);
+    for (int o = 0; o < s.rb; ++o)
+        for (int q = 0; q < h.R.o[o].count(); ++q)
+            if (h.R.o[o].left[q] < 0 || h.R.o[o].left[q] >= s.nr || h.R.o[o].right[q] < 0 ||
+                h.R.o[o].right[q] >= s.nr)
+                return set_error(DMRG_E_ARG, "R[%d] block %d has sectors outside %d", o, q, s.nr);
+
+    struct TermB {
+        int out_pos;
+        int64_t l_off;
+        int lda;
+        int t_index;
+        int k;
+        double w;
+    };
+    std::vector<TermB> termsB;
+    struct TaskA {
+        int pos;       // ket block
+        int64_t r_off; // R block offset
+        int b_l, b_j, a_k;
+        int64_t t_off;
+    };
+    std::vector<TaskA> tasks;
+    h.t_size = 0;
+    double fa_alg = 0, fb = 0, fa_exec = 0;
+
+    for (int o2 = 0; o2 < s.rb; ++o2) {
+        const BlockListDesc& Ro = h.R.o[o2];
+        for (int i = 0; i < Ro.count(); ++i) {
+            const int ldx = Ro.left[i], jdx = Ro.right[i];
+            const int rr = Ro.rows[i], rc = Ro.cols[i];
+            if (rr == 0) continue;  // the reference skips empty blocks
+            for (int pos : same_right[ldx]) {
+                const int kdx = ket.left[pos];
+                const int p2 = s.p(kdx, ldx);
+                if (!s.right_nonzero(o2, p2)) continue;
+                const int a_k = ket.rows[pos], b_l = ket.cols[pos];
+                if (b_l != rr)
+                    return set_error(DMRG_E_ARG, "ket block %d is %dx%d but R[%d] block %d is %dx%d", pos, a_k,
+                                     b_l, o2, i, rr, rc);
+                fa_alg += 2.0 * a_k * b_l * rc;
+                if (a_k == 0 || b_l == 0 || rc == 0) continue;  // empty product
+                const int t_index = (int)tasks.size();
+                bool used = false;
+                for (int pos2 : same_right[jdx]) {
+                    const int idx = ket.left[pos2];
+                    const int p1 = s.p(idx, jdx);
+                    for (int o1 = 0; o1 < s.lb; ++o1) {
+                        const double w = s.w(o1, o2, p1, p2);
+                        if (w == 0.0) continue;
+                        const int q = h.L.o[o1].find(idx, kdx);
+                        if (q == -1) continue;
+                        const int lr = h.L.o[o1].rows[q], lc = h.L.o[o1].cols[q];
+                        if (lc != a_k || lr != ket.rows[pos2] || rc != ket.cols[pos2])
+                            return set_error(DMRG_E_ARG,
+                                             "shape mismatch: L[%d] block %d %dx%d, K %dx%d, R %dx%d, out %dx%d", o1,
+                                             q, lr, lc, a_k, b_l, rr, rc, ket.rows[pos2], ket.cols[pos2]);
+                        if (lr == 0) continue;
+                        termsB.push_back(TermB{pos2, h.L.base[o1] + h.L.o[o1].off[q], lc, t_index, a_k, w});
+                        fb += 2.0 * lr * lc * rc;
+                        used = true;
+                    }
+                }
+                if (used) {
+                    tasks.push_back(TaskA{pos, h.R.base[o2] + Ro.off[i], b_l, rc, a_k, h.t_size});
+                    h.t_size += (int64_t)a_k * rc;
+                    fa_exec += 2.0 * a_k * b_l * rc;
+                }
+            }
+        }
+    }
+
+    // Stage A: one group per T.
+    h.sa.reset();
+    for (const TaskA& t : tasks) {
+        h.sa.add_group(t.t_off, t.b_j, t.a_k, t.b_j);
+        h.sa.add_term(ket.off[t.pos], t.b_l, t.r_off, t.b_j, t.b_l, 1.0);
+    }
+    // Stage B: one group per output block, terms in generation order.
+    h.sb.reset();
+    std::vector<std::vector<int>> per_out(ket.count());
+    for (int i = 0; i < (int)termsB.size(); ++i) per_out[termsB[i].out_pos].push_back(i);
+    for (int pos2 = 0; pos2 < ket.count(); ++pos2) {
+        if (per_out[pos2].empty()) continue;
+        h.sb.add_group(ket.off[pos2], ket.cols[pos2], ket.rows[pos2], ket.cols[pos2]);
+        for (int i : per_out[pos2]) {
+            const TermB& t = termsB[i];
+            const TaskA& ta = tasks[t.t_index];
+            h.sb.add_term(t.l_off, t.lda, ta.t_off, ta.b_j, t.k, t.w);
+        }
+    }
+    h.flops_alg = fa_alg + fb;
+    h.flops_exec = fa_exec + fb;
+    cudaStream_t st = h.ctx->stream;
+    DMRG_TRY(h.sa.finalize(64, 64, 16, st));
+    DMRG_TRY(h.sb.finalize(64, 64, 16, st));
+    DMRG_TRY(h.T.alloc((size_t)std::max<int64_t>(h.t_size, 1) * sizeof(double)));
+    return DMRG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int dmrg_heff_create(dmrg_ctx_t ctx, int nl, int nr, const int* phys, const dmrg_blocks_t* ket, int d, int lb,
+                     int rb, const double* W, const dmrg_blocks_t* L, const dmrg_blocks_t* R, int precision,
+                     dmrg_heff_t* out) {
+    if (!ctx || !out || !L || !R) return set_error(DMRG_E_ARG, "null argument");
+    if (precision != DMRG_PREC_FP64)
+        return set_error(DMRG_E_ARG, "unknown precision %d", precision);
+    *out = nullptr;
+    DMRG_CUDA_TRY(cudaSetDevice(ctx->device));
+    auto* h = new dmrg_heff_s();
+    h->ctx = ctx;
+    h->precision = precision;
+    int rc = build_site_desc(h->site, nl, nr, phys, ket, d, lb, rb, W);
+    if (rc == DMRG_OK && !h->L.assign(L, lb)) rc = set_error(DMRG_E_ARG, "invalid L block lists");
+    if (rc == DMRG_OK && !h->R.assign(R, rb)) rc = set_error(DMRG_E_ARG, "invalid R block lists");
+    if (rc == DMRG_OK) rc = build_heff(*h);
+    if (rc != DMRG_OK) {
+        delete h;
+        return rc;
+    }
+    *out = h;
+    return DMRG_OK;
+}
+
+int dmrg_heff_destroy(dmrg_heff_t h) {
+    delete h;
+    return DMRG_OK;
+}
+
+int dmrg_heff_sizes(dmrg_heff_t h, int64_t* psi_dim, int64_t* lsize, int64_t* rsize) {
+    if (!h) return set_error(DMRG_E_ARG, "null operator");
+    if (psi_dim) *psi_dim = h->site.ket.size;
+    if (lsize) *lsize = h->L.size;
+    if (rsize) *rsize = h->R.size;
+    return DMRG_OK;
+}
+
+int dmrg_heff_flops(dmrg_heff_t h, double* alg, double* exec) {
+    if (!h) return set_error(DMRG_E_ARG, "null operator");
+    if (alg) *alg = h->flops_alg;
+    if (exec) *exec = h->flops_exec;
+    return DMRG_OK;
+}
+
+int dmrg_heff_set_env(dmrg_heff_t h, const double* L_dev, const double* R_dev) {
+    if (!h) return set_error(DMRG_E_ARG, "null operator");
+    if ((!L_dev && h->L.size) || (!R_dev && h->R.size)) return set_error(DMRG_E_ARG, "null environment pointer");
+    h->L_dev = L_dev;
+    h->R_dev = R_dev;
+    return DMRG_OK;
+}
+
+int dmrg_heff_apply(dmrg_heff_t h, const double* psi, double* out, int accumulate) {
+    if (!h) return set_error(DMRG_E_ARG, "null operator");
+    if ((!h->L_dev && h->L.size) || (!h->R_dev && h->R.size))
+        return set_error(DMRG_E_STATE, "dmrg_heff_set_env was not called");
+    cudaStream_t st = h->ctx->stream;
+    if (!accumulate && h->site.ket.size)
+        DMRG_CUDA_TRY(cudaMemsetAsync(out, 0, (size_t)h->site.ket.size * sizeof(double), st));
+    DMRG_TRY(launch_gemm_f64(h->sa, psi, h->R_dev, h->T.as<double>(), false, st));
+    DMRG_TRY(launch_gemm_f64(h->sb, h->L_dev, h->T.as<double>(), out, true, st));
+    return DMRG_OK;
+}
+
+int dmrg_heff_profile(dmrg_heff_t h, const double* psi, double* out, double* ms_stage_a, double* ms_stage_b) {
+    if (!h || !ms_stage_a || !ms_stage_b) return set_error(DMRG_E_ARG, "null argument");
+    if ((!h->L_dev && h->L.size) || (!h->R_dev && h->R.size))
+        return set_error(DMRG_E_STATE, "dmrg_heff_set_env was not called");
+    cudaStream_t st = h->ctx->stream;
+    cudaEvent_t ev[3];
+    for (auto& e : ev) DMRG_CUDA_TRY(cudaEventCreate(&e));
+    DMRG_CUDA_TRY(cudaEventRecord(ev[0], st));
+    int rc = launch_gemm_f64(h->sa, psi, h->R_dev, h->T.as<double>(), false, st);
+    cudaEventRecord(ev[1], st);
+    if (rc == DMRG_OK) rc = launch_gemm_f64(h->sb, h->L_dev, h->T.as<double>(), out, true, st);
+    cudaEventRecord(ev[2], st);
+    cudaError_t err = cudaEventSynchronize(ev[2]);
+    float a = 0, b = 0;
+    cudaEventElapsedTime(&a, ev[0], ev[1]);
+    cudaEventElapsedTime(&b, ev[1], ev[2]);
+    for (auto& e : ev) cudaEventDestroy(e);
+    if (rc != DMRG_OK) return rc;
+    if (err != cudaSuccess) return set_error(DMRG_E_CUDA, "profile: %s", cudaGetErrorString(err));
+    *ms_stage_a = a;
+    *ms_stage_b = b;
+    return DMRG_OK;
+}
+
+int dmrg_heff_apply_host(dmrg_heff_t h, const double* psi_host, double* out_host, int accumulate) {
+    if (!h) return set_error(DMRG_E_ARG, "null operator");
+    const size_t bytes = (size_t)h->site.ket.size * sizeof(double);
+    DMRG_TRY(h->io_psi.alloc(std::max<size_t>(bytes, 8)));
+    DMRG_TRY(h->io_out.alloc(std::max<size_t>(bytes, 8)));
+    cudaStream_t st = h->ctx->stream;
+    if (bytes) {
+        DMRG_CUDA_TRY(cudaMemcpyAsync(h->io_psi.ptr, psi_host, bytes, cudaMemcpyHostToDevice, st));
+        if (accumulate) DMRG_CUDA_TRY(cudaMemcpyAsync(h->io_out.ptr, out_host, bytes, cudaMemcpyHostToDevice, st));
+    }
+    DMRG_TRY(dmrg_heff_apply(h, h->io_psi.as<double>(), h->io_out.as<double>(), accumulate));
+    if (bytes) DMRG_CUDA_TRY(cudaMemcpyAsync(out_host, h->io_out.ptr, bytes, cudaMemcpyDeviceToHost, st));
+    DMRG_CUDA_TRY(cudaStreamSynchronize(st));
+    return DMRG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,153 @@
+/*
+ * dmrg_b200.h - C ABI of libdmrg_b200, the sm_100a implementation of the
+ * dmrgcc DMRG hot path (block-sparse H_eff*psi, environment updates, Lanczos,
+ * per-sector SVD truncation).
+ *
+ * The reference (jiandong94/dmrgcc) has no FFI: its hot path is reached through
+ * C++ member functions whose numeric work bottoms out in MKL.  Each entry point
+ * below names the reference member it stands in for.  All arguments are plain
+ * pointers and sizes.  Every call returns 0 on success or a negative DMRG_E*
+ * code; dmrg_last_error() gives the message.  No entry point exits the process.
+ *
+ * Storage conventions (identical to the reference's):
+ *   - a block list ("RealMatrixBlock") is an ordered list of dense blocks, each
+ *     row-major, packed back to back in list order (VectorizeMatrixBlock,
+ *     src/tensor/real_matrix_block.cc:173-194).  A site tensor's packed storage
+ *     IS the Lanczos vector;
+ *   - an environment is one block list per MPO bond index, packed index-major;
+ *   - the MPO site tensor W is dense [left_bond][right_bond][d][d] (row p1,
+ *     column p2), as RealTensorOperator::tensor_operator_[l][r](p1, p2).
+ * Device pointers ("_dev") are CUDA global memory on the context's device;
+ * host pointers ("_host") are ordinary (optionally pinned) host memory.
+ */
+#ifndef DMRG_B200_H_
+#define DMRG_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DMRG_OK 0
+#define DMRG_E_ARG (-1)      /* invalid argument / inconsistent block shapes */
+#define DMRG_E_CUDA (-2)     /* a CUDA runtime call failed */
+#define DMRG_E_NOMEM (-3)    /* device allocation failed */
+#define DMRG_E_NUMERIC (-4)  /* an iterative device routine hit its iteration cap */
+#define DMRG_E_STATE (-5)    /* call made in the wrong state */
+
+/* Arithmetic of the block GEMMs.  FP64: plain double.  SPLIT_BF16X3:
+ * tensor-core products of bf16 hi/lo splits with FP32 accumulation. */
+#define DMRG_PREC_FP64 0
+#define DMRG_PREC_BF16X3 1
+
+typedef struct dmrg_ctx_s* dmrg_ctx_t;
+typedef struct dmrg_heff_s* dmrg_heff_t;
+typedef struct dmrg_env_s* dmrg_env_t;
+
+/* Shape of one block list: block k has sector indices (left[k], right[k]) and a
+ * rows[k] x cols[k] row-major matrix.  Stands in for RealMatrixBlock's
+ * left_index_/right_index_/matrix_block_ (src/tensor/real_matrix_block.h:6-40). */
+typedef struct {
+    int nblocks;
+    const int* left;
+    const int* right;
+    const int* rows;
+    const int* cols;
+} dmrg_blocks_t;
+
+/* ---- context --------------------------------------------------------------- */
+const char* dmrg_version(void);
+/* Last error message of this thread (never NULL). */
+const char* dmrg_last_error(void);
+/* Creates a context on CUDA device `device` with its own non-blocking stream. */
+int dmrg_ctx_create(int device, dmrg_ctx_t* out);
+int dmrg_ctx_destroy(dmrg_ctx_t ctx);
+/* Replaces the context's stream (a cudaStream_t passed as void*; NULL = own). */
+int dmrg_ctx_set_stream(dmrg_ctx_t ctx, void* stream);
+void* dmrg_ctx_stream(dmrg_ctx_t ctx);
+int dmrg_ctx_sync(dmrg_ctx_t ctx);
+/* Device memory helpers for callers without their own allocator. */
+int dmrg_malloc(dmrg_ctx_t ctx, size_t bytes, void** dev);
+int dmrg_free(dmrg_ctx_t ctx, void* dev);
+int dmrg_memcpy_h2d(dmrg_ctx_t ctx, void* dst_dev, const void* src_host, size_t bytes);
+int dmrg_memcpy_d2h(dmrg_ctx_t ctx, void* dst_host, const void* src_dev, size_t bytes);
+int dmrg_memset(dmrg_ctx_t ctx, void* dev, int value, size_t bytes);
+/* Seeded synthetic values for benchmarks and tests: dev[i] = element start+i of
+ * the splitmix64 stream seeded with `seed`, mapped to [-1, 1).  No reference
+ * counterpart (the reference draws its random tensors from glibc rand()). */
+int dmrg_fill_uniform(dmrg_ctx_t ctx, double* dev, int64_t n, uint64_t seed, int64_t start);
+/* FP64 throughput of this GPU, measured by a register-only loop of DMMA
+ * (mode 0) or DFMA (mode 1) instructions on all SMs: the roofline denominator
+ * of the FP64 block GEMMs.  No reference counterpart. */
+int dmrg_fp64_peak(dmrg_ctx_t ctx, int mode, int iters, double* tflops);
+
+/* ---- a1: H_eff * psi --------------------------------------------------------
+ * Replaces RealTensorContraction::MultiplyEffectHamilton(RealTensorLattice*,
+ * RealTensorOperator*, double* state)
+ * (src/dmrg/realdmrg/real_tensor_contraction.h:91-92, .cc:1223-1291).
+ *
+ * dmrg_heff_create builds the block-product schedule once per site from the
+ * site tensor's block list `ket` (sector pair of each block and its physics
+ * index physics_index[num_left_sector * num_right_sector], -1 = no block),
+ * the dense MPO tensor W and the block structure of the left environment
+ * L[0..left_bond) and right environment R[0..right_bond) (L blocks are
+ * (bra, ket) sector pairs, R blocks (ket, bra), as in the reference).
+ * precision: DMRG_PREC_*. */
+int dmrg_heff_create(dmrg_ctx_t ctx, int num_left_sector, int num_right_sector,
+                     const int* physics_index, const dmrg_blocks_t* ket, int physics_dim,
+                     int left_bond, int right_bond, const double* W, const dmrg_blocks_t* L,
+                     const dmrg_blocks_t* R, int precision, dmrg_heff_t* out);
+int dmrg_heff_destroy(dmrg_heff_t h);
+/* Number of doubles of the packed site tensor / left env / right env. */
+int dmrg_heff_sizes(dmrg_heff_t h, int64_t* psi_dim, int64_t* left_env_size,
+                    int64_t* right_env_size);
+/* FLOPs of one application: `algorithmic` counts the reference loop's GEMMs
+ * (real_tensor_contraction.cc:1243-1285), `executed` what the schedule runs. */
+int dmrg_heff_flops(dmrg_heff_t h, double* algorithmic, double* executed);
+/* Points the operator at device-resident environments (packed as above).  For
+ * DMRG_PREC_BF16X3 this also splits them into bf16 planes (kept until the next
+ * call).  The pointers must stay valid while the operator is used. */
+int dmrg_heff_set_env(dmrg_heff_t h, const double* L_dev, const double* R_dev);
+/* out_dev (+)= H_eff * psi_dev on the context stream (accumulate != 0 adds into
+ * out_dev like the reference's `state +=`; 0 overwrites).  Asynchronous. */
+int dmrg_heff_apply(dmrg_heff_t h, const double* psi_dev, double* out_dev, int accumulate);
+/* Same with host buffers: copies psi in, applies, copies the result out, and
+ * waits.  This is the drop-in for the reference call on a host `state`. */
+int dmrg_heff_apply_host(dmrg_heff_t h, const double* psi_host, double* out_host, int accumulate);
+/* One accumulating application with CUDA events between its two grouped
+ * launches (K*R products, then L*(KR) sums); waits and returns each launch's
+ * duration in milliseconds.  For roofline accounting; no reference counterpart. */
+int dmrg_heff_profile(dmrg_heff_t h, const double* psi_dev, double* out_dev, double* ms_stage_a,
+                      double* ms_stage_b);
+
+/* ---- a2/a3: environment update ---------------------------------------------
+ * side 0 replaces RealTensorContraction::LeftComputeTensorContraction
+ * (real_tensor_contraction.cc:782-940): env_in = L[0..left_bond) of this site,
+ * result = L[0..right_bond) of the next site.  side 1 replaces
+ * RightComputeTensorContraction (:959-1119): env_in = R[0..right_bond), result =
+ * R[0..left_bond) of the previous site.  The result's block structure (the
+ * reference's zero_flag pass, :797-883 / :974-1060) is decided at create time
+ * and can be read back with dmrg_env_out_blocks. */
+int dmrg_env_create(dmrg_ctx_t ctx, int side, int num_left_sector, int num_right_sector,
+                    const int* physics_index, const dmrg_blocks_t* ket, int physics_dim,
+                    int left_bond, int right_bond, const double* W, const dmrg_blocks_t* env_in,
+                    int precision, dmrg_env_t* out);
+int dmrg_env_destroy(dmrg_env_t e);
+/* Output bond count and total packed size (doubles). */
+int dmrg_env_out_info(dmrg_env_t e, int* out_bond, int64_t* out_size);
+/* Block structure of output bond index o: arrays of capacity `cap`;
+ * *nblocks receives the count. */
+int dmrg_env_out_blocks(dmrg_env_t e, int o, int cap, int* nblocks, int* left, int* right,
+                        int* rows, int* cols);
+int dmrg_env_flops(dmrg_env_t e, double* algorithmic, double* executed);
+/* env_out_dev = updated environment (overwritten).  Asynchronous. */
+int dmrg_env_apply(dmrg_env_t e, const double* ket_dev, const double* env_in_dev,
+                   double* env_out_dev);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DMRG_B200_H_ */

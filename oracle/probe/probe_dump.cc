@@ -1,0 +1,224 @@
+// Test infrastructure: instrumented run of the unmodified reference DMRG.
+//
+// The reference's own sweep (RealTensorRundmrg::Run, src/dmrg/realdmrg/
+// real_tensor_rundmrg.cc:115-245) runs untouched.  The linker's --wrap option
+// routes its calls to four hot-path members through the __wrap_* functions
+// below, which serialise inputs and outputs to .nac files at the requested call
+// indices and then call the real member:
+//   RealTensorLanczos::LanczosMethod              real_tensor_lanczos.cc:14
+//   RealTensorContraction::Left/RightCompute...   real_tensor_contraction.cc:782,959
+//   RealTensorLattice::Left/RightCanonical...     real_tensor_lattice.cc:558,794
+//
+// Usage: probe_dump <input file>
+//   PROBE_OUT=dir          output directory (default ".")
+//   PROBE_HEFF=i,j,...     Lanczos call indices whose H_eff problem is dumped
+//   PROBE_STRUCT_ONLY=1    H_eff dumps carry block structure only (no values)
+//   PROBE_ENV=i,j,...      environment-update call indices to dump
+//   PROBE_CANON=i,j,...    canonicalisation call indices to dump
+//   PROBE_STOP=n           exit(0) right after Lanczos call n
+// Always writes PROBE_OUT/steps.txt: one line per Lanczos call with the site,
+// iteration cap, psi_dim and the energy the reference returned.
+#include "probe_common.h"
+
+using probe::NacWriter;
+
+static RealTensorSpace* g_space = nullptr;
+static RealTensorHamiltonian* g_ham = nullptr;
+static std::string g_out = ".";
+static std::vector<int> g_heff, g_env, g_canon;
+static bool g_struct_only = false;
+static int g_stop = -1;
+static FILE* g_steps = nullptr;
+static int n_lanczos = 0, n_env = 0, n_canon = 0;
+
+static std::vector<int> parse_list(const char* s) {
+    std::vector<int> v;
+    if (!s) return v;
+    std::stringstream ss(s);
+    std::string tok;
+    while (std::getline(ss, tok, ',')) if (!tok.empty()) v.push_back(std::atoi(tok.c_str()));
+    return v;
+}
+static bool wanted(const std::vector<int>& v, int i) {
+    for (int x : v) if (x == i || x == -1) return true;
+    return false;
+}
+static int site_of(RealTensorLattice* t) {
+    for (int i = 0; i < g_space->num_site_; ++i) if (g_space->tensor_lattice_[i] == t) return i;
+    return -1;
+}
+
+static void write_struct_only_block(NacWriter& w, const std::string& p, RealMatrixBlock* b) {
+    std::vector<int> li, ri, rows, cols;
+    int nb = b ? b->num_block_ : 0;
+    for (int k = 0; k < nb; ++k) {
+        li.push_back(b->left_index_[k]);
+        ri.push_back(b->right_index_[k]);
+        rows.push_back(b->matrix_block_[k]->row_);
+        cols.push_back(b->matrix_block_[k]->column_);
+    }
+    w.ints(p + ".left", li);
+    w.ints(p + ".right", ri);
+    w.ints(p + ".rows", rows);
+    w.ints(p + ".cols", cols);
+}
+
+extern "C" {
+void __real__ZN17RealTensorLanczos13LanczosMethodEiiRd(RealTensorLanczos*, int, int, double&);
+void __real__ZN21RealTensorContraction28LeftComputeTensorContractionEP17RealTensorLatticeP18RealTensorOperatorPS_(
+    RealTensorContraction*, RealTensorLattice*, RealTensorOperator*, RealTensorContraction*);
+void __real__ZN21RealTensorContraction29RightComputeTensorContractionEP17RealTensorLatticeP18RealTensorOperatorPS_(
+    RealTensorContraction*, RealTensorLattice*, RealTensorOperator*, RealTensorContraction*);
+void __real__ZN17RealTensorLattice26LeftCanonicalTensorLatticeEid(RealTensorLattice*, int, double);
+void __real__ZN17RealTensorLattice27RightCanonicalTensorLatticeEid(RealTensorLattice*, int, double);
+
+void __wrap__ZN17RealTensorLanczos13LanczosMethodEiiRd(RealTensorLanczos* self, int niter, int site,
+                                                       double& result) {
+    int call = n_lanczos++;
+    RealTensorLattice* lat = self->space_->get_tensor_lattice(site);
+    RealTensorOperator* op = self->hamiltonian_->get_tensor_hamiltonian(site);
+    RealTensorContraction* con = self->network_->get_tensor_contraction(site);
+    int psi_dim = lat->ComputeKetTensorDim();
+    if (wanted(g_heff, call)) {
+        NacWriter w(g_out + "/heff_" + std::to_string(call) + ".nac");
+        w.scalar_i("site", site);
+        w.scalar_i("call", call);
+        w.scalar_i("niter", niter);
+        if (g_struct_only) {
+            w.scalar_i("physics_dim", lat->physics_dim_);
+            w.ints("lattice.left_dim", std::vector<int>(lat->left_dim_, lat->left_dim_ + lat->num_left_block_));
+            w.ints("lattice.right_dim", std::vector<int>(lat->right_dim_, lat->right_dim_ + lat->num_right_block_));
+            std::vector<int> phys;
+            for (int i = 0; i < lat->num_left_block_; ++i)
+                for (int j = 0; j < lat->num_right_block_; ++j) phys.push_back(lat->physics_index_[i][j]);
+            w.ints("lattice.physics_index", phys);
+            write_struct_only_block(w, "lattice.ket", lat->ket_tensor_);
+            probe::write_operator(w, "op", op);
+            w.scalar_i("L.bond", op->left_bond_);
+            for (int o = 0; o < op->left_bond_; ++o)
+                write_struct_only_block(w, "L." + std::to_string(o), con->left_contraction_tensor_[o]);
+            w.scalar_i("R.bond", op->right_bond_);
+            for (int o = 0; o < op->right_bond_; ++o)
+                write_struct_only_block(w, "R." + std::to_string(o), con->right_contraction_tensor_[o]);
+        } else {
+            probe::write_lattice(w, "lattice", lat);
+            probe::write_operator(w, "op", op);
+            probe::write_env(w, "L", con->left_contraction_tensor_, op->left_bond_);
+            probe::write_env(w, "R", con->right_contraction_tensor_, op->right_bond_);
+            std::vector<double> out(psi_dim, 0.0);
+            con->MultiplyEffectHamilton(lat, op, out.data());
+            w.dbls("heff_out", out);
+            if (psi_dim < 400) {
+                std::vector<double> h((size_t)psi_dim * psi_dim, 0.0);
+                con->ComputeEffectHamilton(lat, op, h.data());
+                w.dbls("heff_dense", h);
+            }
+        }
+    }
+    double t0 = GetWallTime();
+    __real__ZN17RealTensorLanczos13LanczosMethodEiiRd(self, niter, site, result);
+    double t1 = GetWallTime();
+    if (wanted(g_heff, call) && !g_struct_only) {
+        NacWriter w(g_out + "/lanczos_" + std::to_string(call) + ".nac");
+        w.scalar_d("energy", result);
+        probe::write_lattice(w, "lattice", lat);
+    }
+    std::fprintf(g_steps, "%d %d %d %d %.15e %.6f\n", call, site, niter, psi_dim, result, t1 - t0);
+    std::fflush(g_steps);
+    if (call == g_stop) std::exit(0);
+}
+
+static void env_common(bool left, RealTensorContraction* self, RealTensorLattice* lat, RealTensorOperator* op,
+                       RealTensorContraction* next) {
+    int call = n_env++;
+    bool dump = wanted(g_env, call);
+    std::string path = g_out + "/env_" + std::to_string(call) + ".nac";
+    NacWriter* w = dump ? new NacWriter(path) : nullptr;
+    if (w) {
+        w->scalar_i("left", left ? 1 : 0);
+        w->scalar_i("site", site_of(lat));
+        probe::write_lattice(*w, "lattice", lat);
+        probe::write_operator(*w, "op", op);
+        if (left) probe::write_env(*w, "env_in", self->left_contraction_tensor_, op->left_bond_);
+        else probe::write_env(*w, "env_in", self->right_contraction_tensor_, op->right_bond_);
+    }
+    if (left)
+        __real__ZN21RealTensorContraction28LeftComputeTensorContractionEP17RealTensorLatticeP18RealTensorOperatorPS_(
+            self, lat, op, next);
+    else
+        __real__ZN21RealTensorContraction29RightComputeTensorContractionEP17RealTensorLatticeP18RealTensorOperatorPS_(
+            self, lat, op, next);
+    if (w) {
+        if (left) probe::write_env(*w, "env_out", next->left_contraction_tensor_, op->right_bond_);
+        else probe::write_env(*w, "env_out", next->right_contraction_tensor_, op->left_bond_);
+        delete w;
+    }
+}
+
+void __wrap__ZN21RealTensorContraction28LeftComputeTensorContractionEP17RealTensorLatticeP18RealTensorOperatorPS_(
+    RealTensorContraction* self, RealTensorLattice* lat, RealTensorOperator* op, RealTensorContraction* next) {
+    env_common(true, self, lat, op, next);
+}
+void __wrap__ZN21RealTensorContraction29RightComputeTensorContractionEP17RealTensorLatticeP18RealTensorOperatorPS_(
+    RealTensorContraction* self, RealTensorLattice* lat, RealTensorOperator* op, RealTensorContraction* next) {
+    env_common(false, self, lat, op, next);
+}
+
+static void canon_common(bool left, RealTensorLattice* self, int max_dim, double canpre) {
+    int call = n_canon++;
+    bool dump = wanted(g_canon, call);
+    NacWriter* w = dump ? new NacWriter(g_out + "/canon_" + std::to_string(call) + ".nac") : nullptr;
+    if (w) {
+        w->scalar_i("left", left ? 1 : 0);
+        w->scalar_i("site", site_of(self));
+        w->scalar_i("max_dim", max_dim);
+        w->scalar_d("canpre", canpre);
+        probe::write_lattice(*w, "before", self);
+    }
+    if (left) __real__ZN17RealTensorLattice26LeftCanonicalTensorLatticeEid(self, max_dim, canpre);
+    else __real__ZN17RealTensorLattice27RightCanonicalTensorLatticeEid(self, max_dim, canpre);
+    if (w) {
+        probe::write_lattice(*w, "after", self);
+        delete w;
+    }
+}
+void __wrap__ZN17RealTensorLattice26LeftCanonicalTensorLatticeEid(RealTensorLattice* self, int m, double c) {
+    canon_common(true, self, m, c);
+}
+void __wrap__ZN17RealTensorLattice27RightCanonicalTensorLatticeEid(RealTensorLattice* self, int m, double c) {
+    canon_common(false, self, m, c);
+}
+}  // extern "C"
+
+int main(int argc, char* argv[]) {
+    if (argc != 2) {
+        std::printf("Usage: %s inputfile\n", argv[0]);
+        return 1;
+    }
+    if (const char* o = std::getenv("PROBE_OUT")) g_out = o;
+    g_heff = parse_list(std::getenv("PROBE_HEFF"));
+    g_env = parse_list(std::getenv("PROBE_ENV"));
+    g_canon = parse_list(std::getenv("PROBE_CANON"));
+    g_struct_only = std::getenv("PROBE_STRUCT_ONLY") != nullptr;
+    if (const char* s = std::getenv("PROBE_STOP")) g_stop = std::atoi(s);
+    g_steps = std::fopen((g_out + "/steps.txt").c_str(), "w");
+
+    auto input = InputGroup(argv[1], "input");
+    int nx = input.getInt("num_site_x");
+    int ny = input.getInt("num_site_y");
+    int nb = input.getInt("num_boson");
+    int d = input.getInt("physics_dim", 2);
+    double flux = input.getDouble("flux");
+    double Jx = input.getDouble("Jx");
+    double Jy = input.getDouble("Jy");
+    double U = input.getDouble("U");
+    double mu = input.getDouble("mu");
+    bool px = input.getBool("period_x");
+    bool py = input.getBool("period_y");
+    g_space = new RealSpinlessBoseSquareSpace(nx, ny, nb, d);
+    g_ham = new RealSpinlessBoseSquareHamiltonian(nx, ny, d, flux * PI, Jx, Jy, U, mu, px, py);
+    RealTensorRundmrg* run = new RealTensorRundmrg(g_space, g_ham, input);
+    run->Run();
+    std::fclose(g_steps);
+    return 0;
+}

@@ -1,0 +1,99 @@
+"""Regenerates the golden fixtures in this directory from the reference itself.
+
+Runs the unmodified reference DMRG, built from its own sources by oracle/Makefile
+(`make -C oracle`), under the instrumented driver oracle/_ref/probe_dump with one
+BLAS thread, on the 16-site Bose-Hubbard chain input (dmrgcc_b200/inputs/
+chain16_spinless.in), and keeps:
+
+  steps_chain16.txt     every Lanczos call: index, site, niter, psi_dim, energy
+  heff_c<k>.nac         an H_eff*psi problem and the reference's output
+  lanczos_c<k>.nac      the energy and ground vector LanczosMethod returned
+  env_c<k>.nac          an environment update, inputs and outputs
+  canon_c<k>.nac        a canonicalisation (SVD truncation), before and after
+  quicksort_cases.txt   inputs with ties and the index order the reference's
+                        QuickSort (src/util/general.ih) returns (probe_sort)
+
+Usage: python tests/golden/make_golden.py [--cylinder]
+  --cylinder additionally dumps the block structure (no values) of the 8x4
+  cylinder at bond dimension 1024, site 16 (minutes of CPU), into
+  heff_struct_cyl8x4_D1024.nac.
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import shutil
+import subprocess
+import sys
+import tempfile
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+PROBE = os.path.join(ROOT, "oracle", "_ref", "probe_dump")
+PROBE_SORT = os.path.join(ROOT, "oracle", "_ref", "probe_sort")
+
+# Lanczos call k of the 16-site chain = half-sweep k // 15, k % 15-th site visited.
+HEFF_CALLS = [20, 158]   # psi_dim 181 (dense H_eff kept) and D=64 mid-chain, site 8
+ENV_CALLS = [173, 187]   # left update site 8 (half-sweep 10), right update site 8 (11)
+CANON_CALLS = [160, 174]  # expansion-on left/right canonicalisation at site 8, D=64
+
+
+def run_probe(inp: str, out: str, env_extra: dict) -> None:
+    env = dict(os.environ, OMP_NUM_THREADS="1", OPENBLAS_NUM_THREADS="1", PROBE_OUT=out, **env_extra)
+    with open(os.path.join(out, "log.txt"), "w") as log:
+        subprocess.run([PROBE, inp], env=env, stdout=log, stderr=subprocess.STDOUT, check=True, cwd=out)
+
+
+def quicksort_cases() -> None:
+    import numpy as np
+
+    rng = np.random.default_rng(7)
+    lines = []
+    for case in range(40):
+        n = int(rng.integers(1, 60))
+        flag = int(case % 2)
+        pool = rng.choice([0.0, 0.125, 0.25, 0.5, 0.75, 1.0, 1e-13], size=int(rng.integers(1, 7)))
+        vals = rng.choice(pool, size=n) if case % 3 else rng.random(n)
+        lines.append(f"{n} {flag} " + " ".join(repr(float(v)) for v in vals))
+    inp = "\n".join(lines) + "\n"
+    r = subprocess.run([PROBE_SORT], input=inp, capture_output=True, text=True, check=True)
+    outs = r.stdout.strip("\n").split("\n")
+    with open(os.path.join(HERE, "quicksort_cases.txt"), "w") as f:
+        for a, b in zip(lines, outs):
+            f.write(a + "\n" + b + "\n")
+
+
+def main() -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--cylinder", action="store_true")
+    args = ap.parse_args()
+    if not (os.path.exists(PROBE) and os.path.exists(PROBE_SORT)):
+        subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "-j8"], check=True)
+    quicksort_cases()
+    tmp = tempfile.mkdtemp(prefix="golden_")
+    inp = os.path.join(ROOT, "dmrgcc_b200", "inputs", "chain16_spinless.in")
+    run_probe(inp, tmp, {
+        "PROBE_HEFF": ",".join(map(str, HEFF_CALLS)),
+        "PROBE_ENV": ",".join(map(str, ENV_CALLS)),
+        "PROBE_CANON": ",".join(map(str, CANON_CALLS)),
+    })
+    shutil.copy(os.path.join(tmp, "steps.txt"), os.path.join(HERE, "steps_chain16.txt"))
+    for kind, calls in (("heff", HEFF_CALLS), ("lanczos", HEFF_CALLS), ("env", ENV_CALLS), ("canon", CANON_CALLS)):
+        for c in calls:
+            shutil.copy(os.path.join(tmp, f"{kind}_{c}.nac"), os.path.join(HERE, f"{kind}_c{c}.nac"))
+    if args.cylinder:
+        tmp2 = tempfile.mkdtemp(prefix="golden_cyl_")
+        inp2 = os.path.join(ROOT, "dmrgcc_b200", "inputs", "cylinder8x4_spinless.in")
+        # Lanczos call 388 = half-sweep 12 (first D=1024 sweep with noise off), site 16.
+        env = {"PROBE_HEFF": "388", "PROBE_STRUCT_ONLY": "1", "PROBE_STOP": "388"}
+        env2 = dict(os.environ, OMP_NUM_THREADS=str(os.cpu_count()), OPENBLAS_NUM_THREADS=str(os.cpu_count()),
+                    PROBE_OUT=tmp2, **env)
+        with open(os.path.join(tmp2, "log.txt"), "w") as log:
+            subprocess.run([PROBE, inp2], env=env2, stdout=log, stderr=subprocess.STDOUT, check=True, cwd=tmp2)
+        shutil.copy(os.path.join(tmp2, "heff_388.nac"), os.path.join(HERE, "heff_struct_cyl8x4_D1024.nac"))
+        shutil.copy(os.path.join(tmp2, "steps.txt"), os.path.join(HERE, "steps_cyl8x4_to_D1024.txt"))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())
