@@ -143,8 +143,12 @@ def run_b200(args) -> None:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
     ctx = capi.Context(local)
-    stream = torch.cuda.current_stream()
+    # A dedicated (non-default) stream shared by torch's events and the library's
+    # launches: the events then bracket exactly the kernels they time.
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     ctx.set_stream(stream.cuda_stream)
+    assert ctx.stream == stream.cuda_stream != 0
 
     step = SiteStep.from_nac(STRUCT)
     prec = {"fp64": capi.DMRG_PREC_FP64, "bf16x3": capi.DMRG_PREC_BF16X3}[args.precision]
@@ -259,8 +263,8 @@ def run_b200(args) -> None:
 def main() -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--precision", choices=["fp64", "bf16x3"], default="fp64")
     ap.add_argument("--cpu-reps", type=int, default=30)

@@ -64,6 +64,7 @@ _SIGS = {
     "dmrg_heff_apply": (C.c_int, [_VP, _VP, _VP, C.c_int]),
     "dmrg_heff_apply_host": (C.c_int, [_VP, _VP, _VP, C.c_int]),
     "dmrg_heff_profile": (C.c_int, [_VP, _VP, _VP, _D, _D]),
+    "dmrg_lanczos": (C.c_int, [_VP, _VP, C.c_int, C.c_double, C.c_double, _D, _I]),
     "dmrg_env_create": (C.c_int, [_VP, C.c_int, C.c_int, C.c_int, _I, C.POINTER(Blocks), C.c_int, C.c_int, C.c_int,
                                   _D, C.POINTER(Blocks), C.c_int, C.POINTER(_VP)]),
     "dmrg_env_destroy": (C.c_int, [_VP]),
@@ -261,6 +262,14 @@ class Heff:
     def apply_host(self, psi: np.ndarray, out: np.ndarray, accumulate: bool = False) -> None:
         check(lib().dmrg_heff_apply_host(self.h, psi.ctypes.data, out.ctypes.data, int(accumulate)),
               "dmrg_heff_apply_host")
+
+    def lanczos(self, psi: DeviceArray, niter: int, precision: float = 1e-15,
+                zero_tol: float = 1e-15) -> tuple[float, int]:
+        """Ground state in place (psi: start vector -> ground vector). Returns (E, dim)."""
+        e, it = C.c_double(), C.c_int()
+        check(lib().dmrg_lanczos(self.h, psi.ptr, niter, precision, zero_tol, C.byref(e), C.byref(it)),
+              "dmrg_lanczos")
+        return e.value, it.value
 
     def close(self) -> None:
         if self.h:

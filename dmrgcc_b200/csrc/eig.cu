@@ -1,0 +1,272 @@
+// Small dense FP64 eigen-solvers on the device (see eig.cuh).
+//
+// Tridiagonal lowest eigenvalue: Sturm sequence counts (number of negative
+// pivots of the LDL^T factorisation of T - xI) evaluated at 128 points per
+// round by one CTA (multisection), starting from the Gershgorin interval.
+// Dense symmetric eigenproblem: two-sided cyclic Jacobi with the round-robin
+// (Brent-Luk) ordering, n/2 disjoint rotations applied per round.
+#include <cfloat>
+
+#include "eig.cuh"
+
+namespace dmrg {
+namespace {
+
+constexpr int kBisectThreads = 128;
+constexpr int kJacobiThreads = 256;
+
+__device__ int sturm_count(const double* alpha, const double* beta, int m, double x, double pivmin) {
+    double d = alpha[0] - x;
+    if (fabs(d) < pivmin) d = -pivmin;
+    int cnt = d < 0.0;
+    for (int k = 1; k < m; ++k) {
+        const double b = beta[k - 1];
+        d = (alpha[k] - x) - b * b / d;
+        if (fabs(d) < pivmin) d = -pivmin;
+        cnt += d < 0.0;
+    }
+    return cnt;
+}
+
+__global__ void __launch_bounds__(kBisectThreads) tridiag_lowest_kernel(const double* __restrict__ alpha,
+                                                                         const double* __restrict__ beta, int m,
+                                                                         double* __restrict__ E, int* state,
+                                                                         double precision, double zero_tol,
+                                                                         int niter) {
+    __shared__ double lo, hi, pivmin;
+    __shared__ int first;
+    if (state[0]) return;  // already converged: later speculative steps are no-ops
+    if (threadIdx.x == 0) {
+        double l = DBL_MAX, h = -DBL_MAX, bmax = 0.0;
+        for (int k = 0; k < m; ++k) {
+            const double r = (k > 0 ? fabs(beta[k - 1]) : 0.0) + (k + 1 < m ? fabs(beta[k]) : 0.0);
+            l = fmin(l, alpha[k] - r);
+            h = fmax(h, alpha[k] + r);
+            if (k + 1 < m) bmax = fmax(bmax, beta[k] * beta[k]);
+        }
+        const double span = fmax(fabs(l), fabs(h));
+        lo = l - 2.0 * DBL_EPSILON * span - DBL_MIN;
+        hi = h + 2.0 * DBL_EPSILON * span + DBL_MIN;
+        pivmin = DBL_MIN * fmax(1.0, bmax);
+    }
+    __syncthreads();
+    for (int round = 0; round < 64; ++round) {
+        const double a = lo, b = hi;
+        if (b - a <= 2.0 * DBL_EPSILON * fmax(fabs(a), fabs(b)) + DBL_MIN) break;
+        if (threadIdx.x == 0) first = kBisectThreads;
+        __syncthreads();
+        const double x = a + (b - a) * (double)(threadIdx.x + 1) / (double)(kBisectThreads + 1);
+        if (sturm_count(alpha, beta, m, x, pivmin) >= 1) atomicMin(&first, (int)threadIdx.x);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const int f = first;
+            const double w = (b - a) / (double)(kBisectThreads + 1);
+            lo = f == 0 ? a : a + w * (double)f;
+            hi = f == kBisectThreads ? b : a + w * (double)(f + 1);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const double lam = 0.5 * (lo + hi);
+        E[m - 1] = lam;
+        const double prev = m >= 2 ? E[m - 2] : 10000.0;  // old_energy starts at 10000 (real_tensor_lanczos.cc:76)
+        if (beta[m - 1] < zero_tol || fabs(lam - prev) < precision || m == niter) {
+            state[0] = 1;
+            state[1] = m;
+        }
+    }
+}
+
+__device__ void round_robin_pair(int r, int i, int N, int& p, int& q) {
+    // Circle method: player 0 fixed, players 1..N-1 rotate.
+    if (i == 0) {
+        p = 0;
+        q = r % (N - 1) + 1;
+    } else {
+        p = (r + i) % (N - 1) + 1;
+        q = (r - i + (N - 1)) % (N - 1) + 1;
+    }
+    if (p > q) {
+        int t = p;
+        p = q;
+        q = t;
+    }
+}
+
+__device__ double block_sum_j(double v, double* sh) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) sh[w] = v;
+    __syncthreads();
+    double r = 0.0;
+    if (threadIdx.x == 0)
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) r += sh[k];
+    __syncthreads();
+    if (threadIdx.x == 0) sh[0] = r;
+    __syncthreads();
+    r = sh[0];
+    __syncthreads();
+    return r;
+}
+
+// Jacobi on A (n x n, global, row-major); Z accumulates the rotations (starts as I).
+// cs: 2*ceil(n/2) doubles, pq: 2*ceil(n/2) ints (shared).
+__device__ bool jacobi_core(double* A, int n, double* Z) {
+    __shared__ double sh[kJacobiThreads / 32];
+    extern __shared__ double dyn[];
+    const int N = n + (n & 1);
+    const int npair = N / 2;
+    double* cs = dyn;                          // [npair][2]
+    int* pq = reinterpret_cast<int*>(dyn + 2 * npair);  // [npair][2]
+    for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) Z[idx] = (idx / n == idx % n) ? 1.0 : 0.0;
+    __syncthreads();
+    if (n <= 1) return true;
+    bool converged = false;
+    for (int sweep = 0; sweep < 60; ++sweep) {
+        double off = 0.0, dia = 0.0;
+        for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
+            const int i = idx / n, j = idx % n;
+            const double v = A[idx];
+            if (i == j) dia += v * v;
+            else off += v * v;
+        }
+        off = block_sum_j(off, sh);
+        dia = block_sum_j(dia, sh);
+        if (off <= 1e-28 * dia || off == 0.0) {  // off-diagonal mass below ~1e-14 of the diagonal
+            converged = true;
+            break;
+        }
+        for (int r = 0; r < N - 1; ++r) {
+            for (int i = threadIdx.x; i < npair; i += blockDim.x) {
+                int p, q;
+                round_robin_pair(r, i, N, p, q);
+                double c = 1.0, s = 0.0;
+                if (q < n) {
+                    const double apq = A[p * n + q];
+                    if (apq != 0.0) {
+                        const double tau = (A[q * n + q] - A[p * n + p]) / (2.0 * apq);
+                        const double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
+                        c = 1.0 / sqrt(1.0 + t * t);
+                        s = t * c;
+                    }
+                }
+                cs[2 * i] = c;
+                cs[2 * i + 1] = s;
+                pq[2 * i] = p;
+                pq[2 * i + 1] = q;
+            }
+            __syncthreads();
+            // rows: A <- J^T A
+            for (int idx = threadIdx.x; idx < npair * n; idx += blockDim.x) {
+                const int i = idx / n, j = idx % n;
+                const int p = pq[2 * i], q = pq[2 * i + 1];
+                const double s = cs[2 * i + 1];
+                if (q >= n || s == 0.0) continue;
+                const double c = cs[2 * i];
+                const double ap = A[p * n + j], aq = A[q * n + j];
+                A[p * n + j] = c * ap - s * aq;
+                A[q * n + j] = s * ap + c * aq;
+            }
+            __syncthreads();
+            // columns: A <- A J, Z <- Z J
+            for (int idx = threadIdx.x; idx < npair * n; idx += blockDim.x) {
+                const int i = idx / n, row = idx % n;
+                const int p = pq[2 * i], q = pq[2 * i + 1];
+                const double s = cs[2 * i + 1];
+                if (q >= n || s == 0.0) continue;
+                const double c = cs[2 * i];
+                const double ap = A[row * n + p], aq = A[row * n + q];
+                A[row * n + p] = c * ap - s * aq;
+                A[row * n + q] = s * ap + c * aq;
+                const double zp = Z[row * n + p], zq = Z[row * n + q];
+                Z[row * n + p] = c * zp - s * zq;
+                Z[row * n + q] = s * zp + c * zq;
+            }
+            __syncthreads();
+        }
+    }
+    return converged;
+}
+
+__global__ void __launch_bounds__(kJacobiThreads) sym_jacobi_kernel(double* A, int n, double* w, double* Zout,
+                                                                    double* ws, int* status) {
+    double* Z = ws;
+    int* order = reinterpret_cast<int*>(ws + (size_t)n * n);
+    const bool ok = jacobi_core(A, n, Z);
+    if (threadIdx.x == 0) {
+        if (!ok) status[0] = DMRG_E_NUMERIC;
+        for (int i = 0; i < n; ++i) order[i] = i;
+        for (int i = 1; i < n; ++i) {  // stable insertion sort by eigenvalue, ascending
+            const int key = order[i];
+            const double kv = A[key * n + key];
+            int j = i - 1;
+            while (j >= 0 && A[order[j] * n + order[j]] > kv) {
+                order[j + 1] = order[j];
+                --j;
+            }
+            order[j + 1] = key;
+        }
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < n; k += blockDim.x) w[k] = A[order[k] * n + order[k]];
+    for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
+        const int i = idx / n, k = idx % n;
+        Zout[idx] = Z[i * n + order[k]];
+    }
+}
+
+__global__ void __launch_bounds__(kJacobiThreads) tridiag_vector_kernel(const double* __restrict__ alpha,
+                                                                        const double* __restrict__ beta,
+                                                                        const int* m_dev, double* y, double* ws,
+                                                                        int* status) {
+    const int n = *m_dev;
+    double* A = ws;
+    double* Z = ws + (size_t)n * n;
+    for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
+        const int i = idx / n, j = idx % n;
+        A[idx] = i == j ? alpha[i] : (j == i + 1 ? beta[i] : (i == j + 1 ? beta[j] : 0.0));
+    }
+    __syncthreads();
+    const bool ok = jacobi_core(A, n, Z);
+    __shared__ int kmin;
+    if (threadIdx.x == 0) {
+        if (!ok) status[0] = DMRG_E_NUMERIC;
+        int best = 0;
+        for (int k = 1; k < n; ++k)
+            if (A[k * n + k] < A[best * n + best]) best = k;
+        kmin = best;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x) y[i] = Z[i * n + kmin];
+}
+
+}  // namespace
+
+int launch_tridiag_lowest(const double* alpha, const double* beta, int m, double* E, int* state, double precision,
+                          double zero_tol, int niter, cudaStream_t st) {
+    tridiag_lowest_kernel<<<1, kBisectThreads, 0, st>>>(alpha, beta, m, E, state, precision, zero_tol, niter);
+    DMRG_CUDA_TRY(cudaGetLastError());
+    return DMRG_OK;
+}
+
+static size_t jacobi_smem(int n) {
+    const int npair = (n + (n & 1)) / 2;
+    return (size_t)npair * 2 * sizeof(double) + (size_t)npair * 2 * sizeof(int);
+}
+
+int launch_sym_jacobi(double* A, int n, double* w, double* Z, double* ws, int* status, cudaStream_t st) {
+    if (n <= 0) return DMRG_OK;
+    sym_jacobi_kernel<<<1, kJacobiThreads, jacobi_smem(n), st>>>(A, n, w, Z, ws, status);
+    DMRG_CUDA_TRY(cudaGetLastError());
+    return DMRG_OK;
+}
+
+int launch_tridiag_ground_vector(const double* alpha, const double* beta, const int* m_dev, int m_max, double* y,
+                                 double* ws, int* status, cudaStream_t st) {
+    tridiag_vector_kernel<<<1, kJacobiThreads, jacobi_smem(m_max), st>>>(alpha, beta, m_dev, y, ws, status);
+    DMRG_CUDA_TRY(cudaGetLastError());
+    return DMRG_OK;
+}
+
+}  // namespace dmrg

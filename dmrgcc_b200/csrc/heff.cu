@@ -13,24 +13,11 @@
 //            (W, L block, T) terms, summed in registers by the tile owner.
 #include <algorithm>
 
-#include "blocksparse.h"
-#include "gemm.cuh"
+#include "heff.cuh"
 
 using namespace dmrg;
 
-struct dmrg_heff_s {
-    dmrg_ctx_t ctx = nullptr;
-    int precision = DMRG_PREC_FP64;
-    SiteDesc site;
-    EnvDesc L, R;
-    GemmSchedule sa, sb;  // A: psi x R -> T ; B: L x T -> out
-    DeviceBuffer T;
-    int64_t t_size = 0;
-    const double* L_dev = nullptr;
-    const double* R_dev = nullptr;
-    double flops_alg = 0, flops_exec = 0;
-    DeviceBuffer io_psi, io_out;  // staging for dmrg_heff_apply_host
-};
+
 
 namespace {
 
@@ -145,6 +132,17 @@ int build_heff(dmrg_heff_s& h) {
 
 }  // namespace
 
+int dmrg::heff_apply_internal(dmrg_heff_s& h, const double* psi, double* out, bool accumulate) {
+    if ((!h.L_dev && h.L.size) || (!h.R_dev && h.R.size))
+        return set_error(DMRG_E_STATE, "dmrg_heff_set_env was not called");
+    cudaStream_t st = h.ctx->stream;
+    if (!accumulate && h.site.ket.size)
+        DMRG_CUDA_TRY(cudaMemsetAsync(out, 0, (size_t)h.site.ket.size * sizeof(double), st));
+    DMRG_TRY(launch_gemm_f64(h.sa, psi, h.R_dev, h.T.as<double>(), false, st));
+    DMRG_TRY(launch_gemm_f64(h.sb, h.L_dev, h.T.as<double>(), out, true, st));
+    return DMRG_OK;
+}
+
 extern "C" {
 
 int dmrg_heff_create(dmrg_ctx_t ctx, int nl, int nr, const int* phys, const dmrg_blocks_t* ket, int d, int lb,
@@ -200,14 +198,7 @@ int dmrg_heff_set_env(dmrg_heff_t h, const double* L_dev, const double* R_dev) {
 
 int dmrg_heff_apply(dmrg_heff_t h, const double* psi, double* out, int accumulate) {
     if (!h) return set_error(DMRG_E_ARG, "null operator");
-    if ((!h->L_dev && h->L.size) || (!h->R_dev && h->R.size))
-        return set_error(DMRG_E_STATE, "dmrg_heff_set_env was not called");
-    cudaStream_t st = h->ctx->stream;
-    if (!accumulate && h->site.ket.size)
-        DMRG_CUDA_TRY(cudaMemsetAsync(out, 0, (size_t)h->site.ket.size * sizeof(double), st));
-    DMRG_TRY(launch_gemm_f64(h->sa, psi, h->R_dev, h->T.as<double>(), false, st));
-    DMRG_TRY(launch_gemm_f64(h->sb, h->L_dev, h->T.as<double>(), out, true, st));
-    return DMRG_OK;
+    return heff_apply_internal(*h, psi, out, accumulate != 0);
 }
 
 int dmrg_heff_profile(dmrg_heff_t h, const double* psi, double* out, double* ms_stage_a, double* ms_stage_b) {

@@ -1,0 +1,31 @@
+// Internal definition of the H_eff operator object (shared by heff.cu and the
+// Lanczos solver).
+#pragma once
+
+#include "blocksparse.h"
+#include "gemm.cuh"
+
+namespace dmrg {
+struct LanczosWork;
+}
+
+struct dmrg_heff_s {
+    dmrg_ctx_t ctx = nullptr;
+    int precision = DMRG_PREC_FP64;
+    dmrg::SiteDesc site;
+    dmrg::EnvDesc L, R;
+    dmrg::GemmSchedule sa, sb;  // A: psi x R -> T ; B: L x T -> out
+    dmrg::DeviceBuffer T;
+    int64_t t_size = 0;
+    const double* L_dev = nullptr;
+    const double* R_dev = nullptr;
+    double flops_alg = 0, flops_exec = 0;
+    dmrg::DeviceBuffer io_psi, io_out;  // staging for dmrg_heff_apply_host
+    dmrg::LanczosWork* lw = nullptr;  // Lanczos workspace, allocated on first use
+    ~dmrg_heff_s();
+};
+
+namespace dmrg {
+// out (+)= H_eff psi on the context stream.
+int heff_apply_internal(dmrg_heff_s& h, const double* psi, double* out, bool accumulate);
+}  // namespace dmrg

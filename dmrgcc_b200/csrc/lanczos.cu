@@ -1,0 +1,169 @@
+// a4/a5: the Lanczos eigensolver of one site step, on the device.
+//
+// Follows RealTensorLanczos::LanczosMethod (src/dmrg/realdmrg/
+// real_tensor_lanczos.cc:14-201):
+//   h starts at 0;  per iteration i:  h += H v_i;  alpha_i = <v_i|h>;
+//   h -= alpha_i v_i;  beta_i = ||h||;  lowest eigenvalue E_i of the tridiagonal;
+//   stop when beta_i < zero_tol, |E_i - E_{i-1}| < precision or i+1 == niter;
+//   else v_{i+1} = h / beta_i, h = -beta_i v_i, v_{i+1} orthogonalised against
+//   v_0..v_i and normalised;  ground vector = sum_k y_k v_k.
+// Differences by design: the reorthogonalisation is classical Gram-Schmidt
+// applied twice (two multi-dot/update launch pairs) instead of one modified
+// Gram-Schmidt pass (2(i+1) dependent launches); the tridiagonal's lowest
+// eigenvalue comes from Sturm bisection on the device instead of dsyevd.
+// psi_dim < 100 takes the reference's exact-diagonalisation branch (:34-56):
+// the dense H_eff is assembled column by column from matvecs on unit vectors
+// and diagonalised by a device Jacobi solver.
+#include <algorithm>
+
+#include "eig.cuh"
+#include "heff.cuh"
+#include "vec.cuh"
+
+namespace dmrg {
+
+struct LanczosWork {
+    int niter = 0;
+    int64_t n = 0;
+    DeviceBuffer V, h, scal, state, jac, y, dense;
+    ReduceScratch rs;
+    int* h_state = nullptr;  // pinned: [done, dim]
+    ~LanczosWork() {
+        if (h_state) cudaFreeHost(h_state);
+    }
+};
+
+}  // namespace dmrg
+
+using namespace dmrg;
+
+dmrg_heff_s::~dmrg_heff_s() { delete lw; }
+
+namespace {
+
+__global__ void unit_vector_kernel(double* x, int64_t n, int64_t c) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        x[i] = i == c ? 1.0 : 0.0;
+}
+
+// A[r][c] = H[r][c] taken from the upper triangle (the reference diagonalises with
+// uplo='U' on the row-major H, general.cc:47-64); cols[c*n + r] = (H e_c)[r].
+__global__ void symmetrize_upper_kernel(const double* __restrict__ cols, double* __restrict__ A, int n) {
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n * n; idx += gridDim.x * blockDim.x) {
+        const int r = idx / n, c = idx % n;
+        A[idx] = r <= c ? cols[(int64_t)c * n + r] : cols[(int64_t)r * n + c];
+    }
+}
+
+__global__ void column_copy_kernel(const double* __restrict__ Z, int n, double* __restrict__ out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = Z[i * n];
+}
+
+int ensure_work(dmrg_heff_s& h, int niter) {
+    if (!h.lw) h.lw = new LanczosWork();
+    LanczosWork& w = *h.lw;
+    const int64_t n = h.site.ket.size;
+    if (w.niter < niter || w.n != n) {
+        DMRG_TRY(w.V.alloc((size_t)std::max(niter, 1) * std::max<int64_t>(n, 1) * sizeof(double)));
+        DMRG_TRY(w.h.alloc((size_t)std::max<int64_t>(n, 1) * sizeof(double)));
+        DMRG_TRY(w.scal.alloc((size_t)(4 * std::max(niter, 1) + 16) * sizeof(double)));
+        DMRG_TRY(w.y.alloc((size_t)std::max(niter, 1) * sizeof(double)));
+        const int m = std::max(niter, 128);
+        DMRG_TRY(w.jac.alloc((size_t)(2 * m * m + 4 * m) * sizeof(double)));
+        w.niter = niter;
+        w.n = n;
+    }
+    DMRG_TRY(w.state.alloc(16 * sizeof(int)));
+    DMRG_TRY(w.rs.alloc(std::max(2 * h.ctx->num_sms, 64), std::max(niter, 1)));
+    if (!w.h_state) DMRG_CUDA_TRY(cudaMallocHost(&w.h_state, 16 * sizeof(int)));
+    return DMRG_OK;
+}
+
+int run_exact(dmrg_heff_s& h, double* psi, double* energy) {
+    LanczosWork& w = *h.lw;
+    const int n = (int)h.site.ket.size;
+    cudaStream_t st = h.ctx->stream;
+    DMRG_TRY(w.dense.alloc((size_t)(3 * n * n + 4 * n + 8) * sizeof(double)));
+    double* cols = w.dense.as<double>();
+    double* A = cols + (size_t)n * n;
+    double* Z = A + (size_t)n * n;
+    double* ev = Z + (size_t)n * n;
+    double* e = w.h.as<double>();
+    for (int c = 0; c < n; ++c) {
+        unit_vector_kernel<<<1, 128, 0, st>>>(e, n, c);
+        DMRG_TRY(heff_apply_internal(h, e, cols + (size_t)c * n, false));
+    }
+    symmetrize_upper_kernel<<<std::max(1, (n * n + 255) / 256), 256, 0, st>>>(cols, A, n);
+    DMRG_CUDA_TRY(cudaMemsetAsync(w.state.ptr, 0, 16 * sizeof(int), st));
+    DMRG_TRY(launch_sym_jacobi(A, n, ev, Z, w.jac.as<double>(), w.state.as<int>() + 2, st));
+    column_copy_kernel<<<1, 128, 0, st>>>(Z, n, psi);
+    double e0 = 0.0;
+    DMRG_CUDA_TRY(cudaMemcpyAsync(&e0, ev, sizeof(double), cudaMemcpyDeviceToHost, st));
+    DMRG_CUDA_TRY(cudaMemcpyAsync(w.h_state, w.state.ptr, 4 * sizeof(int), cudaMemcpyDeviceToHost, st));
+    DMRG_CUDA_TRY(cudaStreamSynchronize(st));
+    if (w.h_state[2] != 0) return set_error(DMRG_E_NUMERIC, "Jacobi eigensolver did not converge (n=%d)", n);
+    *energy = e0;
+    return DMRG_OK;
+}
+
+}  // namespace
+
+extern "C" int dmrg_lanczos(dmrg_heff_t hp, double* psi, int niter, double precision, double zero_tol,
+                            double* energy, int* iters) {
+    if (!hp || !psi || !energy || niter <= 0) return set_error(DMRG_E_ARG, "invalid Lanczos arguments");
+    if (niter > kMaxVec) return set_error(DMRG_E_ARG, "niter %d above %d", niter, kMaxVec);
+    dmrg_heff_s& h = *hp;
+    DMRG_TRY(ensure_work(h, niter));
+    LanczosWork& w = *h.lw;
+    const int64_t n = h.site.ket.size;
+    cudaStream_t st = h.ctx->stream;
+    if (n < 100) {  // exact diagonalisation branch (real_tensor_lanczos.cc:34)
+        if (iters) *iters = 0;
+        return run_exact(h, psi, energy);
+    }
+    const int blocks = std::min<int64_t>((n + kVecThreads - 1) / kVecThreads, 2 * h.ctx->num_sms);
+    double* V = w.V.as<double>();
+    double* hv = w.h.as<double>();
+    double* alpha = w.scal.as<double>();
+    double* beta = alpha + niter;
+    double* E = beta + niter;
+    double* c = E + niter;
+    double* tmp = c + niter;
+    int* state = w.state.as<int>();
+    DMRG_CUDA_TRY(cudaMemcpyAsync(V, psi, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    DMRG_CUDA_TRY(cudaMemsetAsync(hv, 0, n * sizeof(double), st));
+    DMRG_CUDA_TRY(cudaMemsetAsync(state, 0, 16 * sizeof(int), st));
+    int dim = 0;
+    for (int i = 0; i < niter; ++i) {
+        double* vi = V + (int64_t)i * n;
+        DMRG_TRY(heff_apply_internal(h, vi, hv, true));
+        DMRG_TRY(vec_dot(vi, hv, n, alpha + i, w.rs, blocks, st));
+        DMRG_TRY(vec_axpy_norm(alpha + i, vi, hv, n, beta + i, w.rs, blocks, st));
+        DMRG_TRY(launch_tridiag_lowest(alpha, beta, i + 1, E, state, precision, zero_tol, niter, st));
+        DMRG_CUDA_TRY(cudaMemcpyAsync(w.h_state, state, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
+        DMRG_CUDA_TRY(cudaStreamSynchronize(st));
+        if (w.h_state[0]) {
+            dim = w.h_state[1];
+            break;
+        }
+        double* vn = V + (int64_t)(i + 1) * n;
+        DMRG_TRY(vec_lanczos_shift(beta + i, vi, hv, vn, n, blocks, st));
+        for (int pass = 0; pass < 2; ++pass) {
+            DMRG_TRY(vec_multidot(V, n, i + 1, vn, n, c, w.rs, blocks, st));
+            DMRG_TRY(vec_combine(V, n, i + 1, c, -1.0, vn, 1.0, n, blocks, st));
+        }
+        DMRG_TRY(vec_normalize(vn, n, tmp, w.rs, blocks, st));
+    }
+    if (dim <= 0) return set_error(DMRG_E_NUMERIC, "Lanczos ended without a converged dimension");
+    DMRG_TRY(launch_tridiag_ground_vector(alpha, beta, state + 1, dim, w.y.as<double>(), w.jac.as<double>(),
+                                          state + 2, st));
+    DMRG_TRY(vec_combine(V, n, dim, w.y.as<double>(), 1.0, psi, 0.0, n, blocks, st));
+    double e = 0.0;
+    DMRG_CUDA_TRY(cudaMemcpyAsync(&e, E + dim - 1, sizeof(double), cudaMemcpyDeviceToHost, st));
+    DMRG_CUDA_TRY(cudaMemcpyAsync(w.h_state, state, 4 * sizeof(int), cudaMemcpyDeviceToHost, st));
+    DMRG_CUDA_TRY(cudaStreamSynchronize(st));
+    if (w.h_state[2] != 0) return set_error(DMRG_E_NUMERIC, "tridiagonal Jacobi did not converge (m=%d)", dim);
+    *energy = e;
+    if (iters) *iters = dim;
+    return DMRG_OK;
+}

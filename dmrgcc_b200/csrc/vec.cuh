@@ -1,0 +1,40 @@
+// FP64 vector kernels for the Lanczos recurrence and reorthogonalisation.
+// All reductions are deterministic: fixed per-block slices, partials reduced
+// in index order by the last block to finish (atomic ticket).
+#pragma once
+
+#include "common.cuh"
+
+namespace dmrg {
+
+constexpr int kVecThreads = 256;
+
+// Scratch shared by the reductions of one context/solver.
+struct ReduceScratch {
+    DeviceBuffer partial;  // doubles, >= kMaxBlocks * kMaxVec
+    DeviceBuffer ticket;   // unsigned counters
+    int max_blocks = 0;
+    int alloc(int blocks, int max_vectors);
+};
+
+// out[0] = <x, y>
+int vec_dot(const double* x, const double* y, int64_t n, double* out, ReduceScratch& rs, int blocks,
+            cudaStream_t st);
+// y -= (*alpha) * x ; out[0] = sqrt(||y||^2)
+int vec_axpy_norm(const double* alpha, const double* x, double* y, int64_t n, double* out, ReduceScratch& rs,
+                  int blocks, cudaStream_t st);
+// c[k] = <V_k, w> for k < m   (V row-major m x n, leading dim ldv)
+int vec_multidot(const double* V, int64_t ldv, int m, const double* w, int64_t n, double* c, ReduceScratch& rs,
+                 int blocks, cudaStream_t st);
+// w = beta_w * w + sign * sum_k c[k] V_k   (c on the device, m <= kMaxVec)
+int vec_combine(const double* V, int64_t ldv, int m, const double* c, double sign, double* w, double beta_w,
+                int64_t n, int blocks, cudaStream_t st);
+// Lanczos step: v_next = h / beta ; h = -beta * v_cur   (beta on the device)
+int vec_lanczos_shift(const double* beta, const double* v_cur, double* h, double* v_next, int64_t n, int blocks,
+                      cudaStream_t st);
+// x /= ||x|| (two kernels: norm then scale); norm written to out[0]
+int vec_normalize(double* x, int64_t n, double* out, ReduceScratch& rs, int blocks, cudaStream_t st);
+
+constexpr int kMaxVec = 512;
+
+}  // namespace dmrg

@@ -122,6 +122,18 @@ int dmrg_heff_apply_host(dmrg_heff_t h, const double* psi_host, double* out_host
 int dmrg_heff_profile(dmrg_heff_t h, const double* psi_dev, double* out_dev, double* ms_stage_a,
                       double* ms_stage_b);
 
+/* ---- a4/a5: Lanczos ground state of H_eff ----------------------------------
+ * Replaces RealTensorLanczos::LanczosMethod(int num_iter, int site, double& result)
+ * (src/dmrg/realdmrg/real_tensor_lanczos.h:23, .cc:14-201).  psi_dev holds the
+ * start vector (the site tensor, packed; used as is, like the reference) and
+ * receives the ground vector.  Stops like the reference: beta < zero_tol,
+ * |E_i - E_{i-1}| < precision (the reference hard-codes both at 1e-15), or
+ * niter iterations.  psi_dim < 100 uses the reference's dense exact
+ * diagonalisation branch (.cc:34-56).  *iters = Krylov dimension (0 for the
+ * dense branch).  niter <= 512.  Synchronous. */
+int dmrg_lanczos(dmrg_heff_t h, double* psi_dev, int niter, double precision, double zero_tol,
+                 double* energy, int* iters);
+
 /* ---- a2/a3: environment update ---------------------------------------------
  * side 0 replaces RealTensorContraction::LeftComputeTensorContraction
  * (real_tensor_contraction.cc:782-940): env_in = L[0..left_bond) of this site,

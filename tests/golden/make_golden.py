@@ -33,7 +33,7 @@ PROBE = os.path.join(ROOT, "oracle", "_ref", "probe_dump")
 PROBE_SORT = os.path.join(ROOT, "oracle", "_ref", "probe_sort")
 
 # Lanczos call k of the 16-site chain = half-sweep k // 15, k % 15-th site visited.
-HEFF_CALLS = [20, 158]   # psi_dim 181 (dense H_eff kept) and D=64 mid-chain, site 8
+HEFF_CALLS = [20, 59, 158]  # psi_dim 181 (dense H_eff kept), 86 (dense ED branch), D=64 site 8
 ENV_CALLS = [173, 187]   # left update site 8 (half-sweep 10), right update site 8 (11)
 CANON_CALLS = [160, 174]  # expansion-on left/right canonicalisation at site 8, D=64
 
