@@ -65,6 +65,15 @@ _SIGS = {
     "dmrg_heff_apply_host": (C.c_int, [_VP, _VP, _VP, C.c_int]),
     "dmrg_heff_profile": (C.c_int, [_VP, _VP, _VP, _D, _D]),
     "dmrg_lanczos": (C.c_int, [_VP, _VP, C.c_int, C.c_double, C.c_double, _D, _I]),
+    "dmrg_canon_create": (C.c_int, [_VP, C.c_int, C.c_int, C.c_int, _I, _I, C.POINTER(Blocks), C.POINTER(_VP)]),
+    "dmrg_canon_destroy": (C.c_int, [_VP]),
+    "dmrg_canon_run": (C.c_int, [_VP, _VP, C.c_int, C.c_double, _I, _D]),
+    "dmrg_canon_out_info": (C.c_int, [_VP, _I64, _I64, _I]),
+    "dmrg_canon_out_blocks": (C.c_int, [_VP, _I, _I, _I, _I, _I]),
+    "dmrg_canon_singular_values": (C.c_int, [_VP, C.c_int, C.c_int, _D, _I]),
+    "dmrg_canon_write": (C.c_int, [_VP, _VP, _VP, _VP]),
+    "dmrg_quicksort_index": (C.c_int, [_D, _I, C.c_int, C.c_int]),
+    "dmrg_truncate_dims": (C.c_int, [C.c_int, _I, _D, C.c_int, C.c_double, _I]),
     "dmrg_env_create": (C.c_int, [_VP, C.c_int, C.c_int, C.c_int, _I, C.POINTER(Blocks), C.c_int, C.c_int, C.c_int,
                                   _D, C.POINTER(Blocks), C.c_int, C.POINTER(_VP)]),
     "dmrg_env_destroy": (C.c_int, [_VP]),
@@ -328,3 +337,77 @@ class Env:
             self.close()
         except Exception:
             pass
+
+
+class Canonical:
+    """Per-sector SVD canonicalisation (Left/RightCanonicalTensorLattice)."""
+
+    def __init__(self, ctx: Context, side: int, left_dim, right_dim, ket: BlockSpec):
+        self.ctx, self.side, self.ket = ctx, side, ket
+        self.left_dim = np.ascontiguousarray(left_dim, dtype=np.int32)
+        self.right_dim = np.ascontiguousarray(right_dim, dtype=np.int32)
+        kb = ket.c()
+        h = _VP()
+        check(lib().dmrg_canon_create(ctx.h, side, len(self.left_dim), len(self.right_dim), _iptr(self.left_dim),
+                                      _iptr(self.right_dim), C.byref(kb), C.byref(h)), "dmrg_canon_create")
+        self.h = h
+        self.nsec = len(self.right_dim) if side == 0 else len(self.left_dim)
+
+    def run(self, ket_dev: DeviceArray, max_dim: int, canpre: float):
+        t = np.zeros(self.nsec, dtype=np.int32)
+        d = C.c_double()
+        check(lib().dmrg_canon_run(self.h, ket_dev.ptr, max_dim, canpre, _iptr(t), C.byref(d)), "dmrg_canon_run")
+        ks, cs, sw = C.c_int64(), C.c_int64(), C.c_int()
+        check(lib().dmrg_canon_out_info(self.h, C.byref(ks), C.byref(cs), C.byref(sw)), "dmrg_canon_out_info")
+        n = len(self.ket.left)
+        kr, kc = np.zeros(max(n, 1), np.int32), np.zeros(max(n, 1), np.int32)
+        cr, cc, md = (np.zeros(self.nsec, np.int32) for _ in range(3))
+        check(lib().dmrg_canon_out_blocks(self.h, _iptr(kr), _iptr(kc), _iptr(cr), _iptr(cc), _iptr(md)),
+              "dmrg_canon_out_blocks")
+        return {"tdim": t, "discarded": d.value, "ket_size": ks.value, "canonical_size": cs.value,
+                "sweeps": sw.value, "ket_rows": kr[:n], "ket_cols": kc[:n], "canon_rows": cr, "canon_cols": cc,
+                "match_dim": md}
+
+    def singular_values(self, sector: int) -> np.ndarray:
+        n = C.c_int()
+        check(lib().dmrg_canon_singular_values(self.h, sector, 0, None, C.byref(n)), "singular_values")
+        out = np.zeros(max(n.value, 1))
+        check(lib().dmrg_canon_singular_values(self.h, sector, n.value, _dptr(out), C.byref(n)), "singular_values")
+        return out[:n.value]
+
+    def write(self, ket_dev: DeviceArray, new_ket: DeviceArray, canonical: DeviceArray) -> None:
+        check(lib().dmrg_canon_write(self.h, ket_dev.ptr, new_ket.ptr, canonical.ptr), "dmrg_canon_write")
+
+    def close(self) -> None:
+        if self.h:
+            lib().dmrg_canon_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def quicksort_index(values, descending: bool = True):
+    """The reference's QuickSort with index, run by the library's host code."""
+    v = np.ascontiguousarray(values, dtype=np.float64).copy()
+    idx = np.arange(len(v), dtype=np.int32)
+    check(lib().dmrg_quicksort_index(_dptr(v), _iptr(idx), len(v), int(descending)), "dmrg_quicksort_index")
+    return v, idx
+
+
+def truncate_dims(svals, max_dim: int, canpre: float):
+    """ComputeTruncateDim through the library (host bookkeeping)."""
+    counts = np.array([len(s) for s in svals], dtype=np.int32)
+    flat = np.ascontiguousarray(np.concatenate([np.asarray(s, dtype=np.float64) for s in svals])
+                                if len(svals) else np.zeros(0))
+    t = np.zeros(max(len(svals), 1), dtype=np.int32)
+    check(lib().dmrg_truncate_dims(len(svals), _iptr(counts), _dptr(flat), max_dim, canpre, _iptr(t)),
+          "dmrg_truncate_dims")
+    out, pos = [], 0
+    for c in counts:
+        out.append(flat[pos:pos + c].copy())
+        pos += c
+    return t[:len(svals)], out

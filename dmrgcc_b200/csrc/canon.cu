@@ -1,0 +1,376 @@
+// a6/a7: canonicalisation of a site tensor by per-sector SVD and truncation.
+//
+// Left (RealTensorLattice::LeftCanonicalTensorLattice, src/dmrg/realdmrg/
+// real_tensor_lattice.cc:558-676): for every right sector r the blocks K(l, r)
+// are stacked vertically (list order) into A_r (sum of rows x right_dim[r]),
+// A_r = U S V^T; the truncation keeps t_r values (ComputeTruncateDim, :501-555,
+// on the host with the reference's QuickSort); K(l, r) <- its rows of U[:, :t_r];
+// canonical[r] = diag(S[:t_r]) V^T[:t_r, :]; right_dim[r] <- t_r.
+// Right (:794-911) mirrors it: blocks K(l, .) stacked horizontally into
+// A_l (left_dim[l] x sum of cols), K(l, r) <- its columns of V^T[:t_l, :],
+// canonical[l] = U[:, :t_l] diag(S[:t_l]); left_dim[l] <- t_l.
+// Sectors without rows (left) / columns (right) keep the reference's special
+// case: one singular value 0, a zero canonical block, the ket untouched.
+#include <algorithm>
+#include <numeric>
+
+#include "blocksparse.h"
+#include "svd.cuh"
+#include "truncate.h"
+
+using namespace dmrg;
+
+namespace {
+
+struct CopyTask {
+    int64_t blk_off;  // ket block offset
+    int rows, cols;   // ket block shape
+    int problem;      // svd problem index
+    int off;          // row0 (left) or col0 (right) inside the stacked sector matrix
+};
+
+struct WriteTask {
+    int64_t out_off;  // new ket block offset
+    int rows, cols;   // new ket block shape
+    int problem;
+    int off;          // row0 / col0
+};
+
+struct CanonTask {
+    int64_t out_off;
+    int rows, cols;   // canonical block shape
+    int problem;      // -1: zero block
+    int64_t sig_off;  // offset of the forced singular values of this sector
+};
+
+// gather: stacked A (m x n) into W (column-major; W = A or W = A^T)
+__global__ void gather_kernel(const double* __restrict__ ket, const CopyTask* __restrict__ tasks,
+                              const SvdProblem* __restrict__ probs, double* __restrict__ W, int side) {
+    const CopyTask t = tasks[blockIdx.x];
+    const SvdProblem p = probs[t.problem];
+    const double* src = ket + t.blk_off;
+    double* w = W + p.w_off;
+    const int64_t total = (int64_t)t.rows * t.cols;
+    for (int64_t e = threadIdx.x; e < total; e += blockDim.x) {
+        const int i = (int)(e / t.cols), j = (int)(e % t.cols);
+        const int ai = side == 0 ? t.off + i : i;  // row in A
+        const int aj = side == 0 ? j : t.off + j;  // column in A
+        if (ai >= p.m || aj >= p.n) continue;
+        const int64_t dst = p.transposed ? (int64_t)ai * p.n + aj : (int64_t)aj * p.m + ai;
+        w[dst] = src[e];
+    }
+}
+
+// new ket blocks: left -> rows of U[:, :t]; right -> columns of V^T[:t, :]
+__global__ void write_ket_kernel(const WriteTask* __restrict__ tasks, const SvdProblem* __restrict__ probs,
+                                 const double* __restrict__ W, const double* __restrict__ Q,
+                                 const double* __restrict__ sig, const int* __restrict__ perm,
+                                 double* __restrict__ out, int side) {
+    const WriteTask t = tasks[blockIdx.x];
+    const SvdProblem p = probs[t.problem];
+    const double* w = W + p.w_off;
+    const double* q = Q + p.q_off;
+    const int64_t total = (int64_t)t.rows * t.cols;
+    for (int64_t e = threadIdx.x; e < total; e += blockDim.x) {
+        const int i = (int)(e / t.cols), j = (int)(e % t.cols);
+        double v;
+        if (side == 0) {  // U[row0 + i][j]
+            const int k = perm[p.perm_off + j];
+            const int row = t.off + i;
+            if (!p.transposed) {
+                const double s = sig[p.s_off + j];
+                v = s > 0.0 ? w[(int64_t)k * p.m + row] / s : 0.0;
+            } else {
+                v = q[(int64_t)k * p.m + row];
+            }
+        } else {  // V^T[i][col0 + j] = v_i[col0 + j]
+            const int k = perm[p.perm_off + i];
+            const int col = t.off + j;
+            if (!p.transposed) {
+                v = q[(int64_t)k * p.n + col];
+            } else {
+                const double s = sig[p.s_off + i];
+                v = s > 0.0 ? w[(int64_t)k * p.n + col] / s : 0.0;
+            }
+        }
+        out[t.out_off + e] = v;
+    }
+}
+
+// canonical blocks: left -> diag(s_forced) V^T[:t, :] (t x n); right -> U[:, :t] diag(s_forced) (m x t)
+__global__ void write_canonical_kernel(const CanonTask* __restrict__ tasks, const SvdProblem* __restrict__ probs,
+                                       const double* __restrict__ W, const double* __restrict__ Q,
+                                       const double* __restrict__ sig, const int* __restrict__ perm,
+                                       const double* __restrict__ forced, double* __restrict__ out, int side) {
+    const CanonTask t = tasks[blockIdx.x];
+    const int64_t total = (int64_t)t.rows * t.cols;
+    if (t.problem < 0) {
+        for (int64_t e = threadIdx.x; e < total; e += blockDim.x) out[t.out_off + e] = 0.0;
+        return;
+    }
+    const SvdProblem p = probs[t.problem];
+    const double* w = W + p.w_off;
+    const double* q = Q + p.q_off;
+    for (int64_t e = threadIdx.x; e < total; e += blockDim.x) {
+        const int i = (int)(e / t.cols), j = (int)(e % t.cols);
+        double v;
+        if (side == 0) {  // s_i * v_i[j]
+            const int k = perm[p.perm_off + i];
+            const double sf = forced[t.sig_off + i];
+            if (!p.transposed) {
+                v = sf * q[(int64_t)k * p.n + j];
+            } else {
+                const double s = sig[p.s_off + i];
+                v = s > 0.0 ? sf * w[(int64_t)k * p.n + j] / s : 0.0;
+            }
+        } else {  // u_j[i] * s_j
+            const int k = perm[p.perm_off + j];
+            const double sf = forced[t.sig_off + j];
+            if (!p.transposed) {
+                const double s = sig[p.s_off + j];
+                v = s > 0.0 ? sf * w[(int64_t)k * p.m + i] / s : 0.0;
+            } else {
+                v = sf * q[(int64_t)k * p.m + i];
+            }
+        }
+        out[t.out_off + e] = v;
+    }
+}
+
+}  // namespace
+
+struct dmrg_canon_s {
+    dmrg_ctx_t ctx = nullptr;
+    int side = 0;
+    int nl = 0, nr = 0;
+    std::vector<int> left_dim, right_dim;
+    BlockListDesc ket;
+    int nsec = 0;
+    std::vector<std::vector<int>> members;  // ket positions of each sector, list order
+    std::vector<int> sec_m, sec_n;          // stacked shape of each sector
+    BatchedSvd svd;
+    std::vector<CopyTask> copies;
+    DeviceBuffer d_copies, d_writes, d_canons, d_forced;
+    // results
+    bool ran = false;
+    std::vector<std::vector<double>> sv;  // singular values per sector (reference semantics)
+    std::vector<int> tdim;
+    BlockListDesc new_ket, canonical;
+    std::vector<int> match_dim;
+    double discarded = 0.0;
+    int sweeps = 0;
+};
+
+extern "C" {
+
+int dmrg_canon_create(dmrg_ctx_t ctx, int side, int nl, int nr, const int* left_dim, const int* right_dim,
+                      const dmrg_blocks_t* ket, dmrg_canon_t* out) {
+    if (!ctx || !out || !ket || !left_dim || !right_dim || nl <= 0 || nr <= 0 || (side != 0 && side != 1))
+        return set_error(DMRG_E_ARG, "invalid canonicalisation arguments");
+    *out = nullptr;
+    DMRG_CUDA_TRY(cudaSetDevice(ctx->device));
+    auto* c = new dmrg_canon_s();
+    c->ctx = ctx;
+    c->side = side;
+    c->nl = nl;
+    c->nr = nr;
+    c->left_dim.assign(left_dim, left_dim + nl);
+    c->right_dim.assign(right_dim, right_dim + nr);
+    if (!c->ket.assign(*ket)) {
+        delete c;
+        return set_error(DMRG_E_ARG, "invalid ket block list");
+    }
+    c->nsec = side == 0 ? nr : nl;
+    c->members = c->ket.by_sector(side == 0 ? 1 : 0, c->nsec);
+    c->sec_m.assign(c->nsec, 0);
+    c->sec_n.assign(c->nsec, 0);
+    for (int s = 0; s < c->nsec; ++s) {
+        int acc = 0;
+        for (int p : c->members[s]) acc += side == 0 ? c->ket.rows[p] : c->ket.cols[p];
+        if (side == 0) {
+            c->sec_m[s] = acc;
+            c->sec_n[s] = c->right_dim[s];
+        } else {
+            c->sec_m[s] = c->left_dim[s];
+            c->sec_n[s] = acc;
+        }
+    }
+    for (int k = 0; k < c->ket.count(); ++k) {
+        const int l = c->ket.left[k], r = c->ket.right[k];
+        if (l < 0 || l >= nl || r < 0 || r >= nr) {
+            delete c;
+            return set_error(DMRG_E_ARG, "ket block %d sectors out of range", k);
+        }
+    }
+    int rc = c->svd.plan(c->sec_m, c->sec_n, ctx->stream);
+    if (rc == DMRG_OK) {
+        for (int s = 0; s < c->nsec; ++s) {
+            if (!c->svd.active(s)) continue;
+            int acc = 0;
+            for (int p : c->members[s]) {
+                c->copies.push_back(CopyTask{c->ket.off[p], c->ket.rows[p], c->ket.cols[p], c->svd.index[s], acc});
+                acc += side == 0 ? c->ket.rows[p] : c->ket.cols[p];
+            }
+        }
+        rc = upload(c->d_copies, c->copies, ctx->stream);
+    }
+    if (rc != DMRG_OK) {
+        delete c;
+        return rc;
+    }
+    *out = c;
+    return DMRG_OK;
+}
+
+int dmrg_canon_destroy(dmrg_canon_t c) {
+    delete c;
+    return DMRG_OK;
+}
+
+int dmrg_canon_run(dmrg_canon_t c, const double* ket_dev, int max_dim, double canpre, int* tdim_out,
+                   double* discarded) {
+    if (!c || (!ket_dev && c->ket.size)) return set_error(DMRG_E_ARG, "null argument");
+    cudaStream_t st = c->ctx->stream;
+    BatchedSvd& svd = c->svd;
+    if (!svd.probs.empty()) {
+        int64_t wsize = 0;
+        for (const auto& p : svd.probs) wsize += (int64_t)p.rows * p.cols;
+        DMRG_CUDA_TRY(cudaMemsetAsync(svd.d_w.ptr, 0, wsize * sizeof(double), st));
+        if (!c->copies.empty())
+            gather_kernel<<<(int)c->copies.size(), 256, 0, st>>>(ket_dev, c->d_copies.as<CopyTask>(),
+                                                                 svd.d_probs.as<SvdProblem>(), svd.d_w.as<double>(),
+                                                                 c->side);
+        DMRG_CUDA_TRY(cudaGetLastError());
+        DMRG_TRY(svd.run(st, &c->sweeps));
+    }
+    std::vector<std::vector<double>> s;
+    DMRG_TRY(svd.singular_values(s, st));
+    // reference semantics for empty sectors: singular_dim = 1, value 0
+    for (int i = 0; i < c->nsec; ++i)
+        if (!svd.active(i)) s[i].assign(1, 0.0);
+    c->sv = s;
+    c->tdim = compute_truncate_dim(max_dim, canpre, s);  // s is modified (forced zeros)
+    // discarded weight: everything except the kept (possibly forced-to-zero) values
+    double all = 0.0, kept = 0.0;
+    for (int i = 0; i < c->nsec; ++i) {
+        for (double v : c->sv[i]) all += v * v;
+        for (int j = 0; j < c->tdim[i] && j < (int)s[i].size(); ++j) kept += s[i][j] * s[i][j];
+    }
+    c->discarded = all - kept;
+    // new shapes
+    c->new_ket = BlockListDesc();
+    for (int k = 0; k < c->ket.count(); ++k) {
+        const int l = c->ket.left[k], r = c->ket.right[k];
+        if (c->side == 0) {
+            const bool touched = svd.active(r);
+            c->new_ket.push(l, r, c->ket.rows[k], touched ? c->tdim[r] : c->ket.cols[k]);
+        } else {
+            const bool touched = svd.active(l);
+            c->new_ket.push(l, r, touched ? c->tdim[l] : c->ket.rows[k], c->ket.cols[k]);
+        }
+    }
+    c->canonical = BlockListDesc();
+    c->match_dim.assign(c->nsec, 0);
+    for (int sct = 0; sct < c->nsec; ++sct) {
+        if (c->side == 0) {
+            c->match_dim[sct] = c->sec_n[sct];
+            c->canonical.push(sct, sct, c->tdim[sct], c->sec_n[sct]);
+        } else {
+            c->match_dim[sct] = c->sec_m[sct];
+            c->canonical.push(sct, sct, c->sec_m[sct], c->tdim[sct]);
+        }
+    }
+    if (tdim_out)
+        for (int i = 0; i < c->nsec; ++i) tdim_out[i] = c->tdim[i];
+    if (discarded) *discarded = c->discarded;
+    // forced singular values (device) for the canonical blocks
+    std::vector<double> forced;
+    std::vector<CanonTask> ctasks;
+    for (int sct = 0; sct < c->nsec; ++sct) {
+        CanonTask t{c->canonical.off[sct], c->canonical.rows[sct], c->canonical.cols[sct],
+                    svd.active(sct) ? svd.index[sct] : -1, (int64_t)forced.size()};
+        for (int i = 0; i < c->tdim[sct]; ++i) forced.push_back(i < (int)s[sct].size() ? s[sct][i] : 0.0);
+        ctasks.push_back(t);
+    }
+    std::vector<WriteTask> wtasks;
+    for (int sct = 0; sct < c->nsec; ++sct) {
+        if (!svd.active(sct)) continue;
+        int acc = 0;
+        for (int p : c->members[sct]) {
+            wtasks.push_back(WriteTask{c->new_ket.off[p], c->new_ket.rows[p], c->new_ket.cols[p], svd.index[sct], acc});
+            acc += c->side == 0 ? c->ket.rows[p] : c->ket.cols[p];
+        }
+    }
+    DMRG_TRY(upload(c->d_forced, forced, st));
+    DMRG_TRY(upload(c->d_canons, ctasks, st));
+    DMRG_TRY(upload(c->d_writes, wtasks, st));
+    c->ran = true;
+    return DMRG_OK;
+}
+
+int dmrg_canon_out_info(dmrg_canon_t c, int64_t* ket_size, int64_t* canonical_size, int* sweeps) {
+    if (!c || !c->ran) return set_error(DMRG_E_STATE, "dmrg_canon_run has not been called");
+    if (ket_size) *ket_size = c->new_ket.size;
+    if (canonical_size) *canonical_size = c->canonical.size;
+    if (sweeps) *sweeps = c->sweeps;
+    return DMRG_OK;
+}
+
+int dmrg_canon_out_blocks(dmrg_canon_t c, int* ket_rows, int* ket_cols, int* canon_rows, int* canon_cols,
+                          int* match_dim) {
+    if (!c || !c->ran) return set_error(DMRG_E_STATE, "dmrg_canon_run has not been called");
+    for (int k = 0; k < c->new_ket.count(); ++k) {
+        if (ket_rows) ket_rows[k] = c->new_ket.rows[k];
+        if (ket_cols) ket_cols[k] = c->new_ket.cols[k];
+    }
+    for (int s = 0; s < c->nsec; ++s) {
+        if (canon_rows) canon_rows[s] = c->canonical.rows[s];
+        if (canon_cols) canon_cols[s] = c->canonical.cols[s];
+        if (match_dim) match_dim[s] = c->match_dim[s];
+    }
+    return DMRG_OK;
+}
+
+int dmrg_canon_singular_values(dmrg_canon_t c, int sector, int cap, double* values, int* count) {
+    if (!c || !c->ran || !count) return set_error(DMRG_E_STATE, "dmrg_canon_run has not been called");
+    if (sector < 0 || sector >= c->nsec) return set_error(DMRG_E_ARG, "sector %d out of range", sector);
+    const auto& s = c->sv[sector];
+    *count = (int)s.size();
+    if (values)
+        for (int i = 0; i < (int)s.size() && i < cap; ++i) values[i] = s[i];
+    return DMRG_OK;
+}
+
+int dmrg_canon_write(dmrg_canon_t c, const double* ket_dev, double* new_ket_dev, double* canonical_dev) {
+    if (!c || !c->ran) return set_error(DMRG_E_STATE, "dmrg_canon_run has not been called");
+    cudaStream_t st = c->ctx->stream;
+    BatchedSvd& svd = c->svd;
+    // blocks of untouched (empty) sectors keep their values
+    for (int s = 0; s < c->nsec; ++s) {
+        if (svd.active(s)) continue;
+        for (int p : c->members[s]) {
+            const size_t bytes = (size_t)c->ket.rows[p] * c->ket.cols[p] * sizeof(double);
+            if (bytes)
+                DMRG_CUDA_TRY(cudaMemcpyAsync(new_ket_dev + c->new_ket.off[p], ket_dev + c->ket.off[p], bytes,
+                                              cudaMemcpyDeviceToDevice, st));
+        }
+    }
+    const int nw = (int)(c->d_writes.bytes / sizeof(WriteTask));
+    int n_writes = 0;
+    for (int s = 0; s < c->nsec; ++s)
+        if (svd.active(s)) n_writes += (int)c->members[s].size();
+    (void)nw;
+    const double* sig = svd.d_s.as<double>();
+    if (n_writes)
+        write_ket_kernel<<<n_writes, 256, 0, st>>>(c->d_writes.as<WriteTask>(), svd.d_probs.as<SvdProblem>(),
+                                                   svd.d_w.as<double>(), svd.d_q.as<double>(), sig,
+                                                   svd.d_perm.as<int>(), new_ket_dev, c->side);
+    write_canonical_kernel<<<c->nsec, 256, 0, st>>>(c->d_canons.as<CanonTask>(), svd.d_probs.as<SvdProblem>(),
+                                                    svd.d_w.as<double>(), svd.d_q.as<double>(), sig,
+                                                    svd.d_perm.as<int>(), c->d_forced.as<double>(), canonical_dev,
+                                                    c->side);
+    DMRG_CUDA_TRY(cudaGetLastError());
+    return DMRG_OK;
+}
+
+}  // extern "C"

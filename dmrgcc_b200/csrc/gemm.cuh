@@ -33,7 +33,18 @@ struct GemmGroup {
     int n;
     int t0;
     int t1;
-    int pad_;
+    int cbuf;  // 0: output goes to C; 1: a split-K chunk, output goes to the schedule's aux buffer
+};
+
+// A group whose term list was split into chunks: aux holds `chunks` consecutive
+// m x n partial tiles that are summed, in chunk order, into C at c_off.
+struct GemmSplit {
+    int64_t c_off;
+    int64_t aux_off;
+    int ldc;
+    int m;
+    int n;
+    int chunks;
 };
 
 struct GemmTile {
@@ -50,8 +61,12 @@ struct GemmSchedule {
     std::vector<GemmTile> tiles;
     bool ta = false, tb = false;
     double flops = 0.0;  // 2*m*n*k summed over terms
+    // execution form built by finalize(): split-K chunks replace long groups
+    std::vector<GemmGroup> exec_groups;
+    std::vector<GemmSplit> splits;
+    int64_t aux_size = 0;
     // device copies
-    DeviceBuffer d_terms, d_groups, d_tiles;
+    DeviceBuffer d_terms, d_groups, d_tiles, d_splits, aux;
 
     void reset() {
         terms.clear();
@@ -59,6 +74,9 @@ struct GemmSchedule {
         tiles.clear();
         ta = tb = false;
         flops = 0.0;
+        exec_groups.clear();
+        splits.clear();
+        aux_size = 0;
     }
     int add_group(int64_t c_off, int ldc, int m, int n) {
         GemmGroup g{c_off, ldc, m, n, (int)terms.size(), (int)terms.size(), 0};
@@ -73,7 +91,10 @@ struct GemmSchedule {
         flops += 2.0 * g.m * g.n * (double)k;
     }
     // Builds the tile list (tile_m x tile_n tiles, heaviest first) and uploads.
-    int finalize(int tile_m, int tile_n, int tile_k, cudaStream_t stream);
+    // With `num_sms` > 0, groups whose k-loop is much longer than the balanced
+    // per-CTA share are split into chunks (split-K) reduced by a second kernel,
+    // so that a few very long output tiles do not leave the GPU idle.
+    int finalize(int tile_m, int tile_n, int tile_k, cudaStream_t stream, int num_sms = 0);
 };
 
 // C (+)= sum of terms for every tile of `s`.  A, B, C are the base pointers.

@@ -89,7 +89,8 @@ __device__ __forceinline__ void compute_stage(const double* As, const double* Bs
 
 template <bool TA, bool TB>
 __global__ void __launch_bounds__(NT) gemm_f64_kernel(const double* __restrict__ A, const double* __restrict__ B,
-                                                      double* __restrict__ C, const GemmTerm* __restrict__ terms,
+                                                      double* __restrict__ C, double* __restrict__ Caux,
+                                                      const GemmTerm* __restrict__ terms,
                                                       const GemmGroup* __restrict__ groups,
                                                       const GemmTile* __restrict__ tiles, int accumulate) {
     __shared__ __align__(16) double smA[2][STAGE];
@@ -142,38 +143,97 @@ __global__ void __launch_bounds__(NT) gemm_f64_kernel(const double* __restrict__
     }
 
     const int fr = lane >> 2, fc = lane & 3;
+    const bool acc_out = accumulate && g.cbuf == 0;
+    double* Cb = g.cbuf ? Caux : C;
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
         const int row = tile.m0 + wm * 32 + i * 8 + fr;
         if (row >= g.m) continue;
-        double* crow = C + g.c_off + (int64_t)row * g.ldc;
+        double* crow = Cb + g.c_off + (int64_t)row * g.ldc;
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
 #pragma unroll
             for (int e = 0; e < 2; ++e) {
                 const int col = tile.n0 + wn * 32 + j * 8 + fc * 2 + e;
-                if (col < g.n) crow[col] = accumulate ? crow[col] + acc[i][j][e] : acc[i][j][e];
+                if (col < g.n) crow[col] = acc_out ? crow[col] + acc[i][j][e] : acc[i][j][e];
             }
         }
     }
 }
 
+// Grid (element slices, split groups): C[c_off + r*ldc + c] (+)= sum over the
+// group's chunks, in chunk order (deterministic).
+__global__ void __launch_bounds__(256) split_reduce_kernel(double* __restrict__ C, const double* __restrict__ Caux,
+                                                           const GemmSplit* __restrict__ splits, int accumulate) {
+    const GemmSplit s = splits[blockIdx.y];
+    const int64_t tile = (int64_t)s.m * s.n;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < tile; e += (int64_t)gridDim.x * blockDim.x) {
+        double v = 0.0;
+        for (int c = 0; c < s.chunks; ++c) v += Caux[s.aux_off + c * tile + e];
+        const int r = (int)(e / s.n), col = (int)(e % s.n);
+        double* p = C + s.c_off + (int64_t)r * s.ldc + col;
+        *p = accumulate ? *p + v : v;
+    }
+}
+
 }  // namespace
 
-int GemmSchedule::finalize(int tile_m, int tile_n, int tile_k, cudaStream_t stream) {
+int GemmSchedule::finalize(int tile_m, int tile_n, int tile_k, cudaStream_t stream, int num_sms) {
     tiles.clear();
-    for (int gi = 0; gi < (int)groups.size(); ++gi) {
-        const GemmGroup& g = groups[gi];
+    exec_groups.clear();
+    splits.clear();
+    aux_size = 0;
+    auto ksteps_of = [&](int t) { return (terms[t].k + tile_k - 1) / tile_k; };
+    auto ntiles_of = [&](const GemmGroup& g) {
+        return (int64_t)((g.m + tile_m - 1) / tile_m) * ((g.n + tile_n - 1) / tile_n);
+    };
+    // balanced share of k-steps per CTA (4 resident CTAs per SM, two waves)
+    int64_t total = 0;
+    for (const GemmGroup& g : groups) {
         if (g.m <= 0 || g.n <= 0) continue;
-        int ksteps = 0;
-        for (int t = g.t0; t < g.t1; ++t) ksteps += (terms[t].k + tile_k - 1) / tile_k;
+        int64_t ks = 0;
+        for (int t = g.t0; t < g.t1; ++t) ks += ksteps_of(t);
+        total += ks * ntiles_of(g);
+    }
+    const int64_t share = num_sms > 0 ? std::max<int64_t>(16, total / ((int64_t)num_sms * 8)) : 0;
+    for (const GemmGroup& g : groups) {
+        if (g.m <= 0 || g.n <= 0 || g.t1 <= g.t0) continue;
+        int64_t ks = 0;
+        for (int t = g.t0; t < g.t1; ++t) ks += ksteps_of(t);
+        if (share == 0 || ks <= 2 * share || g.t1 - g.t0 < 2) {
+            exec_groups.push_back(g);
+            continue;
+        }
+        // split the term range into contiguous chunks of about `share` k-steps
+        GemmSplit sp{g.c_off, aux_size, g.ldc, g.m, g.n, 0};
+        int t0 = g.t0;
+        int64_t acc = 0;
+        for (int t = g.t0; t < g.t1; ++t) {
+            acc += ksteps_of(t);
+            if (acc >= share || t + 1 == g.t1) {
+                GemmGroup c{aux_size + (int64_t)sp.chunks * g.m * g.n, g.n, g.m, g.n, t0, t + 1, 1};
+                exec_groups.push_back(c);
+                sp.chunks++;
+                t0 = t + 1;
+                acc = 0;
+            }
+        }
+        aux_size += (int64_t)sp.chunks * g.m * g.n;
+        splits.push_back(sp);
+    }
+    for (int gi = 0; gi < (int)exec_groups.size(); ++gi) {
+        const GemmGroup& g = exec_groups[gi];
+        int ks = 0;
+        for (int t = g.t0; t < g.t1; ++t) ks += ksteps_of(t);
         for (int m0 = 0; m0 < g.m; m0 += tile_m)
-            for (int n0 = 0; n0 < g.n; n0 += tile_n) tiles.push_back(GemmTile{gi, m0, n0, ksteps});
+            for (int n0 = 0; n0 < g.n; n0 += tile_n) tiles.push_back(GemmTile{gi, m0, n0, ks});
     }
     std::stable_sort(tiles.begin(), tiles.end(), [](const GemmTile& a, const GemmTile& b) { return a.cost > b.cost; });
     DMRG_TRY(upload(d_terms, terms, stream));
-    DMRG_TRY(upload(d_groups, groups, stream));
+    DMRG_TRY(upload(d_groups, exec_groups, stream));
     DMRG_TRY(upload(d_tiles, tiles, stream));
+    DMRG_TRY(upload(d_splits, splits, stream));
+    DMRG_TRY(aux.alloc((size_t)std::max<int64_t>(aux_size, 1) * sizeof(double)));
     return DMRG_OK;
 }
 
@@ -185,10 +245,18 @@ int launch_gemm_f64(const GemmSchedule& s, const double* A, const double* B, dou
     const auto* gr = s.d_groups.as<GemmGroup>();
     const auto* tl = s.d_tiles.as<GemmTile>();
     const int acc = accumulate ? 1 : 0;
-    if (!s.ta && !s.tb) gemm_f64_kernel<false, false><<<n, NT, 0, stream>>>(A, B, C, tr, gr, tl, acc);
-    else if (s.ta && !s.tb) gemm_f64_kernel<true, false><<<n, NT, 0, stream>>>(A, B, C, tr, gr, tl, acc);
-    else if (!s.ta && s.tb) gemm_f64_kernel<false, true><<<n, NT, 0, stream>>>(A, B, C, tr, gr, tl, acc);
-    else gemm_f64_kernel<true, true><<<n, NT, 0, stream>>>(A, B, C, tr, gr, tl, acc);
+    double* X = s.aux.as<double>();
+    if (!s.ta && !s.tb) gemm_f64_kernel<false, false><<<n, NT, 0, stream>>>(A, B, C, X, tr, gr, tl, acc);
+    else if (s.ta && !s.tb) gemm_f64_kernel<true, false><<<n, NT, 0, stream>>>(A, B, C, X, tr, gr, tl, acc);
+    else if (!s.ta && s.tb) gemm_f64_kernel<false, true><<<n, NT, 0, stream>>>(A, B, C, X, tr, gr, tl, acc);
+    else gemm_f64_kernel<true, true><<<n, NT, 0, stream>>>(A, B, C, X, tr, gr, tl, acc);
+    if (!s.splits.empty()) {
+        int64_t biggest = 0;
+        for (const GemmSplit& sp : s.splits) biggest = std::max<int64_t>(biggest, (int64_t)sp.m * sp.n);
+        const int gx = (int)std::min<int64_t>((biggest + 255) / 256, 64);
+        split_reduce_kernel<<<dim3(gx, (unsigned)s.splits.size()), 256, 0, stream>>>(C, X, s.d_splits.as<GemmSplit>(),
+                                                                                     acc);
+    }
     DMRG_CUDA_TRY(cudaGetLastError());
     return DMRG_OK;
 }

@@ -125,7 +125,7 @@ int build_heff(dmrg_heff_s& h) {
     h.flops_exec = fa_exec + fb;
     cudaStream_t st = h.ctx->stream;
     DMRG_TRY(h.sa.finalize(64, 64, 16, st));
-    DMRG_TRY(h.sb.finalize(64, 64, 16, st));
+    DMRG_TRY(h.sb.finalize(64, 64, 16, st, h.ctx->num_sms));
     DMRG_TRY(h.T.alloc((size_t)std::max<int64_t>(h.t_size, 1) * sizeof(double)));
     return DMRG_OK;
 }

@@ -1,0 +1,400 @@
+// Host-side model layer (see model.h).
+#include "host/model.h"
+
+#include <cmath>
+#include <stdexcept>
+
+#include "truncate.h"
+
+namespace dmrg {
+
+// ---------------------------------------------------------------------------
+// RealTensorOperator
+// ---------------------------------------------------------------------------
+void RealTensorOperator::ExpanTensorOperator(const std::vector<HostMatrix>& basic, int leigh, int op, double coeff) {
+    int e0 = 1, e1 = 1;
+    if (leigh == 0) e0 = 0;
+    if (leigh == 1) e1 = 0;
+    int nlb, nrb;
+    if (lb_ == 0 && rb_ == 0) {
+        nlb = 1;
+        nrb = 1;
+    } else {
+        nlb = lb_ + e0;
+        nrb = rb_ + e1;
+    }
+    std::vector<double> old = W_;
+    const int olb = lb_, orb = rb_;
+    resize(nlb, nrb);
+    for (int l = 0; l < olb; ++l)
+        for (int r = 0; r < orb; ++r)
+            for (int p1 = 0; p1 < d_; ++p1)
+                for (int p2 = 0; p2 < d_; ++p2) w(l, r, p1, p2) = old[(((size_t)l * orb + r) * d_ + p1) * d_ + p2];
+    const int il = e0 * olb, ir = e1 * orb;
+    for (int p1 = 0; p1 < d_; ++p1)
+        for (int p2 = 0; p2 < d_; ++p2) w(il, ir, p1, p2) = coeff * basic[op].at(p1, p2);
+}
+
+namespace {
+
+// The reference's element test for parallel columns/rows (util/general.h:
+// isParallelElement): a zero reference entry must face a zero; otherwise all
+// ratios must agree within 1e-8 (the first defines the prefactor).
+void parallel_element(double e0, double e1, int position, int& info, double& prefactor, bool& zero) {
+    if (std::fabs(e1) <= 1e-10) {
+        if (std::fabs(e0) > 1e-10) {
+            info = -1;
+            prefactor = 1.0;
+        }
+    } else {
+        const double factor = e0 / e1;
+        if (zero) {
+            info = position;
+            prefactor = factor;
+            zero = false;
+        } else if (std::fabs(factor - prefactor) > 1e-8) {
+            info = -1;
+            prefactor = 1.0;
+        }
+    }
+}
+
+}  // namespace
+
+void parallel_matrix(const HostMatrix& M, int leigh, int& nu, std::vector<int>& pos, HostMatrix& T) {
+    int info = 0;
+    double prefactor = 0.0;
+    bool zero = true;
+    if (leigh == 0) {
+        pos.assign(M.cols, -1);
+        pos[0] = 0;
+        T = HostMatrix(M.cols, M.cols);
+        T.at(0, 0) = 1.0;
+        nu = 1;
+        for (int r = 0; r < M.cols; ++r) {
+            for (int k = 0; k < nu; ++k) {
+                info = nu;
+                prefactor = 0.0;
+                zero = true;
+                for (int l = 0; l < M.rows; ++l) {
+                    parallel_element(M.at(l, r), M.at(l, pos[k]), pos[k], info, prefactor, zero);
+                    if (info == -1) break;
+                }
+                if (info != -1) {
+                    T.at(k, r) = prefactor;
+                    break;
+                }
+            }
+            if (info == -1) {
+                pos[nu] = r;
+                T.at(nu, r) = 1.0;
+                ++nu;
+            }
+        }
+    } else {
+        pos.assign(M.rows, -1);
+        pos[0] = 0;
+        T = HostMatrix(M.rows, M.rows);
+        T.at(0, 0) = 1.0;
+        nu = 1;
+        for (int l = 0; l < M.rows; ++l) {
+            for (int k = 0; k < nu; ++k) {
+                info = nu;
+                prefactor = 0.0;
+                zero = true;
+                for (int r = 0; r < M.cols; ++r) {
+                    parallel_element(M.at(l, r), M.at(pos[k], r), pos[k], info, prefactor, zero);
+                    if (info == -1) break;
+                }
+                if (info != -1) {
+                    T.at(l, k) = prefactor;
+                    break;
+                }
+            }
+            if (info == -1) {
+                pos[nu] = l;
+                T.at(l, nu) = 1.0;
+                ++nu;
+            }
+        }
+    }
+}
+
+void RealTensorOperator::LeftParallelTensorOperator(int& nu, std::vector<int>& pos, HostMatrix& T) {
+    HostMatrix R(lb_ * d_ * d_, rb_);
+    for (int l = 0; l < lb_; ++l)
+        for (int r = 0; r < rb_; ++r)
+            for (int p1 = 0; p1 < d_; ++p1)
+                for (int p2 = 0; p2 < d_; ++p2) R.at(p2 + (p1 + l * d_) * d_, r) = w(l, r, p1, p2);
+    parallel_matrix(R, 0, nu, pos, T);
+    resize(lb_, nu);
+    for (int l = 0; l < lb_; ++l)
+        for (int r = 0; r < rb_; ++r)
+            for (int p1 = 0; p1 < d_; ++p1)
+                for (int p2 = 0; p2 < d_; ++p2) w(l, r, p1, p2) = R.at(p2 + (p1 + l * d_) * d_, pos[r]);
+}
+
+void RealTensorOperator::RightParallelTensorOperator(int& nu, std::vector<int>& pos, HostMatrix& T) {
+    HostMatrix R(lb_, rb_ * d_ * d_);
+    for (int l = 0; l < lb_; ++l)
+        for (int r = 0; r < rb_; ++r)
+            for (int p1 = 0; p1 < d_; ++p1)
+                for (int p2 = 0; p2 < d_; ++p2) R.at(l, p2 + (p1 + r * d_) * d_) = w(l, r, p1, p2);
+    parallel_matrix(R, 1, nu, pos, T);
+    resize(nu, rb_);
+    for (int l = 0; l < lb_; ++l)
+        for (int r = 0; r < rb_; ++r)
+            for (int p1 = 0; p1 < d_; ++p1)
+                for (int p2 = 0; p2 < d_; ++p2) w(l, r, p1, p2) = R.at(pos[l], p2 + (p1 + r * d_) * d_);
+}
+
+void RealTensorOperator::LeftMergeTensorOperator(int nu, const HostMatrix& T) {
+    const int merge = T.cols;
+    if (merge != lb_) throw std::runtime_error("merge dimension is not match in LeftMergeTensorOperator");
+    std::vector<double> old = W_;
+    const int orb = rb_;
+    resize(nu, orb);
+    for (int l = 0; l < nu; ++l)
+        for (int r = 0; r < orb; ++r)
+            for (int p1 = 0; p1 < d_; ++p1)
+                for (int p2 = 0; p2 < d_; ++p2) {
+                    double e = 0.0;
+                    for (int m = 0; m < merge; ++m)
+                        e += T.at(l, m) * old[(((size_t)m * orb + r) * d_ + p1) * d_ + p2];
+                    w(l, r, p1, p2) = e;
+                }
+}
+
+void RealTensorOperator::RightMergeTensorOperator(int nu, const HostMatrix& T) {
+    const int merge = T.rows;
+    if (merge != rb_) throw std::runtime_error("merge dimension is not match in RightMergeTensorOperator");
+    std::vector<double> old = W_;
+    const int olb = lb_, orb = rb_;
+    resize(olb, nu);
+    for (int l = 0; l < olb; ++l)
+        for (int r = 0; r < nu; ++r)
+            for (int p1 = 0; p1 < d_; ++p1)
+                for (int p2 = 0; p2 < d_; ++p2) {
+                    double e = 0.0;
+                    for (int m = 0; m < merge; ++m)
+                        e += T.at(m, r) * old[(((size_t)l * orb + m) * d_ + p1) * d_ + p2];
+                    w(l, r, p1, p2) = e;
+                }
+}
+
+bool RealTensorOperator::LeftCheckZero(int l, int p1) const {
+    for (int r = 0; r < rb_; ++r)
+        for (int p2 = 0; p2 < d_; ++p2)
+            if (std::fabs(w(l, r, p1, p2)) > 1e-15) return true;
+    return false;
+}
+bool RealTensorOperator::RightCheckZero(int r, int p2) const {
+    for (int l = 0; l < lb_; ++l)
+        for (int p1 = 0; p1 < d_; ++p1)
+            if (std::fabs(w(l, r, p1, p2)) > 1e-15) return true;
+    return false;
+}
+bool RealTensorOperator::MixedCheckZero(int l, int p2) const {
+    for (int r = 0; r < rb_; ++r)
+        for (int p1 = 0; p1 < d_; ++p1)
+            if (std::fabs(w(l, r, p1, p2)) > 1e-15) return true;
+    return false;
+}
+
+// ---------------------------------------------------------------------------
+// RealTensorHamiltonian
+// ---------------------------------------------------------------------------
+void RealTensorHamiltonian::init(int num_site, int d, int num_quantum) {
+    num_site_ = num_site;
+    num_quantum_ = num_quantum;
+    qtab_.assign(num_site + 1, {});
+    ops_.assign(num_site, RealTensorOperator(d));
+}
+
+void RealTensorHamiltonian::ExpanTensorHamiltonian(int site, int op, double coeff, const std::vector<int>& table) {
+    int leigh = -1;
+    if (site == 0) leigh = 0;
+    if (site == num_site_ - 1) leigh = 1;
+    ops_[site].ExpanTensorOperator(basic_, leigh, op, coeff);
+    if (site < num_site_ - 1) qtab_[site + 1].push_back(table);
+}
+
+void RealTensorHamiltonian::ParallelQuantumTable(int site, int nu, const std::vector<int>& pos) {
+    std::vector<std::vector<int>> t(nu);
+    for (int i = 0; i < nu; ++i) t[i] = qtab_[site][pos[i]];
+    qtab_[site] = t;
+}
+
+void RealTensorHamiltonian::ParallelTensorHamiltonian() {
+    int nu;
+    std::vector<int> pos;
+    HostMatrix T;
+    for (int i = 0; i < num_site_ - 1; ++i) {
+        ops_[i].LeftParallelTensorOperator(nu, pos, T);
+        ops_[i + 1].LeftMergeTensorOperator(nu, T);
+        ParallelQuantumTable(i + 1, nu, pos);
+    }
+    for (int i = num_site_ - 1; i > 0; --i) {
+        ops_[i].RightParallelTensorOperator(nu, pos, T);
+        ops_[i - 1].RightMergeTensorOperator(nu, T);
+        ParallelQuantumTable(i, nu, pos);
+    }
+}
+
+RealSpinlessBoseSquareHamiltonian::RealSpinlessBoseSquareHamiltonian(int nx, int ny, int d, double flux_value,
+                                                                     double hop_x, double hop_y, double inter,
+                                                                     double chem, bool px, bool py)
+    : nx_(nx), ny_(ny), d_(d), hop_x_(hop_x), hop_y_(hop_y), inter_(inter), chem_(chem), px_(px), py_(py) {
+    (void)flux_value;  // stored but unused by the real spinless model (as in the reference)
+    init(nx * ny, d, 1);
+    // 0 = I, 1 = b+, 2 = b, 3 = n, 4 = mu n + U n(n-1)
+    basic_.assign(5, HostMatrix(d, d));
+    for (int i = 0; i < d; ++i) {
+        basic_[0].at(i, i) = 1.0;
+        basic_[3].at(i, i) = i;
+        basic_[4].at(i, i) = chem * i + inter * i * (i - 1);
+    }
+    for (int i = 1; i < d; ++i) {
+        basic_[1].at(i, i - 1) = std::sqrt((double)i);
+        basic_[2].at(i - 1, i) = std::sqrt((double)i);
+    }
+}
+
+void RealSpinlessBoseSquareHamiltonian::DefineHamiltonian1(int p1, int p2, double coeff) {
+    if (p1 >= p2) throw std::runtime_error("position1 >= position2 in DefineHamiltonian1");
+    for (int i = 0; i < num_site_; ++i) {
+        int op = 0, q = 0;
+        double c = 1.0;
+        if (i == p1) {
+            op = 1;
+            q = 1;
+        }
+        if (i > p1 && i < p2) q = 1;
+        if (i == p2) {
+            op = 2;
+            c = coeff;
+            q = 0;
+        }
+        ExpanTensorHamiltonian(i, op, c, {q});
+    }
+}
+
+void RealSpinlessBoseSquareHamiltonian::DefineHamiltonian2(int p1, int p2, double coeff) {
+    if (p1 >= p2) throw std::runtime_error("position1 >= position2 in DefineHamiltonian2");
+    for (int i = 0; i < num_site_; ++i) {
+        int op = 0, q = 0;
+        double c = 1.0;
+        if (i == p1) {
+            op = 2;
+            q = -1;
+        }
+        if (i > p1 && i < p2) q = -1;
+        if (i == p2) {
+            op = 1;
+            c = coeff;
+            q = 0;
+        }
+        ExpanTensorHamiltonian(i, op, c, {q});
+    }
+}
+
+void RealSpinlessBoseSquareHamiltonian::DefineHamiltonian3(int p, double coeff) {
+    for (int i = 0; i < num_site_; ++i) {
+        int op = 0;
+        double c = 1.0;
+        if (i == p) {
+            op = 4;
+            c = coeff;
+        }
+        ExpanTensorHamiltonian(i, op, c, {0});
+    }
+}
+
+void RealSpinlessBoseSquareHamiltonian::DefineTensorHamiltonian() {
+    qtab_[0] = {{0}};
+    qtab_[num_site_] = {{0}};
+    for (int i = 0; i < nx_; ++i)
+        for (int j = 0; j < ny_; ++j) {
+            const int p0 = j + i * ny_;  // column-major site order (p = j + i * Ny)
+            if (hop_x_ != 0) {
+                const int p1 = j + ((i + 1) % nx_) * ny_;
+                if (i + 1 < nx_) {
+                    DefineHamiltonian1(p0, p1, hop_x_);
+                    DefineHamiltonian2(p0, p1, hop_x_);
+                } else if (nx_ > 2 && px_) {
+                    DefineHamiltonian1(p1, p0, hop_x_);
+                    DefineHamiltonian2(p1, p0, hop_x_);
+                }
+            }
+            if (hop_y_ != 0) {
+                const int p1 = (j + 1) % ny_ + i * ny_;
+                if (j + 1 < ny_) {
+                    DefineHamiltonian1(p0, p1, hop_y_);
+                    DefineHamiltonian2(p0, p1, hop_y_);
+                } else if (ny_ > 2 && py_) {
+                    DefineHamiltonian1(p1, p0, hop_y_);
+                    DefineHamiltonian2(p1, p0, hop_y_);
+                }
+            }
+            if (chem_ != 0 || inter_ != 0) DefineHamiltonian3(p0, 1.0);
+            ParallelTensorHamiltonian();
+        }
+}
+
+// ---------------------------------------------------------------------------
+// Quantum tables of the MPS bonds
+// ---------------------------------------------------------------------------
+void QuantumSpace::ReorderQuantumTable(std::vector<std::vector<int>>& table, const std::vector<double>& mean) {
+    const int n = (int)table.size();
+    if (n == 0) return;
+    std::vector<double> dev(n, 0.0);
+    std::vector<int> index(n);
+    for (int i = 0; i < n; ++i) {
+        index[i] = i;
+        for (int j = 0; j < num_quantum_; ++j) dev[i] += std::pow(table[i][j] - mean[j], 2);
+    }
+    quicksort_with_index(dev.data(), index.data(), n, false);
+    std::vector<std::vector<int>> out(n);
+    for (int k = 0; k < n; ++k) out[k] = table[index[k]];
+    table = out;
+}
+
+RealSpinlessBoseSquareSpace::RealSpinlessBoseSquareSpace(int nx, int ny, int num_boson, int d)
+    : num_boson_(num_boson) {
+    num_site_ = nx * ny;
+    d_ = d;
+    num_quantum_ = 1;
+    qtab_.assign(num_site_ + 1, {});
+    for (int i = 0; i <= num_site_; ++i) {
+        int lo, hi;
+        double mean;
+        if (i == 0) {
+            lo = hi = 0;
+            mean = 0.0;
+        } else {
+            const int min_left = 0, max_left = (d - 1) * i;
+            const int min_right = num_boson - (num_site_ - i) * (d - 1), max_right = num_boson;
+            lo = std::max(min_left, min_right);
+            hi = std::min(max_left, max_right);
+            mean = (double)num_boson / num_site_ * i;
+        }
+        std::vector<std::vector<int>> t;
+        for (int q = lo; q <= hi; ++q) t.push_back({q});
+        ReorderQuantumTable(t, {mean});
+        qtab_[i] = t;
+    }
+}
+
+int RealSpinlessBoseSquareSpace::CheckQuantumTable(int, const std::vector<int>& left,
+                                                   const std::vector<int>& right) const {
+    for (int i = 0; i < d_; ++i)
+        if (left[0] + i == right[0]) return i;
+    return -1;
+}
+
+std::vector<int> RealSpinlessBoseSquareSpace::MergeQuantumTable(const std::vector<int>& op,
+                                                                const std::vector<int>& space) const {
+    return {op[0] + space[0]};
+}
+
+}  // namespace dmrg

@@ -1,0 +1,137 @@
+// Host-side model layer: MPO site operators, the MPO (Hamiltonian) with its
+// per-bond operator quantum numbers, and the U(1) quantum-number tables of the
+// MPS bonds.  Pure bookkeeping, built once on the host, exactly as the
+// reference builds them (the block maps and the MPO feed the device schedules).
+#pragma once
+
+#include <string>
+#include <vector>
+
+namespace dmrg {
+
+// Dense row-major host matrix used for the small one-time MPO algebra.
+struct HostMatrix {
+    int rows = 0, cols = 0;
+    std::vector<double> v;
+    HostMatrix() = default;
+    HostMatrix(int r, int c) : rows(r), cols(c), v((size_t)r * c, 0.0) {}
+    double& at(int i, int j) { return v[(size_t)i * cols + j]; }
+    double at(int i, int j) const { return v[(size_t)i * cols + j]; }
+};
+
+// RealTensorOperator (src/dmrg/realdmrg/real_tensor_operator.{h,cc}): an MPO
+// site tensor W[l][r](p1, p2).
+class RealTensorOperator {
+public:
+    explicit RealTensorOperator(int physics_dim = 0) : d_(physics_dim) {}
+    int get_physics_dim() const { return d_; }
+    int get_left_bond() const { return lb_; }
+    int get_right_bond() const { return rb_; }
+    double w(int l, int r, int p1, int p2) const { return W_[idx(l, r, p1, p2)]; }
+    double& w(int l, int r, int p1, int p2) { return W_[idx(l, r, p1, p2)]; }
+    const std::vector<double>& data() const { return W_; }
+
+    // Appends one term: leigh 0 (first site) grows the right bond, 1 (last site)
+    // the left bond, otherwise both; the new corner is coeff * basic[op]
+    // (ExpanTensorOperator, real_tensor_operator.cc:141-197).
+    void ExpanTensorOperator(const std::vector<HostMatrix>& basic, int leigh, int op, double coeff);
+    // Deparallelisation of the right bond (:199-237) / left bond (:239-275).
+    void LeftParallelTensorOperator(int& num_unparallel, std::vector<int>& position, HostMatrix& transfer);
+    void RightParallelTensorOperator(int& num_unparallel, std::vector<int>& position, HostMatrix& transfer);
+    // Absorbs a neighbour's transfer matrix into the left (:277-319) / right (:321-361) bond.
+    void LeftMergeTensorOperator(int num_unparallel, const HostMatrix& transfer);
+    void RightMergeTensorOperator(int num_unparallel, const HostMatrix& transfer);
+    // Any |W| > 1e-15 in the given row/column slice (:363-409).
+    bool LeftCheckZero(int l, int p1) const;
+    bool RightCheckZero(int r, int p2) const;
+    bool MixedCheckZero(int l, int p2) const;
+
+private:
+    size_t idx(int l, int r, int p1, int p2) const { return (((size_t)l * rb_ + r) * d_ + p1) * d_ + p2; }
+    void resize(int lb, int rb) {
+        lb_ = lb;
+        rb_ = rb;
+        W_.assign((size_t)lb * rb * d_ * d_, 0.0);
+    }
+    int d_ = 0, lb_ = 0, rb_ = 0;
+    std::vector<double> W_;
+};
+
+// RealMatrix::ParallelMatrix (src/tensor/real_matrix.cc:438-531): removes
+// columns (leigh 0) or rows (leigh 1) parallel to an earlier one.
+void parallel_matrix(const HostMatrix& M, int leigh, int& num_unparallel, std::vector<int>& position,
+                     HostMatrix& transfer);
+
+// RealTensorHamiltonian (+ the spin-less Bose-Hubbard square-lattice model,
+// model/hamiltonian/real_spinless_bose_square_hamiltonian.cc).
+class RealTensorHamiltonian {
+public:
+    virtual ~RealTensorHamiltonian() = default;
+    int num_site() const { return num_site_; }
+    RealTensorOperator& get_tensor_hamiltonian(int site) { return ops_[site]; }
+    const RealTensorOperator& get_tensor_hamiltonian(int site) const { return ops_[site]; }
+    // operator quantum numbers of MPO bond b (b = 0..num_site): rows x num_quantum
+    const std::vector<std::vector<int>>& quantum_table(int b) const { return qtab_[b]; }
+    int num_quantum() const { return num_quantum_; }
+    virtual void DefineTensorHamiltonian() = 0;
+
+protected:
+    void init(int num_site, int physics_dim, int num_quantum);
+    void ExpanTensorHamiltonian(int site, int op, double coeff, const std::vector<int>& expan_table);
+    void ParallelTensorHamiltonian();
+    void ParallelQuantumTable(int site, int num_unparallel, const std::vector<int>& position);
+
+    int num_site_ = 0, num_quantum_ = 1;
+    std::vector<HostMatrix> basic_;
+    std::vector<std::vector<std::vector<int>>> qtab_;
+    std::vector<RealTensorOperator> ops_;
+};
+
+class RealSpinlessBoseSquareHamiltonian : public RealTensorHamiltonian {
+public:
+    RealSpinlessBoseSquareHamiltonian(int nx, int ny, int physics_dim, double flux_value, double hop_x, double hop_y,
+                                      double inter_value, double chemical_value, bool period_x, bool period_y);
+    void DefineTensorHamiltonian() override;
+
+private:
+    void DefineHamiltonian1(int p1, int p2, double coeff);  // b+_p1 b_p2
+    void DefineHamiltonian2(int p1, int p2, double coeff);  // b_p1 b+_p2
+    void DefineHamiltonian3(int p, double coeff);           // mu n + U n(n-1)
+    int nx_, ny_, d_;
+    double hop_x_, hop_y_, inter_, chem_;
+    bool px_, py_;
+};
+
+// Quantum-number tables of the MPS bonds (RealTensorSpace's quantum_table_ and
+// its model hooks, real_tensor_space.cc:716-736 and
+// model/space/real_spinless_bose_square_space.cc).
+class QuantumSpace {
+public:
+    virtual ~QuantumSpace() = default;
+    int num_site() const { return num_site_; }
+    int physics_dim() const { return d_; }
+    int num_quantum() const { return num_quantum_; }
+    const std::vector<std::vector<int>>& table(int bond) const { return qtab_[bond]; }
+    // physics index p with left + p == right, or -1
+    virtual int CheckQuantumTable(int site, const std::vector<int>& left, const std::vector<int>& right) const = 0;
+    virtual std::vector<int> MergeQuantumTable(const std::vector<int>& op, const std::vector<int>& space) const = 0;
+
+protected:
+    // Sorts a bond's rows by squared deviation from `mean` (ascending, the
+    // reference's quicksort order) (ReorderQuantumTable).
+    void ReorderQuantumTable(std::vector<std::vector<int>>& table, const std::vector<double>& mean);
+    int num_site_ = 0, d_ = 0, num_quantum_ = 1;
+    std::vector<std::vector<std::vector<int>>> qtab_;
+};
+
+class RealSpinlessBoseSquareSpace : public QuantumSpace {
+public:
+    RealSpinlessBoseSquareSpace(int nx, int ny, int num_boson, int physics_dim);
+    int CheckQuantumTable(int site, const std::vector<int>& left, const std::vector<int>& right) const override;
+    std::vector<int> MergeQuantumTable(const std::vector<int>& op, const std::vector<int>& space) const override;
+
+private:
+    int num_boson_;
+};
+
+}  // namespace dmrg

@@ -1,0 +1,60 @@
+// Batched FP64 SVD of the sector matrices of one canonicalisation, on the device.
+//
+// Algorithm: one-sided (Hestenes) Jacobi with 32-column blocks.  Each sector
+// matrix A (m x n) is held as a column-major working matrix W with c <= r
+// columns: W = A when n <= m (right rotations accumulate V), W = A^T otherwise
+// (they accumulate U).  A sweep visits every pair of column blocks once in the
+// round-robin order; in a round all pairs of all sectors are independent and
+// each is handled by one CTA: 64x64 Gram matrix of the pair, a few cyclic
+// Jacobi sweeps on it in shared memory, then the pair's columns of W and of the
+// accumulated rotation are multiplied by the 64x64 rotation.  Converged when no
+// pair has |g_ij| > tol * sqrt(g_ii g_jj) (high relative accuracy, which the
+// reference's canpre cut at 1e-12 needs).  Singular values are the final column
+// norms, sorted in descending order.
+#pragma once
+
+#include <vector>
+
+#include "common.cuh"
+
+namespace dmrg {
+
+struct SvdProblem {
+    int m, n;            // the sector matrix A is m x n
+    int rows, cols;      // working matrix W: rows x cols, cols <= rows, column-major (ld = rows)
+    int transposed;      // 1: W = A^T
+    int nbe;             // number of 32-column blocks, rounded up to even (>= 2)
+    int64_t w_off;       // offset of W in the W buffer (doubles)
+    int64_t q_off;       // offset of the accumulated rotation (cols x cols, column-major)
+    int64_t s_off;       // offset of the sorted singular values (cols doubles)
+    int64_t perm_off;    // offset of the sort permutation (cols ints)
+};
+
+struct SvdTask {
+    int problem;
+    int pair;
+};
+
+class BatchedSvd {
+public:
+    // Plans the batch for the given sector shapes (m[i] x n[i]; entries with
+    // m*n == 0 are skipped and report no singular values).
+    int plan(const std::vector<int>& m, const std::vector<int>& n, cudaStream_t st);
+    // Device address of sector i's working matrix W (fill it before run()).
+    double* w(int i) const { return d_w.as<double>() + probs[index[i]].w_off; }
+    bool active(int i) const { return index[i] >= 0; }
+    const SvdProblem& problem(int i) const { return probs[index[i]]; }
+    // Runs the Jacobi sweeps to convergence (sync per sweep) and sorts.
+    int run(cudaStream_t st, int* sweeps_out = nullptr);
+    // Sorted singular values of every active sector, copied to the host.
+    int singular_values(std::vector<std::vector<double>>& out, cudaStream_t st);
+
+    DeviceBuffer d_w, d_q, d_s, d_perm, d_probs, d_tasks, d_conv;
+    std::vector<SvdProblem> probs;
+    std::vector<int> index;             // sector -> problem (-1 when empty)
+    std::vector<int> round_first;       // task offset of each round
+    std::vector<SvdTask> tasks;
+    int max_rounds = 0;
+};
+
+}  // namespace dmrg

@@ -45,6 +45,7 @@ extern "C" {
 typedef struct dmrg_ctx_s* dmrg_ctx_t;
 typedef struct dmrg_heff_s* dmrg_heff_t;
 typedef struct dmrg_env_s* dmrg_env_t;
+typedef struct dmrg_canon_s* dmrg_canon_t;
 
 /* Shape of one block list: block k has sector indices (left[k], right[k]) and a
  * rows[k] x cols[k] row-major matrix.  Stands in for RealMatrixBlock's
@@ -157,6 +158,44 @@ int dmrg_env_flops(dmrg_env_t e, double* algorithmic, double* executed);
 /* env_out_dev = updated environment (overwritten).  Asynchronous. */
 int dmrg_env_apply(dmrg_env_t e, const double* ket_dev, const double* env_in_dev,
                    double* env_out_dev);
+
+/* ---- a6/a7: canonicalisation by per-sector SVD + truncation ---------------
+ * side 0 replaces RealTensorLattice::LeftCanonicalTensorLattice(int max_dim,
+ * double canonical_precision) (src/dmrg/realdmrg/real_tensor_lattice.h:186,
+ * .cc:558-676); side 1 replaces RightCanonicalTensorLattice (:194, .cc:794-911).
+ * left_dim[num_left_sector], right_dim[num_right_sector] are the lattice's
+ * sector dimensions; `ket` the site tensor's block list.  Three steps:
+ *   dmrg_canon_run: stacks each sector's blocks on the device, batched one-sided
+ *     Jacobi SVD, truncation exactly as ComputeTruncateDim (:501-555) -> the kept
+ *     dimension of every sector (tdim_out[num sectors]: right sectors for side 0,
+ *     left sectors for side 1) and the discarded weight (sum of dropped sigma^2,
+ *     which the reference does not report);
+ *   dmrg_canon_out_info / _out_blocks: sizes of the new ket (block order kept)
+ *     and of the canonical tensor (one block per sector; match_dim as the
+ *     reference's match_dim_);
+ *   dmrg_canon_write: new ket blocks (U or V^T slices) and canonical blocks
+ *     (S V^T or U S) into caller-allocated device buffers. */
+int dmrg_canon_create(dmrg_ctx_t ctx, int side, int num_left_sector, int num_right_sector,
+                      const int* left_dim, const int* right_dim, const dmrg_blocks_t* ket,
+                      dmrg_canon_t* out);
+int dmrg_canon_destroy(dmrg_canon_t c);
+int dmrg_canon_run(dmrg_canon_t c, const double* ket_dev, int max_dim, double canpre, int* tdim_out,
+                   double* discarded);
+int dmrg_canon_out_info(dmrg_canon_t c, int64_t* ket_size, int64_t* canonical_size, int* sweeps);
+int dmrg_canon_out_blocks(dmrg_canon_t c, int* ket_rows, int* ket_cols, int* canon_rows,
+                          int* canon_cols, int* match_dim);
+int dmrg_canon_singular_values(dmrg_canon_t c, int sector, int cap, double* values, int* count);
+int dmrg_canon_write(dmrg_canon_t c, const double* ket_dev, double* new_ket_dev, double* canonical_dev);
+
+/* ---- host bookkeeping helpers (no device work) ----------------------------
+ * dmrg_quicksort_index: the reference's QuickSort with index
+ * (src/util/general.ih:7-65), same tie order; descending != 0 for flag 0.
+ * dmrg_truncate_dims: ComputeTruncateDim over nsec sectors whose singular values
+ * are concatenated in `values` (counts[i] each; modified in place like the
+ * reference's array). */
+int dmrg_quicksort_index(double* values, int* index, int n, int descending);
+int dmrg_truncate_dims(int nsec, const int* counts, double* values, int max_dim, double canpre,
+                       int* tdim_out);
 
 #ifdef __cplusplus
 }

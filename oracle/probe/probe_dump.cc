@@ -71,6 +71,31 @@ void __real__ZN21RealTensorContraction29RightComputeTensorContractionEP17RealTen
     RealTensorContraction*, RealTensorLattice*, RealTensorOperator*, RealTensorContraction*);
 void __real__ZN17RealTensorLattice26LeftCanonicalTensorLatticeEid(RealTensorLattice*, int, double);
 void __real__ZN17RealTensorLattice27RightCanonicalTensorLatticeEid(RealTensorLattice*, int, double);
+void __real__ZN17RealTensorLattice20CombineTensorLatticeEiRiRPiS2_PS_(RealTensorLattice*, int, int&, int*&, int*&,
+                                                                      RealTensorLattice*);
+
+// CombineTensorLattice's first counting loop bounds its inner scan by the size
+// of the second list (real_tensor_lattice.cc:427-438).  Record every call whose
+// count differs from the plain union of the two sector lists.
+static FILE* g_combine = nullptr;
+void __wrap__ZN17RealTensorLattice20CombineTensorLatticeEiRiRPiS2_PS_(RealTensorLattice* self, int leigh, int& num,
+                                                                      int*& blocks, int*& dims,
+                                                                      RealTensorLattice* expan) {
+    const int n0 = leigh == 0 ? self->num_left_block_ : self->num_right_block_;
+    const int n1 = leigh == 0 ? expan->num_left_block_ : expan->num_right_block_;
+    const int* b0 = leigh == 0 ? self->left_block_ : self->right_block_;
+    const int* b1 = leigh == 0 ? expan->left_block_ : expan->right_block_;
+    int uni = n0;
+    for (int j = 0; j < n1; ++j) {
+        bool f = false;
+        for (int i = 0; i < n0; ++i) f = f || b0[i] == b1[j];
+        uni += !f;
+    }
+    __real__ZN17RealTensorLattice20CombineTensorLatticeEiRiRPiS2_PS_(self, leigh, num, blocks, dims, expan);
+    if (!g_combine) g_combine = std::fopen((g_out + "/combine.txt").c_str(), "w");
+    std::fprintf(g_combine, "%d %d %d %d %d%s\n", leigh, n0, n1, uni, num, uni != num ? " MISMATCH" : "");
+    std::fflush(g_combine);
+}
 
 void __wrap__ZN17RealTensorLanczos13LanczosMethodEiiRd(RealTensorLanczos* self, int niter, int site,
                                                        double& result) {
