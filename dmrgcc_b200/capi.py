@@ -74,6 +74,16 @@ _SIGS = {
     "dmrg_canon_write": (C.c_int, [_VP, _VP, _VP, _VP]),
     "dmrg_quicksort_index": (C.c_int, [_D, _I, C.c_int, C.c_int]),
     "dmrg_truncate_dims": (C.c_int, [C.c_int, _I, _D, C.c_int, C.c_double, _I]),
+    "dmrg_run_create": (C.c_int, [_VP, C.c_char_p, C.c_char_p, _VP, C.POINTER(_VP)]),
+    "dmrg_run_execute": (C.c_int, [_VP]),
+    "dmrg_run_destroy": (C.c_int, [_VP]),
+    "dmrg_run_half_sweeps": (C.c_int, [_VP, C.c_int, _D, _D, _I]),
+    "dmrg_run_steps": (C.c_int, [_VP, C.c_int, _I, _I, _D, _I, _D, _I64, _D, _I]),
+    "dmrg_model_create": (C.c_int, [C.c_char_p, C.c_char_p, C.POINTER(_VP)]),
+    "dmrg_model_destroy": (C.c_int, [_VP]),
+    "dmrg_model_info": (C.c_int, [_VP, _I, _I, _I]),
+    "dmrg_model_mpo": (C.c_int, [_VP, C.c_int, _I, _I, C.c_int, _D]),
+    "dmrg_model_quantum_table": (C.c_int, [_VP, C.c_int, C.c_int, C.c_int, _I, _I]),
     "dmrg_env_create": (C.c_int, [_VP, C.c_int, C.c_int, C.c_int, _I, C.POINTER(Blocks), C.c_int, C.c_int, C.c_int,
                                   _D, C.POINTER(Blocks), C.c_int, C.POINTER(_VP)]),
     "dmrg_env_destroy": (C.c_int, [_VP]),
@@ -411,3 +421,95 @@ def truncate_dims(svals, max_dim: int, canpre: float):
         out.append(flat[pos:pos + c].copy())
         pos += c
     return t[:len(svals)], out
+
+
+class RunOptions(C.Structure):
+    """dmrg_run_options_t."""
+
+    _fields_ = [("precision", C.c_int), ("verbose", C.c_int), ("seed", C.c_uint),
+                ("stop_after_half_sweeps", C.c_int), ("lanczos_precision", C.c_double)]
+
+
+class Run:
+    """A whole DMRG run of a reference input file on the device (RealTensorRundmrg)."""
+
+    def __init__(self, ctx: Context, input_path: str, model: str = "real_spinless_bose_square", verbose: int = 0,
+                 seed: int = 1, stop_after_half_sweeps: int = -1, precision: int = DMRG_PREC_FP64):
+        self.ctx = ctx
+        self._opt = RunOptions(precision, verbose, seed, stop_after_half_sweeps, 0.0)
+        h = _VP()
+        check(lib().dmrg_run_create(ctx.h, input_path.encode(), model.encode(), C.byref(self._opt), C.byref(h)),
+              "dmrg_run_create")
+        self.h = h
+
+    def execute(self) -> None:
+        check(lib().dmrg_run_execute(self.h), "dmrg_run_execute")
+
+    def half_sweeps(self):
+        n = C.c_int()
+        check(lib().dmrg_run_half_sweeps(self.h, 0, None, None, C.byref(n)), "dmrg_run_half_sweeps")
+        e, s = np.zeros(max(n.value, 1)), np.zeros(max(n.value, 1))
+        check(lib().dmrg_run_half_sweeps(self.h, n.value, _dptr(e), _dptr(s), C.byref(n)), "dmrg_run_half_sweeps")
+        return e[:n.value], s[:n.value]
+
+    def steps(self) -> dict:
+        n = C.c_int()
+        check(lib().dmrg_run_steps(self.h, 0, None, None, None, None, None, None, None, C.byref(n)), "dmrg_run_steps")
+        k = max(n.value, 1)
+        hs, st, dims = (np.zeros(k, np.int32) for _ in range(3))
+        en, dis, sec = (np.zeros(k) for _ in range(3))
+        psi = np.zeros(k, np.int64)
+        check(lib().dmrg_run_steps(self.h, n.value, _iptr(hs), _iptr(st), _dptr(en), _iptr(dims), _dptr(dis),
+                                   psi.ctypes.data_as(_I64), _dptr(sec), C.byref(n)), "dmrg_run_steps")
+        m = n.value
+        return {"half_sweep": hs[:m], "site": st[:m], "energy": en[:m], "lanczos_dim": dims[:m],
+                "discarded": dis[:m], "psi_dim": psi[:m], "seconds": sec[:m]}
+
+    def close(self) -> None:
+        if self.h:
+            lib().dmrg_run_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Model:
+    """The model layer (MPO and quantum tables) of an input file; host only."""
+
+    def __init__(self, input_path: str, model: str = "real_spinless_bose_square"):
+        h = _VP()
+        check(lib().dmrg_model_create(input_path.encode(), model.encode(), C.byref(h)), "dmrg_model_create")
+        self.h = h
+        a, b, c = C.c_int(), C.c_int(), C.c_int()
+        check(lib().dmrg_model_info(h, C.byref(a), C.byref(b), C.byref(c)), "dmrg_model_info")
+        self.num_site, self.physics_dim, self.num_quantum = a.value, b.value, c.value
+
+    def mpo(self, site: int) -> np.ndarray:
+        lb, rb = C.c_int(), C.c_int()
+        check(lib().dmrg_model_mpo(self.h, site, C.byref(lb), C.byref(rb), 0, None), "dmrg_model_mpo")
+        d = self.physics_dim
+        w = np.zeros(lb.value * rb.value * d * d)
+        check(lib().dmrg_model_mpo(self.h, site, C.byref(lb), C.byref(rb), w.size, _dptr(w)), "dmrg_model_mpo")
+        return w.reshape(lb.value, rb.value, d, d)
+
+    def quantum_table(self, which: int, bond: int) -> np.ndarray:
+        rows = C.c_int()
+        check(lib().dmrg_model_quantum_table(self.h, which, bond, 0, None, C.byref(rows)), "quantum_table")
+        v = np.zeros(max(rows.value * self.num_quantum, 1), np.int32)
+        check(lib().dmrg_model_quantum_table(self.h, which, bond, v.size, _iptr(v), C.byref(rows)), "quantum_table")
+        return v[:rows.value * self.num_quantum].reshape(rows.value, self.num_quantum)
+
+    def close(self) -> None:
+        if self.h:
+            lib().dmrg_model_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

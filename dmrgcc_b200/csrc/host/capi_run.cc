@@ -1,0 +1,174 @@
+// C ABI of the sweep engine: runs a reference input file end to end, and
+// exposes the model layer (MPO, quantum tables) for inspection.
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+
+#include "dmrg_b200.h"
+#include "host/engine.h"
+#include "host/input.h"
+#include "host/model.h"
+
+using namespace dmrg;
+
+namespace {
+
+struct ModelSpec {
+    std::unique_ptr<QuantumSpace> space;
+    std::unique_ptr<RealTensorHamiltonian> ham;
+};
+
+// The model executables' main() (model/real_spinless_bose_square_model.cc:11-35):
+// read the model keys and build the space and the Hamiltonian.
+ModelSpec make_model(InputGroup& input, const std::string& model) {
+    ModelSpec m;
+    if (model != "real_spinless_bose_square")
+        throw std::runtime_error("unknown model '" + model + "' (supported: real_spinless_bose_square)");
+    const int nx = input.getInt("num_site_x");
+    const int ny = input.getInt("num_site_y");
+    const int nb = input.getInt("num_boson");
+    const int d = input.getInt("physics_dim", 2);
+    const double flux = input.getDouble("flux");
+    const double jx = input.getDouble("Jx");
+    const double jy = input.getDouble("Jy");
+    const double u = input.getDouble("U");
+    const double mu = input.getDouble("mu");
+    const bool px = input.getBool("period_x");
+    const bool py = input.getBool("period_y");
+    m.space.reset(new RealSpinlessBoseSquareSpace(nx, ny, nb, d));
+    m.ham.reset(new RealSpinlessBoseSquareHamiltonian(nx, ny, d, flux * 3.14159265358979323846, jx, jy, u, mu, px, py));
+    return m;
+}
+
+}  // namespace
+
+struct dmrg_run_s {
+    std::unique_ptr<Engine> engine;
+    double total_seconds = 0.0;
+};
+
+struct dmrg_model_s {
+    ModelSpec spec;
+};
+
+extern "C" {
+
+int dmrg_run_create(dmrg_ctx_t ctx, const char* input_path, const char* model, const dmrg_run_options_t* opt,
+                    dmrg_run_t* out) {
+    if (!ctx || !input_path || !out) return set_error(DMRG_E_ARG, "null argument");
+    *out = nullptr;
+    try {
+        RunOptions o;
+        if (opt) {
+            o.precision = opt->precision;
+            o.verbose = opt->verbose;
+            o.seed = opt->seed ? opt->seed : 1;
+            o.stop_after_half_sweeps = opt->stop_after_half_sweeps;
+            if (opt->lanczos_precision > 0) o.lanczos_precision = opt->lanczos_precision;
+        }
+        InputGroup input(input_path, "input", o.verbose != 0);
+        ModelSpec m = make_model(input, model ? model : "real_spinless_bose_square");
+        auto* r = new dmrg_run_s();
+        r->engine.reset(new Engine(ctx, std::move(m.space), std::move(m.ham), input, o));
+        *out = r;
+        return DMRG_OK;
+    } catch (const std::exception& e) {
+        return set_error(DMRG_E_ARG, "%s", e.what());
+    }
+}
+
+int dmrg_run_execute(dmrg_run_t r) {
+    if (!r) return set_error(DMRG_E_ARG, "null run");
+    return r->engine->Run();
+}
+
+int dmrg_run_destroy(dmrg_run_t r) {
+    delete r;
+    return DMRG_OK;
+}
+
+int dmrg_run_half_sweeps(dmrg_run_t r, int cap, double* energies, double* seconds, int* count) {
+    if (!r || !count) return set_error(DMRG_E_ARG, "null argument");
+    const auto& e = r->engine->half_sweep_energies();
+    const auto& s = r->engine->half_sweep_seconds();
+    *count = (int)e.size();
+    for (int i = 0; i < (int)e.size() && i < cap; ++i) {
+        if (energies) energies[i] = e[i];
+        if (seconds) seconds[i] = s[i];
+    }
+    return DMRG_OK;
+}
+
+int dmrg_run_steps(dmrg_run_t r, int cap, int* half_sweep, int* site, double* energy, int* lanczos_dim,
+                   double* discarded, int64_t* psi_dim, double* seconds, int* count) {
+    if (!r || !count) return set_error(DMRG_E_ARG, "null argument");
+    const auto& rec = r->engine->records();
+    *count = (int)rec.size();
+    for (int i = 0; i < (int)rec.size() && i < cap; ++i) {
+        if (half_sweep) half_sweep[i] = rec[i].half_sweep;
+        if (site) site[i] = rec[i].site;
+        if (energy) energy[i] = rec[i].energy;
+        if (lanczos_dim) lanczos_dim[i] = rec[i].lanczos_dim;
+        if (discarded) discarded[i] = rec[i].discarded;
+        if (psi_dim) psi_dim[i] = rec[i].psi_dim;
+        if (seconds) seconds[i] = rec[i].seconds;
+    }
+    return DMRG_OK;
+}
+
+int dmrg_model_create(const char* input_path, const char* model, dmrg_model_t* out) {
+    if (!input_path || !out) return set_error(DMRG_E_ARG, "null argument");
+    *out = nullptr;
+    try {
+        InputGroup input(input_path, "input", false);
+        auto* m = new dmrg_model_s();
+        m->spec = make_model(input, model ? model : "real_spinless_bose_square");
+        m->spec.ham->DefineTensorHamiltonian();
+        *out = m;
+        return DMRG_OK;
+    } catch (const std::exception& e) {
+        return set_error(DMRG_E_ARG, "%s", e.what());
+    }
+}
+
+int dmrg_model_destroy(dmrg_model_t m) {
+    delete m;
+    return DMRG_OK;
+}
+
+int dmrg_model_info(dmrg_model_t m, int* num_site, int* physics_dim, int* num_quantum) {
+    if (!m) return set_error(DMRG_E_ARG, "null model");
+    if (num_site) *num_site = m->spec.space->num_site();
+    if (physics_dim) *physics_dim = m->spec.space->physics_dim();
+    if (num_quantum) *num_quantum = m->spec.space->num_quantum();
+    return DMRG_OK;
+}
+
+int dmrg_model_mpo(dmrg_model_t m, int site, int* left_bond, int* right_bond, int cap, double* W) {
+    if (!m || !left_bond || !right_bond) return set_error(DMRG_E_ARG, "null argument");
+    if (site < 0 || site >= m->spec.ham->num_site()) return set_error(DMRG_E_ARG, "site out of range");
+    const RealTensorOperator& op = m->spec.ham->get_tensor_hamiltonian(site);
+    *left_bond = op.get_left_bond();
+    *right_bond = op.get_right_bond();
+    const auto& v = op.data();
+    if (W)
+        for (int i = 0; i < (int)v.size() && i < cap; ++i) W[i] = v[i];
+    return DMRG_OK;
+}
+
+int dmrg_model_quantum_table(dmrg_model_t m, int which, int bond, int cap, int* values, int* rows) {
+    if (!m || !rows) return set_error(DMRG_E_ARG, "null argument");
+    if (bond < 0 || bond > m->spec.space->num_site()) return set_error(DMRG_E_ARG, "bond out of range");
+    const auto& t = which == 0 ? m->spec.space->table(bond) : m->spec.ham->quantum_table(bond);
+    *rows = (int)t.size();
+    int k = 0;
+    for (const auto& row : t)
+        for (int q : row) {
+            if (values && k < cap) values[k] = q;
+            ++k;
+        }
+    return DMRG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,150 @@
+// The DMRG sweep engine: the reference's lattice / space / contraction /
+// network / Lanczos / sweep-driver classes (src/dmrg/realdmrg/*) with every
+// tensor resident on the device.  Host code keeps the sector bookkeeping (block
+// maps, truncation, the glibc rand() stream of the initial MPS and of the
+// subspace expansion) identical to the reference; all arithmetic runs in
+// libdmrg_b200's kernels.
+#pragma once
+
+#include <cstdio>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "blockops.cuh"
+#include "blocksparse.h"
+#include "common.cuh"
+#include "host/input.h"
+#include "host/model.h"
+#include "vec.cuh"
+
+namespace dmrg {
+
+// RealMatrixBlock with its values on the device (packed, list order).
+struct DevBlocks {
+    BlockListDesc d;
+    DeviceBuffer buf;
+    double* ptr() const { return buf.as<double>(); }
+    int alloc(cudaStream_t st, bool zero);
+    void set_shape_zero() {  // ResetMatrixBlock: every block 0 x 0
+        for (int k = 0; k < d.count(); ++k) d.rows[k] = d.cols[k] = 0;
+        d.size = 0;
+        for (int k = 0; k < d.count(); ++k) d.off[k] = 0;
+    }
+};
+
+// RealTensorLattice (real_tensor_lattice.h:10-42).
+struct TensorLattice {
+    int physics_dim = 0;
+    std::vector<int> left_block, left_dim, right_block, right_dim;
+    std::vector<int> phys;  // [num_left x num_right], -1: no block
+    DevBlocks ket;
+    bool has_canonical = false;
+    DevBlocks canonical;
+    std::vector<int> match_dim;
+    int nl() const { return (int)left_block.size(); }
+    int nr() const { return (int)right_block.size(); }
+    int p(int l, int r) const { return phys[(size_t)l * nr() + r]; }
+    int64_t psi_dim() const { return ket.d.size; }
+};
+
+// One environment (all MPO bond indices of one side), packed index-major.
+struct EnvData {
+    EnvDesc desc;
+    DeviceBuffer buf;
+    double* ptr() const { return buf.as<double>(); }
+};
+
+// RealTensorContraction (real_tensor_contraction.h:8-16): left/right environments.
+struct TensorContraction {
+    int left_bond = 0, right_bond = 0;
+    EnvData L, R;
+};
+
+struct SweepRecord {  // one site step
+    int half_sweep, site, direction;  // direction 0: left->right
+    double energy;
+    int lanczos_dim;
+    double discarded;
+    int64_t psi_dim;
+    double seconds;
+};
+
+struct RunOptions {
+    int precision = DMRG_PREC_FP64;
+    int verbose = 1;
+    double lanczos_precision = 1e-15;  // hard-coded in the reference (real_tensor_lanczos.cc:29-30)
+    double zero_tolerance = 1e-15;
+    unsigned seed = 1;                  // glibc rand() seed; 1 = the reference's implicit seed
+    int stop_after_half_sweeps = -1;    // run only this many half-sweeps (-1: all)
+};
+
+class Engine {
+public:
+    Engine(dmrg_ctx_t ctx, std::unique_ptr<QuantumSpace> space, std::unique_ptr<RealTensorHamiltonian> ham,
+           InputGroup& input, const RunOptions& opt);
+    ~Engine();
+    // RealTensorRundmrg::Run (real_tensor_rundmrg.cc:115-245).
+    int Run();
+    const std::vector<SweepRecord>& records() const { return records_; }
+    double last_energy() const { return energy_; }
+    const std::vector<double>& half_sweep_energies() const { return half_energies_; }
+    const std::vector<double>& half_sweep_seconds() const { return half_seconds_; }
+    TensorLattice& lattice(int i) { return *lat_[i]; }
+    TensorContraction& contraction(int i) { return *con_[i]; }
+    int num_site() const { return n_; }
+
+    // building blocks (public for the C ABI and tests)
+    int Initialize();
+    int DefineTensorSpace(int initial_block, int initial_dim);
+    int CanonicalTensorSpace(int leigh, int site, double* discarded = nullptr);
+    int MergeTensorSpace(int leigh, int site);
+    int ExpanTensorSpace(int leigh, int site);
+    int MatchTensorSpace(int leigh, int site);
+    int ExpanTensorNetwork(int leigh, int site);
+    int ComputeTensorNetwork(int leigh, int site);
+    int LanczosMethod(int niter, int site, double& energy, int& dim);
+
+private:
+    // bookkeeping (host)
+    void ComputeLatticeBlock(int site, std::vector<int>& left_block, std::vector<int>& right_block);
+    void ComputeTensorIndex(int site, std::vector<int>& li, std::vector<int>& ri, std::vector<int>& pi);
+    void DefineLatticeSectors(TensorLattice& t, const std::vector<int>& lb, const std::vector<int>& rb,
+                              const std::vector<int>& ld, const std::vector<int>& rd);
+    int DefineLatticeBlocks(TensorLattice& t, const std::vector<int>& li, const std::vector<int>& ri,
+                            const std::vector<int>& pi, int row, int column);
+    void ComputeExpanTensorLattice(int leigh, int site, std::vector<std::vector<int>>& mapping);
+    int LeftExpanTensorContraction(int site, const std::vector<std::vector<int>>& mapping);
+    int RightExpanTensorContraction(int site, const std::vector<std::vector<int>>& mapping);
+    int ExpanLattice(int leigh, TensorLattice& t, const TensorLattice& origin, const TensorLattice* expan);
+    int Normalize(TensorLattice& t);
+    void DefineTensorNetwork();
+    int ResetEnv(int leigh, int site);
+
+    dmrg_ctx_t ctx_;
+    cudaStream_t st_;
+    RunOptions opt_;
+    std::unique_ptr<QuantumSpace> space_;
+    std::unique_ptr<RealTensorHamiltonian> ham_;
+    int n_ = 0;
+    std::vector<std::unique_ptr<TensorLattice>> lat_;
+    std::vector<std::unique_ptr<TensorContraction>> con_;
+    std::unique_ptr<TensorLattice> expan_;
+    // sweep table (real_tensor_rundmrg.cc:70-113)
+    int num_sweep_ = 0;
+    std::vector<int> max_dim_, max_block_, num_iter_;
+    std::vector<double> canpre_, noise_;
+    int first_block_ = 0, first_dim_ = 0;
+    // current parameters (RealTensorSpace::DefineTensorSpaceParameter)
+    int p_max_block_ = 0, p_max_dim_ = -1;
+    double p_canpre_ = 1e-30, p_noise_ = 10.0;
+    // scratch
+    DeviceBuffer copy_tasks_, scratch_, scratch2_, norm_;
+    ReduceScratch rs_;
+    std::vector<SweepRecord> records_;
+    std::vector<double> half_energies_, half_seconds_;
+    double energy_ = 0.0;
+    int half_sweep_ = 0;
+};
+
+}  // namespace dmrg

@@ -46,6 +46,8 @@ typedef struct dmrg_ctx_s* dmrg_ctx_t;
 typedef struct dmrg_heff_s* dmrg_heff_t;
 typedef struct dmrg_env_s* dmrg_env_t;
 typedef struct dmrg_canon_s* dmrg_canon_t;
+typedef struct dmrg_run_s* dmrg_run_t;
+typedef struct dmrg_model_s* dmrg_model_t;
 
 /* Shape of one block list: block k has sector indices (left[k], right[k]) and a
  * rows[k] x cols[k] row-major matrix.  Stands in for RealMatrixBlock's
@@ -186,6 +188,46 @@ int dmrg_canon_out_blocks(dmrg_canon_t c, int* ket_rows, int* ket_cols, int* can
                           int* canon_cols, int* match_dim);
 int dmrg_canon_singular_values(dmrg_canon_t c, int sector, int cap, double* values, int* count);
 int dmrg_canon_write(dmrg_canon_t c, const double* ket_dev, double* new_ket_dev, double* canonical_dev);
+
+/* ---- whole runs: the sweep engine ------------------------------------------
+ * dmrg_run_create reads a reference input file (the model keys of
+ * model/real_spinless_bose_square_model.cc:11-35 plus the RealTensorRundmrg keys
+ * and sweep table, real_tensor_rundmrg.cc:3-113), builds the quantum-number
+ * tables and the MPO on the host, and the initial MPS on the device
+ * (RealTensorSpace::DefineTensorSpace, glibc rand() seeded with opt->seed, 1 =
+ * the reference's implicit seed).  dmrg_run_execute replaces
+ * RealTensorRundmrg::Run (:115-245): every site step (Lanczos, subspace
+ * expansion, SVD truncation, environment update, merge) runs on the device.
+ * model: "real_spinless_bose_square" (NULL = that). */
+typedef struct {
+    int precision;              /* DMRG_PREC_FP64 */
+    int verbose;                /* 1: print like the reference */
+    unsigned seed;              /* 0 or 1: the reference's stream */
+    int stop_after_half_sweeps; /* -1: the whole table */
+    double lanczos_precision;   /* 0: the reference's 1e-15 */
+} dmrg_run_options_t;
+int dmrg_run_create(dmrg_ctx_t ctx, const char* input_path, const char* model,
+                    const dmrg_run_options_t* opt, dmrg_run_t* out);
+int dmrg_run_execute(dmrg_run_t r);
+int dmrg_run_destroy(dmrg_run_t r);
+/* Energy after each half-sweep (the reference's "right/left energy =" lines)
+ * and its wall time. */
+int dmrg_run_half_sweeps(dmrg_run_t r, int cap, double* energies, double* seconds, int* count);
+/* One record per site step: half-sweep index, site, Lanczos energy, Krylov
+ * dimension, discarded weight of the truncation, psi_dim, seconds. */
+int dmrg_run_steps(dmrg_run_t r, int cap, int* half_sweep, int* site, double* energy, int* lanczos_dim,
+                   double* discarded, int64_t* psi_dim, double* seconds, int* count);
+
+/* ---- model layer (host only) -----------------------------------------------
+ * The MPO of RealSpinlessBoseSquareHamiltonian::DefineTensorHamiltonian
+ * (model/hamiltonian/real_spinless_bose_square_hamiltonian.cc:171-228) and the
+ * quantum tables (which 0: MPS bonds, RealTensorSpace; 1: MPO bonds,
+ * RealTensorHamiltonian), built from an input file without a GPU. */
+int dmrg_model_create(const char* input_path, const char* model, dmrg_model_t* out);
+int dmrg_model_destroy(dmrg_model_t m);
+int dmrg_model_info(dmrg_model_t m, int* num_site, int* physics_dim, int* num_quantum);
+int dmrg_model_mpo(dmrg_model_t m, int site, int* left_bond, int* right_bond, int cap, double* W);
+int dmrg_model_quantum_table(dmrg_model_t m, int which, int bond, int cap, int* values, int* rows);
 
 /* ---- host bookkeeping helpers (no device work) ----------------------------
  * dmrg_quicksort_index: the reference's QuickSort with index

@@ -1,0 +1,64 @@
+"""Exact diagonalisation of the spin-less Bose-Hubbard model in a fixed-N
+sector (test infrastructure): an algorithm-independent check of DMRG energies
+for small lattices.
+
+Conventions follow the reference's MPO (model/hamiltonian/
+real_spinless_bose_square_hamiltonian.cc): H = sum over bonds <p0,p1> of
+J (b+_p0 b_p1 + b_p0 b+_p1) + sum_i [mu n_i + U n_i (n_i - 1)], J = Jx on
+x-bonds and Jy on y-bonds, sites ordered p = j + i * Ny, periodic wraps only
+for a dimension of more than two sites."""
+from __future__ import annotations
+
+import itertools
+
+import numpy as np
+import scipy.sparse as sp
+import scipy.sparse.linalg as sla
+
+
+def bonds(nx: int, ny: int, px: bool, py: bool):
+    out = []
+    for i in range(nx):
+        for j in range(ny):
+            p0 = j + i * ny
+            if i + 1 < nx:
+                out.append((p0, j + (i + 1) * ny, "x"))
+            elif nx > 2 and px:
+                out.append((j, p0, "x"))
+            if j + 1 < ny:
+                out.append((p0, (j + 1) + i * ny, "y"))
+            elif ny > 2 and py:
+                out.append((i * ny, p0, "y"))
+    return out
+
+
+def ground_energy(nx: int, ny: int, nboson: int, d: int, jx: float, jy: float, u: float, mu: float,
+                  px: bool = False, py: bool = False) -> float:
+    L = nx * ny
+    states = [s for s in itertools.product(range(d), repeat=L) if sum(s) == nboson]
+    index = {s: k for k, s in enumerate(states)}
+    rows, cols, vals = [], [], []
+    for k, s in enumerate(states):
+        diag = sum(mu * n + u * n * (n - 1) for n in s)
+        rows.append(k)
+        cols.append(k)
+        vals.append(diag)
+        for a, b, kind in bonds(nx, ny, px, py):
+            J = jx if kind == "x" else jy
+            if J == 0:
+                continue
+            for src, dst in ((a, b), (b, a)):  # b+_dst b_src
+                if s[src] == 0 or s[dst] == d - 1:
+                    continue
+                t = list(s)
+                amp = np.sqrt(t[src]) * np.sqrt(t[dst] + 1)
+                t[src] -= 1
+                t[dst] += 1
+                rows.append(index[tuple(t)])
+                cols.append(k)
+                vals.append(J * amp)
+    n = len(states)
+    H = sp.csr_matrix((vals, (rows, cols)), shape=(n, n))
+    if n < 400:
+        return float(np.linalg.eigvalsh(H.toarray())[0])
+    return float(sla.eigsh(H, k=1, which="SA")[0][0])

@@ -100,6 +100,23 @@ void __wrap__ZN17RealTensorLattice20CombineTensorLatticeEiRiRPiS2_PS_(RealTensor
 void __wrap__ZN17RealTensorLanczos13LanczosMethodEiiRd(RealTensorLanczos* self, int niter, int site,
                                                        double& result) {
     int call = n_lanczos++;
+    if (call == 0) {  // the MPO and the quantum tables, once
+        NacWriter w(g_out + "/model.nac");
+        RealTensorHamiltonian* H = self->hamiltonian_;
+        RealTensorSpace* S = self->space_;
+        w.scalar_i("num_site", H->num_site_);
+        for (int i = 0; i < H->num_site_; ++i) probe::write_operator(w, "op" + std::to_string(i), H->tensor_hamiltonian_[i]);
+        for (int b = 0; b <= H->num_site_; ++b) {
+            std::vector<int> q;
+            for (int j = 0; j < H->num_table_[b]; ++j)
+                for (int k = 0; k < H->num_quantum_; ++k) q.push_back(H->quantum_table_[b][j][k]);
+            w.ints("hq" + std::to_string(b), q);
+            std::vector<int> sq;
+            for (int j = 0; j < S->num_table_[b]; ++j)
+                for (int k = 0; k < S->num_quantum_; ++k) sq.push_back(S->quantum_table_[b][j][k]);
+            w.ints("sq" + std::to_string(b), sq);
+        }
+    }
     RealTensorLattice* lat = self->space_->get_tensor_lattice(site);
     RealTensorOperator* op = self->hamiltonian_->get_tensor_hamiltonian(site);
     RealTensorContraction* con = self->network_->get_tensor_contraction(site);

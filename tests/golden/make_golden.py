@@ -10,6 +10,8 @@ chain16_spinless.in), and keeps:
   lanczos_c<k>.nac      the energy and ground vector LanczosMethod returned
   env_c<k>.nac          an environment update, inputs and outputs
   canon_c<k>.nac        a canonicalisation (SVD truncation), before and after
+  steps_chain6.txt, steps_cylinder3x3.txt   whole runs of two small inputs
+  model_chain16.nac     the MPO per site and the quantum tables (first call)
   quicksort_cases.txt   inputs with ties and the index order the reference's
                         QuickSort (src/util/general.ih) returns (probe_sort)
 
@@ -78,6 +80,11 @@ def main() -> int:
         "PROBE_CANON": ",".join(map(str, CANON_CALLS)),
     })
     shutil.copy(os.path.join(tmp, "steps.txt"), os.path.join(HERE, "steps_chain16.txt"))
+    shutil.copy(os.path.join(tmp, "model.nac"), os.path.join(HERE, "model_chain16.nac"))
+    for name in ("chain6", "cylinder3x3"):
+        t = tempfile.mkdtemp(prefix="golden_" + name)
+        run_probe(os.path.join(ROOT, "dmrgcc_b200", "inputs", f"{name}_spinless.in"), t, {})
+        shutil.copy(os.path.join(t, "steps.txt"), os.path.join(HERE, f"steps_{name}.txt"))
     for kind, calls in (("heff", HEFF_CALLS), ("lanczos", HEFF_CALLS), ("env", ENV_CALLS), ("canon", CANON_CALLS)):
         for c in calls:
             shutil.copy(os.path.join(tmp, f"{kind}_{c}.nac"), os.path.join(HERE, f"{kind}_c{c}.nac"))
@@ -92,6 +99,7 @@ def main() -> int:
             subprocess.run([PROBE, inp2], env=env2, stdout=log, stderr=subprocess.STDOUT, check=True, cwd=tmp2)
         shutil.copy(os.path.join(tmp2, "heff_388.nac"), os.path.join(HERE, "heff_struct_cyl8x4_D1024.nac"))
         shutil.copy(os.path.join(tmp2, "steps.txt"), os.path.join(HERE, "steps_cyl8x4_to_D1024.txt"))
+        shutil.copy(os.path.join(tmp2, "model.nac"), os.path.join(HERE, "model_cyl8x4.nac"))
     return 0
 
 
