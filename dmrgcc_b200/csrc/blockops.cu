@@ -25,9 +25,17 @@ __global__ void scale_by_kernel(double* __restrict__ x, int64_t n, const double*
 
 }  // namespace
 
-int launch_rect_copies(const std::vector<RectCopy>& tasks, const double* src, double* dst, DeviceBuffer& scratch,
-                       cudaStream_t st) {
+int launch_rect_copies(const std::vector<RectCopy>& tasks, const double* src, int64_t src_size, double* dst,
+                       int64_t dst_size, DeviceBuffer& scratch, cudaStream_t st) {
     if (tasks.empty()) return DMRG_OK;
+    for (const RectCopy& t : tasks) {
+        if (t.rows <= 0 || t.cols <= 0) continue;
+        const int64_t se = t.src_off + (int64_t)(t.rows - 1) * t.src_ld + t.cols;
+        const int64_t de = t.dst_off + (int64_t)(t.rows - 1) * t.dst_ld + t.cols;
+        if (t.src_off < 0 || t.dst_off < 0 || se > src_size || de > dst_size || t.cols > t.src_ld || t.cols > t.dst_ld)
+            return set_error(DMRG_E_ARG, "block copy outside its buffers (src end %lld of %lld, dst end %lld of %lld)",
+                             (long long)se, (long long)src_size, (long long)de, (long long)dst_size);
+    }
     DMRG_TRY(scratch.alloc(tasks.size() * sizeof(RectCopy)));
     DMRG_CUDA_TRY(cudaMemcpyAsync(scratch.ptr, tasks.data(), tasks.size() * sizeof(RectCopy), cudaMemcpyHostToDevice,
                                   st));

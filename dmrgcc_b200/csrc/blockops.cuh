@@ -21,8 +21,9 @@ struct RectCopy {
 
 // dst[dst_off + i*dst_ld + j] = scale * src[src_off + i*src_ld + j] for every task.
 // `scratch` keeps the uploaded task list alive until the launch has run.
-int launch_rect_copies(const std::vector<RectCopy>& tasks, const double* src, double* dst, DeviceBuffer& scratch,
-                       cudaStream_t st);
+// Every rectangle is checked against src_size / dst_size (doubles) first.
+int launch_rect_copies(const std::vector<RectCopy>& tasks, const double* src, int64_t src_size, double* dst,
+                       int64_t dst_size, DeviceBuffer& scratch, cudaStream_t st);
 
 // x *= s (s read on the device)
 int launch_scale_by(double* x, int64_t n, const double* s, bool inverse, cudaStream_t st);

@@ -65,7 +65,7 @@ __global__ void gather_kernel(const double* __restrict__ ket, const CopyTask* __
 __global__ void write_ket_kernel(const WriteTask* __restrict__ tasks, const SvdProblem* __restrict__ probs,
                                  const double* __restrict__ W, const double* __restrict__ Q,
                                  const double* __restrict__ sig, const int* __restrict__ perm,
-                                 double* __restrict__ out, int side) {
+                                 const double* __restrict__ sgn, double* __restrict__ out, int side) {
     const WriteTask t = tasks[blockIdx.x];
     const SvdProblem p = probs[t.problem];
     const double* w = W + p.w_off;
@@ -83,6 +83,7 @@ __global__ void write_ket_kernel(const WriteTask* __restrict__ tasks, const SvdP
             } else {
                 v = q[(int64_t)k * p.m + row];
             }
+            v *= sgn[p.s_off + j];
         } else {  // V^T[i][col0 + j] = v_i[col0 + j]
             const int k = perm[p.perm_off + i];
             const int col = t.off + j;
@@ -92,6 +93,7 @@ __global__ void write_ket_kernel(const WriteTask* __restrict__ tasks, const SvdP
                 const double s = sig[p.s_off + i];
                 v = s > 0.0 ? w[(int64_t)k * p.n + col] / s : 0.0;
             }
+            v *= sgn[p.s_off + i];
         }
         out[t.out_off + e] = v;
     }
@@ -101,7 +103,8 @@ __global__ void write_ket_kernel(const WriteTask* __restrict__ tasks, const SvdP
 __global__ void write_canonical_kernel(const CanonTask* __restrict__ tasks, const SvdProblem* __restrict__ probs,
                                        const double* __restrict__ W, const double* __restrict__ Q,
                                        const double* __restrict__ sig, const int* __restrict__ perm,
-                                       const double* __restrict__ forced, double* __restrict__ out, int side) {
+                                       const double* __restrict__ forced, const double* __restrict__ sgn,
+                                       double* __restrict__ out, int side) {
     const CanonTask t = tasks[blockIdx.x];
     const int64_t total = (int64_t)t.rows * t.cols;
     if (t.problem < 0) {
@@ -123,6 +126,7 @@ __global__ void write_canonical_kernel(const CanonTask* __restrict__ tasks, cons
                 const double s = sig[p.s_off + i];
                 v = s > 0.0 ? sf * w[(int64_t)k * p.n + j] / s : 0.0;
             }
+            v *= sgn[p.s_off + i];
         } else {  // u_j[i] * s_j
             const int k = perm[p.perm_off + j];
             const double sf = forced[t.sig_off + j];
@@ -132,6 +136,7 @@ __global__ void write_canonical_kernel(const CanonTask* __restrict__ tasks, cons
             } else {
                 v = sf * q[(int64_t)k * p.m + i];
             }
+            v *= sgn[p.s_off + j];
         }
         out[t.out_off + e] = v;
     }
@@ -364,11 +369,11 @@ int dmrg_canon_write(dmrg_canon_t c, const double* ket_dev, double* new_ket_dev,
     if (n_writes)
         write_ket_kernel<<<n_writes, 256, 0, st>>>(c->d_writes.as<WriteTask>(), svd.d_probs.as<SvdProblem>(),
                                                    svd.d_w.as<double>(), svd.d_q.as<double>(), sig,
-                                                   svd.d_perm.as<int>(), new_ket_dev, c->side);
+                                                   svd.d_perm.as<int>(), svd.d_sign.as<double>(), new_ket_dev, c->side);
     write_canonical_kernel<<<c->nsec, 256, 0, st>>>(c->d_canons.as<CanonTask>(), svd.d_probs.as<SvdProblem>(),
                                                     svd.d_w.as<double>(), svd.d_q.as<double>(), sig,
-                                                    svd.d_perm.as<int>(), c->d_forced.as<double>(), canonical_dev,
-                                                    c->side);
+                                                    svd.d_perm.as<int>(), c->d_forced.as<double>(),
+                                                    svd.d_sign.as<double>(), canonical_dev, c->side);
     DMRG_CUDA_TRY(cudaGetLastError());
     return DMRG_OK;
 }

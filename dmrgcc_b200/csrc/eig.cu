@@ -189,6 +189,18 @@ __device__ bool jacobi_core(double* A, int n, double* Z) {
     return converged;
 }
 
+// Sign convention for an eigenvector (stride `stride`): its largest-magnitude
+// component is positive; components within a relative 1e-6 of the largest
+// count as equal and the first of them decides.  Sequential (n is small).
+__device__ double eigvec_sign(const double* v, int n, int stride) {
+    double mx = 0.0;
+    for (int i = 0; i < n; ++i) mx = fmax(mx, fabs(v[(int64_t)i * stride]));
+    if (mx == 0.0) return 1.0;
+    for (int i = 0; i < n; ++i)
+        if (fabs(v[(int64_t)i * stride]) >= mx * (1.0 - 1e-6)) return v[(int64_t)i * stride] < 0.0 ? -1.0 : 1.0;
+    return 1.0;
+}
+
 __global__ void __launch_bounds__(kJacobiThreads) sym_jacobi_kernel(double* A, int n, double* w, double* Zout,
                                                                     double* ws, int* status) {
     double* Z = ws;
@@ -214,6 +226,10 @@ __global__ void __launch_bounds__(kJacobiThreads) sym_jacobi_kernel(double* A, i
         const int i = idx / n, k = idx % n;
         Zout[idx] = Z[i * n + order[k]];
     }
+    __syncthreads();
+    for (int k = threadIdx.x; k < n; k += blockDim.x)  // one column per thread
+        if (eigvec_sign(Zout + k, n, n) < 0.0)
+            for (int i = 0; i < n; ++i) Zout[i * n + k] = -Zout[i * n + k];
 }
 
 __global__ void __launch_bounds__(kJacobiThreads) tridiag_vector_kernel(const double* __restrict__ alpha,
@@ -238,7 +254,10 @@ __global__ void __launch_bounds__(kJacobiThreads) tridiag_vector_kernel(const do
         kmin = best;
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < n; i += blockDim.x) y[i] = Z[i * n + kmin];
+    __shared__ double sgn;
+    if (threadIdx.x == 0) sgn = eigvec_sign(Z + kmin, n, n);
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x) y[i] = sgn * Z[i * n + kmin];
 }
 
 }  // namespace

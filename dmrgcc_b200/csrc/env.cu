@@ -290,6 +290,8 @@ int dmrg_env_create(dmrg_ctx_t ctx, int side, int nl, int nr, const int* phys, c
         rc = set_error(DMRG_E_ARG, "invalid input environment");
     if (rc == DMRG_OK) rc = side == 0 ? build_left(*e) : build_right(*e);
     cudaStream_t st = ctx->stream;
+    if (rc == DMRG_OK) rc = e->s1.check_bounds(e->site.ket.size, e->in.size, e->scratch_size);
+    if (rc == DMRG_OK) rc = e->s2.check_bounds(e->scratch_size, e->site.ket.size, e->out.size);
     if (rc == DMRG_OK) rc = e->s1.finalize(64, 64, 16, st);
     if (rc == DMRG_OK) rc = e->s2.finalize(64, 64, 16, st, ctx->num_sms);
     if (rc == DMRG_OK) rc = e->scratch.alloc((size_t)std::max<int64_t>(e->scratch_size, 1) * sizeof(double));

@@ -90,6 +90,9 @@ struct GemmSchedule {
         g.t1 = (int)terms.size();
         flops += 2.0 * g.m * g.n * (double)k;
     }
+    // Verifies that every read of A/B and every write of C stays inside buffers
+    // of the given sizes (doubles); returns DMRG_E_ARG (no launch) otherwise.
+    int check_bounds(int64_t a_size, int64_t b_size, int64_t c_size) const;
     // Builds the tile list (tile_m x tile_n tiles, heaviest first) and uploads.
     // With `num_sms` > 0, groups whose k-loop is much longer than the balanced
     // per-CTA share are split into chunks (split-K) reduced by a second kernel,

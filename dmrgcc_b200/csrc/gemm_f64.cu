@@ -178,6 +178,25 @@ __global__ void __launch_bounds__(256) split_reduce_kernel(double* __restrict__ 
 
 }  // namespace
 
+int GemmSchedule::check_bounds(int64_t a_size, int64_t b_size, int64_t c_size) const {
+    for (const GemmGroup& g : groups) {
+        if (g.m <= 0 || g.n <= 0) continue;
+        if (g.c_off < 0 || g.c_off + (int64_t)(g.m - 1) * g.ldc + g.n > c_size || g.n > g.ldc)
+            return set_error(DMRG_E_ARG, "GEMM output %lld (%dx%d, ld %d) outside %lld", (long long)g.c_off, g.m, g.n,
+                             g.ldc, (long long)c_size);
+        for (int ti = g.t0; ti < g.t1; ++ti) {
+            const GemmTerm& t = terms[ti];
+            if (t.k <= 0) continue;
+            const int64_t ae = ta ? t.a_off + (int64_t)(t.k - 1) * t.lda + g.m : t.a_off + (int64_t)(g.m - 1) * t.lda + t.k;
+            const int64_t be = tb ? t.b_off + (int64_t)(g.n - 1) * t.ldb + t.k : t.b_off + (int64_t)(t.k - 1) * t.ldb + g.n;
+            if (t.a_off < 0 || ae > a_size || t.b_off < 0 || be > b_size)
+                return set_error(DMRG_E_ARG, "GEMM operand outside its buffer (A end %lld of %lld, B end %lld of %lld)",
+                                 (long long)ae, (long long)a_size, (long long)be, (long long)b_size);
+        }
+    }
+    return DMRG_OK;
+}
+
 int GemmSchedule::finalize(int tile_m, int tile_n, int tile_k, cudaStream_t stream, int num_sms) {
     tiles.clear();
     exec_groups.clear();

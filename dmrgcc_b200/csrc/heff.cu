@@ -123,6 +123,8 @@ int build_heff(dmrg_heff_s& h) {
     }
     h.flops_alg = fa_alg + fb;
     h.flops_exec = fa_exec + fb;
+    DMRG_TRY(h.sa.check_bounds(ket.size, h.R.size, h.t_size));
+    DMRG_TRY(h.sb.check_bounds(h.L.size, h.t_size, ket.size));
     cudaStream_t st = h.ctx->stream;
     DMRG_TRY(h.sa.finalize(64, 64, 16, st));
     DMRG_TRY(h.sb.finalize(64, 64, 16, st, h.ctx->num_sms));

@@ -36,7 +36,10 @@ dmrg_blocks_t as_blocks(const BlockListDesc& b) {
 
 // RealMatrix::RandomMatrix (src/tensor/real_matrix.cc:201-208): column-major
 // draws of 0.01 * (rand() % 100) into a rows x cols row-major block.
+long long g_rand_draws = 0;  // rand() draws made by engines in this process (trace output)
+
 void random_block(std::vector<double>& out, size_t off, int rows, int cols) {
+    g_rand_draws += (long long)rows * cols;
     for (int j = 0; j < cols; ++j)
         for (int i = 0; i < rows; ++i) out[off + (size_t)i * cols + j] = 0.01 * (rand() % 100);
 }
@@ -103,12 +106,15 @@ Engine::Engine(dmrg_ctx_t ctx, std::unique_ptr<QuantumSpace> space, std::unique_
     }
     for (int i = 0; i < num_sweep_; ++i) noise_[i] = std::pow(0.1, noise_[i]);
 
+    rs_.alloc(2 * ctx_->num_sms, 1);
+    if (const char* tp = std::getenv("DMRG_TRACE")) trace_ = std::fopen(tp, "w");
     lat_.resize(n_);
     for (int i = 0; i < n_; ++i) {
         lat_[i].reset(new TensorLattice());
         lat_[i]->physics_dim = space_->physics_dim();
     }
     srand(opt_.seed);
+    g_rand_draws = 0;
     int rc = DefineTensorSpace(first_block_, first_dim_);
     if (rc != DMRG_OK) throw std::runtime_error(std::string("DefineTensorSpace: ") + dmrg_last_error());
     ham_->DefineTensorHamiltonian();
@@ -127,10 +133,46 @@ Engine::Engine(dmrg_ctx_t ctx, std::unique_ptr<QuantumSpace> space, std::unique_
         con_[i]->R.desc.o.assign(con_[i]->right_bond, BlockListDesc());
         con_[i]->R.desc.rebase();
     }
-    rs_.alloc(2 * ctx_->num_sms, 1);
 }
 
-Engine::~Engine() = default;
+Engine::~Engine() {
+    if (trace_) std::fclose(trace_);
+}
+
+// Sector dimensions of a site after an operation (same format as the reference
+// probe's trace, for step-by-step comparison).
+void Engine::Trace(const char* tag, int leigh, int site) {
+    if (!trace_) return;
+    const TensorLattice& t = *lat_[site];
+    std::fprintf(trace_, "%s %d %d L:", tag, leigh, site);
+    for (int d : t.left_dim) std::fprintf(trace_, "%d,", d);
+    std::fprintf(trace_, " R:");
+    for (int d : t.right_dim) std::fprintf(trace_, "%d,", d);
+    auto fetch = [&](const DevBlocks& b, std::vector<double>& h) {
+        h.assign((size_t)b.d.size, 0.0);
+        if (!h.empty() &&
+            (cudaMemcpyAsync(h.data(), b.ptr(), h.size() * sizeof(double), cudaMemcpyDeviceToHost, st_) != cudaSuccess ||
+             cudaStreamSynchronize(st_) != cudaSuccess))
+            h.assign(h.size(), 0.0);
+    };
+    std::vector<double> h;
+    fetch(t.ket, h);
+    double norm2 = 0.0;
+    for (double v : h) norm2 += v * v;
+    std::fprintf(trace_, " P:%lld N:%.10e Q:%lld", (long long)t.psi_dim(), norm2, g_rand_draws);
+    if (tag[0] == 'C' && t.has_canonical) {  // per-block squared norms of S V^T (or U S)
+        fetch(t.canonical, h);
+        std::fprintf(trace_, " S:");
+        for (int k = 0; k < t.canonical.d.count(); ++k) {
+            double s2 = 0.0;
+            for (int64_t i = 0; i < (int64_t)t.canonical.d.rows[k] * t.canonical.d.cols[k]; ++i)
+                s2 += h[t.canonical.d.off[k] + i] * h[t.canonical.d.off[k] + i];
+            std::fprintf(trace_, "%.8e,", s2);
+        }
+    }
+    std::fprintf(trace_, "\n");
+    std::fflush(trace_);
+}
 
 // ---------------------------------------------------------------------------
 // sector bookkeeping (RealTensorSpace, real_tensor_space.cc)
@@ -262,6 +304,7 @@ int Engine::CanonicalTensorSpace(int leigh, int site, double* discarded) {
     if (leigh == 0) t.right_dim = tdim;
     else t.left_dim = tdim;
     if (discarded) *discarded = disc;
+    Trace("C", leigh, site);
     return DMRG_OK;
 }
 
@@ -307,6 +350,8 @@ int Engine::MergeTensorSpace(int leigh, int site) {
             s.add_term(t.ket.d.off[k], t.ket.d.cols[k], o.canonical.d.off[sec], o.canonical.d.cols[sec],
                        t.ket.d.cols[k], 1.0);
     }
+    if (leigh == 0) DMRG_TRY(s.check_bounds(o.canonical.d.size, t.ket.d.size, nk.d.size));
+    else DMRG_TRY(s.check_bounds(t.ket.d.size, o.canonical.d.size, nk.d.size));
     DMRG_TRY(s.finalize(64, 64, 16, st_));
     if (leigh == 0) DMRG_TRY(launch_gemm_f64(s, o.canonical.ptr(), t.ket.ptr(), nk.ptr(), false, st_));
     else DMRG_TRY(launch_gemm_f64(s, t.ket.ptr(), o.canonical.ptr(), nk.ptr(), false, st_));
@@ -318,6 +363,7 @@ int Engine::MergeTensorSpace(int leigh, int site) {
         for (int r = 0; r < t.nr(); ++r) t.right_dim[r] = o.canonical.d.cols[r];
     t.ket = std::move(nk);
     DMRG_TRY(Normalize(t));
+    Trace("M", leigh, site);
     o.has_canonical = false;
     o.canonical = DevBlocks();
     o.match_dim.clear();
@@ -412,10 +458,11 @@ int Engine::ExpanLattice(int leigh, TensorLattice& t, const TensorLattice& origi
                        nd.cols[k], sr, sc, 1.0};
             (p.src == 0 ? from_origin : from_expan).push_back(c);
         }
-    DMRG_TRY(launch_rect_copies(from_origin, origin.ket.ptr(), nk.ptr(), copy_tasks_, st_));
+    DMRG_TRY(launch_rect_copies(from_origin, origin.ket.ptr(), origin.ket.d.size, nk.ptr(), nd.size, copy_tasks_, st_));
     if (!from_expan.empty()) {
         DMRG_CUDA_TRY(cudaStreamSynchronize(st_));
-        DMRG_TRY(launch_rect_copies(from_expan, expan->ket.ptr(), nk.ptr(), copy_tasks_, st_));
+        DMRG_TRY(launch_rect_copies(from_expan, expan->ket.ptr(), expan->ket.d.size, nk.ptr(), nd.size, copy_tasks_,
+                                    st_));
     }
     DMRG_CUDA_TRY(cudaStreamSynchronize(st_));
     t.ket = std::move(nk);
@@ -467,6 +514,21 @@ int Engine::ExpanTensorSpace(int leigh, int site) {
     ComputeTensorIndex(site, li, ri, pi);
     DMRG_TRY(DefineLatticeBlocks(t, li, ri, pi, 1, 1));
     t.ket.set_shape_zero();
+    if (trace_) {  // the expansion term, block by block, before it is merged
+        const DevBlocks& eb = expan_->ket;
+        std::vector<double> h((size_t)eb.d.size);
+        if (!h.empty()) {
+            DMRG_CUDA_TRY(cudaMemcpyAsync(h.data(), eb.ptr(), h.size() * sizeof(double), cudaMemcpyDeviceToHost, st_));
+            DMRG_CUDA_TRY(cudaStreamSynchronize(st_));
+        }
+        std::fprintf(trace_, "Y %d %d", leigh, site);
+        for (int k = 0; k < eb.d.count(); ++k) {
+            double s2 = 0.0;
+            for (int64_t i = 0; i < (int64_t)eb.d.rows[k] * eb.d.cols[k]; ++i) s2 += h[eb.d.off[k] + i] * h[eb.d.off[k] + i];
+            std::fprintf(trace_, " %d.%d:%dx%d=%.8e", eb.d.left[k], eb.d.right[k], eb.d.rows[k], eb.d.cols[k], s2);
+        }
+        std::fprintf(trace_, "\n");
+    }
     DMRG_TRY(ExpanLattice(leigh, t, origin, expan_.get()));
     expan_.reset();
     return DMRG_OK;
@@ -670,6 +732,8 @@ int Engine::LeftExpanTensorContraction(int site, const std::vector<std::vector<i
     for (int b = 0; b < eb.count(); ++b) {
         int rows = 0, cols = 0;
         for (const Contrib& c : contrib[b]) {
+            if (rows && rows != firsts[c.first].m)
+                return set_error(DMRG_E_ARG, "row or column dimension is not match in ExpanMatrix");
             rows = firsts[c.first].m;
             cols += c.d1;
         }
@@ -718,6 +782,8 @@ int Engine::LeftExpanTensorContraction(int site, const std::vector<std::vector<i
             col += c.d1;
         }
     }
+    DMRG_TRY(sf.check_bounds(con.L.desc.size, t.ket.d.size, first_size));
+    DMRG_TRY(ss.check_bounds(first_size, (int64_t)rnd.size(), packed.size));
     DMRG_TRY(sf.finalize(64, 64, 16, st_));
     DMRG_TRY(ss.finalize(64, 64, 16, st_));
     DMRG_TRY(launch_gemm_f64(sf, con.L.ptr(), t.ket.ptr(), scratch_.as<double>(), false, st_));
@@ -832,6 +898,8 @@ int Engine::RightExpanTensorContraction(int site, const std::vector<std::vector<
     for (int b = 0; b < eb.count(); ++b) {
         int rows = 0, cols = 0;
         for (const Contrib& c : contrib[b]) {
+            if (cols && cols != firsts[c.first].n)
+                return set_error(DMRG_E_ARG, "row or column dimension is not match in ExpanMatrix");
             cols = firsts[c.first].n;
             rows += c.d0;
         }
@@ -880,6 +948,8 @@ int Engine::RightExpanTensorContraction(int site, const std::vector<std::vector<
             row += c.d0;
         }
     }
+    DMRG_TRY(sf.check_bounds(t.ket.d.size, con.R.desc.size, first_size));
+    DMRG_TRY(ss.check_bounds((int64_t)rnd.size(), first_size, packed.size));
     DMRG_TRY(sf.finalize(64, 64, 16, st_));
     DMRG_TRY(ss.finalize(64, 64, 16, st_));
     DMRG_TRY(launch_gemm_f64(sf, t.ket.ptr(), con.R.ptr(), scratch_.as<double>(), false, st_));
@@ -1046,16 +1116,20 @@ int Engine::Run() {
             const int j = l2r ? k : n_ - 1 - k;
             const double ts = wall_time();
             int dim = 0;
+            const int64_t psi_dim = lat_[j]->psi_dim();  // at the Lanczos call, like the reference's log
             DMRG_TRY(LanczosMethod(num_iter_[h], j, energy_, dim));
+            if (trace_) std::fprintf(trace_, "E %d %d P:%lld %.12e\n", lanczos_calls_, j, (long long)psi_dim, energy_);
+            ++lanczos_calls_;
             DMRG_TRY(ResetEnv(l2r ? 1 : 0, j));
             DMRG_TRY(ExpanTensorNetwork(l2r ? 0 : 1, j));
             DMRG_TRY(ExpanTensorSpace(l2r ? 0 : 1, j));
+            Trace("X", l2r ? 0 : 1, j);
             double disc = 0.0;
-            const int64_t psi_dim = lat_[j]->psi_dim();
             DMRG_TRY(CanonicalTensorSpace(l2r ? 0 : 1, j, &disc));
             DMRG_TRY(ComputeTensorNetwork(l2r ? 0 : 1, j));
             const int nxt = l2r ? j + 1 : j - 1;
             DMRG_TRY(MatchTensorSpace(l2r ? 0 : 1, nxt));
+            Trace("T", l2r ? 0 : 1, nxt);
             DMRG_TRY(MergeTensorSpace(l2r ? 0 : 1, nxt));
             records_.push_back(SweepRecord{h, j, l2r ? 0 : 1, energy_, dim, disc, psi_dim, wall_time() - ts});
         }

@@ -118,6 +118,7 @@ private:
     int RightExpanTensorContraction(int site, const std::vector<std::vector<int>>& mapping);
     int ExpanLattice(int leigh, TensorLattice& t, const TensorLattice& origin, const TensorLattice* expan);
     int Normalize(TensorLattice& t);
+    void Trace(const char* tag, int leigh, int site);
     void DefineTensorNetwork();
     int ResetEnv(int leigh, int site);
 
@@ -145,6 +146,8 @@ private:
     std::vector<double> half_energies_, half_seconds_;
     double energy_ = 0.0;
     int half_sweep_ = 0;
+    int lanczos_calls_ = 0;
+    FILE* trace_ = nullptr;  // DMRG_TRACE=<file>: structure trace, one line per step operation
 };
 
 }  // namespace dmrg

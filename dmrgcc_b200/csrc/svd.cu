@@ -16,6 +16,11 @@ constexpr int kThreads = 256;
 constexpr int kLd = kPair + 1;  // padded row of the shared 64x64 matrices
 constexpr int kInnerSweeps = 4;
 constexpr int kMaxSweeps = 40;
+// Columns whose norm is below kZeroRel * sqrt(rows) * ||A||_F are rounding
+// residue of a rank-deficient matrix: they take part in no rotation and in no
+// convergence test (their values are below any truncation threshold that is
+// meaningful in FP64; rotating them only stirs rounding noise).
+constexpr double kZeroRel = 4.0 * DBL_EPSILON;
 
 struct SvdSmem {
     double G[kPair * kLd];
@@ -98,6 +103,7 @@ __device__ __forceinline__ void rotate_chunk(SvdSmem& S) {
 __global__ void __launch_bounds__(kThreads) jacobi_round_kernel(const SvdProblem* __restrict__ probs,
                                                                 const SvdTask* __restrict__ tasks, int round,
                                                                 double* __restrict__ W, double* __restrict__ Qacc,
+                                                                const double* __restrict__ fro2,
                                                                 unsigned long long* __restrict__ conv) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     SvdSmem& S = *reinterpret_cast<SvdSmem*>(smem_raw);
@@ -109,6 +115,7 @@ __global__ void __launch_bounds__(kThreads) jacobi_round_kernel(const SvdProblem
     double* Wp = W + p.w_off;
     double* Qp = Qacc + p.q_off;
     const double tol = 2.0 * DBL_EPSILON * sqrt((double)p.rows);
+    const double zero2 = kZeroRel * kZeroRel * (double)p.rows * fro2[task.problem];
 
     // ---- Gram matrix of the pair: G = X^T X over all rows -----------------------
     const int ty = threadIdx.x / 16, tx = threadIdx.x % 16;  // 4x4 micro-tile (rows ty*4.., cols tx*4..)
@@ -146,8 +153,8 @@ __global__ void __launch_bounds__(kThreads) jacobi_round_kernel(const SvdProblem
     for (int idx = threadIdx.x; idx < kPair * kPair; idx += kThreads) {
         const int a = idx / kPair, b = idx % kPair;
         if (a >= b) continue;
-        const double d = S.G[a * kLd + a] * S.G[b * kLd + b];
-        if (d > 0.0) worst = fmax(worst, fabs(S.G[a * kLd + b]) / sqrt(d));
+        const double ga = S.G[a * kLd + a], gb = S.G[b * kLd + b];
+        if (ga > zero2 && gb > zero2) worst = fmax(worst, fabs(S.G[a * kLd + b]) / sqrt(ga * gb));
     }
     worst = block_max(worst, S);
     if (threadIdx.x == 0) atomicMax(conv + task.problem, (unsigned long long)__double_as_longlong(worst));
@@ -162,7 +169,7 @@ __global__ void __launch_bounds__(kThreads) jacobi_round_kernel(const SvdProblem
                 const double apq = S.G[a * kLd + b];
                 double c = 1.0, s = 0.0;
                 const double daa = S.G[a * kLd + a], dbb = S.G[b * kLd + b];
-                if (apq != 0.0 && fabs(apq) > DBL_EPSILON * 1e-3 * sqrt(fabs(daa * dbb))) {
+                if (apq != 0.0 && daa > zero2 && dbb > zero2 && fabs(apq) > DBL_EPSILON * 1e-3 * sqrt(daa * dbb)) {
                     const double tau = (dbb - daa) / (2.0 * apq);
                     const double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
                     c = 1.0 / sqrt(1.0 + t * t);
@@ -219,6 +226,23 @@ __global__ void __launch_bounds__(kThreads) jacobi_round_kernel(const SvdProblem
     }
 }
 
+// Squared Frobenius norm of each working matrix (fixed-order block reduction).
+__global__ void __launch_bounds__(256) fro2_kernel(const SvdProblem* __restrict__ probs, const double* __restrict__ W,
+                                                   double* __restrict__ fro2) {
+    __shared__ double red[256];
+    const SvdProblem p = probs[blockIdx.x];
+    const double* w = W + p.w_off;
+    double s = 0.0;
+    for (int64_t i = threadIdx.x; i < (int64_t)p.rows * p.cols; i += blockDim.x) s += w[i] * w[i];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) fro2[blockIdx.x] = red[0];
+}
+
 __global__ void init_identity_kernel(const SvdProblem* __restrict__ probs, double* __restrict__ Q) {
     const SvdProblem p = probs[blockIdx.x];
     double* q = Q + p.q_off;
@@ -250,6 +274,35 @@ __global__ void __launch_bounds__(256) finalize_kernel(const SvdProblem* __restr
         sig[p.s_off + rank] = v;
         perm[p.perm_off + rank] = j;
     }
+}
+
+// Sign convention for each singular triplet (rank j, sorted): the left singular
+// vector u_j is taken with its largest-magnitude component positive; components
+// within a relative 1e-6 of the largest count as equal and the first decides.
+// u_j is column perm[j] of W (scaled by 1/s_j) when W = A, of Q when W = A^T.
+// One warp per rank.
+__global__ void __launch_bounds__(256) sign_kernel(const SvdProblem* __restrict__ probs, const double* __restrict__ W,
+                                                   const double* __restrict__ Q, const int* __restrict__ perm,
+                                                   double* __restrict__ sign) {
+    const SvdProblem p = probs[blockIdx.x];
+    const int lane = threadIdx.x & 31;
+    const int j = blockIdx.y * 8 + (threadIdx.x >> 5);
+    if (j >= p.cols) return;
+    const int k = perm[p.perm_off + j];
+    const double* u = p.transposed ? Q + p.q_off + (int64_t)k * p.m : W + p.w_off + (int64_t)k * p.m;
+    double mx = 0.0;
+    for (int i = lane; i < p.m; i += 32) mx = fmax(mx, fabs(u[i]));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    int first = p.m;
+    for (int i = lane; i < p.m; i += 32)
+        if (mx > 0.0 && fabs(u[i]) >= mx * (1.0 - 1e-6)) {
+            first = i;
+            break;
+        }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) first = min(first, __shfl_xor_sync(0xffffffffu, first, o));
+    if (lane == 0) sign[p.s_off + j] = (first < p.m && u[first] < 0.0) ? -1.0 : 1.0;
 }
 
 }  // namespace
@@ -294,6 +347,8 @@ int BatchedSvd::plan(const std::vector<int>& m, const std::vector<int>& n, cudaS
     DMRG_TRY(d_s.alloc((size_t)std::max<int64_t>(2 * soff, 1) * sizeof(double)));
     DMRG_TRY(d_perm.alloc((size_t)std::max<int64_t>(soff, 1) * sizeof(int)));
     DMRG_TRY(d_conv.alloc(std::max<size_t>(probs.size(), 1) * sizeof(unsigned long long)));
+    DMRG_TRY(d_fro2.alloc(std::max<size_t>(probs.size(), 1) * sizeof(double)));
+    DMRG_TRY(d_sign.alloc((size_t)std::max<int64_t>(soff, 1) * sizeof(double)));
     DMRG_TRY(upload(d_probs, probs, st));
     DMRG_TRY(upload(d_tasks, tasks, st));
     DMRG_CUDA_TRY(cudaFuncSetAttribute(jacobi_round_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -308,8 +363,10 @@ int BatchedSvd::run(cudaStream_t st, int* sweeps_out) {
     }
     const int np = (int)probs.size();
     init_identity_kernel<<<np, 256, 0, st>>>(d_probs.as<SvdProblem>(), d_q.as<double>());
+    fro2_kernel<<<np, 256, 0, st>>>(d_probs.as<SvdProblem>(), d_w.as<double>(), d_fro2.as<double>());
     std::vector<unsigned long long> conv(np);
-    int sweep = 0;
+    int sweep = 0, worst_at = 0;
+    double worst_left = 0.0;
     for (; sweep < kMaxSweeps; ++sweep) {
         DMRG_CUDA_TRY(cudaMemsetAsync(d_conv.ptr, 0, np * sizeof(unsigned long long), st));
         for (int r = 0; r < max_rounds; ++r) {
@@ -317,7 +374,7 @@ int BatchedSvd::run(cudaStream_t st, int* sweeps_out) {
             if (n == 0) continue;
             jacobi_round_kernel<<<n, kThreads, sizeof(SvdSmem), st>>>(
                 d_probs.as<SvdProblem>(), d_tasks.as<SvdTask>() + round_first[r], r, d_w.as<double>(),
-                d_q.as<double>(), d_conv.as<unsigned long long>());
+                d_q.as<double>(), d_fro2.as<double>(), d_conv.as<unsigned long long>());
         }
         DMRG_CUDA_TRY(cudaGetLastError());
         DMRG_CUDA_TRY(cudaMemcpyAsync(conv.data(), d_conv.ptr, np * sizeof(unsigned long long),
@@ -327,13 +384,25 @@ int BatchedSvd::run(cudaStream_t st, int* sweeps_out) {
         for (int i = 0; i < np; ++i) {
             double worst;
             std::memcpy(&worst, &conv[i], sizeof(double));
-            if (worst > 2.0 * DBL_EPSILON * std::sqrt((double)probs[i].rows)) done = false;
+            if (worst > 2.0 * DBL_EPSILON * std::sqrt((double)probs[i].rows)) {
+                done = false;
+                if (sweep == kMaxSweeps - 1 && worst > worst_left) {
+                    worst_left = worst;
+                    worst_at = i;
+                }
+            }
         }
         if (done) break;
     }
-    if (sweep == kMaxSweeps) return set_error(DMRG_E_NUMERIC, "Jacobi SVD did not converge in %d sweeps", kMaxSweeps);
+    if (sweep == kMaxSweeps)
+        return set_error(DMRG_E_NUMERIC, "Jacobi SVD did not converge in %d sweeps (sector %d x %d: off-diagonal %.3e)",
+                         kMaxSweeps, probs[worst_at].m, probs[worst_at].n, worst_left);
     finalize_kernel<<<np, 256, 0, st>>>(d_probs.as<SvdProblem>(), d_w.as<double>(), d_s.as<double>(),
                                         d_perm.as<int>(), d_s.as<double>() + (d_s.bytes / sizeof(double)) / 2);
+    int max_cols = 0;
+    for (const SvdProblem& p : probs) max_cols = std::max(max_cols, p.cols);
+    sign_kernel<<<dim3(np, (max_cols + 7) / 8), 256, 0, st>>>(d_probs.as<SvdProblem>(), d_w.as<double>(),
+                                                               d_q.as<double>(), d_perm.as<int>(), d_sign.as<double>());
     DMRG_CUDA_TRY(cudaGetLastError());
     if (sweeps_out) *sweeps_out = sweep + 1;
     return DMRG_OK;

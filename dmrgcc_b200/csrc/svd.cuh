@@ -9,8 +9,12 @@
 // Jacobi sweeps on it in shared memory, then the pair's columns of W and of the
 // accumulated rotation are multiplied by the 64x64 rotation.  Converged when no
 // pair has |g_ij| > tol * sqrt(g_ii g_jj) (high relative accuracy, which the
-// reference's canpre cut at 1e-12 needs).  Singular values are the final column
-// norms, sorted in descending order.
+// reference's canpre cut at 1e-12 needs); columns of a rank-deficient matrix
+// whose norm falls to rounding level (4 eps sqrt(rows) ||A||_F) are left out of
+// rotations and of that test.  Singular values are the final column
+// norms, sorted in descending order.  The free sign of each singular pair is
+// fixed by a convention: the left singular vector's largest-magnitude component
+// is positive (ties within a relative 1e-6: the first such component).
 #pragma once
 
 #include <vector>
@@ -49,7 +53,8 @@ public:
     // Sorted singular values of every active sector, copied to the host.
     int singular_values(std::vector<std::vector<double>>& out, cudaStream_t st);
 
-    DeviceBuffer d_w, d_q, d_s, d_perm, d_probs, d_tasks, d_conv;
+    DeviceBuffer d_w, d_q, d_s, d_perm, d_probs, d_tasks, d_conv, d_fro2;
+    DeviceBuffer d_sign;  // +-1 per sorted singular triplet (sign convention, set by run())
     std::vector<SvdProblem> probs;
     std::vector<int> index;             // sector -> problem (-1 when empty)
     std::vector<int> round_first;       // task offset of each round

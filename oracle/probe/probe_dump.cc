@@ -16,6 +16,8 @@
 //   PROBE_ENV=i,j,...      environment-update call indices to dump
 //   PROBE_CANON=i,j,...    canonicalisation call indices to dump
 //   PROBE_STOP=n           exit(0) right after Lanczos call n
+//   PROBE_GAUGE=1          fix the free signs of LAPACK's singular vectors and
+//                          eigenvectors by the library's convention (see below)
 // Always writes PROBE_OUT/steps.txt: one line per Lanczos call with the site,
 // iteration cap, psi_dim and the energy the reference returned.
 #include "probe_common.h"
@@ -48,6 +50,88 @@ static int site_of(RealTensorLattice* t) {
     return -1;
 }
 
+// Structure trace (PROBE_TRACE=1): one line per canonicalisation, expansion,
+// match and merge with the sector dimensions of the site afterwards; the
+// device engine writes the same lines (DMRG_TRACE) for comparison.
+static FILE* g_trace = nullptr;
+// PROBE_GAUGE=1: LAPACK leaves the sign of every singular vector pair and
+// eigenvector free.  With this switch each is fixed after the call by one
+// convention, also used by libdmrg_b200: the component of largest magnitude of
+// the left singular vector (the eigenvector) is positive, where components
+// within a relative 1e-6 of the largest count as equal and the first of them
+// decides.  The decomposition stays exact; only the free signs are pinned, so
+// the two implementations follow one trajectory through the noise-driven
+// subspace expansion (whose random matrices act in the gauge-dependent basis).
+static bool g_gauge = false;
+static double sign_of_column(const double* a, long n, long stride) {
+    double m = 0.0;
+    for (long i = 0; i < n; ++i) m = std::fabs(a[i * stride]) > m ? std::fabs(a[i * stride]) : m;
+    if (m == 0.0) return 1.0;
+    for (long i = 0; i < n; ++i)
+        if (std::fabs(a[i * stride]) >= m * (1.0 - 1e-6)) return a[i * stride] < 0.0 ? -1.0 : 1.0;
+    return 1.0;
+}
+extern "C" lapack_int __real_LAPACKE_dgesvd(int, char, char, lapack_int, lapack_int, double*, lapack_int, double*,
+                                            double*, lapack_int, double*, lapack_int, double*);
+extern "C" lapack_int __wrap_LAPACKE_dgesvd(int layout, char jobu, char jobvt, lapack_int m, lapack_int n, double* a,
+                                            lapack_int lda, double* s, double* u, lapack_int ldu, double* vt,
+                                            lapack_int ldvt, double* superb) {
+    const lapack_int info = __real_LAPACKE_dgesvd(layout, jobu, jobvt, m, n, a, lda, s, u, ldu, vt, ldvt, superb);
+    if (g_gauge && info == 0 && layout == LAPACK_ROW_MAJOR && jobu == 'S' && jobvt == 'S') {
+        const lapack_int k = m < n ? m : n;  // (the reference's headers define min/max as macros)
+        for (lapack_int c = 0; c < k; ++c)
+            if (sign_of_column(u + c, m, ldu) < 0.0) {
+                for (lapack_int i = 0; i < m; ++i) u[(long)i * ldu + c] = -u[(long)i * ldu + c];
+                for (lapack_int j = 0; j < n; ++j) vt[(long)c * ldvt + j] = -vt[(long)c * ldvt + j];
+            }
+    }
+    return info;
+}
+extern "C" lapack_int __real_LAPACKE_dsyevd(int, char, char, lapack_int, double*, lapack_int, double*);
+extern "C" lapack_int __wrap_LAPACKE_dsyevd(int layout, char jobz, char uplo, lapack_int n, double* a, lapack_int lda,
+                                            double* w) {
+    const lapack_int info = __real_LAPACKE_dsyevd(layout, jobz, uplo, n, a, lda, w);
+    if (g_gauge && info == 0 && layout == LAPACK_ROW_MAJOR && jobz == 'V')
+        for (lapack_int c = 0; c < n; ++c)
+            if (sign_of_column(a + c, n, lda) < 0.0)
+                for (lapack_int i = 0; i < n; ++i) a[(long)i * lda + c] = -a[(long)i * lda + c];
+    return info;
+}
+
+static long long g_rand_calls = 0;  // glibc rand() draws so far (the reference's only random source)
+extern "C" int __real_rand(void);
+extern "C" int __wrap_rand(void) {
+    ++g_rand_calls;
+    return __real_rand();
+}
+static double g_cut_gap = -1.0, g_pre_gap = -1.0;  // truncation_gap() of the step being traced
+static void trace(const char* tag, int leigh, RealTensorLattice* t) {
+    if (!g_trace) return;
+    std::fprintf(g_trace, "%s %d %d L:", tag, leigh, site_of(t));
+    for (int i = 0; i < t->num_left_block_; ++i) std::fprintf(g_trace, "%d,", t->left_dim_[i]);
+    std::fprintf(g_trace, " R:");
+    for (int i = 0; i < t->num_right_block_; ++i) std::fprintf(g_trace, "%d,", t->right_dim_[i]);
+    double norm2 = 0.0;
+    RealMatrixBlock* kb = t->ket_tensor_;
+    for (int k = 0; kb && k < kb->num_block_; ++k) {
+        const RealMatrix* m = kb->matrix_block_[k];
+        for (long i = 0; i < (long)m->row_ * m->column_; ++i) norm2 += m->matrix_element_[i] * m->matrix_element_[i];
+    }
+    std::fprintf(g_trace, " P:%d N:%.10e Q:%lld", t->ComputeKetTensorDim(), norm2, g_rand_calls);
+    if (tag[0] == 'C' && t->canonical_tensor_) {  // per-block squared norms of S V^T (or U S)
+        std::fprintf(g_trace, " S:");
+        RealMatrixBlock* cb = t->canonical_tensor_;
+        for (int k = 0; k < cb->num_block_; ++k) {
+            const RealMatrix* m = cb->matrix_block_[k];
+            double s2 = 0.0;
+            for (long i = 0; i < (long)m->row_ * m->column_; ++i) s2 += m->matrix_element_[i] * m->matrix_element_[i];
+            std::fprintf(g_trace, "%.8e,", s2);
+        }
+    }
+    if (tag[0] == 'C') std::fprintf(g_trace, " G:%.3e,%.3e", g_cut_gap, g_pre_gap);
+    std::fprintf(g_trace, "\n");
+}
+
 static void write_struct_only_block(NacWriter& w, const std::string& p, RealMatrixBlock* b) {
     std::vector<int> li, ri, rows, cols;
     int nb = b ? b->num_block_ : 0;
@@ -71,6 +155,38 @@ void __real__ZN21RealTensorContraction29RightComputeTensorContractionEP17RealTen
     RealTensorContraction*, RealTensorLattice*, RealTensorOperator*, RealTensorContraction*);
 void __real__ZN17RealTensorLattice26LeftCanonicalTensorLatticeEid(RealTensorLattice*, int, double);
 void __real__ZN17RealTensorLattice27RightCanonicalTensorLatticeEid(RealTensorLattice*, int, double);
+void __real__ZN15RealTensorSpace16ExpanTensorSpaceEii(RealTensorSpace*, int, int);
+void __real__ZN15RealTensorSpace16MatchTensorSpaceEii(RealTensorSpace*, int, int);
+void __real__ZN17RealTensorLattice22LeftMergeTensorLatticeEPS_(RealTensorLattice*, RealTensorLattice*);
+void __real__ZN17RealTensorLattice23RightMergeTensorLatticeEPS_(RealTensorLattice*, RealTensorLattice*);
+void __wrap__ZN15RealTensorSpace16ExpanTensorSpaceEii(RealTensorSpace* self, int leigh, int site) {
+    if (g_trace && self->expan_tensor_lattice_) {  // the expansion term, block by block, before it is merged
+        RealMatrixBlock* kb = self->expan_tensor_lattice_->ket_tensor_;
+        std::fprintf(g_trace, "Y %d %d", leigh, site);
+        for (int k = 0; kb && k < kb->num_block_; ++k) {
+            const RealMatrix* m = kb->matrix_block_[k];
+            double s2 = 0.0;
+            for (long i = 0; i < (long)m->row_ * m->column_; ++i) s2 += m->matrix_element_[i] * m->matrix_element_[i];
+            std::fprintf(g_trace, " %d.%d:%dx%d=%.8e", kb->left_index_[k], kb->right_index_[k], m->row_, m->column_,
+                         s2);
+        }
+        std::fprintf(g_trace, "\n");
+    }
+    __real__ZN15RealTensorSpace16ExpanTensorSpaceEii(self, leigh, site);
+    trace("X", leigh, self->tensor_lattice_[site]);
+}
+void __wrap__ZN15RealTensorSpace16MatchTensorSpaceEii(RealTensorSpace* self, int leigh, int site) {
+    __real__ZN15RealTensorSpace16MatchTensorSpaceEii(self, leigh, site);
+    trace("T", leigh, self->tensor_lattice_[site]);
+}
+void __wrap__ZN17RealTensorLattice22LeftMergeTensorLatticeEPS_(RealTensorLattice* self, RealTensorLattice* o) {
+    __real__ZN17RealTensorLattice22LeftMergeTensorLatticeEPS_(self, o);
+    trace("M", 0, self);
+}
+void __wrap__ZN17RealTensorLattice23RightMergeTensorLatticeEPS_(RealTensorLattice* self, RealTensorLattice* o) {
+    __real__ZN17RealTensorLattice23RightMergeTensorLatticeEPS_(self, o);
+    trace("M", 1, self);
+}
 void __real__ZN17RealTensorLattice20CombineTensorLatticeEiRiRPiS2_PS_(RealTensorLattice*, int, int&, int*&, int*&,
                                                                       RealTensorLattice*);
 
@@ -166,6 +282,7 @@ void __wrap__ZN17RealTensorLanczos13LanczosMethodEiiRd(RealTensorLanczos* self, 
         probe::write_lattice(w, "lattice", lat);
     }
     std::fprintf(g_steps, "%d %d %d %d %.15e %.6f\n", call, site, niter, psi_dim, result, t1 - t0);
+    if (g_trace) std::fprintf(g_trace, "E %d %d P:%d %.12e\n", call, site, psi_dim, result);
     std::fflush(g_steps);
     if (call == g_stop) std::exit(0);
 }
@@ -206,8 +323,71 @@ void __wrap__ZN21RealTensorContraction29RightComputeTensorContractionEP17RealTen
     env_common(false, self, lat, op, next);
 }
 
+// Conditioning of a canonicalisation's truncation decision, in units of the
+// tensor's Frobenius norm: (cut) the distance between the last kept and the
+// first dropped singular value when max_dim cuts the sorted list (-1 when it
+// does not), and (pre) the smallest kept sigma / canpre over the values above
+// canpre (a count of values above canpre decided by values only a few decades
+// above it depends on the accuracy of the state, ~1e-8 after Lanczos).
+// Sector matrices are stacked as the reference stacks them (blocks in list
+// order).  A small value marks a step whose block dimensions can legitimately
+// differ between two correct implementations.
+static double truncation_gap(bool left, RealTensorLattice* t, int max_dim, double canpre) {
+    RealMatrixBlock* kb = t->ket_tensor_;
+    const int nsec = left ? t->num_right_block_ : t->num_left_block_;
+    std::vector<double> all;
+    double fro2 = 0.0;
+    for (int sct = 0; sct < nsec; ++sct) {
+        int m = 0, n = 0;
+        std::vector<int> members;
+        for (int k = 0; kb && k < kb->num_block_; ++k)
+            if ((left ? kb->right_index_[k] : kb->left_index_[k]) == sct) members.push_back(k);
+        for (int k : members) {
+            const RealMatrix* b = kb->matrix_block_[k];
+            if (left) { m += b->row_; n = n > b->column_ ? n : b->column_; }
+            else { n += b->column_; m = m > b->row_ ? m : b->row_; }
+        }
+        if (left) n = n > t->right_dim_[sct] ? n : t->right_dim_[sct];
+        else m = m > t->left_dim_[sct] ? m : t->left_dim_[sct];
+        if ((long)m * n == 0) continue;
+        std::vector<double> a((size_t)m * n, 0.0);
+        int at = 0;
+        for (int k : members) {
+            const RealMatrix* b = kb->matrix_block_[k];
+            for (int i = 0; i < b->row_; ++i)
+                for (int j = 0; j < b->column_; ++j) {
+                    const double v = b->matrix_element_[(long)i * b->column_ + j];
+                    if (left) a[(size_t)(at + i) * n + j] = v;
+                    else a[(size_t)i * n + at + j] = v;
+                }
+            at += left ? b->row_ : b->column_;
+        }
+        for (double v : a) fro2 += v * v;
+        const int k = m < n ? m : n;
+        std::vector<double> sv(k), sup(k > 1 ? k - 1 : 1);
+        if (__real_LAPACKE_dgesvd(LAPACK_ROW_MAJOR, 'N', 'N', m, n, a.data(), n, sv.data(), nullptr, 1, nullptr, 1,
+                                  sup.data()) != 0)
+            return -2.0;
+        all.insert(all.end(), sv.begin(), sv.end());
+    }
+    if (all.empty() || fro2 == 0.0) return -1.0;
+    if (canpre > 1) canpre = 0.0;
+    std::sort(all.begin(), all.end(), [](double x, double y) { return x > y; });
+    const double fro = std::sqrt(fro2);
+    g_pre_gap = 1e300;
+    if (canpre > 0.0)
+        for (double v : all)
+            if (v > canpre && v / canpre < g_pre_gap) g_pre_gap = v / canpre;
+    long above = 0;
+    for (double v : all) above += v > canpre;
+    if (max_dim > 0 && max_dim < above) return (all[max_dim - 1] - all[max_dim]) / fro;
+    return -1.0;
+}
+
 static void canon_common(bool left, RealTensorLattice* self, int max_dim, double canpre) {
     int call = n_canon++;
+    g_pre_gap = -1.0;
+    g_cut_gap = g_trace ? truncation_gap(left, self, max_dim, canpre) : -1.0;
     bool dump = wanted(g_canon, call);
     NacWriter* w = dump ? new NacWriter(g_out + "/canon_" + std::to_string(call) + ".nac") : nullptr;
     if (w) {
@@ -219,6 +399,7 @@ static void canon_common(bool left, RealTensorLattice* self, int max_dim, double
     }
     if (left) __real__ZN17RealTensorLattice26LeftCanonicalTensorLatticeEid(self, max_dim, canpre);
     else __real__ZN17RealTensorLattice27RightCanonicalTensorLatticeEid(self, max_dim, canpre);
+    trace("C", left ? 0 : 1, self);
     if (w) {
         probe::write_lattice(*w, "after", self);
         delete w;
@@ -243,6 +424,8 @@ int main(int argc, char* argv[]) {
     g_canon = parse_list(std::getenv("PROBE_CANON"));
     g_struct_only = std::getenv("PROBE_STRUCT_ONLY") != nullptr;
     if (const char* s = std::getenv("PROBE_STOP")) g_stop = std::atoi(s);
+    g_gauge = std::getenv("PROBE_GAUGE") != nullptr && std::atoi(std::getenv("PROBE_GAUGE")) != 0;
+    if (std::getenv("PROBE_TRACE")) g_trace = std::fopen((g_out + "/trace.txt").c_str(), "w");
     g_steps = std::fopen((g_out + "/steps.txt").c_str(), "w");
 
     auto input = InputGroup(argv[1], "input");

@@ -11,6 +11,12 @@ chain16_spinless.in), and keeps:
   env_c<k>.nac          an environment update, inputs and outputs
   canon_c<k>.nac        a canonicalisation (SVD truncation), before and after
   steps_chain6.txt, steps_cylinder3x3.txt   whole runs of two small inputs
+  trace_gauge_<input>.txt   whole runs of the three inputs with the free signs of
+                        LAPACK's singular vectors / eigenvectors fixed by the
+                        library's convention (PROBE_GAUGE=1): one line per
+                        operation (E: Lanczos energy; X: expansion, C:
+                        canonicalisation with its truncation gaps, T: match,
+                        M: merge, with the sector dimensions after it)
   model_chain16.nac     the MPO per site and the quantum tables (first call)
   quicksort_cases.txt   inputs with ties and the index order the reference's
                         QuickSort (src/util/general.ih) returns (probe_sort)
@@ -44,6 +50,20 @@ def run_probe(inp: str, out: str, env_extra: dict) -> None:
     env = dict(os.environ, OMP_NUM_THREADS="1", OPENBLAS_NUM_THREADS="1", PROBE_OUT=out, **env_extra)
     with open(os.path.join(out, "log.txt"), "w") as log:
         subprocess.run([PROBE, inp], env=env, stdout=log, stderr=subprocess.STDOUT, check=True, cwd=out)
+
+
+def gauge_trace(name: str) -> None:
+    """Structure trace of a gauge-pinned reference run (norm, rand-count and
+    per-block fields dropped; they are diagnostics, not fixtures)."""
+    t = tempfile.mkdtemp(prefix="golden_gauge_" + name)
+    run_probe(os.path.join(ROOT, "dmrgcc_b200", "inputs", f"{name}_spinless.in"), t,
+              {"PROBE_GAUGE": "1", "PROBE_TRACE": "1"})
+    with open(os.path.join(t, "trace.txt")) as f, open(os.path.join(HERE, f"trace_gauge_{name}.txt"), "w") as g:
+        for line in f:
+            if line.startswith("Y"):
+                continue
+            parts = [p for p in line.split() if not p.startswith(("N:", "Q:", "S:"))]
+            g.write(" ".join(parts) + "\n")
 
 
 def quicksort_cases() -> None:
@@ -85,6 +105,8 @@ def main() -> int:
         t = tempfile.mkdtemp(prefix="golden_" + name)
         run_probe(os.path.join(ROOT, "dmrgcc_b200", "inputs", f"{name}_spinless.in"), t, {})
         shutil.copy(os.path.join(t, "steps.txt"), os.path.join(HERE, f"steps_{name}.txt"))
+    for name in ("chain6", "cylinder3x3", "chain16"):
+        gauge_trace(name)
     for kind, calls in (("heff", HEFF_CALLS), ("lanczos", HEFF_CALLS), ("env", ENV_CALLS), ("canon", CANON_CALLS)):
         for c in calls:
             shutil.copy(os.path.join(tmp, f"{kind}_{c}.nac"), os.path.join(HERE, f"{kind}_c{c}.nac"))
