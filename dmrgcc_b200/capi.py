@@ -64,6 +64,8 @@ _SIGS = {
     "dmrg_heff_apply": (C.c_int, [_VP, _VP, _VP, C.c_int]),
     "dmrg_heff_apply_host": (C.c_int, [_VP, _VP, _VP, C.c_int]),
     "dmrg_heff_profile": (C.c_int, [_VP, _VP, _VP, _D, _D]),
+    "dmrg_heff_apply_noalloc": (C.c_int, [C.c_int, C.c_int, _I, C.POINTER(Blocks), C.c_int, C.c_int, C.c_int, _D,
+                                          C.POINTER(Blocks), C.POINTER(Blocks), _VP, _VP, _VP, _VP, C.c_int, _VP]),
     "dmrg_lanczos": (C.c_int, [_VP, _VP, C.c_int, C.c_double, C.c_double, _D, _I]),
     "dmrg_canon_create": (C.c_int, [_VP, C.c_int, C.c_int, C.c_int, _I, _I, C.POINTER(Blocks), C.POINTER(_VP)]),
     "dmrg_canon_destroy": (C.c_int, [_VP]),

@@ -280,4 +280,19 @@ int launch_gemm_f64(const GemmSchedule& s, const double* A, const double* B, dou
     return DMRG_OK;
 }
 
+int launch_gemm_f64_tables(const GemmTerm* terms, const GemmGroup* groups, const GemmTile* tiles, int ntiles,
+                           bool ta, bool tb, const double* A, const double* B, double* C, bool accumulate,
+                           cudaStream_t stream) {
+    // Same kernel as launch_gemm_f64, with device tables supplied by the caller
+    // (no split-K groups: every group writes C directly).
+    if (ntiles <= 0) return DMRG_OK;
+    const int acc = accumulate ? 1 : 0;
+    if (!ta && !tb) gemm_f64_kernel<false, false><<<ntiles, NT, 0, stream>>>(A, B, C, nullptr, terms, groups, tiles, acc);
+    else if (ta && !tb) gemm_f64_kernel<true, false><<<ntiles, NT, 0, stream>>>(A, B, C, nullptr, terms, groups, tiles, acc);
+    else if (!ta && tb) gemm_f64_kernel<false, true><<<ntiles, NT, 0, stream>>>(A, B, C, nullptr, terms, groups, tiles, acc);
+    else gemm_f64_kernel<true, true><<<ntiles, NT, 0, stream>>>(A, B, C, nullptr, terms, groups, tiles, acc);
+    DMRG_CUDA_TRY(cudaGetLastError());
+    return DMRG_OK;
+}
+
 }  // namespace dmrg

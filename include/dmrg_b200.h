@@ -125,6 +125,24 @@ int dmrg_heff_apply_host(dmrg_heff_t h, const double* psi_host, double* out_host
 int dmrg_heff_profile(dmrg_heff_t h, const double* psi_dev, double* out_dev, double* ms_stage_a,
                       double* ms_stage_b);
 
+/* The same H_eff * psi for callers that cannot call cudaMalloc (for example a
+ * host framework that owns every device allocation under a fixed budget).  No
+ * reference counterpart: the reference has no device code.  It allocates
+ * nothing: it takes the block structure directly (as dmrg_heff_create) plus the
+ * device environments, psi and out, and keeps its schedule and the K*R
+ * intermediate in one static device array of 16 MiB per GPU that loads the
+ * library (held until exit).  Problems needing more return DMRG_E_ARG with the
+ * size required.  All calls share that array: calls that overlap on the GPU
+ * race.  The first call on a device looks up the array's device address; make
+ * it before any stream capture.  Runs on `stream` (a cudaStream_t; NULL = the
+ * legacy default stream) and returns after the work is queued and the
+ * schedule copied (it synchronises `stream`). */
+int dmrg_heff_apply_noalloc(int num_left_sector, int num_right_sector, const int* physics_index,
+                            const dmrg_blocks_t* ket, int physics_dim, int left_bond, int right_bond,
+                            const double* W, const dmrg_blocks_t* L, const dmrg_blocks_t* R,
+                            const double* L_dev, const double* R_dev, const double* psi_dev,
+                            double* out_dev, int accumulate, void* stream);
+
 /* ---- a4/a5: Lanczos ground state of H_eff ----------------------------------
  * Replaces RealTensorLanczos::LanczosMethod(int num_iter, int site, double& result)
  * (src/dmrg/realdmrg/real_tensor_lanczos.h:23, .cc:14-201).  psi_dev holds the
