@@ -81,6 +81,7 @@ _SIGS = {
     "dmrg_run_destroy": (C.c_int, [_VP]),
     "dmrg_run_half_sweeps": (C.c_int, [_VP, C.c_int, _D, _D, _I]),
     "dmrg_run_steps": (C.c_int, [_VP, C.c_int, _I, _I, _D, _I, _D, _I64, _D, _I]),
+    "dmrg_run_phases": (C.c_int, [_VP, C.c_int, _D, _I, _I]),
     "dmrg_model_create": (C.c_int, [C.c_char_p, C.c_char_p, C.POINTER(_VP)]),
     "dmrg_model_destroy": (C.c_int, [_VP]),
     "dmrg_model_info": (C.c_int, [_VP, _I, _I, _I]),
@@ -453,6 +454,18 @@ class Run:
         e, s = np.zeros(max(n.value, 1)), np.zeros(max(n.value, 1))
         check(lib().dmrg_run_half_sweeps(self.h, n.value, _dptr(e), _dptr(s), C.byref(n)), "dmrg_run_half_sweeps")
         return e[:n.value], s[:n.value]
+
+    PHASES = ("lanczos", "expansion", "canonicalisation", "environment", "match_merge")
+
+    def phases(self):
+        """(seconds[half_sweep, phase] in PHASES order, Jacobi SVD sweeps per half-sweep)."""
+        n = C.c_int()
+        check(lib().dmrg_run_phases(self.h, 0, None, None, C.byref(n)), "dmrg_run_phases")
+        k = max(n.value, 1)
+        sec = np.zeros((k, len(self.PHASES)))
+        sw = np.zeros(k, np.int32)
+        check(lib().dmrg_run_phases(self.h, n.value, _dptr(sec), _iptr(sw), C.byref(n)), "dmrg_run_phases")
+        return sec[:n.value], sw[:n.value]
 
     def steps(self) -> dict:
         n = C.c_int()

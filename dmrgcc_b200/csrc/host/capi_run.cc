@@ -117,6 +117,19 @@ int dmrg_run_steps(dmrg_run_t r, int cap, int* half_sweep, int* site, double* en
     return DMRG_OK;
 }
 
+int dmrg_run_phases(dmrg_run_t r, int cap, double* seconds, int* svd_sweeps, int* count) {
+    if (!r || !count) return set_error(DMRG_E_ARG, "null argument");
+    const auto& ph = r->engine->half_sweep_phases();
+    const auto& sw = r->engine->half_sweep_svd_sweeps();
+    *count = (int)ph.size();
+    for (int i = 0; i < (int)ph.size() && i < cap; ++i) {
+        if (seconds)
+            for (int k = 0; k < Engine::kPhases; ++k) seconds[(size_t)i * Engine::kPhases + k] = ph[i][k];
+        if (svd_sweeps) svd_sweeps[i] = sw[i];
+    }
+    return DMRG_OK;
+}
+
 int dmrg_model_create(const char* input_path, const char* model, dmrg_model_t* out) {
     if (!input_path || !out) return set_error(DMRG_E_ARG, "null argument");
     *out = nullptr;

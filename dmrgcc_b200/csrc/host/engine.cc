@@ -280,6 +280,7 @@ int Engine::CanonicalTensorSpace(int leigh, int site, double* discarded) {
     int64_t ks = 0, cs = 0;
     int sweeps = 0;
     if (rc == DMRG_OK) rc = dmrg_canon_out_info(c, &ks, &cs, &sweeps);
+    svd_sweeps_ += sweeps;
     const int nb = t.ket.d.count();
     std::vector<int> kr(std::max(nb, 1)), kc(std::max(nb, 1)), cr(nsec), cc(nsec), md(nsec);
     if (rc == DMRG_OK) rc = dmrg_canon_out_blocks(c, kr.data(), kc.data(), cr.data(), cc.data(), md.data());
@@ -1111,30 +1112,50 @@ int Engine::Run() {
         p_canpre_ = canpre_[h];
         p_noise_ = noise_[h];
         const bool l2r = (h % 2) == 0;
+        std::array<double, kPhases> ph{};
+        svd_sweeps_ = 0;
+        // phase clock: every phase ends with its stream drained
+        double tp = wall_time();
+        auto lap = [&](int k) -> int {
+            DMRG_CUDA_TRY(cudaStreamSynchronize(st_));
+            const double now = wall_time();
+            ph[k] += now - tp;
+            tp = now;
+            return DMRG_OK;
+        };
         if (l2r && opt_.verbose) std::printf("------------------------ sweep=%d ------------------------\n", h / 2);
         for (int k = 0; k < n_ - 1; ++k) {
             const int j = l2r ? k : n_ - 1 - k;
             const double ts = wall_time();
             int dim = 0;
             const int64_t psi_dim = lat_[j]->psi_dim();  // at the Lanczos call, like the reference's log
+            tp = wall_time();
             DMRG_TRY(LanczosMethod(num_iter_[h], j, energy_, dim));
+            DMRG_TRY(lap(0));
             if (trace_) std::fprintf(trace_, "E %d %d P:%lld %.12e\n", lanczos_calls_, j, (long long)psi_dim, energy_);
             ++lanczos_calls_;
             DMRG_TRY(ResetEnv(l2r ? 1 : 0, j));
             DMRG_TRY(ExpanTensorNetwork(l2r ? 0 : 1, j));
             DMRG_TRY(ExpanTensorSpace(l2r ? 0 : 1, j));
+            DMRG_TRY(lap(1));
             Trace("X", l2r ? 0 : 1, j);
             double disc = 0.0;
+            tp = wall_time();
             DMRG_TRY(CanonicalTensorSpace(l2r ? 0 : 1, j, &disc));
+            DMRG_TRY(lap(2));
             DMRG_TRY(ComputeTensorNetwork(l2r ? 0 : 1, j));
+            DMRG_TRY(lap(3));
             const int nxt = l2r ? j + 1 : j - 1;
             DMRG_TRY(MatchTensorSpace(l2r ? 0 : 1, nxt));
             Trace("T", l2r ? 0 : 1, nxt);
             DMRG_TRY(MergeTensorSpace(l2r ? 0 : 1, nxt));
+            DMRG_TRY(lap(4));
             records_.push_back(SweepRecord{h, j, l2r ? 0 : 1, energy_, dim, disc, psi_dim, wall_time() - ts});
         }
         half_energies_.push_back(energy_);
         half_seconds_.push_back(wall_time() - th);
+        half_phases_.push_back(ph);
+        half_svd_sweeps_.push_back(svd_sweeps_);
         if (opt_.verbose) std::printf("%s energy = %.12f\n", l2r ? "right" : "left", energy_);
     }
     if (opt_.verbose) std::printf("Total Time : %.12f s\n", wall_time() - t0);

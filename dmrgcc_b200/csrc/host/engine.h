@@ -6,6 +6,7 @@
 // libdmrg_b200's kernels.
 #pragma once
 
+#include <array>
 #include <cstdio>
 #include <memory>
 #include <string>
@@ -90,6 +91,10 @@ public:
     double last_energy() const { return energy_; }
     const std::vector<double>& half_sweep_energies() const { return half_energies_; }
     const std::vector<double>& half_sweep_seconds() const { return half_seconds_; }
+    // Per half-sweep: seconds in each phase (kPhases order) and Jacobi SVD sweeps.
+    static constexpr int kPhases = 5;  // Lanczos, expansion, canonicalisation, environment, match + merge
+    const std::vector<std::array<double, kPhases>>& half_sweep_phases() const { return half_phases_; }
+    const std::vector<int>& half_sweep_svd_sweeps() const { return half_svd_sweeps_; }
     TensorLattice& lattice(int i) { return *lat_[i]; }
     TensorContraction& contraction(int i) { return *con_[i]; }
     int num_site() const { return n_; }
@@ -144,6 +149,9 @@ private:
     ReduceScratch rs_;
     std::vector<SweepRecord> records_;
     std::vector<double> half_energies_, half_seconds_;
+    std::vector<std::array<double, kPhases>> half_phases_;
+    std::vector<int> half_svd_sweeps_;
+    int svd_sweeps_ = 0;  // Jacobi sweeps of the canonicalisations of the current half-sweep
     double energy_ = 0.0;
     int half_sweep_ = 0;
     int lanczos_calls_ = 0;

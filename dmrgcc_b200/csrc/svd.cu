@@ -2,6 +2,8 @@
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 
 #include "svd.cuh"
@@ -25,7 +27,6 @@ constexpr double kZeroRel = 4.0 * DBL_EPSILON;
 struct SvdSmem {
     double G[kPair * kLd];
     double Q[kPair * kLd];
-    double X[kChunk * kLd];
     double cs[kPair];
     int pq[kPair];
     double red[kThreads / 32];
@@ -63,104 +64,113 @@ __device__ double block_max(double v, SvdSmem& S) {
     return r;
 }
 
-// Loads rows [k0, k0+kChunk) of the pair's 64 columns (zero outside) into S.X[k][c].
-__device__ __forceinline__ void load_chunk(SvdSmem& S, const double* __restrict__ base, int ld, int nrows,
-                                           int ncols, int colI, int colJ, int k0) {
-    for (int idx = threadIdx.x; idx < kChunk * kPair; idx += kThreads) {
-        const int c = idx / kChunk, k = idx % kChunk;
-        const int gc = c < kBlk ? colI + c : colJ + c - kBlk;
-        const bool v = gc < ncols && k0 + k < nrows;
-        S.X[k * kLd + c] = v ? base[(int64_t)gc * ld + k0 + k] : 0.0;
-    }
+__device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
 }
 
-__device__ __forceinline__ void store_chunk(SvdSmem& S, double* __restrict__ base, int ld, int nrows, int ncols,
-                                            int colI, int colJ, int k0) {
-    for (int idx = threadIdx.x; idx < kChunk * kPair; idx += kThreads) {
-        const int c = idx / kChunk, k = idx % kChunk;
-        const int gc = c < kBlk ? colI + c : colJ + c - kBlk;
-        if (gc < ncols && k0 + k < nrows) base[(int64_t)gc * ld + k0 + k] = S.X[k * kLd + c];
-    }
-}
-
-// X (kChunk x 64, in S.X) <- X * Q  (in place through registers)
-__device__ __forceinline__ void rotate_chunk(SvdSmem& S) {
-    const int k = threadIdx.x / 8, c0 = (threadIdx.x % 8) * 8;
-    double y[8];
-#pragma unroll
-    for (int e = 0; e < 8; ++e) y[e] = 0.0;
-    for (int c = 0; c < kPair; ++c) {
-        const double x = S.X[k * kLd + c];
-#pragma unroll
-        for (int e = 0; e < 8; ++e) y[e] += x * S.Q[c * kLd + c0 + e];
-    }
-    __syncthreads();
-#pragma unroll
-    for (int e = 0; e < 8; ++e) S.X[k * kLd + c0 + e] = y[e];
-    __syncthreads();
-}
-
-__global__ void __launch_bounds__(kThreads) jacobi_round_kernel(const SvdProblem* __restrict__ probs,
-                                                                const SvdTask* __restrict__ tasks, int round,
-                                                                double* __restrict__ W, double* __restrict__ Qacc,
-                                                                const double* __restrict__ fro2,
-                                                                unsigned long long* __restrict__ conv) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    SvdSmem& S = *reinterpret_cast<SvdSmem*>(smem_raw);
-    const SvdTask task = tasks[blockIdx.x];
+// Stage 1 of a round: partial Gram matrices.  Item = (pair task, row range of W);
+// 128 threads (2x2 warps, 32x32 each = 4x4 DMMA tiles); G_part = X^T X over the
+// item's rows, X = the pair's 64 columns, streamed 32 rows at a time into a
+// column-major shared tile (row pad 4: conflict-free stores and fragment reads).
+constexpr int kGramLd = kChunk + 4;
+__global__ void __launch_bounds__(128) gram_kernel(const SvdProblem* __restrict__ probs,
+                                                   const SvdTask* __restrict__ tasks,
+                                                   const SvdItem* __restrict__ items, int round,
+                                                   const double* __restrict__ W, double* __restrict__ gpart) {
+    __shared__ double Xt[kPair * kGramLd];  // Xt[c][k]
+    const SvdItem it = items[blockIdx.x];
+    const SvdTask task = tasks[it.task];
     const SvdProblem p = probs[task.problem];
     int I, J;
     rr_pair(round, task.pair, p.nbe, I, J);
     const int colI = I * kBlk, colJ = J * kBlk;
-    double* Wp = W + p.w_off;
-    double* Qp = Qacc + p.q_off;
-    const double tol = 2.0 * DBL_EPSILON * sqrt((double)p.rows);
-    const double zero2 = kZeroRel * kZeroRel * (double)p.rows * fro2[task.problem];
-
-    // ---- Gram matrix of the pair: G = X^T X over all rows -----------------------
-    const int ty = threadIdx.x / 16, tx = threadIdx.x % 16;  // 4x4 micro-tile (rows ty*4.., cols tx*4..)
-    double g[4][4];
+    const double* Wp = W + p.w_off;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int wm = warp >> 1, wn = warp & 1, fr = lane >> 2, fc = lane & 3;
+    double acc[4][4][2];
 #pragma unroll
-    for (int a = 0; a < 4; ++a)
+    for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int b = 0; b < 4; ++b) g[a][b] = 0.0;
-    for (int k0 = 0; k0 < p.rows; k0 += kChunk) {
-        load_chunk(S, Wp, p.rows, p.rows, p.cols, colI, colJ, k0);
+        for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+    for (int k0 = it.r0; k0 < it.r1; k0 += kChunk) {
+        for (int idx = threadIdx.x; idx < kChunk * kPair; idx += 128) {
+            const int c = idx / kChunk, k = idx % kChunk;
+            const int gc = c < kBlk ? colI + c : colJ + c - kBlk;
+            const bool v = gc < p.cols && k0 + k < it.r1;
+            Xt[c * kGramLd + k] = v ? Wp[(int64_t)gc * p.rows + k0 + k] : 0.0;
+        }
         __syncthreads();
-        for (int k = 0; k < kChunk; ++k) {
-            double xa[4], xb[4];
 #pragma unroll
-            for (int a = 0; a < 4; ++a) xa[a] = S.X[k * kLd + ty * 4 + a];
+        for (int kk = 0; kk < kChunk; kk += 4) {
+            double a[4], b[4];
 #pragma unroll
-            for (int b = 0; b < 4; ++b) xb[b] = S.X[k * kLd + tx * 4 + b];
+            for (int i = 0; i < 4; ++i) a[i] = Xt[(wm * 32 + i * 8 + fr) * kGramLd + kk + fc];
 #pragma unroll
-            for (int a = 0; a < 4; ++a)
+            for (int j = 0; j < 4; ++j) b[j] = Xt[(wn * 32 + j * 8 + fr) * kGramLd + kk + fc];
 #pragma unroll
-                for (int b = 0; b < 4; ++b) g[a][b] += xa[a] * xb[b];
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) dmma_8x8x4(acc[i][j][0], acc[i][j][1], a[i], b[j]);
         }
         __syncthreads();
     }
+    double* g = gpart + (int64_t)blockIdx.x * kPair * kPair;
 #pragma unroll
-    for (int a = 0; a < 4; ++a)
+    for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int b = 0; b < 4; ++b) S.G[(ty * 4 + a) * kLd + tx * 4 + b] = g[a][b];
-    for (int idx = threadIdx.x; idx < kPair * kPair; idx += kThreads)
+        for (int j = 0; j < 4; ++j) {
+            const int row = wm * 32 + i * 8 + fr, col = wn * 32 + j * 8 + 2 * fc;
+            g[row * kPair + col] = acc[i][j][0];
+            g[row * kPair + col + 1] = acc[i][j][1];
+        }
+}
+
+// Stage 2: one CTA per pair task.  Sums the task's partial Gram matrices (fixed
+// order), measures the pair's convergence, and (unless converged) runs a few
+// cyclic Jacobi sweeps on the 64x64 Gram matrix, writing the accumulated 64x64
+// rotation to rot[task - first] and skip[task - first] = 0.
+__global__ void __launch_bounds__(kThreads) solve_kernel(const SvdProblem* __restrict__ probs,
+                                                         const SvdTask* __restrict__ tasks, int first,
+                                                         const double* __restrict__ gpart,
+                                                         const double* __restrict__ fro2, double* __restrict__ rot,
+                                                         int* __restrict__ skip, unsigned long long* __restrict__ conv) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    SvdSmem& S = *reinterpret_cast<SvdSmem*>(smem_raw);
+    const int t = first + blockIdx.x;
+    const SvdTask task = tasks[t];
+    const SvdProblem p = probs[task.problem];
+    const double tol = 2.0 * DBL_EPSILON * sqrt((double)p.rows);
+    const double zero2 = kZeroRel * kZeroRel * (double)p.rows * fro2[task.problem];
+    for (int idx = threadIdx.x; idx < kPair * kPair; idx += kThreads) {
+        double v = 0.0;
+        for (int c = 0; c < task.g_count; ++c) v += gpart[(int64_t)(task.g_first + c) * kPair * kPair + idx];
+        S.G[(idx / kPair) * kLd + idx % kPair] = v;
         S.Q[(idx / kPair) * kLd + idx % kPair] = (idx / kPair == idx % kPair) ? 1.0 : 0.0;
+    }
     __syncthreads();
 
-    // ---- outer convergence measure: max |g_ij| / sqrt(g_ii g_jj) over the pair --
+    // ---- convergence measure over the pair: |g_ij| / (||A||_F max(|x_i|, |x_j|)),
+    // the size (relative to ||A||_F) of the perturbation of A that leaving the pair
+    // unrotated amounts to.  Below tol the pair is as converged as a backward
+    // stable SVD can tell (for two columns of norm ~||A|| this is the usual
+    // relative test; a column far below ||A|| needs only an angle ~tol ||A|| / |x|).
+    const double fro = sqrt(fro2[task.problem]);
     double worst = 0.0;
     for (int idx = threadIdx.x; idx < kPair * kPair; idx += kThreads) {
         const int a = idx / kPair, b = idx % kPair;
         if (a >= b) continue;
         const double ga = S.G[a * kLd + a], gb = S.G[b * kLd + b];
-        if (ga > zero2 && gb > zero2) worst = fmax(worst, fabs(S.G[a * kLd + b]) / sqrt(ga * gb));
+        if (ga > zero2 && gb > zero2) worst = fmax(worst, fabs(S.G[a * kLd + b]) / (fro * sqrt(fmax(ga, gb))));
     }
     worst = block_max(worst, S);
-    if (threadIdx.x == 0) atomicMax(conv + task.problem, (unsigned long long)__double_as_longlong(worst));
+    if (threadIdx.x == 0) {
+        atomicMax(conv + task.problem, (unsigned long long)__double_as_longlong(worst));
+        skip[blockIdx.x] = worst <= tol ? 1 : 0;
+    }
     if (worst <= tol) return;  // pair already orthogonal: nothing to rotate
 
-    // ---- inner cyclic Jacobi on the 64x64 Gram matrix, accumulating Q ----------
     for (int sweep = 0; sweep < kInnerSweeps; ++sweep) {
         for (int r = 0; r < kPair - 1; ++r) {
             if (threadIdx.x < kPair / 2) {
@@ -169,11 +179,12 @@ __global__ void __launch_bounds__(kThreads) jacobi_round_kernel(const SvdProblem
                 const double apq = S.G[a * kLd + b];
                 double c = 1.0, s = 0.0;
                 const double daa = S.G[a * kLd + a], dbb = S.G[b * kLd + b];
-                if (apq != 0.0 && daa > zero2 && dbb > zero2 && fabs(apq) > DBL_EPSILON * 1e-3 * sqrt(daa * dbb)) {
+                if (apq != 0.0 && daa > zero2 && dbb > zero2 &&
+                    fabs(apq) > DBL_EPSILON * 1e-3 * fro * sqrt(fmax(daa, dbb))) {
                     const double tau = (dbb - daa) / (2.0 * apq);
-                    const double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
-                    c = 1.0 / sqrt(1.0 + t * t);
-                    s = t * c;
+                    const double tt = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
+                    c = 1.0 / sqrt(1.0 + tt * tt);
+                    s = tt * c;
                 }
                 S.cs[2 * threadIdx.x] = c;
                 S.cs[2 * threadIdx.x + 1] = s;
@@ -208,21 +219,75 @@ __global__ void __launch_bounds__(kThreads) jacobi_round_kernel(const SvdProblem
             __syncthreads();
         }
     }
+    double* R = rot + (int64_t)blockIdx.x * kPair * kPair;
+    for (int idx = threadIdx.x; idx < kPair * kPair; idx += kThreads) R[idx] = S.Q[(idx / kPair) * kLd + idx % kPair];
+}
 
-    // ---- apply the pair rotation to W's and to the accumulated rotation's columns
-    for (int k0 = 0; k0 < p.rows; k0 += kChunk) {
-        load_chunk(S, Wp, p.rows, p.rows, p.cols, colI, colJ, k0);
-        __syncthreads();
-        rotate_chunk(S);
-        store_chunk(S, Wp, p.rows, p.rows, p.cols, colI, colJ, k0);
-        __syncthreads();
+// Stage 3: item = (pair task, segment, row range): the pair's 64 columns of W
+// (segment 0) or of the accumulated rotation (segment 1), rows [r0, r1) with
+// r1 - r0 <= 64, are multiplied by the task's 64x64 rotation (DMMA, in place).
+// Shared tiles: Xt[c][row] and R[c][col], row pad 4 (conflict-free).
+constexpr int kRotLd = kPair + 4;
+constexpr size_t kRotSmem = 2 * sizeof(double) * kPair * kRotLd;
+__global__ void __launch_bounds__(128) rotate_kernel(const SvdProblem* __restrict__ probs,
+                                                     const SvdTask* __restrict__ tasks,
+                                                     const SvdItem* __restrict__ items, int round, int first,
+                                                     const double* __restrict__ rot, const int* __restrict__ skip,
+                                                     double* __restrict__ W, double* __restrict__ Qacc) {
+    extern __shared__ __align__(16) double rsm[];
+    double* Xt = rsm;                   // [64 cols][kRotLd]
+    double* R = rsm + kPair * kRotLd;   // [64][kRotLd]
+    const SvdItem it = items[blockIdx.x];
+    if (skip[it.task - first]) return;
+    const SvdTask task = tasks[it.task];
+    const SvdProblem p = probs[task.problem];
+    int I, J;
+    rr_pair(round, task.pair, p.nbe, I, J);
+    const int colI = I * kBlk, colJ = J * kBlk;
+    double* base = it.seg == 0 ? W + p.w_off : Qacc + p.q_off;
+    const int ld = it.seg == 0 ? p.rows : p.cols;
+    const double* Rg = rot + (int64_t)(it.task - first) * kPair * kPair;
+    for (int idx = threadIdx.x; idx < kPair * kPair; idx += 128) {
+        const int c = idx / kPair, k = idx % kPair;  // consecutive threads: consecutive rows of a column
+        const int gc = c < kBlk ? colI + c : colJ + c - kBlk;
+        const bool v = gc < p.cols && it.r0 + k < it.r1;
+        Xt[c * kRotLd + k] = v ? base[(int64_t)gc * ld + it.r0 + k] : 0.0;
+        R[c * kRotLd + k] = Rg[idx];
     }
-    for (int k0 = 0; k0 < p.cols; k0 += kChunk) {
-        load_chunk(S, Qp, p.cols, p.cols, p.cols, colI, colJ, k0);
-        __syncthreads();
-        rotate_chunk(S);
-        store_chunk(S, Qp, p.cols, p.cols, p.cols, colI, colJ, k0);
-        __syncthreads();
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int wm = warp >> 1, wn = warp & 1, fr = lane >> 2, fc = lane & 3;
+    double acc[4][4][2];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+#pragma unroll 4
+    for (int kk = 0; kk < kPair; kk += 4) {
+        double a[4], b[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) a[i] = Xt[(kk + fc) * kRotLd + wm * 32 + i * 8 + fr];  // X[row][c]
+#pragma unroll
+        for (int j = 0; j < 4; ++j) b[j] = R[(kk + fc) * kRotLd + wn * 32 + j * 8 + fr];   // R[c][col]
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) dmma_8x8x4(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int row = wm * 32 + i * 8 + fr, col = wn * 32 + j * 8 + 2 * fc;
+            Xt[col * kRotLd + row] = acc[i][j][0];
+            Xt[(col + 1) * kRotLd + row] = acc[i][j][1];
+        }
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < kPair * kPair; idx += 128) {
+        const int c = idx / kPair, k = idx % kPair;
+        const int gc = c < kBlk ? colI + c : colJ + c - kBlk;
+        if (gc < p.cols && it.r0 + k < it.r1) base[(int64_t)gc * ld + it.r0 + k] = Xt[c * kRotLd + k];
     }
 }
 
@@ -335,13 +400,47 @@ int BatchedSvd::plan(const std::vector<int>& m, const std::vector<int>& n, cudaS
         probs.push_back(p);
         max_rounds = std::max(max_rounds, p.nbe - 1);
     }
+    // Row ranges of the Gram items: at least 256 rows each, fewer items than
+    // ~4 per SM in the widest round (bounds the partial-Gram buffer).
+    int64_t widest = 0;
+    for (int r = 0; r < max_rounds; ++r) {
+        int64_t rows = 0;
+        for (const SvdProblem& p : probs)
+            if (r < p.nbe - 1) rows += (int64_t)p.rows * (p.nbe / 2);
+        widest = std::max(widest, rows);
+    }
+    const int gram_rows = (int)std::max<int64_t>(256, ((widest / 600 + 31) / 32) * 32);
+    gram_items.clear();
+    rot_items.clear();
+    round_gram_first.clear();
+    round_rot_first.clear();
+    max_round_tasks = max_round_gram = 0;
     for (int r = 0; r < max_rounds; ++r) {
         round_first.push_back((int)tasks.size());
-        for (int pi = 0; pi < (int)probs.size(); ++pi)
-            if (r < probs[pi].nbe - 1)
-                for (int k = 0; k < probs[pi].nbe / 2; ++k) tasks.push_back(SvdTask{pi, k});
+        round_gram_first.push_back((int)gram_items.size());
+        round_rot_first.push_back((int)rot_items.size());
+        for (int pi = 0; pi < (int)probs.size(); ++pi) {
+            const SvdProblem& p = probs[pi];
+            if (r >= p.nbe - 1) continue;
+            for (int k = 0; k < p.nbe / 2; ++k) {
+                const int t = (int)tasks.size();
+                SvdTask task{pi, k, (int)gram_items.size() - round_gram_first.back(), 0};
+                for (int r0 = 0; r0 < p.rows; r0 += gram_rows)
+                    gram_items.push_back(SvdItem{t, 0, r0, std::min(p.rows, r0 + gram_rows)});
+                task.g_count = (int)gram_items.size() - round_gram_first.back() - task.g_first;
+                tasks.push_back(task);
+                for (int r0 = 0; r0 < p.rows; r0 += kPair)
+                    rot_items.push_back(SvdItem{t, 0, r0, std::min(p.rows, r0 + kPair)});
+                for (int r0 = 0; r0 < p.cols; r0 += kPair)
+                    rot_items.push_back(SvdItem{t, 1, r0, std::min(p.cols, r0 + kPair)});
+            }
+        }
+        max_round_tasks = std::max(max_round_tasks, (int)tasks.size() - round_first.back());
+        max_round_gram = std::max(max_round_gram, (int)gram_items.size() - round_gram_first.back());
     }
     round_first.push_back((int)tasks.size());
+    round_gram_first.push_back((int)gram_items.size());
+    round_rot_first.push_back((int)rot_items.size());
     DMRG_TRY(d_w.alloc((size_t)std::max<int64_t>(woff, 1) * sizeof(double)));
     DMRG_TRY(d_q.alloc((size_t)std::max<int64_t>(qoff, 1) * sizeof(double)));
     DMRG_TRY(d_s.alloc((size_t)std::max<int64_t>(2 * soff, 1) * sizeof(double)));
@@ -351,8 +450,14 @@ int BatchedSvd::plan(const std::vector<int>& m, const std::vector<int>& n, cudaS
     DMRG_TRY(d_sign.alloc((size_t)std::max<int64_t>(soff, 1) * sizeof(double)));
     DMRG_TRY(upload(d_probs, probs, st));
     DMRG_TRY(upload(d_tasks, tasks, st));
-    DMRG_CUDA_TRY(cudaFuncSetAttribute(jacobi_round_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    DMRG_TRY(upload(d_gram_items, gram_items, st));
+    DMRG_TRY(upload(d_rot_items, rot_items, st));
+    DMRG_TRY(d_gpart.alloc((size_t)std::max(max_round_gram, 1) * kPair * kPair * sizeof(double)));
+    DMRG_TRY(d_rot.alloc((size_t)std::max(max_round_tasks, 1) * kPair * kPair * sizeof(double)));
+    DMRG_TRY(d_skip.alloc((size_t)std::max(max_round_tasks, 1) * sizeof(int)));
+    DMRG_CUDA_TRY(cudaFuncSetAttribute(solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)sizeof(SvdSmem)));
+    DMRG_CUDA_TRY(cudaFuncSetAttribute(rotate_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRotSmem));
     return DMRG_OK;
 }
 
@@ -365,22 +470,46 @@ int BatchedSvd::run(cudaStream_t st, int* sweeps_out) {
     init_identity_kernel<<<np, 256, 0, st>>>(d_probs.as<SvdProblem>(), d_q.as<double>());
     fro2_kernel<<<np, 256, 0, st>>>(d_probs.as<SvdProblem>(), d_w.as<double>(), d_fro2.as<double>());
     std::vector<unsigned long long> conv(np);
+    static const bool debug = std::getenv("DMRG_SVD_DEBUG") != nullptr;  // per-sweep convergence to stderr
     int sweep = 0, worst_at = 0;
     double worst_left = 0.0;
     for (; sweep < kMaxSweeps; ++sweep) {
         DMRG_CUDA_TRY(cudaMemsetAsync(d_conv.ptr, 0, np * sizeof(unsigned long long), st));
         for (int r = 0; r < max_rounds; ++r) {
-            const int n = round_first[r + 1] - round_first[r];
-            if (n == 0) continue;
-            jacobi_round_kernel<<<n, kThreads, sizeof(SvdSmem), st>>>(
-                d_probs.as<SvdProblem>(), d_tasks.as<SvdTask>() + round_first[r], r, d_w.as<double>(),
-                d_q.as<double>(), d_fro2.as<double>(), d_conv.as<unsigned long long>());
+            const int nt = round_first[r + 1] - round_first[r];
+            const int ng = round_gram_first[r + 1] - round_gram_first[r];
+            const int nr = round_rot_first[r + 1] - round_rot_first[r];
+            if (nt == 0) continue;
+            gram_kernel<<<ng, 128, 0, st>>>(d_probs.as<SvdProblem>(), d_tasks.as<SvdTask>(),
+                                            d_gram_items.as<SvdItem>() + round_gram_first[r], r, d_w.as<double>(),
+                                            d_gpart.as<double>());
+            solve_kernel<<<nt, kThreads, sizeof(SvdSmem), st>>>(
+                d_probs.as<SvdProblem>(), d_tasks.as<SvdTask>(), round_first[r], d_gpart.as<double>(),
+                d_fro2.as<double>(), d_rot.as<double>(), d_skip.as<int>(), d_conv.as<unsigned long long>());
+            rotate_kernel<<<nr, 128, kRotSmem, st>>>(d_probs.as<SvdProblem>(), d_tasks.as<SvdTask>(),
+                                                     d_rot_items.as<SvdItem>() + round_rot_first[r], r,
+                                                     round_first[r], d_rot.as<double>(), d_skip.as<int>(),
+                                                     d_w.as<double>(), d_q.as<double>());
         }
         DMRG_CUDA_TRY(cudaGetLastError());
         DMRG_CUDA_TRY(cudaMemcpyAsync(conv.data(), d_conv.ptr, np * sizeof(unsigned long long),
                                       cudaMemcpyDeviceToHost, st));
         DMRG_CUDA_TRY(cudaStreamSynchronize(st));
         bool done = true;
+        if (debug) {
+            double w = 0.0;
+            int wi = 0;
+            for (int i = 0; i < np; ++i) {
+                double x;
+                std::memcpy(&x, &conv[i], sizeof(double));
+                if (x > w) {
+                    w = x;
+                    wi = i;
+                }
+            }
+            std::fprintf(stderr, "svd sweep %d: worst %.3e (sector %d x %d)%s", sweep, w, probs[wi].m, probs[wi].n,
+                         sweep % 4 == 3 ? "\n" : "; ");
+        }
         for (int i = 0; i < np; ++i) {
             double worst;
             std::memcpy(&worst, &conv[i], sizeof(double));

@@ -5,11 +5,16 @@
 // columns: W = A when n <= m (right rotations accumulate V), W = A^T otherwise
 // (they accumulate U).  A sweep visits every pair of column blocks once in the
 // round-robin order; in a round all pairs of all sectors are independent and
-// each is handled by one CTA: 64x64 Gram matrix of the pair, a few cyclic
-// Jacobi sweeps on it in shared memory, then the pair's columns of W and of the
-// accumulated rotation are multiplied by the 64x64 rotation.  Converged when no
-// pair has |g_ij| > tol * sqrt(g_ii g_jj) (high relative accuracy, which the
-// reference's canpre cut at 1e-12 needs); columns of a rank-deficient matrix
+// is split over CTAs by rows: (1) partial 64x64 Gram matrices of the pair over
+// row ranges (DMMA), (2) one CTA per pair sums them and runs a few cyclic
+// Jacobi sweeps on the Gram matrix in shared memory, (3) 64-row slices of the
+// pair's columns of W and of the accumulated rotation are multiplied by the
+// resulting 64x64 rotation (DMMA).  Converged when no
+// pair has |g_ij| > tol ||A||_F max(|x_i|, |x_j|), tol = 2 eps sqrt(rows): the
+// remaining non-orthogonality is a backward perturbation of A below rounding
+// level, the accuracy of a backward-stable SVD such as the reference's dgesvd
+// (singular values to ~eps ||A||, enough for its canpre cut at 1e-12 of a
+// normalised state); columns of a rank-deficient matrix
 // whose norm falls to rounding level (4 eps sqrt(rows) ||A||_F) are left out of
 // rotations and of that test.  Singular values are the final column
 // norms, sorted in descending order.  The free sign of each singular pair is
@@ -37,6 +42,13 @@ struct SvdProblem {
 struct SvdTask {
     int problem;
     int pair;
+    int g_first, g_count;  // its Gram items, as indices into the round's item list
+};
+
+struct SvdItem {   // a row range of one pair task's columns
+    int task;      // index into the task list
+    int seg;       // 0: rows of W, 1: rows of the accumulated rotation
+    int r0, r1;
 };
 
 class BatchedSvd {
@@ -55,11 +67,14 @@ public:
 
     DeviceBuffer d_w, d_q, d_s, d_perm, d_probs, d_tasks, d_conv, d_fro2;
     DeviceBuffer d_sign;  // +-1 per sorted singular triplet (sign convention, set by run())
+    DeviceBuffer d_gram_items, d_rot_items, d_gpart, d_rot, d_skip;
     std::vector<SvdProblem> probs;
     std::vector<int> index;             // sector -> problem (-1 when empty)
     std::vector<int> round_first;       // task offset of each round
     std::vector<SvdTask> tasks;
-    int max_rounds = 0;
+    std::vector<SvdItem> gram_items, rot_items;    // per round, contiguous
+    std::vector<int> round_gram_first, round_rot_first;
+    int max_rounds = 0, max_round_tasks = 0, max_round_gram = 0;
 };
 
 }  // namespace dmrg

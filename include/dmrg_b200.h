@@ -235,6 +235,12 @@ int dmrg_run_half_sweeps(dmrg_run_t r, int cap, double* energies, double* second
  * dimension, discarded weight of the truncation, psi_dim, seconds. */
 int dmrg_run_steps(dmrg_run_t r, int cap, int* half_sweep, int* site, double* energy, int* lanczos_dim,
                    double* discarded, int64_t* psi_dim, double* seconds, int* count);
+/* Where each half-sweep's time went (no reference counterpart; the reference
+ * prints only totals): seconds[5*i + k] for phase k of half-sweep i, k = 0
+ * Lanczos, 1 subspace expansion, 2 canonicalisation (SVD + truncation), 3
+ * environment update, 4 match + merge; svd_sweeps[i] = Jacobi sweeps summed over
+ * the half-sweep's canonicalisations. */
+int dmrg_run_phases(dmrg_run_t r, int cap, double* seconds, int* svd_sweeps, int* count);
 
 /* ---- model layer (host only) -----------------------------------------------
  * The MPO of RealSpinlessBoseSquareHamiltonian::DefineTensorHamiltonian
