@@ -16,7 +16,7 @@ constexpr int kPair = 64;       // columns per pair
 constexpr int kChunk = 32;      // rows per streamed chunk
 constexpr int kThreads = 256;
 constexpr int kLd = kPair + 1;  // padded row of the shared 64x64 matrices
-constexpr int kInnerSweeps = 4;
+constexpr int kInnerSweeps = 2;
 constexpr int kMaxSweeps = 40;
 // Columns whose norm is below kZeroRel * sqrt(rows) * ||A||_F are rounding
 // residue of a rank-deficient matrix: they take part in no rotation and in no
@@ -78,7 +78,8 @@ constexpr int kGramLd = kChunk + 4;
 __global__ void __launch_bounds__(128) gram_kernel(const SvdProblem* __restrict__ probs,
                                                    const SvdTask* __restrict__ tasks,
                                                    const SvdItem* __restrict__ items, int round,
-                                                   const double* __restrict__ W, double* __restrict__ gpart) {
+                                                   const int* __restrict__ colmap, const double* __restrict__ W,
+                                                   double* __restrict__ gpart) {
     __shared__ double Xt[kPair * kGramLd];  // Xt[c][k]
     const SvdItem it = items[blockIdx.x];
     const SvdTask task = tasks[it.task];
@@ -97,9 +98,9 @@ __global__ void __launch_bounds__(128) gram_kernel(const SvdProblem* __restrict_
     for (int k0 = it.r0; k0 < it.r1; k0 += kChunk) {
         for (int idx = threadIdx.x; idx < kChunk * kPair; idx += 128) {
             const int c = idx / kChunk, k = idx % kChunk;
-            const int gc = c < kBlk ? colI + c : colJ + c - kBlk;
-            const bool v = gc < p.cols && k0 + k < it.r1;
-            Xt[c * kGramLd + k] = v ? Wp[(int64_t)gc * p.rows + k0 + k] : 0.0;
+            const int vc = c < kBlk ? colI + c : colJ + c - kBlk;
+            const bool v = vc < p.cols && k0 + k < it.r1;
+            Xt[c * kGramLd + k] = v ? Wp[(int64_t)colmap[p.perm_off + vc] * p.rows + k0 + k] : 0.0;
         }
         __syncthreads();
 #pragma unroll
@@ -135,7 +136,8 @@ __global__ void __launch_bounds__(kThreads) solve_kernel(const SvdProblem* __res
                                                          const SvdTask* __restrict__ tasks, int first,
                                                          const double* __restrict__ gpart,
                                                          const double* __restrict__ fro2, double* __restrict__ rot,
-                                                         int* __restrict__ skip, unsigned long long* __restrict__ conv) {
+                                                         int* __restrict__ skip, unsigned long long* __restrict__ conv,
+                                                         int inner_sweeps) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     SvdSmem& S = *reinterpret_cast<SvdSmem*>(smem_raw);
     const int t = first + blockIdx.x;
@@ -171,7 +173,7 @@ __global__ void __launch_bounds__(kThreads) solve_kernel(const SvdProblem* __res
     }
     if (worst <= tol) return;  // pair already orthogonal: nothing to rotate
 
-    for (int sweep = 0; sweep < kInnerSweeps; ++sweep) {
+    for (int sweep = 0; sweep < inner_sweeps; ++sweep) {
         for (int r = 0; r < kPair - 1; ++r) {
             if (threadIdx.x < kPair / 2) {
                 int a, b;
@@ -233,7 +235,8 @@ __global__ void __launch_bounds__(128) rotate_kernel(const SvdProblem* __restric
                                                      const SvdTask* __restrict__ tasks,
                                                      const SvdItem* __restrict__ items, int round, int first,
                                                      const double* __restrict__ rot, const int* __restrict__ skip,
-                                                     double* __restrict__ W, double* __restrict__ Qacc) {
+                                                     const int* __restrict__ colmap, double* __restrict__ W,
+                                                     double* __restrict__ Qacc) {
     extern __shared__ __align__(16) double rsm[];
     double* Xt = rsm;                   // [64 cols][kRotLd]
     double* R = rsm + kPair * kRotLd;   // [64][kRotLd]
@@ -249,9 +252,9 @@ __global__ void __launch_bounds__(128) rotate_kernel(const SvdProblem* __restric
     const double* Rg = rot + (int64_t)(it.task - first) * kPair * kPair;
     for (int idx = threadIdx.x; idx < kPair * kPair; idx += 128) {
         const int c = idx / kPair, k = idx % kPair;  // consecutive threads: consecutive rows of a column
-        const int gc = c < kBlk ? colI + c : colJ + c - kBlk;
-        const bool v = gc < p.cols && it.r0 + k < it.r1;
-        Xt[c * kRotLd + k] = v ? base[(int64_t)gc * ld + it.r0 + k] : 0.0;
+        const int vc = c < kBlk ? colI + c : colJ + c - kBlk;
+        const bool v = vc < p.cols && it.r0 + k < it.r1;
+        Xt[c * kRotLd + k] = v ? base[(int64_t)colmap[p.perm_off + vc] * ld + it.r0 + k] : 0.0;
         R[c * kRotLd + k] = Rg[idx];
     }
     __syncthreads();
@@ -286,8 +289,8 @@ __global__ void __launch_bounds__(128) rotate_kernel(const SvdProblem* __restric
     __syncthreads();
     for (int idx = threadIdx.x; idx < kPair * kPair; idx += 128) {
         const int c = idx / kPair, k = idx % kPair;
-        const int gc = c < kBlk ? colI + c : colJ + c - kBlk;
-        if (gc < p.cols && it.r0 + k < it.r1) base[(int64_t)gc * ld + it.r0 + k] = Xt[c * kRotLd + k];
+        const int vc = c < kBlk ? colI + c : colJ + c - kBlk;
+        if (vc < p.cols && it.r0 + k < it.r1) base[(int64_t)colmap[p.perm_off + vc] * ld + it.r0 + k] = Xt[c * kRotLd + k];
     }
 }
 
@@ -315,20 +318,28 @@ __global__ void init_identity_kernel(const SvdProblem* __restrict__ probs, doubl
         q[idx] = (idx / p.cols == idx % p.cols) ? 1.0 : 0.0;
 }
 
-// Column norms -> singular values, sorted descending (ties by column index).
-__global__ void __launch_bounds__(256) finalize_kernel(const SvdProblem* __restrict__ probs,
-                                                       const double* __restrict__ W, double* __restrict__ sig,
-                                                       int* __restrict__ perm, double* __restrict__ tmp) {
+// Column norms of every working matrix, one warp per column (fixed reduction order).
+__global__ void __launch_bounds__(256) colnorm_kernel(const SvdProblem* __restrict__ probs,
+                                                      const double* __restrict__ W, double* __restrict__ norm) {
     const SvdProblem p = probs[blockIdx.x];
-    const double* Wp = W + p.w_off;
-    double* t = tmp + p.s_off;
-    for (int j = threadIdx.x; j < p.cols; j += blockDim.x) {
-        const double* col = Wp + (int64_t)j * p.rows;
-        double s = 0.0;
-        for (int k = 0; k < p.rows; ++k) s += col[k] * col[k];
-        t[j] = sqrt(s);
-    }
-    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const int j = blockIdx.y * 8 + (threadIdx.x >> 5);
+    if (j >= p.cols) return;
+    const double* col = W + p.w_off + (int64_t)j * p.rows;
+    double s = 0.0;
+    for (int k = lane; k < p.rows; k += 32) s += col[k] * col[k];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) norm[p.s_off + j] = sqrt(s);
+}
+
+// Descending order of the column norms (ties by column index): order[rank] = column;
+// with `sig`, also the sorted values.
+__global__ void __launch_bounds__(256) rank_kernel(const SvdProblem* __restrict__ probs,
+                                                   const double* __restrict__ norm, int* __restrict__ order,
+                                                   double* __restrict__ sig) {
+    const SvdProblem p = probs[blockIdx.x];
+    const double* t = norm + p.s_off;
     for (int j = threadIdx.x; j < p.cols; j += blockDim.x) {
         const double v = t[j];
         int rank = 0;
@@ -336,8 +347,8 @@ __global__ void __launch_bounds__(256) finalize_kernel(const SvdProblem* __restr
             const double u = t[o];
             rank += (u > v) || (u == v && o < j);
         }
-        sig[p.s_off + rank] = v;
-        perm[p.perm_off + rank] = j;
+        order[p.perm_off + rank] = j;
+        if (sig) sig[p.s_off + rank] = v;
     }
 }
 
@@ -448,6 +459,8 @@ int BatchedSvd::plan(const std::vector<int>& m, const std::vector<int>& n, cudaS
     DMRG_TRY(d_conv.alloc(std::max<size_t>(probs.size(), 1) * sizeof(unsigned long long)));
     DMRG_TRY(d_fro2.alloc(std::max<size_t>(probs.size(), 1) * sizeof(double)));
     DMRG_TRY(d_sign.alloc((size_t)std::max<int64_t>(soff, 1) * sizeof(double)));
+    DMRG_TRY(d_colmap.alloc((size_t)std::max<int64_t>(soff, 1) * sizeof(int)));
+    DMRG_TRY(d_norm.alloc((size_t)std::max<int64_t>(soff, 1) * sizeof(double)));
     DMRG_TRY(upload(d_probs, probs, st));
     DMRG_TRY(upload(d_tasks, tasks, st));
     DMRG_TRY(upload(d_gram_items, gram_items, st));
@@ -471,25 +484,34 @@ int BatchedSvd::run(cudaStream_t st, int* sweeps_out) {
     fro2_kernel<<<np, 256, 0, st>>>(d_probs.as<SvdProblem>(), d_w.as<double>(), d_fro2.as<double>());
     std::vector<unsigned long long> conv(np);
     static const bool debug = std::getenv("DMRG_SVD_DEBUG") != nullptr;  // per-sweep convergence to stderr
+    int max_cols = 0;
+    for (const SvdProblem& p : probs) max_cols = std::max(max_cols, p.cols);
+    const dim3 colgrid(np, (max_cols + 7) / 8);
     int sweep = 0, worst_at = 0;
     double worst_left = 0.0;
     for (; sweep < kMaxSweeps; ++sweep) {
         DMRG_CUDA_TRY(cudaMemsetAsync(d_conv.ptr, 0, np * sizeof(unsigned long long), st));
+        // the sweep visits columns in descending norm order: blocks hold columns of
+        // similar size, which keeps the many tiny singular values of a noise-expanded
+        // tensor from converging only linearly
+        colnorm_kernel<<<colgrid, 256, 0, st>>>(d_probs.as<SvdProblem>(), d_w.as<double>(), d_norm.as<double>());
+        rank_kernel<<<np, 256, 0, st>>>(d_probs.as<SvdProblem>(), d_norm.as<double>(), d_colmap.as<int>(), nullptr);
         for (int r = 0; r < max_rounds; ++r) {
             const int nt = round_first[r + 1] - round_first[r];
             const int ng = round_gram_first[r + 1] - round_gram_first[r];
             const int nr = round_rot_first[r + 1] - round_rot_first[r];
             if (nt == 0) continue;
             gram_kernel<<<ng, 128, 0, st>>>(d_probs.as<SvdProblem>(), d_tasks.as<SvdTask>(),
-                                            d_gram_items.as<SvdItem>() + round_gram_first[r], r, d_w.as<double>(),
-                                            d_gpart.as<double>());
+                                            d_gram_items.as<SvdItem>() + round_gram_first[r], r,
+                                            d_colmap.as<int>(), d_w.as<double>(), d_gpart.as<double>());
             solve_kernel<<<nt, kThreads, sizeof(SvdSmem), st>>>(
                 d_probs.as<SvdProblem>(), d_tasks.as<SvdTask>(), round_first[r], d_gpart.as<double>(),
-                d_fro2.as<double>(), d_rot.as<double>(), d_skip.as<int>(), d_conv.as<unsigned long long>());
+                d_fro2.as<double>(), d_rot.as<double>(), d_skip.as<int>(), d_conv.as<unsigned long long>(),
+                kInnerSweeps);
             rotate_kernel<<<nr, 128, kRotSmem, st>>>(d_probs.as<SvdProblem>(), d_tasks.as<SvdTask>(),
                                                      d_rot_items.as<SvdItem>() + round_rot_first[r], r,
                                                      round_first[r], d_rot.as<double>(), d_skip.as<int>(),
-                                                     d_w.as<double>(), d_q.as<double>());
+                                                     d_colmap.as<int>(), d_w.as<double>(), d_q.as<double>());
         }
         DMRG_CUDA_TRY(cudaGetLastError());
         DMRG_CUDA_TRY(cudaMemcpyAsync(conv.data(), d_conv.ptr, np * sizeof(unsigned long long),
@@ -526,11 +548,10 @@ int BatchedSvd::run(cudaStream_t st, int* sweeps_out) {
     if (sweep == kMaxSweeps)
         return set_error(DMRG_E_NUMERIC, "Jacobi SVD did not converge in %d sweeps (sector %d x %d: off-diagonal %.3e)",
                          kMaxSweeps, probs[worst_at].m, probs[worst_at].n, worst_left);
-    finalize_kernel<<<np, 256, 0, st>>>(d_probs.as<SvdProblem>(), d_w.as<double>(), d_s.as<double>(),
-                                        d_perm.as<int>(), d_s.as<double>() + (d_s.bytes / sizeof(double)) / 2);
-    int max_cols = 0;
-    for (const SvdProblem& p : probs) max_cols = std::max(max_cols, p.cols);
-    sign_kernel<<<dim3(np, (max_cols + 7) / 8), 256, 0, st>>>(d_probs.as<SvdProblem>(), d_w.as<double>(),
+    // singular values = final column norms, sorted
+    colnorm_kernel<<<colgrid, 256, 0, st>>>(d_probs.as<SvdProblem>(), d_w.as<double>(), d_norm.as<double>());
+    rank_kernel<<<np, 256, 0, st>>>(d_probs.as<SvdProblem>(), d_norm.as<double>(), d_perm.as<int>(), d_s.as<double>());
+    sign_kernel<<<colgrid, 256, 0, st>>>(d_probs.as<SvdProblem>(), d_w.as<double>(),
                                                                d_q.as<double>(), d_perm.as<int>(), d_sign.as<double>());
     DMRG_CUDA_TRY(cudaGetLastError());
     if (sweeps_out) *sweeps_out = sweep + 1;

@@ -3,7 +3,10 @@
 // Algorithm: one-sided (Hestenes) Jacobi with 32-column blocks.  Each sector
 // matrix A (m x n) is held as a column-major working matrix W with c <= r
 // columns: W = A when n <= m (right rotations accumulate V), W = A^T otherwise
-// (they accumulate U).  A sweep visits every pair of column blocks once in the
+// (they accumulate U).  A sweep first orders the columns by descending norm
+// (de Rijk's pivoting, applied block-wise: blocks then hold columns of similar
+// size, which halves the sweeps on noise-expanded tensors whose spectra are
+// mostly tiny), then visits every pair of column blocks once in the
 // round-robin order; in a round all pairs of all sectors are independent and
 // is split over CTAs by rows: (1) partial 64x64 Gram matrices of the pair over
 // row ranges (DMMA), (2) one CTA per pair sums them and runs a few cyclic
@@ -68,6 +71,7 @@ public:
     DeviceBuffer d_w, d_q, d_s, d_perm, d_probs, d_tasks, d_conv, d_fro2;
     DeviceBuffer d_sign;  // +-1 per sorted singular triplet (sign convention, set by run())
     DeviceBuffer d_gram_items, d_rot_items, d_gpart, d_rot, d_skip;
+    DeviceBuffer d_colmap, d_norm;  // per sweep: columns in descending norm order
     std::vector<SvdProblem> probs;
     std::vector<int> index;             // sector -> problem (-1 when empty)
     std::vector<int> round_first;       // task offset of each round
