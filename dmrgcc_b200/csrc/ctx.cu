@@ -1,5 +1,6 @@
 // Context, error reporting and memory entry points of the C ABI.
 #include <cstring>
+#include <mutex>
 
 #include "blocksparse.h"
 #include "common.cuh"
@@ -43,6 +44,56 @@ int build_site_desc(SiteDesc& s, int nl, int nr, const int* phys, const dmrg_blo
 
 }  // namespace dmrg
 
+namespace dmrg {
+namespace {
+struct ScopeState {
+    bool active = false;
+    cudaStream_t stream = nullptr;
+};
+thread_local ScopeState g_scope;
+std::mutex g_pool_mutex;
+cudaMemPool_t g_pools[64] = {};
+}  // namespace
+
+AllocScope::AllocScope(cudaStream_t st) : prev_active_(g_scope.active), prev_stream_(g_scope.stream) {
+    g_scope.active = true;
+    g_scope.stream = st;
+}
+AllocScope::~AllocScope() {
+    g_scope.active = prev_active_;
+    g_scope.stream = prev_stream_;
+}
+
+bool alloc_scope(cudaStream_t* st) {
+    if (st) *st = g_scope.stream;
+    return g_scope.active;
+}
+
+cudaError_t pool_malloc(void** ptr, size_t bytes, cudaStream_t st) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    cudaMemPool_t pool;
+    {
+        std::lock_guard<std::mutex> lock(g_pool_mutex);
+        if (!g_pools[dev]) {
+            cudaMemPoolProps props = {};
+            props.allocType = cudaMemAllocationTypePinned;
+            props.location.type = cudaMemLocationTypeDevice;
+            props.location.id = dev;
+            e = cudaMemPoolCreate(&g_pools[dev], &props);
+            if (e != cudaSuccess) return e;
+            uint64_t keep = UINT64_MAX;  // freed blocks stay in the pool
+            e = cudaMemPoolSetAttribute(g_pools[dev], cudaMemPoolAttrReleaseThreshold, &keep);
+            if (e != cudaSuccess) return e;
+        }
+        pool = g_pools[dev];
+    }
+    return cudaMallocFromPoolAsync(ptr, bytes, pool, st);
+}
+}  // namespace dmrg
+
 using namespace dmrg;
 
 extern "C" {
@@ -50,6 +101,7 @@ extern "C" {
 const char* dmrg_version(void) { return "dmrg_b200 0.1 (sm_100a)"; }
 
 const char* dmrg_last_error(void) { return g_last_error.c_str(); }
+
 
 int dmrg_ctx_create(int device, dmrg_ctx_t* out) {
     if (!out) return set_error(DMRG_E_ARG, "null output pointer");

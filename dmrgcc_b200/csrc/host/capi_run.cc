@@ -69,6 +69,7 @@ int dmrg_run_create(dmrg_ctx_t ctx, const char* input_path, const char* model, c
         }
         InputGroup input(input_path, "input", o.verbose != 0);
         ModelSpec m = make_model(input, model ? model : "real_spinless_bose_square");
+        AllocScope pool(ctx->stream);  // the run's tensors come from the stream-ordered pool
         auto* r = new dmrg_run_s();
         r->engine.reset(new Engine(ctx, std::move(m.space), std::move(m.ham), input, o));
         *out = r;
@@ -80,6 +81,7 @@ int dmrg_run_create(dmrg_ctx_t ctx, const char* input_path, const char* model, c
 
 int dmrg_run_execute(dmrg_run_t r) {
     if (!r) return set_error(DMRG_E_ARG, "null run");
+    AllocScope pool(r->engine->stream());
     return r->engine->Run();
 }
 

@@ -98,6 +98,7 @@ public:
     TensorLattice& lattice(int i) { return *lat_[i]; }
     TensorContraction& contraction(int i) { return *con_[i]; }
     int num_site() const { return n_; }
+    cudaStream_t stream() const { return st_; }
 
     // building blocks (public for the C ABI and tests)
     int Initialize();

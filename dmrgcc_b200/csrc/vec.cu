@@ -134,7 +134,7 @@ int ReduceScratch::alloc(int blocks, int max_vectors) {
     DMRG_TRY(partial.alloc((size_t)blocks * (max_vectors > 0 ? max_vectors : 1) * sizeof(double)));
     if (!ticket.ptr) {
         DMRG_TRY(ticket.alloc(64 * sizeof(unsigned)));
-        DMRG_CUDA_TRY(cudaMemset(ticket.ptr, 0, 64 * sizeof(unsigned)));
+        DMRG_TRY(ticket.zero());
     }
     return DMRG_OK;
 }
