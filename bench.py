@@ -10,6 +10,9 @@ synthetic values.  A step = one matvec.
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
                     [--precision fp64]
 
+The line also carries `sweep`: the wall time of one whole DMRG run of the same
+cylinder input (8 sweeps, D up to 1024) through dmrg_run_execute (N=1 only).
+
 Multi-GPU: replicas only (each rank runs its own matvec; no collective on the
 data path); value = all ranks' FLOPs / max-over-ranks time.
 """
@@ -29,6 +32,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 STRUCT = os.path.join(ROOT, "tests", "golden", "heff_struct_cyl8x4_D1024.nac")
+CYL_INPUT = os.path.join(ROOT, "dmrgcc_b200", "inputs", "cylinder8x4_spinless.in")
 METRIC = "sweep time & H·ψ TFLOP/s, split-prec vs FP64 on 1 B200 at |ΔE/site|≤1e-10"
 WORKLOAD = "H_eff*psi, 8x4 Bose-Hubbard cylinder (d=5, N=16, U=8), D=1024, site 16"
 PROBE = os.path.join(ROOT, "oracle", "_ref", "probe_heff")
@@ -122,6 +126,30 @@ def run_reference(args) -> None:
         "e2e": {"value": tflops, "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
+
+
+def sweep_time(ctx) -> dict:
+    """One whole run of the 8x4 cylinder input (D ramp 128 -> 1024, 8 sweeps =
+    16 half-sweeps, niter 100, noise on for the first 12 half-sweeps), wall
+    clock on the host around dmrg_run_execute (device work + host bookkeeping)."""
+    from dmrgcc_b200 import capi
+
+    run = capi.Run(ctx, CYL_INPUT, verbose=0)
+    t0 = time.perf_counter()
+    run.execute()
+    total = time.perf_counter() - t0
+    e, s = run.half_sweeps()
+    ph, sw = run.phases()
+    return {
+        "workload": "whole DMRG run, 8x4 Bose-Hubbard cylinder (d=5, N=16, U=8), D 128->1024, 8 sweeps",
+        "precision": "fp64", "total_s": total,
+        "per_sweep_s": [float(s[2 * i] + s[2 * i + 1]) for i in range(len(s) // 2)],
+        "phase_s": {k: float(v) for k, v in zip(capi.Run.PHASES, ph.sum(axis=0))},
+        "svd_sweeps": int(sw.sum()), "final_energy": float(e[-1]),
+        "reference_cpu": {"total_s": 557.0, "final_energy": -45.653161401383, "cores": 8,
+                          "note": "the reference built from its sources with OpenBLAS, measured in the build "
+                                  "container (not on the GPU box); 8 threads"},
+    }
 
 
 def run_b200(args) -> None:
@@ -245,6 +273,8 @@ def run_b200(args) -> None:
             },
             "clocks": clk.summary(),
         }
+        if world == 1 and not args.no_sweep:
+            line["sweep"] = sweep_time(ctx)
         cpu = cpu_reference(args.cpu_reps, 1, os.cpu_count() or 1) if not args.no_cpu else {"unavailable": "skipped"}
         if "unavailable" not in cpu:
             line["cpu_baseline"] = {"value": cpu["gflop"] / cpu["mean_s"] * 1e-3, "unit": "TFLOP/s",
@@ -269,6 +299,7 @@ def main() -> int:
     ap.add_argument("--precision", choices=["fp64", "bf16x3"], default="fp64")
     ap.add_argument("--cpu-reps", type=int, default=30)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-sweep", action="store_true", help="skip the whole-run sweep-time measurement")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
