@@ -179,7 +179,7 @@ def run_b200(args) -> None:
     assert ctx.stream == stream.cuda_stream != 0
 
     step = SiteStep.from_nac(STRUCT)
-    prec = {"fp64": capi.DMRG_PREC_FP64, "bf16x3": capi.DMRG_PREC_BF16X3}[args.precision]
+    prec = {"fp64": capi.DMRG_PREC_FP64, "tf32x3": capi.DMRG_PREC_TF32X3}[args.precision]
     heff = capi.Heff(ctx, step.site, step.L, step.R, precision=prec)
     psi, L, R = step.synthetic_device(ctx, seed=SEED + rank)
     heff.set_env(L, R)
@@ -254,7 +254,7 @@ def run_b200(args) -> None:
         line = {
             "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "bf16x3->f32",
+            "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "tf32x3 (f32 accumulate, f64 storage)",
             "data": "synthetic (seeded splitmix64 values on the reference's own D=1024 block structure)",
             "config": {"workload": WORKLOAD, "precision": args.precision, "psi_dim": step.psi_dim,
                        "gflop_per_step_algorithmic": alg_flops * 1e-9, "gflop_per_step_executed": exec_flops * 1e-9,
@@ -296,7 +296,7 @@ def main() -> int:
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    ap.add_argument("--precision", choices=["fp64", "bf16x3"], default="fp64")
+    ap.add_argument("--precision", choices=["fp64", "tf32x3"], default="fp64")
     ap.add_argument("--cpu-reps", type=int, default=30)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-sweep", action="store_true", help="skip the whole-run sweep-time measurement")

@@ -17,6 +17,7 @@ LIB_PATH = os.path.join(_PKG, "lib", "libdmrg_b200.so")
 
 DMRG_PREC_FP64 = 0
 DMRG_PREC_BF16X3 = 1
+DMRG_PREC_TF32X3 = 2
 
 _lib: C.CDLL | None = None
 

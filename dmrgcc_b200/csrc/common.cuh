@@ -49,6 +49,10 @@ private:
     bool prev_active_;
     cudaStream_t prev_stream_;
 };
+// Reads and clears the context's device status word (waits for the stream);
+// returns DMRG_OK or the code a kernel recorded (for example a bounded wait that
+// timed out).
+int take_device_status(dmrg_ctx_t ctx);
 // The innermost scope's stream, or false when none is active on this thread.
 bool alloc_scope(cudaStream_t* st);
 // cudaMallocFromPoolAsync on the current device's pool (created on first use,

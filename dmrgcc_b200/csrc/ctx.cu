@@ -64,6 +64,15 @@ AllocScope::~AllocScope() {
     g_scope.stream = prev_stream_;
 }
 
+int take_device_status(dmrg_ctx_t ctx) {
+    int code = 0;
+    DMRG_CUDA_TRY(cudaMemcpyAsync(&code, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    DMRG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    if (code == 0) return DMRG_OK;
+    DMRG_CUDA_TRY(cudaMemsetAsync(ctx->d_status, 0, sizeof(int), ctx->stream));
+    return set_error(code, "a device routine gave up waiting (status %d); its output is incomplete", code);
+}
+
 bool alloc_scope(cudaStream_t* st) {
     if (st) *st = g_scope.stream;
     return g_scope.active;
@@ -151,7 +160,7 @@ void* dmrg_ctx_stream(dmrg_ctx_t ctx) { return ctx ? (void*)ctx->stream : nullpt
 int dmrg_ctx_sync(dmrg_ctx_t ctx) {
     if (!ctx) return set_error(DMRG_E_ARG, "null context");
     DMRG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-    return DMRG_OK;
+    return dmrg::take_device_status(ctx);
 }
 
 int dmrg_malloc(dmrg_ctx_t ctx, size_t bytes, void** dev) {

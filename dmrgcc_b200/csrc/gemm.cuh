@@ -65,9 +65,19 @@ struct GemmSchedule {
     std::vector<GemmGroup> exec_groups;
     std::vector<GemmSplit> splits;
     int64_t aux_size = 0;
+    int tile_m = 0, tile_n = 0, tile_k = 0;  // set by finalize()
     // device copies
     DeviceBuffer d_terms, d_groups, d_tiles, d_splits, aux;
 
+    // Copies the groups and terms of another schedule (not its execution form).
+    void copy_plan(const GemmSchedule& o) {
+        reset();
+        terms = o.terms;
+        groups = o.groups;
+        ta = o.ta;
+        tb = o.tb;
+        flops = o.flops;
+    }
     void reset() {
         terms.clear();
         groups.clear();
@@ -103,5 +113,11 @@ struct GemmSchedule {
 // C (+)= sum of terms for every tile of `s`.  A, B, C are the base pointers.
 int launch_gemm_f64(const GemmSchedule& s, const double* A, const double* B, double* C,
                     bool accumulate, cudaStream_t stream);
+
+// The same on the tcgen05 tensor cores with TF32 hi/lo splits (gemm_tf32x3.cu);
+// `s` must be finalized with 128 x 64 x 32 tiles.  A wait that times out sets
+// *status = DMRG_E_NUMERIC (device word) instead of hanging.
+int launch_gemm_tf32x3(const GemmSchedule& s, const double* A, const double* B, double* C, bool accumulate,
+                       int* status, cudaStream_t stream);
 
 }  // namespace dmrg

@@ -202,6 +202,9 @@ int GemmSchedule::finalize(int tile_m, int tile_n, int tile_k, cudaStream_t stre
     exec_groups.clear();
     splits.clear();
     aux_size = 0;
+    this->tile_m = tile_m;
+    this->tile_n = tile_n;
+    this->tile_k = tile_k;
     auto ksteps_of = [&](int t) { return (terms[t].k + tile_k - 1) / tile_k; };
     auto ntiles_of = [&](const GemmGroup& g) {
         return (int64_t)((g.m + tile_m - 1) / tile_m) * ((g.n + tile_n - 1) / tile_n);

@@ -128,13 +128,19 @@ int build_heff(dmrg_heff_s& h) {
     cudaStream_t st = h.ctx->stream;
     DMRG_TRY(h.sa.finalize(64, 64, 16, st));
     DMRG_TRY(h.sb.finalize(64, 64, 16, st, h.ctx->num_sms));
+    if (h.precision == DMRG_PREC_TF32X3) {
+        h.sa3.copy_plan(h.sa);
+        h.sb3.copy_plan(h.sb);
+        DMRG_TRY(h.sa3.finalize(128, 64, 32, st));
+        DMRG_TRY(h.sb3.finalize(128, 64, 32, st, h.ctx->num_sms));
+    }
     DMRG_TRY(h.T.alloc((size_t)std::max<int64_t>(h.t_size, 1) * sizeof(double)));
     return DMRG_OK;
 }
 
 }  // namespace
 
-int dmrg::heff_apply_internal(dmrg_heff_s& h, const double* psi, double* out, bool accumulate) {
+int dmrg::heff_apply_fp64(dmrg_heff_s& h, const double* psi, double* out, bool accumulate) {
     if ((!h.L_dev && h.L.size) || (!h.R_dev && h.R.size))
         return set_error(DMRG_E_STATE, "dmrg_heff_set_env was not called");
     cudaStream_t st = h.ctx->stream;
@@ -145,14 +151,26 @@ int dmrg::heff_apply_internal(dmrg_heff_s& h, const double* psi, double* out, bo
     return DMRG_OK;
 }
 
+int dmrg::heff_apply_internal(dmrg_heff_s& h, const double* psi, double* out, bool accumulate) {
+    if (h.precision != DMRG_PREC_TF32X3) return heff_apply_fp64(h, psi, out, accumulate);
+    if ((!h.L_dev && h.L.size) || (!h.R_dev && h.R.size))
+        return set_error(DMRG_E_STATE, "dmrg_heff_set_env was not called");
+    cudaStream_t st = h.ctx->stream;
+    if (!accumulate && h.site.ket.size)
+        DMRG_CUDA_TRY(cudaMemsetAsync(out, 0, (size_t)h.site.ket.size * sizeof(double), st));
+    DMRG_TRY(launch_gemm_tf32x3(h.sa3, psi, h.R_dev, h.T.as<double>(), false, h.ctx->d_status, st));
+    DMRG_TRY(launch_gemm_tf32x3(h.sb3, h.L_dev, h.T.as<double>(), out, true, h.ctx->d_status, st));
+    return DMRG_OK;
+}
+
 extern "C" {
 
 int dmrg_heff_create(dmrg_ctx_t ctx, int nl, int nr, const int* phys, const dmrg_blocks_t* ket, int d, int lb,
                      int rb, const double* W, const dmrg_blocks_t* L, const dmrg_blocks_t* R, int precision,
                      dmrg_heff_t* out) {
     if (!ctx || !out || !L || !R) return set_error(DMRG_E_ARG, "null argument");
-    if (precision != DMRG_PREC_FP64)
-        return set_error(DMRG_E_ARG, "unknown precision %d", precision);
+    if (precision != DMRG_PREC_FP64 && precision != DMRG_PREC_TF32X3)
+        return set_error(DMRG_E_ARG, "unsupported precision %d (DMRG_PREC_FP64 or DMRG_PREC_TF32X3)", precision);
     *out = nullptr;
     DMRG_CUDA_TRY(cudaSetDevice(ctx->device));
     auto* h = new dmrg_heff_s();
@@ -210,10 +228,14 @@ int dmrg_heff_profile(dmrg_heff_t h, const double* psi, double* out, double* ms_
     cudaStream_t st = h->ctx->stream;
     cudaEvent_t ev[3];
     for (auto& e : ev) DMRG_CUDA_TRY(cudaEventCreate(&e));
+    const bool split = h->precision == DMRG_PREC_TF32X3;
     DMRG_CUDA_TRY(cudaEventRecord(ev[0], st));
-    int rc = launch_gemm_f64(h->sa, psi, h->R_dev, h->T.as<double>(), false, st);
+    int rc = split ? launch_gemm_tf32x3(h->sa3, psi, h->R_dev, h->T.as<double>(), false, h->ctx->d_status, st)
+                   : launch_gemm_f64(h->sa, psi, h->R_dev, h->T.as<double>(), false, st);
     cudaEventRecord(ev[1], st);
-    if (rc == DMRG_OK) rc = launch_gemm_f64(h->sb, h->L_dev, h->T.as<double>(), out, true, st);
+    if (rc == DMRG_OK)
+        rc = split ? launch_gemm_tf32x3(h->sb3, h->L_dev, h->T.as<double>(), out, true, h->ctx->d_status, st)
+                   : launch_gemm_f64(h->sb, h->L_dev, h->T.as<double>(), out, true, st);
     cudaEventRecord(ev[2], st);
     cudaError_t err = cudaEventSynchronize(ev[2]);
     float a = 0, b = 0;
@@ -240,6 +262,7 @@ int dmrg_heff_apply_host(dmrg_heff_t h, const double* psi_host, double* out_host
     DMRG_TRY(dmrg_heff_apply(h, h->io_psi.as<double>(), h->io_out.as<double>(), accumulate));
     if (bytes) DMRG_CUDA_TRY(cudaMemcpyAsync(out_host, h->io_out.ptr, bytes, cudaMemcpyDeviceToHost, st));
     DMRG_CUDA_TRY(cudaStreamSynchronize(st));
+    if (h->precision == DMRG_PREC_TF32X3) return take_device_status(h->ctx);  // bounded tensor-core waits
     return DMRG_OK;
 }
 

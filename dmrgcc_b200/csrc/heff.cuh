@@ -14,7 +14,8 @@ struct dmrg_heff_s {
     int precision = DMRG_PREC_FP64;
     dmrg::SiteDesc site;
     dmrg::EnvDesc L, R;
-    dmrg::GemmSchedule sa, sb;  // A: psi x R -> T ; B: L x T -> out
+    dmrg::GemmSchedule sa, sb;    // A: psi x R -> T ; B: L x T -> out (FP64 tiles)
+    dmrg::GemmSchedule sa3, sb3;  // the same products in TF32X3 tiles (DMRG_PREC_TF32X3 only)
     dmrg::DeviceBuffer T;
     int64_t t_size = 0;
     const double* L_dev = nullptr;
@@ -26,6 +27,8 @@ struct dmrg_heff_s {
 };
 
 namespace dmrg {
-// out (+)= H_eff psi on the context stream.
+// out (+)= H_eff psi on the context stream, in the operator's precision.
 int heff_apply_internal(dmrg_heff_s& h, const double* psi, double* out, bool accumulate);
+// out (+)= H_eff psi in FP64 whatever the operator's precision.
+int heff_apply_fp64(dmrg_heff_s& h, const double* psi, double* out, bool accumulate);
 }  // namespace dmrg

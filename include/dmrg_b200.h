@@ -37,10 +37,15 @@ extern "C" {
 #define DMRG_E_NUMERIC (-4)  /* an iterative device routine hit its iteration cap */
 #define DMRG_E_STATE (-5)    /* call made in the wrong state */
 
-/* Arithmetic of the block GEMMs.  FP64: plain double.  SPLIT_BF16X3:
- * tensor-core products of bf16 hi/lo splits with FP32 accumulation. */
+/* Arithmetic of the block GEMMs.  FP64: plain double (FP64 tensor path).
+ * TF32X3: 5th-generation tensor cores (tcgen05): every FP64 operand is rounded
+ * to FP32 and split into TF32 hi + lo parts, each product is taken as
+ * hi*hi + hi*lo + lo*hi with FP32 accumulation in tensor memory, and results are
+ * stored as FP64 (relative error ~1e-6 of a block sum).  BF16X3 is reserved and
+ * rejected. */
 #define DMRG_PREC_FP64 0
 #define DMRG_PREC_BF16X3 1
+#define DMRG_PREC_TF32X3 2
 
 typedef struct dmrg_ctx_s* dmrg_ctx_t;
 typedef struct dmrg_heff_s* dmrg_heff_t;
@@ -109,9 +114,8 @@ int dmrg_heff_sizes(dmrg_heff_t h, int64_t* psi_dim, int64_t* left_env_size,
 /* FLOPs of one application: `algorithmic` counts the reference loop's GEMMs
  * (real_tensor_contraction.cc:1243-1285), `executed` what the schedule runs. */
 int dmrg_heff_flops(dmrg_heff_t h, double* algorithmic, double* executed);
-/* Points the operator at device-resident environments (packed as above).  For
- * DMRG_PREC_BF16X3 this also splits them into bf16 planes (kept until the next
- * call).  The pointers must stay valid while the operator is used. */
+/* Points the operator at device-resident environments (packed as above).  The
+ * pointers must stay valid while the operator is used. */
 int dmrg_heff_set_env(dmrg_heff_t h, const double* L_dev, const double* R_dev);
 /* out_dev (+)= H_eff * psi_dev on the context stream (accumulate != 0 adds into
  * out_dev like the reference's `state +=`; 0 overwrites).  Asynchronous. */
