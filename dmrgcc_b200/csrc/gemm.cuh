@@ -69,15 +69,6 @@ struct GemmSchedule {
     // device copies
     DeviceBuffer d_terms, d_groups, d_tiles, d_splits, aux;
 
-    // Copies the groups and terms of another schedule (not its execution form).
-    void copy_plan(const GemmSchedule& o) {
-        reset();
-        terms = o.terms;
-        groups = o.groups;
-        ta = o.ta;
-        tb = o.tb;
-        flops = o.flops;
-    }
     void reset() {
         terms.clear();
         groups.clear();
@@ -114,10 +105,90 @@ struct GemmSchedule {
 int launch_gemm_f64(const GemmSchedule& s, const double* A, const double* B, double* C,
                     bool accumulate, cudaStream_t stream);
 
-// The same on the tcgen05 tensor cores with TF32 hi/lo splits (gemm_tf32x3.cu);
-// `s` must be finalized with 128 x 64 x 32 tiles.  A wait that times out sets
-// *status = DMRG_E_NUMERIC (device word) instead of hanging.
-int launch_gemm_tf32x3(const GemmSchedule& s, const double* A, const double* B, double* C, bool accumulate,
-                       int* status, cudaStream_t stream);
+// ---------------------------------------------------------------------------
+// Split-precision (TF32X3) path on the tcgen05 tensor cores (gemm_tf32x3.cu).
+//
+// Operands are packed once into "images": for an operand block X (rows x k,
+// K-major), image (panel p, slice s) holds rows [p*R, p*R+R) x k [32 s, 32 s+32)
+// as a TF32 hi plane followed by a TF32 lo plane (x ~ hi + lo, x rounded to FP32
+// first), each in the tcgen05 canonical K-major no-swizzle layout: byte offset of
+// (row r, k) = (k/4)*16R + (r/8)*128 + (r%8)*16 + (k%4)*4.  Zero outside X.
+// R = 128 for the A role (output rows), 64 for the B role (output columns).
+// A GEMM stage then is two contiguous bulk copies (32 KB + 16 KB).
+constexpr int kPackK = 32;
+constexpr int kPackRowsA = 128, kPackRowsB = 64;
+constexpr int kImageA = 2 * kPackRowsA * kPackK * 4;  // bytes: hi + lo
+constexpr int kImageB = 2 * kPackRowsB * kPackK * 4;
+
+struct PackJob {
+    int64_t src_off;  // doubles
+    int64_t img_off;  // bytes, into the image buffer
+    int rows, k, ld;  // logical X: rows x k; X(r, c) = src[src_off + (trans ? c*ld + r : r*ld + c)]
+    int trans;
+    int prow;         // rows per panel (kPackRowsA or kPackRowsB)
+    int slices;       // ceil(k / 32)
+};
+struct PackImage {
+    int job, panel, slice, pad_;
+};
+struct PackSchedule {
+    std::vector<PackJob> jobs;
+    std::vector<PackImage> images;
+    int64_t bytes = 0;
+    DeviceBuffer d_jobs, d_images;
+    // Appends the images of one operand block; returns its image offset (bytes).
+    int64_t add(int64_t src_off, int rows, int k, int ld, bool trans, int prow);
+    int finalize(cudaStream_t stream);
+};
+// dst (images) <- split-precision images of the jobs' blocks of src.
+int launch_pack(const PackSchedule& p, const double* src, unsigned char* dst, cudaStream_t stream);
+
+struct PackedTerm {
+    int64_t a_img, b_img;  // image offsets (bytes) of the A operand (A role) and the B operand (B role)
+    int slices;            // ceil(k / 32), the same for both
+    int pad_;
+    double w;              // weight of this product
+};
+struct PackedGroup {
+    int t0, t1;            // terms
+    int m, n;              // output block
+    int64_t c_off;         // output mode 0: FP64 block at C + c_off (ldc), or its split-K chunk in aux
+    int ldc;
+    int cbuf;              // 1: split-K chunk, written to aux
+    int64_t t_img;         // output mode 1: the output written as B-role images (rows = columns n,
+    int t_slices;          // k = rows m) for a following packed GEMM; t_slices = ceil(m / 32)
+    int pad_;
+};
+struct PackedTile {
+    int group, pm, pn, cost;
+};
+struct PackedSchedule {
+    std::vector<PackedTerm> terms;
+    std::vector<PackedGroup> groups;
+    int out_mode = 0;  // 0: FP64 output blocks, 1: B-role images
+    std::vector<PackedGroup> exec_groups;
+    std::vector<GemmSplit> splits;
+    std::vector<PackedTile> tiles;
+    int64_t aux_size = 0;
+    DeviceBuffer d_terms, d_groups, d_tiles, d_splits, aux;
+    void reset() {
+        terms.clear();
+        groups.clear();
+        exec_groups.clear();
+        splits.clear();
+        tiles.clear();
+        aux_size = 0;
+    }
+    // Verifies every image read and every output write against the buffer sizes
+    // (bytes for images, doubles for c_size); DMRG_E_ARG, no launch, otherwise.
+    int check_bounds(int64_t a_bytes, int64_t b_bytes, int64_t c_size, int64_t t_bytes) const;
+    // Builds tiles (128 x 64 per tile, heaviest first), splits long mode-0 groups
+    // (num_sms > 0), uploads.
+    int finalize(cudaStream_t stream, int num_sms = 0);
+};
+// C (+)= the products of every group (mode 0), or t_out <- images of them (mode 1).
+// A wait that gives up sets *status = DMRG_E_NUMERIC (device word).
+int launch_gemm_tf32x3(const PackedSchedule& s, const unsigned char* a_imgs, const unsigned char* b_imgs,
+                       double* C, unsigned char* t_out, bool accumulate, int* status, cudaStream_t stream);
 
 }  // namespace dmrg

@@ -1,24 +1,31 @@
 // Split-precision grouped multi-term block GEMM on the 5th-generation tensor
-// cores (tcgen05, accumulators in tensor memory): the same schedules as
-// gemm_f64.cu, with every FP64 operand rounded to FP32 and split on the fly into
-// two TF32 parts, x ~ hi + lo, and each product taken as hi*hi + hi*lo + lo*hi
-// (the lo*lo term, ~2^-22 relative, is dropped), accumulated in FP32 in TMEM and
-// stored as FP64.  Relative error of a block sum ~1e-6.
+// cores (tcgen05, accumulators in tensor memory), on packed operand images.
 //
-// CTA: 128 threads, output tile 128 x 64 (tcgen05.mma M=128, N=64, K=8 per
-// instruction), k-step 32 per stage, two stages.  All threads load the FP64
-// operands (four consecutive K values per thread), scale A by the term's
-// weight, split, and store hi and lo planes in shared memory in the canonical
-// K-major no-swizzle layout: core matrices of 8 rows x 16 bytes, 8-row groups
-// 128 bytes apart (SBO), 16-byte K chunks LBO apart; LBO carries a 16-byte pad
-// so that the 16-byte stores of consecutive threads hit distinct banks.  One
-// thread issues the stage's 12 MMAs (4 k-substeps x 3 products) and commits
-// them to the stage's mbarrier; a stage is refilled only after that barrier
-// completes.  Epilogue: warp w reads TMEM lanes 32w..32w+31 (= tile rows) with
-// tcgen05.ld and writes or adds the FP64 results.
-// Every wait is bounded: on a timeout the kernel records DMRG_E_NUMERIC in the
-// status word, waits (bounded again) for its MMAs in flight, frees its TMEM and
-// returns; the decision to stop is block-uniform.
+// Arithmetic: every FP64 operand is rounded to FP32 and split into TF32 parts,
+// x ~ hi + lo; each product is taken as hi*hi + hi*lo + lo*hi (the lo*lo term,
+// ~2^-22 relative, is dropped) by three kind::tf32 MMAs into an FP32 accumulator
+// in tensor memory.  Each term's accumulator is read out and added, scaled by
+// the term's weight, into FP64 registers, so the terms of a block sum
+// accumulate in FP64.  Relative error of a block sum ~1e-6.
+//
+// Packing (launch_pack): one CTA per image writes the hi/lo planes of one
+// (panel, 32-wide k slice) of an operand block in the tcgen05 canonical K-major
+// no-swizzle layout (see gemm.cuh).  A GEMM stage is then two contiguous bulk
+// copies (cp.async.bulk, no multicast) of 32 KB (A) and 16 KB (B).
+//
+// GEMM (one CTA per 128 x 64 output tile, 192 threads, warp-specialised):
+//   warp 0 lane 0   producer: per stage waits the stage's "empty" barrier, arms
+//                   the "full" barrier with the byte count, issues the copies;
+//   warp 1 lane 0   MMA issuer: per stage waits "full", issues 4 k-substeps x 3
+//                   MMAs into the term's accumulator (two 64-column accumulators
+//                   alternate between terms), commits to "empty"; after a term's
+//                   last stage commits to the accumulator's "full" barrier;
+//   warps 2..5      epilogue: per term wait, tcgen05.ld the 128 x 64 FP32 tile
+//                   (warp w: TMEM lanes 32(w%4)..), add w_t * value into FP64
+//                   registers, release the accumulator; finally store FP64 rows
+//                   (or write the result as B-role images for the next GEMM).
+// Every wait is bounded: on a timeout a role records DMRG_E_NUMERIC in the
+// status word and stops; the CTA frees its tensor memory and returns.
 #include <algorithm>
 #include <cstdint>
 
@@ -27,20 +34,20 @@
 namespace dmrg {
 namespace {
 
-constexpr int TM = 128, TN = 64, TK = 32, NT = 128;
-constexpr int CHUNKS = TK / 4;               // 16-byte K chunks per stage (4 tf32 each)
-constexpr int LBO_A = TM * 16 + 16;          // bytes between K chunks of A (padded)
-constexpr int LBO_B = TN * 16 + 16;
-constexpr int SBO = 128;                     // bytes between 8-row core-matrix groups
-constexpr int PLANE_A = CHUNKS * LBO_A;      // one of hi / lo
-constexpr int PLANE_B = CHUNKS * LBO_B;
-constexpr int STAGE_BYTES = 2 * PLANE_A + 2 * PLANE_B;
-constexpr int SMEM_BYTES = 2 * STAGE_BYTES + 64;
-constexpr uint32_t TMEM_COLS = 64;
-constexpr long long kWaitLimit = 4000000;    // try_wait polls before a wait gives up
+constexpr int TM = kPackRowsA, TN = kPackRowsB, TK = kPackK;
+constexpr int NSTAGE = 4;
+constexpr int STAGE_BYTES = kImageA + kImageB;               // 48 KB
+constexpr int LBO_A = TM * 16, LBO_B = TN * 16;              // bytes between 16-byte k chunks
+constexpr int SBO = 128;                                     // bytes between 8-row groups
+constexpr int PLANE_A = TM * TK * 4, PLANE_B = TN * TK * 4;  // hi plane; lo follows
+constexpr int NT = 192;
+constexpr int BAR_OFF = NSTAGE * STAGE_BYTES;
+constexpr int SMEM_BYTES = BAR_OFF + 256;
+constexpr uint32_t TMEM_COLS = 128;                          // two 64-column accumulators
+constexpr long long kWaitLimit = 4000000;                    // try_wait polls before a wait gives up
 
-static_assert(LBO_A % 16 == 0 && LBO_B % 16 == 0 && STAGE_BYTES % 16 == 0, "16-byte descriptor units");
-static_assert((LBO_A >> 4) < (1 << 14) && (LBO_B >> 4) < (1 << 14), "LBO fits the descriptor field");
+static_assert(SMEM_BYTES <= 227 * 1024, "shared memory per CTA");
+static_assert((LBO_A >> 4) < (1 << 14), "LBO fits the descriptor field");
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -70,6 +77,22 @@ __device__ __forceinline__ void mma_commit(uint64_t* bar) {
                  : "memory");
 }
 
+__device__ __forceinline__ void mbar_init(uint64_t* bar, int count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}\n" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}\n" ::"r"(
+                     smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t phase) {
     uint32_t ok;
     asm volatile(
@@ -81,11 +104,20 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t phase) {
     return ok != 0;
 }
 
-// bounded wait for the completion of phase `phase`; false on timeout
+// bounded wait for the completion of the phase of parity `phase`; false on timeout
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase) {
     for (long long i = 0; i < kWaitLimit; ++i)
         if (mbar_try_wait(bar, phase)) return true;
     return false;
+}
+
+// Bulk copy global -> shared (16-byte aligned, size multiple of 16), completing
+// as transaction bytes on `bar`.  No multicast.
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
 }
 
 __device__ __forceinline__ uint32_t tf32_bits(float x) {
@@ -112,165 +144,223 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
         : "r"(taddr));
 }
 
-// One stage: A (TM x TK, scaled by the term weight) and B (TN x TK), K-major planes.
-template <bool TA, bool TB>
-__device__ __forceinline__ void fill_stage(unsigned char* st, const double* __restrict__ A,
-                                           const double* __restrict__ B, const GemmTerm& t, int k0, int m0, int n0,
-                                           int m, int n, int tid) {
-    unsigned char* a_hi = st;
-    unsigned char* a_lo = st + PLANE_A;
-    unsigned char* b_hi = st + 2 * PLANE_A;
-    unsigned char* b_lo = b_hi + PLANE_B;
-    const double scale = t.scale;
-#pragma unroll 2
-    for (int idx = tid; idx < TM * CHUNKS; idx += NT) {
-        const int r = TA ? (idx % TM) : (idx / CHUNKS);
-        const int c = TA ? (idx / TM) : (idx % CHUNKS);
-        uint32_t h[4], l[4];
-#pragma unroll
-        for (int e = 0; e < 4; ++e) {
-            const int k = k0 + 4 * c + e;
-            double v = 0.0;
-            if (m0 + r < m && k < t.k)
-                v = TA ? A[t.a_off + (int64_t)k * t.lda + (m0 + r)] : A[t.a_off + (int64_t)(m0 + r) * t.lda + k];
-            split(v * scale, h[e], l[e]);
-        }
-        const int off = c * LBO_A + (r >> 3) * SBO + (r & 7) * 16;
-        *reinterpret_cast<uint4*>(a_hi + off) = make_uint4(h[0], h[1], h[2], h[3]);
-        *reinterpret_cast<uint4*>(a_lo + off) = make_uint4(l[0], l[1], l[2], l[3]);
-    }
-#pragma unroll 2
-    for (int idx = tid; idx < TN * CHUNKS; idx += NT) {
-        const int r = TB ? (idx / CHUNKS) : (idx % TN);
-        const int c = TB ? (idx % CHUNKS) : (idx / TN);
-        uint32_t h[4], l[4];
-#pragma unroll
-        for (int e = 0; e < 4; ++e) {
-            const int k = k0 + 4 * c + e;
-            double v = 0.0;
-            if (n0 + r < n && k < t.k)
-                v = TB ? B[t.b_off + (int64_t)(n0 + r) * t.ldb + k] : B[t.b_off + (int64_t)k * t.ldb + (n0 + r)];
-            split(v, h[e], l[e]);
-        }
-        const int off = c * LBO_B + (r >> 3) * SBO + (r & 7) * 16;
-        *reinterpret_cast<uint4*>(b_hi + off) = make_uint4(h[0], h[1], h[2], h[3]);
-        *reinterpret_cast<uint4*>(b_lo + off) = make_uint4(l[0], l[1], l[2], l[3]);
+// byte offset of (row r, k) inside one plane with `rows` rows per panel
+__device__ __forceinline__ int plane_off(int r, int k, int rows) {
+    return (k >> 2) * (rows * 16) + (r >> 3) * 128 + (r & 7) * 16 + (k & 3) * 4;
+}
+
+// ---- packing: one CTA (128 threads) per image ----------------------------------
+__global__ void __launch_bounds__(128) pack_kernel(const PackJob* __restrict__ jobs, const PackImage* __restrict__ imgs,
+                                                   const double* __restrict__ src, unsigned char* __restrict__ dst) {
+    const PackImage im = imgs[blockIdx.x];
+    const PackJob j = jobs[im.job];
+    const int img_bytes = 2 * j.prow * TK * 4;
+    unsigned char* out = dst + j.img_off + ((int64_t)im.panel * j.slices + im.slice) * img_bytes;
+    uint32_t* hi = reinterpret_cast<uint32_t*>(out);
+    uint32_t* lo = reinterpret_cast<uint32_t*>(out + img_bytes / 2);
+    const int r0 = im.panel * j.prow, k0 = im.slice * TK;
+    const double* s = src + j.src_off;
+    for (int idx = threadIdx.x; idx < j.prow * TK; idx += blockDim.x) {
+        // consecutive threads: consecutive k for row-major X, consecutive rows for transposed X
+        const int r = j.trans ? idx % j.prow : idx / TK;
+        const int k = j.trans ? idx / j.prow : idx % TK;
+        double v = 0.0;
+        if (r0 + r < j.rows && k0 + k < j.k)
+            v = j.trans ? s[(int64_t)(k0 + k) * j.ld + (r0 + r)] : s[(int64_t)(r0 + r) * j.ld + (k0 + k)];
+        uint32_t h, l;
+        split(v, h, l);
+        const int off = plane_off(r, k, j.prow) >> 2;
+        hi[off] = h;
+        lo[off] = l;
     }
 }
 
-template <bool TA, bool TB>
-__global__ void __launch_bounds__(NT) gemm_tf32x3_kernel(const double* __restrict__ A, const double* __restrict__ B,
-                                                         double* __restrict__ C, double* __restrict__ Caux,
-                                                         const GemmTerm* __restrict__ terms,
-                                                         const GemmGroup* __restrict__ groups,
-                                                         const GemmTile* __restrict__ tiles, int accumulate,
-                                                         int* __restrict__ status) {
-    extern __shared__ __align__(1024) unsigned char smem[];
-    unsigned char* stage_mem[2] = {smem, smem + STAGE_BYTES};
-    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + 2 * STAGE_BYTES);          // 2 stage barriers
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + 2 * STAGE_BYTES + 32);
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const GemmTile tile = tiles[blockIdx.x];
-    const GemmGroup g = groups[tile.group];
+// ---- the GEMM ------------------------------------------------------------------
+struct Bars {
+    uint64_t full[NSTAGE], empty[NSTAGE], accf[2], acce[2];
+    uint32_t tmem;
+};
+static_assert(sizeof(Bars) <= 256, "barrier block");
 
-    if (warp == 0) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+__global__ void __launch_bounds__(NT, 1) gemm_tf32x3_kernel(const unsigned char* __restrict__ a_imgs,
+                                                            const unsigned char* __restrict__ b_imgs,
+                                                            double* __restrict__ C, double* __restrict__ Caux,
+                                                            unsigned char* __restrict__ t_out,
+                                                            const PackedTerm* __restrict__ terms,
+                                                            const PackedGroup* __restrict__ groups,
+                                                            const PackedTile* __restrict__ tiles, int accumulate,
+                                                            int out_mode, int* __restrict__ status) {
+    extern __shared__ __align__(1024) unsigned char smem[];
+    Bars& B = *reinterpret_cast<Bars*>(smem + BAR_OFF);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const PackedTile tile = tiles[blockIdx.x];
+    const PackedGroup g = groups[tile.group];
+
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&B.tmem)),
                      "r"(TMEM_COLS)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bars[0])) : "memory");
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bars[1])) : "memory");
+        for (int s = 0; s < NSTAGE; ++s) {
+            mbar_init(&B.full[s], 1);
+            mbar_init(&B.empty[s], 1);
+        }
+        for (int a = 0; a < 2; ++a) {
+            mbar_init(&B.accf[a], 1);
+            mbar_init(&B.acce[a], 4);
+        }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    const uint32_t tmem = *tmem_slot;
-
+    const uint32_t tmem = B.tmem;
     bool ok = true;
-    int issued = 0;              // stages committed so far
-    uint32_t phase[2] = {0, 0};  // parity of the next completion to wait for, per stage
-    int t = g.t0, k0 = 0;
-    GemmTerm cur = terms[t];
-    while (t < g.t1) {
-        const int s = issued & 1;
-        bool mine = true;
-        if (issued >= 2) {  // the MMAs that last read this stage must be done
-            mine = mbar_wait(&bars[s], phase[s]);
-            phase[s] ^= 1u;
-        }
-        if (mine) fill_stage<TA, TB>(stage_mem[s], A, B, cur, k0, tile.m0, tile.n0, g.m, g.n, tid);
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        if (!__syncthreads_and(mine ? 1 : 0)) {
-            ok = false;
-            break;
-        }
-        if (tid == 0) {
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const uint32_t a_base = smem_u32(stage_mem[s]);
-            const uint32_t b_base = a_base + 2 * PLANE_A;
-#pragma unroll
-            for (int ks = 0; ks < TK / 8; ++ks) {
-                const uint64_t ahi = make_smem_desc(a_base + 2 * ks * LBO_A, LBO_A, SBO);
-                const uint64_t alo = make_smem_desc(a_base + PLANE_A + 2 * ks * LBO_A, LBO_A, SBO);
-                const uint64_t bhi = make_smem_desc(b_base + 2 * ks * LBO_B, LBO_B, SBO);
-                const uint64_t blo = make_smem_desc(b_base + PLANE_B + 2 * ks * LBO_B, LBO_B, SBO);
-                mma_tf32(tmem, ahi, bhi, (issued > 0 || ks > 0) ? 1u : 0u);
-                mma_tf32(tmem, ahi, blo, 1u);
-                mma_tf32(tmem, alo, bhi, 1u);
+
+    if (warp == 0) {
+        // ---- producer ----
+        if (lane == 0) {
+            int it = 0;
+            for (int t = g.t0; t < g.t1 && ok; ++t) {
+                const PackedTerm tm = terms[t];
+                const unsigned char* a = a_imgs + tm.a_img + (int64_t)tile.pm * tm.slices * kImageA;
+                const unsigned char* b = b_imgs + tm.b_img + (int64_t)tile.pn * tm.slices * kImageB;
+                for (int s = 0; s < tm.slices; ++s, ++it) {
+                    const int st = it % NSTAGE;
+                    if (it >= NSTAGE && !mbar_wait(&B.empty[st], ((it / NSTAGE) - 1) & 1)) {
+                        ok = false;
+                        break;
+                    }
+                    unsigned char* dst = smem + st * STAGE_BYTES;
+                    mbar_arrive_expect_tx(&B.full[st], STAGE_BYTES);
+                    bulk_g2s(dst, a + (int64_t)s * kImageA, kImageA, &B.full[st]);
+                    bulk_g2s(dst + kImageA, b + (int64_t)s * kImageB, kImageB, &B.full[st]);
+                }
             }
-            mma_commit(&bars[s]);
+            // Tail: nothing asynchronous may still target this CTA's shared memory
+            // when it exits.  Wait until the copies of the last stages have landed
+            // and until the MMAs that read them have completed and their commits
+            // have arrived on the "empty" barriers (earlier stages were waited for
+            // before their buffers were refilled).
+            const int first = it > NSTAGE ? it - NSTAGE : 0;
+            for (int j = first; j < it; ++j)
+                if (!mbar_wait(&B.full[j % NSTAGE], (j / NSTAGE) & 1)) ok = false;
+            for (int j = first; j < it; ++j)
+                if (!mbar_wait(&B.empty[j % NSTAGE], (j / NSTAGE) & 1)) ok = false;
         }
-        ++issued;
-        k0 += TK;
-        if (k0 >= cur.k) {
-            k0 = 0;
-            ++t;
-            if (t < g.t1) cur = terms[t];
+    } else if (warp == 1) {
+        // ---- MMA issuer ----
+        if (lane == 0) {
+            int it = 0, ti = 0;
+            for (int t = g.t0; t < g.t1 && ok; ++t, ++ti) {
+                const int acc = ti & 1;
+                if (ti >= 2 && !mbar_wait(&B.acce[acc], ((ti >> 1) - 1) & 1)) {
+                    ok = false;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const int slices = terms[t].slices;
+                const uint32_t d = tmem + (uint32_t)(acc * TN);
+                for (int s = 0; s < slices; ++s, ++it) {
+                    const int st = it % NSTAGE;
+                    if (!mbar_wait(&B.full[st], (it / NSTAGE) & 1)) {
+                        ok = false;
+                        break;
+                    }
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    const uint32_t a_base = smem_u32(smem + st * STAGE_BYTES);
+                    const uint32_t b_base = a_base + kImageA;
+#pragma unroll
+                    for (int ks = 0; ks < TK / 8; ++ks) {
+                        const uint64_t ahi = make_smem_desc(a_base + 2 * ks * LBO_A, LBO_A, SBO);
+                        const uint64_t alo = make_smem_desc(a_base + PLANE_A + 2 * ks * LBO_A, LBO_A, SBO);
+                        const uint64_t bhi = make_smem_desc(b_base + 2 * ks * LBO_B, LBO_B, SBO);
+                        const uint64_t blo = make_smem_desc(b_base + PLANE_B + 2 * ks * LBO_B, LBO_B, SBO);
+                        mma_tf32(d, ahi, bhi, (s > 0 || ks > 0) ? 1u : 0u);
+                        mma_tf32(d, ahi, blo, 1u);
+                        mma_tf32(d, alo, bhi, 1u);
+                    }
+                    mma_commit(&B.empty[st]);  // the stage's buffer is free once these MMAs are done
+                }
+                if (!ok) break;
+                mma_commit(&B.accf[acc]);      // the term's accumulator is complete
+            }
         }
-    }
-    // every commit not yet waited for (the last one or two stages) must complete,
-    // on the error path too, before TMEM is read or freed
-    bool drained = true;
-    for (int j = 0; j < 2 && j < issued; ++j) {
-        const int st_idx = (issued - 1 - j) & 1;
-        if (!mbar_wait(&bars[st_idx], phase[st_idx])) drained = false;
-    }
-    ok = __syncthreads_and((ok && drained) ? 1 : 0) != 0;
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    if (ok && issued > 0) {
-        const bool acc_out = accumulate && g.cbuf == 0;
-        double* Cb = g.cbuf ? Caux : C;
-        const int row = tile.m0 + warp * 32 + lane;
+    } else {
+        // ---- epilogue: warps 2..5 ----
+        const int quarter = warp & 3;
+        const int row = quarter * 32 + lane;  // tile row = TMEM lane
+        double sum[TN];
 #pragma unroll
-        for (int half = 0; half < TN / 32; ++half) {
-            uint32_t v[32];
-            tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(half * 32), v);
-            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-            if (row < g.m) {
-                double* crow = Cb + g.c_off + (int64_t)row * g.ldc;
+        for (int j = 0; j < TN; ++j) sum[j] = 0.0;
+        int ti = 0;
+        for (int t = g.t0; t < g.t1; ++t, ++ti) {
+            const int acc = ti & 1;
+            const bool got = mbar_wait(&B.accf[acc], (ti >> 1) & 1);
+            if (!__all_sync(0xffffffffu, got)) {  // warp-uniform: tcgen05.ld below is .sync.aligned
+                ok = false;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const double w = terms[t].w;
 #pragma unroll
-                for (int j = 0; j < 32; ++j) {
-                    const int col = tile.n0 + half * 32 + j;
-                    if (col < g.n) {
-                        const double x = (double)__uint_as_float(v[j]);
-                        crow[col] = acc_out ? crow[col] + x : x;
+            for (int h = 0; h < TN / 32; ++h) {
+                uint32_t v[32];
+                tmem_ld32(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(acc * TN + h * 32), v);
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+                for (int j = 0; j < 32; ++j) sum[h * 32 + j] += w * (double)__uint_as_float(v[j]);
+            }
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&B.acce[acc]);
+        }
+        if (ok) {
+            const int grow = tile.pm * TM + row;  // row of the output block
+            if (out_mode == 0) {
+                if (grow < g.m) {
+                    double* Cb = g.cbuf ? Caux : C;
+                    const bool acc_out = accumulate && g.cbuf == 0;
+                    double* crow = Cb + g.c_off + (int64_t)grow * g.ldc;
+#pragma unroll
+                    for (int j = 0; j < TN; ++j) {
+                        const int col = tile.pn * TN + j;
+                        if (col < g.n) crow[col] = acc_out ? crow[col] + sum[j] : sum[j];
+                    }
+                }
+            } else {
+                // the output as B-role images of X = output^T (rows = columns of the
+                // output, k = rows of the output); zeros in the padding
+                const int slice = grow / TK;
+                if (slice < g.t_slices) {
+                    unsigned char* img = t_out + g.t_img + ((int64_t)tile.pn * g.t_slices + slice) * kImageB;
+                    uint32_t* hi = reinterpret_cast<uint32_t*>(img);
+                    uint32_t* lo = reinterpret_cast<uint32_t*>(img + PLANE_B);
+                    const int k = grow % TK;
+#pragma unroll
+                    for (int j = 0; j < TN; ++j) {
+                        const int col = tile.pn * TN + j;
+                        uint32_t h = 0, l = 0;
+                        if (grow < g.m && col < g.n) split(sum[j], h, l);
+                        const int off = plane_off(j, k, TN) >> 2;
+                        hi[off] = h;
+                        lo[off] = l;
                     }
                 }
             }
         }
     }
-    if (!ok && tid == 0) atomicExch(status, DMRG_E_NUMERIC);
+    __syncwarp();  // producer and MMA warps: lanes 1..31 wait for lane 0
+    if (!ok) atomicExch(status, DMRG_E_NUMERIC);
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
-    if (warp == 0)
+    if (warp == 1)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
 }
 
-// Deterministic split-K reduction (the same scheme as gemm_f64.cu): grid (element
-// slices, split groups), chunks summed in a fixed order.
+// Deterministic split-K reduction (the scheme of gemm_f64.cu): chunks summed in order.
 __global__ void __launch_bounds__(256) split_reduce_tf32_kernel(double* __restrict__ C,
                                                                 const double* __restrict__ Caux,
                                                                 const GemmSplit* __restrict__ splits, int accumulate) {
@@ -285,32 +375,131 @@ __global__ void __launch_bounds__(256) split_reduce_tf32_kernel(double* __restri
     }
 }
 
-template <bool TA, bool TB>
-int launch_variant(const GemmSchedule& s, const double* A, const double* B, double* C, bool accumulate, int* status,
-                   cudaStream_t st) {
-    static bool attr = false;
-    if (!attr) {
-        DMRG_CUDA_TRY(cudaFuncSetAttribute(gemm_tf32x3_kernel<TA, TB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           SMEM_BYTES));
-        attr = true;
-    }
-    gemm_tf32x3_kernel<TA, TB><<<(int)s.tiles.size(), NT, SMEM_BYTES, st>>>(
-        A, B, C, s.aux.as<double>(), s.d_terms.as<GemmTerm>(), s.d_groups.as<GemmGroup>(), s.d_tiles.as<GemmTile>(),
-        accumulate ? 1 : 0, status);
+}  // namespace
+
+int64_t PackSchedule::add(int64_t src_off, int rows, int k, int ld, bool trans, int prow) {
+    PackJob j{};
+    j.src_off = src_off;
+    j.img_off = bytes;
+    j.rows = rows;
+    j.k = k;
+    j.ld = ld;
+    j.trans = trans ? 1 : 0;
+    j.prow = prow;
+    j.slices = (k + TK - 1) / TK;
+    const int panels = (rows + prow - 1) / prow;
+    const int job = (int)jobs.size();
+    jobs.push_back(j);
+    for (int p = 0; p < panels; ++p)
+        for (int s = 0; s < j.slices; ++s) images.push_back(PackImage{job, p, s, 0});
+    bytes += (int64_t)panels * j.slices * 2 * prow * TK * 4;
+    return j.img_off;
+}
+
+int PackSchedule::finalize(cudaStream_t stream) {
+    DMRG_TRY(upload(d_jobs, jobs, stream));
+    DMRG_TRY(upload(d_images, images, stream));
     return DMRG_OK;
 }
 
-}  // namespace
+int launch_pack(const PackSchedule& p, const double* src, unsigned char* dst, cudaStream_t stream) {
+    if (p.images.empty()) return DMRG_OK;
+    pack_kernel<<<(int)p.images.size(), 128, 0, stream>>>(p.d_jobs.as<PackJob>(), p.d_images.as<PackImage>(), src,
+                                                          dst);
+    DMRG_CUDA_TRY(cudaGetLastError());
+    return DMRG_OK;
+}
 
-int launch_gemm_tf32x3(const GemmSchedule& s, const double* A, const double* B, double* C, bool accumulate,
-                       int* status, cudaStream_t stream) {
+int PackedSchedule::finalize(cudaStream_t stream, int num_sms) {
+    exec_groups.clear();
+    splits.clear();
+    tiles.clear();
+    aux_size = 0;
+    auto stages = [&](const PackedGroup& g) {
+        int64_t s = 0;
+        for (int t = g.t0; t < g.t1; ++t) s += terms[t].slices;
+        return s;
+    };
+    int64_t total = 0;
+    for (const PackedGroup& g : groups)
+        total += stages(g) * ((g.m + TM - 1) / TM) * ((g.n + TN - 1) / TN);
+    const int64_t share = (num_sms > 0 && out_mode == 0) ? std::max<int64_t>(8, total / ((int64_t)num_sms * 2)) : 0;
+    for (const PackedGroup& g : groups) {
+        if (g.m <= 0 || g.n <= 0 || g.t1 <= g.t0) continue;
+        const int64_t st = stages(g);
+        if (share == 0 || st <= 2 * share || g.t1 - g.t0 < 2) {
+            exec_groups.push_back(g);
+            continue;
+        }
+        GemmSplit sp{g.c_off, aux_size, g.ldc, g.m, g.n, 0};
+        int t0 = g.t0;
+        int64_t acc = 0;
+        for (int t = g.t0; t < g.t1; ++t) {
+            acc += terms[t].slices;
+            if (acc >= share || t + 1 == g.t1) {
+                PackedGroup c = g;
+                c.t0 = t0;
+                c.t1 = t + 1;
+                c.c_off = aux_size + (int64_t)sp.chunks * g.m * g.n;
+                c.ldc = g.n;
+                c.cbuf = 1;
+                exec_groups.push_back(c);
+                sp.chunks++;
+                t0 = t + 1;
+                acc = 0;
+            }
+        }
+        aux_size += (int64_t)sp.chunks * g.m * g.n;
+        splits.push_back(sp);
+    }
+    for (int gi = 0; gi < (int)exec_groups.size(); ++gi) {
+        const PackedGroup& g = exec_groups[gi];
+        const int cost = (int)stages(g);
+        for (int pm = 0; pm * TM < g.m; ++pm)
+            for (int pn = 0; pn * TN < g.n; ++pn) tiles.push_back(PackedTile{gi, pm, pn, cost});
+    }
+    std::stable_sort(tiles.begin(), tiles.end(), [](const PackedTile& a, const PackedTile& b) { return a.cost > b.cost; });
+    DMRG_TRY(upload(d_terms, terms, stream));
+    DMRG_TRY(upload(d_groups, exec_groups, stream));
+    DMRG_TRY(upload(d_tiles, tiles, stream));
+    DMRG_TRY(upload(d_splits, splits, stream));
+    DMRG_TRY(aux.alloc((size_t)std::max<int64_t>(aux_size, 1) * sizeof(double)));
+    return DMRG_OK;
+}
+
+int PackedSchedule::check_bounds(int64_t a_bytes, int64_t b_bytes, int64_t c_size, int64_t t_bytes) const {
+    for (const PackedGroup& g : groups) {
+        if (g.m <= 0 || g.n <= 0) continue;
+        const int64_t pm = (g.m + TM - 1) / TM, pn = (g.n + TN - 1) / TN;
+        for (int t = g.t0; t < g.t1; ++t) {
+            const PackedTerm& tm = terms[t];
+            if (tm.a_img < 0 || tm.a_img + pm * tm.slices * kImageA > a_bytes || tm.b_img < 0 ||
+                tm.b_img + pn * tm.slices * kImageB > b_bytes || tm.a_img % 16 || tm.b_img % 16)
+                return set_error(DMRG_E_ARG, "packed GEMM term %d reads outside its images", t);
+        }
+        if (out_mode == 0) {
+            if (g.c_off < 0 || g.c_off + (int64_t)(g.m - 1) * g.ldc + g.n > c_size || g.n > g.ldc)
+                return set_error(DMRG_E_ARG, "packed GEMM output %lld outside %lld", (long long)g.c_off,
+                                 (long long)c_size);
+        } else if (g.t_img < 0 || g.t_img + pn * g.t_slices * kImageB > t_bytes || (int64_t)g.t_slices * TK < g.m ||
+                   g.t_img % 16) {
+            return set_error(DMRG_E_ARG, "packed GEMM output images outside their buffer");
+        }
+    }
+    return DMRG_OK;
+}
+
+int launch_gemm_tf32x3(const PackedSchedule& s, const unsigned char* a_imgs, const unsigned char* b_imgs, double* C,
+                       unsigned char* t_out, bool accumulate, int* status, cudaStream_t stream) {
     if (s.tiles.empty()) return DMRG_OK;
-    if (s.tile_m != TM || s.tile_n != TN)
-        return set_error(DMRG_E_ARG, "TF32X3 GEMM needs a %dx%d tile schedule (got %dx%d)", TM, TN, s.tile_m, s.tile_n);
-    if (!s.ta && !s.tb) DMRG_TRY((launch_variant<false, false>(s, A, B, C, accumulate, status, stream)));
-    else if (s.ta && !s.tb) DMRG_TRY((launch_variant<true, false>(s, A, B, C, accumulate, status, stream)));
-    else if (!s.ta && s.tb) DMRG_TRY((launch_variant<false, true>(s, A, B, C, accumulate, status, stream)));
-    else DMRG_TRY((launch_variant<true, true>(s, A, B, C, accumulate, status, stream)));
+    static bool attr = false;
+    if (!attr) {
+        DMRG_CUDA_TRY(cudaFuncSetAttribute(gemm_tf32x3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
+        attr = true;
+    }
+    gemm_tf32x3_kernel<<<(int)s.tiles.size(), NT, SMEM_BYTES, stream>>>(
+        a_imgs, b_imgs, C, s.aux.as<double>(), t_out, s.d_terms.as<PackedTerm>(), s.d_groups.as<PackedGroup>(),
+        s.d_tiles.as<PackedTile>(), accumulate ? 1 : 0, s.out_mode, status);
     if (!s.splits.empty()) {
         int64_t biggest = 0;
         for (const GemmSplit& sp : s.splits) biggest = std::max<int64_t>(biggest, (int64_t)sp.m * sp.n);

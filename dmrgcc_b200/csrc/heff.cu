@@ -12,6 +12,7 @@
 //   stage B: one group per output block (i, j) holding all of its
 //            (W, L block, T) terms, summed in registers by the tile owner.
 #include <algorithm>
+#include <map>
 
 #include "heff.cuh"
 
@@ -129,10 +130,65 @@ int build_heff(dmrg_heff_s& h) {
     DMRG_TRY(h.sa.finalize(64, 64, 16, st));
     DMRG_TRY(h.sb.finalize(64, 64, 16, st, h.ctx->num_sms));
     if (h.precision == DMRG_PREC_TF32X3) {
-        h.sa3.copy_plan(h.sa);
-        h.sb3.copy_plan(h.sb);
-        DMRG_TRY(h.sa3.finalize(128, 64, 32, st));
-        DMRG_TRY(h.sb3.finalize(128, 64, 32, st, h.ctx->num_sms));
+        // operand images: psi blocks and L blocks in the A role, R blocks (transposed)
+        // in the B role, and the K*R intermediates written directly as B-role images
+        std::vector<int64_t> psi_img(ket.count());
+        for (int pos = 0; pos < ket.count(); ++pos)
+            psi_img[pos] = h.pk_psi.add(ket.off[pos], ket.rows[pos], ket.cols[pos], ket.cols[pos], false, kPackRowsA);
+        std::map<int64_t, int64_t> r_img, l_img;
+        auto slices = [](int k) { return (k + kPackK - 1) / kPackK; };
+        std::vector<int64_t> t_img(tasks.size());
+        h.pa.reset();
+        h.pa.out_mode = 1;
+        h.t_img_bytes = 0;
+        for (size_t i = 0; i < tasks.size(); ++i) {
+            const TaskA& t = tasks[i];
+            auto it = r_img.find(t.r_off);
+            if (it == r_img.end())
+                it = r_img.emplace(t.r_off, h.pk_R.add(t.r_off, t.b_j, t.b_l, t.b_j, true, kPackRowsB)).first;
+            t_img[i] = h.t_img_bytes;
+            h.t_img_bytes += (int64_t)((t.b_j + kPackRowsB - 1) / kPackRowsB) * slices(t.a_k) * kImageB;
+            PackedGroup g{};
+            g.t0 = (int)h.pa.terms.size();
+            g.m = t.a_k;
+            g.n = t.b_j;
+            g.t_img = t_img[i];
+            g.t_slices = slices(t.a_k);
+            h.pa.terms.push_back(PackedTerm{psi_img[t.pos], it->second, slices(t.b_l), 0, 1.0});
+            g.t1 = (int)h.pa.terms.size();
+            h.pa.groups.push_back(g);
+        }
+        h.pb.reset();
+        h.pb.out_mode = 0;
+        for (int pos2 = 0; pos2 < ket.count(); ++pos2) {
+            if (per_out[pos2].empty()) continue;
+            PackedGroup g{};
+            g.t0 = (int)h.pb.terms.size();
+            g.m = ket.rows[pos2];
+            g.n = ket.cols[pos2];
+            g.c_off = ket.off[pos2];
+            g.ldc = ket.cols[pos2];
+            for (int i : per_out[pos2]) {
+                const TermB& t = termsB[i];
+                auto it = l_img.find(t.l_off);
+                if (it == l_img.end())
+                    it = l_img.emplace(t.l_off, h.pk_L.add(t.l_off, ket.rows[pos2], t.k, t.lda, false, kPackRowsA)).first;
+                h.pb.terms.push_back(PackedTerm{it->second, t_img[t.t_index], slices(t.k), 0, t.w});
+            }
+            g.t1 = (int)h.pb.terms.size();
+            h.pb.groups.push_back(g);
+        }
+        DMRG_TRY(h.pa.check_bounds(h.pk_psi.bytes, h.pk_R.bytes, 0, h.t_img_bytes));
+        DMRG_TRY(h.pb.check_bounds(h.pk_L.bytes, h.t_img_bytes, ket.size, 0));
+        DMRG_TRY(h.pk_psi.finalize(st));
+        DMRG_TRY(h.pk_L.finalize(st));
+        DMRG_TRY(h.pk_R.finalize(st));
+        DMRG_TRY(h.pa.finalize(st));
+        DMRG_TRY(h.pb.finalize(st, h.ctx->num_sms));
+        DMRG_TRY(h.img_psi.alloc((size_t)std::max<int64_t>(h.pk_psi.bytes, 16)));
+        DMRG_TRY(h.img_L.alloc((size_t)std::max<int64_t>(h.pk_L.bytes, 16)));
+        DMRG_TRY(h.img_R.alloc((size_t)std::max<int64_t>(h.pk_R.bytes, 16)));
+        DMRG_TRY(h.img_T.alloc((size_t)std::max<int64_t>(h.t_img_bytes, 16)));
     }
     DMRG_TRY(h.T.alloc((size_t)std::max<int64_t>(h.t_size, 1) * sizeof(double)));
     return DMRG_OK;
@@ -158,8 +214,11 @@ int dmrg::heff_apply_internal(dmrg_heff_s& h, const double* psi, double* out, bo
     cudaStream_t st = h.ctx->stream;
     if (!accumulate && h.site.ket.size)
         DMRG_CUDA_TRY(cudaMemsetAsync(out, 0, (size_t)h.site.ket.size * sizeof(double), st));
-    DMRG_TRY(launch_gemm_tf32x3(h.sa3, psi, h.R_dev, h.T.as<double>(), false, h.ctx->d_status, st));
-    DMRG_TRY(launch_gemm_tf32x3(h.sb3, h.L_dev, h.T.as<double>(), out, true, h.ctx->d_status, st));
+    DMRG_TRY(launch_pack(h.pk_psi, psi, h.img_psi.as<unsigned char>(), st));
+    DMRG_TRY(launch_gemm_tf32x3(h.pa, h.img_psi.as<unsigned char>(), h.img_R.as<unsigned char>(), nullptr,
+                                h.img_T.as<unsigned char>(), false, h.ctx->d_status, st));
+    DMRG_TRY(launch_gemm_tf32x3(h.pb, h.img_L.as<unsigned char>(), h.img_T.as<unsigned char>(), out, nullptr, true,
+                                h.ctx->d_status, st));
     return DMRG_OK;
 }
 
@@ -213,6 +272,10 @@ int dmrg_heff_set_env(dmrg_heff_t h, const double* L_dev, const double* R_dev) {
     if ((!L_dev && h->L.size) || (!R_dev && h->R.size)) return set_error(DMRG_E_ARG, "null environment pointer");
     h->L_dev = L_dev;
     h->R_dev = R_dev;
+    if (h->precision == DMRG_PREC_TF32X3) {  // environment images, kept until the next call
+        DMRG_TRY(launch_pack(h->pk_L, L_dev, h->img_L.as<unsigned char>(), h->ctx->stream));
+        DMRG_TRY(launch_pack(h->pk_R, R_dev, h->img_R.as<unsigned char>(), h->ctx->stream));
+    }
     return DMRG_OK;
 }
 
@@ -230,11 +293,19 @@ int dmrg_heff_profile(dmrg_heff_t h, const double* psi, double* out, double* ms_
     for (auto& e : ev) DMRG_CUDA_TRY(cudaEventCreate(&e));
     const bool split = h->precision == DMRG_PREC_TF32X3;
     DMRG_CUDA_TRY(cudaEventRecord(ev[0], st));
-    int rc = split ? launch_gemm_tf32x3(h->sa3, psi, h->R_dev, h->T.as<double>(), false, h->ctx->d_status, st)
-                   : launch_gemm_f64(h->sa, psi, h->R_dev, h->T.as<double>(), false, st);
+    int rc = DMRG_OK;
+    if (split) {  // stage A includes packing psi
+        rc = launch_pack(h->pk_psi, psi, h->img_psi.as<unsigned char>(), st);
+        if (rc == DMRG_OK)
+            rc = launch_gemm_tf32x3(h->pa, h->img_psi.as<unsigned char>(), h->img_R.as<unsigned char>(), nullptr,
+                                    h->img_T.as<unsigned char>(), false, h->ctx->d_status, st);
+    } else {
+        rc = launch_gemm_f64(h->sa, psi, h->R_dev, h->T.as<double>(), false, st);
+    }
     cudaEventRecord(ev[1], st);
     if (rc == DMRG_OK)
-        rc = split ? launch_gemm_tf32x3(h->sb3, h->L_dev, h->T.as<double>(), out, true, h->ctx->d_status, st)
+        rc = split ? launch_gemm_tf32x3(h->pb, h->img_L.as<unsigned char>(), h->img_T.as<unsigned char>(), out,
+                                        nullptr, true, h->ctx->d_status, st)
                    : launch_gemm_f64(h->sb, h->L_dev, h->T.as<double>(), out, true, st);
     cudaEventRecord(ev[2], st);
     cudaError_t err = cudaEventSynchronize(ev[2]);

@@ -15,7 +15,11 @@ struct dmrg_heff_s {
     dmrg::SiteDesc site;
     dmrg::EnvDesc L, R;
     dmrg::GemmSchedule sa, sb;    // A: psi x R -> T ; B: L x T -> out (FP64 tiles)
-    dmrg::GemmSchedule sa3, sb3;  // the same products in TF32X3 tiles (DMRG_PREC_TF32X3 only)
+    // DMRG_PREC_TF32X3 only: split-precision operand images and packed schedules
+    dmrg::PackSchedule pk_psi, pk_L, pk_R;     // which blocks to pack, where
+    dmrg::PackedSchedule pa, pb;               // A: psi x R -> T images ; B: L x T -> out
+    dmrg::DeviceBuffer img_psi, img_L, img_R, img_T;
+    int64_t t_img_bytes = 0;
     dmrg::DeviceBuffer T;
     int64_t t_size = 0;
     const double* L_dev = nullptr;

@@ -1039,7 +1039,7 @@ int Engine::ComputeTensorNetwork(int leigh, int site) {
     dmrg_blocks_t kb = as_blocks(t.ket.d);
     dmrg_env_t e = nullptr;
     DMRG_TRY(dmrg_env_create(ctx_, leigh, t.nl(), t.nr(), t.phys.data(), &kb, W.get_physics_dim(), W.get_left_bond(),
-                             W.get_right_bond(), W.data().data(), ib.data(), opt_.precision == DMRG_PREC_FP64 ? 0 : 0,
+                             W.get_right_bond(), W.data().data(), ib.data(), DMRG_PREC_FP64,
                              &e));
     int bond = 0;
     int64_t size = 0;
@@ -1078,7 +1078,7 @@ int Engine::LanczosMethod(int niter, int site, double& energy, int& dim) {
     dmrg_blocks_t kb = as_blocks(t.ket.d);
     dmrg_heff_t h = nullptr;
     DMRG_TRY(dmrg_heff_create(ctx_, t.nl(), t.nr(), t.phys.data(), &kb, W.get_physics_dim(), W.get_left_bond(),
-                              W.get_right_bond(), W.data().data(), lb.data(), rb.data(), DMRG_PREC_FP64, &h));
+                              W.get_right_bond(), W.data().data(), lb.data(), rb.data(), opt_.precision, &h));
     int rc = dmrg_heff_set_env(h, c.L.ptr(), c.R.ptr());
     if (rc == DMRG_OK)
         rc = dmrg_lanczos(h, t.ket.ptr(), niter, opt_.lanczos_precision, opt_.zero_tolerance, &energy, &dim);

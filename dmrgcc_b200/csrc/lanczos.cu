@@ -14,6 +14,10 @@
 // psi_dim < 100 takes the reference's exact-diagonalisation branch (:34-56):
 // the dense H_eff is assembled column by column from matvecs on unit vectors
 // and diagonalised by a device Jacobi solver.
+// DMRG_PREC_TF32X3 operators: a first Krylov run with tensor-core split-precision
+// matvecs, then the FP64 run above from its Ritz vector (FP64 for the dense
+// branch, the recurrence, reorthogonalisation, the tridiagonal problem and the
+// energy).
 #include <algorithm>
 
 #include "eig.cuh"
@@ -28,6 +32,7 @@ struct LanczosWork {
     DeviceBuffer V, h, scal, state, jac, y, dense;
     ReduceScratch rs;
     int* h_state = nullptr;  // pinned: [done, dim]
+    int split_iters = 0;     // Krylov dimension of the last split-precision phase
     ~LanczosWork() {
         if (h_state) cudaFreeHost(h_state);
     }
@@ -40,6 +45,10 @@ using namespace dmrg;
 dmrg_heff_s::~dmrg_heff_s() { delete lw; }
 
 namespace {
+
+// Convergence of the split-precision phase: |E_i - E_{i-1}| below this (the
+// matvec's relative error is ~1e-6, the Ritz value settles well before).
+constexpr double kSplitPrecision = 1e-9;
 
 __global__ void unit_vector_kernel(double* x, int64_t n, int64_t c) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
@@ -91,7 +100,7 @@ int run_exact(dmrg_heff_s& h, double* psi, double* energy) {
     double* e = w.h.as<double>();
     for (int c = 0; c < n; ++c) {
         unit_vector_kernel<<<1, 128, 0, st>>>(e, n, c);
-        DMRG_TRY(heff_apply_internal(h, e, cols + (size_t)c * n, false));
+        DMRG_TRY(heff_apply_fp64(h, e, cols + (size_t)c * n, false));  // the dense branch stays FP64
     }
     symmetrize_upper_kernel<<<std::max(1, (n * n + 255) / 256), 256, 0, st>>>(cols, A, n);
     DMRG_CUDA_TRY(cudaMemsetAsync(w.state.ptr, 0, 16 * sizeof(int), st));
@@ -106,21 +115,14 @@ int run_exact(dmrg_heff_s& h, double* psi, double* energy) {
     return DMRG_OK;
 }
 
-}  // namespace
-
-extern "C" int dmrg_lanczos(dmrg_heff_t hp, double* psi, int niter, double precision, double zero_tol,
-                            double* energy, int* iters) {
-    if (!hp || !psi || !energy || niter <= 0) return set_error(DMRG_E_ARG, "invalid Lanczos arguments");
-    if (niter > kMaxVec) return set_error(DMRG_E_ARG, "niter %d above %d", niter, kMaxVec);
-    dmrg_heff_s& h = *hp;
-    DMRG_TRY(ensure_work(h, niter));
+// One Lanczos run from psi (real_tensor_lanczos.cc:57-185): matvecs in the
+// operator's split precision when `split`, else FP64; vectors, recurrence,
+// reorthogonalisation and the tridiagonal problem always FP64.
+int krylov(dmrg_heff_s& h, double* psi, int niter, double precision, double zero_tol, bool split, double* energy,
+           int* iters) {
     LanczosWork& w = *h.lw;
     const int64_t n = h.site.ket.size;
     cudaStream_t st = h.ctx->stream;
-    if (n < 100) {  // exact diagonalisation branch (real_tensor_lanczos.cc:34)
-        if (iters) *iters = 0;
-        return run_exact(h, psi, energy);
-    }
     const int blocks = std::min<int64_t>((n + kVecThreads - 1) / kVecThreads, 2 * h.ctx->num_sms);
     double* V = w.V.as<double>();
     double* hv = w.h.as<double>();
@@ -136,7 +138,7 @@ extern "C" int dmrg_lanczos(dmrg_heff_t hp, double* psi, int niter, double preci
     int dim = 0;
     for (int i = 0; i < niter; ++i) {
         double* vi = V + (int64_t)i * n;
-        DMRG_TRY(heff_apply_internal(h, vi, hv, true));
+        DMRG_TRY(split ? heff_apply_internal(h, vi, hv, true) : heff_apply_fp64(h, vi, hv, true));
         DMRG_TRY(vec_dot(vi, hv, n, alpha + i, w.rs, blocks, st));
         DMRG_TRY(vec_axpy_norm(alpha + i, vi, hv, n, beta + i, w.rs, blocks, st));
         DMRG_TRY(launch_tridiag_lowest(alpha, beta, i + 1, E, state, precision, zero_tol, niter, st));
@@ -163,7 +165,38 @@ extern "C" int dmrg_lanczos(dmrg_heff_t hp, double* psi, int niter, double preci
     DMRG_CUDA_TRY(cudaMemcpyAsync(w.h_state, state, 4 * sizeof(int), cudaMemcpyDeviceToHost, st));
     DMRG_CUDA_TRY(cudaStreamSynchronize(st));
     if (w.h_state[2] != 0) return set_error(DMRG_E_NUMERIC, "tridiagonal Jacobi did not converge (m=%d)", dim);
+    if (split) DMRG_TRY(take_device_status(h.ctx));  // a tensor-core wait that gave up
     *energy = e;
     if (iters) *iters = dim;
+    return DMRG_OK;
+}
+
+}  // namespace
+
+extern "C" int dmrg_lanczos(dmrg_heff_t hp, double* psi, int niter, double precision, double zero_tol,
+                            double* energy, int* iters) {
+    if (!hp || !psi || !energy || niter <= 0) return set_error(DMRG_E_ARG, "invalid Lanczos arguments");
+    if (niter > kMaxVec) return set_error(DMRG_E_ARG, "niter %d above %d", niter, kMaxVec);
+    dmrg_heff_s& h = *hp;
+    DMRG_TRY(ensure_work(h, niter));
+    const int64_t n = h.site.ket.size;
+    if (n < 100) {  // exact diagonalisation branch (real_tensor_lanczos.cc:34)
+        if (iters) *iters = 0;
+        return run_exact(h, psi, energy);
+    }
+    if (h.precision != DMRG_PREC_TF32X3) return krylov(h, psi, niter, precision, zero_tol, false, energy, iters);
+    // Mixed precision: a Krylov run on split-precision matvecs until the Ritz
+    // value settles at the split arithmetic's resolution, then the FP64 run of
+    // the reference from that Ritz vector, which fixes the energy and the state.
+    double e_split = 0.0;
+    int it_split = 0;
+    DMRG_TRY(krylov(h, psi, niter, kSplitPrecision, zero_tol, true, &e_split, &it_split));
+    LanczosWork& w = *h.lw;
+    const int blocks = (int)std::min<int64_t>((n + kVecThreads - 1) / kVecThreads, 2 * h.ctx->num_sms);
+    DMRG_TRY(vec_normalize(psi, n, w.scal.as<double>() + 4 * niter, w.rs, blocks, h.ctx->stream));
+    int it_fp64 = 0;
+    DMRG_TRY(krylov(h, psi, niter, precision, zero_tol, false, energy, &it_fp64));
+    w.split_iters = it_split;
+    if (iters) *iters = it_fp64;
     return DMRG_OK;
 }

@@ -222,7 +222,9 @@ int dmrg_canon_write(dmrg_canon_t c, const double* ket_dev, double* new_ket_dev,
  * expansion, SVD truncation, environment update, merge) runs on the device.
  * model: "real_spinless_bose_square" (NULL = that). */
 typedef struct {
-    int precision;              /* DMRG_PREC_FP64 */
+    int precision;              /* DMRG_PREC_FP64, or DMRG_PREC_TF32X3: Lanczos
+                                   matvecs first in split precision, then the
+                                   FP64 Lanczos from that vector (dmrg_lanczos) */
     int verbose;                /* 1: print like the reference */
     unsigned seed;              /* 0 or 1: the reference's stream */
     int stop_after_half_sweeps; /* -1: the whole table */

@@ -63,3 +63,23 @@ def test_tf32x3_heff_matches_fp64_at_d1024(ctx):
     # the same rounding every call (fixed summation order)
     _, got2, _ = _compare(ctx, h64, h3, psi, step.psi_dim)
     assert np.array_equal(got, got2)
+
+
+@pytest.mark.parametrize("call", [20, 158])
+def test_mixed_precision_lanczos_matches_reference(ctx, call):
+    """A DMRG_PREC_TF32X3 operator runs the Lanczos first on split-precision
+    matvecs, then the FP64 Lanczos from that vector: the energy and the state
+    meet the FP64 parity bar (|dE|/site <= 1e-12, overlap 1 - 1e-9)."""
+    from dmrgcc_b200.problem import read_nac
+    step = SiteStep.from_nac(os.path.join(GOLD, f"heff_c{call}.nac"))
+    ref = read_nac(os.path.join(GOLD, f"lanczos_c{call}.nac"))
+    niter = int(read_nac(os.path.join(GOLD, f"heff_c{call}.nac"))["niter"][0])
+    L = capi.DeviceArray.from_host(ctx, step.L_data)
+    R = capi.DeviceArray.from_host(ctx, step.R_data)
+    h = capi.Heff(ctx, step.site, step.L, step.R, precision=capi.DMRG_PREC_TF32X3)
+    h.set_env(L, R)
+    psi = capi.DeviceArray.from_host(ctx, step.ket_data)
+    e, dim = h.lanczos(psi, niter)
+    assert abs(e - float(ref["energy"][0])) / 16 <= 1e-12
+    v = psi.download()
+    assert 1.0 - abs(float(v @ np.asarray(ref["lattice.ket.data"]))) <= 1e-9
