@@ -10,8 +10,10 @@ synthetic values.  A step = one matvec.
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
                     [--precision fp64]
 
-The line also carries `sweep`: the wall time of one whole DMRG run of the same
-cylinder input (8 sweeps, D up to 1024) through dmrg_run_execute (N=1 only).
+The line also carries `split`: the same matvec through a DMRG_PREC_TF32X3
+operator (tcgen05 tensor cores), its time and its error against the FP64 result;
+and `sweep`: the wall time of one whole DMRG run of the same cylinder input (8
+sweeps, D up to 1024) through dmrg_run_execute (N=1 only).
 
 Multi-GPU: replicas only (each rank runs its own matvec; no collective on the
 data path); value = all ranks' FLOPs / max-over-ranks time.
@@ -126,6 +128,43 @@ def run_reference(args) -> None:
         "e2e": {"value": tflops, "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
+
+
+def split_form(ctx, step, psi, L, R, out_ref, steps: int, flush, stream) -> dict:
+    """The same matvec through a DMRG_PREC_TF32X3 operator (tcgen05 tensor cores,
+    TF32 hi/lo splits): per-step time with the same L2 flush, and its error
+    against the FP64 result on the same vectors."""
+    import numpy as np
+    import torch
+
+    from dmrgcc_b200 import capi
+
+    h3 = capi.Heff(ctx, step.site, step.L, step.R, precision=capi.DMRG_PREC_TF32X3)
+    h3.set_env(L, R)
+    out = capi.DeviceArray(ctx, step.psi_dim)
+    for _ in range(3):
+        h3.apply(psi, out, accumulate=False)
+    ctx.sync()
+    got = out.download()
+    ref = out_ref.download()
+    rel = float(np.max(np.abs(got - ref)) / np.max(np.abs(ref)))
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    torch.cuda.synchronize()
+    for e0, e1 in evs:
+        flush.zero()
+        e0.record(stream)
+        h3.apply(psi, out, accumulate=False)
+        e1.record(stream)
+    torch.cuda.synchronize()
+    ctx.sync()  # reports a tensor-core wait that gave up
+    ms = sum(e0.elapsed_time(e1) for e0, e1 in evs) / steps
+    alg, _ = h3.flops()
+    prof = [h3.profile(psi, out) for _ in range(3)]
+    return {"precision": "tf32x3", "value": alg / (ms * 1e-3) * 1e-12, "unit": "TFLOP/s", "ms_per_step": ms,
+            "speedup_vs_fp64": None, "max_rel_err_vs_fp64": rel,
+            "stage_ms": {"stage_a_with_psi_packing": float(np.mean([p[0] for p in prof])),
+                         "stage_b": float(np.mean([p[1] for p in prof]))},
+            "kernel": "gemm_tf32x3_kernel (tcgen05.mma kind::tf32, 3 products, FP32 accumulation in TMEM)"}
 
 
 def sweep_time(ctx) -> dict:
@@ -260,7 +299,9 @@ def run_b200(args) -> None:
                        "gflop_per_step_algorithmic": alg_flops * 1e-9, "gflop_per_step_executed": exec_flops * 1e-9,
                        "l2": "256 MiB write between timed steps (outside the per-step CUDA-event pair)",
                        "parallelism": f"replicas x{world}"},
-            "gpu_launches": 2 * args.steps,
+            # per matvec: stage A grouped GEMM, stage B grouped GEMM, stage B split-K reduce
+            # (this structure splits its longest stage-B groups; see the ncu launch list)
+            "gpu_launches": 3 * args.steps,
             "e2e": {"value": e2e_value, "unit": "TFLOP/s", "h2d_bytes_per_step": step.psi_dim * 8,
                     "d2h_bytes_per_step": step.psi_dim * 8,
                     "note": "dmrg_heff_apply_host: pinned psi in, matvec, result out, sync; environments resident"},
@@ -273,6 +314,11 @@ def run_b200(args) -> None:
             },
             "clocks": clk.summary(),
         }
+        if args.precision == "fp64" and not args.no_split:
+            ref_out = capi.DeviceArray(ctx, step.psi_dim)
+            heff.apply(psi, ref_out, accumulate=False)
+            line["split"] = split_form(ctx, step, psi, L, R, ref_out, min(args.steps, 500), flush, stream)
+            line["split"]["speedup_vs_fp64"] = ms_per_step / line["split"]["ms_per_step"]
         if world == 1 and not args.no_sweep:
             line["sweep"] = sweep_time(ctx)
         cpu = cpu_reference(args.cpu_reps, 1, os.cpu_count() or 1) if not args.no_cpu else {"unavailable": "skipped"}
@@ -300,6 +346,7 @@ def main() -> int:
     ap.add_argument("--cpu-reps", type=int, default=30)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-sweep", action="store_true", help="skip the whole-run sweep-time measurement")
+    ap.add_argument("--no-split", action="store_true", help="skip the TF32X3 form of the matvec")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

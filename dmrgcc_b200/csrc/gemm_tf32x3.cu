@@ -13,7 +13,8 @@
 // no-swizzle layout (see gemm.cuh).  A GEMM stage is then two contiguous bulk
 // copies (cp.async.bulk, no multicast) of 32 KB (A) and 16 KB (B).
 //
-// GEMM (one CTA per 128 x 64 output tile, 192 threads, warp-specialised):
+// GEMM (persistent: one CTA per SM walks 128 x 64 output tiles, 192 threads,
+// warp-specialised; stage counters and the accumulator pair run on across tiles):
 //   warp 0 lane 0   producer: per stage waits the stage's "empty" barrier, arms
 //                   the "full" barrier with the byte count, issues the copies;
 //   warp 1 lane 0   MMA issuer: per stage waits "full", issues 4 k-substeps x 3
@@ -188,13 +189,11 @@ __global__ void __launch_bounds__(NT, 1) gemm_tf32x3_kernel(const unsigned char*
                                                             unsigned char* __restrict__ t_out,
                                                             const PackedTerm* __restrict__ terms,
                                                             const PackedGroup* __restrict__ groups,
-                                                            const PackedTile* __restrict__ tiles, int accumulate,
-                                                            int out_mode, int* __restrict__ status) {
+                                                            const PackedTile* __restrict__ tiles, int ntiles,
+                                                            int accumulate, int out_mode, int* __restrict__ status) {
     extern __shared__ __align__(1024) unsigned char smem[];
     Bars& B = *reinterpret_cast<Bars*>(smem + BAR_OFF);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const PackedTile tile = tiles[blockIdx.x];
-    const PackedGroup g = groups[tile.group];
 
     if (warp == 1) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&B.tmem)),
@@ -223,6 +222,9 @@ __global__ void __launch_bounds__(NT, 1) gemm_tf32x3_kernel(const unsigned char*
         // ---- producer ----
         if (lane == 0) {
             int it = 0;
+            for (int tt = blockIdx.x; tt < ntiles && ok; tt += gridDim.x) {
+            const PackedTile tile = tiles[tt];
+            const PackedGroup g = groups[tile.group];
             for (int t = g.t0; t < g.t1 && ok; ++t) {
                 const PackedTerm tm = terms[t];
                 const unsigned char* a = a_imgs + tm.a_img + (int64_t)tile.pm * tm.slices * kImageA;
@@ -239,6 +241,7 @@ __global__ void __launch_bounds__(NT, 1) gemm_tf32x3_kernel(const unsigned char*
                     bulk_g2s(dst + kImageA, b + (int64_t)s * kImageB, kImageB, &B.full[st]);
                 }
             }
+            }
             // Tail: nothing asynchronous may still target this CTA's shared memory
             // when it exits.  Wait until the copies of the last stages have landed
             // and until the MMAs that read them have completed and their commits
@@ -254,6 +257,8 @@ __global__ void __launch_bounds__(NT, 1) gemm_tf32x3_kernel(const unsigned char*
         // ---- MMA issuer ----
         if (lane == 0) {
             int it = 0, ti = 0;
+            for (int tt = blockIdx.x; tt < ntiles && ok; tt += gridDim.x) {
+            const PackedGroup g = groups[tiles[tt].group];
             for (int t = g.t0; t < g.t1 && ok; ++t, ++ti) {
                 const int acc = ti & 1;
                 if (ti >= 2 && !mbar_wait(&B.acce[acc], ((ti >> 1) - 1) & 1)) {
@@ -287,15 +292,19 @@ __global__ void __launch_bounds__(NT, 1) gemm_tf32x3_kernel(const unsigned char*
                 if (!ok) break;
                 mma_commit(&B.accf[acc]);      // the term's accumulator is complete
             }
+            }
         }
     } else {
         // ---- epilogue: warps 2..5 ----
         const int quarter = warp & 3;
         const int row = quarter * 32 + lane;  // tile row = TMEM lane
+        int ti = 0;
+        for (int tt = blockIdx.x; tt < ntiles && ok; tt += gridDim.x) {
+        const PackedTile tile = tiles[tt];
+        const PackedGroup g = groups[tile.group];
         double sum[TN];
 #pragma unroll
         for (int j = 0; j < TN; ++j) sum[j] = 0.0;
-        int ti = 0;
         for (int t = g.t0; t < g.t1; ++t, ++ti) {
             const int acc = ti & 1;
             const bool got = mbar_wait(&B.accf[acc], (ti >> 1) & 1);
@@ -350,6 +359,7 @@ __global__ void __launch_bounds__(NT, 1) gemm_tf32x3_kernel(const unsigned char*
                     }
                 }
             }
+        }
         }
     }
     __syncwarp();  // producer and MMA warps: lanes 1..31 wait for lane 0
@@ -497,9 +507,15 @@ int launch_gemm_tf32x3(const PackedSchedule& s, const unsigned char* a_imgs, con
         DMRG_CUDA_TRY(cudaFuncSetAttribute(gemm_tf32x3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
         attr = true;
     }
-    gemm_tf32x3_kernel<<<(int)s.tiles.size(), NT, SMEM_BYTES, stream>>>(
+    // persistent: one CTA per SM walks the (cost-sorted) tiles round-robin; its
+    // stage ring and accumulator pair carry over from one tile to the next
+    int dev = 0, sms = 148;
+    DMRG_CUDA_TRY(cudaGetDevice(&dev));
+    DMRG_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const int ntiles = (int)s.tiles.size();
+    gemm_tf32x3_kernel<<<std::min(ntiles, sms), NT, SMEM_BYTES, stream>>>(
         a_imgs, b_imgs, C, s.aux.as<double>(), t_out, s.d_terms.as<PackedTerm>(), s.d_groups.as<PackedGroup>(),
-        s.d_tiles.as<PackedTile>(), accumulate ? 1 : 0, s.out_mode, status);
+        s.d_tiles.as<PackedTile>(), ntiles, accumulate ? 1 : 0, s.out_mode, status);
     if (!s.splits.empty()) {
         int64_t biggest = 0;
         for (const GemmSplit& sp : s.splits) biggest = std::max<int64_t>(biggest, (int64_t)sp.m * sp.n);
