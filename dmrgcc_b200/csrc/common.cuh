@@ -143,4 +143,7 @@ struct dmrg_ctx_s {
     int num_sms = 148;
     // Device-side error word: kernels with iteration caps write a nonzero code.
     int* d_status = nullptr;
+    // Pinned host words for small per-iteration device->host reads (Lanczos
+    // convergence flags); one context is used by one host thread at a time.
+    int* h_pinned = nullptr;
 };

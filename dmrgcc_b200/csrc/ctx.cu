@@ -135,6 +135,13 @@ int dmrg_ctx_create(int device, dmrg_ctx_t* out) {
         return set_error(DMRG_E_NOMEM, "cudaMalloc status: %s", cudaGetErrorString(e));
     }
     cudaMemset(c->d_status, 0, sizeof(int) * 16);
+    e = cudaMallocHost(&c->h_pinned, sizeof(int) * 64);
+    if (e != cudaSuccess) {
+        cudaFree(c->d_status);
+        cudaStreamDestroy(c->own_stream);
+        delete c;
+        return set_error(DMRG_E_NOMEM, "cudaMallocHost: %s", cudaGetErrorString(e));
+    }
     *out = c;
     return DMRG_OK;
 }
@@ -144,6 +151,7 @@ int dmrg_ctx_destroy(dmrg_ctx_t ctx) {
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
     cudaFree(ctx->d_status);
+    cudaFreeHost(ctx->h_pinned);
     cudaStreamDestroy(ctx->own_stream);
     delete ctx;
     return DMRG_OK;

@@ -1077,12 +1077,18 @@ int Engine::LanczosMethod(int niter, int site, double& energy, int& dim) {
     std::vector<dmrg_blocks_t> lb = env_blocks(c.L.desc), rb = env_blocks(c.R.desc);
     dmrg_blocks_t kb = as_blocks(t.ket.d);
     dmrg_heff_t h = nullptr;
+    const double t0 = wall_time();
     DMRG_TRY(dmrg_heff_create(ctx_, t.nl(), t.nr(), t.phys.data(), &kb, W.get_physics_dim(), W.get_left_bond(),
                               W.get_right_bond(), W.data().data(), lb.data(), rb.data(), opt_.precision, &h));
     int rc = dmrg_heff_set_env(h, c.L.ptr(), c.R.ptr());
+    const double t1 = wall_time();
     if (rc == DMRG_OK)
         rc = dmrg_lanczos(h, t.ket.ptr(), niter, opt_.lanczos_precision, opt_.zero_tolerance, &energy, &dim);
+    const double t2 = wall_time();
     dmrg_heff_destroy(h);
+    if (trace_)  // set-up / solve / tear-down times of this call
+        std::fprintf(trace_, "L %d %.3f %.3f %.3f %d\n", site, 1e3 * (t1 - t0), 1e3 * (t2 - t1),
+                     1e3 * (wall_time() - t2), dim);
     return rc;
 }
 

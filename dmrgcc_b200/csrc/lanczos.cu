@@ -31,11 +31,8 @@ struct LanczosWork {
     int64_t n = 0;
     DeviceBuffer V, h, scal, state, jac, y, dense;
     ReduceScratch rs;
-    int* h_state = nullptr;  // pinned: [done, dim]
+    int* h_state = nullptr;  // the context's pinned words: [done, dim, ...]
     int split_iters = 0;     // Krylov dimension of the last split-precision phase
-    ~LanczosWork() {
-        if (h_state) cudaFreeHost(h_state);
-    }
 };
 
 }  // namespace dmrg
@@ -84,7 +81,7 @@ int ensure_work(dmrg_heff_s& h, int niter) {
     }
     DMRG_TRY(w.state.alloc(16 * sizeof(int)));
     DMRG_TRY(w.rs.alloc(std::max(2 * h.ctx->num_sms, 64), std::max(niter, 1)));
-    if (!w.h_state) DMRG_CUDA_TRY(cudaMallocHost(&w.h_state, 16 * sizeof(int)));
+    w.h_state = h.ctx->h_pinned;
     return DMRG_OK;
 }
 

@@ -50,7 +50,7 @@ def parse_trace(path):
     with open(path) as f:
         for line in f:
             p = line.split()
-            if not p or p[0] == "Y":
+            if not p or p[0] in ("Y", "L"):  # expansion blocks, Lanczos timings: diagnostics
                 continue
             if p[0] == "E":
                 rows.append(("E", f"{p[2]} {p[3]}", float(p[4]), None))
