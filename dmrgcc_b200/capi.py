@@ -77,6 +77,7 @@ _SIGS = {
     "dmrg_canon_write": (C.c_int, [_VP, _VP, _VP, _VP]),
     "dmrg_quicksort_index": (C.c_int, [_D, _I, C.c_int, C.c_int]),
     "dmrg_truncate_dims": (C.c_int, [C.c_int, _I, _D, C.c_int, C.c_double, _I]),
+    "dmrg_rand_stream": (C.c_int, [C.c_uint, C.c_int, _I]),
     "dmrg_run_create": (C.c_int, [_VP, C.c_char_p, C.c_char_p, _VP, C.POINTER(_VP)]),
     "dmrg_run_execute": (C.c_int, [_VP]),
     "dmrg_run_destroy": (C.c_int, [_VP]),

@@ -2,6 +2,7 @@
 #include <vector>
 
 #include "dmrg_b200.h"
+#include "host/grand.h"
 #include "truncate.h"
 
 namespace dmrg {
@@ -9,6 +10,13 @@ int set_error(int code, const char* fmt, ...);
 }
 
 extern "C" {
+
+int dmrg_rand_stream(unsigned seed, int n, int* out) {
+    if (n < 0 || (n > 0 && !out)) return dmrg::set_error(DMRG_E_ARG, "invalid arguments");
+    dmrg::GlibcRand rng(seed);
+    for (int i = 0; i < n; ++i) out[i] = rng.next();
+    return DMRG_OK;
+}
 
 int dmrg_quicksort_index(double* values, int* index, int n, int descending) {
     if (n < 0 || (n > 0 && (!values || !index))) return dmrg::set_error(DMRG_E_ARG, "invalid quicksort arguments");

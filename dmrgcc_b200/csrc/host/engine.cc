@@ -35,13 +35,12 @@ dmrg_blocks_t as_blocks(const BlockListDesc& b) {
 }
 
 // RealMatrix::RandomMatrix (src/tensor/real_matrix.cc:201-208): column-major
-// draws of 0.01 * (rand() % 100) into a rows x cols row-major block.
-long long g_rand_draws = 0;  // rand() draws made by engines in this process (trace output)
-
-void random_block(std::vector<double>& out, size_t off, int rows, int cols) {
-    g_rand_draws += (long long)rows * cols;
+// draws of 0.01 * (rand() % 100) into a rows x cols row-major block; `draws`
+// counts them (trace output).
+void random_block(GlibcRand& rng, long long& draws, std::vector<double>& out, size_t off, int rows, int cols) {
+    draws += (long long)rows * cols;
     for (int j = 0; j < cols; ++j)
-        for (int i = 0; i < rows; ++i) out[off + (size_t)i * cols + j] = 0.01 * (rand() % 100);
+        for (int i = 0; i < rows; ++i) out[off + (size_t)i * cols + j] = 0.01 * (rng.next() % 100);
 }
 
 int find_value(const std::vector<int>& v, int x) {
@@ -113,8 +112,8 @@ Engine::Engine(dmrg_ctx_t ctx, std::unique_ptr<QuantumSpace> space, std::unique_
         lat_[i].reset(new TensorLattice());
         lat_[i]->physics_dim = space_->physics_dim();
     }
-    srand(opt_.seed);
-    g_rand_draws = 0;
+    rng_.seed_with(opt_.seed);
+    rand_draws_ = 0;
     int rc = DefineTensorSpace(first_block_, first_dim_);
     if (rc != DMRG_OK) throw std::runtime_error(std::string("DefineTensorSpace: ") + dmrg_last_error());
     ham_->DefineTensorHamiltonian();
@@ -159,7 +158,7 @@ void Engine::Trace(const char* tag, int leigh, int site) {
     fetch(t.ket, h);
     double norm2 = 0.0;
     for (double v : h) norm2 += v * v;
-    std::fprintf(trace_, " P:%lld N:%.10e Q:%lld", (long long)t.psi_dim(), norm2, g_rand_draws);
+    std::fprintf(trace_, " P:%lld N:%.10e Q:%lld", (long long)t.psi_dim(), norm2, rand_draws_);
     if (tag[0] == 'C' && t.has_canonical) {  // per-block squared norms of S V^T (or U S)
         fetch(t.canonical, h);
         std::fprintf(trace_, " S:");
@@ -231,7 +230,7 @@ int Engine::DefineLatticeBlocks(TensorLattice& t, const std::vector<int>& li, co
         t.ket.d.push(li[k], ri[k], row, column);
     }
     std::vector<double> host((size_t)std::max<int64_t>(t.ket.d.size, 0));
-    for (size_t k = 0; k < li.size(); ++k) random_block(host, (size_t)t.ket.d.off[k], row, column);
+    for (size_t k = 0; k < li.size(); ++k) random_block(rng_, rand_draws_, host, (size_t)t.ket.d.off[k], row, column);
     DMRG_TRY(t.ket.alloc(st_, false));
     if (!host.empty())
         DMRG_CUDA_TRY(cudaMemcpyAsync(t.ket.ptr(), host.data(), host.size() * sizeof(double), cudaMemcpyHostToDevice,
@@ -716,7 +715,7 @@ int Engine::LeftExpanTensorContraction(int site, const std::vector<std::vector<i
                     if (el == 0.0) continue;
                     const int64_t ro = (int64_t)rnd.size();
                     rnd.resize(rnd.size() + (size_t)d0 * d1);
-                    random_block(rnd, ro, d0, d1);
+                    random_block(rng_, rand_draws_, rnd, ro, d0, d1);
                     for (int q = 0; q < std::min(d0, d1); ++q) rnd[ro + (size_t)q * d1 + q] = 0.1 * el;
                     if (fidx < 0) {
                         fidx = (int)firsts.size();
@@ -883,7 +882,7 @@ int Engine::RightExpanTensorContraction(int site, const std::vector<std::vector<
                     if (el == 0.0) continue;
                     const int64_t ro = (int64_t)rnd.size();
                     rnd.resize(rnd.size() + (size_t)d0 * d1);
-                    random_block(rnd, ro, d0, d1);
+                    random_block(rng_, rand_draws_, rnd, ro, d0, d1);
                     for (int q = 0; q < std::min(d0, d1); ++q) rnd[ro + (size_t)q * d1 + q] = 0.1 * el;
                     if (fidx < 0) {
                         fidx = (int)firsts.size();

@@ -15,6 +15,7 @@
 #include "blockops.cuh"
 #include "blocksparse.h"
 #include "common.cuh"
+#include "host/grand.h"
 #include "host/input.h"
 #include "host/model.h"
 #include "vec.cuh"
@@ -157,6 +158,8 @@ private:
     int half_sweep_ = 0;
     int lanczos_calls_ = 0;
     FILE* trace_ = nullptr;  // DMRG_TRACE=<file>: structure trace, one line per step operation
+    GlibcRand rng_;          // the reference's rand() stream (seeded with opt.seed)
+    long long rand_draws_ = 0;
 };
 
 }  // namespace dmrg

@@ -194,29 +194,32 @@ __global__ void __launch_bounds__(kThreads) solve_kernel(const SvdProblem* __res
                 S.pq[2 * threadIdx.x + 1] = b;
             }
             __syncthreads();
-            for (int idx = threadIdx.x; idx < (kPair / 2) * kPair; idx += kThreads) {
-                const int i = idx / kPair, j = idx % kPair;
-                const double s = S.cs[2 * i + 1];
-                if (s == 0.0) continue;
-                const double c = S.cs[2 * i];
-                const int a = S.pq[2 * i], b = S.pq[2 * i + 1];
-                const double ga = S.G[a * kLd + j], gb = S.G[b * kLd + j];
-                S.G[a * kLd + j] = c * ga - s * gb;
-                S.G[b * kLd + j] = s * ga + c * gb;
+            // G <- J^T G J in one pass: every 2x2 block (rows of pair i, columns of
+            // pair j) gets both rotations at once; Q <- Q J
+            for (int idx = threadIdx.x; idx < (kPair / 2) * (kPair / 2); idx += kThreads) {
+                const int i = idx / (kPair / 2), j = idx % (kPair / 2);
+                const double si = S.cs[2 * i + 1], sj = S.cs[2 * j + 1];
+                if (si == 0.0 && sj == 0.0) continue;
+                const double ci = S.cs[2 * i], cj = S.cs[2 * j];
+                const int ai = S.pq[2 * i], bi = S.pq[2 * i + 1], aj = S.pq[2 * j], bj = S.pq[2 * j + 1];
+                const double x11 = S.G[ai * kLd + aj], x12 = S.G[ai * kLd + bj];
+                const double x21 = S.G[bi * kLd + aj], x22 = S.G[bi * kLd + bj];
+                const double y11 = ci * x11 - si * x21, y12 = ci * x12 - si * x22;  // rows
+                const double y21 = si * x11 + ci * x21, y22 = si * x12 + ci * x22;
+                S.G[ai * kLd + aj] = cj * y11 - sj * y12;                            // columns
+                S.G[ai * kLd + bj] = sj * y11 + cj * y12;
+                S.G[bi * kLd + aj] = cj * y21 - sj * y22;
+                S.G[bi * kLd + bj] = sj * y21 + cj * y22;
             }
-            __syncthreads();
             for (int idx = threadIdx.x; idx < (kPair / 2) * kPair; idx += kThreads) {
-                const int i = idx / kPair, row = idx % kPair;
-                const double s = S.cs[2 * i + 1];
-                if (s == 0.0) continue;
-                const double c = S.cs[2 * i];
-                const int a = S.pq[2 * i], b = S.pq[2 * i + 1];
-                const double ga = S.G[row * kLd + a], gb = S.G[row * kLd + b];
-                S.G[row * kLd + a] = c * ga - s * gb;
-                S.G[row * kLd + b] = s * ga + c * gb;
+                const int j = idx / kPair, row = idx % kPair;
+                const double sj = S.cs[2 * j + 1];
+                if (sj == 0.0) continue;
+                const double cj = S.cs[2 * j];
+                const int a = S.pq[2 * j], b = S.pq[2 * j + 1];
                 const double qa = S.Q[row * kLd + a], qb = S.Q[row * kLd + b];
-                S.Q[row * kLd + a] = c * qa - s * qb;
-                S.Q[row * kLd + b] = s * qa + c * qb;
+                S.Q[row * kLd + a] = cj * qa - sj * qb;
+                S.Q[row * kLd + b] = sj * qa + cj * qb;
             }
             __syncthreads();
         }

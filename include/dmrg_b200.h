@@ -268,6 +268,10 @@ int dmrg_model_quantum_table(dmrg_model_t m, int which, int bond, int cap, int* 
 int dmrg_quicksort_index(double* values, int* index, int n, int descending);
 int dmrg_truncate_dims(int nsec, const int* counts, double* values, int max_dim, double canpre,
                        int* tdim_out);
+/* dmrg_rand_stream: the first n values of the stream that srand(seed) + rand()
+ * give with glibc (the reference's random source: RandomMatrix,
+ * src/tensor/real_matrix.cc:201-208), from the engine's own generator. */
+int dmrg_rand_stream(unsigned seed, int n, int* out);
 
 #ifdef __cplusplus
 }
