@@ -130,16 +130,16 @@ def run_reference(args) -> None:
     print(json.dumps(line))
 
 
-def split_form(ctx, step, psi, L, R, out_ref, steps: int, flush, stream) -> dict:
-    """The same matvec through a DMRG_PREC_TF32X3 operator (tcgen05 tensor cores,
-    TF32 hi/lo splits): per-step time with the same L2 flush, and its error
-    against the FP64 result on the same vectors."""
+def split_form(ctx, step, psi, L, R, out_ref, steps: int, flush, stream, prec: int, name: str) -> dict:
+    """The same matvec through a split-precision operator (tcgen05 tensor cores,
+    TF32 or BF16 hi/lo parts): per-step time with the same L2 flush, and its
+    error against the FP64 result on the same vectors."""
     import numpy as np
     import torch
 
     from dmrgcc_b200 import capi
 
-    h3 = capi.Heff(ctx, step.site, step.L, step.R, precision=capi.DMRG_PREC_TF32X3)
+    h3 = capi.Heff(ctx, step.site, step.L, step.R, precision=prec)
     h3.set_env(L, R)
     out = capi.DeviceArray(ctx, step.psi_dim)
     for _ in range(3):
@@ -160,11 +160,12 @@ def split_form(ctx, step, psi, L, R, out_ref, steps: int, flush, stream) -> dict
     ms = sum(e0.elapsed_time(e1) for e0, e1 in evs) / steps
     alg, _ = h3.flops()
     prof = [h3.profile(psi, out) for _ in range(3)]
-    return {"precision": "tf32x3", "value": alg / (ms * 1e-3) * 1e-12, "unit": "TFLOP/s", "ms_per_step": ms,
+    return {"precision": name, "value": alg / (ms * 1e-3) * 1e-12, "unit": "TFLOP/s", "ms_per_step": ms,
             "speedup_vs_fp64": None, "max_rel_err_vs_fp64": rel,
             "stage_ms": {"stage_a_with_psi_packing": float(np.mean([p[0] for p in prof])),
                          "stage_b": float(np.mean([p[1] for p in prof]))},
-            "kernel": "gemm_tf32x3_kernel (tcgen05.mma kind::tf32, 3 products, FP32 accumulation in TMEM)"}
+            "kernel": "gemm_split_kernel (tcgen05.mma kind::%s, 3 products, FP32 accumulation in TMEM)"
+                      % ("f16 on bf16" if name == "bf16x3" else "tf32")}
 
 
 def sweep_time(ctx) -> dict:
@@ -218,7 +219,8 @@ def run_b200(args) -> None:
     assert ctx.stream == stream.cuda_stream != 0
 
     step = SiteStep.from_nac(STRUCT)
-    prec = {"fp64": capi.DMRG_PREC_FP64, "tf32x3": capi.DMRG_PREC_TF32X3}[args.precision]
+    prec = {"fp64": capi.DMRG_PREC_FP64, "tf32x3": capi.DMRG_PREC_TF32X3,
+            "bf16x3": capi.DMRG_PREC_BF16X3}[args.precision]
     heff = capi.Heff(ctx, step.site, step.L, step.R, precision=prec)
     psi, L, R = step.synthetic_device(ctx, seed=SEED + rank)
     heff.set_env(L, R)
@@ -293,7 +295,7 @@ def run_b200(args) -> None:
         line = {
             "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "tf32x3 (f32 accumulate, f64 storage)",
+            "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else args.precision + " (f32 accumulate per term, f64 sums)",
             "data": "synthetic (seeded splitmix64 values on the reference's own D=1024 block structure)",
             "config": {"workload": WORKLOAD, "precision": args.precision, "psi_dim": step.psi_dim,
                        "gflop_per_step_algorithmic": alg_flops * 1e-9, "gflop_per_step_executed": exec_flops * 1e-9,
@@ -317,8 +319,10 @@ def run_b200(args) -> None:
         if args.precision == "fp64" and not args.no_split:
             ref_out = capi.DeviceArray(ctx, step.psi_dim)
             heff.apply(psi, ref_out, accumulate=False)
-            line["split"] = split_form(ctx, step, psi, L, R, ref_out, min(args.steps, 500), flush, stream)
-            line["split"]["speedup_vs_fp64"] = ms_per_step / line["split"]["ms_per_step"]
+            line["split"] = [split_form(ctx, step, psi, L, R, ref_out, min(args.steps, 500), flush, stream, p, n)
+                             for p, n in ((capi.DMRG_PREC_TF32X3, "tf32x3"), (capi.DMRG_PREC_BF16X3, "bf16x3"))]
+            for sp in line["split"]:
+                sp["speedup_vs_fp64"] = ms_per_step / sp["ms_per_step"]
         if world == 1 and not args.no_sweep:
             line["sweep"] = sweep_time(ctx)
         cpu = cpu_reference(args.cpu_reps, 1, os.cpu_count() or 1) if not args.no_cpu else {"unavailable": "skipped"}
@@ -342,7 +346,7 @@ def main() -> int:
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    ap.add_argument("--precision", choices=["fp64", "tf32x3"], default="fp64")
+    ap.add_argument("--precision", choices=["fp64", "tf32x3", "bf16x3"], default="fp64")
     ap.add_argument("--cpu-reps", type=int, default=30)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-sweep", action="store_true", help="skip the whole-run sweep-time measurement")

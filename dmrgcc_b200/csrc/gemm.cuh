@@ -106,19 +106,24 @@ int launch_gemm_f64(const GemmSchedule& s, const double* A, const double* B, dou
                     bool accumulate, cudaStream_t stream);
 
 // ---------------------------------------------------------------------------
-// Split-precision (TF32X3) path on the tcgen05 tensor cores (gemm_tf32x3.cu).
+// Split-precision paths on the tcgen05 tensor cores (gemm_split.cu).
 //
 // Operands are packed once into "images": for an operand block X (rows x k,
-// K-major), image (panel p, slice s) holds rows [p*R, p*R+R) x k [32 s, 32 s+32)
-// as a TF32 hi plane followed by a TF32 lo plane (x ~ hi + lo, x rounded to FP32
-// first), each in the tcgen05 canonical K-major no-swizzle layout: byte offset of
-// (row r, k) = (k/4)*16R + (r/8)*128 + (r%8)*16 + (k%4)*4.  Zero outside X.
+// K-major), image (panel p, slice s) holds rows [p*R, p*R+R) x one k slice as a
+// hi plane followed by a lo plane (x ~ hi + lo), each in the tcgen05 canonical
+// K-major no-swizzle layout: 128 bytes of k per row in 16-byte chunks, byte
+// offset of (row r, k) = (k*E / 16)*16R + (r/8)*128 + (r%8)*16 + (k*E)%16 for
+// E-byte elements.  Zero outside X.  Two formats share this geometry:
+//   TF32 (E = 4): x rounded to FP32, hi = tf32(x), lo = tf32(x - hi); 32 k per slice;
+//   BF16 (E = 2): hi = bf16(x), lo = bf16(x - hi); 64 k per slice.
 // R = 128 for the A role (output rows), 64 for the B role (output columns).
 // A GEMM stage then is two contiguous bulk copies (32 KB + 16 KB).
-constexpr int kPackK = 32;
+constexpr int kFmtTF32 = 0, kFmtBF16 = 1;
+constexpr int kPackRowBytes = 128;
 constexpr int kPackRowsA = 128, kPackRowsB = 64;
-constexpr int kImageA = 2 * kPackRowsA * kPackK * 4;  // bytes: hi + lo
-constexpr int kImageB = 2 * kPackRowsB * kPackK * 4;
+constexpr int kImageA = 2 * kPackRowsA * kPackRowBytes;  // bytes: hi + lo
+constexpr int kImageB = 2 * kPackRowsB * kPackRowBytes;
+inline int pack_k(int fmt) { return fmt == kFmtBF16 ? 64 : 32; }  // k per slice
 
 struct PackJob {
     int64_t src_off;  // doubles
@@ -126,12 +131,15 @@ struct PackJob {
     int rows, k, ld;  // logical X: rows x k; X(r, c) = src[src_off + (trans ? c*ld + r : r*ld + c)]
     int trans;
     int prow;         // rows per panel (kPackRowsA or kPackRowsB)
-    int slices;       // ceil(k / 32)
+    int slices;       // ceil(k / pack_k(fmt))
+    int fmt;          // kFmtTF32 or kFmtBF16
+    int pad_;
 };
 struct PackImage {
     int job, panel, slice, pad_;
 };
 struct PackSchedule {
+    int fmt = kFmtTF32;
     std::vector<PackJob> jobs;
     std::vector<PackImage> images;
     int64_t bytes = 0;
@@ -145,7 +153,7 @@ int launch_pack(const PackSchedule& p, const double* src, unsigned char* dst, cu
 
 struct PackedTerm {
     int64_t a_img, b_img;  // image offsets (bytes) of the A operand (A role) and the B operand (B role)
-    int slices;            // ceil(k / 32), the same for both
+    int slices;            // ceil(k / pack_k(fmt)), the same for both
     int pad_;
     double w;              // weight of this product
 };
@@ -156,13 +164,14 @@ struct PackedGroup {
     int ldc;
     int cbuf;              // 1: split-K chunk, written to aux
     int64_t t_img;         // output mode 1: the output written as B-role images (rows = columns n,
-    int t_slices;          // k = rows m) for a following packed GEMM; t_slices = ceil(m / 32)
+    int t_slices;          // k = rows m) for a following packed GEMM; t_slices = ceil(m / pack_k(fmt))
     int pad_;
 };
 struct PackedTile {
     int group, pm, pn, cost;
 };
 struct PackedSchedule {
+    int fmt = kFmtTF32;
     std::vector<PackedTerm> terms;
     std::vector<PackedGroup> groups;
     int out_mode = 0;  // 0: FP64 output blocks, 1: B-role images
@@ -186,9 +195,9 @@ struct PackedSchedule {
     // (num_sms > 0), uploads.
     int finalize(cudaStream_t stream, int num_sms = 0);
 };
-// C (+)= the products of every group (mode 0), or t_out <- images of them (mode 1).
-// A wait that gives up sets *status = DMRG_E_NUMERIC (device word).
-int launch_gemm_tf32x3(const PackedSchedule& s, const unsigned char* a_imgs, const unsigned char* b_imgs,
+// C (+)= the products of every group (mode 0), or t_out <- images of them (mode 1),
+// in the schedule's format.  A wait that gives up sets *status = DMRG_E_NUMERIC.
+int launch_gemm_split(const PackedSchedule& s, const unsigned char* a_imgs, const unsigned char* b_imgs,
                        double* C, unsigned char* t_out, bool accumulate, int* status, cudaStream_t stream);
 
 }  // namespace dmrg

@@ -1,12 +1,14 @@
 // Split-precision grouped multi-term block GEMM on the 5th-generation tensor
 // cores (tcgen05, accumulators in tensor memory), on packed operand images.
 //
-// Arithmetic: every FP64 operand is rounded to FP32 and split into TF32 parts,
-// x ~ hi + lo; each product is taken as hi*hi + hi*lo + lo*hi (the lo*lo term,
-// ~2^-22 relative, is dropped) by three kind::tf32 MMAs into an FP32 accumulator
-// in tensor memory.  Each term's accumulator is read out and added, scaled by
-// the term's weight, into FP64 registers, so the terms of a block sum
-// accumulate in FP64.  Relative error of a block sum ~1e-6.
+// Arithmetic: every FP64 operand is split into two parts of a narrow format,
+// x ~ hi + lo, and each product is taken as hi*hi + hi*lo + lo*hi (the lo*lo
+// term is dropped) by three MMAs into an FP32 accumulator in tensor memory:
+//   TF32: kind::tf32 MMAs, x rounded to FP32 first; block sums to ~1e-6;
+//   BF16: kind::f16 MMAs on bf16 parts (half the bytes, twice the math rate);
+//         ~16 bits per operand, block sums to ~1e-5.
+// Each term's accumulator is read out and added, scaled by the term's weight,
+// into FP64 registers, so the terms of a block sum accumulate in FP64.
 //
 // Packing (launch_pack): one CTA per image writes the hi/lo planes of one
 // (panel, 32-wide k slice) of an operand block in the tcgen05 canonical K-major
@@ -35,12 +37,12 @@
 namespace dmrg {
 namespace {
 
-constexpr int TM = kPackRowsA, TN = kPackRowsB, TK = kPackK;
+constexpr int TM = kPackRowsA, TN = kPackRowsB;
 constexpr int NSTAGE = 4;
 constexpr int STAGE_BYTES = kImageA + kImageB;               // 48 KB
 constexpr int LBO_A = TM * 16, LBO_B = TN * 16;              // bytes between 16-byte k chunks
 constexpr int SBO = 128;                                     // bytes between 8-row groups
-constexpr int PLANE_A = TM * TK * 4, PLANE_B = TN * TK * 4;  // hi plane; lo follows
+constexpr int PLANE_A = TM * kPackRowBytes, PLANE_B = TN * kPackRowBytes;  // hi plane; lo follows
 constexpr int NT = 192;
 constexpr int BAR_OFF = NSTAGE * STAGE_BYTES;
 constexpr int SMEM_BYTES = BAR_OFF + 256;
@@ -61,16 +63,29 @@ __device__ __forceinline__ uint64_t make_smem_desc(uint32_t saddr, uint32_t lbo,
     return d;
 }
 
-// Instruction descriptor: D = F32, A = B = TF32, both K-major, N = 64, M = 128.
-constexpr uint32_t IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(TN >> 3) << 17) |
-                           ((uint32_t)(TM >> 4) << 24);
+// Instruction descriptor: D = F32, A = B = TF32 (format 2) or BF16 (format 1),
+// both K-major, N = 64, M = 128.
+template <int FMT>
+__host__ __device__ constexpr uint32_t idesc() {
+    return (1u << 4) | ((FMT == kFmtBF16 ? 1u : 2u) << 7) | ((FMT == kFmtBF16 ? 1u : 2u) << 10) |
+           ((uint32_t)(TN >> 3) << 17) | ((uint32_t)(TM >> 4) << 24);
+}
 
-__device__ __forceinline__ void mma_tf32(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t acc) {
-    asm volatile(
-        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
-        "l"(a), "l"(b), "r"(IDESC), "r"(acc)
-        : "memory");
+// One MMA of 32 bytes of k (8 tf32 or 16 bf16 per row).
+template <int FMT>
+__device__ __forceinline__ void mma_split(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t acc) {
+    if constexpr (FMT == kFmtBF16)
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+            "l"(a), "l"(b), "r"(idesc<FMT>()), "r"(acc)
+            : "memory");
+    else
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+            "l"(a), "l"(b), "r"(idesc<FMT>()), "r"(acc)
+            : "memory");
 }
 
 __device__ __forceinline__ void mma_commit(uint64_t* bar) {
@@ -133,6 +148,38 @@ __device__ __forceinline__ void split(double v, uint32_t& hi, uint32_t& lo) {
     lo = tf32_bits(f - __uint_as_float(hi));
 }
 
+// bf16 parts (round to nearest even): hi = bf16(x), lo = bf16(x - hi)
+__device__ __forceinline__ uint16_t bf16_bits(float x) {
+    uint16_t r;
+    asm("cvt.rn.bf16.f32 %0, %1;" : "=h"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ void split_bf16(double v, uint16_t& hi, uint16_t& lo) {
+    const float f = (float)v;
+    hi = bf16_bits(f);
+    lo = bf16_bits(f - __uint_as_float((uint32_t)hi << 16));
+}
+
+// Stores the split parts of v at (row r, k) of an image with `rows` rows per panel.
+__device__ __forceinline__ void put_split(unsigned char* img, int rows, int r, int k, double v, int fmt) {
+    const int plane = rows * kPackRowBytes;
+    if (fmt == kFmtBF16) {
+        const int kb = k * 2;
+        const int off = (kb >> 4) * (rows * 16) + (r >> 3) * 128 + (r & 7) * 16 + (kb & 15);
+        uint16_t h, l;
+        split_bf16(v, h, l);
+        *reinterpret_cast<uint16_t*>(img + off) = h;
+        *reinterpret_cast<uint16_t*>(img + plane + off) = l;
+    } else {
+        const int kb = k * 4;
+        const int off = (kb >> 4) * (rows * 16) + (r >> 3) * 128 + (r & 7) * 16 + (kb & 15);
+        uint32_t h, l;
+        split(v, h, l);
+        *reinterpret_cast<uint32_t*>(img + off) = h;
+        *reinterpret_cast<uint32_t*>(img + plane + off) = l;
+    }
+}
+
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
@@ -145,34 +192,24 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
         : "r"(taddr));
 }
 
-// byte offset of (row r, k) inside one plane with `rows` rows per panel
-__device__ __forceinline__ int plane_off(int r, int k, int rows) {
-    return (k >> 2) * (rows * 16) + (r >> 3) * 128 + (r & 7) * 16 + (k & 3) * 4;
-}
-
 // ---- packing: one CTA (128 threads) per image ----------------------------------
 __global__ void __launch_bounds__(128) pack_kernel(const PackJob* __restrict__ jobs, const PackImage* __restrict__ imgs,
                                                    const double* __restrict__ src, unsigned char* __restrict__ dst) {
     const PackImage im = imgs[blockIdx.x];
     const PackJob j = jobs[im.job];
-    const int img_bytes = 2 * j.prow * TK * 4;
+    const int img_bytes = 2 * j.prow * kPackRowBytes;
+    const int tk = j.fmt == kFmtBF16 ? 64 : 32;
     unsigned char* out = dst + j.img_off + ((int64_t)im.panel * j.slices + im.slice) * img_bytes;
-    uint32_t* hi = reinterpret_cast<uint32_t*>(out);
-    uint32_t* lo = reinterpret_cast<uint32_t*>(out + img_bytes / 2);
-    const int r0 = im.panel * j.prow, k0 = im.slice * TK;
+    const int r0 = im.panel * j.prow, k0 = im.slice * tk;
     const double* s = src + j.src_off;
-    for (int idx = threadIdx.x; idx < j.prow * TK; idx += blockDim.x) {
+    for (int idx = threadIdx.x; idx < j.prow * tk; idx += blockDim.x) {
         // consecutive threads: consecutive k for row-major X, consecutive rows for transposed X
-        const int r = j.trans ? idx % j.prow : idx / TK;
-        const int k = j.trans ? idx / j.prow : idx % TK;
+        const int r = j.trans ? idx % j.prow : idx / tk;
+        const int k = j.trans ? idx / j.prow : idx % tk;
         double v = 0.0;
         if (r0 + r < j.rows && k0 + k < j.k)
             v = j.trans ? s[(int64_t)(k0 + k) * j.ld + (r0 + r)] : s[(int64_t)(r0 + r) * j.ld + (k0 + k)];
-        uint32_t h, l;
-        split(v, h, l);
-        const int off = plane_off(r, k, j.prow) >> 2;
-        hi[off] = h;
-        lo[off] = l;
+        put_split(out, j.prow, r, k, v, j.fmt);
     }
 }
 
@@ -183,7 +220,8 @@ struct Bars {
 };
 static_assert(sizeof(Bars) <= 256, "barrier block");
 
-__global__ void __launch_bounds__(NT, 1) gemm_tf32x3_kernel(const unsigned char* __restrict__ a_imgs,
+template <int FMT>
+__global__ void __launch_bounds__(NT, 1) gemm_split_kernel(const unsigned char* __restrict__ a_imgs,
                                                             const unsigned char* __restrict__ b_imgs,
                                                             double* __restrict__ C, double* __restrict__ Caux,
                                                             unsigned char* __restrict__ t_out,
@@ -278,14 +316,14 @@ __global__ void __launch_bounds__(NT, 1) gemm_tf32x3_kernel(const unsigned char*
                     const uint32_t a_base = smem_u32(smem + st * STAGE_BYTES);
                     const uint32_t b_base = a_base + kImageA;
 #pragma unroll
-                    for (int ks = 0; ks < TK / 8; ++ks) {
+                    for (int ks = 0; ks < kPackRowBytes / 32; ++ks) {  // 32 bytes of k per MMA
                         const uint64_t ahi = make_smem_desc(a_base + 2 * ks * LBO_A, LBO_A, SBO);
                         const uint64_t alo = make_smem_desc(a_base + PLANE_A + 2 * ks * LBO_A, LBO_A, SBO);
                         const uint64_t bhi = make_smem_desc(b_base + 2 * ks * LBO_B, LBO_B, SBO);
                         const uint64_t blo = make_smem_desc(b_base + PLANE_B + 2 * ks * LBO_B, LBO_B, SBO);
-                        mma_tf32(d, ahi, bhi, (s > 0 || ks > 0) ? 1u : 0u);
-                        mma_tf32(d, ahi, blo, 1u);
-                        mma_tf32(d, alo, bhi, 1u);
+                        mma_split<FMT>(d, ahi, bhi, (s > 0 || ks > 0) ? 1u : 0u);
+                        mma_split<FMT>(d, ahi, blo, 1u);
+                        mma_split<FMT>(d, alo, bhi, 1u);
                     }
                     mma_commit(&B.empty[st]);  // the stage's buffer is free once these MMAs are done
                 }
@@ -342,20 +380,15 @@ __global__ void __launch_bounds__(NT, 1) gemm_tf32x3_kernel(const unsigned char*
             } else {
                 // the output as B-role images of X = output^T (rows = columns of the
                 // output, k = rows of the output); zeros in the padding
-                const int slice = grow / TK;
+                constexpr int tk = FMT == kFmtBF16 ? 64 : 32;
+                const int slice = grow / tk;
                 if (slice < g.t_slices) {
                     unsigned char* img = t_out + g.t_img + ((int64_t)tile.pn * g.t_slices + slice) * kImageB;
-                    uint32_t* hi = reinterpret_cast<uint32_t*>(img);
-                    uint32_t* lo = reinterpret_cast<uint32_t*>(img + PLANE_B);
-                    const int k = grow % TK;
+                    const int k = grow % tk;
 #pragma unroll
                     for (int j = 0; j < TN; ++j) {
                         const int col = tile.pn * TN + j;
-                        uint32_t h = 0, l = 0;
-                        if (grow < g.m && col < g.n) split(sum[j], h, l);
-                        const int off = plane_off(j, k, TN) >> 2;
-                        hi[off] = h;
-                        lo[off] = l;
+                        put_split(img, TN, j, k, (grow < g.m && col < g.n) ? sum[j] : 0.0, FMT);
                     }
                 }
             }
@@ -388,7 +421,9 @@ __global__ void __launch_bounds__(256) split_reduce_tf32_kernel(double* __restri
 }  // namespace
 
 int64_t PackSchedule::add(int64_t src_off, int rows, int k, int ld, bool trans, int prow) {
+    const int tk = pack_k(fmt);
     PackJob j{};
+    j.fmt = fmt;
     j.src_off = src_off;
     j.img_off = bytes;
     j.rows = rows;
@@ -396,13 +431,13 @@ int64_t PackSchedule::add(int64_t src_off, int rows, int k, int ld, bool trans, 
     j.ld = ld;
     j.trans = trans ? 1 : 0;
     j.prow = prow;
-    j.slices = (k + TK - 1) / TK;
+    j.slices = (k + tk - 1) / tk;
     const int panels = (rows + prow - 1) / prow;
     const int job = (int)jobs.size();
     jobs.push_back(j);
     for (int p = 0; p < panels; ++p)
         for (int s = 0; s < j.slices; ++s) images.push_back(PackImage{job, p, s, 0});
-    bytes += (int64_t)panels * j.slices * 2 * prow * TK * 4;
+    bytes += (int64_t)panels * j.slices * 2 * prow * kPackRowBytes;
     return j.img_off;
 }
 
@@ -491,7 +526,8 @@ int PackedSchedule::check_bounds(int64_t a_bytes, int64_t b_bytes, int64_t c_siz
             if (g.c_off < 0 || g.c_off + (int64_t)(g.m - 1) * g.ldc + g.n > c_size || g.n > g.ldc)
                 return set_error(DMRG_E_ARG, "packed GEMM output %lld outside %lld", (long long)g.c_off,
                                  (long long)c_size);
-        } else if (g.t_img < 0 || g.t_img + pn * g.t_slices * kImageB > t_bytes || (int64_t)g.t_slices * TK < g.m ||
+        } else if (g.t_img < 0 || g.t_img + pn * g.t_slices * kImageB > t_bytes ||
+                   (int64_t)g.t_slices * pack_k(fmt) < g.m ||
                    g.t_img % 16) {
             return set_error(DMRG_E_ARG, "packed GEMM output images outside their buffer");
         }
@@ -499,23 +535,34 @@ int PackedSchedule::check_bounds(int64_t a_bytes, int64_t b_bytes, int64_t c_siz
     return DMRG_OK;
 }
 
-int launch_gemm_tf32x3(const PackedSchedule& s, const unsigned char* a_imgs, const unsigned char* b_imgs, double* C,
-                       unsigned char* t_out, bool accumulate, int* status, cudaStream_t stream) {
-    if (s.tiles.empty()) return DMRG_OK;
+namespace {
+template <int FMT>
+int launch_fmt(const PackedSchedule& s, const unsigned char* a_imgs, const unsigned char* b_imgs, double* C,
+               unsigned char* t_out, bool accumulate, int* status, int grid, cudaStream_t stream) {
     static bool attr = false;
     if (!attr) {
-        DMRG_CUDA_TRY(cudaFuncSetAttribute(gemm_tf32x3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
+        DMRG_CUDA_TRY(
+            cudaFuncSetAttribute(gemm_split_kernel<FMT>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
         attr = true;
     }
+    gemm_split_kernel<FMT><<<grid, NT, SMEM_BYTES, stream>>>(
+        a_imgs, b_imgs, C, s.aux.as<double>(), t_out, s.d_terms.as<PackedTerm>(), s.d_groups.as<PackedGroup>(),
+        s.d_tiles.as<PackedTile>(), (int)s.tiles.size(), accumulate ? 1 : 0, s.out_mode, status);
+    return DMRG_OK;
+}
+}  // namespace
+
+int launch_gemm_split(const PackedSchedule& s, const unsigned char* a_imgs, const unsigned char* b_imgs, double* C,
+                      unsigned char* t_out, bool accumulate, int* status, cudaStream_t stream) {
+    if (s.tiles.empty()) return DMRG_OK;
     // persistent: one CTA per SM walks the (cost-sorted) tiles round-robin; its
     // stage ring and accumulator pair carry over from one tile to the next
     int dev = 0, sms = 148;
     DMRG_CUDA_TRY(cudaGetDevice(&dev));
     DMRG_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    const int ntiles = (int)s.tiles.size();
-    gemm_tf32x3_kernel<<<std::min(ntiles, sms), NT, SMEM_BYTES, stream>>>(
-        a_imgs, b_imgs, C, s.aux.as<double>(), t_out, s.d_terms.as<PackedTerm>(), s.d_groups.as<PackedGroup>(),
-        s.d_tiles.as<PackedTile>(), ntiles, accumulate ? 1 : 0, s.out_mode, status);
+    const int grid = std::min((int)s.tiles.size(), sms);
+    if (s.fmt == kFmtBF16) DMRG_TRY(launch_fmt<kFmtBF16>(s, a_imgs, b_imgs, C, t_out, accumulate, status, grid, stream));
+    else DMRG_TRY(launch_fmt<kFmtTF32>(s, a_imgs, b_imgs, C, t_out, accumulate, status, grid, stream));
     if (!s.splits.empty()) {
         int64_t biggest = 0;
         for (const GemmSplit& sp : s.splits) biggest = std::max<int64_t>(biggest, (int64_t)sp.m * sp.n);

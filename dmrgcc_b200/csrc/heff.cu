@@ -129,14 +129,17 @@ int build_heff(dmrg_heff_s& h) {
     cudaStream_t st = h.ctx->stream;
     DMRG_TRY(h.sa.finalize(64, 64, 16, st));
     DMRG_TRY(h.sb.finalize(64, 64, 16, st, h.ctx->num_sms));
-    if (h.precision == DMRG_PREC_TF32X3) {
+    if (is_split(h.precision)) {
+        const int fmt = split_fmt(h.precision);
+        h.pk_psi.fmt = h.pk_L.fmt = h.pk_R.fmt = h.pa.fmt = h.pb.fmt = fmt;
         // operand images: psi blocks and L blocks in the A role, R blocks (transposed)
         // in the B role, and the K*R intermediates written directly as B-role images
         std::vector<int64_t> psi_img(ket.count());
         for (int pos = 0; pos < ket.count(); ++pos)
             psi_img[pos] = h.pk_psi.add(ket.off[pos], ket.rows[pos], ket.cols[pos], ket.cols[pos], false, kPackRowsA);
         std::map<int64_t, int64_t> r_img, l_img;
-        auto slices = [](int k) { return (k + kPackK - 1) / kPackK; };
+        const int tk = pack_k(fmt);
+        auto slices = [tk](int k) { return (k + tk - 1) / tk; };
         std::vector<int64_t> t_img(tasks.size());
         h.pa.reset();
         h.pa.out_mode = 1;
@@ -208,16 +211,16 @@ int dmrg::heff_apply_fp64(dmrg_heff_s& h, const double* psi, double* out, bool a
 }
 
 int dmrg::heff_apply_internal(dmrg_heff_s& h, const double* psi, double* out, bool accumulate) {
-    if (h.precision != DMRG_PREC_TF32X3) return heff_apply_fp64(h, psi, out, accumulate);
+    if (!is_split(h.precision)) return heff_apply_fp64(h, psi, out, accumulate);
     if ((!h.L_dev && h.L.size) || (!h.R_dev && h.R.size))
         return set_error(DMRG_E_STATE, "dmrg_heff_set_env was not called");
     cudaStream_t st = h.ctx->stream;
     if (!accumulate && h.site.ket.size)
         DMRG_CUDA_TRY(cudaMemsetAsync(out, 0, (size_t)h.site.ket.size * sizeof(double), st));
     DMRG_TRY(launch_pack(h.pk_psi, psi, h.img_psi.as<unsigned char>(), st));
-    DMRG_TRY(launch_gemm_tf32x3(h.pa, h.img_psi.as<unsigned char>(), h.img_R.as<unsigned char>(), nullptr,
+    DMRG_TRY(launch_gemm_split(h.pa, h.img_psi.as<unsigned char>(), h.img_R.as<unsigned char>(), nullptr,
                                 h.img_T.as<unsigned char>(), false, h.ctx->d_status, st));
-    DMRG_TRY(launch_gemm_tf32x3(h.pb, h.img_L.as<unsigned char>(), h.img_T.as<unsigned char>(), out, nullptr, true,
+    DMRG_TRY(launch_gemm_split(h.pb, h.img_L.as<unsigned char>(), h.img_T.as<unsigned char>(), out, nullptr, true,
                                 h.ctx->d_status, st));
     return DMRG_OK;
 }
@@ -228,8 +231,8 @@ int dmrg_heff_create(dmrg_ctx_t ctx, int nl, int nr, const int* phys, const dmrg
                      int rb, const double* W, const dmrg_blocks_t* L, const dmrg_blocks_t* R, int precision,
                      dmrg_heff_t* out) {
     if (!ctx || !out || !L || !R) return set_error(DMRG_E_ARG, "null argument");
-    if (precision != DMRG_PREC_FP64 && precision != DMRG_PREC_TF32X3)
-        return set_error(DMRG_E_ARG, "unsupported precision %d (DMRG_PREC_FP64 or DMRG_PREC_TF32X3)", precision);
+    if (precision != DMRG_PREC_FP64 && !is_split(precision))
+        return set_error(DMRG_E_ARG, "unsupported precision %d (DMRG_PREC_FP64, _TF32X3 or _BF16X3)", precision);
     *out = nullptr;
     DMRG_CUDA_TRY(cudaSetDevice(ctx->device));
     auto* h = new dmrg_heff_s();
@@ -272,7 +275,7 @@ int dmrg_heff_set_env(dmrg_heff_t h, const double* L_dev, const double* R_dev) {
     if ((!L_dev && h->L.size) || (!R_dev && h->R.size)) return set_error(DMRG_E_ARG, "null environment pointer");
     h->L_dev = L_dev;
     h->R_dev = R_dev;
-    if (h->precision == DMRG_PREC_TF32X3) {  // environment images, kept until the next call
+    if (is_split(h->precision)) {  // environment images, kept until the next call
         DMRG_TRY(launch_pack(h->pk_L, L_dev, h->img_L.as<unsigned char>(), h->ctx->stream));
         DMRG_TRY(launch_pack(h->pk_R, R_dev, h->img_R.as<unsigned char>(), h->ctx->stream));
     }
@@ -291,20 +294,20 @@ int dmrg_heff_profile(dmrg_heff_t h, const double* psi, double* out, double* ms_
     cudaStream_t st = h->ctx->stream;
     cudaEvent_t ev[3];
     for (auto& e : ev) DMRG_CUDA_TRY(cudaEventCreate(&e));
-    const bool split = h->precision == DMRG_PREC_TF32X3;
+    const bool split = is_split(h->precision);
     DMRG_CUDA_TRY(cudaEventRecord(ev[0], st));
     int rc = DMRG_OK;
     if (split) {  // stage A includes packing psi
         rc = launch_pack(h->pk_psi, psi, h->img_psi.as<unsigned char>(), st);
         if (rc == DMRG_OK)
-            rc = launch_gemm_tf32x3(h->pa, h->img_psi.as<unsigned char>(), h->img_R.as<unsigned char>(), nullptr,
+            rc = launch_gemm_split(h->pa, h->img_psi.as<unsigned char>(), h->img_R.as<unsigned char>(), nullptr,
                                     h->img_T.as<unsigned char>(), false, h->ctx->d_status, st);
     } else {
         rc = launch_gemm_f64(h->sa, psi, h->R_dev, h->T.as<double>(), false, st);
     }
     cudaEventRecord(ev[1], st);
     if (rc == DMRG_OK)
-        rc = split ? launch_gemm_tf32x3(h->pb, h->img_L.as<unsigned char>(), h->img_T.as<unsigned char>(), out,
+        rc = split ? launch_gemm_split(h->pb, h->img_L.as<unsigned char>(), h->img_T.as<unsigned char>(), out,
                                         nullptr, true, h->ctx->d_status, st)
                    : launch_gemm_f64(h->sb, h->L_dev, h->T.as<double>(), out, true, st);
     cudaEventRecord(ev[2], st);
@@ -333,7 +336,7 @@ int dmrg_heff_apply_host(dmrg_heff_t h, const double* psi_host, double* out_host
     DMRG_TRY(dmrg_heff_apply(h, h->io_psi.as<double>(), h->io_out.as<double>(), accumulate));
     if (bytes) DMRG_CUDA_TRY(cudaMemcpyAsync(out_host, h->io_out.ptr, bytes, cudaMemcpyDeviceToHost, st));
     DMRG_CUDA_TRY(cudaStreamSynchronize(st));
-    if (h->precision == DMRG_PREC_TF32X3) return take_device_status(h->ctx);  // bounded tensor-core waits
+    if (is_split(h->precision)) return take_device_status(h->ctx);  // bounded tensor-core waits
     return DMRG_OK;
 }
 

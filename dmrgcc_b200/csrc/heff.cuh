@@ -15,7 +15,8 @@ struct dmrg_heff_s {
     dmrg::SiteDesc site;
     dmrg::EnvDesc L, R;
     dmrg::GemmSchedule sa, sb;    // A: psi x R -> T ; B: L x T -> out (FP64 tiles)
-    // DMRG_PREC_TF32X3 only: split-precision operand images and packed schedules
+    // split precisions (DMRG_PREC_TF32X3 / DMRG_PREC_BF16X3) only: operand images
+    // and packed schedules
     dmrg::PackSchedule pk_psi, pk_L, pk_R;     // which blocks to pack, where
     dmrg::PackedSchedule pa, pb;               // A: psi x R -> T images ; B: L x T -> out
     dmrg::DeviceBuffer img_psi, img_L, img_R, img_T;
@@ -31,6 +32,8 @@ struct dmrg_heff_s {
 };
 
 namespace dmrg {
+inline bool is_split(int precision) { return precision == DMRG_PREC_TF32X3 || precision == DMRG_PREC_BF16X3; }
+inline int split_fmt(int precision) { return precision == DMRG_PREC_BF16X3 ? kFmtBF16 : kFmtTF32; }
 // out (+)= H_eff psi on the context stream, in the operator's precision.
 int heff_apply_internal(dmrg_heff_s& h, const double* psi, double* out, bool accumulate);
 // out (+)= H_eff psi in FP64 whatever the operator's precision.

@@ -62,8 +62,8 @@ int dmrg_run_create(dmrg_ctx_t ctx, const char* input_path, const char* model, c
         RunOptions o;
         if (opt) {
             o.precision = opt->precision;
-            if (o.precision != DMRG_PREC_FP64 && o.precision != DMRG_PREC_TF32X3)
-                return set_error(DMRG_E_ARG, "unsupported precision %d (DMRG_PREC_FP64 or DMRG_PREC_TF32X3)",
+            if (o.precision != DMRG_PREC_FP64 && o.precision != DMRG_PREC_TF32X3 && o.precision != DMRG_PREC_BF16X3)
+                return set_error(DMRG_E_ARG, "unsupported precision %d (DMRG_PREC_FP64, _TF32X3 or _BF16X3)",
                                  o.precision);
             o.verbose = opt->verbose;
             o.seed = opt->seed ? opt->seed : 1;

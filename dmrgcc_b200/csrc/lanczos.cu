@@ -14,7 +14,7 @@
 // psi_dim < 100 takes the reference's exact-diagonalisation branch (:34-56):
 // the dense H_eff is assembled column by column from matvecs on unit vectors
 // and diagonalised by a device Jacobi solver.
-// DMRG_PREC_TF32X3 operators: a first Krylov run with tensor-core split-precision
+// Split-precision operators (DMRG_PREC_TF32X3 / _BF16X3): a first Krylov run with tensor-core
 // matvecs, then the FP64 run above from its Ritz vector (FP64 for the dense
 // branch, the recurrence, reorthogonalisation, the tridiagonal problem and the
 // energy).
@@ -181,7 +181,7 @@ extern "C" int dmrg_lanczos(dmrg_heff_t hp, double* psi, int niter, double preci
         if (iters) *iters = 0;
         return run_exact(h, psi, energy);
     }
-    if (h.precision != DMRG_PREC_TF32X3) return krylov(h, psi, niter, precision, zero_tol, false, energy, iters);
+    if (!is_split(h.precision)) return krylov(h, psi, niter, precision, zero_tol, false, energy, iters);
     // Mixed precision: a Krylov run on split-precision matvecs until the Ritz
     // value settles at the split arithmetic's resolution, then the FP64 run of
     // the reference from that Ritz vector, which fixes the energy and the state.

@@ -38,11 +38,11 @@ extern "C" {
 #define DMRG_E_STATE (-5)    /* call made in the wrong state */
 
 /* Arithmetic of the block GEMMs.  FP64: plain double (FP64 tensor path).
- * TF32X3: 5th-generation tensor cores (tcgen05): every FP64 operand is rounded
- * to FP32 and split into TF32 hi + lo parts, each product is taken as
- * hi*hi + hi*lo + lo*hi with FP32 accumulation in tensor memory, and results are
- * stored as FP64 (relative error ~1e-6 of a block sum).  BF16X3 is reserved and
- * rejected. */
+ * TF32X3 / BF16X3: 5th-generation tensor cores (tcgen05): every FP64 operand is
+ * split into hi + lo parts (TF32 after rounding to FP32, or BF16), each product
+ * is taken as hi*hi + hi*lo + lo*hi with FP32 accumulation in tensor memory,
+ * the terms of a block sum are added in FP64 and results are stored as FP64
+ * (relative error of a block sum ~1e-6 for TF32X3, ~1e-5 for BF16X3). */
 #define DMRG_PREC_FP64 0
 #define DMRG_PREC_BF16X3 1
 #define DMRG_PREC_TF32X3 2

@@ -1,8 +1,9 @@
-"""Split-precision H_eff*psi (DMRG_PREC_TF32X3, tcgen05 tensor cores with TF32
-hi/lo splits and FP32 accumulation) against the FP64 path on the same operator
-and vectors.  The products drop the lo*lo term (~2^-22 relative) and round each
-operand to FP32 first, and the block sums accumulate in FP32, so the bound is
-relative to the largest output: max |TF32X3 - FP64| <= 2e-5 * max |FP64|."""
+"""Split-precision H_eff*psi on the tcgen05 tensor cores against the FP64 path
+on the same operator and vectors.  DMRG_PREC_TF32X3 (TF32 hi/lo parts of each
+operand rounded to FP32, FP32 accumulation per term): max |split - FP64| <=
+2e-5 * max |FP64|.  DMRG_PREC_BF16X3 (bf16 hi/lo parts, ~16 bits per operand):
+<= 2e-4 * max |FP64|.  Both drop the lo*lo product and add the terms of a block
+sum in FP64."""
 import os
 
 import numpy as np
@@ -13,12 +14,13 @@ from dmrgcc_b200.problem import SiteStep
 
 pytestmark = pytest.mark.gpu
 GOLD = os.path.join(os.path.dirname(__file__), "golden")
-TOL = 2e-5
+TOLS = {capi.DMRG_PREC_TF32X3: 2e-5, capi.DMRG_PREC_BF16X3: 2e-4}
+SPLITS = [capi.DMRG_PREC_TF32X3, capi.DMRG_PREC_BF16X3]
 
 
-def _pair(ctx, step, L, R):
+def _pair(ctx, step, L, R, split):
     hs = []
-    for prec in (capi.DMRG_PREC_FP64, capi.DMRG_PREC_TF32X3):
+    for prec in (capi.DMRG_PREC_FP64, split):
         h = capi.Heff(ctx, step.site, step.L, step.R, precision=prec)
         h.set_env(L, R)
         hs.append(h)
@@ -38,11 +40,13 @@ def _compare(ctx, h64, h3, psi, n):
     return ref, got, err
 
 
-def test_tf32x3_heff_matches_fp64_on_reference_operator(ctx):
+@pytest.mark.parametrize("split", SPLITS)
+def test_split_heff_matches_fp64_on_reference_operator(ctx, split):
+    TOL = TOLS[split]
     step = SiteStep.from_nac(os.path.join(GOLD, "heff_c158.nac"))
     L = capi.DeviceArray.from_host(ctx, step.L_data)
     R = capi.DeviceArray.from_host(ctx, step.R_data)
-    h64, h3 = _pair(ctx, step, L, R)
+    h64, h3 = _pair(ctx, step, L, R, split)
     psi = capi.DeviceArray.from_host(ctx, step.ket_data)
     ref, got, err = _compare(ctx, h64, h3, psi, step.psi_dim)
     assert err <= TOL, err
@@ -54,10 +58,12 @@ def test_tf32x3_heff_matches_fp64_on_reference_operator(ctx):
     assert np.max(np.abs(out.download() - 2 * ref)) <= 2 * TOL * np.max(np.abs(ref))
 
 
-def test_tf32x3_heff_matches_fp64_at_d1024(ctx):
+@pytest.mark.parametrize("split", SPLITS)
+def test_split_heff_matches_fp64_at_d1024(ctx, split):
+    TOL = TOLS[split]
     step = SiteStep.from_nac(os.path.join(GOLD, "heff_struct_cyl8x4_D1024.nac"))
     psi, L, R = step.synthetic_device(ctx, seed=11)
-    h64, h3 = _pair(ctx, step, L, R)
+    h64, h3 = _pair(ctx, step, L, R, split)
     ref, got, err = _compare(ctx, h64, h3, psi, step.psi_dim)
     assert err <= TOL, err
     # the same rounding every call (fixed summation order)
@@ -65,9 +71,10 @@ def test_tf32x3_heff_matches_fp64_at_d1024(ctx):
     assert np.array_equal(got, got2)
 
 
+@pytest.mark.parametrize("split", SPLITS)
 @pytest.mark.parametrize("call", [20, 158])
-def test_mixed_precision_lanczos_matches_reference(ctx, call):
-    """A DMRG_PREC_TF32X3 operator runs the Lanczos first on split-precision
+def test_mixed_precision_lanczos_matches_reference(ctx, call, split):
+    """A split-precision operator runs the Lanczos first on split-precision
     matvecs, then the FP64 Lanczos from that vector: the energy and the state
     meet the FP64 parity bar (|dE|/site <= 1e-12, overlap 1 - 1e-9)."""
     from dmrgcc_b200.problem import read_nac
@@ -76,7 +83,7 @@ def test_mixed_precision_lanczos_matches_reference(ctx, call):
     niter = int(read_nac(os.path.join(GOLD, f"heff_c{call}.nac"))["niter"][0])
     L = capi.DeviceArray.from_host(ctx, step.L_data)
     R = capi.DeviceArray.from_host(ctx, step.R_data)
-    h = capi.Heff(ctx, step.site, step.L, step.R, precision=capi.DMRG_PREC_TF32X3)
+    h = capi.Heff(ctx, step.site, step.L, step.R, precision=split)
     h.set_env(L, R)
     psi = capi.DeviceArray.from_host(ctx, step.ket_data)
     e, dim = h.lanczos(psi, niter)
