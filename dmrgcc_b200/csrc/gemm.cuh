@@ -111,9 +111,12 @@ int launch_gemm_f64(const GemmSchedule& s, const double* A, const double* B, dou
 // Operands are packed once into "images": for an operand block X (rows x k,
 // K-major), image (panel p, slice s) holds rows [p*R, p*R+R) x one k slice as a
 // hi plane followed by a lo plane (x ~ hi + lo), each in the tcgen05 canonical
-// K-major no-swizzle layout: 128 bytes of k per row in 16-byte chunks, byte
-// offset of (row r, k) = (k*E / 16)*16R + (r/8)*128 + (r%8)*16 + (k*E)%16 for
-// E-byte elements.  Zero outside X.  Two formats share this geometry:
+// K-major no-swizzle layout: 128 bytes of k per row in 16-byte chunks; a core
+// matrix is 8 rows x 16 bytes, the 8 chunks of an 8-row group are contiguous
+// (LBO = 128) and groups follow each other (SBO = 1024), so the first m rows of
+// a plane are one contiguous prefix: byte offset of (row r, k) =
+// (r/8)*1024 + (k*E/16)*128 + (r%8)*16 + (k*E)%16 for E-byte elements.  Zero
+// outside X.  Two formats share this geometry:
 //   TF32 (E = 4): x rounded to FP32, hi = tf32(x), lo = tf32(x - hi); 32 k per slice;
 //   BF16 (E = 2): hi = bf16(x), lo = bf16(x - hi); 64 k per slice.
 // R = 128 for the A role (output rows), 64 for the B role (output columns).

@@ -12,8 +12,9 @@
 //
 // Packing (launch_pack): one CTA per image writes the hi/lo planes of one
 // (panel, 32-wide k slice) of an operand block in the tcgen05 canonical K-major
-// no-swizzle layout (see gemm.cuh).  A GEMM stage is then two contiguous bulk
-// copies (cp.async.bulk, no multicast) of 32 KB (A) and 16 KB (B).
+// no-swizzle layout (see gemm.cuh).  A GEMM stage is then one bulk copy
+// (cp.async.bulk, no multicast) per plane of each operand, covering only the
+// rows of the tile that hold data.
 //
 // GEMM (persistent: one CTA per SM walks 128 x 64 output tiles, 192 threads,
 // warp-specialised; stage counters and the accumulator pair run on across tiles):
@@ -40,8 +41,8 @@ namespace {
 constexpr int TM = kPackRowsA, TN = kPackRowsB;
 constexpr int NSTAGE = 4;
 constexpr int STAGE_BYTES = kImageA + kImageB;               // 48 KB
-constexpr int LBO_A = TM * 16, LBO_B = TN * 16;              // bytes between 16-byte k chunks
-constexpr int SBO = 128;                                     // bytes between 8-row groups
+constexpr int LBO = 128;   // bytes between the 16-byte k chunks of one 8-row core-matrix group
+constexpr int SBO = 1024;  // bytes between 8-row groups: a group's 8 chunks are contiguous
 constexpr int PLANE_A = TM * kPackRowBytes, PLANE_B = TN * kPackRowBytes;  // hi plane; lo follows
 constexpr int NT = 192;
 constexpr int BAR_OFF = NSTAGE * STAGE_BYTES;
@@ -50,7 +51,7 @@ constexpr uint32_t TMEM_COLS = 128;                          // two 64-column ac
 constexpr long long kWaitLimit = 4000000;                    // try_wait polls before a wait gives up
 
 static_assert(SMEM_BYTES <= 227 * 1024, "shared memory per CTA");
-static_assert((LBO_A >> 4) < (1 << 14), "LBO fits the descriptor field");
+static_assert((SBO >> 4) < (1 << 14), "SBO fits the descriptor field");
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -165,14 +166,14 @@ __device__ __forceinline__ void put_split(unsigned char* img, int rows, int r, i
     const int plane = rows * kPackRowBytes;
     if (fmt == kFmtBF16) {
         const int kb = k * 2;
-        const int off = (kb >> 4) * (rows * 16) + (r >> 3) * 128 + (r & 7) * 16 + (kb & 15);
+        const int off = (r >> 3) * SBO + (kb >> 4) * LBO + (r & 7) * 16 + (kb & 15);
         uint16_t h, l;
         split_bf16(v, h, l);
         *reinterpret_cast<uint16_t*>(img + off) = h;
         *reinterpret_cast<uint16_t*>(img + plane + off) = l;
     } else {
         const int kb = k * 4;
-        const int off = (kb >> 4) * (rows * 16) + (r >> 3) * 128 + (r & 7) * 16 + (kb & 15);
+        const int off = (r >> 3) * SBO + (kb >> 4) * LBO + (r & 7) * 16 + (kb & 15);
         uint32_t h, l;
         split(v, h, l);
         *reinterpret_cast<uint32_t*>(img + off) = h;
@@ -263,6 +264,13 @@ __global__ void __launch_bounds__(NT, 1) gemm_split_kernel(const unsigned char* 
             for (int tt = blockIdx.x; tt < ntiles && ok; tt += gridDim.x) {
             const PackedTile tile = tiles[tt];
             const PackedGroup g = groups[tile.group];
+            // Only the image rows that hold data are copied (rounded up to a core
+            // matrix of 8 rows, which the layout keeps contiguous): one bulk copy
+            // per plane.  Rows left stale in shared memory feed only accumulator
+            // rows (A) or columns (B) past the block, which are never stored.
+            const uint32_t ca = (uint32_t)((min(TM, g.m - tile.pm * TM) + 7) & ~7) * kPackRowBytes;
+            const uint32_t cb = (uint32_t)((min(TN, g.n - tile.pn * TN) + 7) & ~7) * kPackRowBytes;
+            const uint32_t tx = 2 * (ca + cb);
             for (int t = g.t0; t < g.t1 && ok; ++t) {
                 const PackedTerm tm = terms[t];
                 const unsigned char* a = a_imgs + tm.a_img + (int64_t)tile.pm * tm.slices * kImageA;
@@ -274,9 +282,13 @@ __global__ void __launch_bounds__(NT, 1) gemm_split_kernel(const unsigned char* 
                         break;
                     }
                     unsigned char* dst = smem + st * STAGE_BYTES;
-                    mbar_arrive_expect_tx(&B.full[st], STAGE_BYTES);
-                    bulk_g2s(dst, a + (int64_t)s * kImageA, kImageA, &B.full[st]);
-                    bulk_g2s(dst + kImageA, b + (int64_t)s * kImageB, kImageB, &B.full[st]);
+                    const unsigned char* as = a + (int64_t)s * kImageA;
+                    const unsigned char* bs = b + (int64_t)s * kImageB;
+                    mbar_arrive_expect_tx(&B.full[st], tx);
+                    bulk_g2s(dst, as, ca, &B.full[st]);
+                    bulk_g2s(dst + PLANE_A, as + PLANE_A, ca, &B.full[st]);
+                    bulk_g2s(dst + kImageA, bs, cb, &B.full[st]);
+                    bulk_g2s(dst + kImageA + PLANE_B, bs + PLANE_B, cb, &B.full[st]);
                 }
             }
             }
@@ -317,10 +329,10 @@ __global__ void __launch_bounds__(NT, 1) gemm_split_kernel(const unsigned char* 
                     const uint32_t b_base = a_base + kImageA;
 #pragma unroll
                     for (int ks = 0; ks < kPackRowBytes / 32; ++ks) {  // 32 bytes of k per MMA
-                        const uint64_t ahi = make_smem_desc(a_base + 2 * ks * LBO_A, LBO_A, SBO);
-                        const uint64_t alo = make_smem_desc(a_base + PLANE_A + 2 * ks * LBO_A, LBO_A, SBO);
-                        const uint64_t bhi = make_smem_desc(b_base + 2 * ks * LBO_B, LBO_B, SBO);
-                        const uint64_t blo = make_smem_desc(b_base + PLANE_B + 2 * ks * LBO_B, LBO_B, SBO);
+                        const uint64_t ahi = make_smem_desc(a_base + 2 * ks * LBO, LBO, SBO);
+                        const uint64_t alo = make_smem_desc(a_base + PLANE_A + 2 * ks * LBO, LBO, SBO);
+                        const uint64_t bhi = make_smem_desc(b_base + 2 * ks * LBO, LBO, SBO);
+                        const uint64_t blo = make_smem_desc(b_base + PLANE_B + 2 * ks * LBO, LBO, SBO);
                         mma_split<FMT>(d, ahi, bhi, (s > 0 || ks > 0) ? 1u : 0u);
                         mma_split<FMT>(d, ahi, blo, 1u);
                         mma_split<FMT>(d, alo, bhi, 1u);
