@@ -180,22 +180,27 @@ struct PackedSchedule {
     int out_mode = 0;  // 0: FP64 output blocks, 1: B-role images
     std::vector<PackedGroup> exec_groups;
     std::vector<GemmSplit> splits;
-    std::vector<PackedTile> tiles;
+    std::vector<PackedTile> tiles;  // grouped by persistent CTA
+    std::vector<int> cta_first;     // CTA c runs tiles [cta_first[c], cta_first[c + 1])
+    int ctas = 0;                   // grid of the persistent launch
     int64_t aux_size = 0;
-    DeviceBuffer d_terms, d_groups, d_tiles, d_splits, aux;
+    DeviceBuffer d_terms, d_groups, d_tiles, d_cta_first, d_splits, aux;
     void reset() {
         terms.clear();
         groups.clear();
         exec_groups.clear();
         splits.clear();
         tiles.clear();
+        cta_first.clear();
+        ctas = 0;
         aux_size = 0;
     }
     // Verifies every image read and every output write against the buffer sizes
     // (bytes for images, doubles for c_size); DMRG_E_ARG, no launch, otherwise.
     int check_bounds(int64_t a_bytes, int64_t b_bytes, int64_t c_size, int64_t t_bytes) const;
-    // Builds tiles (128 x 64 per tile, heaviest first), splits long mode-0 groups
-    // (num_sms > 0), uploads.
+    // Splits long mode-0 groups (num_sms > 0), builds the 128 x 64 tiles and
+    // assigns them to min(tiles, num_sms or 148) persistent CTAs by cost
+    // (longest first, to the least loaded CTA), uploads.
     int finalize(cudaStream_t stream, int num_sms = 0);
 };
 // C (+)= the products of every group (mode 0), or t_out <- images of them (mode 1),

@@ -45,8 +45,14 @@ constexpr int LBO = 128;   // bytes between the 16-byte k chunks of one 8-row co
 constexpr int SBO = 1024;  // bytes between 8-row groups: a group's 8 chunks are contiguous
 constexpr int PLANE_A = TM * kPackRowBytes, PLANE_B = TN * kPackRowBytes;  // hi plane; lo follows
 constexpr int NT = 192;
-constexpr int BAR_OFF = NSTAGE * STAGE_BYTES;
+// Epilogue staging: per epilogue warp 32 rows x 33 doubles (the output rows of
+// the warp, 32 columns at a time, padded against bank conflicts), also used for
+// one plane of the warp's share of an output image.
+constexpr int EPI_OFF = NSTAGE * STAGE_BYTES;
+constexpr int EPI_WARP_BYTES = 32 * 33 * 8;                 // 8448
+constexpr int BAR_OFF = EPI_OFF + 4 * EPI_WARP_BYTES;
 constexpr int SMEM_BYTES = BAR_OFF + 256;
+static_assert(EPI_WARP_BYTES >= PLANE_B && EPI_WARP_BYTES % 16 == 0, "epilogue staging holds one B-role plane");
 constexpr uint32_t TMEM_COLS = 128;                          // two 64-column accumulators
 constexpr long long kWaitLimit = 4000000;                    // try_wait polls before a wait gives up
 
@@ -228,7 +234,8 @@ __global__ void __launch_bounds__(NT, 1) gemm_split_kernel(const unsigned char* 
                                                             unsigned char* __restrict__ t_out,
                                                             const PackedTerm* __restrict__ terms,
                                                             const PackedGroup* __restrict__ groups,
-                                                            const PackedTile* __restrict__ tiles, int ntiles,
+                                                            const PackedTile* __restrict__ tiles,
+                                                            const int* __restrict__ cta_first,
                                                             int accumulate, int out_mode, int* __restrict__ status) {
     extern __shared__ __align__(1024) unsigned char smem[];
     Bars& B = *reinterpret_cast<Bars*>(smem + BAR_OFF);
@@ -255,13 +262,14 @@ __global__ void __launch_bounds__(NT, 1) gemm_split_kernel(const unsigned char* 
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = B.tmem;
+    const int tile_begin = cta_first[blockIdx.x], tile_end = cta_first[blockIdx.x + 1];
     bool ok = true;
 
     if (warp == 0) {
         // ---- producer ----
         if (lane == 0) {
             int it = 0;
-            for (int tt = blockIdx.x; tt < ntiles && ok; tt += gridDim.x) {
+            for (int tt = tile_begin; tt < tile_end && ok; ++tt) {
             const PackedTile tile = tiles[tt];
             const PackedGroup g = groups[tile.group];
             // Only the image rows that hold data are copied (rounded up to a core
@@ -307,7 +315,7 @@ __global__ void __launch_bounds__(NT, 1) gemm_split_kernel(const unsigned char* 
         // ---- MMA issuer ----
         if (lane == 0) {
             int it = 0, ti = 0;
-            for (int tt = blockIdx.x; tt < ntiles && ok; tt += gridDim.x) {
+            for (int tt = tile_begin; tt < tile_end && ok; ++tt) {
             const PackedGroup g = groups[tiles[tt].group];
             for (int t = g.t0; t < g.t1 && ok; ++t, ++ti) {
                 const int acc = ti & 1;
@@ -349,7 +357,7 @@ __global__ void __launch_bounds__(NT, 1) gemm_split_kernel(const unsigned char* 
         const int quarter = warp & 3;
         const int row = quarter * 32 + lane;  // tile row = TMEM lane
         int ti = 0;
-        for (int tt = blockIdx.x; tt < ntiles && ok; tt += gridDim.x) {
+        for (int tt = tile_begin; tt < tile_end && ok; ++tt) {
         const PackedTile tile = tiles[tt];
         const PackedGroup g = groups[tile.group];
         double sum[TN];
@@ -377,30 +385,87 @@ __global__ void __launch_bounds__(NT, 1) gemm_split_kernel(const unsigned char* 
             if (lane == 0) mbar_arrive(&B.acce[acc]);
         }
         if (ok) {
-            const int grow = tile.pm * TM + row;  // row of the output block
+            // Output through this warp's staging buffer, so that global stores are
+            // coalesced (a thread holds one output row; rows are written by the warp).
+            unsigned char* stg = smem + EPI_OFF + quarter * EPI_WARP_BYTES;
+            const int r0 = tile.pm * TM + quarter * 32;  // first output row of this warp
             if (out_mode == 0) {
-                if (grow < g.m) {
-                    double* Cb = g.cbuf ? Caux : C;
-                    const bool acc_out = accumulate && g.cbuf == 0;
-                    double* crow = Cb + g.c_off + (int64_t)grow * g.ldc;
+                double* sd = reinterpret_cast<double*>(stg);
+                double* Cb = g.cbuf ? Caux : C;
+                const bool acc_out = accumulate && g.cbuf == 0;
+                const int rows = min(32, g.m - r0);
 #pragma unroll
-                    for (int j = 0; j < TN; ++j) {
-                        const int col = tile.pn * TN + j;
-                        if (col < g.n) crow[col] = acc_out ? crow[col] + sum[j] : sum[j];
+                for (int h = 0; h < TN / 32; ++h) {
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) sd[lane * 33 + j] = sum[h * 32 + j];
+                    __syncwarp();
+                    const int col = tile.pn * TN + h * 32 + lane;
+                    if (col < g.n) {
+                        double* cp = Cb + g.c_off + (int64_t)r0 * g.ldc + col;
+                        if (acc_out) {
+                            // the old values are loaded 8 rows at a time ahead of the
+                            // stores: a load after a store through the same pointer
+                            // would wait for it, one memory round trip per row
+                            for (int rb = 0; rb < rows; rb += 8) {
+                                double old[8];
+#pragma unroll
+                                for (int u = 0; u < 8; ++u)
+                                    old[u] = rb + u < rows ? cp[(int64_t)(rb + u) * g.ldc] : 0.0;
+#pragma unroll
+                                for (int u = 0; u < 8; ++u)
+                                    if (rb + u < rows) cp[(int64_t)(rb + u) * g.ldc] = old[u] + sd[(rb + u) * 33 + lane];
+                            }
+                        } else {
+                            for (int r = 0; r < rows; ++r, cp += g.ldc) *cp = sd[r * 33 + lane];
+                        }
                     }
+                    __syncwarp();
                 }
             } else {
-                // the output as B-role images of X = output^T (rows = columns of the
-                // output, k = rows of the output); zeros in the padding
+                // The output as B-role images of X = output^T (image rows = output
+                // columns, k = output rows), zeros in the padding.  The warp's 32
+                // output rows are 32 consecutive k of one slice: per 8-row group of
+                // the image a run of 32 * esize bytes per row, 8 rows = `run` bytes
+                // at byte kb0 * 8 of the group.  Each plane is assembled compactly
+                // in shared memory (16-byte slots XOR-swizzled by chunk against bank
+                // conflicts), then written with 16-byte stores.
                 constexpr int tk = FMT == kFmtBF16 ? 64 : 32;
-                const int slice = grow / tk;
+                constexpr int esize = FMT == kFmtBF16 ? 2 : 4;
+                constexpr int run = 8 * 32 * esize;  // bytes per 8-row group
+                const int slice = r0 / tk;
+                const int kb0 = (r0 % tk) * esize;   // first k byte of the warp in a row
+                const int kk = lane * esize;         // this lane's k byte within the warp's span
                 if (slice < g.t_slices) {
                     unsigned char* img = t_out + g.t_img + ((int64_t)tile.pn * g.t_slices + slice) * kImageB;
-                    const int k = grow % tk;
+                    const bool row_ok = row < TM && (tile.pm * TM + row) < g.m;
+                    const int c = kk >> 4;           // 16-byte chunk within the span
 #pragma unroll
-                    for (int j = 0; j < TN; ++j) {
-                        const int col = tile.pn * TN + j;
-                        put_split(img, TN, j, k, (grow < g.m && col < g.n) ? sum[j] : 0.0, FMT);
+                    for (int p = 0; p < 2; ++p) {
+#pragma unroll
+                        for (int j = 0; j < TN; ++j) {
+                            const int col = tile.pn * TN + j;
+                            const double v = (row_ok && col < g.n) ? sum[j] : 0.0;
+                            const int so = (j >> 3) * run + c * 128 + (((j & 7) ^ c) & 7) * 16 + (kk & 15);
+                            if constexpr (FMT == kFmtBF16) {
+                                uint16_t hb, lb;
+                                split_bf16(v, hb, lb);
+                                *reinterpret_cast<uint16_t*>(stg + so) = p ? lb : hb;
+                            } else {
+                                uint32_t hb, lb;
+                                split(v, hb, lb);
+                                *reinterpret_cast<uint32_t*>(stg + so) = p ? lb : hb;
+                            }
+                        }
+                        __syncwarp();
+                        unsigned char* dst = img + p * PLANE_B + kb0 * 8;
+#pragma unroll
+                        for (int u = lane; u < 8 * run / 16; u += 32) {
+                            const int grp = (u * 16) / run, rem = (u * 16) % run;
+                            const int cc = rem >> 7, slot = (rem >> 4) & 7;
+                            *reinterpret_cast<uint4*>(dst + grp * SBO + cc * LBO + ((slot ^ cc) & 7) * 16) =
+                                *reinterpret_cast<const uint4*>(stg + u * 16);
+                        }
+                        __syncwarp();
                     }
                 }
             }
@@ -509,16 +574,46 @@ int PackedSchedule::finalize(cudaStream_t stream, int num_sms) {
         aux_size += (int64_t)sp.chunks * g.m * g.n;
         splits.push_back(sp);
     }
+    // Tile cost in quarter stages: 4 per stage (its MMAs), 1 per term (the
+    // accumulator read-out), 6 per tile (pipeline fill and the output store).
+    std::vector<PackedTile> all;
     for (int gi = 0; gi < (int)exec_groups.size(); ++gi) {
         const PackedGroup& g = exec_groups[gi];
-        const int cost = (int)stages(g);
+        const int cost = (int)(4 * stages(g) + (g.t1 - g.t0) + 6);
         for (int pm = 0; pm * TM < g.m; ++pm)
-            for (int pn = 0; pn * TN < g.n; ++pn) tiles.push_back(PackedTile{gi, pm, pn, cost});
+            for (int pn = 0; pn * TN < g.n; ++pn) all.push_back(PackedTile{gi, pm, pn, cost});
     }
-    std::stable_sort(tiles.begin(), tiles.end(), [](const PackedTile& a, const PackedTile& b) { return a.cost > b.cost; });
+    std::stable_sort(all.begin(), all.end(), [](const PackedTile& a, const PackedTile& b) { return a.cost > b.cost; });
+    // Longest-processing-time-first assignment to the persistent CTAs: each
+    // tile, heaviest first, goes to the least loaded CTA (lowest index on ties).
+    // A CTA's tiles are stored contiguously, heaviest first.
+    ctas = (int)std::min<int64_t>((int64_t)all.size(), num_sms > 0 ? num_sms : 148);
+    std::vector<int> owner(all.size());
+    std::vector<int> count(std::max(ctas, 1), 0);
+    {
+        std::vector<std::pair<int64_t, int>> heap;
+        for (int c = 0; c < ctas; ++c) heap.push_back({0, c});
+        auto later = [](const std::pair<int64_t, int>& a, const std::pair<int64_t, int>& b) { return a > b; };
+        for (size_t i = 0; i < all.size(); ++i) {
+            std::pop_heap(heap.begin(), heap.end(), later);
+            auto& least = heap.back();
+            least.first += all[i].cost;
+            owner[i] = least.second;
+            count[least.second]++;
+            std::push_heap(heap.begin(), heap.end(), later);
+        }
+    }
+    cta_first.assign(ctas + 1, 0);
+    for (int c = 0; c < ctas; ++c) cta_first[c + 1] = cta_first[c] + count[c];
+    tiles.resize(all.size());
+    {
+        std::vector<int> next(cta_first.begin(), cta_first.end() - 1);
+        for (size_t i = 0; i < all.size(); ++i) tiles[next[owner[i]]++] = all[i];
+    }
     DMRG_TRY(upload(d_terms, terms, stream));
     DMRG_TRY(upload(d_groups, exec_groups, stream));
     DMRG_TRY(upload(d_tiles, tiles, stream));
+    DMRG_TRY(upload(d_cta_first, cta_first, stream));
     DMRG_TRY(upload(d_splits, splits, stream));
     DMRG_TRY(aux.alloc((size_t)std::max<int64_t>(aux_size, 1) * sizeof(double)));
     return DMRG_OK;
@@ -559,7 +654,7 @@ int launch_fmt(const PackedSchedule& s, const unsigned char* a_imgs, const unsig
     }
     gemm_split_kernel<FMT><<<grid, NT, SMEM_BYTES, stream>>>(
         a_imgs, b_imgs, C, s.aux.as<double>(), t_out, s.d_terms.as<PackedTerm>(), s.d_groups.as<PackedGroup>(),
-        s.d_tiles.as<PackedTile>(), (int)s.tiles.size(), accumulate ? 1 : 0, s.out_mode, status);
+        s.d_tiles.as<PackedTile>(), s.d_cta_first.as<int>(), accumulate ? 1 : 0, s.out_mode, status);
     return DMRG_OK;
 }
 }  // namespace
@@ -567,12 +662,10 @@ int launch_fmt(const PackedSchedule& s, const unsigned char* a_imgs, const unsig
 int launch_gemm_split(const PackedSchedule& s, const unsigned char* a_imgs, const unsigned char* b_imgs, double* C,
                       unsigned char* t_out, bool accumulate, int* status, cudaStream_t stream) {
     if (s.tiles.empty()) return DMRG_OK;
-    // persistent: one CTA per SM walks the (cost-sorted) tiles round-robin; its
-    // stage ring and accumulator pair carry over from one tile to the next
-    int dev = 0, sms = 148;
-    DMRG_CUDA_TRY(cudaGetDevice(&dev));
-    DMRG_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    const int grid = std::min((int)s.tiles.size(), sms);
+    // persistent: one CTA per SM walks its own run of tiles (assigned at
+    // finalize); its stage ring and accumulator pair carry over from one tile
+    // to the next
+    const int grid = s.ctas;
     if (s.fmt == kFmtBF16) DMRG_TRY(launch_fmt<kFmtBF16>(s, a_imgs, b_imgs, C, t_out, accumulate, status, grid, stream));
     else DMRG_TRY(launch_fmt<kFmtTF32>(s, a_imgs, b_imgs, C, t_out, accumulate, status, grid, stream));
     if (!s.splits.empty()) {

@@ -186,7 +186,7 @@ int build_heff(dmrg_heff_s& h) {
         DMRG_TRY(h.pk_psi.finalize(st));
         DMRG_TRY(h.pk_L.finalize(st));
         DMRG_TRY(h.pk_R.finalize(st));
-        DMRG_TRY(h.pa.finalize(st));
+        DMRG_TRY(h.pa.finalize(st, h.ctx->num_sms));
         DMRG_TRY(h.pb.finalize(st, h.ctx->num_sms));
         DMRG_TRY(h.img_psi.alloc((size_t)std::max<int64_t>(h.pk_psi.bytes, 16)));
         DMRG_TRY(h.img_L.alloc((size_t)std::max<int64_t>(h.pk_L.bytes, 16)));
