@@ -111,29 +111,41 @@ int launch_gemm_f64(const GemmSchedule& s, const double* A, const double* B, dou
 // Operands are packed once into "images": for an operand block X (rows x k,
 // K-major), image (panel p, slice s) holds rows [p*R, p*R+R) x one k slice as a
 // hi plane followed by a lo plane (x ~ hi + lo), each in the tcgen05 canonical
-// K-major no-swizzle layout: 128 bytes of k per row in 16-byte chunks; a core
-// matrix is 8 rows x 16 bytes, the 8 chunks of an 8-row group are contiguous
-// (LBO = 128) and groups follow each other (SBO = 1024), so the first m rows of
+// K-major no-swizzle layout: 64 bytes of k per row in 16-byte chunks; a core
+// matrix is 8 rows x 16 bytes, the 4 chunks of an 8-row group are contiguous
+// (LBO = 128) and groups follow each other (SBO = 512), so the first m rows of
 // a plane are one contiguous prefix: byte offset of (row r, k) =
-// (r/8)*1024 + (k*E/16)*128 + (r%8)*16 + (k*E)%16 for E-byte elements.  Zero
+// (r/8)*512 + (k*E/16)*128 + (r%8)*16 + (k*E)%16 for E-byte elements.  Zero
 // outside X.  Two formats share this geometry:
-//   TF32 (E = 4): x rounded to FP32, hi = tf32(x), lo = tf32(x - hi); 32 k per slice;
-//   BF16 (E = 2): hi = bf16(x), lo = bf16(x - hi); 64 k per slice.
-// R = 128 for the A role (output rows), 64 for the B role (output columns).
-// A GEMM stage then is two contiguous bulk copies (32 KB + 16 KB).
+//   TF32 (E = 4): x rounded to FP32, hi = tf32(x), lo = tf32(x - hi); 16 k per slice;
+//   BF16 (E = 2): hi = bf16(x), lo = bf16(x - hi); 32 k per slice.
+// R = 128 rows per panel in both roles (A: output rows, B: output columns),
+// except the last panel of a block, which keeps only the block's remaining rows
+// rounded up to a core matrix of 8 (its images are that much shorter).  The
+// images of panel p follow those of the full panels before it, slice by slice.
+// A GEMM stage then is one contiguous bulk copy per plane of each operand.
 constexpr int kFmtTF32 = 0, kFmtBF16 = 1;
-constexpr int kPackRowBytes = 128;
-constexpr int kPackRowsA = 128, kPackRowsB = 64;
-constexpr int kImageA = 2 * kPackRowsA * kPackRowBytes;  // bytes: hi + lo
-constexpr int kImageB = 2 * kPackRowsB * kPackRowBytes;
-inline int pack_k(int fmt) { return fmt == kFmtBF16 ? 64 : 32; }  // k per slice
+constexpr int kPackRowBytes = 64;
+constexpr int kPackRows = 128;
+constexpr int kImage = 2 * kPackRows * kPackRowBytes;  // bytes of a full image: hi + lo
+inline int pack_k(int fmt) { return fmt == kFmtBF16 ? 32 : 16; }  // k per slice
+// rows held by panel p of a block of `rows` rows
+__host__ __device__ inline int panel_rows(int rows, int p) {
+    const int r = (rows - p * kPackRows + 7) & ~7;
+    return r < kPackRows ? r : kPackRows;
+}
+// bytes of all images of a block of `rows` rows and `slices` k slices
+inline int64_t image_bytes(int rows, int slices) {
+    const int64_t full = rows / kPackRows, rest = rows - full * kPackRows;
+    return (full * kPackRows + ((rest + 7) & ~7)) * 2 * kPackRowBytes * slices;
+}
 
 struct PackJob {
     int64_t src_off;  // doubles
     int64_t img_off;  // bytes, into the image buffer
     int rows, k, ld;  // logical X: rows x k; X(r, c) = src[src_off + (trans ? c*ld + r : r*ld + c)]
     int trans;
-    int prow;         // rows per panel (kPackRowsA or kPackRowsB)
+    int prow_;
     int slices;       // ceil(k / pack_k(fmt))
     int fmt;          // kFmtTF32 or kFmtBF16
     int pad_;
@@ -148,7 +160,7 @@ struct PackSchedule {
     int64_t bytes = 0;
     DeviceBuffer d_jobs, d_images;
     // Appends the images of one operand block; returns its image offset (bytes).
-    int64_t add(int64_t src_off, int rows, int k, int ld, bool trans, int prow);
+    int64_t add(int64_t src_off, int rows, int k, int ld, bool trans);
     int finalize(cudaStream_t stream);
 };
 // dst (images) <- split-precision images of the jobs' blocks of src.
@@ -198,7 +210,7 @@ struct PackedSchedule {
     // Verifies every image read and every output write against the buffer sizes
     // (bytes for images, doubles for c_size); DMRG_E_ARG, no launch, otherwise.
     int check_bounds(int64_t a_bytes, int64_t b_bytes, int64_t c_size, int64_t t_bytes) const;
-    // Splits long mode-0 groups (num_sms > 0), builds the 128 x 64 tiles and
+    // Splits long mode-0 groups (num_sms > 0), builds the 128 x 128 tiles and
     // assigns them to min(tiles, num_sms or 148) persistent CTAs by cost
     // (longest first, to the least loaded CTA), uploads.
     int finalize(cudaStream_t stream, int num_sms = 0);

@@ -11,23 +11,30 @@
 // into FP64 registers, so the terms of a block sum accumulate in FP64.
 //
 // Packing (launch_pack): one CTA per image writes the hi/lo planes of one
-// (panel, 32-wide k slice) of an operand block in the tcgen05 canonical K-major
+// (panel, k slice) of an operand block in the tcgen05 canonical K-major
 // no-swizzle layout (see gemm.cuh).  A GEMM stage is then one bulk copy
 // (cp.async.bulk, no multicast) per plane of each operand, covering only the
 // rows of the tile that hold data.
 //
-// GEMM (persistent: one CTA per SM walks 128 x 64 output tiles, 192 threads,
+// Tile shape: 128 x 128 outputs, the MMA's N trimmed per tile to the block's
+// columns (a multiple of 16).  A tcgen05.mma carries a fixed issue cost of
+// some 60 cycles, about what a 128 x 64 x 8 TF32 product takes at full rate,
+// so narrow tiles leave the tensor pipe mostly idle; at N = 128 the three
+// products of a k step run at close to the pipe's rate.
+//
+// GEMM (persistent: one CTA per SM walks its own list of tiles, 576 threads,
 // warp-specialised; stage counters and the accumulator pair run on across tiles):
 //   warp 0 lane 0   producer: per stage waits the stage's "empty" barrier, arms
 //                   the "full" barrier with the byte count, issues the copies;
-//   warp 1 lane 0   MMA issuer: per stage waits "full", issues 4 k-substeps x 3
-//                   MMAs into the term's accumulator (two 64-column accumulators
+//   warp 1 lane 0   MMA issuer: per stage waits "full", issues 2 k-substeps x 3
+//                   MMAs into the term's accumulator (two 128-column accumulators
 //                   alternate between terms), commits to "empty"; after a term's
 //                   last stage commits to the accumulator's "full" barrier;
-//   warps 2..5      epilogue: per term wait, tcgen05.ld the 128 x 64 FP32 tile
-//                   (warp w: TMEM lanes 32(w%4)..), add w_t * value into FP64
-//                   registers, release the accumulator; finally store FP64 rows
-//                   (or write the result as B-role images for the next GEMM).
+//   warps 2..17     epilogue: warp w reads TMEM lanes 32(w%4).. and columns
+//                   32((w-2)/4)..+31: per term wait, tcgen05.ld, add w_t * value
+//                   into FP64 registers, release the accumulator; finally store
+//                   FP64 rows (or write the result as B-role images for the next
+//                   GEMM) through a per-warp shared-memory staging buffer.
 // Every wait is bounded: on a timeout a role records DMRG_E_NUMERIC in the
 // status word and stops; the CTA frees its tensor memory and returns.
 #include <algorithm>
@@ -38,22 +45,29 @@
 namespace dmrg {
 namespace {
 
-constexpr int TM = kPackRowsA, TN = kPackRowsB;
-constexpr int NSTAGE = 4;
-constexpr int STAGE_BYTES = kImageA + kImageB;               // 48 KB
-constexpr int LBO = 128;   // bytes between the 16-byte k chunks of one 8-row core-matrix group
-constexpr int SBO = 1024;  // bytes between 8-row groups: a group's 8 chunks are contiguous
-constexpr int PLANE_A = TM * kPackRowBytes, PLANE_B = TN * kPackRowBytes;  // hi plane; lo follows
-constexpr int NT = 192;
-// Epilogue staging: per epilogue warp 32 rows x 33 doubles (the output rows of
-// the warp, 32 columns at a time, padded against bank conflicts), also used for
-// one plane of the warp's share of an output image.
+constexpr int TM = kPackRows, TN = kPackRows;
+constexpr int NSTAGE = 5;
+constexpr int STAGE_BYTES = 2 * kImage;                     // 32 KB: A image, then B image
+constexpr int LBO = 128;  // bytes between the 16-byte k chunks of one 8-row core-matrix group
+constexpr int SBO = 512;  // bytes between 8-row groups: a group's 4 chunks are contiguous
+constexpr int PLANE = kPackRows * kPackRowBytes;            // a full hi plane in a stage; lo follows
+constexpr int KSUB = kPackRowBytes / 32;                     // MMAs (32 bytes of k) per slice
+#ifndef DMRG_SPLIT_EPILOGUE_WARPS
+#define DMRG_SPLIT_EPILOGUE_WARPS 8
+#endif
+constexpr int NEPI = DMRG_SPLIT_EPILOGUE_WARPS;              // epilogue warps: 4 per TMEM lane quarter x column parts
+constexpr int NT = 32 * (2 + NEPI);
+constexpr int ECOLS = TN * 4 / NEPI;                         // accumulator columns per epilogue warp
+// Epilogue staging per epilogue warp: 32 output rows x 16 doubles (16 columns
+// at a time), or both planes of the warp's share of one slice of an output
+// image (ECOLS image rows x 64 bytes of k, twice).
 constexpr int EPI_OFF = NSTAGE * STAGE_BYTES;
-constexpr int EPI_WARP_BYTES = 32 * 33 * 8;                 // 8448
-constexpr int BAR_OFF = EPI_OFF + 4 * EPI_WARP_BYTES;
+constexpr int EPI_WARP_BYTES = 2 * ECOLS * kPackRowBytes;
+constexpr int BAR_OFF = EPI_OFF + NEPI * EPI_WARP_BYTES;
 constexpr int SMEM_BYTES = BAR_OFF + 256;
-static_assert(EPI_WARP_BYTES >= PLANE_B && EPI_WARP_BYTES % 16 == 0, "epilogue staging holds one B-role plane");
-constexpr uint32_t TMEM_COLS = 128;                          // two 64-column accumulators
+static_assert(NEPI % 4 == 0 && ECOLS % 16 == 0 && ECOLS * NEPI == 4 * TN && TM == 128, "epilogue geometry");
+static_assert(EPI_WARP_BYTES >= 32 * 16 * 8, "staging holds 32 rows x 16 doubles");
+constexpr uint32_t TMEM_COLS = 2 * TN;                       // two 128-column accumulators
 constexpr long long kWaitLimit = 4000000;                    // try_wait polls before a wait gives up
 
 static_assert(SMEM_BYTES <= 227 * 1024, "shared memory per CTA");
@@ -71,27 +85,27 @@ __device__ __forceinline__ uint64_t make_smem_desc(uint32_t saddr, uint32_t lbo,
 }
 
 // Instruction descriptor: D = F32, A = B = TF32 (format 2) or BF16 (format 1),
-// both K-major, N = 64, M = 128.
+// both K-major, M = 128, N = n (a multiple of 16, at most 256).
 template <int FMT>
-__host__ __device__ constexpr uint32_t idesc() {
+__host__ __device__ constexpr uint32_t idesc(int n) {
     return (1u << 4) | ((FMT == kFmtBF16 ? 1u : 2u) << 7) | ((FMT == kFmtBF16 ? 1u : 2u) << 10) |
-           ((uint32_t)(TN >> 3) << 17) | ((uint32_t)(TM >> 4) << 24);
+           ((uint32_t)(n >> 3) << 17) | ((uint32_t)(TM >> 4) << 24);
 }
 
 // One MMA of 32 bytes of k (8 tf32 or 16 bf16 per row).
 template <int FMT>
-__device__ __forceinline__ void mma_split(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t acc) {
+__device__ __forceinline__ void mma_split(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t id, uint32_t acc) {
     if constexpr (FMT == kFmtBF16)
         asm volatile(
             "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
             "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
-            "l"(a), "l"(b), "r"(idesc<FMT>()), "r"(acc)
+            "l"(a), "l"(b), "r"(id), "r"(acc)
             : "memory");
     else
         asm volatile(
             "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
             "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
-            "l"(a), "l"(b), "r"(idesc<FMT>()), "r"(acc)
+            "l"(a), "l"(b), "r"(id), "r"(acc)
             : "memory");
 }
 
@@ -143,11 +157,10 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
                  : "memory");
 }
 
-__device__ __forceinline__ uint32_t tf32_bits(float x) {
-    uint32_t r;
-    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-    return r;
-}
+// TF32 rounding of an FP32 value, to nearest with ties away from zero: add half
+// a unit of the 10-bit mantissa's last place to the magnitude bits, then clear
+// the 13 bits below it (the sign bit is untouched, so it works on either sign).
+__device__ __forceinline__ uint32_t tf32_bits(float x) { return (__float_as_uint(x) + 0x1000u) & 0xFFFFE000u; }
 
 __device__ __forceinline__ void split(double v, uint32_t& hi, uint32_t& lo) {
     const float f = (float)v;
@@ -187,15 +200,12 @@ __device__ __forceinline__ void put_split(unsigned char* img, int rows, int r, i
     }
 }
 
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
     asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
-        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
-          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
-          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
         : "r"(taddr));
 }
 
@@ -204,19 +214,19 @@ __global__ void __launch_bounds__(128) pack_kernel(const PackJob* __restrict__ j
                                                    const double* __restrict__ src, unsigned char* __restrict__ dst) {
     const PackImage im = imgs[blockIdx.x];
     const PackJob j = jobs[im.job];
-    const int img_bytes = 2 * j.prow * kPackRowBytes;
-    const int tk = j.fmt == kFmtBF16 ? 64 : 32;
-    unsigned char* out = dst + j.img_off + ((int64_t)im.panel * j.slices + im.slice) * img_bytes;
-    const int r0 = im.panel * j.prow, k0 = im.slice * tk;
+    const int prow = panel_rows(j.rows, im.panel);  // rows of this panel's images
+    const int tk = j.fmt == kFmtBF16 ? 32 : 16;     // k per slice
+    unsigned char* out = dst + j.img_off + (int64_t)im.panel * j.slices * kImage + (int64_t)im.slice * 2 * prow * kPackRowBytes;
+    const int r0 = im.panel * kPackRows, k0 = im.slice * tk;
     const double* s = src + j.src_off;
-    for (int idx = threadIdx.x; idx < j.prow * tk; idx += blockDim.x) {
+    for (int idx = threadIdx.x; idx < prow * tk; idx += blockDim.x) {
         // consecutive threads: consecutive k for row-major X, consecutive rows for transposed X
-        const int r = j.trans ? idx % j.prow : idx / tk;
-        const int k = j.trans ? idx / j.prow : idx % tk;
+        const int r = j.trans ? idx % prow : idx / tk;
+        const int k = j.trans ? idx / prow : idx % tk;
         double v = 0.0;
         if (r0 + r < j.rows && k0 + k < j.k)
             v = j.trans ? s[(int64_t)(k0 + k) * j.ld + (r0 + r)] : s[(int64_t)(r0 + r) * j.ld + (k0 + k)];
-        put_split(out, j.prow, r, k, v, j.fmt);
+        put_split(out, prow, r, k, v, j.fmt);
     }
 }
 
@@ -226,6 +236,10 @@ struct Bars {
     uint32_t tmem;
 };
 static_assert(sizeof(Bars) <= 256, "barrier block");
+
+// MMA width of the tile at column panel pn of an n-column block: the columns
+// left in the block rounded up to 16, at most TN.
+__device__ __forceinline__ int mma_n(int n, int pn) { return min(TN, (n - pn * TN + 15) & ~15); }
 
 template <int FMT>
 __global__ void __launch_bounds__(NT, 1) gemm_split_kernel(const unsigned char* __restrict__ a_imgs,
@@ -254,7 +268,7 @@ __global__ void __launch_bounds__(NT, 1) gemm_split_kernel(const unsigned char* 
         }
         for (int a = 0; a < 2; ++a) {
             mbar_init(&B.accf[a], 1);
-            mbar_init(&B.acce[a], 4);
+            mbar_init(&B.acce[a], NEPI);
         }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -270,35 +284,35 @@ __global__ void __launch_bounds__(NT, 1) gemm_split_kernel(const unsigned char* 
         if (lane == 0) {
             int it = 0;
             for (int tt = tile_begin; tt < tile_end && ok; ++tt) {
-            const PackedTile tile = tiles[tt];
-            const PackedGroup g = groups[tile.group];
-            // Only the image rows that hold data are copied (rounded up to a core
-            // matrix of 8 rows, which the layout keeps contiguous): one bulk copy
-            // per plane.  Rows left stale in shared memory feed only accumulator
-            // rows (A) or columns (B) past the block, which are never stored.
-            const uint32_t ca = (uint32_t)((min(TM, g.m - tile.pm * TM) + 7) & ~7) * kPackRowBytes;
-            const uint32_t cb = (uint32_t)((min(TN, g.n - tile.pn * TN) + 7) & ~7) * kPackRowBytes;
-            const uint32_t tx = 2 * (ca + cb);
-            for (int t = g.t0; t < g.t1 && ok; ++t) {
-                const PackedTerm tm = terms[t];
-                const unsigned char* a = a_imgs + tm.a_img + (int64_t)tile.pm * tm.slices * kImageA;
-                const unsigned char* b = b_imgs + tm.b_img + (int64_t)tile.pn * tm.slices * kImageB;
-                for (int s = 0; s < tm.slices; ++s, ++it) {
-                    const int st = it % NSTAGE;
-                    if (it >= NSTAGE && !mbar_wait(&B.empty[st], ((it / NSTAGE) - 1) & 1)) {
-                        ok = false;
-                        break;
+                const PackedTile tile = tiles[tt];
+                const PackedGroup g = groups[tile.group];
+                // Only the image rows that hold data are copied (rounded up to a core
+                // matrix of 8 rows, which the layout keeps contiguous): one bulk copy
+                // per plane.  Rows left stale in shared memory feed only accumulator
+                // rows (A) or columns (B) past the block, which are never stored.
+                const uint32_t ca = (uint32_t)panel_rows(g.m, tile.pm) * kPackRowBytes;  // plane bytes
+                const uint32_t cb = (uint32_t)panel_rows(g.n, tile.pn) * kPackRowBytes;
+                const uint32_t tx = 2 * (ca + cb);
+                for (int t = g.t0; t < g.t1 && ok; ++t) {
+                    const PackedTerm tm = terms[t];
+                    const unsigned char* a = a_imgs + tm.a_img + (int64_t)tile.pm * tm.slices * kImage;
+                    const unsigned char* b = b_imgs + tm.b_img + (int64_t)tile.pn * tm.slices * kImage;
+                    for (int s = 0; s < tm.slices; ++s, ++it) {
+                        const int st = it % NSTAGE;
+                        if (it >= NSTAGE && !mbar_wait(&B.empty[st], ((it / NSTAGE) - 1) & 1)) {
+                            ok = false;
+                            break;
+                        }
+                        unsigned char* dst = smem + st * STAGE_BYTES;
+                        const unsigned char* as = a + (int64_t)s * 2 * ca;  // the panel's images: hi, lo planes
+                        const unsigned char* bs = b + (int64_t)s * 2 * cb;
+                        mbar_arrive_expect_tx(&B.full[st], tx);
+                        bulk_g2s(dst, as, ca, &B.full[st]);
+                        bulk_g2s(dst + PLANE, as + ca, ca, &B.full[st]);
+                        bulk_g2s(dst + kImage, bs, cb, &B.full[st]);
+                        bulk_g2s(dst + kImage + PLANE, bs + cb, cb, &B.full[st]);
                     }
-                    unsigned char* dst = smem + st * STAGE_BYTES;
-                    const unsigned char* as = a + (int64_t)s * kImageA;
-                    const unsigned char* bs = b + (int64_t)s * kImageB;
-                    mbar_arrive_expect_tx(&B.full[st], tx);
-                    bulk_g2s(dst, as, ca, &B.full[st]);
-                    bulk_g2s(dst + PLANE_A, as + PLANE_A, ca, &B.full[st]);
-                    bulk_g2s(dst + kImageA, bs, cb, &B.full[st]);
-                    bulk_g2s(dst + kImageA + PLANE_B, bs + PLANE_B, cb, &B.full[st]);
                 }
-            }
             }
             // Tail: nothing asynchronous may still target this CTA's shared memory
             // when it exits.  Wait until the copies of the last stages have landed
@@ -316,160 +330,196 @@ __global__ void __launch_bounds__(NT, 1) gemm_split_kernel(const unsigned char* 
         if (lane == 0) {
             int it = 0, ti = 0;
             for (int tt = tile_begin; tt < tile_end && ok; ++tt) {
-            const PackedGroup g = groups[tiles[tt].group];
-            for (int t = g.t0; t < g.t1 && ok; ++t, ++ti) {
-                const int acc = ti & 1;
-                if (ti >= 2 && !mbar_wait(&B.acce[acc], ((ti >> 1) - 1) & 1)) {
-                    ok = false;
-                    break;
-                }
-                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                const int slices = terms[t].slices;
-                const uint32_t d = tmem + (uint32_t)(acc * TN);
-                for (int s = 0; s < slices; ++s, ++it) {
-                    const int st = it % NSTAGE;
-                    if (!mbar_wait(&B.full[st], (it / NSTAGE) & 1)) {
+                const PackedTile tile = tiles[tt];
+                const PackedGroup g = groups[tile.group];
+                const uint32_t id = idesc<FMT>(mma_n(g.n, tile.pn));
+                for (int t = g.t0; t < g.t1 && ok; ++t, ++ti) {
+                    const int acc = ti & 1;
+                    if (ti >= 2 && !mbar_wait(&B.acce[acc], ((ti >> 1) - 1) & 1)) {
                         ok = false;
                         break;
                     }
                     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                    const uint32_t a_base = smem_u32(smem + st * STAGE_BYTES);
-                    const uint32_t b_base = a_base + kImageA;
+                    const int slices = terms[t].slices;
+                    const uint32_t d = tmem + (uint32_t)(acc * TN);
+                    for (int s = 0; s < slices; ++s, ++it) {
+                        const int st = it % NSTAGE;
+                        if (!mbar_wait(&B.full[st], (it / NSTAGE) & 1)) {
+                            ok = false;
+                            break;
+                        }
+                        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                        const uint32_t a_base = smem_u32(smem + st * STAGE_BYTES);
+                        const uint32_t b_base = a_base + kImage;
 #pragma unroll
-                    for (int ks = 0; ks < kPackRowBytes / 32; ++ks) {  // 32 bytes of k per MMA
-                        const uint64_t ahi = make_smem_desc(a_base + 2 * ks * LBO, LBO, SBO);
-                        const uint64_t alo = make_smem_desc(a_base + PLANE_A + 2 * ks * LBO, LBO, SBO);
-                        const uint64_t bhi = make_smem_desc(b_base + 2 * ks * LBO, LBO, SBO);
-                        const uint64_t blo = make_smem_desc(b_base + PLANE_B + 2 * ks * LBO, LBO, SBO);
-                        mma_split<FMT>(d, ahi, bhi, (s > 0 || ks > 0) ? 1u : 0u);
-                        mma_split<FMT>(d, ahi, blo, 1u);
-                        mma_split<FMT>(d, alo, bhi, 1u);
+                        for (int ks = 0; ks < KSUB; ++ks) {  // 32 bytes of k per MMA
+                            const uint64_t ahi = make_smem_desc(a_base + 2 * ks * LBO, LBO, SBO);
+                            const uint64_t alo = make_smem_desc(a_base + PLANE + 2 * ks * LBO, LBO, SBO);
+                            const uint64_t bhi = make_smem_desc(b_base + 2 * ks * LBO, LBO, SBO);
+                            const uint64_t blo = make_smem_desc(b_base + PLANE + 2 * ks * LBO, LBO, SBO);
+                            mma_split<FMT>(d, ahi, bhi, id, (s > 0 || ks > 0) ? 1u : 0u);
+                            mma_split<FMT>(d, ahi, blo, id, 1u);
+                            mma_split<FMT>(d, alo, bhi, id, 1u);
+                        }
+                        mma_commit(&B.empty[st]);  // the stage's buffer is free once these MMAs are done
                     }
-                    mma_commit(&B.empty[st]);  // the stage's buffer is free once these MMAs are done
+                    if (!ok) break;
+                    mma_commit(&B.accf[acc]);      // the term's accumulator is complete
                 }
-                if (!ok) break;
-                mma_commit(&B.accf[acc]);      // the term's accumulator is complete
-            }
             }
         }
     } else {
-        // ---- epilogue: warps 2..5 ----
-        const int quarter = warp & 3;
-        const int row = quarter * 32 + lane;  // tile row = TMEM lane
+        // ---- epilogue: warps 2..17 ----
+        const int quarter = warp & 3;                // TMEM lanes 32*quarter.. (rows of the tile)
+        const int cq = (warp - 2) >> 2;              // accumulator columns cq*ECOLS..
+        unsigned char* stg = smem + EPI_OFF + (warp - 2) * EPI_WARP_BYTES;
         int ti = 0;
         for (int tt = tile_begin; tt < tile_end && ok; ++tt) {
-        const PackedTile tile = tiles[tt];
-        const PackedGroup g = groups[tile.group];
-        double sum[TN];
+            const PackedTile tile = tiles[tt];
+            const PackedGroup g = groups[tile.group];
+            const bool live = cq * ECOLS < mma_n(g.n, tile.pn);  // the MMAs write this warp's columns
+            double sum[ECOLS];
 #pragma unroll
-        for (int j = 0; j < TN; ++j) sum[j] = 0.0;
-        for (int t = g.t0; t < g.t1; ++t, ++ti) {
-            const int acc = ti & 1;
-            const bool got = mbar_wait(&B.accf[acc], (ti >> 1) & 1);
-            if (!__all_sync(0xffffffffu, got)) {  // warp-uniform: tcgen05.ld below is .sync.aligned
-                ok = false;
-                break;
+            for (int j = 0; j < ECOLS; ++j) sum[j] = 0.0;
+            for (int t = g.t0; t < g.t1; ++t, ++ti) {
+                const int acc = ti & 1;
+                const bool got = mbar_wait(&B.accf[acc], (ti >> 1) & 1);
+                if (!__all_sync(0xffffffffu, got)) {  // warp-uniform: tcgen05.ld below is .sync.aligned
+                    ok = false;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                if (live) {
+                    const double w = terms[t].w;
+#pragma unroll
+                    for (int h = 0; h < ECOLS / 16; ++h) {
+                        uint32_t v[16];
+                        tmem_ld16(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(acc * TN + cq * ECOLS + h * 16),
+                                  v);
+                        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+                        for (int j = 0; j < 16; ++j) sum[h * 16 + j] += w * (double)__uint_as_float(v[j]);
+                    }
+                }
+                asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&B.acce[acc]);
             }
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const double w = terms[t].w;
-#pragma unroll
-            for (int h = 0; h < TN / 32; ++h) {
-                uint32_t v[32];
-                tmem_ld32(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(acc * TN + h * 32), v);
-                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-                for (int j = 0; j < 32; ++j) sum[h * 32 + j] += w * (double)__uint_as_float(v[j]);
-            }
-            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&B.acce[acc]);
-        }
-        if (ok) {
+            if (!ok) break;
             // Output through this warp's staging buffer, so that global stores are
             // coalesced (a thread holds one output row; rows are written by the warp).
-            unsigned char* stg = smem + EPI_OFF + quarter * EPI_WARP_BYTES;
-            const int r0 = tile.pm * TM + quarter * 32;  // first output row of this warp
+            const int r0 = tile.pm * TM + quarter * 32;      // first output row of this warp
+            const int c0 = tile.pn * TN + cq * ECOLS;        // first output column of this warp
             if (out_mode == 0) {
+                // staging: 32 rows x 16 doubles, element (r, c) at r*16 + (c ^ (r & 15))
                 double* sd = reinterpret_cast<double*>(stg);
                 double* Cb = g.cbuf ? Caux : C;
                 const bool acc_out = accumulate && g.cbuf == 0;
                 const int rows = min(32, g.m - r0);
+                const int sub = lane >> 4, cl = lane & 15;    // lanes 0-15: even rows, 16-31: odd rows
 #pragma unroll
-                for (int h = 0; h < TN / 32; ++h) {
+                for (int h = 0; h < ECOLS / 16; ++h) {
 #pragma unroll
-                    for (int j = 0; j < 32; ++j) sd[lane * 33 + j] = sum[h * 32 + j];
+                    for (int j = 0; j < 16; ++j) sd[lane * 16 + (j ^ (lane & 15))] = sum[h * 16 + j];
                     __syncwarp();
-                    const int col = tile.pn * TN + h * 32 + lane;
+                    const int col = c0 + h * 16 + cl;
                     if (col < g.n) {
                         double* cp = Cb + g.c_off + (int64_t)r0 * g.ldc + col;
                         if (acc_out) {
                             // the old values are loaded 8 rows at a time ahead of the
                             // stores: a load after a store through the same pointer
                             // would wait for it, one memory round trip per row
-                            for (int rb = 0; rb < rows; rb += 8) {
+                            for (int rb = 0; rb < rows; rb += 16) {
                                 double old[8];
 #pragma unroll
-                                for (int u = 0; u < 8; ++u)
-                                    old[u] = rb + u < rows ? cp[(int64_t)(rb + u) * g.ldc] : 0.0;
+                                for (int u = 0; u < 8; ++u) {
+                                    const int r = rb + sub + 2 * u;
+                                    old[u] = r < rows ? cp[(int64_t)r * g.ldc] : 0.0;
+                                }
 #pragma unroll
-                                for (int u = 0; u < 8; ++u)
-                                    if (rb + u < rows) cp[(int64_t)(rb + u) * g.ldc] = old[u] + sd[(rb + u) * 33 + lane];
+                                for (int u = 0; u < 8; ++u) {
+                                    const int r = rb + sub + 2 * u;
+                                    if (r < rows) cp[(int64_t)r * g.ldc] = old[u] + sd[r * 16 + (cl ^ (r & 15))];
+                                }
                             }
                         } else {
-                            for (int r = 0; r < rows; ++r, cp += g.ldc) *cp = sd[r * 33 + lane];
+                            for (int r = sub; r < rows; r += 2) cp[(int64_t)r * g.ldc] = sd[r * 16 + (cl ^ (r & 15))];
                         }
                     }
                     __syncwarp();
                 }
             } else {
                 // The output as B-role images of X = output^T (image rows = output
-                // columns, k = output rows), zeros in the padding.  The warp's 32
-                // output rows are 32 consecutive k of one slice: per 8-row group of
-                // the image a run of 32 * esize bytes per row, 8 rows = `run` bytes
-                // at byte kb0 * 8 of the group.  Each plane is assembled compactly
-                // in shared memory (16-byte slots XOR-swizzled by chunk against bank
-                // conflicts), then written with 16-byte stores.
-                constexpr int tk = FMT == kFmtBF16 ? 64 : 32;
+                // columns, k = output rows), zeros in the padding.  The warp's share
+                // of one slice is its 32 image rows x the slice's 64 bytes of k in
+                // each plane: 2 KB per plane, contiguous in the image.  Both planes
+                // are assembled in shared memory (16-byte slots XOR-swizzled by chunk
+                // against bank conflicts), then written with 16-byte stores.  Each
+                // lane holds one k (output row).  TF32 slices hold 16 k: the 16 lanes
+                // that own the slice write image rows 0..15 and the other 16 write
+                // rows 16..31 with the owners' values (lane ^ 16); BF16 slices hold
+                // 32 k, one per lane.
+                constexpr int tk = FMT == kFmtBF16 ? 32 : 16;
                 constexpr int esize = FMT == kFmtBF16 ? 2 : 4;
-                constexpr int run = 8 * 32 * esize;  // bytes per 8-row group
-                const int slice = r0 / tk;
-                const int kb0 = (r0 % tk) * esize;   // first k byte of the warp in a row
-                const int kk = lane * esize;         // this lane's k byte within the warp's span
-                if (slice < g.t_slices) {
-                    unsigned char* img = t_out + g.t_img + ((int64_t)tile.pn * g.t_slices + slice) * kImageB;
-                    const bool row_ok = row < TM && (tile.pm * TM + row) < g.m;
-                    const int c = kk >> 4;           // 16-byte chunk within the span
+                constexpr int JN = FMT == kFmtBF16 ? ECOLS : ECOLS / 2;  // image rows per lane and slice
+                constexpr int PSH = ECOLS * kPackRowBytes;                // staging bytes per plane
+                const int grow = r0 + lane;
+                const int kb = (grow % tk) * esize;          // byte of this lane's k within the slice
+                const int cc = kb >> 4;                      // its 16-byte chunk
+                uint32_t xo[8];                              // staging offset of image row q (mod 8)
 #pragma unroll
-                    for (int p = 0; p < 2; ++p) {
+                for (int q = 0; q < 8; ++q) xo[q] = cc * LBO + ((q ^ cc) & 7) * 16 + (kb & 15);
+                const int prow = panel_rows(g.n, tile.pn);   // image rows of this panel
+                const int wrows = min(ECOLS, prow - cq * ECOLS);  // of them this warp's (multiple of 8)
+#pragma unroll 1
+                for (int si = 0; si < 32 / tk; ++si) {
+                    const int slice = r0 / tk + si;
+                    if (slice >= g.t_slices) break;
+                    const bool owner = lane / tk == si;      // always true for BF16
+                    const int jo = owner ? 0 : JN;           // first image row this lane writes
+                    // rows jj < ncol hold data (the row of the value is the lane's or its partner's)
+                    const int ncol = (owner ? grow : (grow ^ 16)) < g.m ? g.n - c0 - jo : 0;
+                    unsigned char* sb = stg + (jo >> 3) * SBO;
 #pragma unroll
-                        for (int j = 0; j < TN; ++j) {
-                            const int col = tile.pn * TN + j;
-                            const double v = (row_ok && col < g.n) ? sum[j] : 0.0;
-                            const int so = (j >> 3) * run + c * 128 + (((j & 7) ^ c) & 7) * 16 + (kk & 15);
-                            if constexpr (FMT == kFmtBF16) {
-                                uint16_t hb, lb;
-                                split_bf16(v, hb, lb);
-                                *reinterpret_cast<uint16_t*>(stg + so) = p ? lb : hb;
-                            } else {
-                                uint32_t hb, lb;
-                                split(v, hb, lb);
-                                *reinterpret_cast<uint32_t*>(stg + so) = p ? lb : hb;
+                    for (int jj = 0; jj < JN; ++jj) {
+                        double x = sum[jj];
+                        if constexpr (FMT != kFmtBF16) {
+                            const double y = __shfl_xor_sync(0xffffffffu, sum[jj + JN], 16);
+                            x = owner ? x : y;
+                        }
+                        const double v = jj < ncol ? x : 0.0;
+                        unsigned char* so = sb + (jj >> 3) * SBO + xo[jj & 7];
+                        if constexpr (FMT == kFmtBF16) {
+                            uint16_t hb, lb;
+                            split_bf16(v, hb, lb);
+                            *reinterpret_cast<uint16_t*>(so) = hb;
+                            *reinterpret_cast<uint16_t*>(so + PSH) = lb;
+                        } else {
+                            uint32_t hb, lb;
+                            split(v, hb, lb);
+                            *reinterpret_cast<uint32_t*>(so) = hb;
+                            *reinterpret_cast<uint32_t*>(so + PSH) = lb;
+                        }
+                    }
+                    __syncwarp();
+                    if (wrows > 0) {
+                        unsigned char* img = t_out + g.t_img + (int64_t)tile.pn * g.t_slices * kImage +
+                                             (int64_t)slice * 2 * prow * kPackRowBytes + cq * (ECOLS / 8) * SBO;
+                        const int nu = wrows * kPackRowBytes / 16;   // 16-byte units per plane
+#pragma unroll
+                        for (int p = 0; p < 2; ++p) {
+                            unsigned char* dst = img + p * prow * kPackRowBytes;
+                            for (int u = lane; u < nu; u += 32) {
+                                const int grp = (u * 16) / SBO, rem = (u * 16) % SBO;
+                                const int c2 = rem / LBO, slot = (rem / 16) & 7;
+                                *reinterpret_cast<uint4*>(dst + grp * SBO + c2 * LBO + ((slot ^ c2) & 7) * 16) =
+                                    *reinterpret_cast<const uint4*>(stg + p * PSH + u * 16);
                             }
                         }
-                        __syncwarp();
-                        unsigned char* dst = img + p * PLANE_B + kb0 * 8;
-#pragma unroll
-                        for (int u = lane; u < 8 * run / 16; u += 32) {
-                            const int grp = (u * 16) / run, rem = (u * 16) % run;
-                            const int cc = rem >> 7, slot = (rem >> 4) & 7;
-                            *reinterpret_cast<uint4*>(dst + grp * SBO + cc * LBO + ((slot ^ cc) & 7) * 16) =
-                                *reinterpret_cast<const uint4*>(stg + u * 16);
-                        }
-                        __syncwarp();
                     }
+                    __syncwarp();
                 }
             }
-        }
         }
     }
     __syncwarp();  // producer and MMA warps: lanes 1..31 wait for lane 0
@@ -497,7 +547,7 @@ __global__ void __launch_bounds__(256) split_reduce_tf32_kernel(double* __restri
 
 }  // namespace
 
-int64_t PackSchedule::add(int64_t src_off, int rows, int k, int ld, bool trans, int prow) {
+int64_t PackSchedule::add(int64_t src_off, int rows, int k, int ld, bool trans) {
     const int tk = pack_k(fmt);
     PackJob j{};
     j.fmt = fmt;
@@ -507,14 +557,13 @@ int64_t PackSchedule::add(int64_t src_off, int rows, int k, int ld, bool trans, 
     j.k = k;
     j.ld = ld;
     j.trans = trans ? 1 : 0;
-    j.prow = prow;
     j.slices = (k + tk - 1) / tk;
-    const int panels = (rows + prow - 1) / prow;
+    const int panels = (rows + kPackRows - 1) / kPackRows;
     const int job = (int)jobs.size();
     jobs.push_back(j);
     for (int p = 0; p < panels; ++p)
         for (int s = 0; s < j.slices; ++s) images.push_back(PackImage{job, p, s, 0});
-    bytes += (int64_t)panels * j.slices * 2 * prow * kPackRowBytes;
+    bytes += image_bytes(rows, j.slices);
     return j.img_off;
 }
 
@@ -622,20 +671,18 @@ int PackedSchedule::finalize(cudaStream_t stream, int num_sms) {
 int PackedSchedule::check_bounds(int64_t a_bytes, int64_t b_bytes, int64_t c_size, int64_t t_bytes) const {
     for (const PackedGroup& g : groups) {
         if (g.m <= 0 || g.n <= 0) continue;
-        const int64_t pm = (g.m + TM - 1) / TM, pn = (g.n + TN - 1) / TN;
         for (int t = g.t0; t < g.t1; ++t) {
             const PackedTerm& tm = terms[t];
-            if (tm.a_img < 0 || tm.a_img + pm * tm.slices * kImageA > a_bytes || tm.b_img < 0 ||
-                tm.b_img + pn * tm.slices * kImageB > b_bytes || tm.a_img % 16 || tm.b_img % 16)
+            if (tm.a_img < 0 || tm.a_img + image_bytes(g.m, tm.slices) > a_bytes || tm.b_img < 0 ||
+                tm.b_img + image_bytes(g.n, tm.slices) > b_bytes || tm.a_img % 16 || tm.b_img % 16)
                 return set_error(DMRG_E_ARG, "packed GEMM term %d reads outside its images", t);
         }
         if (out_mode == 0) {
             if (g.c_off < 0 || g.c_off + (int64_t)(g.m - 1) * g.ldc + g.n > c_size || g.n > g.ldc)
                 return set_error(DMRG_E_ARG, "packed GEMM output %lld outside %lld", (long long)g.c_off,
                                  (long long)c_size);
-        } else if (g.t_img < 0 || g.t_img + pn * g.t_slices * kImageB > t_bytes ||
-                   (int64_t)g.t_slices * pack_k(fmt) < g.m ||
-                   g.t_img % 16) {
+        } else if (g.t_img < 0 || g.t_img + image_bytes(g.n, g.t_slices) > t_bytes ||
+                   (int64_t)g.t_slices * pack_k(fmt) < g.m || g.t_img % 16) {
             return set_error(DMRG_E_ARG, "packed GEMM output images outside their buffer");
         }
     }

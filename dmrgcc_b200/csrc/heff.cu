@@ -136,7 +136,7 @@ int build_heff(dmrg_heff_s& h) {
         // in the B role, and the K*R intermediates written directly as B-role images
         std::vector<int64_t> psi_img(ket.count());
         for (int pos = 0; pos < ket.count(); ++pos)
-            psi_img[pos] = h.pk_psi.add(ket.off[pos], ket.rows[pos], ket.cols[pos], ket.cols[pos], false, kPackRowsA);
+            psi_img[pos] = h.pk_psi.add(ket.off[pos], ket.rows[pos], ket.cols[pos], ket.cols[pos], false);
         std::map<int64_t, int64_t> r_img, l_img;
         const int tk = pack_k(fmt);
         auto slices = [tk](int k) { return (k + tk - 1) / tk; };
@@ -148,9 +148,9 @@ int build_heff(dmrg_heff_s& h) {
             const TaskA& t = tasks[i];
             auto it = r_img.find(t.r_off);
             if (it == r_img.end())
-                it = r_img.emplace(t.r_off, h.pk_R.add(t.r_off, t.b_j, t.b_l, t.b_j, true, kPackRowsB)).first;
+                it = r_img.emplace(t.r_off, h.pk_R.add(t.r_off, t.b_j, t.b_l, t.b_j, true)).first;
             t_img[i] = h.t_img_bytes;
-            h.t_img_bytes += (int64_t)((t.b_j + kPackRowsB - 1) / kPackRowsB) * slices(t.a_k) * kImageB;
+            h.t_img_bytes += image_bytes(t.b_j, slices(t.a_k));
             PackedGroup g{};
             g.t0 = (int)h.pa.terms.size();
             g.m = t.a_k;
@@ -175,7 +175,7 @@ int build_heff(dmrg_heff_s& h) {
                 const TermB& t = termsB[i];
                 auto it = l_img.find(t.l_off);
                 if (it == l_img.end())
-                    it = l_img.emplace(t.l_off, h.pk_L.add(t.l_off, ket.rows[pos2], t.k, t.lda, false, kPackRowsA)).first;
+                    it = l_img.emplace(t.l_off, h.pk_L.add(t.l_off, ket.rows[pos2], t.k, t.lda, false)).first;
                 h.pb.terms.push_back(PackedTerm{it->second, t_img[t.t_index], slices(t.k), 0, t.w});
             }
             g.t1 = (int)h.pb.terms.size();
