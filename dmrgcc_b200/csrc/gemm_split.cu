@@ -46,7 +46,10 @@ namespace dmrg {
 namespace {
 
 constexpr int TM = kPackRows, TN = kPackRows;
-constexpr int NSTAGE = 5;
+#ifndef DMRG_SPLIT_STAGES
+#define DMRG_SPLIT_STAGES 6
+#endif
+constexpr int NSTAGE = DMRG_SPLIT_STAGES;
 constexpr int STAGE_BYTES = 2 * kImage;                     // 32 KB: A image, then B image
 constexpr int LBO = 128;  // bytes between the 16-byte k chunks of one 8-row core-matrix group
 constexpr int SBO = 512;  // bytes between 8-row groups: a group's 4 chunks are contiguous
@@ -58,15 +61,15 @@ constexpr int KSUB = kPackRowBytes / 32;                     // MMAs (32 bytes o
 constexpr int NEPI = DMRG_SPLIT_EPILOGUE_WARPS;              // epilogue warps: 4 per TMEM lane quarter x column parts
 constexpr int NT = 32 * (2 + NEPI);
 constexpr int ECOLS = TN * 4 / NEPI;                         // accumulator columns per epilogue warp
-// Epilogue staging per epilogue warp: 32 output rows x 16 doubles (16 columns
-// at a time), or both planes of the warp's share of one slice of an output
-// image (ECOLS image rows x 64 bytes of k, twice).
+// Epilogue staging per epilogue warp, 4 KB: 32 output rows x 16 doubles (16
+// columns at a time), or one plane of the warp's share of one slice of an output
+// image (ECOLS image rows x 64 bytes of k).
 constexpr int EPI_OFF = NSTAGE * STAGE_BYTES;
-constexpr int EPI_WARP_BYTES = 2 * ECOLS * kPackRowBytes;
+constexpr int EPI_WARP_BYTES = 4096;
 constexpr int BAR_OFF = EPI_OFF + NEPI * EPI_WARP_BYTES;
 constexpr int SMEM_BYTES = BAR_OFF + 256;
 static_assert(NEPI % 4 == 0 && ECOLS % 16 == 0 && ECOLS * NEPI == 4 * TN && TM == 128, "epilogue geometry");
-static_assert(EPI_WARP_BYTES >= 32 * 16 * 8, "staging holds 32 rows x 16 doubles");
+static_assert(EPI_WARP_BYTES >= 32 * 16 * 8 && EPI_WARP_BYTES >= ECOLS * kPackRowBytes, "staging sizes");
 constexpr uint32_t TMEM_COLS = 2 * TN;                       // two 128-column accumulators
 constexpr long long kWaitLimit = 4000000;                    // try_wait polls before a wait gives up
 
@@ -450,71 +453,57 @@ __global__ void __launch_bounds__(NT, 1) gemm_split_kernel(const unsigned char* 
                 }
             } else {
                 // The output as B-role images of X = output^T (image rows = output
-                // columns, k = output rows), zeros in the padding.  The warp's share
-                // of one slice is its 32 image rows x the slice's 64 bytes of k in
-                // each plane: 2 KB per plane, contiguous in the image.  Both planes
-                // are assembled in shared memory (16-byte slots XOR-swizzled by chunk
-                // against bank conflicts), then written with 16-byte stores.  Each
-                // lane holds one k (output row).  TF32 slices hold 16 k: the 16 lanes
-                // that own the slice write image rows 0..15 and the other 16 write
-                // rows 16..31 with the owners' values (lane ^ 16); BF16 slices hold
-                // 32 k, one per lane.
+                // columns, k = output rows), zeros in the padding.  The warp's 32
+                // output rows are 32 consecutive k: two TF32 slices or one BF16 slice.
+                // Per pass of 16 columns the rows go through the staging buffer
+                // (as above); each lane then reads one 16-byte chunk's worth of k
+                // (4 TF32 or 8 BF16 values) of one image row, splits them and
+                // stores the hi and lo chunks.  The 32 lanes of one store cover 8
+                // image rows x 4 chunks: 512 contiguous bytes of a plane.
                 constexpr int tk = FMT == kFmtBF16 ? 32 : 16;
-                constexpr int esize = FMT == kFmtBF16 ? 2 : 4;
-                constexpr int JN = FMT == kFmtBF16 ? ECOLS : ECOLS / 2;  // image rows per lane and slice
-                constexpr int PSH = ECOLS * kPackRowBytes;                // staging bytes per plane
-                const int grow = r0 + lane;
-                const int kb = (grow % tk) * esize;          // byte of this lane's k within the slice
-                const int cc = kb >> 4;                      // its 16-byte chunk
-                uint32_t xo[8];                              // staging offset of image row q (mod 8)
+                constexpr int kc = FMT == kFmtBF16 ? 8 : 4;          // k per 16-byte chunk
+                constexpr int NIT = 32 / tk * 2;                     // (slice, 8-row group) pairs per pass
+                double* sd = reinterpret_cast<double*>(stg);         // 32 rows x 16, (r, c) at r*16 + (c ^ (r & 15))
+                const int prow = panel_rows(g.n, tile.pn);           // image rows of this panel
+                const int j8 = lane & 7, cs = lane >> 3;             // row in an 8-row group, chunk in a slice
 #pragma unroll
-                for (int q = 0; q < 8; ++q) xo[q] = cc * LBO + ((q ^ cc) & 7) * 16 + (kb & 15);
-                const int prow = panel_rows(g.n, tile.pn);   // image rows of this panel
-                const int wrows = min(ECOLS, prow - cq * ECOLS);  // of them this warp's (multiple of 8)
-#pragma unroll 1
-                for (int si = 0; si < 32 / tk; ++si) {
-                    const int slice = r0 / tk + si;
-                    if (slice >= g.t_slices) break;
-                    const bool owner = lane / tk == si;      // always true for BF16
-                    const int jo = owner ? 0 : JN;           // first image row this lane writes
-                    // rows jj < ncol hold data (the row of the value is the lane's or its partner's)
-                    const int ncol = (owner ? grow : (grow ^ 16)) < g.m ? g.n - c0 - jo : 0;
-                    unsigned char* sb = stg + (jo >> 3) * SBO;
+                for (int h = 0; h < ECOLS / 16; ++h) {
 #pragma unroll
-                    for (int jj = 0; jj < JN; ++jj) {
-                        double x = sum[jj];
-                        if constexpr (FMT != kFmtBF16) {
-                            const double y = __shfl_xor_sync(0xffffffffu, sum[jj + JN], 16);
-                            x = owner ? x : y;
-                        }
-                        const double v = jj < ncol ? x : 0.0;
-                        unsigned char* so = sb + (jj >> 3) * SBO + xo[jj & 7];
-                        if constexpr (FMT == kFmtBF16) {
-                            uint16_t hb, lb;
-                            split_bf16(v, hb, lb);
-                            *reinterpret_cast<uint16_t*>(so) = hb;
-                            *reinterpret_cast<uint16_t*>(so + PSH) = lb;
-                        } else {
-                            uint32_t hb, lb;
-                            split(v, hb, lb);
-                            *reinterpret_cast<uint32_t*>(so) = hb;
-                            *reinterpret_cast<uint32_t*>(so + PSH) = lb;
-                        }
-                    }
+                    for (int j = 0; j < 16; ++j) sd[lane * 16 + (j ^ (lane & 15))] = sum[h * 16 + j];
                     __syncwarp();
-                    if (wrows > 0) {
-                        unsigned char* img = t_out + g.t_img + (int64_t)tile.pn * g.t_slices * kImage +
-                                             (int64_t)slice * 2 * prow * kPackRowBytes + cq * (ECOLS / 8) * SBO;
-                        const int nu = wrows * kPackRowBytes / 16;   // 16-byte units per plane
 #pragma unroll
-                        for (int p = 0; p < 2; ++p) {
-                            unsigned char* dst = img + p * prow * kPackRowBytes;
-                            for (int u = lane; u < nu; u += 32) {
-                                const int grp = (u * 16) / SBO, rem = (u * 16) % SBO;
-                                const int c2 = rem / LBO, slot = (rem / 16) & 7;
-                                *reinterpret_cast<uint4*>(dst + grp * SBO + c2 * LBO + ((slot ^ c2) & 7) * 16) =
-                                    *reinterpret_cast<const uint4*>(stg + p * PSH + u * 16);
+                    for (int it = 0; it < NIT; ++it) {
+                        const int sh = it >> 1, gj = it & 1;         // slice of the warp's two (TF32), row group
+                        const int jx = gj * 8 + j8;                  // column within the pass
+                        const int jl = cq * ECOLS + h * 16 + jx;     // image row within the panel
+                        const int slice = (r0 + sh * tk) / tk;
+                        const int rk0 = sh * tk + cs * kc;           // first of this chunk's k, within the warp's rows
+                        if (jl < prow && slice < g.t_slices) {
+                            const bool col_ok = c0 + h * 16 + jx < g.n;
+                            uint32_t hw[4], lw[4];
+#pragma unroll
+                            for (int q = 0; q < 4; ++q) {
+                                if constexpr (FMT == kFmtBF16) {
+                                    uint16_t hb[2], lb[2];
+#pragma unroll
+                                    for (int e = 0; e < 2; ++e) {
+                                        const int rk = rk0 + 2 * q + e;
+                                        const double v = (col_ok && r0 + rk < g.m) ? sd[rk * 16 + (jx ^ (rk & 15))] : 0.0;
+                                        split_bf16(v, hb[e], lb[e]);
+                                    }
+                                    hw[q] = (uint32_t)hb[0] | ((uint32_t)hb[1] << 16);
+                                    lw[q] = (uint32_t)lb[0] | ((uint32_t)lb[1] << 16);
+                                } else {
+                                    const int rk = rk0 + q;
+                                    const double v = (col_ok && r0 + rk < g.m) ? sd[rk * 16 + (jx ^ (rk & 15))] : 0.0;
+                                    split(v, hw[q], lw[q]);
+                                }
                             }
+                            unsigned char* dst = t_out + g.t_img + (int64_t)tile.pn * g.t_slices * kImage +
+                                                 (int64_t)slice * 2 * prow * kPackRowBytes + (jl >> 3) * SBO + cs * LBO +
+                                                 j8 * 16;
+                            *reinterpret_cast<uint4*>(dst) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+                            *reinterpret_cast<uint4*>(dst + prow * kPackRowBytes) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
                         }
                     }
                     __syncwarp();
