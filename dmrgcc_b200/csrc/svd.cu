@@ -14,7 +14,7 @@ namespace {
 constexpr int kBlk = 32;        // columns per block
 constexpr int kPair = 64;       // columns per pair
 constexpr int kChunk = 32;      // rows per streamed chunk
-constexpr int kThreads = 256;
+constexpr int kThreads = 512;   // pair-solve CTA
 constexpr int kLd = kPair + 1;  // padded row of the shared 64x64 matrices
 constexpr int kInnerSweeps = 2;
 constexpr int kMaxSweeps = 40;
@@ -31,6 +31,7 @@ struct SvdSmem {
     int pq[kPair];
     double red[kThreads / 32];
     double flag;
+    int active;   // the current step rotates something
 };
 
 __device__ __forceinline__ void rr_pair(int r, int i, int N, int& p, int& q) {
@@ -173,7 +174,12 @@ __global__ void __launch_bounds__(kThreads) solve_kernel(const SvdProblem* __res
     }
     if (worst <= tol) return;  // pair already orthogonal: nothing to rotate
 
+    // A pair whose off-diagonal measure is at or below tol needs no rotation (the
+    // same test decides convergence); a step that rotates nothing skips the
+    // update, and an inner sweep that rotates nothing ends the solve.
+    static_assert((kPair / 2) * (kPair / 2) % kThreads == 0 && (kPair / 2) * kPair % kThreads == 0, "even split");
     for (int sweep = 0; sweep < inner_sweeps; ++sweep) {
+        int rotated = 0;
         for (int r = 0; r < kPair - 1; ++r) {
             if (threadIdx.x < kPair / 2) {
                 int a, b;
@@ -181,48 +187,66 @@ __global__ void __launch_bounds__(kThreads) solve_kernel(const SvdProblem* __res
                 const double apq = S.G[a * kLd + b];
                 double c = 1.0, s = 0.0;
                 const double daa = S.G[a * kLd + a], dbb = S.G[b * kLd + b];
-                if (apq != 0.0 && daa > zero2 && dbb > zero2 &&
-                    fabs(apq) > DBL_EPSILON * 1e-3 * fro * sqrt(fmax(daa, dbb))) {
-                    const double tau = (dbb - daa) / (2.0 * apq);
-                    const double tt = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
-                    c = 1.0 / sqrt(1.0 + tt * tt);
-                    s = tt * c;
+                if (daa > zero2 && dbb > zero2 && fabs(apq) > tol * fro * sqrt(fmax(daa, dbb))) {
+                    // The rotation with tan = sign(x) y / (|x| + sqrt(x^2 + y^2)),
+                    // x = dbb - daa, y = 2 apq (the smaller root of the Jacobi
+                    // equation), as c = u / sqrt(u^2 + y^2), s = sign(x) y / sqrt(u^2 + y^2)
+                    // with u = |x| + sqrt(x^2 + y^2): no division.
+                    const double x = dbb - daa, y = 2.0 * apq;
+                    const double u = fabs(x) + sqrt(x * x + y * y);
+                    const double rn = rsqrt(u * u + y * y);
+                    c = u * rn;
+                    s = (x >= 0.0 ? y : -y) * rn;
                 }
                 S.cs[2 * threadIdx.x] = c;
                 S.cs[2 * threadIdx.x + 1] = s;
                 S.pq[2 * threadIdx.x] = a;
                 S.pq[2 * threadIdx.x + 1] = b;
+                const bool any = __any_sync(0xffffffffu, s != 0.0);
+                if (threadIdx.x == 0) S.active = any ? 1 : 0;
             }
             __syncthreads();
+            if (!S.active) {
+                __syncthreads();  // every thread has read the flag before the next step rewrites it
+                continue;
+            }
+            rotated = 1;
             // G <- J^T G J in one pass: every 2x2 block (rows of pair i, columns of
             // pair j) gets both rotations at once; Q <- Q J
-            for (int idx = threadIdx.x; idx < (kPair / 2) * (kPair / 2); idx += kThreads) {
+#pragma unroll
+            for (int u = 0; u < (kPair / 2) * (kPair / 2) / kThreads; ++u) {
+                const int idx = threadIdx.x + u * kThreads;
                 const int i = idx / (kPair / 2), j = idx % (kPair / 2);
                 const double si = S.cs[2 * i + 1], sj = S.cs[2 * j + 1];
-                if (si == 0.0 && sj == 0.0) continue;
-                const double ci = S.cs[2 * i], cj = S.cs[2 * j];
-                const int ai = S.pq[2 * i], bi = S.pq[2 * i + 1], aj = S.pq[2 * j], bj = S.pq[2 * j + 1];
-                const double x11 = S.G[ai * kLd + aj], x12 = S.G[ai * kLd + bj];
-                const double x21 = S.G[bi * kLd + aj], x22 = S.G[bi * kLd + bj];
-                const double y11 = ci * x11 - si * x21, y12 = ci * x12 - si * x22;  // rows
-                const double y21 = si * x11 + ci * x21, y22 = si * x12 + ci * x22;
-                S.G[ai * kLd + aj] = cj * y11 - sj * y12;                            // columns
-                S.G[ai * kLd + bj] = sj * y11 + cj * y12;
-                S.G[bi * kLd + aj] = cj * y21 - sj * y22;
-                S.G[bi * kLd + bj] = sj * y21 + cj * y22;
+                if (si != 0.0 || sj != 0.0) {
+                    const double ci = S.cs[2 * i], cj = S.cs[2 * j];
+                    const int ai = S.pq[2 * i], bi = S.pq[2 * i + 1], aj = S.pq[2 * j], bj = S.pq[2 * j + 1];
+                    const double x11 = S.G[ai * kLd + aj], x12 = S.G[ai * kLd + bj];
+                    const double x21 = S.G[bi * kLd + aj], x22 = S.G[bi * kLd + bj];
+                    const double y11 = ci * x11 - si * x21, y12 = ci * x12 - si * x22;  // rows
+                    const double y21 = si * x11 + ci * x21, y22 = si * x12 + ci * x22;
+                    S.G[ai * kLd + aj] = cj * y11 - sj * y12;                            // columns
+                    S.G[ai * kLd + bj] = sj * y11 + cj * y12;
+                    S.G[bi * kLd + aj] = cj * y21 - sj * y22;
+                    S.G[bi * kLd + bj] = sj * y21 + cj * y22;
+                }
             }
-            for (int idx = threadIdx.x; idx < (kPair / 2) * kPair; idx += kThreads) {
+#pragma unroll
+            for (int u = 0; u < (kPair / 2) * kPair / kThreads; ++u) {
+                const int idx = threadIdx.x + u * kThreads;
                 const int j = idx / kPair, row = idx % kPair;
                 const double sj = S.cs[2 * j + 1];
-                if (sj == 0.0) continue;
-                const double cj = S.cs[2 * j];
-                const int a = S.pq[2 * j], b = S.pq[2 * j + 1];
-                const double qa = S.Q[row * kLd + a], qb = S.Q[row * kLd + b];
-                S.Q[row * kLd + a] = cj * qa - sj * qb;
-                S.Q[row * kLd + b] = sj * qa + cj * qb;
+                if (sj != 0.0) {
+                    const double cj = S.cs[2 * j];
+                    const int a = S.pq[2 * j], b = S.pq[2 * j + 1];
+                    const double qa = S.Q[row * kLd + a], qb = S.Q[row * kLd + b];
+                    S.Q[row * kLd + a] = cj * qa - sj * qb;
+                    S.Q[row * kLd + b] = sj * qa + cj * qb;
+                }
             }
             __syncthreads();
         }
+        if (!rotated) break;  // uniform: every thread saw the same flags
     }
     double* R = rot + (int64_t)blockIdx.x * kPair * kPair;
     for (int idx = threadIdx.x; idx < kPair * kPair; idx += kThreads) R[idx] = S.Q[(idx / kPair) * kLd + idx % kPair];
