@@ -145,22 +145,6 @@ __global__ void __launch_bounds__(NT) gemm_f64_kernel(const double* __restrict__
     const int fr = lane >> 2, fc = lane & 3;
     const bool acc_out = accumulate && g.cbuf == 0;
     double* Cb = g.cbuf ? Caux : C;
-    // With accumulation every old value is loaded before the first store: a load
-    // after a store through the same pointer would wait for it.
-    if (acc_out) {
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            const int row = tile.m0 + wm * 32 + i * 8 + fr;
-            const double* crow = Cb + g.c_off + (int64_t)row * g.ldc;
-#pragma unroll
-            for (int j = 0; j < 4; ++j)
-#pragma unroll
-                for (int e = 0; e < 2; ++e) {
-                    const int col = tile.n0 + wn * 32 + j * 8 + fc * 2 + e;
-                    if (row < g.m && col < g.n) acc[i][j][e] += crow[col];
-                }
-        }
-    }
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
         const int row = tile.m0 + wm * 32 + i * 8 + fr;
@@ -171,7 +155,7 @@ __global__ void __launch_bounds__(NT) gemm_f64_kernel(const double* __restrict__
 #pragma unroll
             for (int e = 0; e < 2; ++e) {
                 const int col = tile.n0 + wn * 32 + j * 8 + fc * 2 + e;
-                if (col < g.n) crow[col] = acc[i][j][e];
+                if (col < g.n) crow[col] = acc_out ? crow[col] + acc[i][j][e] : acc[i][j][e];
             }
         }
     }
