@@ -232,32 +232,92 @@ __global__ void __launch_bounds__(kJacobiThreads) sym_jacobi_kernel(double* A, i
             for (int i = 0; i < n; ++i) Zout[i * n + k] = -Zout[i * n + k];
 }
 
-__global__ void __launch_bounds__(kJacobiThreads) tridiag_vector_kernel(const double* __restrict__ alpha,
-                                                                        const double* __restrict__ beta,
-                                                                        const int* m_dev, double* y, double* ws,
-                                                                        int* status) {
+// Ground vector of the Lanczos tridiagonal T (alpha, beta; size *m_dev) by
+// inverse iteration at its lowest eigenvalue lam = E[m - 1] (from the
+// bisection, accurate to rounding): T - lam I is factored once by Gaussian
+// elimination with partial pivoting (the tridiagonal scheme of LAPACK's
+// dgttrf: pivoting rows k, k+1 fills a second superdiagonal), pivots below
+// eps * ||T||_1 are raised to that size (the matrix is singular to rounding by
+// construction), and three solves starting from the vector of ones give the
+// eigenvector (normalised; the sign convention of eigvec_sign).  One thread:
+// the recurrences are serial and m <= kMaxVec.
+constexpr int kTriMax = 512;
+__global__ void __launch_bounds__(32) tridiag_vector_kernel(const double* __restrict__ alpha,
+                                                            const double* __restrict__ beta,
+                                                            const double* __restrict__ E, const int* m_dev,
+                                                            double* y, int* status) {
+    __shared__ double d[kTriMax], du[kTriMax], du2[kTriMax], dl[kTriMax], x[kTriMax];
+    __shared__ unsigned char swp[kTriMax];
+    if (threadIdx.x != 0) return;
     const int n = *m_dev;
-    double* A = ws;
-    double* Z = ws + (size_t)n * n;
-    for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
-        const int i = idx / n, j = idx % n;
-        A[idx] = i == j ? alpha[i] : (j == i + 1 ? beta[i] : (i == j + 1 ? beta[j] : 0.0));
+    if (n <= 0 || n > kTriMax) {
+        status[0] = DMRG_E_NUMERIC;
+        return;
     }
-    __syncthreads();
-    const bool ok = jacobi_core(A, n, Z);
-    __shared__ int kmin;
-    if (threadIdx.x == 0) {
-        if (!ok) status[0] = DMRG_E_NUMERIC;
-        int best = 0;
-        for (int k = 1; k < n; ++k)
-            if (A[k * n + k] < A[best * n + best]) best = k;
-        kmin = best;
+    if (n == 1) {
+        y[0] = 1.0;
+        return;
     }
-    __syncthreads();
-    __shared__ double sgn;
-    if (threadIdx.x == 0) sgn = eigvec_sign(Z + kmin, n, n);
-    __syncthreads();
-    for (int i = threadIdx.x; i < n; i += blockDim.x) y[i] = sgn * Z[i * n + kmin];
+    const double lam = E[n - 1];
+    double tnorm = 0.0;  // ||T||_1
+    for (int k = 0; k < n; ++k) {
+        d[k] = alpha[k] - lam;
+        tnorm = fmax(tnorm, fabs(alpha[k]) + (k > 0 ? fabs(beta[k - 1]) : 0.0) + (k + 1 < n ? fabs(beta[k]) : 0.0));
+        if (k + 1 < n) dl[k] = du[k] = beta[k];
+    }
+    const double tiny = DBL_EPSILON * fmax(tnorm, DBL_MIN);
+    // factor: rows k and k+1 are swapped when the subdiagonal entry is larger
+    for (int k = 0; k + 1 < n; ++k) {
+        if (fabs(d[k]) >= fabs(dl[k])) {
+            swp[k] = 0;
+            const double f = d[k] != 0.0 ? dl[k] / d[k] : 0.0;
+            dl[k] = f;
+            d[k + 1] -= f * du[k];
+            du2[k] = 0.0;
+        } else {
+            swp[k] = 1;
+            const double f = d[k] / dl[k];
+            d[k] = dl[k];
+            dl[k] = f;
+            const double t = du[k];
+            du[k] = d[k + 1];
+            d[k + 1] = t - f * d[k + 1];
+            if (k + 2 < n) {
+                du2[k] = du[k + 1];
+                du[k + 1] = -f * du[k + 1];
+            } else {
+                du2[k] = 0.0;
+            }
+        }
+    }
+    for (int k = 0; k < n; ++k)
+        if (fabs(d[k]) < tiny) d[k] = d[k] < 0.0 ? -tiny : tiny;
+    for (int k = 0; k < n; ++k) x[k] = 1.0;
+    for (int it = 0; it < 3; ++it) {
+        for (int k = 0; k + 1 < n; ++k) {  // L solve, with the row swaps
+            if (swp[k]) {
+                const double t = x[k];
+                x[k] = x[k + 1];
+                x[k + 1] = t - dl[k] * x[k];
+            } else {
+                x[k + 1] -= dl[k] * x[k];
+            }
+        }
+        x[n - 1] /= d[n - 1];  // U solve
+        x[n - 2] = (x[n - 2] - du[n - 2] * x[n - 1]) / d[n - 2];
+        for (int k = n - 3; k >= 0; --k) x[k] = (x[k] - du[k] * x[k + 1] - du2[k] * x[k + 2]) / d[k];
+        double mx = 0.0;
+        for (int k = 0; k < n; ++k) mx = fmax(mx, fabs(x[k]));
+        if (!(mx > 0.0) || !isfinite(mx)) {
+            status[0] = DMRG_E_NUMERIC;
+            return;
+        }
+        for (int k = 0; k < n; ++k) x[k] /= mx;  // keeps the next solve in range
+    }
+    double nrm = 0.0;
+    for (int k = 0; k < n; ++k) nrm += x[k] * x[k];
+    const double sc = eigvec_sign(x, n, 1) / sqrt(nrm);
+    for (int k = 0; k < n; ++k) y[k] = sc * x[k];
 }
 
 }  // namespace
@@ -281,9 +341,9 @@ int launch_sym_jacobi(double* A, int n, double* w, double* Z, double* ws, int* s
     return DMRG_OK;
 }
 
-int launch_tridiag_ground_vector(const double* alpha, const double* beta, const int* m_dev, int m_max, double* y,
-                                 double* ws, int* status, cudaStream_t st) {
-    tridiag_vector_kernel<<<1, kJacobiThreads, jacobi_smem(m_max), st>>>(alpha, beta, m_dev, y, ws, status);
+int launch_tridiag_ground_vector(const double* alpha, const double* beta, const double* E, const int* m_dev,
+                                 double* y, int* status, cudaStream_t st) {
+    tridiag_vector_kernel<<<1, 32, 0, st>>>(alpha, beta, E, m_dev, y, status);
     DMRG_CUDA_TRY(cudaGetLastError());
     return DMRG_OK;
 }

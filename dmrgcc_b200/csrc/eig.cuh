@@ -20,10 +20,11 @@ int launch_tridiag_lowest(const double* alpha, const double* beta, int m, double
 // 2*n*n + 4*n doubles.  status[0] = DMRG_E_NUMERIC if 60 sweeps did not converge.
 int launch_sym_jacobi(double* A, int n, double* w, double* Z, double* ws, int* status, cudaStream_t st);
 
-// Same as launch_sym_jacobi for the tridiagonal (alpha, beta) of size *m_dev
-// (read on the device: the Lanczos dimension is only known there).  Only the
-// eigenvector of the lowest eigenvalue is kept: y[0..m).
-int launch_tridiag_ground_vector(const double* alpha, const double* beta, const int* m_dev, int m_max, double* y,
-                                 double* ws, int* status, cudaStream_t st);
+// Eigenvector y[0..m) of the tridiagonal (alpha, beta) of size *m_dev (read on
+// the device: the Lanczos dimension is only known there) for its lowest
+// eigenvalue E[m - 1], by inverse iteration; unit norm, largest component
+// positive.  status[0] = DMRG_E_NUMERIC on m > 512 or a non-finite iterate.
+int launch_tridiag_ground_vector(const double* alpha, const double* beta, const double* E, const int* m_dev,
+                                 double* y, int* status, cudaStream_t st);
 
 }  // namespace dmrg

@@ -132,6 +132,13 @@ int krylov(dmrg_heff_s& h, double* psi, int niter, double precision, double zero
     DMRG_CUDA_TRY(cudaMemcpyAsync(V, psi, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
     DMRG_CUDA_TRY(cudaMemsetAsync(hv, 0, n * sizeof(double), st));
     DMRG_CUDA_TRY(cudaMemsetAsync(state, 0, 16 * sizeof(int), st));
+    // The convergence test runs on the device (tridiag_lowest_kernel records the
+    // first dimension that meets it and ignores later calls).  The host reads it
+    // once per `chunk` iterations instead of after each one, so the GPU is not
+    // left idle between iterations; the few iterations enqueued past
+    // convergence write vectors and coefficients beyond `dim`, which nothing
+    // reads.  Cheap matvecs get longer chunks.
+    const int chunk = (int)std::min<int64_t>(8, std::max<int64_t>(2, 2000000 / (n + 100000)));
     int dim = 0;
     for (int i = 0; i < niter; ++i) {
         double* vi = V + (int64_t)i * n;
@@ -139,12 +146,15 @@ int krylov(dmrg_heff_s& h, double* psi, int niter, double precision, double zero
         DMRG_TRY(vec_dot(vi, hv, n, alpha + i, w.rs, blocks, st));
         DMRG_TRY(vec_axpy_norm(alpha + i, vi, hv, n, beta + i, w.rs, blocks, st));
         DMRG_TRY(launch_tridiag_lowest(alpha, beta, i + 1, E, state, precision, zero_tol, niter, st));
-        DMRG_CUDA_TRY(cudaMemcpyAsync(w.h_state, state, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
-        DMRG_CUDA_TRY(cudaStreamSynchronize(st));
-        if (w.h_state[0]) {
-            dim = w.h_state[1];
-            break;
+        if ((i + 1) % chunk == 0 || i + 1 == niter) {
+            DMRG_CUDA_TRY(cudaMemcpyAsync(w.h_state, state, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
+            DMRG_CUDA_TRY(cudaStreamSynchronize(st));
+            if (w.h_state[0]) {
+                dim = w.h_state[1];
+                break;
+            }
         }
+        if (i + 1 == niter) break;  // the last vector slot is V[niter - 1]
         double* vn = V + (int64_t)(i + 1) * n;
         DMRG_TRY(vec_lanczos_shift(beta + i, vi, hv, vn, n, blocks, st));
         for (int pass = 0; pass < 2; ++pass) {
@@ -154,14 +164,13 @@ int krylov(dmrg_heff_s& h, double* psi, int niter, double precision, double zero
         DMRG_TRY(vec_normalize(vn, n, tmp, w.rs, blocks, st));
     }
     if (dim <= 0) return set_error(DMRG_E_NUMERIC, "Lanczos ended without a converged dimension");
-    DMRG_TRY(launch_tridiag_ground_vector(alpha, beta, state + 1, dim, w.y.as<double>(), w.jac.as<double>(),
-                                          state + 2, st));
+    DMRG_TRY(launch_tridiag_ground_vector(alpha, beta, E, state + 1, w.y.as<double>(), state + 2, st));
     DMRG_TRY(vec_combine(V, n, dim, w.y.as<double>(), 1.0, psi, 0.0, n, blocks, st));
     double e = 0.0;
     DMRG_CUDA_TRY(cudaMemcpyAsync(&e, E + dim - 1, sizeof(double), cudaMemcpyDeviceToHost, st));
     DMRG_CUDA_TRY(cudaMemcpyAsync(w.h_state, state, 4 * sizeof(int), cudaMemcpyDeviceToHost, st));
     DMRG_CUDA_TRY(cudaStreamSynchronize(st));
-    if (w.h_state[2] != 0) return set_error(DMRG_E_NUMERIC, "tridiagonal Jacobi did not converge (m=%d)", dim);
+    if (w.h_state[2] != 0) return set_error(DMRG_E_NUMERIC, "tridiagonal ground vector failed (m=%d)", dim);
     if (split) DMRG_TRY(take_device_status(h.ctx));  // a tensor-core wait that gave up
     *energy = e;
     if (iters) *iters = dim;
