@@ -157,11 +157,11 @@ int krylov(dmrg_heff_s& h, double* psi, int niter, double precision, double zero
         if (i + 1 == niter) break;  // the last vector slot is V[niter - 1]
         double* vn = V + (int64_t)(i + 1) * n;
         DMRG_TRY(vec_lanczos_shift(beta + i, vi, hv, vn, n, blocks, st));
-        for (int pass = 0; pass < 2; ++pass) {
-            DMRG_TRY(vec_multidot(V, n, i + 1, vn, n, c, w.rs, blocks, st));
-            DMRG_TRY(vec_combine(V, n, i + 1, c, -1.0, vn, 1.0, n, blocks, st));
-        }
-        DMRG_TRY(vec_normalize(vn, n, tmp, w.rs, blocks, st));
+        // classical Gram-Schmidt twice; the second pass also normalises
+        DMRG_TRY(vec_multidot(V, n, i + 1, vn, n, c, w.rs, blocks, st));
+        DMRG_TRY(vec_combine(V, n, i + 1, c, -1.0, vn, 1.0, n, blocks, st));
+        DMRG_TRY(vec_multidot(V, n, i + 1, vn, n, c, w.rs, blocks, st));
+        DMRG_TRY(vec_combine_normalize(V, n, i + 1, c, -1.0, vn, n, tmp, w.rs, blocks, st));
     }
     if (dim <= 0) return set_error(DMRG_E_NUMERIC, "Lanczos ended without a converged dimension");
     DMRG_TRY(launch_tridiag_ground_vector(alpha, beta, E, state + 1, w.y.as<double>(), state + 2, st));

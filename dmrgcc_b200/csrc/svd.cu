@@ -1,6 +1,7 @@
 // Batched one-sided block-Jacobi SVD (see svd.cuh).
 #include <algorithm>
 #include <cfloat>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -14,9 +15,15 @@ namespace {
 constexpr int kBlk = 32;        // columns per block
 constexpr int kPair = 64;       // columns per pair
 constexpr int kChunk = 32;      // rows per streamed chunk
-constexpr int kThreads = 512;   // pair-solve CTA
+#ifndef DMRG_SVD_SOLVE_THREADS
+#define DMRG_SVD_SOLVE_THREADS 512
+#endif
+constexpr int kThreads = DMRG_SVD_SOLVE_THREADS;   // pair-solve CTA
 constexpr int kLd = kPair + 1;  // padded row of the shared 64x64 matrices
-constexpr int kInnerSweeps = 2;
+#ifndef DMRG_SVD_INNER_SWEEPS
+#define DMRG_SVD_INNER_SWEEPS 2
+#endif
+constexpr int kInnerSweeps = DMRG_SVD_INNER_SWEEPS;
 constexpr int kMaxSweeps = 40;
 // Columns whose norm is below kZeroRel * sqrt(rows) * ||A||_F are rounding
 // residue of a rank-deficient matrix: they take part in no rotation and in no
@@ -176,7 +183,8 @@ __global__ void __launch_bounds__(kThreads) solve_kernel(const SvdProblem* __res
 
     // A pair whose off-diagonal measure is at or below tol needs no rotation (the
     // same test decides convergence); a step that rotates nothing skips the
-    // update, and an inner sweep that rotates nothing ends the solve.
+    // update, and the solve ends once a sweep leaves every measure at or below tol.
+    const double tol2f = tol * tol * fro * fro;
     static_assert((kPair / 2) * (kPair / 2) % kThreads == 0 && (kPair / 2) * kPair % kThreads == 0, "even split");
     for (int sweep = 0; sweep < inner_sweeps; ++sweep) {
         int rotated = 0;
@@ -187,7 +195,7 @@ __global__ void __launch_bounds__(kThreads) solve_kernel(const SvdProblem* __res
                 const double apq = S.G[a * kLd + b];
                 double c = 1.0, s = 0.0;
                 const double daa = S.G[a * kLd + a], dbb = S.G[b * kLd + b];
-                if (daa > zero2 && dbb > zero2 && fabs(apq) > tol * fro * sqrt(fmax(daa, dbb))) {
+                if (daa > zero2 && dbb > zero2 && apq * apq > tol2f * fmax(daa, dbb)) {
                     // The rotation with tan = sign(x) y / (|x| + sqrt(x^2 + y^2)),
                     // x = dbb - daa, y = 2 apq (the smaller root of the Jacobi
                     // equation), as c = u / sqrt(u^2 + y^2), s = sign(x) y / sqrt(u^2 + y^2)
@@ -246,7 +254,16 @@ __global__ void __launch_bounds__(kThreads) solve_kernel(const SvdProblem* __res
             }
             __syncthreads();
         }
-        if (!rotated) break;  // uniform: every thread saw the same flags
+        if (!rotated || sweep + 1 == inner_sweeps) break;  // uniform: every thread saw the same flags
+        // the pair's measure after this sweep: a further sweep only if some entry is above tol
+        double off = 0.0;
+        for (int idx = threadIdx.x; idx < kPair * kPair; idx += kThreads) {
+            const int a = idx / kPair, b = idx % kPair;
+            if (a >= b) continue;
+            const double ga = S.G[a * kLd + a], gb = S.G[b * kLd + b], g = S.G[a * kLd + b];
+            if (ga > zero2 && gb > zero2 && g * g > tol2f * fmax(ga, gb)) off = 1.0;
+        }
+        if (block_max(off, S) == 0.0) break;
     }
     double* R = rot + (int64_t)blockIdx.x * kPair * kPair;
     for (int idx = threadIdx.x; idx < kPair * kPair; idx += kThreads) R[idx] = S.Q[(idx / kPair) * kLd + idx % kPair];
@@ -516,6 +533,7 @@ int BatchedSvd::run(cudaStream_t st, int* sweeps_out) {
     const dim3 colgrid(np, (max_cols + 7) / 8);
     int sweep = 0, worst_at = 0;
     double worst_left = 0.0;
+    auto t_sweep = std::chrono::steady_clock::now();
     for (; sweep < kMaxSweeps; ++sweep) {
         DMRG_CUDA_TRY(cudaMemsetAsync(d_conv.ptr, 0, np * sizeof(unsigned long long), st));
         // the sweep visits columns in descending norm order: blocks hold columns of
@@ -556,8 +574,17 @@ int BatchedSvd::run(cudaStream_t st, int* sweeps_out) {
                     wi = i;
                 }
             }
-            std::fprintf(stderr, "svd sweep %d: worst %.3e (sector %d x %d)%s", sweep, w, probs[wi].m, probs[wi].n,
-                         sweep % 4 == 3 ? "\n" : "; ");
+            int nconv = 0;
+            for (int i = 0; i < np; ++i) {
+                double x;
+                std::memcpy(&x, &conv[i], sizeof(double));
+                if (x <= 2.0 * DBL_EPSILON * std::sqrt((double)probs[i].rows)) ++nconv;
+            }
+            const auto now = std::chrono::steady_clock::now();
+            std::fprintf(stderr, "svd sweep %d: %.2f ms, worst %.3e (sector %d x %d), %d of %d sectors converged\n",
+                         sweep, std::chrono::duration<double, std::milli>(now - t_sweep).count(), w, probs[wi].m,
+                         probs[wi].n, nconv, np);
+            t_sweep = now;
         }
         for (int i = 0; i < np; ++i) {
             double worst;

@@ -72,10 +72,13 @@ __global__ void __launch_bounds__(kVecThreads) axpy_norm_kernel(const double* __
     last_block_finalize(partial, ticket, out, true);
 }
 
-// grid (nb, m): block (b, k) reduces its slice of <V_k, w> into partial[k * nb + b].
+// grid (nb, m): block (b, k) reduces its slice of <V_k, w> into partial[k * nb + b];
+// the last block of row k to finish sums the row in index order into c[k]
+// (tickets[k] counts the row's blocks and is reset).
 __global__ void __launch_bounds__(kVecThreads) multidot_kernel(const double* __restrict__ V, int64_t ldv,
                                                                const double* __restrict__ w, int64_t n,
-                                                               double* partial) {
+                                                               double* partial, unsigned* tickets,
+                                                               double* __restrict__ c) {
     const int k = blockIdx.y;
     const double* v = V + (int64_t)k * ldv;
     double acc = 0.0;
@@ -83,29 +86,43 @@ __global__ void __launch_bounds__(kVecThreads) multidot_kernel(const double* __r
         acc += v[i] * w[i];
     acc = block_sum(acc);
     if (threadIdx.x == 0) partial[(int64_t)k * gridDim.x + blockIdx.x] = acc;
+    __shared__ bool is_last;
+    __threadfence();
+    if (threadIdx.x == 0) is_last = (atomicAdd(tickets + k, 1u) == gridDim.x - 1);
+    __syncthreads();
+    if (!is_last) return;
+    __threadfence();
+    double r = 0.0;
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x)
+        r += ((volatile double*)partial)[(int64_t)k * gridDim.x + b];
+    r = block_sum(r);
+    if (threadIdx.x == 0) {
+        c[k] = r;
+        tickets[k] = 0u;
+    }
 }
 
-// one block per k: c[k] = sum_b partial[k * nb + b] in index order
-__global__ void __launch_bounds__(kVecThreads) rows_reduce_kernel(const double* __restrict__ partial, int nb,
-                                                                  double* __restrict__ c) {
-    const int k = blockIdx.x;
-    double v = 0.0;
-    for (int b = threadIdx.x; b < nb; b += blockDim.x) v += partial[(int64_t)k * nb + b];
-    v = block_sum(v);
-    if (threadIdx.x == 0) c[k] = v;
-}
-
+// w = beta_w * w + sign * sum_k c[k] V_k; with `partial` non-null also the norm
+// of the new w into *out (the reduction of dot_kernel(w, w): same slices, same
+// order).
 __global__ void __launch_bounds__(kVecThreads) combine_kernel(const double* __restrict__ V, int64_t ldv, int m,
                                                               const double* __restrict__ c, double sign,
-                                                              double* __restrict__ w, double beta_w, int64_t n) {
+                                                              double* __restrict__ w, double beta_w, int64_t n,
+                                                              double* partial, unsigned* ticket, double* out) {
     __shared__ double cs[kMaxVec];
     for (int k = threadIdx.x; k < m; k += blockDim.x) cs[k] = sign * c[k];
     __syncthreads();
+    double nrm = 0.0;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         double acc = beta_w == 0.0 ? 0.0 : beta_w * w[i];
         for (int k = 0; k < m; ++k) acc += cs[k] * V[(int64_t)k * ldv + i];
         w[i] = acc;
+        nrm += acc * acc;
     }
+    if (partial == nullptr) return;  // uniform
+    nrm = block_sum(nrm);
+    if (threadIdx.x == 0) partial[blockIdx.x] = nrm;
+    last_block_finalize(partial, ticket, out, true);
 }
 
 __global__ void __launch_bounds__(kVecThreads) lanczos_shift_kernel(const double* __restrict__ beta,
@@ -133,7 +150,7 @@ int ReduceScratch::alloc(int blocks, int max_vectors) {
     max_blocks = blocks;
     DMRG_TRY(partial.alloc((size_t)blocks * (max_vectors > 0 ? max_vectors : 1) * sizeof(double)));
     if (!ticket.ptr) {
-        DMRG_TRY(ticket.alloc(64 * sizeof(unsigned)));
+        DMRG_TRY(ticket.alloc((kRowTickets + kMaxVec) * sizeof(unsigned)));
         DMRG_TRY(ticket.zero());
     }
     return DMRG_OK;
@@ -164,8 +181,8 @@ int vec_multidot(const double* V, int64_t ldv, int m, const double* w, int64_t n
     if (nb > rs.max_blocks) nb = rs.max_blocks;
     if ((size_t)nb * m * sizeof(double) > rs.partial.bytes)
         return set_error(DMRG_E_ARG, "multidot scratch too small (%d x %d)", nb, m);
-    multidot_kernel<<<dim3(nb, m), kVecThreads, 0, st>>>(V, ldv, w, n, rs.partial.as<double>());
-    rows_reduce_kernel<<<m, kVecThreads, 0, st>>>(rs.partial.as<double>(), nb, c);
+    multidot_kernel<<<dim3(nb, m), kVecThreads, 0, st>>>(V, ldv, w, n, rs.partial.as<double>(),
+                                                         rs.ticket.as<unsigned>() + kRowTickets, c);
     DMRG_CUDA_TRY(cudaGetLastError());
     return DMRG_OK;
 }
@@ -173,7 +190,7 @@ int vec_multidot(const double* V, int64_t ldv, int m, const double* w, int64_t n
 int vec_combine(const double* V, int64_t ldv, int m, const double* c, double sign, double* w, double beta_w,
                 int64_t n, int blocks, cudaStream_t st) {
     if (m > kMaxVec) return set_error(DMRG_E_ARG, "combine of %d > %d vectors", m, kMaxVec);
-    combine_kernel<<<blocks, kVecThreads, 0, st>>>(V, ldv, m, c, sign, w, beta_w, n);
+    combine_kernel<<<blocks, kVecThreads, 0, st>>>(V, ldv, m, c, sign, w, beta_w, n, nullptr, nullptr, nullptr);
     DMRG_CUDA_TRY(cudaGetLastError());
     return DMRG_OK;
 }
@@ -181,6 +198,17 @@ int vec_combine(const double* V, int64_t ldv, int m, const double* c, double sig
 int vec_lanczos_shift(const double* beta, const double* v_cur, double* h, double* v_next, int64_t n, int blocks,
                       cudaStream_t st) {
     lanczos_shift_kernel<<<blocks, kVecThreads, 0, st>>>(beta, v_cur, h, v_next, n);
+    DMRG_CUDA_TRY(cudaGetLastError());
+    return DMRG_OK;
+}
+
+int vec_combine_normalize(const double* V, int64_t ldv, int m, const double* c, double sign, double* w, int64_t n,
+                          double* out, ReduceScratch& rs, int blocks, cudaStream_t st) {
+    if (m > kMaxVec) return set_error(DMRG_E_ARG, "combine of %d > %d vectors", m, kMaxVec);
+    blocks = blocks < rs.max_blocks ? blocks : rs.max_blocks;
+    combine_kernel<<<blocks, kVecThreads, 0, st>>>(V, ldv, m, c, sign, w, 1.0, n, rs.partial.as<double>(),
+                                                   rs.ticket.as<unsigned>() + 2, out);
+    scale_inv_kernel<<<blocks, kVecThreads, 0, st>>>(w, out, n);
     DMRG_CUDA_TRY(cudaGetLastError());
     return DMRG_OK;
 }

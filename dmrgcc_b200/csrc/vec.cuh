@@ -32,9 +32,14 @@ int vec_combine(const double* V, int64_t ldv, int m, const double* c, double sig
 // Lanczos step: v_next = h / beta ; h = -beta * v_cur   (beta on the device)
 int vec_lanczos_shift(const double* beta, const double* v_cur, double* h, double* v_next, int64_t n, int blocks,
                       cudaStream_t st);
+// w = w + sign * sum_k c[k] V_k, then w /= ||w|| (norm written to out[0]): the
+// same arithmetic as vec_combine followed by vec_normalize, in two kernels
+int vec_combine_normalize(const double* V, int64_t ldv, int m, const double* c, double sign, double* w, int64_t n,
+                          double* out, ReduceScratch& rs, int blocks, cudaStream_t st);
 // x /= ||x|| (two kernels: norm then scale); norm written to out[0]
 int vec_normalize(double* x, int64_t n, double* out, ReduceScratch& rs, int blocks, cudaStream_t st);
 
 constexpr int kMaxVec = 512;
+constexpr int kRowTickets = 64;  // ticket slots before the per-row ones of vec_multidot
 
 }  // namespace dmrg
