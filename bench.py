@@ -168,28 +168,45 @@ def split_form(ctx, step, psi, L, R, out_ref, steps: int, flush, stream, prec: i
                       % ("f16 on bf16" if name == "bf16x3" else "tf32")}
 
 
-def sweep_time(ctx) -> dict:
+def sweep_time(ctx, precision: int = 0, name: str = "fp64") -> dict:
     """One whole run of the 8x4 cylinder input (D ramp 128 -> 1024, 8 sweeps =
     16 half-sweeps, niter 100, noise on for the first 12 half-sweeps), wall
-    clock on the host around dmrg_run_execute (device work + host bookkeeping)."""
+    clock on the host around dmrg_run_execute (device work + host bookkeeping),
+    with the H_eff*psi products in `precision` (FP64 Lanczos, eigensolve and SVD
+    in every case)."""
     from dmrgcc_b200 import capi
 
-    run = capi.Run(ctx, CYL_INPUT, verbose=0)
+    run = capi.Run(ctx, CYL_INPUT, verbose=0, precision=precision)
     t0 = time.perf_counter()
     run.execute()
     total = time.perf_counter() - t0
     e, s = run.half_sweeps()
     ph, sw = run.phases()
-    return {
+    out = {
         "workload": "whole DMRG run, 8x4 Bose-Hubbard cylinder (d=5, N=16, U=8), D 128->1024, 8 sweeps",
-        "precision": "fp64", "total_s": total,
+        "precision": name, "total_s": total,
         "per_sweep_s": [float(s[2 * i] + s[2 * i + 1]) for i in range(len(s) // 2)],
         "phase_s": {k: float(v) for k, v in zip(capi.Run.PHASES, ph.sum(axis=0))},
         "svd_sweeps": int(sw.sum()), "final_energy": float(e[-1]),
-        "reference_cpu": {"total_s": 557.0, "final_energy": -45.653161401383, "cores": 8,
-                          "note": "the reference built from its sources with OpenBLAS, measured in the build "
-                                  "container (not on the GPU box); 8 threads"},
     }
+    run.close()
+    return out
+
+
+def sweep_pair(ctx) -> dict:
+    """The whole run in FP64 and with TF32X3 matvecs, back to back: times, the
+    split run's speedup per sweep and its final-energy difference per site
+    (32 sites) against the FP64 run."""
+    fp64 = sweep_time(ctx)
+    split = sweep_time(ctx, 2, "tf32x3")
+    fp64["reference_cpu"] = {"total_s": 557.0, "final_energy": -45.653161401383, "cores": 8,
+                             "note": "the reference built from its sources with OpenBLAS, measured in the build "
+                                     "container (not on the GPU box); 8 threads"}
+    fp64["split"] = {"precision": "tf32x3", "total_s": split["total_s"], "per_sweep_s": split["per_sweep_s"],
+                     "phase_s": split["phase_s"], "final_energy": split["final_energy"],
+                     "speedup_vs_fp64": fp64["total_s"] / split["total_s"],
+                     "abs_dE_per_site_vs_fp64": abs(split["final_energy"] - fp64["final_energy"]) / 32.0}
+    return fp64
 
 
 def run_b200(args) -> None:
@@ -324,7 +341,7 @@ def run_b200(args) -> None:
             for sp in line["split"]:
                 sp["speedup_vs_fp64"] = ms_per_step / sp["ms_per_step"]
         if world == 1 and not args.no_sweep:
-            line["sweep"] = sweep_time(ctx)
+            line["sweep"] = sweep_pair(ctx)
         cpu = cpu_reference(args.cpu_reps, 1, os.cpu_count() or 1) if not args.no_cpu else {"unavailable": "skipped"}
         if "unavailable" not in cpu:
             line["cpu_baseline"] = {"value": cpu["gflop"] / cpu["mean_s"] * 1e-3, "unit": "TFLOP/s",
