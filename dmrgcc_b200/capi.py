@@ -59,6 +59,8 @@ _SIGS = {
     "dmrg_heff_create": (C.c_int, [_VP, C.c_int, C.c_int, _I, C.POINTER(Blocks), C.c_int, C.c_int, C.c_int, _D,
                                    C.POINTER(Blocks), C.POINTER(Blocks), C.c_int, C.POINTER(_VP)]),
     "dmrg_heff_destroy": (C.c_int, [_VP]),
+    "dmrg_heff_set_split_threshold": (C.c_int, [_VP, C.c_int64]),
+    "dmrg_heff_split_iters": (C.c_int, [_VP, _I]),
     "dmrg_heff_sizes": (C.c_int, [_VP, _I64, _I64, _I64]),
     "dmrg_heff_flops": (C.c_int, [_VP, _D, _D]),
     "dmrg_heff_set_env": (C.c_int, [_VP, _VP, _VP]),
@@ -286,6 +288,14 @@ class Heff:
     def apply_host(self, psi: np.ndarray, out: np.ndarray, accumulate: bool = False) -> None:
         check(lib().dmrg_heff_apply_host(self.h, psi.ctypes.data, out.ctypes.data, int(accumulate)),
               "dmrg_heff_apply_host")
+
+    def set_split_threshold(self, min_psi_dim: int) -> None:
+        check(lib().dmrg_heff_set_split_threshold(self.h, int(min_psi_dim)), "dmrg_heff_set_split_threshold")
+
+    def split_iters(self) -> int:
+        it = C.c_int(0)
+        check(lib().dmrg_heff_split_iters(self.h, C.byref(it)), "dmrg_heff_split_iters")
+        return it.value
 
     def lanczos(self, psi: DeviceArray, niter: int, precision: float = 1e-15,
                 zero_tol: float = 1e-15) -> tuple[float, int]:

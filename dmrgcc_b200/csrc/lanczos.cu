@@ -179,6 +179,18 @@ int krylov(dmrg_heff_s& h, double* psi, int niter, double precision, double zero
 
 }  // namespace
 
+extern "C" int dmrg_heff_set_split_threshold(dmrg_heff_t h, int64_t min_psi_dim) {
+    if (!h || min_psi_dim < 0) return set_error(DMRG_E_ARG, "invalid split threshold");
+    h->split_min_dim = min_psi_dim;
+    return DMRG_OK;
+}
+
+extern "C" int dmrg_heff_split_iters(dmrg_heff_t h, int* iters) {
+    if (!h || !iters) return set_error(DMRG_E_ARG, "null argument");
+    *iters = h->lw ? h->lw->split_iters : 0;
+    return DMRG_OK;
+}
+
 extern "C" int dmrg_lanczos(dmrg_heff_t hp, double* psi, int niter, double precision, double zero_tol,
                             double* energy, int* iters) {
     if (!hp || !psi || !energy || niter <= 0) return set_error(DMRG_E_ARG, "invalid Lanczos arguments");
@@ -190,7 +202,13 @@ extern "C" int dmrg_lanczos(dmrg_heff_t hp, double* psi, int niter, double preci
         if (iters) *iters = 0;
         return run_exact(h, psi, energy);
     }
-    if (!is_split(h.precision)) return krylov(h, psi, niter, precision, zero_tol, false, energy, iters);
+    // A split Krylov phase pays off only where the split matvec is clearly faster
+    // than the FP64 one (large blocks); below h.split_min_dim the FP64 run alone
+    // is cheaper than the two phases.
+    if (!is_split(h.precision) || n < h.split_min_dim) {
+        h.lw->split_iters = 0;
+        return krylov(h, psi, niter, precision, zero_tol, false, energy, iters);
+    }
     // Mixed precision: a Krylov run on split-precision matvecs until the Ritz
     // value settles at the split arithmetic's resolution, then the FP64 run of
     // the reference from that Ritz vector, which fixes the energy and the state.

@@ -158,6 +158,15 @@ int dmrg_heff_apply_noalloc(int num_left_sector, int num_right_sector, const int
  * dense branch).  niter <= 512.  Synchronous. */
 int dmrg_lanczos(dmrg_heff_t h, double* psi_dev, int niter, double precision, double zero_tol,
                  double* energy, int* iters);
+/* For a split-precision operator (DMRG_PREC_TF32X3 / BF16X3), dmrg_lanczos runs
+ * a Krylov phase on split-precision matvecs and then the FP64 Lanczos from its
+ * Ritz vector, when psi_dim >= min_psi_dim (default 200000: below it the split
+ * matvec is not enough faster to pay for two phases and the FP64 run is used
+ * alone).  No reference counterpart (the reference has FP64 only). */
+int dmrg_heff_set_split_threshold(dmrg_heff_t h, int64_t min_psi_dim);
+/* Krylov dimension of the split phase of the last dmrg_lanczos call (0 when it
+ * ran FP64 only). */
+int dmrg_heff_split_iters(dmrg_heff_t h, int* iters);
 
 /* ---- a2/a3: environment update ---------------------------------------------
  * side 0 replaces RealTensorContraction::LeftComputeTensorContraction

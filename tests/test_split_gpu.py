@@ -85,8 +85,30 @@ def test_mixed_precision_lanczos_matches_reference(ctx, call, split):
     R = capi.DeviceArray.from_host(ctx, step.R_data)
     h = capi.Heff(ctx, step.site, step.L, step.R, precision=split)
     h.set_env(L, R)
+    h.set_split_threshold(0)  # the mixed path at any size (the default keeps it for large psi_dim)
     psi = capi.DeviceArray.from_host(ctx, step.ket_data)
     e, dim = h.lanczos(psi, niter)
+    assert h.split_iters() > 0
     assert abs(e - float(ref["energy"][0])) / 16 <= 1e-12
     v = psi.download()
     assert 1.0 - abs(float(v @ np.asarray(ref["lattice.ket.data"]))) <= 1e-9
+
+
+@pytest.mark.parametrize("split", SPLITS)
+def test_split_operator_small_problem_runs_fp64_lanczos(ctx, split):
+    """Below the split threshold (default psi_dim 200000) a split-precision
+    operator's Lanczos is the FP64 one: same dimension, energy and vector."""
+    from dmrgcc_b200.problem import read_nac
+    step = SiteStep.from_nac(os.path.join(GOLD, "heff_c158.nac"))
+    niter = int(read_nac(os.path.join(GOLD, "heff_c158.nac"))["niter"][0])
+    L = capi.DeviceArray.from_host(ctx, step.L_data)
+    R = capi.DeviceArray.from_host(ctx, step.R_data)
+    res = []
+    for prec in (capi.DMRG_PREC_FP64, split):
+        h = capi.Heff(ctx, step.site, step.L, step.R, precision=prec)
+        h.set_env(L, R)
+        psi = capi.DeviceArray.from_host(ctx, step.ket_data)
+        res.append(h.lanczos(psi, niter) + (psi.download(),))
+        assert h.split_iters() == 0
+    (e0, d0, v0), (e1, d1, v1) = res
+    assert d0 == d1 and e0 == e1 and np.array_equal(v0, v1)
