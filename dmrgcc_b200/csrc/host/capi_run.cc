@@ -73,9 +73,9 @@ int dmrg_run_create(dmrg_ctx_t ctx, const char* input_path, const char* model, c
         InputGroup input(input_path, "input", o.verbose != 0);
         ModelSpec m = make_model(input, model ? model : "real_spinless_bose_square");
         AllocScope pool(ctx->stream);  // the run's tensors come from the stream-ordered pool
-        auto* r = new dmrg_run_s();
+        std::unique_ptr<dmrg_run_s> r(new dmrg_run_s());
         r->engine.reset(new Engine(ctx, std::move(m.space), std::move(m.ham), input, o));
-        *out = r;
+        *out = r.release();
         return DMRG_OK;
     } catch (const std::exception& e) {
         return set_error(DMRG_E_ARG, "%s", e.what());

@@ -64,11 +64,15 @@ Engine::Engine(dmrg_ctx_t ctx, std::unique_ptr<QuantumSpace> space, std::unique_
                InputGroup& input, const RunOptions& opt)
     : ctx_(ctx), st_(ctx->stream), opt_(opt), space_(std::move(space)), ham_(std::move(ham)) {
     n_ = space_->num_site();
-    // The disk cache keys are read for compatibility; every tensor stays resident.
+    // disk_cache (tensors swapped to files between uses) is read for compatibility
+    // and ignored: every tensor stays resident.  cache_record / cache_resume
+    // write and read the reference's checkpoint file (real_tensor_rundmrg.cc:16-23).
     input.getBool("disk_cache", false);
-    input.getString("cache_name", ".");
-    input.getBool("cache_record", false);
-    input.getBool("cache_resume", false);
+    cache_name_ = input.getString("cache_name", ".");
+    cache_record_ = input.getBool("cache_record", false);
+    record_name_ = input.getString("record_name", "record.dat");
+    cache_resume_ = input.getBool("cache_resume", false);
+    if (cache_resume_) resume_name_ = input.getString("resume_name", "");
     first_block_ = input.getInt("first_block");
     first_dim_ = input.getInt("first_dim");
     const int num_sweep = input.getInt("num_sweep");
@@ -114,8 +118,12 @@ Engine::Engine(dmrg_ctx_t ctx, std::unique_ptr<QuantumSpace> space, std::unique_
     }
     rng_.seed_with(opt_.seed);
     rand_draws_ = 0;
-    int rc = DefineTensorSpace(first_block_, first_dim_);
-    if (rc != DMRG_OK) throw std::runtime_error(std::string("DefineTensorSpace: ") + dmrg_last_error());
+    // a resumed run starts from the recorded MPS instead of the random one (and so
+    // draws no random numbers before its first expansion), like the reference (:44-51)
+    int rc = cache_resume_ ? ReadTensorSpace(resume_name_) : DefineTensorSpace(first_block_, first_dim_);
+    if (rc != DMRG_OK)
+        throw std::runtime_error(std::string(cache_resume_ ? "ReadTensorSpace: " : "DefineTensorSpace: ") +
+                                 dmrg_last_error());
     ham_->DefineTensorHamiltonian();
     con_.resize(n_ + 1);
     for (int i = 0; i <= n_; ++i) {
@@ -1162,8 +1170,193 @@ int Engine::Run() {
         half_phases_.push_back(ph);
         half_svd_sweeps_.push_back(svd_sweeps_);
         if (opt_.verbose) std::printf("%s energy = %.12f\n", l2r ? "right" : "left", energy_);
+        // after every full sweep, like the reference (:229-233)
+        if (!l2r && cache_record_) DMRG_TRY(WriteTensorSpace(cache_name_ + "/" + record_name_));
     }
     if (opt_.verbose) std::printf("Total Time : %.12f s\n", wall_time() - t0);
+    return DMRG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// checkpoint file: RealTensorSpace::WriteTensorSpace / ReadTensorSpace
+// (real_tensor_space.cc:182-277), RealTensorLattice::Write/ReadTensorLattice
+// (real_tensor_lattice.cc:218-300), RealMatrixBlock::Write/ReadMatrixBlock
+// (real_matrix_block.cc:227-285), RealMatrix::Write/ReadMatrix
+// (real_matrix.cc:139-180).  Native-endian binary, in this order:
+//   int num_site, num_site + 1, num_site - 1, num_quantum;
+//   int num_table[b] for the num_site + 1 bonds; int quantum_table[b][j][k];
+//   per site: int physics_dim; int nl; (int left_block, int left_dim) x nl;
+//     int nr; (int right_block, int right_dim) x nr; int physics_index[nl][nr];
+//     int num_block; per block: int left, right, rows, cols, rows*cols;
+//     double values[rows * cols] (row-major);
+//   int max_block, max_dim; double canonical_precision, noise_factor.
+// ---------------------------------------------------------------------------
+namespace {
+struct BinOut {
+    std::FILE* f;
+    bool ok = true;
+    template <class T>
+    void put(const T& v) { ok = ok && std::fwrite(&v, sizeof(T), 1, f) == 1; }
+    void put_n(const double* v, size_t n) { ok = ok && (n == 0 || std::fwrite(v, sizeof(double), n, f) == n); }
+};
+struct BinIn {
+    std::FILE* f;
+    bool ok = true;
+    template <class T>
+    T get() {
+        T v{};
+        ok = ok && std::fread(&v, sizeof(T), 1, f) == 1;
+        return v;
+    }
+    void get_n(double* v, size_t n) { ok = ok && (n == 0 || std::fread(v, sizeof(double), n, f) == n); }
+};
+}  // namespace
+
+int Engine::WriteTensorSpace(const std::string& path) {
+    std::FILE* f = std::fopen(path.c_str(), "wb");
+    if (!f) return set_error(DMRG_E_IO, "cannot open %s for writing", path.c_str());
+    BinOut o{f};
+    const int nq = space_->num_quantum();
+    o.put(n_);
+    o.put(n_ + 1);
+    o.put(n_ - 1);
+    o.put(nq);
+    for (int b = 0; b <= n_; ++b) o.put((int)space_->table(b).size());
+    for (int b = 0; b <= n_; ++b)
+        for (const auto& row : space_->table(b))
+            for (int k = 0; k < nq; ++k) o.put(row[k]);
+    std::vector<double> host;
+    int rc = DMRG_OK;
+    for (int i = 0; i < n_ && o.ok && rc == DMRG_OK; ++i) {
+        const TensorLattice& t = *lat_[i];
+        o.put(t.physics_dim);
+        o.put(t.nl());
+        for (int l = 0; l < t.nl(); ++l) {
+            o.put(t.left_block[l]);
+            o.put(t.left_dim[l]);
+        }
+        o.put(t.nr());
+        for (int r = 0; r < t.nr(); ++r) {
+            o.put(t.right_block[r]);
+            o.put(t.right_dim[r]);
+        }
+        for (int l = 0; l < t.nl(); ++l)
+            for (int r = 0; r < t.nr(); ++r) o.put(t.p(l, r));
+        const BlockListDesc& d = t.ket.d;
+        host.assign((size_t)std::max<int64_t>(d.size, 0), 0.0);
+        if (d.size > 0) {
+            cudaError_t e = cudaMemcpyAsync(host.data(), t.ket.ptr(), (size_t)d.size * sizeof(double),
+                                            cudaMemcpyDeviceToHost, st_);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(st_);
+            if (e != cudaSuccess) rc = set_error(DMRG_E_CUDA, "site tensor download: %s", cudaGetErrorString(e));
+        }
+        o.put(d.count());
+        for (int k = 0; k < d.count() && rc == DMRG_OK; ++k) {
+            o.put(d.left[k]);
+            o.put(d.right[k]);
+            o.put(d.rows[k]);
+            o.put(d.cols[k]);
+            o.put(d.rows[k] * d.cols[k]);
+            o.put_n(host.data() + d.off[k], (size_t)d.rows[k] * d.cols[k]);
+        }
+    }
+    o.put(p_max_block_);
+    o.put(p_max_dim_);
+    o.put(p_canpre_);
+    o.put(p_noise_);
+    const bool closed = std::fclose(f) == 0;
+    DMRG_TRY(rc);
+    if (!o.ok || !closed) return set_error(DMRG_E_IO, "write to %s failed", path.c_str());
+    return DMRG_OK;
+}
+
+int Engine::ReadTensorSpace(const std::string& path) {
+    std::FILE* f = std::fopen(path.c_str(), "rb");
+    if (!f) return set_error(DMRG_E_IO, "cannot open %s", path.c_str());
+    BinIn in{f};
+    auto fail = [&](const char* what) {
+        std::fclose(f);
+        return set_error(DMRG_E_IO, "%s: %s", path.c_str(), what);
+    };
+    const int nq = space_->num_quantum();
+    const int ns = in.get<int>(), nspp = in.get<int>(), nsmm = in.get<int>(), fq = in.get<int>();
+    if (!in.ok || ns != n_ || nspp != n_ + 1 || nsmm != n_ - 1 || fq != nq)
+        return fail("number of sites or quantum numbers differs from the model");
+    std::vector<int> ntab(n_ + 1);
+    for (int b = 0; b <= n_; ++b) ntab[b] = in.get<int>();
+    for (int b = 0; b <= n_ && in.ok; ++b) {
+        if (ntab[b] != (int)space_->table(b).size()) return fail("quantum table differs from the model");
+        for (int j = 0; j < ntab[b]; ++j)
+            for (int k = 0; k < nq; ++k)
+                if (in.get<int>() != space_->table(b)[j][k]) return fail("quantum table differs from the model");
+    }
+    std::vector<double> host;
+    for (int i = 0; i < n_; ++i) {
+        TensorLattice& t = *lat_[i];
+        const int pd = in.get<int>();
+        const int nl = in.get<int>();
+        if (!in.ok || pd != space_->physics_dim() || nl < 0 || nl > 1 << 20) return fail("malformed site header");
+        std::vector<int> lb(nl), ld(nl);
+        for (int l = 0; l < nl; ++l) {
+            lb[l] = in.get<int>();
+            ld[l] = in.get<int>();
+        }
+        const int nr = in.get<int>();
+        if (!in.ok || nr < 0 || nr > 1 << 20) return fail("malformed site header");
+        std::vector<int> rb(nr), rd(nr);
+        for (int r = 0; r < nr; ++r) {
+            rb[r] = in.get<int>();
+            rd[r] = in.get<int>();
+        }
+        for (int l = 0; l < nl; ++l)
+            if (lb[l] < 0 || lb[l] >= ntab[i] || ld[l] < 0) return fail("left sector out of range");
+        for (int r = 0; r < nr; ++r)
+            if (rb[r] < 0 || rb[r] >= ntab[i + 1] || rd[r] < 0) return fail("right sector out of range");
+        DefineLatticeSectors(t, lb, rb, ld, rd);
+        t.physics_dim = pd;
+        for (int l = 0; l < nl; ++l)
+            for (int r = 0; r < nr; ++r) {
+                const int p = in.get<int>();
+                if (p < -1 || p >= pd) return fail("physics index out of range");
+                t.phys[(size_t)l * nr + r] = p;
+            }
+        const int nb = in.get<int>();
+        if (!in.ok || nb < 0 || nb > nl * nr) return fail("malformed block list");
+        DevBlocks ket;
+        host.clear();
+        for (int k = 0; k < nb; ++k) {
+            const int l = in.get<int>(), r = in.get<int>(), rows = in.get<int>(), cols = in.get<int>();
+            const int total = in.get<int>();
+            if (!in.ok || l < 0 || l >= nl || r < 0 || r >= nr || rows < 0 || cols < 0 ||
+                (int64_t)rows * cols != total || t.p(l, r) < 0)
+                return fail("malformed block");
+            ket.d.push(l, r, rows, cols);
+            const size_t at = host.size();
+            host.resize(at + (size_t)total);
+            in.get_n(host.data() + at, (size_t)total);
+        }
+        if (!in.ok) return fail("truncated block values");
+        t.has_canonical = false;
+        t.match_dim.clear();
+        int rc = ket.alloc(st_, false);
+        if (rc == DMRG_OK && !host.empty()) {
+            cudaError_t e = cudaMemcpyAsync(ket.ptr(), host.data(), host.size() * sizeof(double),
+                                            cudaMemcpyHostToDevice, st_);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(st_);
+            if (e != cudaSuccess) rc = set_error(DMRG_E_CUDA, "site tensor upload: %s", cudaGetErrorString(e));
+        }
+        if (rc != DMRG_OK) {
+            std::fclose(f);
+            return rc;
+        }
+        t.ket = std::move(ket);
+    }
+    p_max_block_ = in.get<int>();
+    p_max_dim_ = in.get<int>();
+    p_canpre_ = in.get<double>();
+    p_noise_ = in.get<double>();
+    if (!in.ok) return fail("truncated parameters");
+    std::fclose(f);
     return DMRG_OK;
 }
 

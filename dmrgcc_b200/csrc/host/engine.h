@@ -111,6 +111,10 @@ public:
     int ExpanTensorNetwork(int leigh, int site);
     int ComputeTensorNetwork(int leigh, int site);
     int LanczosMethod(int niter, int site, double& energy, int& dim);
+    // RealTensorSpace::WriteTensorSpace / ReadTensorSpace (real_tensor_space.cc:
+    // 182-277): the MPS in the reference's binary checkpoint format.
+    int WriteTensorSpace(const std::string& path);
+    int ReadTensorSpace(const std::string& path);
 
 private:
     // bookkeeping (host)
@@ -143,6 +147,9 @@ private:
     std::vector<int> max_dim_, max_block_, num_iter_;
     std::vector<double> canpre_, noise_;
     int first_block_ = 0, first_dim_ = 0;
+    // checkpoints (cache_record / cache_resume, real_tensor_rundmrg.cc:16-23,44-51,229-233)
+    bool cache_record_ = false, cache_resume_ = false;
+    std::string cache_name_ = ".", record_name_ = "record.dat", resume_name_;
     // current parameters (RealTensorSpace::DefineTensorSpaceParameter)
     int p_max_block_ = 0, p_max_dim_ = -1;
     double p_canpre_ = 1e-30, p_noise_ = 10.0;

@@ -36,6 +36,7 @@ extern "C" {
 #define DMRG_E_NOMEM (-3)    /* device allocation failed */
 #define DMRG_E_NUMERIC (-4)  /* an iterative device routine hit its iteration cap */
 #define DMRG_E_STATE (-5)    /* call made in the wrong state */
+#define DMRG_E_IO (-6)       /* a file could not be opened, read or written, or is malformed */
 
 /* Arithmetic of the block GEMMs.  FP64: plain double (FP64 tensor path).
  * TF32X3 / BF16X3: 5th-generation tensor cores (tcgen05): every FP64 operand is

@@ -16,6 +16,8 @@
 //   PROBE_ENV=i,j,...      environment-update call indices to dump
 //   PROBE_CANON=i,j,...    canonicalisation call indices to dump
 //   PROBE_STOP=n           exit(0) right after Lanczos call n
+// cache_resume in the input reads the checkpoint through a corrected copy of
+// the reference's reader (see __wrap__ZN15RealTensorSpace15ReadTensorSpaceEPKc).
 //   PROBE_GAUGE=1          fix the free signs of LAPACK's singular vectors and
 //                          eigenvectors by the library's convention (see below)
 // Always writes PROBE_OUT/steps.txt: one line per Lanczos call with the site,
@@ -178,6 +180,47 @@ void __wrap__ZN15RealTensorSpace16ExpanTensorSpaceEii(RealTensorSpace* self, int
 void __wrap__ZN15RealTensorSpace16MatchTensorSpaceEii(RealTensorSpace* self, int leigh, int site) {
     __real__ZN15RealTensorSpace16MatchTensorSpaceEii(self, leigh, site);
     trace("T", leigh, self->tensor_lattice_[site]);
+}
+// RealTensorSpace::ReadTensorSpace(const char*) (real_tensor_space.cc:212-277,
+// used by cache_resume) with its table allocation corrected: the reference
+// sizes num_table_ and quantum_table_ by num_quantum_ where num_site_pp_ entries
+// are read into them (:245,249), which overruns the heap and makes its resumed
+// runs meaningless.  Same file format, same fields; the site tensors are read by
+// the reference's own RealTensorLattice::ReadTensorLattice.
+void __wrap__ZN15RealTensorSpace15ReadTensorSpaceEPKc(RealTensorSpace* self, const char* name) {
+    std::ifstream f(name, std::ios::binary | std::ios::in);
+    if (!f) {
+        std::fprintf(stderr, "probe: cannot open %s\n", name);
+        std::exit(2);
+    }
+    auto get = [&](auto& v) { f.read(reinterpret_cast<char*>(&v), sizeof(v)); };
+    get(self->num_site_);
+    get(self->num_site_pp_);
+    get(self->num_site_mm_);
+    get(self->num_quantum_);
+    self->num_table_ = new int[self->num_site_pp_];
+    for (int i = 0; i < self->num_site_pp_; ++i) get(self->num_table_[i]);
+    self->quantum_table_ = new int**[self->num_site_pp_];
+    for (int i = 0; i < self->num_site_pp_; ++i) {
+        self->quantum_table_[i] = new int*[self->num_table_[i]];
+        for (int j = 0; j < self->num_table_[i]; ++j) {
+            self->quantum_table_[i][j] = new int[self->num_quantum_];
+            for (int k = 0; k < self->num_quantum_; ++k) get(self->quantum_table_[i][j][k]);
+        }
+    }
+    self->tensor_lattice_ = new RealTensorLattice*[self->num_site_];
+    for (int i = 0; i < self->num_site_; ++i) {
+        self->tensor_lattice_[i] = new RealTensorLattice();
+        self->tensor_lattice_[i]->ReadTensorLattice(f);
+    }
+    get(self->max_block_);
+    get(self->max_dim_);
+    get(self->canonical_precision_);
+    get(self->noise_factor_);
+    if (!f) {
+        std::fprintf(stderr, "probe: %s is truncated\n", name);
+        std::exit(2);
+    }
 }
 void __wrap__ZN17RealTensorLattice22LeftMergeTensorLatticeEPS_(RealTensorLattice* self, RealTensorLattice* o) {
     __real__ZN17RealTensorLattice22LeftMergeTensorLatticeEPS_(self, o);

@@ -20,8 +20,14 @@ chain16_spinless.in), and keeps:
   model_chain16.nac     the MPO per site and the quantum tables (first call)
   quicksort_cases.txt   inputs with ties and the index order the reference's
                         QuickSort (src/util/general.ih) returns (probe_sort)
+  record_chain6.dat     the reference's checkpoint file (cache_record) of the
+                        6-site chain after its first two sweeps, gauge-pinned
+  trace_gauge_chain6_resume.txt, steps_chain6_resume.txt   the gauge-pinned
+                        reference run resumed from that file (cache_resume,
+                        full sweep table)
 
-Usage: python tests/golden/make_golden.py [--cylinder]
+Usage: python tests/golden/make_golden.py [--cylinder] [--resume-only]
+  --resume-only regenerates only the checkpoint fixtures.
   --cylinder additionally dumps the block structure (no values) of the 8x4
   cylinder at bond dimension 1024, site 16 (minutes of CPU), into
   heff_struct_cyl8x4_D1024.nac.
@@ -66,6 +72,44 @@ def gauge_trace(name: str) -> None:
             g.write(" ".join(parts) + "\n")
 
 
+def input_with(src: str, **values) -> str:
+    """The input file text `src` with the given `key = value` lines replaced."""
+    import re
+
+    for k, v in values.items():
+        src, n = re.subn(rf"(?m)^(\s*){k}\s*=.*$", rf"\g<1>{k} = {v}", src)
+        assert n == 1, k
+    return src
+
+
+def resume_case() -> None:
+    """Checkpoint fixtures: the gauge-pinned reference records the 6-site chain
+    after two sweeps (cache_record, RealTensorSpace::WriteTensorSpace), then a
+    second reference run resumes from that file with the full sweep table
+    (cache_resume, ReadTensorSpace)."""
+    src = open(os.path.join(ROOT, "dmrgcc_b200", "inputs", "chain6_spinless.in")).read()
+    t = tempfile.mkdtemp(prefix="golden_record_")
+    rec_in = os.path.join(t, "record.in")
+    with open(rec_in, "w") as f:
+        f.write(input_with(src, num_sweep=2, cache_record="true", cache_name=t, record_name="record.dat"))
+    run_probe(rec_in, t, {"PROBE_GAUGE": "1"})
+    record = os.path.join(HERE, "record_chain6.dat")
+    shutil.copy(os.path.join(t, "record.dat"), record)
+    t2 = tempfile.mkdtemp(prefix="golden_resume_")
+    res_in = os.path.join(t2, "resume.in")
+    with open(res_in, "w") as f:
+        f.write(input_with(src, cache_resume="true", resume_name=record))
+    run_probe(res_in, t2, {"PROBE_GAUGE": "1", "PROBE_TRACE": "1"})
+    shutil.copy(os.path.join(t2, "steps.txt"), os.path.join(HERE, "steps_chain6_resume.txt"))
+    with open(os.path.join(t2, "trace.txt")) as f, \
+            open(os.path.join(HERE, "trace_gauge_chain6_resume.txt"), "w") as g:
+        for line in f:
+            if line.startswith("Y"):
+                continue
+            parts = [p for p in line.split() if not p.startswith(("N:", "Q:", "S:"))]
+            g.write(" ".join(parts) + "\n")
+
+
 def quicksort_cases() -> None:
     import numpy as np
 
@@ -88,9 +132,13 @@ def quicksort_cases() -> None:
 def main() -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--cylinder", action="store_true")
+    ap.add_argument("--resume-only", action="store_true")
     args = ap.parse_args()
     if not (os.path.exists(PROBE) and os.path.exists(PROBE_SORT)):
         subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "-j8"], check=True)
+    if args.resume_only:
+        resume_case()
+        return 0
     quicksort_cases()
     tmp = tempfile.mkdtemp(prefix="golden_")
     inp = os.path.join(ROOT, "dmrgcc_b200", "inputs", "chain16_spinless.in")
@@ -107,6 +155,7 @@ def main() -> int:
         shutil.copy(os.path.join(t, "steps.txt"), os.path.join(HERE, f"steps_{name}.txt"))
     for name in ("chain6", "cylinder3x3", "chain16"):
         gauge_trace(name)
+    resume_case()
     for kind, calls in (("heff", HEFF_CALLS), ("lanczos", HEFF_CALLS), ("env", ENV_CALLS), ("canon", CANON_CALLS)):
         for c in calls:
             shutil.copy(os.path.join(tmp, f"{kind}_{c}.nac"), os.path.join(HERE, f"{kind}_c{c}.nac"))
