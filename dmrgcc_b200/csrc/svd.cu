@@ -34,8 +34,8 @@ constexpr double kZeroRel = 4.0 * DBL_EPSILON;
 struct SvdSmem {
     double G[kPair * kLd];
     double Q[kPair * kLd];
-    double cs[kPair];
-    int pq[kPair];
+    double2 cs[kPair / 2];   // (c, s) of the step's rotation k
+    int2 pq[kPair / 2];      // the columns (a, b), a < b, that rotation k mixes
     double red[kThreads / 32];
     double flag;
     int active;   // the current step rotates something
@@ -185,7 +185,9 @@ __global__ void __launch_bounds__(kThreads) solve_kernel(const SvdProblem* __res
     // same test decides convergence); a step that rotates nothing skips the
     // update, and the solve ends once a sweep leaves every measure at or below tol.
     const double tol2f = tol * tol * fro * fro;
-    static_assert((kPair / 2) * (kPair / 2) % kThreads == 0 && (kPair / 2) * kPair % kThreads == 0, "even split");
+    static_assert(kThreads % 32 == 0 && (kPair / 2) * (kPair / 2) % kThreads == 0 &&
+                      (kPair / 2) * kPair % kThreads == 0,
+                  "even split");
     for (int sweep = 0; sweep < inner_sweeps; ++sweep) {
         int rotated = 0;
         for (int r = 0; r < kPair - 1; ++r) {
@@ -206,10 +208,8 @@ __global__ void __launch_bounds__(kThreads) solve_kernel(const SvdProblem* __res
                     c = u * rn;
                     s = (x >= 0.0 ? y : -y) * rn;
                 }
-                S.cs[2 * threadIdx.x] = c;
-                S.cs[2 * threadIdx.x + 1] = s;
-                S.pq[2 * threadIdx.x] = a;
-                S.pq[2 * threadIdx.x + 1] = b;
+                S.cs[threadIdx.x] = make_double2(c, s);
+                S.pq[threadIdx.x] = make_int2(a, b);
                 const bool any = __any_sync(0xffffffffu, s != 0.0);
                 if (threadIdx.x == 0) S.active = any ? 1 : 0;
             }
@@ -219,37 +219,60 @@ __global__ void __launch_bounds__(kThreads) solve_kernel(const SvdProblem* __res
                 continue;
             }
             rotated = 1;
-            // G <- J^T G J in one pass: every 2x2 block (rows of pair i, columns of
-            // pair j) gets both rotations at once; Q <- Q J
+            // G <- J^T G J: thread (i, j = lane) takes the 2x2 block of rows (a_i, b_i)
+            // and columns (a_j, b_j), both rotations at once; Q <- Q J: thread
+            // (row, j = lane).  The step's rotations touch disjoint entries, so every
+            // thread first loads all it updates and then stores.
+            constexpr int kGItems = (kPair / 2) * (kPair / 2) / kThreads;
+            constexpr int kQItems = kPair * (kPair / 2) / kThreads;
+            const int lane = threadIdx.x & 31;
+            const double2 csj = S.cs[lane];
+            const int2 pqj = S.pq[lane];
+            double2 csi[kGItems];
+            int2 pqi[kGItems];
+            double x[kGItems][4];
+            bool gon[kGItems];
 #pragma unroll
-            for (int u = 0; u < (kPair / 2) * (kPair / 2) / kThreads; ++u) {
-                const int idx = threadIdx.x + u * kThreads;
-                const int i = idx / (kPair / 2), j = idx % (kPair / 2);
-                const double si = S.cs[2 * i + 1], sj = S.cs[2 * j + 1];
-                if (si != 0.0 || sj != 0.0) {
-                    const double ci = S.cs[2 * i], cj = S.cs[2 * j];
-                    const int ai = S.pq[2 * i], bi = S.pq[2 * i + 1], aj = S.pq[2 * j], bj = S.pq[2 * j + 1];
-                    const double x11 = S.G[ai * kLd + aj], x12 = S.G[ai * kLd + bj];
-                    const double x21 = S.G[bi * kLd + aj], x22 = S.G[bi * kLd + bj];
-                    const double y11 = ci * x11 - si * x21, y12 = ci * x12 - si * x22;  // rows
-                    const double y21 = si * x11 + ci * x21, y22 = si * x12 + ci * x22;
-                    S.G[ai * kLd + aj] = cj * y11 - sj * y12;                            // columns
-                    S.G[ai * kLd + bj] = sj * y11 + cj * y12;
-                    S.G[bi * kLd + aj] = cj * y21 - sj * y22;
-                    S.G[bi * kLd + bj] = sj * y21 + cj * y22;
+            for (int u = 0; u < kGItems; ++u) {
+                const int i = (threadIdx.x + u * kThreads) >> 5;
+                csi[u] = S.cs[i];
+                pqi[u] = S.pq[i];
+                gon[u] = csi[u].y != 0.0 || csj.y != 0.0;
+                if (gon[u]) {
+                    x[u][0] = S.G[pqi[u].x * kLd + pqj.x];
+                    x[u][1] = S.G[pqi[u].x * kLd + pqj.y];
+                    x[u][2] = S.G[pqi[u].y * kLd + pqj.x];
+                    x[u][3] = S.G[pqi[u].y * kLd + pqj.y];
+                }
+            }
+            double q[kQItems][2];
+            const bool qon = csj.y != 0.0;
+            if (qon) {
+#pragma unroll
+                for (int u = 0; u < kQItems; ++u) {
+                    const int row = (threadIdx.x + u * kThreads) >> 5;
+                    q[u][0] = S.Q[row * kLd + pqj.x];
+                    q[u][1] = S.Q[row * kLd + pqj.y];
                 }
             }
 #pragma unroll
-            for (int u = 0; u < (kPair / 2) * kPair / kThreads; ++u) {
-                const int idx = threadIdx.x + u * kThreads;
-                const int j = idx / kPair, row = idx % kPair;
-                const double sj = S.cs[2 * j + 1];
-                if (sj != 0.0) {
-                    const double cj = S.cs[2 * j];
-                    const int a = S.pq[2 * j], b = S.pq[2 * j + 1];
-                    const double qa = S.Q[row * kLd + a], qb = S.Q[row * kLd + b];
-                    S.Q[row * kLd + a] = cj * qa - sj * qb;
-                    S.Q[row * kLd + b] = sj * qa + cj * qb;
+            for (int u = 0; u < kGItems; ++u) {
+                if (gon[u]) {
+                    const double ci = csi[u].x, si = csi[u].y, cj = csj.x, sj = csj.y;
+                    const double y11 = ci * x[u][0] - si * x[u][2], y12 = ci * x[u][1] - si * x[u][3];  // rows
+                    const double y21 = si * x[u][0] + ci * x[u][2], y22 = si * x[u][1] + ci * x[u][3];
+                    S.G[pqi[u].x * kLd + pqj.x] = cj * y11 - sj * y12;                                  // columns
+                    S.G[pqi[u].x * kLd + pqj.y] = sj * y11 + cj * y12;
+                    S.G[pqi[u].y * kLd + pqj.x] = cj * y21 - sj * y22;
+                    S.G[pqi[u].y * kLd + pqj.y] = sj * y21 + cj * y22;
+                }
+            }
+            if (qon) {
+#pragma unroll
+                for (int u = 0; u < kQItems; ++u) {
+                    const int row = (threadIdx.x + u * kThreads) >> 5;
+                    S.Q[row * kLd + pqj.x] = csj.x * q[u][0] - csj.y * q[u][1];
+                    S.Q[row * kLd + pqj.y] = csj.y * q[u][0] + csj.x * q[u][1];
                 }
             }
             __syncthreads();
