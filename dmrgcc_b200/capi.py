@@ -19,6 +19,9 @@ DMRG_PREC_FP64 = 0
 DMRG_PREC_BF16X3 = 1
 DMRG_PREC_TF32X3 = 2
 
+# status codes (DMRG_OK, DMRG_E_*)
+OK, E_ARG, E_CUDA, E_NOMEM, E_NUMERIC, E_STATE, E_IO = 0, -1, -2, -3, -4, -5, -6
+
 _lib: C.CDLL | None = None
 
 

@@ -77,6 +77,8 @@ int dmrg_run_create(dmrg_ctx_t ctx, const char* input_path, const char* model, c
         r->engine.reset(new Engine(ctx, std::move(m.space), std::move(m.ham), input, o));
         *out = r.release();
         return DMRG_OK;
+    } catch (const StatusError& e) {
+        return set_error(e.status, "%s", e.what());
     } catch (const std::exception& e) {
         return set_error(DMRG_E_ARG, "%s", e.what());
     }

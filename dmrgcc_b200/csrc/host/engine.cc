@@ -122,8 +122,8 @@ Engine::Engine(dmrg_ctx_t ctx, std::unique_ptr<QuantumSpace> space, std::unique_
     // draws no random numbers before its first expansion), like the reference (:44-51)
     int rc = cache_resume_ ? ReadTensorSpace(resume_name_) : DefineTensorSpace(first_block_, first_dim_);
     if (rc != DMRG_OK)
-        throw std::runtime_error(std::string(cache_resume_ ? "ReadTensorSpace: " : "DefineTensorSpace: ") +
-                                 dmrg_last_error());
+        throw StatusError(rc, std::string(cache_resume_ ? "ReadTensorSpace: " : "DefineTensorSpace: ") +
+                                  dmrg_last_error());
     ham_->DefineTensorHamiltonian();
     con_.resize(n_ + 1);
     for (int i = 0; i <= n_; ++i) {

@@ -9,6 +9,7 @@
 #include <array>
 #include <cstdio>
 #include <memory>
+#include <stdexcept>
 #include <string>
 #include <vector>
 
@@ -21,6 +22,13 @@
 #include "vec.cuh"
 
 namespace dmrg {
+
+// A failure raised while building a run, carrying the DMRG_E_* status that the
+// C-ABI returns for it (an unreadable checkpoint file is DMRG_E_IO).
+struct StatusError : std::runtime_error {
+    int status;
+    StatusError(int st, const std::string& what) : std::runtime_error(what), status(st) {}
+};
 
 // RealMatrixBlock with its values on the device (packed, list order).
 struct DevBlocks {

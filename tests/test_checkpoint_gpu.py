@@ -125,11 +125,14 @@ def test_resume_refuses_bad_files(ctx, tmp_path):
         data = f.read()
     with open(cut, "wb") as f:
         f.write(data[: len(data) // 2])
-    with pytest.raises(capi.DmrgError, match="truncated|malformed"):
+    with pytest.raises(capi.DmrgError, match="truncated|malformed") as err:
         capi.Run(ctx, input_with("chain6", tmp_path, cache_resume="true", resume_name=cut))
+    assert err.value.code == capi.E_IO
     other = input_with("chain16", tmp_path, cache_resume="true", resume_name=RECORD)
-    with pytest.raises(capi.DmrgError, match="number of sites"):
+    with pytest.raises(capi.DmrgError, match="number of sites") as err:
         capi.Run(ctx, other)
+    assert err.value.code == capi.E_IO
     missing = str(tmp_path / "none.dat")
-    with pytest.raises(capi.DmrgError, match="cannot open"):
+    with pytest.raises(capi.DmrgError, match="cannot open") as err:
         capi.Run(ctx, input_with("chain6", tmp_path, cache_resume="true", resume_name=missing))
+    assert err.value.code == capi.E_IO
