@@ -80,6 +80,7 @@ _SIGS = {
     "dmrg_canon_out_blocks": (C.c_int, [_VP, _I, _I, _I, _I, _I]),
     "dmrg_canon_singular_values": (C.c_int, [_VP, C.c_int, C.c_int, _D, _I]),
     "dmrg_canon_write": (C.c_int, [_VP, _VP, _VP, _VP]),
+    "dmrg_svd_pair_schedule": (C.c_int, [C.POINTER(C.c_ushort)]),
     "dmrg_quicksort_index": (C.c_int, [_D, _I, C.c_int, C.c_int]),
     "dmrg_truncate_dims": (C.c_int, [C.c_int, _I, _D, C.c_int, C.c_double, _I]),
     "dmrg_rand_stream": (C.c_int, [C.c_uint, C.c_int, _I]),
@@ -439,6 +440,14 @@ def truncate_dims(svals, max_dim: int, canpre: float):
         out.append(flat[pos:pos + c].copy())
         pos += c
     return t[:len(svals)], out
+
+
+def svd_pair_schedule() -> np.ndarray:
+    """The Jacobi pair solve's rotation schedule, [63 steps, 32 lanes] of
+    a | b << 6 | flip << 12 (host data; no GPU needed)."""
+    out = np.zeros(63 * 32, dtype=np.uint16)
+    check(lib().dmrg_svd_pair_schedule(out.ctypes.data_as(C.POINTER(C.c_ushort))), "dmrg_svd_pair_schedule")
+    return out.reshape(63, 32)
 
 
 class RunOptions(C.Structure):

@@ -4,6 +4,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdint>
 #include <cstdlib>
 #include <cstring>
 
@@ -35,13 +36,14 @@ struct SvdSmem {
     double G[kPair * kLd];
     double Q[kPair * kLd];
     double2 cs[kPair / 2];   // (c, s) of the step's rotation k
-    int2 pq[kPair / 2];      // the columns (a, b), a < b, that rotation k mixes
+    int2 pq[kPair / 2];      // the columns (first, second) that rotation k mixes
     double red[kThreads / 32];
     double flag;
     int active;   // the current step rotates something
+    uint16_t sched[(kPair - 1) * (kPair / 2)];   // the pair schedule (pair_schedule())
 };
 
-__device__ __forceinline__ void rr_pair(int r, int i, int N, int& p, int& q) {
+__host__ __device__ __forceinline__ void rr_pair(int r, int i, int N, int& p, int& q) {
     if (i == 0) {
         p = 0;
         q = r % (N - 1) + 1;
@@ -145,7 +147,7 @@ __global__ void __launch_bounds__(kThreads) solve_kernel(const SvdProblem* __res
                                                          const double* __restrict__ gpart,
                                                          const double* __restrict__ fro2, double* __restrict__ rot,
                                                          int* __restrict__ skip, unsigned long long* __restrict__ conv,
-                                                         int inner_sweeps) {
+                                                         const uint16_t* __restrict__ sched, int inner_sweeps) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     SvdSmem& S = *reinterpret_cast<SvdSmem*>(smem_raw);
     const int t = first + blockIdx.x;
@@ -159,6 +161,7 @@ __global__ void __launch_bounds__(kThreads) solve_kernel(const SvdProblem* __res
         S.G[(idx / kPair) * kLd + idx % kPair] = v;
         S.Q[(idx / kPair) * kLd + idx % kPair] = (idx / kPair == idx % kPair) ? 1.0 : 0.0;
     }
+    for (int idx = threadIdx.x; idx < (kPair - 1) * (kPair / 2); idx += kThreads) S.sched[idx] = sched[idx];
     __syncthreads();
 
     // ---- convergence measure over the pair: |g_ij| / (||A||_F max(|x_i|, |x_j|)),
@@ -192,8 +195,9 @@ __global__ void __launch_bounds__(kThreads) solve_kernel(const SvdProblem* __res
         int rotated = 0;
         for (int r = 0; r < kPair - 1; ++r) {
             if (threadIdx.x < kPair / 2) {
-                int a, b;
-                rr_pair(r, threadIdx.x, kPair, a, b);
+                const unsigned e = S.sched[r * (kPair / 2) + threadIdx.x];
+                const int a = e & 63, b = (e >> 6) & 63;  // a < b
+                const bool flip = (e >> 12) & 1;
                 const double apq = S.G[a * kLd + b];
                 double c = 1.0, s = 0.0;
                 const double daa = S.G[a * kLd + a], dbb = S.G[b * kLd + b];
@@ -208,8 +212,9 @@ __global__ void __launch_bounds__(kThreads) solve_kernel(const SvdProblem* __res
                     c = u * rn;
                     s = (x >= 0.0 ? y : -y) * rn;
                 }
-                S.cs[threadIdx.x] = make_double2(c, s);
-                S.pq[threadIdx.x] = make_int2(a, b);
+                // rotating (b, a) by (c, -s) is rotating (a, b) by (c, s)
+                S.cs[threadIdx.x] = make_double2(c, flip ? -s : s);
+                S.pq[threadIdx.x] = flip ? make_int2(b, a) : make_int2(a, b);
                 const bool any = __any_sync(0xffffffffu, s != 0.0);
                 if (threadIdx.x == 0) S.active = any ? 1 : 0;
             }
@@ -448,6 +453,103 @@ __global__ void __launch_bounds__(256) sign_kernel(const SvdProblem* __restrict_
     if (lane == 0) sign[p.s_off + j] = (first < p.m && u[first] < 0.0) ? -1.0 : 1.0;
 }
 
+// Lane order of the pair solve's rotations.  Step r rotates the 32 column pairs
+// of the round-robin schedule rr_pair(r, k); chosen here is which lane takes
+// which pair and which of its two columns the lane addresses first.  Entry
+// (r, lane) = a | b << 6 | flip << 12, a < b, flip = the lane addresses b first.
+// In each half-warp the 16 first columns lie in 16 distinct 8-byte shared-memory
+// banks (column mod 16), and so do the 16 second columns, so that every 8-byte
+// access of a step's update takes the minimum of two wavefronts.  Such an order
+// always exists: a step's pairs are the edges of a 4-regular multigraph on the 16
+// residues; orienting it along closed trails gives each residue in- and
+// out-degree 2, and the oriented edges split into two perfect matchings (tail
+// residue -> head residue), one per half-warp.  Returns DMRG_OK or, if a check
+// of the result fails, DMRG_E_STATE.
+int build_pair_schedule(std::vector<uint16_t>& tab) {
+    constexpr int kP = kPair / 2, kR = 16, kSteps = kPair - 1;
+    tab.assign(kSteps * kP, 0);
+    std::vector<int> met(kPair * kPair, 0);
+    for (int r = 0; r < kSteps; ++r) {
+        int pa[kP], pb[kP], first[kP], tail[kP], head[kP], side[kP];
+        bool used[kP];
+        std::vector<int> adj[kR];
+        for (int k = 0; k < kP; ++k) {
+            rr_pair(r, k, kPair, pa[k], pb[k]);
+            adj[pa[k] % kR].push_back(k);
+            adj[pb[k] % kR].push_back(k);
+            used[k] = false;
+            side[k] = -1;
+        }
+        // closed trails: from v0, leave each residue along an unused edge; with
+        // even degrees the walk can only stop back at v0
+        for (int v0 = 0; v0 < kR; ++v0) {
+            for (;;) {
+                int cur = v0, len = 0;
+                for (;;) {
+                    int e = -1;
+                    for (int x : adj[cur])
+                        if (!used[x]) {
+                            e = x;
+                            break;
+                        }
+                    if (e < 0) break;
+                    used[e] = true;
+                    ++len;
+                    const bool from_a = pa[e] % kR == cur;
+                    first[e] = from_a ? pa[e] : pb[e];
+                    tail[e] = cur;
+                    head[e] = (from_a ? pb[e] : pa[e]) % kR;
+                    cur = head[e];
+                }
+                if (len == 0) break;
+                if (cur != v0) return set_error(DMRG_E_STATE, "pair schedule: open trail");
+            }
+        }
+        // alternate the edges around each cycle of the 2-regular bipartite graph
+        for (int e0 = 0; e0 < kP; ++e0) {
+            for (int e = e0; side[e] < 0;) {
+                side[e] = 0;
+                int e2 = -1, e3 = -1;
+                for (int k = 0; k < kP; ++k)
+                    if (k != e && head[k] == head[e]) e2 = k;  // the other edge into head(e)
+                if (e2 < 0 || side[e2] >= 0) break;
+                side[e2] = 1;
+                for (int k = 0; k < kP; ++k)
+                    if (k != e2 && tail[k] == tail[e2]) e3 = k;  // the other edge out of tail(e2)
+                if (e3 < 0) break;
+                e = e3;
+            }
+        }
+        int n[2] = {0, 0};
+        for (int k = 0; k < kP; ++k) {
+            if (side[k] < 0 || n[side[k]] >= kP / 2) return set_error(DMRG_E_STATE, "pair schedule: unbalanced split");
+            const int slot = side[k] * (kP / 2) + n[side[k]]++;
+            tab[r * kP + slot] = (uint16_t)(pa[k] | pb[k] << 6 | (first[k] != pa[k] ? 1 : 0) << 12);
+        }
+        for (int h = 0; h < 2; ++h) {
+            unsigned fm = 0, sm = 0;
+            for (int l = 0; l < kP / 2; ++l) {
+                const unsigned e = tab[r * kP + h * (kP / 2) + l];
+                const int a = e & 63, b = (e >> 6) & 63, f = (e >> 12) & 1;
+                fm |= 1u << ((f ? b : a) % kR);
+                sm |= 1u << ((f ? a : b) % kR);
+                ++met[a * kPair + b];
+            }
+            if (fm != 0xFFFFu || sm != 0xFFFFu) return set_error(DMRG_E_STATE, "pair schedule: bank collision");
+        }
+    }
+    for (int a = 0; a < kPair; ++a)
+        for (int b = a + 1; b < kPair; ++b)
+            if (met[a * kPair + b] != 1) return set_error(DMRG_E_STATE, "pair schedule: pair (%d, %d) missed", a, b);
+    return DMRG_OK;
+}
+
+const std::vector<uint16_t>* pair_schedule() {
+    static std::vector<uint16_t> tab;
+    static const int rc = build_pair_schedule(tab);
+    return rc == DMRG_OK ? &tab : nullptr;
+}
+
 }  // namespace
 
 int BatchedSvd::plan(const std::vector<int>& m, const std::vector<int>& n, cudaStream_t st) {
@@ -528,6 +630,11 @@ int BatchedSvd::plan(const std::vector<int>& m, const std::vector<int>& n, cudaS
     DMRG_TRY(d_sign.alloc((size_t)std::max<int64_t>(soff, 1) * sizeof(double)));
     DMRG_TRY(d_colmap.alloc((size_t)std::max<int64_t>(soff, 1) * sizeof(int)));
     DMRG_TRY(d_norm.alloc((size_t)std::max<int64_t>(soff, 1) * sizeof(double)));
+    if (!d_sched.ptr) {
+        const std::vector<uint16_t>* sched = pair_schedule();
+        if (!sched) return set_error(DMRG_E_STATE, "no pair schedule");
+        DMRG_TRY(upload(d_sched, *sched, st));
+    }
     DMRG_TRY(upload(d_probs, probs, st));
     DMRG_TRY(upload(d_tasks, tasks, st));
     DMRG_TRY(upload(d_gram_items, gram_items, st));
@@ -575,7 +682,7 @@ int BatchedSvd::run(cudaStream_t st, int* sweeps_out) {
             solve_kernel<<<nt, kThreads, sizeof(SvdSmem), st>>>(
                 d_probs.as<SvdProblem>(), d_tasks.as<SvdTask>(), round_first[r], d_gpart.as<double>(),
                 d_fro2.as<double>(), d_rot.as<double>(), d_skip.as<int>(), d_conv.as<unsigned long long>(),
-                kInnerSweeps);
+                d_sched.as<uint16_t>(), kInnerSweeps);
             rotate_kernel<<<nr, 128, kRotSmem, st>>>(d_probs.as<SvdProblem>(), d_tasks.as<SvdTask>(),
                                                      d_rot_items.as<SvdItem>() + round_rot_first[r], r,
                                                      round_first[r], d_rot.as<double>(), d_skip.as<int>(),
@@ -652,3 +759,11 @@ int BatchedSvd::singular_values(std::vector<std::vector<double>>& out, cudaStrea
 }
 
 }  // namespace dmrg
+
+extern "C" int dmrg_svd_pair_schedule(unsigned short* out) {
+    if (!out) return dmrg::set_error(DMRG_E_ARG, "null argument");
+    const std::vector<uint16_t>* tab = dmrg::pair_schedule();
+    if (!tab) return DMRG_E_STATE;
+    std::memcpy(out, tab->data(), tab->size() * sizeof(uint16_t));
+    return DMRG_OK;
+}

@@ -72,6 +72,7 @@ public:
     DeviceBuffer d_sign;  // +-1 per sorted singular triplet (sign convention, set by run())
     DeviceBuffer d_gram_items, d_rot_items, d_gpart, d_rot, d_skip;
     DeviceBuffer d_colmap, d_norm;  // per sweep: columns in descending norm order
+    DeviceBuffer d_sched;           // lane order of the pair solve's rotations (uploaded once)
     std::vector<SvdProblem> probs;
     std::vector<int> index;             // sector -> problem (-1 when empty)
     std::vector<int> round_first;       // task offset of each round

@@ -220,6 +220,12 @@ int dmrg_canon_out_blocks(dmrg_canon_t c, int* ket_rows, int* ket_cols, int* can
                           int* canon_cols, int* match_dim);
 int dmrg_canon_singular_values(dmrg_canon_t c, int sector, int cap, double* values, int* count);
 int dmrg_canon_write(dmrg_canon_t c, const double* ket_dev, double* new_ket_dev, double* canonical_dev);
+/* The Jacobi pair solve's rotation schedule (diagnostic; no reference
+ * counterpart): out[63 * 32], entry (step r, lane) = a | b << 6 | flip << 12 with
+ * (a, b), a < b, the pair of the pair's 64 columns that the lane rotates in step
+ * r and flip = the lane addresses b first.  Every two columns share one step;
+ * within each half-warp the first (and the second) columns are distinct mod 16. */
+int dmrg_svd_pair_schedule(unsigned short* out);
 
 /* ---- whole runs: the sweep engine ------------------------------------------
  * dmrg_run_create reads a reference input file (the model keys of
