@@ -105,14 +105,31 @@ __global__ void __launch_bounds__(128) gram_kernel(const SvdProblem* __restrict_
     for (int i = 0; i < 4; ++i)
 #pragma unroll
         for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+    // thread: row k of each chunk in columns c = warp + 4e (e < 16); the column
+    // offsets are looked up once, and the next chunk is loaded into registers
+    // while the tensor cores work on the current one
+    constexpr int kCols = kChunk * kPair / 128;
+    static_assert(kChunk == 32 && kCols * 128 == kChunk * kPair, "one row per lane");
+    const int k = lane;
+    int64_t coff[kCols];
+#pragma unroll
+    for (int e = 0; e < kCols; ++e) {
+        const int c = warp + 4 * e;
+        const int vc = c < kBlk ? colI + c : colJ + c - kBlk;
+        coff[e] = vc < p.cols ? (int64_t)colmap[p.perm_off + vc] * p.rows : -1;
+    }
+    double nxt[kCols];
+#pragma unroll
+    for (int e = 0; e < kCols; ++e) nxt[e] = (coff[e] >= 0 && it.r0 + k < it.r1) ? Wp[coff[e] + it.r0 + k] : 0.0;
     for (int k0 = it.r0; k0 < it.r1; k0 += kChunk) {
-        for (int idx = threadIdx.x; idx < kChunk * kPair; idx += 128) {
-            const int c = idx / kChunk, k = idx % kChunk;
-            const int vc = c < kBlk ? colI + c : colJ + c - kBlk;
-            const bool v = vc < p.cols && k0 + k < it.r1;
-            Xt[c * kGramLd + k] = v ? Wp[(int64_t)colmap[p.perm_off + vc] * p.rows + k0 + k] : 0.0;
-        }
+#pragma unroll
+        for (int e = 0; e < kCols; ++e) Xt[(warp + 4 * e) * kGramLd + k] = nxt[e];
         __syncthreads();
+        const int k1 = k0 + kChunk;
+        if (k1 < it.r1) {
+#pragma unroll
+            for (int e = 0; e < kCols; ++e) nxt[e] = (coff[e] >= 0 && k1 + k < it.r1) ? Wp[coff[e] + k1 + k] : 0.0;
+        }
 #pragma unroll
         for (int kk = 0; kk < kChunk; kk += 4) {
             double a[4], b[4];
@@ -155,11 +172,24 @@ __global__ void __launch_bounds__(kThreads) solve_kernel(const SvdProblem* __res
     const SvdProblem p = probs[task.problem];
     const double tol = 2.0 * DBL_EPSILON * sqrt((double)p.rows);
     const double zero2 = kZeroRel * kZeroRel * (double)p.rows * fro2[task.problem];
-    for (int idx = threadIdx.x; idx < kPair * kPair; idx += kThreads) {
-        double v = 0.0;
-        for (int c = 0; c < task.g_count; ++c) v += gpart[(int64_t)(task.g_first + c) * kPair * kPair + idx];
-        S.G[(idx / kPair) * kLd + idx % kPair] = v;
-        S.Q[(idx / kPair) * kLd + idx % kPair] = (idx / kPair == idx % kPair) ? 1.0 : 0.0;
+    {
+        // the partials in a fixed order (c ascending) per entry; the entries of
+        // a thread are independent, so all of a partial's loads are in flight
+        constexpr int kElems = kPair * kPair / kThreads;
+        static_assert(kPair * kPair % kThreads == 0, "even split");
+        double v[kElems];
+#pragma unroll
+        for (int u = 0; u < kElems; ++u) v[u] = 0.0;
+        const double* gp = gpart + (int64_t)task.g_first * kPair * kPair + threadIdx.x;
+        for (int c = 0; c < task.g_count; ++c, gp += kPair * kPair)
+#pragma unroll
+            for (int u = 0; u < kElems; ++u) v[u] += gp[u * kThreads];
+#pragma unroll
+        for (int u = 0; u < kElems; ++u) {
+            const int idx = threadIdx.x + u * kThreads;
+            S.G[(idx / kPair) * kLd + idx % kPair] = v[u];
+            S.Q[(idx / kPair) * kLd + idx % kPair] = (idx / kPair == idx % kPair) ? 1.0 : 0.0;
+        }
     }
     for (int idx = threadIdx.x; idx < (kPair - 1) * (kPair / 2); idx += kThreads) S.sched[idx] = sched[idx];
     __syncthreads();
