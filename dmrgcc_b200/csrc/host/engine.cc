@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <stdexcept>
+#include <thread>
 
 #include "gemm.cuh"
 
@@ -231,7 +232,7 @@ void Engine::DefineLatticeSectors(TensorLattice& t, const std::vector<int>& lb, 
 // RealTensorLattice::DefineTensorLattice(blocks, row, column) (:328-343): every
 // block row x column, random from the glibc stream.
 int Engine::DefineLatticeBlocks(TensorLattice& t, const std::vector<int>& li, const std::vector<int>& ri,
-                                const std::vector<int>& pi, int row, int column) {
+                                const std::vector<int>& pi, int row, int column, bool device) {
     t.ket = DevBlocks();
     for (size_t k = 0; k < li.size(); ++k) {
         t.phys[(size_t)li[k] * t.nr() + ri[k]] = pi[k];
@@ -239,6 +240,7 @@ int Engine::DefineLatticeBlocks(TensorLattice& t, const std::vector<int>& li, co
     }
     std::vector<double> host((size_t)std::max<int64_t>(t.ket.d.size, 0));
     for (size_t k = 0; k < li.size(); ++k) random_block(rng_, rand_draws_, host, (size_t)t.ket.d.off[k], row, column);
+    if (!device) return DMRG_OK;  // the draws only advance the stream (the caller discards the values)
     DMRG_TRY(t.ket.alloc(st_, false));
     if (!host.empty())
         DMRG_CUDA_TRY(cudaMemcpyAsync(t.ket.ptr(), host.data(), host.size() * sizeof(double), cudaMemcpyHostToDevice,
@@ -623,7 +625,7 @@ void Engine::ComputeExpanTensorLattice(int leigh, int site, std::vector<std::vec
                 pi.push_back(info);
             }
         }
-    DefineLatticeBlocks(e, li, ri, pi, 1, 1);  // draws from rand() like the reference
+    DefineLatticeBlocks(e, li, ri, pi, 1, 1, false);  // draws from rand() like the reference; values unused
     e.ket.set_shape_zero();
 }
 
@@ -638,6 +640,8 @@ int Engine::LeftExpanTensorContraction(int site, const std::vector<std::vector<i
     const int lb = W.get_left_bond(), rb = W.get_right_bond();
     auto same_left = t.ket.d.by_sector(0, t.nl());
     const bool compute = expansion_enabled(p_max_block_, p_max_dim_, p_noise_);
+    xw_.active = true;
+    xw_.compute = compute;
     // pass 1: which expanded right sectors receive something
     std::vector<char> exist(e.nr(), 0);
     for (int o1 = 0; o1 < lb; ++o1) {
@@ -686,20 +690,13 @@ int Engine::LeftExpanTensorContraction(int site, const std::vector<std::vector<i
         for (int k = 0; k < e.nr(); ++k)
             if (e.p(l, k) != -1) eb.push(l, k, 0, 0);
     // pass 2: contributions, in the reference's order; rand() draws for each
-    struct Contrib {
-        int first;    // index of the L*K product
-        int d0, d1;   // random matrix shape
-        int64_t rnd;  // offset of its values
-    };
-    struct First {
-        int64_t l_off, k_off;
-        int m, k, n;  // (m x k) * (k x n)
-        int64_t off;
-    };
-    std::vector<First> firsts;
-    std::vector<std::vector<Contrib>> contrib(eb.count());
-    std::vector<double> rnd;
-    int64_t first_size = 0;
+    using First = ExpanWork::First;
+    using Contrib = ExpanWork::Contrib;
+    std::vector<First>& firsts = xw_.firsts;
+    std::vector<std::vector<Contrib>>& contrib = xw_.contrib;
+    contrib.assign(eb.count(), {});
+    std::vector<double>& rnd = xw_.rnd;
+    int64_t& first_size = xw_.first_size;
     for (int o1 = 0; o1 < lb; ++o1) {
         const BlockListDesc& Lo = con.L.desc.o[o1];
         for (int i = 0; i < Lo.count(); ++i) {
@@ -766,37 +763,9 @@ int Engine::LeftExpanTensorContraction(int site, const std::vector<std::vector<i
             }
         }
     }
-    BlockListDesc packed;
+    BlockListDesc& packed = xw_.packed;
+    packed = BlockListDesc();
     for (int b = 0; b < eb.count(); ++b) packed.push(eb.left[b], eb.right[b], eb.rows[b], eb.cols[b]);
-    e.ket = DevBlocks();
-    e.ket.d = packed;
-    DMRG_TRY(e.ket.alloc(st_, true));
-    if (!compute || firsts.empty()) return DMRG_OK;  // rand() stream advanced; products unused
-    // device: F = L K, then each block's column ranges = noise * F R_rand
-    DMRG_TRY(scratch_.alloc((size_t)std::max<int64_t>(first_size, 1) * sizeof(double)));
-    DMRG_TRY(scratch2_.alloc(std::max<size_t>(rnd.size(), 1) * sizeof(double)));
-    DMRG_CUDA_TRY(cudaMemcpyAsync(scratch2_.ptr, rnd.data(), rnd.size() * sizeof(double), cudaMemcpyHostToDevice, st_));
-    GemmSchedule sf, ss;
-    for (const First& f : firsts) {
-        sf.add_group(f.off, f.n, f.m, f.n);
-        sf.add_term(f.l_off, f.k, f.k_off, f.n, f.k, 1.0);
-    }
-    for (int b = 0; b < packed.count(); ++b) {
-        int col = 0;
-        for (const Contrib& c : contrib[b]) {
-            const First& f = firsts[c.first];
-            ss.add_group(packed.off[b] + col, packed.cols[b], f.m, c.d1);
-            ss.add_term(f.off, f.n, c.rnd, c.d1, c.d0, p_noise_);
-            col += c.d1;
-        }
-    }
-    DMRG_TRY(sf.check_bounds(con.L.desc.size, t.ket.d.size, first_size));
-    DMRG_TRY(ss.check_bounds(first_size, (int64_t)rnd.size(), packed.size));
-    DMRG_TRY(sf.finalize(64, 64, 16, st_));
-    DMRG_TRY(ss.finalize(64, 64, 16, st_));
-    DMRG_TRY(launch_gemm_f64(sf, con.L.ptr(), t.ket.ptr(), scratch_.as<double>(), false, st_));
-    DMRG_TRY(launch_gemm_f64(ss, scratch_.as<double>(), scratch2_.as<double>(), e.ket.ptr(), false, st_));
-    DMRG_CUDA_TRY(cudaStreamSynchronize(st_));
     return DMRG_OK;
 }
 
@@ -808,6 +777,8 @@ int Engine::RightExpanTensorContraction(int site, const std::vector<std::vector<
     const int lb = W.get_left_bond(), rb = W.get_right_bond();
     auto same_right = t.ket.d.by_sector(1, t.nr());
     const bool compute = expansion_enabled(p_max_block_, p_max_dim_, p_noise_);
+    xw_.active = true;
+    xw_.compute = compute;
     std::vector<char> exist(e.nl(), 0);
     for (int o2 = 0; o2 < rb; ++o2) {
         const BlockListDesc& Ro = con.R.desc.o[o2];
@@ -853,20 +824,13 @@ int Engine::RightExpanTensorContraction(int site, const std::vector<std::vector<
     for (int l = 0; l < e.nl(); ++l)
         for (int r = 0; r < e.nr(); ++r)
             if (e.p(l, r) != -1) eb.push(l, r, 0, 0);
-    struct Contrib {
-        int first;
-        int d0, d1;
-        int64_t rnd;
-    };
-    struct First {
-        int64_t k_off, r_off;
-        int m, k, n;
-        int64_t off;
-    };
-    std::vector<First> firsts;
-    std::vector<std::vector<Contrib>> contrib(eb.count());
-    std::vector<double> rnd;
-    int64_t first_size = 0;
+    using First = ExpanWork::First;
+    using Contrib = ExpanWork::Contrib;
+    std::vector<First>& firsts = xw_.firsts;
+    std::vector<std::vector<Contrib>>& contrib = xw_.contrib;
+    contrib.assign(eb.count(), {});
+    std::vector<double>& rnd = xw_.rnd;
+    int64_t& first_size = xw_.first_size;
     for (int o2 = 0; o2 < rb; ++o2) {
         const BlockListDesc& Ro = con.R.desc.o[o2];
         for (int i = 0; i < Ro.count(); ++i) {
@@ -933,42 +897,82 @@ int Engine::RightExpanTensorContraction(int site, const std::vector<std::vector<
             }
         }
     }
-    BlockListDesc packed;
+    BlockListDesc& packed = xw_.packed;
+    packed = BlockListDesc();
     for (int b = 0; b < eb.count(); ++b) packed.push(eb.left[b], eb.right[b], eb.rows[b], eb.cols[b]);
+    return DMRG_OK;
+}
+
+// The device half of the planned expansion: the expanded lattice's blocks, then
+// F = L K (K R) per product and each block's column (row) ranges = noise * F Rand
+// (Rand K R), in the reference's order of contributions.
+int Engine::ExecuteExpanTensorNetwork() {
+    if (!xw_.active) return DMRG_OK;
+    if (!expan_) return set_error(DMRG_E_STATE, "expan_tensor_lattice is nullptr!");
+    TensorLattice& e = *expan_;
+    const BlockListDesc& packed = xw_.packed;
     e.ket = DevBlocks();
     e.ket.d = packed;
     DMRG_TRY(e.ket.alloc(st_, true));
-    if (!compute || firsts.empty()) return DMRG_OK;
+    if (!xw_.compute || xw_.firsts.empty()) return DMRG_OK;  // rand() stream advanced; products unused
+    const TensorLattice& t = *lat_[xw_.site];
+    const TensorContraction& con = *con_[xw_.site];
+    const std::vector<double>& rnd = xw_.rnd;
+    const int64_t first_size = xw_.first_size;
     DMRG_TRY(scratch_.alloc((size_t)std::max<int64_t>(first_size, 1) * sizeof(double)));
     DMRG_TRY(scratch2_.alloc(std::max<size_t>(rnd.size(), 1) * sizeof(double)));
     DMRG_CUDA_TRY(cudaMemcpyAsync(scratch2_.ptr, rnd.data(), rnd.size() * sizeof(double), cudaMemcpyHostToDevice, st_));
     GemmSchedule sf, ss;
-    for (const First& f : firsts) {
+    for (const ExpanWork::First& f : xw_.firsts) {
         sf.add_group(f.off, f.n, f.m, f.n);
-        sf.add_term(f.k_off, f.k, f.r_off, f.n, f.k, 1.0);
+        sf.add_term(f.a_off, f.k, f.b_off, f.n, f.k, 1.0);
     }
     for (int b = 0; b < packed.count(); ++b) {
-        int row = 0;
-        for (const Contrib& c : contrib[b]) {
-            const First& f = firsts[c.first];
-            ss.add_group(packed.off[b] + (int64_t)row * packed.cols[b], packed.cols[b], c.d0, f.n);
-            ss.add_term(c.rnd, c.d1, f.off, f.n, c.d1, p_noise_);
-            row += c.d0;
+        int at = 0;
+        for (const ExpanWork::Contrib& c : xw_.contrib[b]) {
+            const ExpanWork::First& f = xw_.firsts[c.first];
+            if (xw_.leigh == 0) {  // columns [at, at + d1) of the block = (L K) * Rand
+                ss.add_group(packed.off[b] + at, packed.cols[b], f.m, c.d1);
+                ss.add_term(f.off, f.n, c.rnd, c.d1, c.d0, p_noise_);
+                at += c.d1;
+            } else {  // rows [at, at + d0) of the block = Rand * (K R)
+                ss.add_group(packed.off[b] + (int64_t)at * packed.cols[b], packed.cols[b], c.d0, f.n);
+                ss.add_term(c.rnd, c.d1, f.off, f.n, c.d1, p_noise_);
+                at += c.d0;
+            }
         }
     }
-    DMRG_TRY(sf.check_bounds(t.ket.d.size, con.R.desc.size, first_size));
-    DMRG_TRY(ss.check_bounds((int64_t)rnd.size(), first_size, packed.size));
+    if (xw_.leigh == 0) {
+        DMRG_TRY(sf.check_bounds(con.L.desc.size, t.ket.d.size, first_size));
+        DMRG_TRY(ss.check_bounds(first_size, (int64_t)rnd.size(), packed.size));
+    } else {
+        DMRG_TRY(sf.check_bounds(t.ket.d.size, con.R.desc.size, first_size));
+        DMRG_TRY(ss.check_bounds((int64_t)rnd.size(), first_size, packed.size));
+    }
     DMRG_TRY(sf.finalize(64, 64, 16, st_));
     DMRG_TRY(ss.finalize(64, 64, 16, st_));
-    DMRG_TRY(launch_gemm_f64(sf, t.ket.ptr(), con.R.ptr(), scratch_.as<double>(), false, st_));
-    DMRG_TRY(launch_gemm_f64(ss, scratch2_.as<double>(), scratch_.as<double>(), e.ket.ptr(), false, st_));
+    if (xw_.leigh == 0) {
+        DMRG_TRY(launch_gemm_f64(sf, con.L.ptr(), t.ket.ptr(), scratch_.as<double>(), false, st_));
+        DMRG_TRY(launch_gemm_f64(ss, scratch_.as<double>(), scratch2_.as<double>(), e.ket.ptr(), false, st_));
+    } else {
+        DMRG_TRY(launch_gemm_f64(sf, t.ket.ptr(), con.R.ptr(), scratch_.as<double>(), false, st_));
+        DMRG_TRY(launch_gemm_f64(ss, scratch2_.as<double>(), scratch_.as<double>(), e.ket.ptr(), false, st_));
+    }
     DMRG_CUDA_TRY(cudaStreamSynchronize(st_));
     return DMRG_OK;
 }
 
 // RealTensorNetwork::ExpanTensorNetwork (real_tensor_network.cc:116-140)
 int Engine::ExpanTensorNetwork(int leigh, int site) {
+    DMRG_TRY(PlanExpanTensorNetwork(leigh, site));
+    return ExecuteExpanTensorNetwork();
+}
+
+int Engine::PlanExpanTensorNetwork(int leigh, int site) {
     std::vector<std::vector<int>> mapping;
+    xw_ = ExpanWork();
+    xw_.leigh = leigh;
+    xw_.site = site;
     ComputeExpanTensorLattice((leigh + 1) % 2, site, mapping);
     if (leigh == 0 && site < n_ - 1) return LeftExpanTensorContraction(site, mapping);
     if (leigh == 1 && site > 0) return RightExpanTensorContraction(site, mapping);
@@ -1143,12 +1147,26 @@ int Engine::Run() {
             int dim = 0;
             const int64_t psi_dim = lat_[j]->psi_dim();  // at the Lanczos call, like the reference's log
             tp = wall_time();
-            DMRG_TRY(LanczosMethod(num_iter_[h], j, energy_, dim));
+            // The expansion's host half (its lattice, its products and their
+            // rand() matrices) depends only on block structures that the Lanczos
+            // leaves as they are, so a second host thread plans it while the
+            // device solves.  No CUDA call is made on that thread.
+            int plan_rc = DMRG_OK;
+            std::string plan_err;
+            expan_.reset();  // a disabled expansion leaves its lattice: free its device blocks on this thread
+            std::thread planner([&] {
+                plan_rc = PlanExpanTensorNetwork(l2r ? 0 : 1, j);
+                if (plan_rc != DMRG_OK) plan_err = dmrg_last_error();
+            });
+            const int lanczos_rc = LanczosMethod(num_iter_[h], j, energy_, dim);
+            planner.join();
+            DMRG_TRY(lanczos_rc);
+            if (plan_rc != DMRG_OK) return set_error(plan_rc, "%s", plan_err.c_str());
             DMRG_TRY(lap(0));
             if (trace_) std::fprintf(trace_, "E %d %d P:%lld %.12e\n", lanczos_calls_, j, (long long)psi_dim, energy_);
             ++lanczos_calls_;
             DMRG_TRY(ResetEnv(l2r ? 1 : 0, j));
-            DMRG_TRY(ExpanTensorNetwork(l2r ? 0 : 1, j));
+            DMRG_TRY(ExecuteExpanTensorNetwork());
             DMRG_TRY(ExpanTensorSpace(l2r ? 0 : 1, j));
             DMRG_TRY(lap(1));
             Trace("X", l2r ? 0 : 1, j);

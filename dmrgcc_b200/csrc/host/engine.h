@@ -116,7 +116,12 @@ public:
     int MergeTensorSpace(int leigh, int site);
     int ExpanTensorSpace(int leigh, int site);
     int MatchTensorSpace(int leigh, int site);
+    // ExpanTensorNetwork = PlanExpanTensorNetwork (host only: the expanded
+    // lattice, the products to form and their rand() matrices; no CUDA call)
+    // followed by ExecuteExpanTensorNetwork (the device products).
     int ExpanTensorNetwork(int leigh, int site);
+    int PlanExpanTensorNetwork(int leigh, int site);
+    int ExecuteExpanTensorNetwork();
     int ComputeTensorNetwork(int leigh, int site);
     int LanczosMethod(int niter, int site, double& energy, int& dim);
     // RealTensorSpace::WriteTensorSpace / ReadTensorSpace (real_tensor_space.cc:
@@ -131,7 +136,7 @@ private:
     void DefineLatticeSectors(TensorLattice& t, const std::vector<int>& lb, const std::vector<int>& rb,
                               const std::vector<int>& ld, const std::vector<int>& rd);
     int DefineLatticeBlocks(TensorLattice& t, const std::vector<int>& li, const std::vector<int>& ri,
-                            const std::vector<int>& pi, int row, int column);
+                            const std::vector<int>& pi, int row, int column, bool device = true);
     void ComputeExpanTensorLattice(int leigh, int site, std::vector<std::vector<int>>& mapping);
     int LeftExpanTensorContraction(int site, const std::vector<std::vector<int>>& mapping);
     int RightExpanTensorContraction(int site, const std::vector<std::vector<int>>& mapping);
@@ -150,6 +155,27 @@ private:
     std::vector<std::unique_ptr<TensorLattice>> lat_;
     std::vector<std::unique_ptr<TensorContraction>> con_;
     std::unique_ptr<TensorLattice> expan_;
+    // the planned half of the current subspace expansion
+    struct ExpanWork {
+        struct First {  // one (m x k) * (k x n) product: L*K (left) or K*R (right)
+            int64_t a_off, b_off;
+            int m, k, n;
+            int64_t off;
+        };
+        struct Contrib {  // one random matrix (d0 x d1) applied to product `first`
+            int first;
+            int d0, d1;
+            int64_t rnd;
+        };
+        bool active = false, compute = false;
+        int leigh = 0, site = 0;
+        std::vector<First> firsts;
+        std::vector<std::vector<Contrib>> contrib;  // per block of the expanded lattice
+        std::vector<double> rnd;
+        int64_t first_size = 0;
+        BlockListDesc packed;
+    };
+    ExpanWork xw_;
     // sweep table (real_tensor_rundmrg.cc:70-113)
     int num_sweep_ = 0;
     std::vector<int> max_dim_, max_block_, num_iter_;
