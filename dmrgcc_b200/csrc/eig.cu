@@ -201,10 +201,26 @@ __device__ double eigvec_sign(const double* v, int n, int stride) {
     return 1.0;
 }
 
-__global__ void __launch_bounds__(kJacobiThreads) sym_jacobi_kernel(double* A, int n, double* w, double* Zout,
+// Dynamic shared memory of the solve: the rotation table (3 * npair doubles,
+// jacobi_core's), then, when they fit, the working copies of A and Z, so that
+// the thousands of barrier-separated passes of a solve stay on the SM.
+constexpr size_t kJacobiSmemCap = 200 * 1024;
+__host__ __device__ inline size_t jacobi_table_doubles(int n) { return (size_t)3 * ((n + (n & 1)) / 2); }
+__host__ __device__ inline bool jacobi_in_smem(int n) {
+    return (jacobi_table_doubles(n) + 2 * (size_t)n * n) * sizeof(double) <= kJacobiSmemCap;
+}
+
+__global__ void __launch_bounds__(kJacobiThreads) sym_jacobi_kernel(double* Ag, int n, double* w, double* Zout,
                                                                     double* ws, int* status) {
-    double* Z = ws;
+    extern __shared__ double dyn[];
+    const bool local = jacobi_in_smem(n);
+    double* A = local ? dyn + jacobi_table_doubles(n) : Ag;
+    double* Z = local ? A + (size_t)n * n : ws;
     int* order = reinterpret_cast<int*>(ws + (size_t)n * n);
+    if (local) {
+        for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) A[idx] = Ag[idx];
+        __syncthreads();
+    }
     const bool ok = jacobi_core(A, n, Z);
     if (threadIdx.x == 0) {
         if (!ok) status[0] = DMRG_E_NUMERIC;
@@ -330,13 +346,15 @@ int launch_tridiag_lowest(const double* alpha, const double* beta, int m, double
 }
 
 static size_t jacobi_smem(int n) {
-    const int npair = (n + (n & 1)) / 2;
-    return (size_t)npair * 2 * sizeof(double) + (size_t)npair * 2 * sizeof(int);
+    return (jacobi_table_doubles(n) + (jacobi_in_smem(n) ? 2 * (size_t)n * n : 0)) * sizeof(double);
 }
 
 int launch_sym_jacobi(double* A, int n, double* w, double* Z, double* ws, int* status, cudaStream_t st) {
     if (n <= 0) return DMRG_OK;
-    sym_jacobi_kernel<<<1, kJacobiThreads, jacobi_smem(n), st>>>(A, n, w, Z, ws, status);
+    const size_t smem = jacobi_smem(n);
+    if (smem > 48 * 1024)
+        DMRG_CUDA_TRY(cudaFuncSetAttribute(sym_jacobi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    sym_jacobi_kernel<<<1, kJacobiThreads, smem, st>>>(A, n, w, Z, ws, status);
     DMRG_CUDA_TRY(cudaGetLastError());
     return DMRG_OK;
 }
