@@ -26,6 +26,10 @@ constexpr int kLd = kPair + 1;  // padded row of the shared 64x64 matrices
 #endif
 constexpr int kInnerSweeps = DMRG_SVD_INNER_SWEEPS;
 constexpr int kMaxSweeps = 40;
+#ifndef DMRG_SVD_GRAM_MIN_ROWS
+#define DMRG_SVD_GRAM_MIN_ROWS 64
+#endif
+constexpr int kGramMinRows = DMRG_SVD_GRAM_MIN_ROWS;  // rows of a Gram item, at least (multiple of 32)
 // Columns whose norm is below kZeroRel * sqrt(rows) * ||A||_F are rounding
 // residue of a rank-deficient matrix: they take part in no rotation and in no
 // convergence test (their values are below any truncation threshold that is
@@ -610,8 +614,8 @@ int BatchedSvd::plan(const std::vector<int>& m, const std::vector<int>& n, cudaS
         probs.push_back(p);
         max_rounds = std::max(max_rounds, p.nbe - 1);
     }
-    // Row ranges of the Gram items: at least 256 rows each, fewer items than
-    // ~4 per SM in the widest round (bounds the partial-Gram buffer).
+    // Row ranges of the Gram items: at least kGramMinRows rows each, fewer items
+    // than ~4 per SM in the widest round (bounds the partial-Gram buffer).
     int64_t widest = 0;
     for (int r = 0; r < max_rounds; ++r) {
         int64_t rows = 0;
@@ -619,7 +623,7 @@ int BatchedSvd::plan(const std::vector<int>& m, const std::vector<int>& n, cudaS
             if (r < p.nbe - 1) rows += (int64_t)p.rows * (p.nbe / 2);
         widest = std::max(widest, rows);
     }
-    const int gram_rows = (int)std::max<int64_t>(256, ((widest / 600 + 31) / 32) * 32);
+    const int gram_rows = (int)std::max<int64_t>(kGramMinRows, ((widest / 600 + 31) / 32) * 32);
     gram_items.clear();
     rot_items.clear();
     round_gram_first.clear();
