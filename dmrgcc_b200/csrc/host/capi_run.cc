@@ -86,8 +86,12 @@ int dmrg_run_create(dmrg_ctx_t ctx, const char* input_path, const char* model, c
 
 int dmrg_run_execute(dmrg_run_t r) {
     if (!r) return set_error(DMRG_E_ARG, "null run");
-    AllocScope pool(r->engine->stream());
-    return r->engine->Run();
+    try {
+        AllocScope pool(r->engine->stream());
+        return r->engine->Run();
+    } catch (const std::exception& e) {  // no exception crosses the C ABI
+        return set_error(DMRG_E_STATE, "%s", e.what());
+    }
 }
 
 int dmrg_run_destroy(dmrg_run_t r) {

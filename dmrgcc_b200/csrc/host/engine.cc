@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <stdexcept>
+#include <system_error>
 #include <thread>
 
 #include "gemm.cuh"
@@ -1154,12 +1155,18 @@ int Engine::Run() {
             int plan_rc = DMRG_OK;
             std::string plan_err;
             expan_.reset();  // a disabled expansion leaves its lattice: free its device blocks on this thread
-            std::thread planner([&] {
+            auto plan = [&] {
                 plan_rc = PlanExpanTensorNetwork(l2r ? 0 : 1, j);
                 if (plan_rc != DMRG_OK) plan_err = dmrg_last_error();
-            });
+            };
+            std::thread planner;
+            try {
+                planner = std::thread(plan);
+            } catch (const std::system_error&) {
+                plan();  // no thread to be had: plan first (same draws, same results)
+            }
             const int lanczos_rc = LanczosMethod(num_iter_[h], j, energy_, dim);
-            planner.join();
+            if (planner.joinable()) planner.join();
             DMRG_TRY(lanczos_rc);
             if (plan_rc != DMRG_OK) return set_error(plan_rc, "%s", plan_err.c_str());
             DMRG_TRY(lap(0));
