@@ -1,5 +1,5 @@
-"""Checkpoint write and resume (cache_record / cache_resume, SURVEY next row:
-on-disk formats) against the reference.
+"""Checkpoint write and resume (cache_record / cache_resume, the on-disk
+tensor-space file) against the reference.
 
 * Writing: the library's record of the 6-site chain after two sweeps equals the
   one the (sign-gauge-pinned) reference wrote for the same run

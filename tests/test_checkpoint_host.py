@@ -1,4 +1,4 @@
-"""Checkpoint format (SURVEY next row: on-disk formats), host side: the reader in
+"""Checkpoint format (the on-disk tensor-space file), host side: the reader in
 oracle/space_file.py restates the reference's writers; it must parse the file
 the reference itself wrote (tests/golden/record_chain6.dat: the 6-site chain
 after its first two sweeps, cache_record) completely and consistently with the
