@@ -17,7 +17,13 @@
 // guarded by a mutex, so concurrent host threads serialise their set-up only.
 // The first call on a device looks up the array's device address
 // (cudaGetSymbolAddress) with that device current; make that first call before
-// any stream capture.
+// any stream capture.  The address is kept for the life of the process, so the
+// library must not be used across a cudaDeviceReset of that device.
+//
+// Every argument is validated on the host before any CUDA call: sector indices
+// of the ket, L and R blocks inside their sector ranges, each ket block's
+// physics index inside [0, d), no negative shape.  A malformed table returns
+// DMRG_E_ARG, like dmrg_heff_create.
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -38,6 +44,8 @@ namespace {
 constexpr size_t kNoAllocScratchBytes = size_t(16) << 20;  // 16 MiB
 constexpr int kMaxDevices = 64;
 constexpr int kMaxOutBlocks = 4096;
+constexpr int kMaxEnvBlocks = 1 << 16;  // blocks of all MPO bond indices of one environment
+constexpr int kMaxBond = 512;
 constexpr int kTile = 64;
 
 __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
@@ -51,6 +59,11 @@ struct PendingTerm {
 };
 PendingTerm g_pending[kNoAllocScratchBytes / sizeof(PendingTerm) / 4];
 int g_count[kMaxOutBlocks + 1];
+// packed offsets (doubles) of every ket block and of every L / R block, bond by
+// bond (the blocks of bond o start at index first[o]); filled once per call
+int64_t g_ket_off[kMaxOutBlocks + 1];
+int64_t g_L_off[kMaxEnvBlocks + 1], g_R_off[kMaxEnvBlocks + 1];
+int g_L_first[kMaxBond + 1], g_R_first[kMaxBond + 1];
 
 size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
@@ -62,10 +75,34 @@ struct View {
 
 View view(const dmrg_blocks_t& b) { return View{b.nblocks, b.left, b.right, b.rows, b.cols}; }
 
-int64_t block_off(const View& v, int k) {
-    int64_t off = 0;
-    for (int i = 0; i < k; ++i) off += (int64_t)v.rows[i] * v.cols[i];
-    return off;
+// Checks one block list: count, non-null arrays, sector indices in [0, nsec)
+// on both sides, no negative shape.
+bool valid_list(const dmrg_blocks_t& b, int nsec_left, int nsec_right) {
+    if (b.nblocks < 0) return false;
+    if (b.nblocks > 0 && (!b.left || !b.right || !b.rows || !b.cols)) return false;
+    for (int k = 0; k < b.nblocks; ++k)
+        if (b.left[k] < 0 || b.left[k] >= nsec_left || b.right[k] < 0 || b.right[k] >= nsec_right || b.rows[k] < 0 ||
+            b.cols[k] < 0)
+            return false;
+    return true;
+}
+
+// Packed offsets of the blocks of `n` consecutive lists into off[first[o] + q];
+// returns the total size, or -1 when more than `cap` blocks.
+int64_t list_offsets(const dmrg_blocks_t* lists, int n, int64_t* off, int* first, int cap) {
+    int64_t acc = 0;
+    int idx = 0;
+    for (int o = 0; o < n; ++o) {
+        first[o] = idx;
+        if (idx + lists[o].nblocks > cap) return -1;
+        for (int q = 0; q < lists[o].nblocks; ++q) {
+            off[idx++] = acc;
+            acc += (int64_t)lists[o].rows[q] * lists[o].cols[q];
+        }
+    }
+    first[n] = idx;
+    off[idx] = acc;
+    return acc;
 }
 
 int find(const View& v, int l, int r) {
@@ -83,6 +120,28 @@ extern "C" int dmrg_heff_apply_noalloc(int nl, int nr, const int* phys, const dm
     if (nl <= 0 || nr <= 0 || !phys || !ket || d <= 0 || lb <= 0 || rb <= 0 || !W || !L || !R || !psi_dev ||
         !out_dev)
         return set_error(DMRG_E_ARG, "dmrg_heff_apply_noalloc: null or empty argument");
+    // ---- validate every table on the host, before any CUDA call -----------------------
+    if (lb > kMaxBond || rb > kMaxBond)
+        return set_error(DMRG_E_ARG, "dmrg_heff_apply_noalloc: MPO bond above %d", kMaxBond);
+    if (ket->nblocks > kMaxOutBlocks)
+        return set_error(DMRG_E_ARG, "dmrg_heff_apply_noalloc: %d ket blocks, at most %d", ket->nblocks,
+                         kMaxOutBlocks);
+    if (!valid_list(*ket, nl, nr))
+        return set_error(DMRG_E_ARG, "dmrg_heff_apply_noalloc: invalid ket block list (sectors outside %dx%d)", nl,
+                         nr);
+    for (int k = 0; k < ket->nblocks; ++k) {
+        const int p = phys[(size_t)ket->left[k] * nr + ket->right[k]];
+        if (p < 0 || p >= d)
+            return set_error(DMRG_E_ARG, "dmrg_heff_apply_noalloc: ket block %d (%d,%d) has physics index %d", k,
+                             ket->left[k], ket->right[k], p);
+    }
+    for (int o = 0; o < lb; ++o)
+        if (!valid_list(L[o], nl, nl))
+            return set_error(DMRG_E_ARG, "dmrg_heff_apply_noalloc: L[%d] has sectors outside %d", o, nl);
+    for (int o = 0; o < rb; ++o)
+        if (!valid_list(R[o], nr, nr))
+            return set_error(DMRG_E_ARG, "dmrg_heff_apply_noalloc: R[%d] has sectors outside %d", o, nr);
+
     cudaStream_t st = (cudaStream_t)stream;
     int dev = 0;
     DMRG_CUDA_TRY(cudaGetDevice(&dev));
@@ -98,8 +157,13 @@ extern "C" int dmrg_heff_apply_noalloc(int nl, int nr, const int* phys, const dm
     unsigned char* scratch = g_scratch_addr[dev];
 
     const View K = view(*ket);
-    if (K.n > kMaxOutBlocks)
-        return set_error(DMRG_E_ARG, "dmrg_heff_apply_noalloc: %d ket blocks, at most %d", K.n, kMaxOutBlocks);
+    int ket_first[2];
+    list_offsets(ket, 1, g_ket_off, ket_first, kMaxOutBlocks);
+    const int64_t Lsize = list_offsets(L, lb, g_L_off, g_L_first, kMaxEnvBlocks);
+    const int64_t Rsize = list_offsets(R, rb, g_R_off, g_R_first, kMaxEnvBlocks);
+    if (Lsize < 0 || Rsize < 0)
+        return set_error(DMRG_E_ARG, "dmrg_heff_apply_noalloc: an environment has more than %d blocks",
+                         kMaxEnvBlocks);
     auto Wat = [&](int o1, int o2, int p1, int p2) { return W[(((size_t)o1 * rb + o2) * d + p1) * d + p2]; };
     auto right_nonzero = [&](int o2, int p2) {
         for (int o1 = 0; o1 < lb; ++o1)
@@ -107,21 +171,6 @@ extern "C" int dmrg_heff_apply_noalloc(int nl, int nr, const int* phys, const dm
                 if (std::fabs(Wat(o1, o2, p1, p2)) > 1e-15) return true;
         return false;
     };
-    // environment base offsets (bond-major packing)
-    int64_t Lbase[512], Rbase[512];
-    if (lb > 512 || rb > 512) return set_error(DMRG_E_ARG, "dmrg_heff_apply_noalloc: MPO bond above 512");
-    {
-        int64_t acc = 0;
-        for (int o = 0; o < lb; ++o) {
-            Lbase[o] = acc;
-            acc += block_off(view(L[o]), L[o].nblocks);
-        }
-        acc = 0;
-        for (int o = 0; o < rb; ++o) {
-            Rbase[o] = acc;
-            acc += block_off(view(R[o]), R[o].nblocks);
-        }
-    }
     // ---- walk the reference loop (real_tensor_contraction.cc:1243-1285) -------------
     // stage A groups/terms go straight to the staging area; stage B terms are
     // collected with their output block and bucketed afterwards.
@@ -163,7 +212,7 @@ extern "C" int dmrg_heff_apply_noalloc(int nl, int nr, const int* phys, const dm
                                 if (tB >= cap_pending)
                                     return set_error(DMRG_E_ARG, "dmrg_heff_apply_noalloc: more than %zu terms",
                                                      cap_pending);
-                                g_pending[tB] = PendingTerm{pos2, GemmTerm{Lbase[o1] + block_off(Lo, q), toff, a_k,
+                                g_pending[tB] = PendingTerm{pos2, GemmTerm{g_L_off[g_L_first[o1] + q], toff, a_k,
                                                                            rc, a_k, 0, w}};
                             }
                             ++tB;
@@ -250,7 +299,7 @@ extern "C" int dmrg_heff_apply_noalloc(int nl, int nr, const int* phys, const dm
                         }
                     }
                     if (used) {
-                        termsA[tA] = GemmTerm{block_off(K, pos), Rbase[o2] + block_off(Ro, i), b_l, rc, b_l, 0, 1.0};
+                        termsA[tA] = GemmTerm{g_ket_off[pos], g_R_off[g_R_first[o2] + i], b_l, rc, b_l, 0, 1.0};
                         ++tA;
                     }
                 }
@@ -277,17 +326,14 @@ extern "C" int dmrg_heff_apply_noalloc(int nl, int nr, const int* phys, const dm
         for (int b = 0; b < K.n; ++b) {
             const int t0 = b == 0 ? 0 : g_count[b - 1], t1 = g_count[b];
             if (t1 == t0) continue;
-            groupsB[gi] = GemmGroup{block_off(K, b), K.cols[b], K.rows[b], K.cols[b], t0, t1, 0};
+            groupsB[gi] = GemmGroup{g_ket_off[b], K.cols[b], K.rows[b], K.cols[b], t0, t1, 0};
             for (int m0 = 0; m0 < K.rows[b]; m0 += kTile)
                 for (int n0 = 0; n0 < K.cols[b]; n0 += kTile) tilesB[k++] = GemmTile{gi, m0, n0, 0};
             ++gi;
         }
     }
     // ---- every operand range inside its buffer (host check, before any device work) ---
-    int64_t Lsize = 0, Rsize = 0;
-    for (int o = 0; o < lb; ++o) Lsize += block_off(view(L[o]), L[o].nblocks);
-    for (int o = 0; o < rb; ++o) Rsize += block_off(view(R[o]), R[o].nblocks);
-    const int64_t psi_size = block_off(K, K.n);
+    const int64_t psi_size = g_ket_off[K.n];
     auto check = [](const GemmTerm* terms, const GemmGroup* groups, size_t ng, int64_t asz, int64_t bsz,
                     int64_t csz) {
         for (size_t g = 0; g < ng; ++g) {
@@ -307,7 +353,7 @@ extern "C" int dmrg_heff_apply_noalloc(int nl, int nr, const int* phys, const dm
         return set_error(DMRG_E_ARG, "dmrg_heff_apply_noalloc: block shapes inconsistent with their buffers");
     // ---- copy the tables into the static device array and launch --------------------
     if (offT) DMRG_CUDA_TRY(cudaMemcpyAsync(scratch, g_staging, offT, cudaMemcpyHostToDevice, st));
-    int64_t psi_dim = block_off(K, K.n);
+    const int64_t psi_dim = g_ket_off[K.n];
     if (!accumulate && psi_dim) DMRG_CUDA_TRY(cudaMemsetAsync(out_dev, 0, (size_t)psi_dim * sizeof(double), st));
     double* T = reinterpret_cast<double*>(scratch + offT);
     DMRG_TRY(launch_gemm_f64_tables(reinterpret_cast<const GemmTerm*>(scratch + offTA),

@@ -138,10 +138,16 @@ int dmrg_heff_profile(dmrg_heff_t h, const double* psi_dev, double* out_dev, dou
  * intermediate in one static device array of 16 MiB per GPU that loads the
  * library (held until exit).  Problems needing more return DMRG_E_ARG with the
  * size required.  All calls share that array: calls that overlap on the GPU
- * race.  The first call on a device looks up the array's device address; make
- * it before any stream capture.  Runs on `stream` (a cudaStream_t; NULL = the
- * legacy default stream) and returns after the work is queued and the
- * schedule copied (it synchronises `stream`). */
+ * race (calls from different host threads are serialised by a lock held until
+ * the call's own stream synchronisation, so only work queued on the GPU by other
+ * means can overlap).  The first call on a device looks up the array's device
+ * address and keeps it for the life of the process; make it before any stream
+ * capture, and do not use the library across a cudaDeviceReset.  Every table is
+ * validated on the host first (sectors in range, each ket block's physics index
+ * in [0, physics_dim)); a malformed one returns DMRG_E_ARG before any CUDA
+ * call.  Runs on `stream` (a cudaStream_t; NULL = the legacy default stream) and
+ * returns after the work is queued and the schedule copied (it synchronises
+ * `stream`). */
 int dmrg_heff_apply_noalloc(int num_left_sector, int num_right_sector, const int* physics_index,
                             const dmrg_blocks_t* ket, int physics_dim, int left_bond, int right_bond,
                             const double* W, const dmrg_blocks_t* L, const dmrg_blocks_t* R,

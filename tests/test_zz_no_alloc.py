@@ -13,9 +13,8 @@ import numpy as np
 import pytest
 
 from dmrgcc_b200 import capi
-from dmrgcc_b200.problem import SiteStep
+from dmrgcc_b200.problem import SiteStep, read_nac
 
-pytestmark = pytest.mark.gpu
 GOLD = os.path.join(os.path.dirname(__file__), "golden")
 TOL = 1e-12
 
@@ -35,6 +34,7 @@ def _blocks(specs):
     return arr
 
 
+@pytest.mark.gpu
 def test_noalloc_matches_allocating_entry_point():
     ctx = capi.Context(0)
     step = SiteStep.from_nac(os.path.join(GOLD, "heff_c158.nac"))
@@ -62,10 +62,17 @@ def test_noalloc_matches_allocating_entry_point():
     assert rc == 0
     ctx.sync()
     assert np.max(np.abs(out.download() - 2 * want)) <= 2 * TOL * scale
+    # the allocating entry point's own output: the reference's heff_out (1e-12)
+    ref_out = np.asarray(read_nac(os.path.join(GOLD, "heff_c158.nac"))["heff_out"])
+    out.upload(np.zeros(step.psi_dim))
+    assert _noalloc(step, Lb, Rb, L, R, psi, out, False, ctx.stream) == 0
+    ctx.sync()
+    assert np.max(np.abs(out.download() - ref_out)) <= TOL * np.max(np.abs(ref_out))
     h.close()
     ctx.close()
 
 
+@pytest.mark.gpu
 def test_noalloc_rejects_problems_beyond_its_scratch():
     ctx = capi.Context(0)
     step = SiteStep.from_nac(os.path.join(GOLD, "heff_struct_cyl8x4_D1024.nac"))
@@ -75,3 +82,40 @@ def test_noalloc_rejects_problems_beyond_its_scratch():
     assert rc == -1  # DMRG_E_ARG, before any device work
     assert b"static scratch holds" in capi.lib().dmrg_last_error()
     ctx.close()
+
+
+class _FakeDev:
+    """A non-null stand-in for a device pointer: the validation under test
+    rejects the call before any pointer is used or any CUDA call is made."""
+    ptr = 0x1000
+
+
+def test_noalloc_rejects_malformed_tables_on_the_host():
+    """A ket block outside the sector range, a physics index outside [0, d) and
+    an environment block outside its sector range each return DMRG_E_ARG before
+    any device work, as dmrg_heff_create does (runs without a GPU)."""
+    step = SiteStep.from_nac(os.path.join(GOLD, "heff_c158.nac"))
+    Lb, Rb = _blocks(step.L), _blocks(step.R)
+    dev = _FakeDev()
+    site = step.site
+    site.phys = site.phys.copy()  # writable copies of the tables to corrupt
+    site.ket = capi.BlockSpec(site.ket.left.copy(), site.ket.right.copy(), site.ket.rows, site.ket.cols)
+    good_phys = site.phys.copy()
+    # a physics index >= d for the first ket block's sector pair
+    k0 = (int(site.ket.left[0]), int(site.ket.right[0]))
+    site.phys[k0[0] * site.nr + k0[1]] = site.d
+    assert _noalloc(step, Lb, Rb, dev, dev, dev, dev, False, None) == -1
+    assert b"physics index" in capi.lib().dmrg_last_error()
+    site.phys[:] = good_phys
+    # a ket block whose left sector is outside [0, nl)
+    saved = int(site.ket.left[0])
+    site.ket.left[0] = site.nl
+    assert _noalloc(step, Lb, Rb, dev, dev, dev, dev, False, None) == -1
+    assert b"ket block list" in capi.lib().dmrg_last_error()
+    site.ket.left[0] = saved
+    # an L block whose ket sector is negative
+    bad = [capi.BlockSpec(s.left.copy(), s.right.copy(), s.rows, s.cols) for s in step.L]
+    o = next(i for i, s in enumerate(bad) if len(s.left))
+    bad[o].right[0] = -1
+    assert _noalloc(step, _blocks(bad), Rb, dev, dev, dev, dev, False, None) == -1
+    assert b"L[" in capi.lib().dmrg_last_error()
