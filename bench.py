@@ -42,6 +42,27 @@ SEED = 2024
 FLUSH_BYTES = 256 << 20  # > 126 MB L2
 
 
+def bench_config(psi_dim: int, gflop: float) -> dict:
+    """The workload description, identical on both arms."""
+    return {"workload": WORKLOAD, "psi_dim": int(psi_dim), "gflop_per_step": round(float(gflop), 6),
+            "structure": os.path.basename(STRUCT), "seed": SEED}
+
+
+def profiled_traffic() -> dict | None:
+    """DRAM bytes per matvec of the FP64 path (stage A + stage B launches), from
+    the committed ncu summary of the same workload (a line
+    `traffic_bytes_per_matvec: <bytes>` in profiles/gemm_f64_heff_cyl8x4_D1024.md)."""
+    p = os.path.join(ROOT, "profiles", "gemm_f64_heff_cyl8x4_D1024.md")
+    try:
+        with open(p) as f:
+            for line in f:
+                if line.startswith("traffic_bytes_per_matvec:"):
+                    return {"bytes": float(line.split(":", 1)[1]), "source": os.path.relpath(p, ROOT)}
+    except OSError:
+        pass
+    return None
+
+
 def peaks() -> dict:
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -121,8 +142,8 @@ def run_reference(args) -> None:
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["mean_s"] * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded splitmix64 values on the "
         "reference's own D=1024 block structure)",
-        "config": {"workload": WORKLOAD, "psi_dim": res["psi_dim"], "gflop_per_step": res["gflop"],
-                   "backend": "reference MultiplyEffectHamilton + OpenBLAS 0.3.15 dgemm"},
+        "config": bench_config(res["psi_dim"], res["gflop"]),
+        "backend": "reference MultiplyEffectHamilton + OpenBLAS 0.3.15 dgemm",
         "cpu_baseline": {"value": tflops, "unit": "TFLOP/s", "cores": res["threads"], "kind": "reference",
                          "sample": f"{args.steps} H_eff*psi calls after {args.warmup} warm-up calls"},
         "e2e": {"value": tflops, "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -193,15 +214,71 @@ def sweep_time(ctx, precision: int = 0, name: str = "fp64") -> dict:
     return out
 
 
+REF_MODEL = os.path.join(ROOT, "oracle", "_ref", "real_spinless_bose_square_model")
+
+
+def first_sweep_input(path: str, out_path: str) -> None:
+    """The input file with its sweep table cut to the first full sweep (two
+    half-sweep rows)."""
+    import re
+
+    with open(path) as f:
+        text = f.read()
+    text = re.sub(r"num_sweep\s*=\s*\d+", "num_sweep = 1", text)
+    head, rest = text.split("sweeps", 1)
+    lines = rest.splitlines()
+    out, rows = [], 0
+    for ln in lines:
+        tok = ln.split()
+        if tok and tok[0].lstrip("-").isdigit():
+            rows += 1
+            if rows > 2:
+                continue
+        out.append(ln)
+    with open(out_path, "w") as f:
+        f.write(head + "sweeps" + "\n".join(out))
+
+
+def reference_sweep_sample(ctx, threads: int) -> dict:
+    """A bounded sample of the whole-run comparison, timed on this host: the
+    first sweep (D=128) of the 8x4 cylinder input, with its initialisation, run
+    by the reference (oracle/_ref, OpenBLAS, `threads` host threads) and by the
+    library (dmrg_run_execute), same input file; wall times and final energies."""
+    import tempfile
+
+    from dmrgcc_b200 import capi
+
+    if not os.path.exists(REF_MODEL):
+        return {"unavailable": f"{REF_MODEL} not built (make -C oracle)"}
+    with tempfile.TemporaryDirectory() as tmp:
+        inp = os.path.join(tmp, "cyl8x4_first_sweep.in")
+        first_sweep_input(CYL_INPUT, inp)
+        env = dict(os.environ, OMP_NUM_THREADS=str(threads), OPENBLAS_NUM_THREADS=str(threads))
+        t0 = time.perf_counter()
+        r = subprocess.run([REF_MODEL, inp], capture_output=True, text=True, env=env, cwd=tmp, timeout=900)
+        ref_wall = time.perf_counter() - t0
+        if r.returncode != 0:
+            return {"unavailable": f"reference run failed: {r.stderr.strip()[-200:]}"}
+        ref_e = [float(ln.split("=")[1]) for ln in r.stdout.splitlines() if "energy =" in ln]
+        run = capi.Run(ctx, inp, verbose=0)
+        t0 = time.perf_counter()
+        run.execute()
+        lib_wall = time.perf_counter() - t0
+        e, _ = run.half_sweeps()
+        run.close()
+    return {"sample": "initialisation + first sweep (D=128) of the 8x4 cylinder input, same input file",
+            "cores": threads, "reference_s": ref_wall, "library_s": lib_wall, "speedup": ref_wall / lib_wall,
+            "reference_energy": ref_e[-1] if ref_e else None, "library_energy": float(e[-1])}
+
+
 def sweep_pair(ctx) -> dict:
     """The whole run in FP64 and with TF32X3 matvecs, back to back: times, the
     split run's speedup per sweep and its final-energy difference per site
-    (32 sites) against the FP64 run."""
+    (32 sites) against the FP64 run; plus a bounded sample of the same input
+    run by the reference on this host."""
     fp64 = sweep_time(ctx)
     split = sweep_time(ctx, 2, "tf32x3")
-    fp64["reference_cpu"] = {"total_s": 557.0, "final_energy": -45.653161401383, "cores": 8,
-                             "note": "the reference built from its sources with OpenBLAS, measured in the build "
-                                     "container (not on the GPU box); 8 threads"}
+    fp64["reference_cpu_sample"] = reference_sweep_sample(ctx, os.cpu_count() or 1)
     fp64["split"] = {"precision": "tf32x3", "total_s": split["total_s"], "per_sweep_s": split["per_sweep_s"],
                      "phase_s": split["phase_s"], "final_energy": split["final_energy"],
                      "speedup_vs_fp64": fp64["total_s"] / split["total_s"],
@@ -258,6 +335,7 @@ def run_b200(args) -> None:
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
+    launches0 = capi.launch_count()
     with ClockSampler(local) as clk:
         for e0, e1 in evs:
             flush.zero()  # evict L2 between timed steps (outside the event pair)
@@ -265,6 +343,7 @@ def run_b200(args) -> None:
             heff.apply(psi, out, accumulate=True)
             e1.record(stream)
         torch.cuda.synchronize()
+    launches = capi.launch_count() - launches0  # this library's kernels in the timed loop
     if dist:
         dist.barrier()
     step_ms = [e0.elapsed_time(e1) for e0, e1 in evs]
@@ -308,26 +387,29 @@ def run_b200(args) -> None:
     e2e_value = world * alg_flops * args.steps / (e2e_ms * 1e-3) * 1e-12
 
     if rank == 0:
+        traffic = profiled_traffic()
         dominant = "stage_b" if ms_b >= ms_a else "stage_a"
         line = {
             "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else args.precision + " (f32 accumulate per term, f64 sums)",
             "data": "synthetic (seeded splitmix64 values on the reference's own D=1024 block structure)",
-            "config": {"workload": WORKLOAD, "precision": args.precision, "psi_dim": step.psi_dim,
-                       "gflop_per_step_algorithmic": alg_flops * 1e-9, "gflop_per_step_executed": exec_flops * 1e-9,
+            "config": bench_config(step.psi_dim, alg_flops * 1e-9),
+            "detail": {"precision": args.precision, "gflop_per_step_executed": exec_flops * 1e-9,
                        "l2": "256 MiB write between timed steps (outside the per-step CUDA-event pair)",
                        "parallelism": f"replicas x{world}"},
-            # per matvec: stage A grouped GEMM, stage B grouped GEMM, stage B split-K reduce
-            # (this structure splits its longest stage-B groups; see the ncu launch list)
-            "gpu_launches": 3 * args.steps,
+            # counted by the library (dmrg_launch_count) around the timed loop: per
+            # matvec the stage A and stage B grouped GEMMs and the stage B split-K reduce
+            "gpu_launches": launches,
             "e2e": {"value": e2e_value, "unit": "TFLOP/s", "h2d_bytes_per_step": step.psi_dim * 8,
                     "d2h_bytes_per_step": step.psi_dim * 8,
                     "note": "dmrg_heff_apply_host: pinned psi in, matvec, result out, sync; environments resident"},
             "roofline": {
                 "bound": "tensor", "kernel": "gemm_f64_kernel (whole matvec: stage A + stage B)",
                 "achieved": alg_flops / (ms_per_step * 1e-3) * 1e-12, "peak": fp64_peak, "unit": "TFLOP/s",
-                "frac": alg_flops / (ms_per_step * 1e-3) * 1e-12 / fp64_peak, "traffic": None,
+                "frac": alg_flops / (ms_per_step * 1e-3) * 1e-12 / fp64_peak,
+                "traffic": traffic["bytes"] if traffic else None,
+                "traffic_source": traffic["source"] if traffic else None,
                 "peak_source": f"measured in this run: DMMA loop {fp64_dmma:.2f}, DFMA loop {fp64_dfma:.2f} TFLOP/s",
                 "stage_ms": {"stage_a": ms_a, "stage_b": ms_b, "dominant": dominant},
             },

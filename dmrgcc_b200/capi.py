@@ -59,11 +59,13 @@ _SIGS = {
     "dmrg_memset": (C.c_int, [_VP, _VP, C.c_int, C.c_size_t]),
     "dmrg_fill_uniform": (C.c_int, [_VP, _VP, C.c_int64, C.c_uint64, C.c_int64]),
     "dmrg_fp64_peak": (C.c_int, [_VP, C.c_int, C.c_int, _D]),
+    "dmrg_launch_count": (C.c_int, [_I64]),
     "dmrg_heff_create": (C.c_int, [_VP, C.c_int, C.c_int, _I, C.POINTER(Blocks), C.c_int, C.c_int, C.c_int, _D,
                                    C.POINTER(Blocks), C.POINTER(Blocks), C.c_int, C.POINTER(_VP)]),
     "dmrg_heff_destroy": (C.c_int, [_VP]),
     "dmrg_heff_set_split_threshold": (C.c_int, [_VP, C.c_int64]),
     "dmrg_heff_split_iters": (C.c_int, [_VP, _I]),
+    "dmrg_heff_set_graph": (C.c_int, [_VP, C.c_int]),
     "dmrg_heff_sizes": (C.c_int, [_VP, _I64, _I64, _I64]),
     "dmrg_heff_flops": (C.c_int, [_VP, _D, _D]),
     "dmrg_heff_set_env": (C.c_int, [_VP, _VP, _VP]),
@@ -127,6 +129,13 @@ def lib() -> C.CDLL:
 def check(rc: int, where: str) -> None:
     if rc != 0:
         raise DmrgError(rc, where)
+
+
+def launch_count() -> int:
+    """Kernels the library has launched in this process (dmrg_launch_count)."""
+    n = C.c_int64(0)
+    check(lib().dmrg_launch_count(C.byref(n)), "dmrg_launch_count")
+    return int(n.value)
 
 
 def _iptr(a: np.ndarray):
@@ -300,6 +309,10 @@ class Heff:
         it = C.c_int(0)
         check(lib().dmrg_heff_split_iters(self.h, C.byref(it)), "dmrg_heff_split_iters")
         return it.value
+
+    def set_graph(self, enable: bool) -> None:
+        """Lanczos loop as one captured CUDA graph (default) or launch by launch."""
+        check(lib().dmrg_heff_set_graph(self.h, int(bool(enable))), "dmrg_heff_set_graph")
 
     def lanczos(self, psi: DeviceArray, niter: int, precision: float = 1e-15,
                 zero_tol: float = 1e-15) -> tuple[float, int]:

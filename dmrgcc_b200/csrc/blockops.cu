@@ -39,7 +39,7 @@ int launch_rect_copies(const std::vector<RectCopy>& tasks, const double* src, in
     DMRG_TRY(scratch.alloc(tasks.size() * sizeof(RectCopy)));
     DMRG_CUDA_TRY(cudaMemcpyAsync(scratch.ptr, tasks.data(), tasks.size() * sizeof(RectCopy), cudaMemcpyHostToDevice,
                                   st));
-    rect_copy_kernel<<<(int)tasks.size(), 256, 0, st>>>(scratch.as<RectCopy>(), src, dst);
+    DMRG_LAUNCH rect_copy_kernel<<<(int)tasks.size(), 256, 0, st>>>(scratch.as<RectCopy>(), src, dst);
     // (a pageable-source cudaMemcpyAsync returns once the source is staged, so the
     // host vector may go away; `scratch` must outlive the launch)
     DMRG_CUDA_TRY(cudaGetLastError());
@@ -49,7 +49,7 @@ int launch_rect_copies(const std::vector<RectCopy>& tasks, const double* src, in
 int launch_scale_by(double* x, int64_t n, const double* s, bool inverse, cudaStream_t st) {
     if (n <= 0) return DMRG_OK;
     const int blocks = (int)std::min<int64_t>((n + 255) / 256, 1184);
-    scale_by_kernel<<<blocks, 256, 0, st>>>(x, n, s, inverse ? 1 : 0);
+    DMRG_LAUNCH scale_by_kernel<<<blocks, 256, 0, st>>>(x, n, s, inverse ? 1 : 0);
     DMRG_CUDA_TRY(cudaGetLastError());
     return DMRG_OK;
 }

@@ -242,7 +242,7 @@ int dmrg_canon_run(dmrg_canon_t c, const double* ket_dev, int max_dim, double ca
         for (const auto& p : svd.probs) wsize += (int64_t)p.rows * p.cols;
         DMRG_CUDA_TRY(cudaMemsetAsync(svd.d_w.ptr, 0, wsize * sizeof(double), st));
         if (!c->copies.empty())
-            gather_kernel<<<(int)c->copies.size(), 256, 0, st>>>(ket_dev, c->d_copies.as<CopyTask>(),
+            DMRG_LAUNCH gather_kernel<<<(int)c->copies.size(), 256, 0, st>>>(ket_dev, c->d_copies.as<CopyTask>(),
                                                                  svd.d_probs.as<SvdProblem>(), svd.d_w.as<double>(),
                                                                  c->side);
         DMRG_CUDA_TRY(cudaGetLastError());
@@ -367,10 +367,10 @@ int dmrg_canon_write(dmrg_canon_t c, const double* ket_dev, double* new_ket_dev,
     (void)nw;
     const double* sig = svd.d_s.as<double>();
     if (n_writes)
-        write_ket_kernel<<<n_writes, 256, 0, st>>>(c->d_writes.as<WriteTask>(), svd.d_probs.as<SvdProblem>(),
+        DMRG_LAUNCH write_ket_kernel<<<n_writes, 256, 0, st>>>(c->d_writes.as<WriteTask>(), svd.d_probs.as<SvdProblem>(),
                                                    svd.d_w.as<double>(), svd.d_q.as<double>(), sig,
                                                    svd.d_perm.as<int>(), svd.d_sign.as<double>(), new_ket_dev, c->side);
-    write_canonical_kernel<<<c->nsec, 256, 0, st>>>(c->d_canons.as<CanonTask>(), svd.d_probs.as<SvdProblem>(),
+    DMRG_LAUNCH write_canonical_kernel<<<c->nsec, 256, 0, st>>>(c->d_canons.as<CanonTask>(), svd.d_probs.as<SvdProblem>(),
                                                     svd.d_w.as<double>(), svd.d_q.as<double>(), sig,
                                                     svd.d_perm.as<int>(), c->d_forced.as<double>(),
                                                     svd.d_sign.as<double>(), canonical_dev, c->side);

@@ -17,6 +17,11 @@ namespace dmrg {
 // Sets the thread's last-error message and returns `code`.
 int set_error(int code, const char* fmt, ...);
 
+// Process-wide count of the kernels this library has launched (read through
+// dmrg_launch_count).  Every launch site is written `DMRG_LAUNCH kernel<<<...>>>(...)`.
+void count_launch();
+#define DMRG_LAUNCH ::dmrg::count_launch(),
+
 #define DMRG_CUDA_TRY(expr)                                                                   \
     do {                                                                                      \
         cudaError_t err_ = (expr);                                                            \

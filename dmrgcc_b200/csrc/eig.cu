@@ -32,10 +32,11 @@ __global__ void __launch_bounds__(kBisectThreads) tridiag_lowest_kernel(const do
                                                                          const double* __restrict__ beta, int m,
                                                                          double* __restrict__ E, int* state,
                                                                          double precision, double zero_tol,
-                                                                         int niter) {
+                                                                         int niter, const int* m_iter) {
     __shared__ double lo, hi, pivmin;
     __shared__ int first;
     if (state[0]) return;  // already converged: later speculative steps are no-ops
+    if (m_iter) m = *m_iter + 1;  // graph-captured loop: the dimension is the device's iteration + 1
     if (threadIdx.x == 0) {
         double l = DBL_MAX, h = -DBL_MAX, bmax = 0.0;
         for (int k = 0; k < m; ++k) {
@@ -340,7 +341,16 @@ __global__ void __launch_bounds__(32) tridiag_vector_kernel(const double* __rest
 
 int launch_tridiag_lowest(const double* alpha, const double* beta, int m, double* E, int* state, double precision,
                           double zero_tol, int niter, cudaStream_t st) {
-    tridiag_lowest_kernel<<<1, kBisectThreads, 0, st>>>(alpha, beta, m, E, state, precision, zero_tol, niter);
+    DMRG_LAUNCH tridiag_lowest_kernel<<<1, kBisectThreads, 0, st>>>(alpha, beta, m, E, state, precision, zero_tol, niter,
+                                                                    nullptr);
+    DMRG_CUDA_TRY(cudaGetLastError());
+    return DMRG_OK;
+}
+
+int launch_tridiag_lowest_it(const double* alpha, const double* beta, const int* iter, double* E, int* state,
+                             double precision, double zero_tol, int niter, cudaStream_t st) {
+    DMRG_LAUNCH tridiag_lowest_kernel<<<1, kBisectThreads, 0, st>>>(alpha, beta, 1, E, state, precision, zero_tol, niter,
+                                                                    iter);
     DMRG_CUDA_TRY(cudaGetLastError());
     return DMRG_OK;
 }
@@ -354,14 +364,14 @@ int launch_sym_jacobi(double* A, int n, double* w, double* Z, double* ws, int* s
     const size_t smem = jacobi_smem(n);
     if (smem > 48 * 1024)
         DMRG_CUDA_TRY(cudaFuncSetAttribute(sym_jacobi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    sym_jacobi_kernel<<<1, kJacobiThreads, smem, st>>>(A, n, w, Z, ws, status);
+    DMRG_LAUNCH sym_jacobi_kernel<<<1, kJacobiThreads, smem, st>>>(A, n, w, Z, ws, status);
     DMRG_CUDA_TRY(cudaGetLastError());
     return DMRG_OK;
 }
 
 int launch_tridiag_ground_vector(const double* alpha, const double* beta, const double* E, const int* m_dev,
                                  double* y, int* status, cudaStream_t st) {
-    tridiag_vector_kernel<<<1, 32, 0, st>>>(alpha, beta, E, m_dev, y, status);
+    DMRG_LAUNCH tridiag_vector_kernel<<<1, 32, 0, st>>>(alpha, beta, E, m_dev, y, status);
     DMRG_CUDA_TRY(cudaGetLastError());
     return DMRG_OK;
 }

@@ -12,6 +12,9 @@ namespace dmrg {
 // E[m-1] receives the eigenvalue.  Skips all work when state[0] is already set.
 int launch_tridiag_lowest(const double* alpha, const double* beta, int m, double* E, int* state, double precision,
                           double zero_tol, int niter, cudaStream_t st);
+// The same with m = *iter + 1 read on the device (graph-captured Lanczos loop).
+int launch_tridiag_lowest_it(const double* alpha, const double* beta, const int* iter, double* E, int* state,
+                             double precision, double zero_tol, int niter, cudaStream_t st);
 
 // Cyclic parallel (round-robin) Jacobi eigensolver for a symmetric n x n matrix A
 // (row-major, global memory, overwritten).  On return w[0..n) holds the

@@ -268,15 +268,15 @@ int launch_gemm_f64(const GemmSchedule& s, const double* A, const double* B, dou
     const auto* tl = s.d_tiles.as<GemmTile>();
     const int acc = accumulate ? 1 : 0;
     double* X = s.aux.as<double>();
-    if (!s.ta && !s.tb) gemm_f64_kernel<false, false><<<n, NT, 0, stream>>>(A, B, C, X, tr, gr, tl, acc);
-    else if (s.ta && !s.tb) gemm_f64_kernel<true, false><<<n, NT, 0, stream>>>(A, B, C, X, tr, gr, tl, acc);
-    else if (!s.ta && s.tb) gemm_f64_kernel<false, true><<<n, NT, 0, stream>>>(A, B, C, X, tr, gr, tl, acc);
-    else gemm_f64_kernel<true, true><<<n, NT, 0, stream>>>(A, B, C, X, tr, gr, tl, acc);
+    if (!s.ta && !s.tb) DMRG_LAUNCH gemm_f64_kernel<false, false><<<n, NT, 0, stream>>>(A, B, C, X, tr, gr, tl, acc);
+    else if (s.ta && !s.tb) DMRG_LAUNCH gemm_f64_kernel<true, false><<<n, NT, 0, stream>>>(A, B, C, X, tr, gr, tl, acc);
+    else if (!s.ta && s.tb) DMRG_LAUNCH gemm_f64_kernel<false, true><<<n, NT, 0, stream>>>(A, B, C, X, tr, gr, tl, acc);
+    else DMRG_LAUNCH gemm_f64_kernel<true, true><<<n, NT, 0, stream>>>(A, B, C, X, tr, gr, tl, acc);
     if (!s.splits.empty()) {
         int64_t biggest = 0;
         for (const GemmSplit& sp : s.splits) biggest = std::max<int64_t>(biggest, (int64_t)sp.m * sp.n);
         const int gx = (int)std::min<int64_t>((biggest + 255) / 256, 64);
-        split_reduce_kernel<<<dim3(gx, (unsigned)s.splits.size()), 256, 0, stream>>>(C, X, s.d_splits.as<GemmSplit>(),
+        DMRG_LAUNCH split_reduce_kernel<<<dim3(gx, (unsigned)s.splits.size()), 256, 0, stream>>>(C, X, s.d_splits.as<GemmSplit>(),
                                                                                      acc);
     }
     DMRG_CUDA_TRY(cudaGetLastError());
@@ -290,10 +290,10 @@ int launch_gemm_f64_tables(const GemmTerm* terms, const GemmGroup* groups, const
     // (no split-K groups: every group writes C directly).
     if (ntiles <= 0) return DMRG_OK;
     const int acc = accumulate ? 1 : 0;
-    if (!ta && !tb) gemm_f64_kernel<false, false><<<ntiles, NT, 0, stream>>>(A, B, C, nullptr, terms, groups, tiles, acc);
-    else if (ta && !tb) gemm_f64_kernel<true, false><<<ntiles, NT, 0, stream>>>(A, B, C, nullptr, terms, groups, tiles, acc);
-    else if (!ta && tb) gemm_f64_kernel<false, true><<<ntiles, NT, 0, stream>>>(A, B, C, nullptr, terms, groups, tiles, acc);
-    else gemm_f64_kernel<true, true><<<ntiles, NT, 0, stream>>>(A, B, C, nullptr, terms, groups, tiles, acc);
+    if (!ta && !tb) DMRG_LAUNCH gemm_f64_kernel<false, false><<<ntiles, NT, 0, stream>>>(A, B, C, nullptr, terms, groups, tiles, acc);
+    else if (ta && !tb) DMRG_LAUNCH gemm_f64_kernel<true, false><<<ntiles, NT, 0, stream>>>(A, B, C, nullptr, terms, groups, tiles, acc);
+    else if (!ta && tb) DMRG_LAUNCH gemm_f64_kernel<false, true><<<ntiles, NT, 0, stream>>>(A, B, C, nullptr, terms, groups, tiles, acc);
+    else DMRG_LAUNCH gemm_f64_kernel<true, true><<<ntiles, NT, 0, stream>>>(A, B, C, nullptr, terms, groups, tiles, acc);
     DMRG_CUDA_TRY(cudaGetLastError());
     return DMRG_OK;
 }

@@ -564,7 +564,7 @@ int PackSchedule::finalize(cudaStream_t stream) {
 
 int launch_pack(const PackSchedule& p, const double* src, unsigned char* dst, cudaStream_t stream) {
     if (p.images.empty()) return DMRG_OK;
-    pack_kernel<<<(int)p.images.size(), 128, 0, stream>>>(p.d_jobs.as<PackJob>(), p.d_images.as<PackImage>(), src,
+    DMRG_LAUNCH pack_kernel<<<(int)p.images.size(), 128, 0, stream>>>(p.d_jobs.as<PackJob>(), p.d_images.as<PackImage>(), src,
                                                           dst);
     DMRG_CUDA_TRY(cudaGetLastError());
     return DMRG_OK;
@@ -688,7 +688,7 @@ int launch_fmt(const PackedSchedule& s, const unsigned char* a_imgs, const unsig
             cudaFuncSetAttribute(gemm_split_kernel<FMT>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
         attr = true;
     }
-    gemm_split_kernel<FMT><<<grid, NT, SMEM_BYTES, stream>>>(
+    DMRG_LAUNCH gemm_split_kernel<FMT><<<grid, NT, SMEM_BYTES, stream>>>(
         a_imgs, b_imgs, C, s.aux.as<double>(), t_out, s.d_terms.as<PackedTerm>(), s.d_groups.as<PackedGroup>(),
         s.d_tiles.as<PackedTile>(), s.d_cta_first.as<int>(), accumulate ? 1 : 0, s.out_mode, status);
     return DMRG_OK;
@@ -708,7 +708,7 @@ int launch_gemm_split(const PackedSchedule& s, const unsigned char* a_imgs, cons
         int64_t biggest = 0;
         for (const GemmSplit& sp : s.splits) biggest = std::max<int64_t>(biggest, (int64_t)sp.m * sp.n);
         const int gx = (int)std::min<int64_t>((biggest + 255) / 256, 64);
-        split_reduce_tf32_kernel<<<dim3(gx, (unsigned)s.splits.size()), 256, 0, stream>>>(
+        DMRG_LAUNCH split_reduce_tf32_kernel<<<dim3(gx, (unsigned)s.splits.size()), 256, 0, stream>>>(
             C, s.aux.as<double>(), s.d_splits.as<GemmSplit>(), accumulate ? 1 : 0);
     }
     DMRG_CUDA_TRY(cudaGetLastError());

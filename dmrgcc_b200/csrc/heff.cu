@@ -12,6 +12,7 @@
 //   stage B: one group per output block (i, j) holding all of its
 //            (W, L block, T) terms, summed in registers by the tile owner.
 #include <algorithm>
+#include <cstdlib>
 #include <map>
 
 #include "heff.cuh"
@@ -238,6 +239,7 @@ int dmrg_heff_create(dmrg_ctx_t ctx, int nl, int nr, const int* phys, const dmrg
     auto* h = new dmrg_heff_s();
     h->ctx = ctx;
     h->precision = precision;
+    if (const char* g = std::getenv("DMRG_LANCZOS_GRAPH")) h->use_graph = std::atoi(g) != 0;  // A/B switch
     int rc = build_site_desc(h->site, nl, nr, phys, ket, d, lb, rb, W);
     if (rc == DMRG_OK && !h->L.assign(L, lb)) rc = set_error(DMRG_E_ARG, "invalid L block lists");
     if (rc == DMRG_OK && !h->R.assign(R, rb)) rc = set_error(DMRG_E_ARG, "invalid R block lists");

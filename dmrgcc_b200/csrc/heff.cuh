@@ -13,6 +13,7 @@ struct dmrg_heff_s {
     dmrg_ctx_t ctx = nullptr;
     int precision = DMRG_PREC_FP64;
     int64_t split_min_dim = 200000;  // psi_dim from which a split operator's Lanczos starts with a split phase
+    bool use_graph = true;            // Lanczos loop as one captured CUDA graph (dmrg_heff_set_graph)
     dmrg::SiteDesc site;
     dmrg::EnvDesc L, R;
     dmrg::GemmSchedule sa, sb;    // A: psi x R -> T ; B: L x T -> out (FP64 tiles)

@@ -29,10 +29,22 @@ namespace dmrg {
 struct LanczosWork {
     int niter = 0;
     int64_t n = 0;
-    DeviceBuffer V, h, scal, state, jac, y, dense;
+    DeviceBuffer V, h, scal, state, jac, y, dense, x;
     ReduceScratch rs;
     int* h_state = nullptr;  // the context's pinned words: [done, dim, ...]
     int split_iters = 0;     // Krylov dimension of the last split-precision phase
+    // the captured Krylov loop, one per matvec precision (0: FP64, 1: split),
+    // with the launch constants it was captured for
+    struct Graph {
+        cudaGraphExec_t exec = nullptr;
+        int niter = 0;
+        double precision = 0, zero_tol = 0;
+        cudaStream_t stream = nullptr;
+    } graph[2];
+    ~LanczosWork() {
+        for (Graph& g : graph)
+            if (g.exec) cudaGraphExecDestroy(g.exec);
+    }
 };
 
 }  // namespace dmrg
@@ -46,6 +58,15 @@ namespace {
 // Convergence of the split-precision phase: |E_i - E_{i-1}| below this (the
 // matvec's relative error is ~1e-6, the Ritz value settles well before).
 constexpr double kSplitPrecision = 1e-9;
+
+// End of one captured Lanczos iteration: advance the device's iteration
+// counter and keep the loop going while the run has not converged.  The loop is
+// bounded: the tridiagonal step marks the run converged at dimension niter.
+__global__ void lanczos_advance_kernel(int* state, int niter, cudaGraphConditionalHandle loop) {
+    const int it = state[kIterSlot] + 1;
+    state[kIterSlot] = it;
+    cudaGraphSetConditional(loop, (state[0] == 0 && it < niter) ? 1u : 0u);
+}
 
 __global__ void unit_vector_kernel(double* x, int64_t n, int64_t c) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
@@ -79,6 +100,7 @@ int ensure_work(dmrg_heff_s& h, int niter) {
         w.niter = niter;
         w.n = n;
     }
+    DMRG_TRY(w.x.alloc((size_t)std::max<int64_t>(n, 1) * sizeof(double)));
     DMRG_TRY(w.state.alloc(16 * sizeof(int)));
     DMRG_TRY(w.rs.alloc(std::max(2 * h.ctx->num_sms, 64), std::max(niter, 1)));
     w.h_state = h.ctx->h_pinned;
@@ -96,19 +118,103 @@ int run_exact(dmrg_heff_s& h, double* psi, double* energy) {
     double* ev = Z + (size_t)n * n;
     double* e = w.h.as<double>();
     for (int c = 0; c < n; ++c) {
-        unit_vector_kernel<<<1, 128, 0, st>>>(e, n, c);
+        DMRG_LAUNCH unit_vector_kernel<<<1, 128, 0, st>>>(e, n, c);
         DMRG_TRY(heff_apply_fp64(h, e, cols + (size_t)c * n, false));  // the dense branch stays FP64
     }
-    symmetrize_upper_kernel<<<std::max(1, (n * n + 255) / 256), 256, 0, st>>>(cols, A, n);
+    DMRG_LAUNCH symmetrize_upper_kernel<<<std::max(1, (n * n + 255) / 256), 256, 0, st>>>(cols, A, n);
     DMRG_CUDA_TRY(cudaMemsetAsync(w.state.ptr, 0, 16 * sizeof(int), st));
     DMRG_TRY(launch_sym_jacobi(A, n, ev, Z, w.jac.as<double>(), w.state.as<int>() + 2, st));
-    column_copy_kernel<<<1, 128, 0, st>>>(Z, n, psi);
+    DMRG_LAUNCH column_copy_kernel<<<1, 128, 0, st>>>(Z, n, psi);
     double e0 = 0.0;
     DMRG_CUDA_TRY(cudaMemcpyAsync(&e0, ev, sizeof(double), cudaMemcpyDeviceToHost, st));
     DMRG_CUDA_TRY(cudaMemcpyAsync(w.h_state, w.state.ptr, 4 * sizeof(int), cudaMemcpyDeviceToHost, st));
     DMRG_CUDA_TRY(cudaStreamSynchronize(st));
     if (w.h_state[2] != 0) return set_error(DMRG_E_NUMERIC, "Jacobi eigensolver did not converge (n=%d)", n);
     *energy = e0;
+    return DMRG_OK;
+}
+
+// One Lanczos iteration i (i read on the device) for the captured loop:
+// h += H x;  alpha_i = <x|h>;  h -= alpha_i x;  beta_i = ||h||;  tridiagonal
+// step and convergence test;  unless converged: V_{i+1} = h / beta_i, h =
+// -beta_i x, reorthogonalised and normalised, x = V_{i+1};  i += 1.  x holds
+// V_i (the matvec input) so that the schedules' fixed operand pointers serve
+// every iteration.
+int capture_iteration(dmrg_heff_s& h, int niter, double precision, double zero_tol, bool split,
+                      cudaGraphConditionalHandle loop, cudaStream_t st) {
+    LanczosWork& w = *h.lw;
+    const int64_t n = h.site.ket.size;
+    const int blocks = std::min<int64_t>((n + kVecThreads - 1) / kVecThreads, 2 * h.ctx->num_sms);
+    double* V = w.V.as<double>();
+    double* hv = w.h.as<double>();
+    double* x = w.x.as<double>();
+    double* alpha = w.scal.as<double>();
+    double* beta = alpha + niter;
+    double* E = beta + niter;
+    double* c = E + niter;
+    double* tmp = c + niter;
+    int* state = w.state.as<int>();
+    DMRG_TRY(split ? heff_apply_internal(h, x, hv, true) : heff_apply_fp64(h, x, hv, true));
+    DMRG_TRY(vec_dot_it(x, hv, n, alpha, state, w.rs, blocks, st));
+    DMRG_TRY(vec_axpy_norm_it(alpha, x, hv, n, beta, state, w.rs, blocks, st));
+    DMRG_TRY(launch_tridiag_lowest_it(alpha, beta, state + kIterSlot, E, state, precision, zero_tol, niter, st));
+    DMRG_TRY(vec_lanczos_step_it(beta, x, hv, V, n, niter, c, tmp, x, state, w.rs, blocks, st));
+    DMRG_LAUNCH lanczos_advance_kernel<<<1, 1, 0, st>>>(state, niter, loop);
+    DMRG_CUDA_TRY(cudaGetLastError());
+    return DMRG_OK;
+}
+
+// Captures the Krylov loop of one run as a CUDA graph: a conditional WHILE node
+// whose body is one iteration (capture_iteration), so a whole Lanczos run is
+// one graph launch with no host round trip; the graph is kept and relaunched
+// while the operator, niter and the stopping constants stay the same.
+int build_loop_graph(dmrg_heff_s& h, int niter, double precision, double zero_tol, bool split) {
+    LanczosWork& w = *h.lw;
+    LanczosWork::Graph& g = w.graph[split ? 1 : 0];
+    cudaStream_t st = h.ctx->stream;
+    if (g.exec && g.niter == niter && g.precision == precision && g.zero_tol == zero_tol && g.stream == st)
+        return DMRG_OK;
+    if (g.exec) {
+        cudaGraphExecDestroy(g.exec);
+        g.exec = nullptr;
+    }
+    cudaGraph_t graph = nullptr;
+    DMRG_CUDA_TRY(cudaGraphCreate(&graph, 0));
+    int rc = DMRG_OK;
+    cudaGraphConditionalHandle loop{};
+    cudaError_t e = cudaGraphConditionalHandleCreate(&loop, graph, 1, cudaGraphCondAssignDefault);
+    cudaGraphNodeParams cp{};
+    cudaGraphNode_t node = nullptr;
+    if (e == cudaSuccess) {
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = loop;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        e = cudaGraphAddNode(&node, graph, nullptr, 0, &cp);
+    }
+    if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(st, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                                            cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) {
+        cudaGraphDestroy(graph);
+        return set_error(DMRG_E_CUDA, "Lanczos loop graph: %s", cudaGetErrorString(e));
+    }
+    rc = capture_iteration(h, niter, precision, zero_tol, split, loop, st);
+    cudaGraph_t body = nullptr;
+    e = cudaStreamEndCapture(st, &body);  // always ends the capture, also after a failed step
+    if (rc == DMRG_OK && e != cudaSuccess) rc = set_error(DMRG_E_CUDA, "Lanczos loop capture: %s", cudaGetErrorString(e));
+    if (rc == DMRG_OK) {
+        e = cudaGraphInstantiate(&g.exec, graph, 0);
+        if (e != cudaSuccess) {
+            g.exec = nullptr;
+            rc = set_error(DMRG_E_CUDA, "Lanczos loop graph instantiation: %s", cudaGetErrorString(e));
+        }
+    }
+    cudaGraphDestroy(graph);
+    if (rc != DMRG_OK) return rc;
+    g.niter = niter;
+    g.precision = precision;
+    g.zero_tol = zero_tol;
+    g.stream = st;
     return DMRG_OK;
 }
 
@@ -132,6 +238,16 @@ int krylov(dmrg_heff_s& h, double* psi, int niter, double precision, double zero
     DMRG_CUDA_TRY(cudaMemcpyAsync(V, psi, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
     DMRG_CUDA_TRY(cudaMemsetAsync(hv, 0, n * sizeof(double), st));
     DMRG_CUDA_TRY(cudaMemsetAsync(state, 0, 16 * sizeof(int), st));
+    int dim = 0;
+    if (h.use_graph) {
+        // the whole loop as one graph launch; the host reads the result once
+        DMRG_TRY(build_loop_graph(h, niter, precision, zero_tol, split));
+        DMRG_CUDA_TRY(cudaMemcpyAsync(w.x.ptr, psi, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        DMRG_CUDA_TRY(cudaGraphLaunch(w.graph[split ? 1 : 0].exec, st));
+        DMRG_CUDA_TRY(cudaMemcpyAsync(w.h_state, state, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
+        DMRG_CUDA_TRY(cudaStreamSynchronize(st));
+        dim = w.h_state[0] ? w.h_state[1] : 0;
+    }
     // The convergence test runs on the device (tridiag_lowest_kernel records the
     // first dimension that meets it and ignores later calls).  The host reads it
     // once per `chunk` iterations instead of after each one, so the GPU is not
@@ -139,8 +255,7 @@ int krylov(dmrg_heff_s& h, double* psi, int niter, double precision, double zero
     // convergence write vectors and coefficients beyond `dim`, which nothing
     // reads.  Cheap matvecs get longer chunks.
     const int chunk = (int)std::min<int64_t>(8, std::max<int64_t>(2, 2000000 / (n + 100000)));
-    int dim = 0;
-    for (int i = 0; i < niter; ++i) {
+    for (int i = 0; i < niter && !h.use_graph; ++i) {
         double* vi = V + (int64_t)i * n;
         DMRG_TRY(split ? heff_apply_internal(h, vi, hv, true) : heff_apply_fp64(h, vi, hv, true));
         DMRG_TRY(vec_dot(vi, hv, n, alpha + i, w.rs, blocks, st));
@@ -178,6 +293,12 @@ int krylov(dmrg_heff_s& h, double* psi, int niter, double precision, double zero
 }
 
 }  // namespace
+
+extern "C" int dmrg_heff_set_graph(dmrg_heff_t h, int enable) {
+    if (!h) return set_error(DMRG_E_ARG, "null operator");
+    h->use_graph = enable != 0;
+    return DMRG_OK;
+}
 
 extern "C" int dmrg_heff_set_split_threshold(dmrg_heff_t h, int64_t min_psi_dim) {
     if (!h || min_psi_dim < 0) return set_error(DMRG_E_ARG, "invalid split threshold");

@@ -56,14 +56,14 @@ extern "C" int dmrg_fp64_peak(dmrg_ctx_t ctx, int mode, int iters, double* tflop
     const int blocks = ctx->num_sms * 8;
     double flops;
     // warm-up
-    if (mode == 0) dmma_loop<<<blocks, 128, 0, ctx->stream>>>(sink.as<double>(), iters / 10 + 1);
-    else dfma_loop<<<blocks, 256, 0, ctx->stream>>>(sink.as<double>(), iters / 10 + 1);
+    if (mode == 0) DMRG_LAUNCH dmma_loop<<<blocks, 128, 0, ctx->stream>>>(sink.as<double>(), iters / 10 + 1);
+    else DMRG_LAUNCH dfma_loop<<<blocks, 256, 0, ctx->stream>>>(sink.as<double>(), iters / 10 + 1);
     cudaEventRecord(e0, ctx->stream);
     if (mode == 0) {
-        dmma_loop<<<blocks, 128, 0, ctx->stream>>>(sink.as<double>(), iters);
+        DMRG_LAUNCH dmma_loop<<<blocks, 128, 0, ctx->stream>>>(sink.as<double>(), iters);
         flops = (double)blocks * 4 /*warps*/ * iters * 8 * (8.0 * 8 * 4 * 2);
     } else {
-        dfma_loop<<<blocks, 256, 0, ctx->stream>>>(sink.as<double>(), iters);
+        DMRG_LAUNCH dfma_loop<<<blocks, 256, 0, ctx->stream>>>(sink.as<double>(), iters);
         flops = (double)blocks * 256 * iters * 8 * 2.0;
     }
     cudaEventRecord(e1, ctx->stream);

@@ -688,8 +688,8 @@ int BatchedSvd::run(cudaStream_t st, int* sweeps_out) {
         return DMRG_OK;
     }
     const int np = (int)probs.size();
-    init_identity_kernel<<<np, 256, 0, st>>>(d_probs.as<SvdProblem>(), d_q.as<double>());
-    fro2_kernel<<<np, 256, 0, st>>>(d_probs.as<SvdProblem>(), d_w.as<double>(), d_fro2.as<double>());
+    DMRG_LAUNCH init_identity_kernel<<<np, 256, 0, st>>>(d_probs.as<SvdProblem>(), d_q.as<double>());
+    DMRG_LAUNCH fro2_kernel<<<np, 256, 0, st>>>(d_probs.as<SvdProblem>(), d_w.as<double>(), d_fro2.as<double>());
     std::vector<unsigned long long> conv(np);
     static const bool debug = std::getenv("DMRG_SVD_DEBUG") != nullptr;  // per-sweep convergence to stderr
     int max_cols = 0;
@@ -703,21 +703,21 @@ int BatchedSvd::run(cudaStream_t st, int* sweeps_out) {
         // the sweep visits columns in descending norm order: blocks hold columns of
         // similar size, which keeps the many tiny singular values of a noise-expanded
         // tensor from converging only linearly
-        colnorm_kernel<<<colgrid, 256, 0, st>>>(d_probs.as<SvdProblem>(), d_w.as<double>(), d_norm.as<double>());
-        rank_kernel<<<np, 256, 0, st>>>(d_probs.as<SvdProblem>(), d_norm.as<double>(), d_colmap.as<int>(), nullptr);
+        DMRG_LAUNCH colnorm_kernel<<<colgrid, 256, 0, st>>>(d_probs.as<SvdProblem>(), d_w.as<double>(), d_norm.as<double>());
+        DMRG_LAUNCH rank_kernel<<<np, 256, 0, st>>>(d_probs.as<SvdProblem>(), d_norm.as<double>(), d_colmap.as<int>(), nullptr);
         for (int r = 0; r < max_rounds; ++r) {
             const int nt = round_first[r + 1] - round_first[r];
             const int ng = round_gram_first[r + 1] - round_gram_first[r];
             const int nr = round_rot_first[r + 1] - round_rot_first[r];
             if (nt == 0) continue;
-            gram_kernel<<<ng, 128, 0, st>>>(d_probs.as<SvdProblem>(), d_tasks.as<SvdTask>(),
+            DMRG_LAUNCH gram_kernel<<<ng, 128, 0, st>>>(d_probs.as<SvdProblem>(), d_tasks.as<SvdTask>(),
                                             d_gram_items.as<SvdItem>() + round_gram_first[r], r,
                                             d_colmap.as<int>(), d_w.as<double>(), d_gpart.as<double>());
-            solve_kernel<<<nt, kThreads, sizeof(SvdSmem), st>>>(
+            DMRG_LAUNCH solve_kernel<<<nt, kThreads, sizeof(SvdSmem), st>>>(
                 d_probs.as<SvdProblem>(), d_tasks.as<SvdTask>(), round_first[r], d_gpart.as<double>(),
                 d_fro2.as<double>(), d_rot.as<double>(), d_skip.as<int>(), d_conv.as<unsigned long long>(),
                 d_sched.as<uint16_t>(), kInnerSweeps);
-            rotate_kernel<<<nr, 128, kRotSmem, st>>>(d_probs.as<SvdProblem>(), d_tasks.as<SvdTask>(),
+            DMRG_LAUNCH rotate_kernel<<<nr, 128, kRotSmem, st>>>(d_probs.as<SvdProblem>(), d_tasks.as<SvdTask>(),
                                                      d_rot_items.as<SvdItem>() + round_rot_first[r], r,
                                                      round_first[r], d_rot.as<double>(), d_skip.as<int>(),
                                                      d_colmap.as<int>(), d_w.as<double>(), d_q.as<double>());
@@ -767,9 +767,9 @@ int BatchedSvd::run(cudaStream_t st, int* sweeps_out) {
         return set_error(DMRG_E_NUMERIC, "Jacobi SVD did not converge in %d sweeps (sector %d x %d: off-diagonal %.3e)",
                          kMaxSweeps, probs[worst_at].m, probs[worst_at].n, worst_left);
     // singular values = final column norms, sorted
-    colnorm_kernel<<<colgrid, 256, 0, st>>>(d_probs.as<SvdProblem>(), d_w.as<double>(), d_norm.as<double>());
-    rank_kernel<<<np, 256, 0, st>>>(d_probs.as<SvdProblem>(), d_norm.as<double>(), d_perm.as<int>(), d_s.as<double>());
-    sign_kernel<<<colgrid, 256, 0, st>>>(d_probs.as<SvdProblem>(), d_w.as<double>(),
+    DMRG_LAUNCH colnorm_kernel<<<colgrid, 256, 0, st>>>(d_probs.as<SvdProblem>(), d_w.as<double>(), d_norm.as<double>());
+    DMRG_LAUNCH rank_kernel<<<np, 256, 0, st>>>(d_probs.as<SvdProblem>(), d_norm.as<double>(), d_perm.as<int>(), d_s.as<double>());
+    DMRG_LAUNCH sign_kernel<<<colgrid, 256, 0, st>>>(d_probs.as<SvdProblem>(), d_w.as<double>(),
                                                                d_q.as<double>(), d_perm.as<int>(), d_sign.as<double>());
     DMRG_CUDA_TRY(cudaGetLastError());
     if (sweeps_out) *sweeps_out = sweep + 1;

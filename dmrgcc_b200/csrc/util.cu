@@ -1,7 +1,13 @@
 // Small device utilities exposed through the C ABI.
+#include <atomic>
+
 #include "common.cuh"
 
 namespace dmrg {
+
+static std::atomic<long long> g_launches{0};
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
 namespace {
 
 // splitmix64 (Steele, Lea, Flood 2014) mapped to [-1, 1): element i of the stream
@@ -26,7 +32,13 @@ extern "C" int dmrg_fill_uniform(dmrg_ctx_t ctx, double* dev, int64_t n, uint64_
     if (!ctx || (!dev && n > 0) || n < 0) return set_error(DMRG_E_ARG, "invalid fill arguments");
     if (n == 0) return DMRG_OK;
     int blocks = (int)std::min<int64_t>((n + 255) / 256, (int64_t)ctx->num_sms * 8);
-    fill_splitmix_kernel<<<blocks, 256, 0, ctx->stream>>>(dev, n, seed, start);
+    DMRG_LAUNCH fill_splitmix_kernel<<<blocks, 256, 0, ctx->stream>>>(dev, n, seed, start);
     DMRG_CUDA_TRY(cudaGetLastError());
+    return DMRG_OK;
+}
+
+extern "C" int dmrg_launch_count(int64_t* count) {
+    if (!count) return set_error(DMRG_E_ARG, "null argument");
+    *count = (int64_t)g_launches.load(std::memory_order_relaxed);
     return DMRG_OK;
 }

@@ -42,4 +42,22 @@ int vec_normalize(double* x, int64_t n, double* out, ReduceScratch& rs, int bloc
 constexpr int kMaxVec = 512;
 constexpr int kRowTickets = 64;  // ticket slots before the per-row ones of vec_multidot
 
+// ---- device-indexed Lanczos steps (for the graph-captured loop) -------------
+// The iteration i is read from state[kIterSlot]; state[0] != 0 (converged)
+// turns every call into a no-op.  The Krylov basis V is niter x n (ldv = n).
+constexpr int kIterSlot = 4;
+// out_base[i] = <x, y>
+int vec_dot_it(const double* x, const double* y, int64_t n, double* out_base, const int* state, ReduceScratch& rs,
+               int blocks, cudaStream_t st);
+// y -= alpha_base[i] * x ; out_base[i] = ||y||
+int vec_axpy_norm_it(const double* alpha_base, const double* x, double* y, int64_t n, double* out_base,
+                     const int* state, ReduceScratch& rs, int blocks, cudaStream_t st);
+// unless i + 1 == niter: V_{i+1} = h / beta_base[i], h = -beta_base[i] x; V_{i+1}
+// orthogonalised against V_0..V_i by classical Gram-Schmidt twice (c: niter
+// scratch doubles) and normalised (norm into *tmp); x_next = V_{i+1}.  The same
+// arithmetic as vec_lanczos_shift + 2 x (vec_multidot, vec_combine[_normalize]).
+int vec_lanczos_step_it(const double* beta_base, const double* x, double* h, double* V, int64_t n, int niter,
+                        double* c, double* tmp, double* x_next, const int* state, ReduceScratch& rs, int blocks,
+                        cudaStream_t st);
+
 }  // namespace dmrg

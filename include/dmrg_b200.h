@@ -91,6 +91,9 @@ int dmrg_fill_uniform(dmrg_ctx_t ctx, double* dev, int64_t n, uint64_t seed, int
  * (mode 0) or DFMA (mode 1) instructions on all SMs: the roofline denominator
  * of the FP64 block GEMMs.  No reference counterpart. */
 int dmrg_fp64_peak(dmrg_ctx_t ctx, int mode, int iters, double* tflops);
+/* Number of kernels this library has launched in this process, on any context
+ * (for launch accounting in benchmarks).  No reference counterpart. */
+int dmrg_launch_count(int64_t* count);
 
 /* ---- a1: H_eff * psi --------------------------------------------------------
  * Replaces RealTensorContraction::MultiplyEffectHamilton(RealTensorLattice*,
@@ -174,6 +177,17 @@ int dmrg_heff_set_split_threshold(dmrg_heff_t h, int64_t min_psi_dim);
 /* Krylov dimension of the split phase of the last dmrg_lanczos call (0 when it
  * ran FP64 only). */
 int dmrg_heff_split_iters(dmrg_heff_t h, int* iters);
+/* enable != 0 (the default; environment variable DMRG_LANCZOS_GRAPH=0 changes
+ * it for new operators): dmrg_lanczos runs its Krylov loop as one CUDA graph
+ * launch, a conditional WHILE node whose body is one iteration (matvec, the
+ * recurrence, the tridiagonal step and convergence test, the
+ * reorthogonalisation) with the iteration index kept on the device, captured on
+ * first use and relaunched while niter and the stopping constants stay the
+ * same; the host reads the result once per run.  0: one launch per kernel and
+ * a host read of the convergence flag every few iterations.  Both give
+ * bit-identical results.  Replaces the iteration loop of
+ * RealTensorLanczos::LanczosMethod (real_tensor_lanczos.cc:57-185). */
+int dmrg_heff_set_graph(dmrg_heff_t h, int enable);
 
 /* ---- a2/a3: environment update ---------------------------------------------
  * side 0 replaces RealTensorContraction::LeftComputeTensorContraction

@@ -20,6 +20,7 @@
 // the reference's reader (see __wrap__ZN15RealTensorSpace15ReadTensorSpaceEPKc).
 //   PROBE_GAUGE=1          fix the free signs of LAPACK's singular vectors and
 //                          eigenvectors by the library's convention (see below)
+//   PROBE_GAUGE_SEED=s     flip each of those signs at random instead (seed s)
 // Always writes PROBE_OUT/steps.txt: one line per Lanczos call with the site,
 // iteration cap, psi_dim and the energy the reference returned.
 #include "probe_common.h"
@@ -65,6 +66,18 @@ static FILE* g_trace = nullptr;
 // the two implementations follow one trajectory through the noise-driven
 // subspace expansion (whose random matrices act in the gauge-dependent basis).
 static bool g_gauge = false;
+// PROBE_GAUGE_SEED=s (s != 0): instead, every singular pair and eigenvector
+// that LAPACK returns has its sign flipped with probability 1/2, from a private
+// splitmix64 stream seeded with s (glibc rand() is left untouched).  Each seed
+// is another equally valid run of the reference; the spread of their final
+// energies is the reference's own gauge spread.
+static unsigned long long g_gauge_seed = 0;
+static bool gauge_coin() {
+    unsigned long long z = (g_gauge_seed += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return ((z ^ (z >> 31)) >> 63) != 0;
+}
 static double sign_of_column(const double* a, long n, long stride) {
     double m = 0.0;
     for (long i = 0; i < n; ++i) m = std::fabs(a[i * stride]) > m ? std::fabs(a[i * stride]) : m;
@@ -82,7 +95,7 @@ extern "C" lapack_int __wrap_LAPACKE_dgesvd(int layout, char jobu, char jobvt, l
     if (g_gauge && info == 0 && layout == LAPACK_ROW_MAJOR && jobu == 'S' && jobvt == 'S') {
         const lapack_int k = m < n ? m : n;  // (the reference's headers define min/max as macros)
         for (lapack_int c = 0; c < k; ++c)
-            if (sign_of_column(u + c, m, ldu) < 0.0) {
+            if (g_gauge_seed ? gauge_coin() : sign_of_column(u + c, m, ldu) < 0.0) {
                 for (lapack_int i = 0; i < m; ++i) u[(long)i * ldu + c] = -u[(long)i * ldu + c];
                 for (lapack_int j = 0; j < n; ++j) vt[(long)c * ldvt + j] = -vt[(long)c * ldvt + j];
             }
@@ -95,7 +108,7 @@ extern "C" lapack_int __wrap_LAPACKE_dsyevd(int layout, char jobz, char uplo, la
     const lapack_int info = __real_LAPACKE_dsyevd(layout, jobz, uplo, n, a, lda, w);
     if (g_gauge && info == 0 && layout == LAPACK_ROW_MAJOR && jobz == 'V')
         for (lapack_int c = 0; c < n; ++c)
-            if (sign_of_column(a + c, n, lda) < 0.0)
+            if (g_gauge_seed ? gauge_coin() : sign_of_column(a + c, n, lda) < 0.0)
                 for (lapack_int i = 0; i < n; ++i) a[(long)i * lda + c] = -a[(long)i * lda + c];
     return info;
 }
@@ -468,6 +481,10 @@ int main(int argc, char* argv[]) {
     g_struct_only = std::getenv("PROBE_STRUCT_ONLY") != nullptr;
     if (const char* s = std::getenv("PROBE_STOP")) g_stop = std::atoi(s);
     g_gauge = std::getenv("PROBE_GAUGE") != nullptr && std::atoi(std::getenv("PROBE_GAUGE")) != 0;
+    if (const char* gs = std::getenv("PROBE_GAUGE_SEED")) {
+        g_gauge_seed = std::strtoull(gs, nullptr, 10);
+        g_gauge = g_gauge || g_gauge_seed != 0;
+    }
     if (std::getenv("PROBE_TRACE")) g_trace = std::fopen((g_out + "/trace.txt").c_str(), "w");
     g_steps = std::fopen((g_out + "/steps.txt").c_str(), "w");
 

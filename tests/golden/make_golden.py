@@ -72,6 +72,38 @@ def gauge_trace(name: str) -> None:
             g.write(" ".join(parts) + "\n")
 
 
+def final_energy(log_path: str) -> float:
+    """The last `... energy = E` line the reference printed (real_tensor_rundmrg.cc:216)."""
+    with open(log_path) as f:
+        return [float(ln.split("=")[1]) for ln in f if "energy =" in ln][-1]
+
+
+def gauge_spread(name: str, seeds, runs=None) -> None:
+    """gauge_spread_<name>.txt: final energies of equally valid runs of the
+    reference on one input (1 BLAS thread): `stock` (LAPACK's own signs),
+    `pinned` (PROBE_GAUGE=1, the library's sign convention) and `seed s`
+    (PROBE_GAUGE_SEED=s: every free sign of LAPACK's singular vectors and
+    eigenvectors flipped at random).  Their spread is the reference's own
+    run-to-run spread of the final energy under a choice the algorithm leaves
+    free.  `runs` maps a label to an existing run directory (holding log.txt)
+    to reuse instead of running it again."""
+    runs = dict(runs or {})
+    inp = os.path.join(ROOT, "dmrgcc_b200", "inputs", f"{name}_spinless.in")
+    todo = [("stock", {}), ("pinned", {"PROBE_GAUGE": "1"})] + [(f"seed {s}", {"PROBE_GAUGE_SEED": str(s)})
+                                                                 for s in seeds]
+    rows = []
+    for label, env in todo:
+        d = runs.get(label)
+        if d is None:
+            d = tempfile.mkdtemp(prefix=f"golden_spread_{name}_")
+            run_probe(inp, d, env)
+        rows.append((label, final_energy(os.path.join(d, "log.txt"))))
+    with open(os.path.join(HERE, f"gauge_spread_{name}.txt"), "w") as f:
+        f.write(f"# final energy of the reference on {name}_spinless.in, 1 BLAS thread, per sign gauge\n")
+        for label, e in rows:
+            f.write(f"{label.replace(' ', '_')} {e:.12f}\n")
+
+
 def input_with(src: str, **values) -> str:
     """The input file text `src` with the given `key = value` lines replaced."""
     import re
@@ -133,11 +165,19 @@ def main() -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--cylinder", action="store_true")
     ap.add_argument("--resume-only", action="store_true")
+    ap.add_argument("--spread", metavar="INPUT", help="only the gauge-spread fixture of one input "
+                    "(chain16 or cylinder8x4; the cylinder takes about an hour per run)")
+    ap.add_argument("--seeds", type=int, default=8, help="random-gauge runs for --spread")
+    ap.add_argument("--reuse", action="append", default=[], metavar="LABEL=DIR",
+                    help="for --spread: take run LABEL (stock, pinned, 'seed s') from DIR/log.txt")
     args = ap.parse_args()
     if not (os.path.exists(PROBE) and os.path.exists(PROBE_SORT)):
         subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "-j8"], check=True)
     if args.resume_only:
         resume_case()
+        return 0
+    if args.spread:
+        gauge_spread(args.spread, range(1, args.seeds + 1), dict(r.split("=", 1) for r in args.reuse))
         return 0
     quicksort_cases()
     tmp = tempfile.mkdtemp(prefix="golden_")

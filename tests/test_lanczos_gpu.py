@@ -62,3 +62,26 @@ def test_lanczos_cylinder_D1024_converges(ctx):
     # random L/R make H_eff non-symmetric; only check the Ritz value is finite and
     # the vector is a unit combination of the Krylov basis
     assert np.isfinite(e) and np.all(np.isfinite(hv))
+
+
+@pytest.mark.parametrize("call", [20, 158])
+def test_lanczos_graph_loop_is_bit_identical(ctx, call):
+    """The Krylov loop as one CUDA graph launch (a conditional WHILE node, the
+    iteration index on the device) gives exactly the energy, dimension and
+    vector of the launch-by-launch loop, on repeated calls (graph relaunched)."""
+    step = SiteStep.from_nac(os.path.join(GOLD, f"heff_c{call}.nac"))
+    niter = int(read_nac(os.path.join(GOLD, f"heff_c{call}.nac"))["niter"][0])
+    h = capi.Heff(ctx, step.site, step.L, step.R)
+    L = capi.DeviceArray.from_host(ctx, step.L_data)
+    R = capi.DeviceArray.from_host(ctx, step.R_data)
+    h.set_env(L, R)
+    res = {}
+    for graph in (False, True, True):
+        h.set_graph(graph)
+        psi = capi.DeviceArray.from_host(ctx, step.ket_data)
+        e, dim = h.lanczos(psi, niter)
+        res.setdefault(graph, []).append((e, dim, psi.download()))
+    (e0, d0, v0), = res[False]
+    for e1, d1, v1 in res[True]:
+        assert d1 == d0 and e1 == e0
+        assert np.array_equal(v1, v0)
