@@ -62,6 +62,8 @@ _SIGS = {
     "dmrg_launch_count": (C.c_int, [_I64]),
     "dmrg_heff_create": (C.c_int, [_VP, C.c_int, C.c_int, _I, C.POINTER(Blocks), C.c_int, C.c_int, C.c_int, _D,
                                    C.POINTER(Blocks), C.POINTER(Blocks), C.c_int, C.POINTER(_VP)]),
+    "dmrg_heff_create_blocks": (C.c_int, [_VP, C.c_int, C.c_int, _I, C.POINTER(Blocks), C.c_int, C.c_int, C.c_int,
+                                          _D, C.POINTER(Blocks), C.POINTER(Blocks), C.c_int, C.POINTER(_VP)]),
     "dmrg_heff_destroy": (C.c_int, [_VP]),
     "dmrg_heff_set_split_threshold": (C.c_int, [_VP, C.c_int64]),
     "dmrg_heff_split_iters": (C.c_int, [_VP, _I]),
@@ -251,10 +253,18 @@ class DeviceArray:
 class SiteProblem:
     """Block structure of one site: sectors, ket blocks, MPO tensor."""
 
-    def __init__(self, nl: int, nr: int, phys: np.ndarray, ket: BlockSpec, W: np.ndarray):
+    def __init__(self, nl: int, nr: int, phys: np.ndarray | None, ket: BlockSpec, W: np.ndarray,
+                 block_phys: np.ndarray | None = None):
+        """`phys`: physics index per sector pair (nl x nr, -1 = no block), or None
+        with `block_phys`: one physics index per ket block (two-site tensors)."""
         self.nl, self.nr = int(nl), int(nr)
-        self.phys = np.ascontiguousarray(phys, dtype=np.int32).reshape(-1)
-        assert self.phys.size == self.nl * self.nr
+        self.block_phys = None if block_phys is None else np.ascontiguousarray(block_phys, dtype=np.int32)
+        if phys is None:
+            assert self.block_phys is not None and self.block_phys.size == len(ket.left)
+            self.phys = None
+        else:
+            self.phys = np.ascontiguousarray(phys, dtype=np.int32).reshape(-1)
+            assert self.phys.size == self.nl * self.nr
         self.ket = ket
         self.W = np.ascontiguousarray(W, dtype=np.float64)
         self.lb, self.rb, self.d = self.W.shape[0], self.W.shape[1], self.W.shape[2]
@@ -269,9 +279,14 @@ class Heff:
         self._L, self._R = _blocks_array(L), _blocks_array(R)
         kb = site.ket.c()
         h = _VP()
-        check(lib().dmrg_heff_create(ctx.h, site.nl, site.nr, _iptr(site.phys), C.byref(kb), site.d, site.lb,
-                                     site.rb, _dptr(site.W), self._L, self._R, precision, C.byref(h)),
-              "dmrg_heff_create")
+        if site.block_phys is not None:
+            check(lib().dmrg_heff_create_blocks(ctx.h, site.nl, site.nr, _iptr(site.block_phys), C.byref(kb), site.d,
+                                                site.lb, site.rb, _dptr(site.W), self._L, self._R, precision,
+                                                C.byref(h)), "dmrg_heff_create_blocks")
+        else:
+            check(lib().dmrg_heff_create(ctx.h, site.nl, site.nr, _iptr(site.phys), C.byref(kb), site.d, site.lb,
+                                         site.rb, _dptr(site.W), self._L, self._R, precision, C.byref(h)),
+                  "dmrg_heff_create")
         self.h = h
         a, b, c = C.c_int64(), C.c_int64(), C.c_int64()
         check(lib().dmrg_heff_sizes(h, C.byref(a), C.byref(b), C.byref(c)), "dmrg_heff_sizes")
@@ -467,16 +482,17 @@ class RunOptions(C.Structure):
     """dmrg_run_options_t."""
 
     _fields_ = [("precision", C.c_int), ("verbose", C.c_int), ("seed", C.c_uint),
-                ("stop_after_half_sweeps", C.c_int), ("lanczos_precision", C.c_double)]
+                ("stop_after_half_sweeps", C.c_int), ("lanczos_precision", C.c_double), ("two_site", C.c_int)]
 
 
 class Run:
     """A whole DMRG run of a reference input file on the device (RealTensorRundmrg)."""
 
     def __init__(self, ctx: Context, input_path: str, model: str = "real_spinless_bose_square", verbose: int = 0,
-                 seed: int = 1, stop_after_half_sweeps: int = -1, precision: int = DMRG_PREC_FP64):
+                 seed: int = 1, stop_after_half_sweeps: int = -1, precision: int = DMRG_PREC_FP64,
+                 two_site: bool = False):
         self.ctx = ctx
-        self._opt = RunOptions(precision, verbose, seed, stop_after_half_sweeps, 0.0)
+        self._opt = RunOptions(precision, verbose, seed, stop_after_half_sweeps, 0.0, int(bool(two_site)))
         h = _VP()
         check(lib().dmrg_run_create(ctx.h, input_path.encode(), model.encode(), C.byref(self._opt), C.byref(h)),
               "dmrg_run_create")

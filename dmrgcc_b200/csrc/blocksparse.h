@@ -92,11 +92,17 @@ struct EnvDesc {
 // Site tensor sectors + MPO tensor.
 struct SiteDesc {
     int nl = 0, nr = 0, d = 0, lb = 0, rb = 0;
-    std::vector<int> phys;    // [nl * nr], -1 = no block
+    std::vector<int> phys;    // [nl * nr], -1 = no block (single-site tensors)
     std::vector<double> W;    // [lb][rb][d][d]
     BlockListDesc ket;
+    // physics index of every ket block, in [0, d).  Single-site tensors have at
+    // most one block per sector pair and take it from `phys`; a two-site tensor
+    // has one block per (left, middle, right) sector triple, several per pair,
+    // with the combined index p1 * d1 + p2.
+    std::vector<int> bphys;
 
     int p(int l, int r) const { return phys[(size_t)l * nr + r]; }
+    int pb(int k) const { return bphys[k]; }
     double w(int o1, int o2, int p1, int p2) const {
         return W[(((size_t)o1 * rb + o2) * d + p1) * d + p2];
     }
@@ -119,5 +125,9 @@ struct SiteDesc {
 // Validates and copies the common site arguments of the C ABI.
 int build_site_desc(SiteDesc& s, int nl, int nr, const int* phys, const dmrg_blocks_t* ket, int d, int lb,
                     int rb, const double* W);
+// The same with a physics index per ket block (block_phys[nblocks]) instead of
+// the sector-pair table; blocks may share a sector pair.
+int build_site_desc_blocks(SiteDesc& s, int nl, int nr, const int* block_phys, const dmrg_blocks_t* ket, int d,
+                           int lb, int rb, const double* W);
 
 }  // namespace dmrg

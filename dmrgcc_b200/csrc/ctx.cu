@@ -31,6 +31,7 @@ int build_site_desc(SiteDesc& s, int nl, int nr, const int* phys, const dmrg_blo
     s.phys.assign(phys, phys + (size_t)nl * nr);
     s.W.assign(W, W + (size_t)lb * rb * d * d);
     if (!s.ket.assign(*ket)) return set_error(DMRG_E_ARG, "invalid ket block list");
+    s.bphys.clear();
     for (int k = 0; k < s.ket.count(); ++k) {
         int l = s.ket.left[k], r = s.ket.right[k];
         if (l < 0 || l >= nl || r < 0 || r >= nr)
@@ -38,6 +39,29 @@ int build_site_desc(SiteDesc& s, int nl, int nr, const int* phys, const dmrg_blo
         int p = s.p(l, r);
         if (p < 0 || p >= d)
             return set_error(DMRG_E_ARG, "ket block %d (%d,%d) has physics index %d", k, l, r, p);
+        s.bphys.push_back(p);
+    }
+    return DMRG_OK;
+}
+
+int build_site_desc_blocks(SiteDesc& s, int nl, int nr, const int* block_phys, const dmrg_blocks_t* ket, int d,
+                           int lb, int rb, const double* W) {
+    if (nl <= 0 || nr <= 0 || !block_phys || !ket || d <= 0 || lb <= 0 || rb <= 0 || !W)
+        return set_error(DMRG_E_ARG, "invalid site description (nl=%d nr=%d d=%d lb=%d rb=%d)", nl, nr, d, lb, rb);
+    s.nl = nl;
+    s.nr = nr;
+    s.d = d;
+    s.lb = lb;
+    s.rb = rb;
+    s.phys.clear();
+    s.W.assign(W, W + (size_t)lb * rb * d * d);
+    if (!s.ket.assign(*ket)) return set_error(DMRG_E_ARG, "invalid ket block list");
+    s.bphys.assign(block_phys, block_phys + s.ket.count());
+    for (int k = 0; k < s.ket.count(); ++k) {
+        const int l = s.ket.left[k], r = s.ket.right[k], p = s.bphys[k];
+        if (l < 0 || l >= nl || r < 0 || r >= nr)
+            return set_error(DMRG_E_ARG, "ket block %d has sectors (%d,%d) outside %dx%d", k, l, r, nl, nr);
+        if (p < 0 || p >= d) return set_error(DMRG_E_ARG, "ket block %d has physics index %d", k, p);
     }
     return DMRG_OK;
 }

@@ -66,7 +66,7 @@ int build_heff(dmrg_heff_s& h) {
             if (rr == 0) continue;  // the reference skips empty blocks
             for (int pos : same_right[ldx]) {
                 const int kdx = ket.left[pos];
-                const int p2 = s.p(kdx, ldx);
+                const int p2 = s.pb(pos);
                 if (!s.right_nonzero(o2, p2)) continue;
                 const int a_k = ket.rows[pos], b_l = ket.cols[pos];
                 if (b_l != rr)
@@ -78,7 +78,7 @@ int build_heff(dmrg_heff_s& h) {
                 bool used = false;
                 for (int pos2 : same_right[jdx]) {
                     const int idx = ket.left[pos2];
-                    const int p1 = s.p(idx, jdx);
+                    const int p1 = s.pb(pos2);
                     for (int o1 = 0; o1 < s.lb; ++o1) {
                         const double w = s.w(o1, o2, p1, p2);
                         if (w == 0.0) continue;
@@ -228,9 +228,9 @@ int dmrg::heff_apply_internal(dmrg_heff_s& h, const double* psi, double* out, bo
 
 extern "C" {
 
-int dmrg_heff_create(dmrg_ctx_t ctx, int nl, int nr, const int* phys, const dmrg_blocks_t* ket, int d, int lb,
-                     int rb, const double* W, const dmrg_blocks_t* L, const dmrg_blocks_t* R, int precision,
-                     dmrg_heff_t* out) {
+static int heff_create(dmrg_ctx_t ctx, int nl, int nr, const int* phys, bool per_block, const dmrg_blocks_t* ket,
+                       int d, int lb, int rb, const double* W, const dmrg_blocks_t* L, const dmrg_blocks_t* R,
+                       int precision, dmrg_heff_t* out) {
     if (!ctx || !out || !L || !R) return set_error(DMRG_E_ARG, "null argument");
     if (precision != DMRG_PREC_FP64 && !is_split(precision))
         return set_error(DMRG_E_ARG, "unsupported precision %d (DMRG_PREC_FP64, _TF32X3 or _BF16X3)", precision);
@@ -240,7 +240,8 @@ int dmrg_heff_create(dmrg_ctx_t ctx, int nl, int nr, const int* phys, const dmrg
     h->ctx = ctx;
     h->precision = precision;
     if (const char* g = std::getenv("DMRG_LANCZOS_GRAPH")) h->use_graph = std::atoi(g) != 0;  // A/B switch
-    int rc = build_site_desc(h->site, nl, nr, phys, ket, d, lb, rb, W);
+    int rc = per_block ? build_site_desc_blocks(h->site, nl, nr, phys, ket, d, lb, rb, W)
+                       : build_site_desc(h->site, nl, nr, phys, ket, d, lb, rb, W);
     if (rc == DMRG_OK && !h->L.assign(L, lb)) rc = set_error(DMRG_E_ARG, "invalid L block lists");
     if (rc == DMRG_OK && !h->R.assign(R, rb)) rc = set_error(DMRG_E_ARG, "invalid R block lists");
     if (rc == DMRG_OK) rc = build_heff(*h);
@@ -250,6 +251,18 @@ int dmrg_heff_create(dmrg_ctx_t ctx, int nl, int nr, const int* phys, const dmrg
     }
     *out = h;
     return DMRG_OK;
+}
+
+int dmrg_heff_create(dmrg_ctx_t ctx, int nl, int nr, const int* phys, const dmrg_blocks_t* ket, int d, int lb,
+                     int rb, const double* W, const dmrg_blocks_t* L, const dmrg_blocks_t* R, int precision,
+                     dmrg_heff_t* out) {
+    return heff_create(ctx, nl, nr, phys, false, ket, d, lb, rb, W, L, R, precision, out);
+}
+
+int dmrg_heff_create_blocks(dmrg_ctx_t ctx, int nl, int nr, const int* block_phys, const dmrg_blocks_t* ket, int d,
+                            int lb, int rb, const double* W, const dmrg_blocks_t* L, const dmrg_blocks_t* R,
+                            int precision, dmrg_heff_t* out) {
+    return heff_create(ctx, nl, nr, block_phys, true, ket, d, lb, rb, W, L, R, precision, out);
 }
 
 int dmrg_heff_destroy(dmrg_heff_t h) {

@@ -1118,6 +1118,7 @@ int Engine::Initialize() {
 
 // RealTensorRundmrg::Run (real_tensor_rundmrg.cc:115-245)
 int Engine::Run() {
+    if (opt_.two_site) return RunTwoSite();
     const double t0 = wall_time();
     DMRG_TRY(Initialize());
     const int halves = opt_.stop_after_half_sweeps >= 0 ? std::min(opt_.stop_after_half_sweeps, num_sweep_)

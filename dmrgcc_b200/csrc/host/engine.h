@@ -87,6 +87,7 @@ struct RunOptions {
     double zero_tolerance = 1e-15;
     unsigned seed = 1;                  // glibc rand() seed; 1 = the reference's implicit seed
     int stop_after_half_sweeps = -1;    // run only this many half-sweeps (-1: all)
+    int two_site = 0;                   // 1: two-site sweeps (RunTwoSite) instead of the reference's single-site ones
 };
 
 class Engine {
@@ -94,8 +95,12 @@ public:
     Engine(dmrg_ctx_t ctx, std::unique_ptr<QuantumSpace> space, std::unique_ptr<RealTensorHamiltonian> ham,
            InputGroup& input, const RunOptions& opt);
     ~Engine();
-    // RealTensorRundmrg::Run (real_tensor_rundmrg.cc:115-245).
+    // RealTensorRundmrg::Run (real_tensor_rundmrg.cc:115-245), or RunTwoSite
+    // when the options ask for two-site sweeps.
     int Run();
+    // Two-site sweeps over the same sweep table (host/twosite.cc); no reference
+    // counterpart.
+    int RunTwoSite();
     const std::vector<SweepRecord>& records() const { return records_; }
     double last_energy() const { return energy_; }
     const std::vector<double>& half_sweep_energies() const { return half_energies_; }
@@ -124,6 +129,10 @@ public:
     int ExecuteExpanTensorNetwork();
     int ComputeTensorNetwork(int leigh, int site);
     int LanczosMethod(int niter, int site, double& energy, int& dim);
+    // One two-site step at bond (j, j+1): merge, Lanczos, split, environment;
+    // adds its phase times to `ph` (0 Lanczos, 2 split, 3 environment, 4 merge).
+    int TwoSiteStep(bool l2r, int j, int niter, double& energy, int& dim, double& discarded, int64_t& theta_dim,
+                    std::array<double, kPhases>& ph);
     // RealTensorSpace::WriteTensorSpace / ReadTensorSpace (real_tensor_space.cc:
     // 182-277): the MPS in the reference's binary checkpoint format.
     int WriteTensorSpace(const std::string& path);

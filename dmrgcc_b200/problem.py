@@ -61,7 +61,10 @@ class SiteStep:
         nr = len(d["lattice.right_dim"])
         dd, lb, rb = (int(x) for x in d["op.dims"])
         W = np.asarray(d["op.W"]).reshape(lb, rb, dd, dd)
-        site = capi.SiteProblem(nl, nr, d["lattice.physics_index"], _spec(d, "lattice.ket"), W)
+        if "lattice.block_phys" in d:  # a two-site tensor: one physics index per block
+            site = capi.SiteProblem(nl, nr, None, _spec(d, "lattice.ket"), W, block_phys=d["lattice.block_phys"])
+        else:
+            site = capi.SiteProblem(nl, nr, d["lattice.physics_index"], _spec(d, "lattice.ket"), W)
         L = [_spec(d, f"L.{o}") for o in range(lb)]
         R = [_spec(d, f"R.{o}") for o in range(rb)]
         step = cls(site, L, R)

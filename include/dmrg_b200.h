@@ -111,6 +111,19 @@ int dmrg_heff_create(dmrg_ctx_t ctx, int num_left_sector, int num_right_sector,
                      const int* physics_index, const dmrg_blocks_t* ket, int physics_dim,
                      int left_bond, int right_bond, const double* W, const dmrg_blocks_t* L,
                      const dmrg_blocks_t* R, int precision, dmrg_heff_t* out);
+/* The same operator for a tensor whose blocks carry their own physics index
+ * (block_phys[ket->nblocks], each in [0, physics_dim)) instead of one index per
+ * sector pair; blocks may then share a sector pair.  This is the two-site
+ * effective Hamiltonian: the two-site tensor Theta(k, p1, p2, l) has one block
+ * per (left sector k, middle sector m, right sector l) with combined index
+ * p1 * d + p2, and W is the two-site MPO W_j W_{j+1} contracted over their
+ * shared bond ([left_bond][right_bond][d*d][d*d]).  The reference is
+ * single-site only (MultiplyEffectHamilton, real_tensor_contraction.cc:
+ * 1223-1291, is this operator with one site's W); there is no counterpart. */
+int dmrg_heff_create_blocks(dmrg_ctx_t ctx, int num_left_sector, int num_right_sector,
+                            const int* block_phys, const dmrg_blocks_t* ket, int physics_dim,
+                            int left_bond, int right_bond, const double* W, const dmrg_blocks_t* L,
+                            const dmrg_blocks_t* R, int precision, dmrg_heff_t* out);
 int dmrg_heff_destroy(dmrg_heff_t h);
 /* Number of doubles of the packed site tensor / left env / right env. */
 int dmrg_heff_sizes(dmrg_heff_t h, int64_t* psi_dim, int64_t* left_env_size,
@@ -265,6 +278,14 @@ typedef struct {
     unsigned seed;              /* 0 or 1: the reference's stream */
     int stop_after_half_sweeps; /* -1: the whole table */
     double lanczos_precision;   /* 0: the reference's 1e-15 */
+    int two_site;               /* 0: the reference's single-site sweeps with
+                                   subspace expansion; 1: two-site sweeps over the
+                                   same sweep table (maxm, niter, canpre per
+                                   half-sweep; no expansion): per bond the
+                                   two-site tensor, its Lanczos ground state
+                                   (dmrg_heff_create_blocks), a per-middle-sector
+                                   SVD truncated to maxm, the environment update.
+                                   No reference counterpart. */
 } dmrg_run_options_t;
 int dmrg_run_create(dmrg_ctx_t ctx, const char* input_path, const char* model,
                     const dmrg_run_options_t* opt, dmrg_run_t* out);
