@@ -85,11 +85,13 @@ _SIGS = {
     "dmrg_canon_singular_values": (C.c_int, [_VP, C.c_int, C.c_int, _D, _I]),
     "dmrg_canon_write": (C.c_int, [_VP, _VP, _VP, _VP]),
     "dmrg_svd_pair_schedule": (C.c_int, [C.POINTER(C.c_ushort)]),
+    "dmrg_svd_set_max_sweeps": (C.c_int, [C.c_int]),
     "dmrg_quicksort_index": (C.c_int, [_D, _I, C.c_int, C.c_int]),
     "dmrg_truncate_dims": (C.c_int, [C.c_int, _I, _D, C.c_int, C.c_double, _I]),
     "dmrg_rand_stream": (C.c_int, [C.c_uint, C.c_int, _I]),
     "dmrg_run_create": (C.c_int, [_VP, C.c_char_p, C.c_char_p, _VP, C.POINTER(_VP)]),
     "dmrg_run_execute": (C.c_int, [_VP]),
+    "dmrg_run_execute_many": (C.c_int, [C.POINTER(_VP), C.c_int, C.c_int, _I]),
     "dmrg_run_destroy": (C.c_int, [_VP]),
     "dmrg_run_half_sweeps": (C.c_int, [_VP, C.c_int, _D, _D, _I]),
     "dmrg_run_steps": (C.c_int, [_VP, C.c_int, _I, _I, _D, _I, _D, _I64, _D, _I]),
@@ -507,6 +509,15 @@ class Run:
         e, s = np.zeros(max(n.value, 1)), np.zeros(max(n.value, 1))
         check(lib().dmrg_run_half_sweeps(self.h, n.value, _dptr(e), _dptr(s), C.byref(n)), "dmrg_run_half_sweeps")
         return e[:n.value], s[:n.value]
+
+    @staticmethod
+    def execute_many(runs: Sequence["Run"], threads: int = 0) -> np.ndarray:
+        """Executes independent runs side by side (each on its own context's
+        stream, `threads` host threads); returns the per-run status codes."""
+        arr = (_VP * max(len(runs), 1))(*[r.h for r in runs])
+        status = np.zeros(max(len(runs), 1), np.int32)
+        check(lib().dmrg_run_execute_many(arr, len(runs), threads, _iptr(status)), "dmrg_run_execute_many")
+        return status[:len(runs)]
 
     PHASES = ("lanczos", "expansion", "canonicalisation", "environment", "match_merge")
 

@@ -1,9 +1,15 @@
 // C ABI of the sweep engine: runs a reference input file end to end, and
 // exposes the model layer (MPO, quantum tables) for inspection.
+#include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <memory>
 #include <stdexcept>
+#include <string>
+#include <system_error>
+#include <thread>
+#include <vector>
 
 #include "dmrg_b200.h"
 #include "host/engine.h"
@@ -88,11 +94,45 @@ int dmrg_run_create(dmrg_ctx_t ctx, const char* input_path, const char* model, c
 int dmrg_run_execute(dmrg_run_t r) {
     if (!r) return set_error(DMRG_E_ARG, "null run");
     try {
+        DMRG_CUDA_TRY(cudaSetDevice(r->engine->device()));
         AllocScope pool(r->engine->stream());
         return r->engine->Run();
     } catch (const std::exception& e) {  // no exception crosses the C ABI
         return set_error(DMRG_E_STATE, "%s", e.what());
     }
+}
+
+int dmrg_run_execute_many(dmrg_run_t* runs, int n, int threads, int* status) {
+    if (!runs || n < 0 || !status) return set_error(DMRG_E_ARG, "null argument");
+    for (int i = 0; i < n; ++i)
+        if (!runs[i]) return set_error(DMRG_E_ARG, "run %d is null", i);
+    for (int i = 0; i < n; ++i)
+        for (int j = i + 1; j < n; ++j)
+            if (runs[i]->engine->stream() == runs[j]->engine->stream())
+                return set_error(DMRG_E_ARG, "runs %d and %d share a stream (give each its own context)", i, j);
+    if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
+    threads = std::min(threads, n);
+    std::atomic<int> next{0};
+    std::vector<std::string> errors(n);
+    auto worker = [&] {
+        for (;;) {
+            const int i = next.fetch_add(1);
+            if (i >= n) return;
+            status[i] = dmrg_run_execute(runs[i]);
+            if (status[i] != DMRG_OK) errors[i] = dmrg_last_error();
+        }
+    };
+    std::vector<std::thread> pool;
+    try {
+        for (int t = 1; t < threads; ++t) pool.emplace_back(worker);
+    } catch (const std::system_error&) {
+        // fewer threads: the calling thread and those started take all runs
+    }
+    worker();
+    for (auto& t : pool) t.join();
+    for (int i = 0; i < n; ++i)
+        if (status[i] != DMRG_OK) return set_error(status[i], "run %d: %s", i, errors[i].c_str());
+    return DMRG_OK;
 }
 
 int dmrg_run_destroy(dmrg_run_t r) {

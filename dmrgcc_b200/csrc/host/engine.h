@@ -113,6 +113,7 @@ public:
     TensorContraction& contraction(int i) { return *con_[i]; }
     int num_site() const { return n_; }
     cudaStream_t stream() const { return st_; }
+    int device() const { return ctx_->device; }
 
     // building blocks (public for the C ABI and tests)
     int Initialize();

@@ -1,4 +1,5 @@
 // Batched one-sided block-Jacobi SVD (see svd.cuh).
+#include <atomic>
 #include <algorithm>
 #include <cfloat>
 #include <chrono>
@@ -26,6 +27,9 @@ constexpr int kLd = kPair + 1;  // padded row of the shared 64x64 matrices
 #endif
 constexpr int kInnerSweeps = DMRG_SVD_INNER_SWEEPS;
 constexpr int kMaxSweeps = 40;
+// The sweep cap in force (dmrg_svd_set_max_sweeps lowers it to provoke the
+// did-not-converge path without touching the device).
+std::atomic<int> g_max_sweeps{kMaxSweeps};
 #ifndef DMRG_SVD_GRAM_MIN_ROWS
 #define DMRG_SVD_GRAM_MIN_ROWS 64
 #endif
@@ -698,7 +702,8 @@ int BatchedSvd::run(cudaStream_t st, int* sweeps_out) {
     int sweep = 0, worst_at = 0;
     double worst_left = 0.0;
     auto t_sweep = std::chrono::steady_clock::now();
-    for (; sweep < kMaxSweeps; ++sweep) {
+    const int max_sweeps = g_max_sweeps.load();
+    for (; sweep < max_sweeps; ++sweep) {
         DMRG_CUDA_TRY(cudaMemsetAsync(d_conv.ptr, 0, np * sizeof(unsigned long long), st));
         // the sweep visits columns in descending norm order: blocks hold columns of
         // similar size, which keeps the many tiny singular values of a noise-expanded
@@ -755,7 +760,7 @@ int BatchedSvd::run(cudaStream_t st, int* sweeps_out) {
             std::memcpy(&worst, &conv[i], sizeof(double));
             if (worst > 2.0 * DBL_EPSILON * std::sqrt((double)probs[i].rows)) {
                 done = false;
-                if (sweep == kMaxSweeps - 1 && worst > worst_left) {
+                if (sweep == max_sweeps - 1 && worst > worst_left) {
                     worst_left = worst;
                     worst_at = i;
                 }
@@ -763,9 +768,9 @@ int BatchedSvd::run(cudaStream_t st, int* sweeps_out) {
         }
         if (done) break;
     }
-    if (sweep == kMaxSweeps)
+    if (sweep == max_sweeps)
         return set_error(DMRG_E_NUMERIC, "Jacobi SVD did not converge in %d sweeps (sector %d x %d: off-diagonal %.3e)",
-                         kMaxSweeps, probs[worst_at].m, probs[worst_at].n, worst_left);
+                         max_sweeps, probs[worst_at].m, probs[worst_at].n, worst_left);
     // singular values = final column norms, sorted
     DMRG_LAUNCH colnorm_kernel<<<colgrid, 256, 0, st>>>(d_probs.as<SvdProblem>(), d_w.as<double>(), d_norm.as<double>());
     DMRG_LAUNCH rank_kernel<<<np, 256, 0, st>>>(d_probs.as<SvdProblem>(), d_norm.as<double>(), d_perm.as<int>(), d_s.as<double>());
@@ -793,6 +798,11 @@ int BatchedSvd::singular_values(std::vector<std::vector<double>>& out, cudaStrea
 }
 
 }  // namespace dmrg
+
+extern "C" int dmrg_svd_set_max_sweeps(int sweeps) {
+    dmrg::g_max_sweeps.store(sweeps > 0 ? sweeps : dmrg::kMaxSweeps);
+    return DMRG_OK;
+}
 
 extern "C" int dmrg_svd_pair_schedule(unsigned short* out) {
     if (!out) return dmrg::set_error(DMRG_E_ARG, "null argument");

@@ -259,6 +259,12 @@ int dmrg_canon_write(dmrg_canon_t c, const double* ket_dev, double* new_ket_dev,
  * r and flip = the lane addresses b first.  Every two columns share one step;
  * within each half-warp the first (and the second) columns are distinct mod 16. */
 int dmrg_svd_pair_schedule(unsigned short* out);
+/* Cap on the Jacobi sweeps of every later canonicalisation in this process
+ * (sweeps <= 0: the default, 40).  A canonicalisation that does not converge
+ * within the cap returns DMRG_E_NUMERIC, as the reference treats a failed
+ * dgesvd (src/tensor/real_matrix.cc:615-619) - but without exiting.  For
+ * fault-injection tests of that path; no reference counterpart. */
+int dmrg_svd_set_max_sweeps(int sweeps);
 
 /* ---- whole runs: the sweep engine ------------------------------------------
  * dmrg_run_create reads a reference input file (the model keys of
@@ -290,6 +296,14 @@ typedef struct {
 int dmrg_run_create(dmrg_ctx_t ctx, const char* input_path, const char* model,
                     const dmrg_run_options_t* opt, dmrg_run_t* out);
 int dmrg_run_execute(dmrg_run_t r);
+/* Executes n independent runs side by side (for example a U/t scan): `threads`
+ * host threads (<= 0: one per hardware thread, at most n) take the runs in
+ * order, each on its own context's stream, so the kernels of different runs
+ * overlap on the GPU.  Every run must have a context (stream) of its own.
+ * status[i] receives run i's return code; the call returns the first failure.
+ * The reference runs one instance per process
+ * (model/real_spinless_bose_square_model.cc:11-42). */
+int dmrg_run_execute_many(dmrg_run_t* runs, int n, int threads, int* status);
 int dmrg_run_destroy(dmrg_run_t r);
 /* Energy after each half-sweep (the reference's "right/left energy =" lines)
  * and its wall time. */

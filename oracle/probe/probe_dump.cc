@@ -21,6 +21,9 @@
 //   PROBE_GAUGE=1          fix the free signs of LAPACK's singular vectors and
 //                          eigenvectors by the library's convention (see below)
 //   PROBE_GAUGE_SEED=s     flip each of those signs at random instead (seed s)
+//   PROBE_SYNTH=s          dumped env updates / canonicalisations run on seeded
+//                          synthetic inputs (see below; with PROBE_STOP)
+//   PROBE_ROUND_F32=1      dumped Lanczos calls run on float32-rounded inputs
 // Always writes PROBE_OUT/steps.txt: one line per Lanczos call with the site,
 // iteration cap, psi_dim and the energy the reference returned.
 #include "probe_common.h"
@@ -66,6 +69,30 @@ static FILE* g_trace = nullptr;
 // the two implementations follow one trajectory through the noise-driven
 // subspace expansion (whose random matrices act in the gauge-dependent basis).
 static bool g_gauge = false;
+// PROBE_SYNTH=s (s != 0): at every dumped environment update and
+// canonicalisation, the inputs (ket values, then the incoming environment
+// bond by bond, blocks in list order, row-major) are first replaced by the
+// splitmix64 stream seeded with s, mapped to [-1, 1) (probe::SplitMix), so that
+// a fixture needs only the block structure, the seed and a digest of the
+// reference's output.  The run is meaningless afterwards: use with PROBE_STOP.
+static unsigned long long g_synth = 0;
+// PROBE_ROUND_F32=1: at every dumped Lanczos call, the operator's environments
+// and the start vector are first rounded to float32 values (stored as doubles),
+// so that a fixture can keep them in float32 without changing the problem the
+// reference solved.
+static bool g_round_f32 = false;
+static void synth_block(RealMatrixBlock* b, probe::SplitMix& rng) {
+    for (int k = 0; b && k < b->num_block_; ++k) {
+        RealMatrix* m = b->matrix_block_[k];
+        for (int e = 0; e < m->total_element_num_; ++e) m->matrix_element_[e] = rng.next();
+    }
+}
+static void round_block(RealMatrixBlock* b) {
+    for (int k = 0; b && k < b->num_block_; ++k) {
+        RealMatrix* m = b->matrix_block_[k];
+        for (int e = 0; e < m->total_element_num_; ++e) m->matrix_element_[e] = (double)(float)m->matrix_element_[e];
+    }
+}
 // PROBE_GAUGE_SEED=s (s != 0): instead, every singular pair and eigenvector
 // that LAPACK returns has its sign flipped with probability 1/2, from a private
 // splitmix64 stream seeded with s (glibc rand() is left untouched).  Each seed
@@ -293,6 +320,11 @@ void __wrap__ZN17RealTensorLanczos13LanczosMethodEiiRd(RealTensorLanczos* self, 
     RealTensorOperator* op = self->hamiltonian_->get_tensor_hamiltonian(site);
     RealTensorContraction* con = self->network_->get_tensor_contraction(site);
     int psi_dim = lat->ComputeKetTensorDim();
+    if (wanted(g_heff, call) && g_round_f32) {
+        round_block(lat->ket_tensor_);
+        for (int o = 0; o < op->left_bond_; ++o) round_block(con->left_contraction_tensor_[o]);
+        for (int o = 0; o < op->right_bond_; ++o) round_block(con->right_contraction_tensor_[o]);
+    }
     if (wanted(g_heff, call)) {
         NacWriter w(g_out + "/heff_" + std::to_string(call) + ".nac");
         w.scalar_i("site", site);
@@ -349,6 +381,13 @@ static void env_common(bool left, RealTensorContraction* self, RealTensorLattice
     bool dump = wanted(g_env, call);
     std::string path = g_out + "/env_" + std::to_string(call) + ".nac";
     NacWriter* w = dump ? new NacWriter(path) : nullptr;
+    if (w && g_synth) {
+        probe::SplitMix rng(g_synth);
+        synth_block(lat->ket_tensor_, rng);
+        RealMatrixBlock** env = left ? self->left_contraction_tensor_ : self->right_contraction_tensor_;
+        for (int o = 0; o < (left ? op->left_bond_ : op->right_bond_); ++o) synth_block(env[o], rng);
+        w->scalar_i("synth_seed", (int)g_synth);
+    }
     if (w) {
         w->scalar_i("left", left ? 1 : 0);
         w->scalar_i("site", site_of(lat));
@@ -446,6 +485,11 @@ static void canon_common(bool left, RealTensorLattice* self, int max_dim, double
     g_cut_gap = g_trace ? truncation_gap(left, self, max_dim, canpre) : -1.0;
     bool dump = wanted(g_canon, call);
     NacWriter* w = dump ? new NacWriter(g_out + "/canon_" + std::to_string(call) + ".nac") : nullptr;
+    if (w && g_synth) {
+        probe::SplitMix rng(g_synth);
+        synth_block(self->ket_tensor_, rng);
+        w->scalar_i("synth_seed", (int)g_synth);
+    }
     if (w) {
         w->scalar_i("left", left ? 1 : 0);
         w->scalar_i("site", site_of(self));
@@ -485,6 +529,8 @@ int main(int argc, char* argv[]) {
         g_gauge_seed = std::strtoull(gs, nullptr, 10);
         g_gauge = g_gauge || g_gauge_seed != 0;
     }
+    if (const char* sy = std::getenv("PROBE_SYNTH")) g_synth = std::strtoull(sy, nullptr, 10);
+    g_round_f32 = std::getenv("PROBE_ROUND_F32") != nullptr;
     if (std::getenv("PROBE_TRACE")) g_trace = std::fopen((g_out + "/trace.txt").c_str(), "w");
     g_steps = std::fopen((g_out + "/steps.txt").c_str(), "w");
 

@@ -71,3 +71,29 @@ def test_canonical_matches_reference(ctx, call):
             ref = kbr[p] @ cbr[s] if side == 0 else cbr[s] @ kbr[p]
             assert np.allclose(mine, ref, atol=1e-11)
     assert res["discarded"] >= 0.0
+
+
+def test_svd_sweep_cap_returns_numeric_error(ctx):
+    """Fault injection on the host: with the Jacobi sweep cap lowered to one
+    sweep, the canonicalisation of a D=64 tensor cannot converge and returns
+    DMRG_E_NUMERIC with a message (the reference exits on a failed dgesvd,
+    src/tensor/real_matrix.cc:615-619); with the cap restored the same call
+    succeeds on the same context.  No device fault is involved: the cap is the
+    host loop's."""
+    d = read_nac(os.path.join(GOLD, "canon_c160.nac"))
+    l, r, rows, cols = _blocks(d, "before.ket")
+    ket = capi.BlockSpec(l, r, rows, cols)
+    kdev = capi.DeviceArray.from_host(ctx, d["before.ket.data"])
+    lib = capi.lib()
+    try:
+        assert lib.dmrg_svd_set_max_sweeps(1) == 0
+        c = capi.Canonical(ctx, 0, d["before.left_dim"], d["before.right_dim"], ket)
+        with pytest.raises(capi.DmrgError) as err:
+            c.run(kdev, int(d["max_dim"][0]), float(d["canpre"][0]))
+        assert err.value.code == capi.E_NUMERIC
+        assert "did not converge" in str(err.value)
+    finally:
+        lib.dmrg_svd_set_max_sweeps(0)
+    c = capi.Canonical(ctx, 0, d["before.left_dim"], d["before.right_dim"], ket)
+    res = c.run(kdev, int(d["max_dim"][0]), float(d["canpre"][0]))
+    assert np.array_equal(res["tdim"], d["after.right_dim"])
