@@ -271,6 +271,62 @@ def reference_sweep_sample(ctx, threads: int) -> dict:
             "reference_energy": ref_e[-1] if ref_e else None, "library_energy": float(e[-1])}
 
 
+def scan_form(threads: int) -> dict:
+    """The batched U/t scan (64 seeded open chains, L in
+    {12..32}, U/t in [1, 20], d=4, unit filling, D<=128, 6 sweeps): all 64 runs
+    side by side on this GPU (dmrg_run_execute_many, one context and stream per
+    instance), in FP64 and with TF32X3 matvecs; aggregate sweeps per second,
+    per-instance |dE/site| of the TF32X3 run against the FP64 run; and the
+    reference binary on the same 64 input files, one process per instance with
+    one BLAS thread, `threads` at a time (the reference runs one instance per
+    process)."""
+    import tempfile
+    from concurrent.futures import ThreadPoolExecutor
+
+    from dmrgcc_b200 import capi, scan
+
+    out = {"workload": "64 Bose-Hubbard chains side by side (seeded U/t scan, D<=128, 6 sweeps)"}
+    with tempfile.TemporaryDirectory() as tmp:
+        paths = scan.write_inputs(tmp)
+        insts = scan.instances()
+        res = {}
+        for name, prec in (("fp64", capi.DMRG_PREC_FP64), ("tf32x3", capi.DMRG_PREC_TF32X3)):
+            ctxs = [capi.Context(0) for _ in paths]
+            runs = [capi.Run(c, p, precision=prec) for c, p in zip(ctxs, paths)]
+            t0 = time.perf_counter()
+            capi.Run.execute_many(runs, 0)
+            wall = time.perf_counter() - t0
+            res[name] = {"wall_s": wall, "sweeps_per_s": 6 * len(runs) / wall,
+                         "energy": [float(r.half_sweeps()[0][-1]) for r in runs]}
+            for r in runs:
+                r.close()
+            for c in ctxs:
+                c.close()
+        de = [abs(a - b) / i["L"] for a, b, i in zip(res["tf32x3"]["energy"], res["fp64"]["energy"], insts)]
+        out.update({"instances": len(paths), "sweeps_total": 6 * len(paths),
+                    "fp64": {k: v for k, v in res["fp64"].items() if k != "energy"},
+                    "tf32x3": {k: v for k, v in res["tf32x3"].items() if k != "energy"},
+                    "max_abs_dE_per_site_tf32x3_vs_fp64": max(de)})
+        if os.path.exists(REF_MODEL):
+            env = dict(os.environ, OMP_NUM_THREADS="1", OPENBLAS_NUM_THREADS="1")
+
+            def one(p):
+                r = subprocess.run([REF_MODEL, p], capture_output=True, text=True, env=env, cwd=tmp, timeout=900)
+                es = [float(ln.split("=")[1]) for ln in r.stdout.splitlines() if "energy =" in ln]
+                return es[-1] if es else float("nan")
+
+            t0 = time.perf_counter()
+            with ThreadPoolExecutor(max_workers=threads) as ex:
+                ref_e = list(ex.map(one, paths))
+            wall = time.perf_counter() - t0
+            dref = [abs(a - b) / i["L"] for a, b, i in zip(res["fp64"]["energy"], ref_e, insts)]
+            out["reference_cpu"] = {"wall_s": wall, "sweeps_per_s": 6 * len(paths) / wall, "cores": threads,
+                                    "processes": "one per instance, 1 BLAS thread each",
+                                    "max_abs_dE_per_site_fp64_vs_reference": max(dref)}
+            out["speedup_vs_reference"] = out["fp64"]["sweeps_per_s"] / out["reference_cpu"]["sweeps_per_s"]
+    return out
+
+
 def sweep_pair(ctx) -> dict:
     """The whole run in FP64 and with TF32X3 matvecs, back to back: times, the
     split run's speedup per sweep and its final-energy difference per site
@@ -424,6 +480,8 @@ def run_b200(args) -> None:
                 sp["speedup_vs_fp64"] = ms_per_step / sp["ms_per_step"]
         if world == 1 and not args.no_sweep:
             line["sweep"] = sweep_pair(ctx)
+        if world == 1 and not args.no_scan:
+            line["scan"] = scan_form(min(os.cpu_count() or 1, 64))
         cpu = cpu_reference(args.cpu_reps, 1, os.cpu_count() or 1) if not args.no_cpu else {"unavailable": "skipped"}
         if "unavailable" not in cpu:
             line["cpu_baseline"] = {"value": cpu["gflop"] / cpu["mean_s"] * 1e-3, "unit": "TFLOP/s",
@@ -449,6 +507,7 @@ def main() -> int:
     ap.add_argument("--cpu-reps", type=int, default=30)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-sweep", action="store_true", help="skip the whole-run sweep-time measurement")
+    ap.add_argument("--no-scan", action="store_true", help="skip the 64-instance U/t scan")
     ap.add_argument("--no-split", action="store_true", help="skip the TF32X3 form of the matvec")
     args = ap.parse_args()
     if args.warmup < 3:

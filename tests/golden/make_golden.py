@@ -104,6 +104,135 @@ def gauge_spread(name: str, seeds, runs=None) -> None:
             f.write(f"{label.replace(' ', '_')} {e:.12f}\n")
 
 
+# D=1024 fixtures of the 8x4 cylinder, half-sweeps 8 (left to right) and 9 (right
+# to left), both with expansion on: (kind, probe call, extra probe settings,
+# Lanczos call to stop after).  Env call = 31 + 31 h + k, canonicalisation call
+# = 64 + 31 h + k, Lanczos call = 31 h + k for step k of half-sweep h.
+D1024_CASES = [
+    ("env", 283, {"PROBE_ENV": "283", "PROBE_SYNTH": "11"}, 253),     # left update, site 4
+    ("env", 314, {"PROBE_ENV": "314", "PROBE_SYNTH": "12"}, 284),     # right update, site 27
+    ("canon", 318, {"PROBE_CANON": "318", "PROBE_SYNTH": "13"}, 255),  # left, site 6, expanded
+    ("canon", 349, {"PROBE_CANON": "349", "PROBE_SYNTH": "14"}, 286),  # right, site 25, expanded
+    ("lanczos", 252, {"PROBE_HEFF": "252", "PROBE_ROUND_F32": "1"}, 252),  # site 4
+]
+N_SAMPLES = 4096
+
+
+def _structure(d: dict, prefixes) -> dict:
+    """The block-structure arrays of a dump (no values)."""
+    return {k: v for k, v in d.items()
+            if any(k.startswith(p) for p in prefixes) and not k.endswith(".data")}
+
+
+def _samples(values, seed: int):
+    """Seeded sample positions (with the first and last element) and the values there."""
+    import numpy as np
+
+    n = len(values)
+    idx = np.unique(np.concatenate([[0, n - 1], np.random.default_rng(seed).integers(0, n, N_SAMPLES)]))
+    return idx.astype(np.int32), np.asarray(values)[idx]
+
+
+def d1024_fixture(kind: str, call: int, run_dir: str) -> None:
+    """Compact fixture from a reference dump at D=1024 (the dump itself is tens of MB):
+    env / canon: the dump's block structures, the seed of its synthetic inputs
+      (PROBE_SYNTH: ket values, then the incoming environment, from the splitmix64
+      stream) and a digest of the reference's output: seeded sample entries, the
+      sum of squares per MPO bond (env) or the singular values and the sampled
+      gauge-invariant products U S V^T per block (canon);
+    lanczos: the float32-rounded environments and start vector it ran on
+      (PROBE_ROUND_F32), the energy and the ground vector (float32)."""
+    import numpy as np
+
+    sys.path.insert(0, ROOT)
+    from oracle.nac import read_nac, write_nac
+
+    if kind == "env":
+        d = read_nac(os.path.join(run_dir, f"env_{call}.nac"))
+        out = _structure(d, ("left", "site", "synth_seed", "lattice.", "op.", "env_in.", "env_out."))
+        bond = int(d["env_out.bond"][0])
+        data = [np.asarray(d[f"env_out.{o}.data"]) for o in range(bond)]
+        flat = np.concatenate(data) if data else np.zeros(0)
+        out["digest.sumsq"] = np.array([float(np.sum(x * x)) for x in data])
+        out["digest.index"], out["digest.value"] = _samples(flat, call)
+        write_nac(os.path.join(HERE, f"env_cyl8x4_D1024_c{call}.nac"), out)
+    elif kind == "canon":
+        d = read_nac(os.path.join(run_dir, f"canon_{call}.nac"))
+        left = bool(d["left"][0])
+        out = _structure(d, ("left", "site", "synth_seed", "max_dim", "canpre", "before.", "after."))
+        # singular values: row norms of S V^T (left) / column norms of U S (right)
+        cr, cc = d["after.canonical.rows"], d["after.canonical.cols"]
+        cdat = np.asarray(d["after.canonical.data"])
+        kr, kc, kl, kri = d["after.ket.rows"], d["after.ket.cols"], d["after.ket.left"], d["after.ket.right"]
+        kdat = np.asarray(d["after.ket.data"])
+        coff = np.concatenate([[0], np.cumsum(cr.astype(np.int64) * cc)])
+        koff = np.concatenate([[0], np.cumsum(kr.astype(np.int64) * kc)])
+        sig, prods = [], []
+        for s in range(len(cr)):
+            c = cdat[coff[s]:coff[s + 1]].reshape(cr[s], cc[s])
+            sig.append(np.linalg.norm(c, axis=1) if left else np.linalg.norm(c, axis=0))
+        for k in range(len(kr)):
+            b = kdat[koff[k]:koff[k + 1]].reshape(kr[k], kc[k])
+            s = kri[k] if left else kl[k]
+            c = cdat[coff[s]:coff[s + 1]].reshape(cr[s], cc[s])
+            prods.append((b @ c if left else c @ b).ravel())
+        out["digest.sigma_count"] = np.array([len(x) for x in sig], dtype=np.int32)
+        out["digest.sigma"] = np.concatenate(sig)
+        flat = np.concatenate(prods) if prods else np.zeros(0)
+        out["digest.index"], out["digest.value"] = _samples(flat, call)
+        out["digest.prod_sumsq"] = np.array([float(np.sum(flat * flat))])
+        write_nac(os.path.join(HERE, f"canon_cyl8x4_D1024_c{call}.nac"), out)
+    else:
+        h = read_nac(os.path.join(run_dir, f"heff_{call}.nac"))
+        lz = read_nac(os.path.join(run_dir, f"lanczos_{call}.nac"))
+        arrays = {k: v for k, v in h.items() if not k.endswith(".data") and k != "heff_out" and k != "heff_dense"}
+        for k, v in h.items():
+            if k.endswith(".data"):
+                f32 = np.asarray(v, dtype=np.float32)
+                assert np.array_equal(f32.astype(np.float64), v), k  # the probe rounded them
+                arrays[k] = f32
+        arrays["energy"] = np.asarray(lz["energy"])
+        arrays["ground"] = np.asarray(lz["lattice.ket.data"], dtype=np.float32)
+        np.savez_compressed(os.path.join(HERE, f"lanczos_cyl8x4_D1024_c{call}.npz"), **arrays)
+
+
+def d1024_fixtures(reuse: dict) -> None:
+    """Runs the reference (1 BLAS thread) up to each D=1024 case, or reuses a
+    finished run directory (label = the case's kind and call, e.g. 'env 283')."""
+    inp = os.path.join(ROOT, "dmrgcc_b200", "inputs", "cylinder8x4_spinless.in")
+    for kind, call, env, stop in D1024_CASES:
+        d = reuse.get(f"{kind} {call}")
+        if d is None:
+            d = tempfile.mkdtemp(prefix=f"golden_d1024_{kind}_{call}_")
+            run_probe(inp, d, dict(env, PROBE_STOP=str(stop)))
+        d1024_fixture(kind, call, d)
+
+
+def scan_reference(jobs: int) -> None:
+    """scan64_reference.txt: the stock reference's final energy on each of the
+    64 U/t-scan inputs (dmrgcc_b200/scan.py), 1 BLAS thread per process."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    sys.path.insert(0, ROOT)
+    from dmrgcc_b200 import scan
+
+    tmp = tempfile.mkdtemp(prefix="golden_scan_")
+    paths = scan.write_inputs(tmp)
+    model = os.path.join(ROOT, "oracle", "_ref", "real_spinless_bose_square_model")
+    env = dict(os.environ, OMP_NUM_THREADS="1", OPENBLAS_NUM_THREADS="1")
+
+    def one(p):
+        r = subprocess.run([model, p], capture_output=True, text=True, env=env, cwd=tmp, check=True)
+        return [float(ln.split("=")[1]) for ln in r.stdout.splitlines() if "energy =" in ln][-1]
+
+    with ThreadPoolExecutor(max_workers=jobs) as ex:
+        energies = list(ex.map(one, paths))
+    with open(os.path.join(HERE, "scan64_reference.txt"), "w") as f:
+        f.write("# instance L U/t final energy of the stock reference (1 BLAS thread)\n")
+        for i, (inst, e) in enumerate(zip(scan.instances(), energies)):
+            f.write(f"{i} {inst['L']} {inst['U']:.17g} {e:.12f}\n")
+
+
 def input_with(src: str, **values) -> str:
     """The input file text `src` with the given `key = value` lines replaced."""
     import re
@@ -168,6 +297,9 @@ def main() -> int:
     ap.add_argument("--spread", metavar="INPUT", help="only the gauge-spread fixture of one input "
                     "(chain16 or cylinder8x4; the cylinder takes about an hour per run)")
     ap.add_argument("--seeds", type=int, default=8, help="random-gauge runs for --spread")
+    ap.add_argument("--d1024", action="store_true", help="only the 8x4 cylinder D=1024 fixtures (each case "
+                    "runs the reference up to its call: minutes of CPU)")
+    ap.add_argument("--scan", action="store_true", help="only the 64-instance U/t scan reference energies")
     ap.add_argument("--reuse", action="append", default=[], metavar="LABEL=DIR",
                     help="for --spread: take run LABEL (stock, pinned, 'seed s') from DIR/log.txt")
     args = ap.parse_args()
@@ -178,6 +310,12 @@ def main() -> int:
         return 0
     if args.spread:
         gauge_spread(args.spread, range(1, args.seeds + 1), dict(r.split("=", 1) for r in args.reuse))
+        return 0
+    if args.d1024:
+        d1024_fixtures(dict(r.split("=", 1) for r in args.reuse))
+        return 0
+    if args.scan:
+        scan_reference(os.cpu_count() or 4)
         return 0
     quicksort_cases()
     tmp = tempfile.mkdtemp(prefix="golden_")
