@@ -22,9 +22,11 @@ using namespace dmrg;
 struct dmrg_env_s {
     dmrg_ctx_t ctx = nullptr;
     int side = 0;
+    int precision = DMRG_PREC_FP64;
     SiteDesc site;
     EnvDesc in, out;
     GemmSchedule s1, s2;
+    SplitPlan p1, p2;  // split precisions: the same two stages on the tcgen05 path
     DeviceBuffer scratch;
     int64_t scratch_size = 0;
     double flops_alg = 0, flops_exec = 0;
@@ -279,12 +281,14 @@ int dmrg_env_create(dmrg_ctx_t ctx, int side, int nl, int nr, const int* phys, c
                     int lb, int rb, const double* W, const dmrg_blocks_t* env_in, int precision, dmrg_env_t* out) {
     if (!ctx || !out || !env_in) return set_error(DMRG_E_ARG, "null argument");
     if (side != 0 && side != 1) return set_error(DMRG_E_ARG, "side must be 0 (left) or 1 (right)");
-    if (precision != DMRG_PREC_FP64) return set_error(DMRG_E_ARG, "unknown precision %d", precision);
+    if (precision != DMRG_PREC_FP64 && precision != DMRG_PREC_TF32X3 && precision != DMRG_PREC_BF16X3)
+        return set_error(DMRG_E_ARG, "unknown precision %d", precision);
     *out = nullptr;
     DMRG_CUDA_TRY(cudaSetDevice(ctx->device));
     auto* e = new dmrg_env_s();
     e->ctx = ctx;
     e->side = side;
+    e->precision = precision;
     int rc = build_site_desc(e->site, nl, nr, phys, ket, d, lb, rb, W);
     if (rc == DMRG_OK && !e->in.assign(env_in, side == 0 ? lb : rb))
         rc = set_error(DMRG_E_ARG, "invalid input environment");
@@ -295,6 +299,11 @@ int dmrg_env_create(dmrg_ctx_t ctx, int side, int nl, int nr, const int* phys, c
     if (rc == DMRG_OK) rc = e->s1.finalize(64, 64, 16, st);
     if (rc == DMRG_OK) rc = e->s2.finalize(64, 64, 16, st, ctx->num_sms);
     if (rc == DMRG_OK) rc = e->scratch.alloc((size_t)std::max<int64_t>(e->scratch_size, 1) * sizeof(double));
+    if (rc == DMRG_OK && precision != DMRG_PREC_FP64) {
+        const int fmt = precision == DMRG_PREC_BF16X3 ? kFmtBF16 : kFmtTF32;
+        rc = e->p1.build(e->s1, fmt, e->site.ket.size, e->in.size, e->scratch_size, st, ctx->num_sms);
+        if (rc == DMRG_OK) rc = e->p2.build(e->s2, fmt, e->scratch_size, e->site.ket.size, e->out.size, st, ctx->num_sms);
+    }
     if (rc != DMRG_OK) {
         delete e;
         return rc;
@@ -343,6 +352,11 @@ int dmrg_env_apply(dmrg_env_t e, const double* ket_dev, const double* env_in_dev
     if (e->out.size) DMRG_CUDA_TRY(cudaMemsetAsync(env_out_dev, 0, (size_t)e->out.size * sizeof(double), st));
     // Both sides: stage 1 reads (ket, env_in) into scratch, stage 2 reads
     // (scratch, ket) into the output; the transposes live in the schedules.
+    if (e->precision != DMRG_PREC_FP64) {  // tcgen05 split products, FP64 sums and FP64 storage
+        DMRG_TRY(e->p1.run(ket_dev, env_in_dev, e->scratch.as<double>(), false, e->ctx->d_status, st));
+        DMRG_TRY(e->p2.run(e->scratch.as<double>(), ket_dev, env_out_dev, true, e->ctx->d_status, st));
+        return DMRG_OK;
+    }
     DMRG_TRY(launch_gemm_f64(e->s1, ket_dev, env_in_dev, e->scratch.as<double>(), false, st));
     DMRG_TRY(launch_gemm_f64(e->s2, e->scratch.as<double>(), ket_dev, env_out_dev, true, st));
     return DMRG_OK;

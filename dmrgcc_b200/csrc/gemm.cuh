@@ -220,4 +220,20 @@ struct PackedSchedule {
 int launch_gemm_split(const PackedSchedule& s, const unsigned char* a_imgs, const unsigned char* b_imgs,
                        double* C, unsigned char* t_out, bool accumulate, int* status, cudaStream_t stream);
 
+// Any FP64 grouped GEMM schedule run in split precision: every distinct A
+// operand block becomes an A-role image, every distinct B operand block a
+// B-role image (its transpose, K-major), and each group's terms accumulate in
+// FP32 tensor memory per term and in FP64 across terms (mode-0 output).
+struct SplitPlan {
+    PackSchedule pa, pb;
+    PackedSchedule ps;
+    DeviceBuffer img_a, img_b;
+    // Builds the plan for `s` (its groups, terms and transposes) in format fmt
+    // (kFmtTF32 or kFmtBF16); a_size / b_size: the operand buffers (doubles).
+    int build(const GemmSchedule& s, int fmt, int64_t a_size, int64_t b_size, int64_t c_size, cudaStream_t st,
+              int num_sms);
+    // C (+)= the schedule's products: packs A and B, then one persistent launch.
+    int run(const double* A, const double* B, double* C, bool accumulate, int* status, cudaStream_t st) const;
+};
+
 }  // namespace dmrg

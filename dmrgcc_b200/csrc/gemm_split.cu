@@ -39,6 +39,8 @@
 // status word and stops; the CTA frees its tensor memory and returns.
 #include <algorithm>
 #include <cstdint>
+#include <map>
+#include <tuple>
 
 #include "gemm.cuh"
 
@@ -713,6 +715,71 @@ int launch_gemm_split(const PackedSchedule& s, const unsigned char* a_imgs, cons
     }
     DMRG_CUDA_TRY(cudaGetLastError());
     return DMRG_OK;
+}
+
+}  // namespace dmrg
+
+namespace dmrg {
+
+int SplitPlan::build(const GemmSchedule& s, int fmt, int64_t a_size, int64_t b_size, int64_t c_size, cudaStream_t st,
+                     int num_sms) {
+    pa = PackSchedule();
+    pb = PackSchedule();
+    ps.reset();
+    pa.fmt = pb.fmt = ps.fmt = fmt;
+    ps.out_mode = 0;
+    const int tk = pack_k(fmt);
+    // one image per distinct operand block (the same block often serves many terms)
+    std::map<std::tuple<int64_t, int, int, int>, int64_t> a_img, b_img;
+    for (const GemmGroup& g : s.groups) {
+        if (g.m <= 0 || g.n <= 0 || g.t1 <= g.t0) continue;
+        PackedGroup pg{};
+        pg.t0 = (int)ps.terms.size();
+        pg.m = g.m;
+        pg.n = g.n;
+        pg.c_off = g.c_off;
+        pg.ldc = g.ldc;
+        for (int t = g.t0; t < g.t1; ++t) {
+            const GemmTerm& x = s.terms[t];
+            if (x.k <= 0) continue;
+            // A role: X = op(A), m x k;  B role: X = op(B)^T, n x k
+            const auto ka = std::make_tuple(x.a_off, g.m, x.k, x.lda);
+            auto ia = a_img.find(ka);
+            if (ia == a_img.end()) ia = a_img.emplace(ka, pa.add(x.a_off, g.m, x.k, x.lda, s.ta)).first;
+            const auto kb = std::make_tuple(x.b_off, g.n, x.k, x.ldb);
+            auto ib = b_img.find(kb);
+            if (ib == b_img.end()) ib = b_img.emplace(kb, pb.add(x.b_off, g.n, x.k, x.ldb, !s.tb)).first;
+            ps.terms.push_back(PackedTerm{ia->second, ib->second, (x.k + tk - 1) / tk, 0, x.scale});
+        }
+        pg.t1 = (int)ps.terms.size();
+        if (pg.t1 > pg.t0) ps.groups.push_back(pg);
+    }
+    // every packed operand inside its source buffer
+    for (const PackJob& j : pa.jobs) {
+        const int64_t end = j.trans ? j.src_off + (int64_t)(j.k - 1) * j.ld + j.rows
+                                    : j.src_off + (int64_t)(j.rows - 1) * j.ld + j.k;
+        if (j.src_off < 0 || end > a_size) return set_error(DMRG_E_ARG, "split plan: A operand outside its buffer");
+    }
+    for (const PackJob& j : pb.jobs) {
+        const int64_t end = j.trans ? j.src_off + (int64_t)(j.k - 1) * j.ld + j.rows
+                                    : j.src_off + (int64_t)(j.rows - 1) * j.ld + j.k;
+        if (j.src_off < 0 || end > b_size) return set_error(DMRG_E_ARG, "split plan: B operand outside its buffer");
+    }
+    DMRG_TRY(ps.check_bounds(pa.bytes, pb.bytes, c_size, 0));
+    DMRG_TRY(pa.finalize(st));
+    DMRG_TRY(pb.finalize(st));
+    DMRG_TRY(ps.finalize(st, num_sms));
+    DMRG_TRY(img_a.alloc((size_t)std::max<int64_t>(pa.bytes, 16)));
+    DMRG_TRY(img_b.alloc((size_t)std::max<int64_t>(pb.bytes, 16)));
+    return DMRG_OK;
+}
+
+int SplitPlan::run(const double* A, const double* B, double* C, bool accumulate, int* status,
+                   cudaStream_t st) const {
+    DMRG_TRY(launch_pack(pa, A, img_a.as<unsigned char>(), st));
+    DMRG_TRY(launch_pack(pb, B, img_b.as<unsigned char>(), st));
+    return launch_gemm_split(ps, img_a.as<unsigned char>(), img_b.as<unsigned char>(), C, nullptr, accumulate,
+                             status, st);
 }
 
 }  // namespace dmrg

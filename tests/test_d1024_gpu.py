@@ -138,3 +138,33 @@ def test_lanczos_D1024_matches_reference(ctx):
     g /= np.linalg.norm(g)
     assert 1.0 - abs(float(v @ g)) <= 1e-7
     assert 1 <= dim <= int(d["niter"][0])
+
+
+@pytest.mark.parametrize("call", [283, 314])
+@pytest.mark.parametrize("prec,tol", [(capi.DMRG_PREC_TF32X3, 2e-5), (capi.DMRG_PREC_BF16X3, 2e-4)])
+def test_env_update_D1024_split_precision(ctx, call, prec, tol):
+    """The same D=1024 environment updates with split-precision products on the
+    tensor cores (tcgen05; hi/lo parts, FP32 accumulation per product, FP64
+    sums): same block maps, values within `tol` of the largest FP64 entry."""
+    d = read_nac(os.path.join(GOLD, f"env_cyl8x4_D1024_c{call}.nac"))
+    side = 0 if d["left"][0] else 1
+    seed = int(d["synth_seed"][0])
+    site = _site(d)
+    nin = int(d["env_in.bond"][0])
+    specs = [_spec(d, f"env_in.{o}") for o in range(nin)]
+    ket = capi.DeviceArray(ctx, site.ket.size)
+    ket.fill_uniform(seed, 0)
+    ein = capi.DeviceArray(ctx, sum(s.size for s in specs))
+    ein.fill_uniform(seed, site.ket.size)
+    outs = []
+    for p in (capi.DMRG_PREC_FP64, prec):
+        e = capi.Env(ctx, side, site, specs, precision=p)
+        eout = capi.DeviceArray(ctx, e.out_size)
+        for _ in range(2):  # repeated applications overwrite
+            e.apply(ket, ein, eout)
+        ctx.sync()
+        outs.append(eout.download())
+    ref, got = outs
+    assert got.shape == ref.shape
+    assert np.max(np.abs(got - ref)) <= tol * np.max(np.abs(ref))
+    assert np.max(np.abs(got - ref)) > 0.0  # the split path did run
