@@ -29,8 +29,26 @@ struct ModelSpec {
 // read the model keys and build the space and the Hamiltonian.
 ModelSpec make_model(InputGroup& input, const std::string& model) {
     ModelSpec m;
+    if (model == "real_spinful_bose_square") {
+        // model/complex_spinful_bose_square_model.cc:11-45 (same keys), real tensors
+        const int nx = input.getInt("num_site_x");
+        const int ny = input.getInt("num_site_y");
+        const int d = input.getInt("physics_dim", 2);
+        const bool px = input.getBool("period_x");
+        const bool py = input.getBool("period_y");
+        const int nb[2] = {input.getInt("Nup"), input.getInt("Ndown")};
+        const double flux = input.getDouble("flux");
+        const double jx = input.getDouble("Jx");
+        const double jy = input.getDouble("Jy");
+        const double mu = input.getDouble("mu");
+        const double u[3] = {input.getDouble("U_uu"), input.getDouble("U_dd"), input.getDouble("U_ud")};
+        m.space.reset(new RealSpinfulBoseSquareSpace(nx, ny, nb, d));
+        m.ham.reset(new RealSpinfulBoseSquareHamiltonian(nx, ny, d, flux, jx, jy, u, mu, px, py));
+        return m;
+    }
     if (model != "real_spinless_bose_square")
-        throw std::runtime_error("unknown model '" + model + "' (supported: real_spinless_bose_square)");
+        throw std::runtime_error("unknown model '" + model +
+                                 "' (supported: real_spinless_bose_square, real_spinful_bose_square)");
     const int nx = input.getInt("num_site_x");
     const int ny = input.getInt("num_site_y");
     const int nb = input.getInt("num_boson");

@@ -398,3 +398,186 @@ std::vector<int> RealSpinlessBoseSquareSpace::MergeQuantumTable(const std::vecto
 }
 
 }  // namespace dmrg
+
+namespace dmrg {
+
+// ---------------------------------------------------------------------------
+// Spinful bosons on interleaved species sites
+// ---------------------------------------------------------------------------
+RealSpinfulBoseSquareHamiltonian::RealSpinfulBoseSquareHamiltonian(int nx, int ny, int d, double flux, double hop_x,
+                                                                   double hop_y, const double inter[3], double chem,
+                                                                   bool px, bool py)
+    : nx_(nx), ny_(ny), d_(d), hop_x_(hop_x), hop_y_(hop_y), chem_(chem), px_(px), py_(py) {
+    if (flux != 0.0)
+        throw std::runtime_error("the spinful model's Peierls phases (flux != 0) need complex tensors");
+    for (int t = 0; t < 3; ++t) inter_[t] = inter[t];
+    init(2 * nx * ny, d, 2);
+    // 0 = I, 1 = a+, 2 = a, 3 = n, 4 = mu n + U_0/2 n(n-1), 5 = mu n + U_1/2 n(n-1)
+    // (one chemical potential for both species, as the reference's operator 5
+    // takes the first species' value, complex_spinful_bose_square_hamiltonian.cc:61)
+    basic_.assign(6, HostMatrix(d, d));
+    for (int i = 0; i < d; ++i) {
+        basic_[0].at(i, i) = 1.0;
+        basic_[3].at(i, i) = i;
+        basic_[4].at(i, i) = chem * i + 0.5 * inter_[0] * i * (i - 1);
+        basic_[5].at(i, i) = chem * i + 0.5 * inter_[1] * i * (i - 1);
+    }
+    for (int i = 1; i < d; ++i) {
+        basic_[1].at(i, i - 1) = std::sqrt((double)i);
+        basic_[2].at(i - 1, i) = std::sqrt((double)i);
+    }
+}
+
+// The operator's quantum number between p1 and p2 is carried by the species of p1.
+void RealSpinfulBoseSquareHamiltonian::DefineHamiltonian1(int p1, int p2, double coeff) {
+    if (p1 >= p2) throw std::runtime_error("position1 >= position2 in DefineHamiltonian1");
+    const std::vector<int> q = p1 % 2 == 0 ? std::vector<int>{1, 0} : std::vector<int>{0, 1};
+    for (int i = 0; i < num_site_; ++i) {
+        int op = 0;
+        double c = 1.0;
+        std::vector<int> t{0, 0};
+        if (i == p1) {
+            op = 1;
+            t = q;
+        }
+        if (i > p1 && i < p2) t = q;
+        if (i == p2) {
+            op = 2;
+            c = coeff;
+            t = {0, 0};
+        }
+        ExpanTensorHamiltonian(i, op, c, t);
+    }
+}
+
+void RealSpinfulBoseSquareHamiltonian::DefineHamiltonian2(int p1, int p2, double coeff) {
+    if (p1 >= p2) throw std::runtime_error("position1 >= position2 in DefineHamiltonian2");
+    const std::vector<int> q = p1 % 2 == 0 ? std::vector<int>{-1, 0} : std::vector<int>{0, -1};
+    for (int i = 0; i < num_site_; ++i) {
+        int op = 0;
+        double c = 1.0;
+        std::vector<int> t{0, 0};
+        if (i == p1) {
+            op = 2;
+            t = q;
+        }
+        if (i > p1 && i < p2) t = q;
+        if (i == p2) {
+            op = 1;
+            c = coeff;
+            t = {0, 0};
+        }
+        ExpanTensorHamiltonian(i, op, c, t);
+    }
+}
+
+void RealSpinfulBoseSquareHamiltonian::DefineHamiltonian3(int p, double coeff) {
+    for (int i = 0; i < num_site_; ++i) {
+        int op = 0;
+        double c = 1.0;
+        if (i == p) {
+            op = p % 2 == 0 ? 4 : 5;
+            c = coeff;
+        }
+        ExpanTensorHamiltonian(i, op, c, {0, 0});
+    }
+}
+
+void RealSpinfulBoseSquareHamiltonian::DefineHamiltonian4(int p1, int p2, double coeff) {
+    for (int i = 0; i < num_site_; ++i) {
+        int op = 0;
+        double c = 1.0;
+        if (i == p1) op = 3;
+        if (i == p2) {
+            op = 3;
+            c = coeff;
+        }
+        ExpanTensorHamiltonian(i, op, c, {0, 0});
+    }
+}
+
+// ComplexSpinfulBoseSquareHamiltonian::DefineTensorHamiltonian (:249-350): the
+// same term order (it decides the MPO bond indices), flux 0.
+void RealSpinfulBoseSquareHamiltonian::DefineTensorHamiltonian() {
+    qtab_[0] = {{0, 0}};
+    qtab_[num_site_] = {{0, 0}};
+    for (int i = 0; i < nx_; ++i)
+        for (int j = 0; j < ny_; ++j) {
+            const int p0 = j + i * ny_;
+            for (int s = 0; s < 2 && hop_x_ != 0; ++s) {
+                const int p1 = j + ((i + 1) % nx_) * ny_;
+                if (i + 1 < nx_) {
+                    DefineHamiltonian1(2 * p0 + s, 2 * p1 + s, hop_x_);
+                    DefineHamiltonian2(2 * p0 + s, 2 * p1 + s, hop_x_);
+                } else if (nx_ > 2 && px_) {
+                    DefineHamiltonian1(2 * p1 + s, 2 * p0 + s, hop_x_);
+                    DefineHamiltonian2(2 * p1 + s, 2 * p0 + s, hop_x_);
+                }
+            }
+            for (int s = 0; s < 2 && hop_y_ != 0; ++s) {
+                const int p1 = (j + 1) % ny_ + i * ny_;
+                if (j + 1 < ny_) {
+                    DefineHamiltonian1(2 * p0 + s, 2 * p1 + s, hop_y_);
+                    DefineHamiltonian2(2 * p0 + s, 2 * p1 + s, hop_y_);
+                } else if (ny_ > 2 && py_) {  // the wrap adds its two terms in the other order
+                    DefineHamiltonian2(2 * p1 + s, 2 * p0 + s, hop_y_);
+                    DefineHamiltonian1(2 * p1 + s, 2 * p0 + s, hop_y_);
+                }
+            }
+            if (chem_ != 0.0 || inter_[0] != 0.0) DefineHamiltonian3(2 * p0, 1.0);
+            if (chem_ != 0.0 || inter_[1] != 0.0) DefineHamiltonian3(2 * p0 + 1, 1.0);
+            if (inter_[2] != 0.0) DefineHamiltonian4(2 * p0, 2 * p0 + 1, inter_[2]);
+            ParallelTensorHamiltonian();
+        }
+}
+
+// ComplexSpinfulBoseSquareSpace::DefineQuantumTable (:28-97): per bond, the
+// admissible (N0, N1) with species 0 counted over the first (i+1)/2 MPS sites
+// and species 1 over the first i/2, enumerated with N0 fastest, then ordered by
+// squared deviation from the mean filling (ReorderQuantumTable).
+RealSpinfulBoseSquareSpace::RealSpinfulBoseSquareSpace(int nx, int ny, const int num_boson[2], int d) {
+    num_boson_[0] = num_boson[0];
+    num_boson_[1] = num_boson[1];
+    num_site_ = 2 * nx * ny;
+    d_ = d;
+    num_quantum_ = 2;
+    qtab_.assign(num_site_ + 1, {});
+    const int half = num_site_ / 2;
+    for (int i = 0; i <= num_site_; ++i) {
+        int lo[2] = {0, 0}, hi[2] = {0, 0};
+        double mean[2] = {0.0, 0.0};
+        if (i > 0) {
+            const int pos[2] = {(i + 1) / 2, i / 2};
+            for (int t = 0; t < 2; ++t) {
+                const int min_left = 0, max_left = (d - 1) * pos[t];
+                const int min_right = num_boson_[t] - (half - pos[t]) * (d - 1), max_right = num_boson_[t];
+                lo[t] = std::max(min_left, min_right);
+                hi[t] = std::min(max_left, max_right);
+                mean[t] = (double)num_boson_[t] / half * pos[t];
+            }
+        }
+        std::vector<std::vector<int>> t;
+        for (int b = lo[1]; b <= hi[1]; ++b)
+            for (int a = lo[0]; a <= hi[0]; ++a) t.push_back({a, b});
+        ReorderQuantumTable(t, {mean[0], mean[1]});
+        qtab_[i] = t;
+    }
+}
+
+int RealSpinfulBoseSquareSpace::CheckQuantumTable(int site, const std::vector<int>& left,
+                                                  const std::vector<int>& right) const {
+    const int shift = site % 2;
+    for (int i = 0; i < d_; ++i) {
+        int p[2] = {0, 0};
+        p[shift] = i;
+        if (left[0] + p[0] == right[0] && left[1] + p[1] == right[1]) return i;
+    }
+    return -1;
+}
+
+std::vector<int> RealSpinfulBoseSquareSpace::MergeQuantumTable(const std::vector<int>& op,
+                                                               const std::vector<int>& space) const {
+    return {op[0] + space[0], op[1] + space[1]};
+}
+
+}  // namespace dmrg

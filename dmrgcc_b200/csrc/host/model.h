@@ -134,4 +134,40 @@ private:
     int num_boson_;
 };
 
+// Two-component (spinful) bosons with U(1) x U(1): the species sit on
+// alternating MPS sites (2 nx ny sites: species 0 of lattice site p at MPS site
+// 2p, species 1 at 2p + 1), each with d = n_max + 1 states; bond quantum numbers
+// are (N0, N1).  ComplexSpinfulBoseSquareSpace (model/space/
+// complex_spinful_bose_square_space.cc:3-125) with real tensors.
+class RealSpinfulBoseSquareSpace : public QuantumSpace {
+public:
+    RealSpinfulBoseSquareSpace(int nx, int ny, const int num_boson[2], int physics_dim);
+    int CheckQuantumTable(int site, const std::vector<int>& left, const std::vector<int>& right) const override;
+    std::vector<int> MergeQuantumTable(const std::vector<int>& op, const std::vector<int>& space) const override;
+
+private:
+    int num_boson_[2];
+};
+
+// H = sum over bonds of J_s (a+_s a_s' + h.c.) per species + sum_i [mu n + U_s/2
+// n(n-1)] per species + U_ud n0 n1: ComplexSpinfulBoseSquareHamiltonian
+// (model/hamiltonian/complex_spinful_bose_square_hamiltonian.cc:3-350) with
+// real coefficients.  Its Peierls phases exp(i 2 pi (x+1) flux) on y-bonds
+// need complex tensors: a nonzero flux is rejected.
+class RealSpinfulBoseSquareHamiltonian : public RealTensorHamiltonian {
+public:
+    RealSpinfulBoseSquareHamiltonian(int nx, int ny, int physics_dim, double flux, double hop_x, double hop_y,
+                                     const double inter[3], double chemical, bool period_x, bool period_y);
+    void DefineTensorHamiltonian() override;
+
+private:
+    void DefineHamiltonian1(int p1, int p2, double coeff);  // a+_p1 a_p2
+    void DefineHamiltonian2(int p1, int p2, double coeff);  // a_p1 a+_p2
+    void DefineHamiltonian3(int p, double coeff);           // mu n + U/2 n(n-1) of the site's species
+    void DefineHamiltonian4(int p1, int p2, double coeff);  // n_p1 n_p2
+    int nx_, ny_, d_;
+    double hop_x_, hop_y_, inter_[3], chem_;
+    bool px_, py_;
+};
+
 }  // namespace dmrg

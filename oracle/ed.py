@@ -62,3 +62,50 @@ def ground_energy(nx: int, ny: int, nboson: int, d: int, jx: float, jy: float, u
     if n < 400:
         return float(np.linalg.eigvalsh(H.toarray())[0])
     return float(sla.eigsh(H, k=1, which="SA")[0][0])
+
+
+def ground_energy_spinful(nx: int, ny: int, nup: int, ndown: int, d: int, jx: float, jy: float, u_uu: float,
+                          u_dd: float, u_ud: float, mu: float, px: bool = False, py: bool = False) -> float:
+    """Two-component bosons in the (N_up, N_down) sector, the reference's
+    spinful model (model/hamiltonian/complex_spinful_bose_square_hamiltonian.cc)
+    at zero flux: per species s, J (a+ a + h.c.) on the bonds of bonds(), mu n +
+    U_s/2 n(n-1) on site; U_ud n_up n_down.  A state lists (n_up, n_down) per
+    lattice site."""
+    L = nx * ny
+    occ = [s for s in itertools.product(range(d), repeat=L)]
+    ups = [s for s in occ if sum(s) == nup]
+    dns = [s for s in occ if sum(s) == ndown]
+    states = [(a, b) for a in ups for b in dns]
+    index = {s: k for k, s in enumerate(states)}
+    U = (u_uu, u_dd)
+    rows, cols, vals = [], [], []
+    for k, (a, b) in enumerate(states):
+        diag = 0.0
+        for sp_, occ_s in enumerate((a, b)):
+            diag += sum(mu * n + 0.5 * U[sp_] * n * (n - 1) for n in occ_s)
+        diag += u_ud * sum(x * y for x, y in zip(a, b))
+        rows.append(k)
+        cols.append(k)
+        vals.append(diag)
+        for p0, p1, kind in bonds(nx, ny, px, py):
+            J = jx if kind == "x" else jy
+            if J == 0:
+                continue
+            for sp_ in range(2):
+                s = (a, b)[sp_]
+                for src, dst in ((p0, p1), (p1, p0)):
+                    if s[src] == 0 or s[dst] == d - 1:
+                        continue
+                    t = list(s)
+                    amp = np.sqrt(t[src]) * np.sqrt(t[dst] + 1)
+                    t[src] -= 1
+                    t[dst] += 1
+                    new = (tuple(t), b) if sp_ == 0 else (a, tuple(t))
+                    rows.append(index[new])
+                    cols.append(k)
+                    vals.append(J * amp)
+    n = len(states)
+    H = sp.csr_matrix((vals, (rows, cols)), shape=(n, n))
+    if n < 400:
+        return float(np.linalg.eigvalsh(H.toarray())[0])
+    return float(sla.eigsh(H, k=1, which="SA")[0][0])

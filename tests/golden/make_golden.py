@@ -233,6 +233,41 @@ def scan_reference(jobs: int) -> None:
             f.write(f"{i} {inst['L']} {inst['U']:.17g} {e:.12f}\n")
 
 
+SPINFUL_MODELS = ("spinful4x4", "spinful3x3_periodic_y")
+
+
+def spinful_fixtures() -> None:
+    """model_<input>.nac: the reference's spinful MPO and quantum tables
+    (oracle/_ref/probe_model; the imaginary parts, zero at flux 0, are checked
+    and dropped), and spinful_reference.txt: the reference's final energy on
+    spinful3x2.in (complex_spinful_bose_square_model, 1 BLAS thread)."""
+    import numpy as np
+
+    sys.path.insert(0, ROOT)
+    from oracle.nac import read_nac, write_nac
+
+    probe = os.path.join(ROOT, "oracle", "_ref", "probe_model")
+    for name in SPINFUL_MODELS:
+        tmp = tempfile.mkdtemp(prefix="golden_model_")
+        out = os.path.join(tmp, "model.nac")
+        subprocess.run([probe, os.path.join(ROOT, "dmrgcc_b200", "inputs", f"{name}.in"), out], check=True,
+                       stdout=subprocess.DEVNULL)
+        d = read_nac(out)
+        for k in [k for k in d if k.endswith(".Wi")]:
+            assert not np.any(d[k]), k
+            del d[k]
+        write_nac(os.path.join(HERE, f"model_{name}.nac"), d)
+    tmp = tempfile.mkdtemp(prefix="golden_spinful_")
+    env = dict(os.environ, OMP_NUM_THREADS="1", OPENBLAS_NUM_THREADS="1")
+    model = os.path.join(ROOT, "oracle", "_ref", "complex_spinful_bose_square_model")
+    r = subprocess.run([model, os.path.join(ROOT, "dmrgcc_b200", "inputs", "spinful3x2.in")], capture_output=True,
+                       text=True, env=env, cwd=tmp, check=True)
+    e = [float(ln.split("=")[1]) for ln in r.stdout.splitlines() if "energy =" in ln][-1]
+    with open(os.path.join(HERE, "spinful_reference.txt"), "w") as f:
+        f.write("# final energy of complex_spinful_bose_square_model on spinful3x2.in (1 BLAS thread)\n")
+        f.write(f"spinful3x2 {e:.14f}\n")
+
+
 def input_with(src: str, **values) -> str:
     """The input file text `src` with the given `key = value` lines replaced."""
     import re
@@ -300,6 +335,7 @@ def main() -> int:
     ap.add_argument("--d1024", action="store_true", help="only the 8x4 cylinder D=1024 fixtures (each case "
                     "runs the reference up to its call: minutes of CPU)")
     ap.add_argument("--scan", action="store_true", help="only the 64-instance U/t scan reference energies")
+    ap.add_argument("--spinful", action="store_true", help="only the spinful model fixtures")
     ap.add_argument("--reuse", action="append", default=[], metavar="LABEL=DIR",
                     help="for --spread: take run LABEL (stock, pinned, 'seed s') from DIR/log.txt")
     args = ap.parse_args()
@@ -316,6 +352,9 @@ def main() -> int:
         return 0
     if args.scan:
         scan_reference(os.cpu_count() or 4)
+        return 0
+    if args.spinful:
+        spinful_fixtures()
         return 0
     quicksort_cases()
     tmp = tempfile.mkdtemp(prefix="golden_")

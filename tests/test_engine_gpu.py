@@ -182,3 +182,20 @@ def test_cylinder8x4_D1024_final_energy_within_reference_spread(ctx):
     assert len(rec["energy"]) == 16 * 31
     assert np.all(rec["discarded"] >= 0)
     assert_within_gauge_spread(rec["energy"][-1], spread, 32)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("two_site", [False, True])
+def test_spinful_run_matches_reference_and_ed(ctx, two_site):
+    """The spinful U(1) x U(1) model end to end on the device (single-site with
+    expansion, and two-site): the final energy equals the reference's converged
+    run and exact diagonalisation to 1e-10 per MPS site."""
+    from oracle.ed import ground_energy_spinful
+
+    run = capi.Run(ctx, os.path.join(INPUTS, "spinful3x2.in"), model="real_spinful_bose_square", two_site=two_site)
+    run.execute()
+    e = run.steps()["energy"][-1]
+    with open(os.path.join(GOLD, "spinful_reference.txt")) as f:
+        e_ref = float([ln.split()[1] for ln in f if ln.startswith("spinful3x2")][0])
+    assert abs(e - e_ref) / 12 <= 1e-10
+    assert abs(e - ground_energy_spinful(3, 2, 3, 3, 3, -1.0, -1.0, 6.0, 6.0, 3.0, 0.0)) / 12 <= 1e-10

@@ -39,3 +39,43 @@ def test_mpo_and_quantum_tables_bit_exact(inp, gold):
     for b in range(n + 1):
         assert np.array_equal(m.quantum_table(0, b).ravel(), ref[f"sq{b}"])
         assert np.array_equal(m.quantum_table(1, b).ravel(), ref[f"hq{b}"])
+
+
+@pytest.mark.parametrize("name", ["spinful4x4", "spinful3x3_periodic_y"])
+def test_spinful_mpo_and_quantum_tables_bit_exact(name):
+    """The spinful U(1) x U(1) model (species on alternating MPS sites): MPO and
+    quantum tables bit-identical to the reference's ComplexSpinfulBoseSquare
+    classes at zero flux (oracle/_ref/probe_model); 4x4 open is BASELINE
+    configuration 4, 3x3 periodic in y exercises the wrap-around terms."""
+    ref = read_nac(os.path.join(GOLD, f"model_{name}.nac"))
+    m = capi.Model(os.path.join(ROOT, "dmrgcc_b200", "inputs", f"{name}.in"), "real_spinful_bose_square")
+    n = int(ref["num_site"][0])
+    assert m.num_site == n and m.num_quantum == 2
+    for i in range(n):
+        W = m.mpo(i)
+        d, lb, rb = (int(x) for x in ref[f"op{i}.dims"])
+        assert W.shape == (lb, rb, d, d)
+        assert np.array_equal(W.ravel(), ref[f"op{i}.W"])
+    for b in range(n + 1):
+        assert np.array_equal(m.quantum_table(0, b).ravel(), ref[f"sq{b}"])
+        assert np.array_equal(m.quantum_table(1, b).ravel(), ref[f"hq{b}"])
+
+
+def test_spinful_model_rejects_flux(tmp_path):
+    """The Peierls phases of a nonzero flux need complex tensors."""
+    src = open(os.path.join(ROOT, "dmrgcc_b200", "inputs", "spinful3x2.in")).read()
+    p = tmp_path / "flux.in"
+    p.write_text(src.replace("flux = 0.0", "flux = 0.1666666666666667"))
+    with pytest.raises(capi.DmrgError):
+        capi.Model(str(p), "real_spinful_bose_square")
+
+
+def test_spinful_exact_diagonalisation_matches_reference():
+    """oracle/ed.py's spinful ground energy equals the reference's converged run
+    of the same 3x2 input (D = 729 covers the whole space): pins the ED."""
+    from oracle.ed import ground_energy_spinful
+
+    with open(os.path.join(GOLD, "spinful_reference.txt")) as f:
+        e_ref = float([ln.split()[1] for ln in f if ln.startswith("spinful3x2")][0])
+    e = ground_energy_spinful(3, 2, 3, 3, 3, -1.0, -1.0, 6.0, 6.0, 3.0, 0.0)
+    assert abs(e - e_ref) / 12 <= 1e-12
