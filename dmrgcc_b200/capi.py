@@ -77,6 +77,13 @@ _SIGS = {
     "dmrg_heff_apply_noalloc": (C.c_int, [C.c_int, C.c_int, _I, C.POINTER(Blocks), C.c_int, C.c_int, C.c_int, _D,
                                           C.POINTER(Blocks), C.POINTER(Blocks), _VP, _VP, _VP, _VP, C.c_int, _VP]),
     "dmrg_lanczos": (C.c_int, [_VP, _VP, C.c_int, C.c_double, C.c_double, _D, _I]),
+    "dmrg_zheff_create": (C.c_int, [_VP, C.c_int, C.c_int, _I, C.POINTER(Blocks), C.c_int, C.c_int, C.c_int, _D,
+                                    C.POINTER(Blocks), C.POINTER(Blocks), C.POINTER(_VP)]),
+    "dmrg_zheff_destroy": (C.c_int, [_VP]),
+    "dmrg_zheff_sizes": (C.c_int, [_VP, _I64, _I64, _I64, _D]),
+    "dmrg_zheff_set_env": (C.c_int, [_VP, _VP, _VP]),
+    "dmrg_zheff_apply": (C.c_int, [_VP, _VP, _VP, C.c_int]),
+    "dmrg_zlanczos": (C.c_int, [_VP, _VP, C.c_int, C.c_double, C.c_double, _D, _I]),
     "dmrg_canon_create": (C.c_int, [_VP, C.c_int, C.c_int, C.c_int, _I, _I, C.POINTER(Blocks), C.POINTER(_VP)]),
     "dmrg_canon_destroy": (C.c_int, [_VP]),
     "dmrg_canon_run": (C.c_int, [_VP, _VP, C.c_int, C.c_double, _I, _D]),
@@ -342,6 +349,50 @@ class Heff:
     def close(self) -> None:
         if self.h:
             lib().dmrg_heff_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class ZHeff:
+    """Complex H_eff*psi operator (ComplexTensorContraction::MultiplyEffectHamilton)
+    and its Lanczos ground state.  Device arrays hold interleaved (re, im) doubles:
+    twice as many doubles as complex elements."""
+
+    def __init__(self, ctx: Context, site: SiteProblem, L: Sequence[BlockSpec], R: Sequence[BlockSpec],
+                 Wc: np.ndarray):
+        self.ctx, self.site = ctx, site
+        self._L, self._R = _blocks_array(L), _blocks_array(R)
+        self._W = np.ascontiguousarray(np.asarray(Wc, dtype=np.complex128)).view(np.float64)
+        kb = site.ket.c()
+        h = _VP()
+        check(lib().dmrg_zheff_create(ctx.h, site.nl, site.nr, _iptr(site.phys), C.byref(kb), site.d, site.lb,
+                                      site.rb, _dptr(self._W), self._L, self._R, C.byref(h)), "dmrg_zheff_create")
+        self.h = h
+        a, b, c, f = C.c_int64(), C.c_int64(), C.c_int64(), C.c_double()
+        check(lib().dmrg_zheff_sizes(h, C.byref(a), C.byref(b), C.byref(c), C.byref(f)), "dmrg_zheff_sizes")
+        self.psi_dim, self.l_size, self.r_size, self.flops = a.value, b.value, c.value, f.value
+
+    def set_env(self, L_dev: "DeviceArray", R_dev: "DeviceArray") -> None:
+        self._env_refs = (L_dev, R_dev)
+        check(lib().dmrg_zheff_set_env(self.h, L_dev.ptr, R_dev.ptr), "dmrg_zheff_set_env")
+
+    def apply(self, psi: "DeviceArray", out: "DeviceArray", accumulate: bool = False) -> None:
+        check(lib().dmrg_zheff_apply(self.h, psi.ptr, out.ptr, int(accumulate)), "dmrg_zheff_apply")
+
+    def lanczos(self, psi: "DeviceArray", niter: int, precision: float = 1e-15, zero_tol: float = 1e-15):
+        e, it = C.c_double(), C.c_int()
+        check(lib().dmrg_zlanczos(self.h, psi.ptr, niter, precision, zero_tol, C.byref(e), C.byref(it)),
+              "dmrg_zlanczos")
+        return e.value, it.value
+
+    def close(self) -> None:
+        if self.h:
+            lib().dmrg_zheff_destroy(self.h)
             self.h = None
 
     def __del__(self):

@@ -202,6 +202,31 @@ int dmrg_heff_split_iters(dmrg_heff_t h, int* iters);
  * RealTensorLanczos::LanczosMethod (real_tensor_lanczos.cc:57-185). */
 int dmrg_heff_set_graph(dmrg_heff_t h, int enable);
 
+/* ---- the complex path (complex128) -------------------------------------------
+ * Complex values are interleaved (re, im) doubles, the layout of the reference's
+ * Complex (src/tensor/complex.h:15-16) and of cuDoubleComplex; offsets and
+ * sizes count complex elements.
+ *
+ * dmrg_zheff_*: ComplexTensorContraction::MultiplyEffectHamilton
+ * (src/dmrg/complexdmrg/complex_tensor_contraction.cc:1244-1312): the same
+ * arguments as dmrg_heff_create with a complex MPO W ([lb][rb][d][d] complex);
+ * products on the FP64 tensor path as four real products per complex product.
+ * dmrg_zlanczos: ComplexTensorLanczos::LanczosMethod (complex_tensor_lanczos.cc:
+ * 14-160; the conjugated inner product, :162-169), same stopping rule and
+ * dense branch (psi_dim < 100) as dmrg_lanczos.  *flops: real FLOPs of one
+ * application over the reference loop. */
+typedef struct dmrg_zheff_s* dmrg_zheff_t;
+int dmrg_zheff_create(dmrg_ctx_t ctx, int num_left_sector, int num_right_sector, const int* physics_index,
+                      const dmrg_blocks_t* ket, int physics_dim, int left_bond, int right_bond,
+                      const double* W, const dmrg_blocks_t* L, const dmrg_blocks_t* R, dmrg_zheff_t* out);
+int dmrg_zheff_destroy(dmrg_zheff_t h);
+int dmrg_zheff_sizes(dmrg_zheff_t h, int64_t* psi_dim, int64_t* left_env_size, int64_t* right_env_size,
+                     double* flops);
+int dmrg_zheff_set_env(dmrg_zheff_t h, const double* L_dev, const double* R_dev);
+int dmrg_zheff_apply(dmrg_zheff_t h, const double* psi_dev, double* out_dev, int accumulate);
+int dmrg_zlanczos(dmrg_zheff_t h, double* psi_dev, int niter, double precision, double zero_tol,
+                  double* energy, int* iters);
+
 /* ---- a2/a3: environment update ---------------------------------------------
  * side 0 replaces RealTensorContraction::LeftComputeTensorContraction
  * (real_tensor_contraction.cc:782-940): env_in = L[0..left_bond) of this site,

@@ -268,6 +268,32 @@ def spinful_fixtures() -> None:
         f.write(f"spinful3x2 {e:.14f}\n")
 
 
+ZHEFF_CALLS = [182, 196]  # site 2 (psi_dim 54: dense branch), site 12 (psi_dim 313), half-sweep 8
+ZENV_CALLS = [219, 241]   # left update at site 12 (half-sweep 8), right update at site 12 (half-sweep 9)
+
+
+def complex_fixtures() -> None:
+    """The complex path's fixtures: the reference's complex DMRG (spinful model
+    executable with Ndown = 0 and flux 1/6: Bose-Hubbard-Hofstadter on a 4x3
+    cylinder, dmrgcc_b200/inputs/hofstadter4x3.in) under oracle/_ref/probe_zdump,
+    1 BLAS thread: zheff_hof_c<k>.nac / zlanczos_hof_c<k>.nac (an H_eff problem,
+    the reference's H*psi on its ket, and LanczosMethod's energy and vector),
+    zenv_hof_c<k>.nac (environment updates), steps_hofstadter4x3.txt."""
+    tmp = tempfile.mkdtemp(prefix="golden_complex_")
+    probe = os.path.join(ROOT, "oracle", "_ref", "probe_zdump")
+    env = dict(os.environ, OMP_NUM_THREADS="1", OPENBLAS_NUM_THREADS="1", PROBE_OUT=tmp,
+               PROBE_HEFF=",".join(map(str, ZHEFF_CALLS)), PROBE_ENV=",".join(map(str, ZENV_CALLS)))
+    with open(os.path.join(tmp, "log.txt"), "w") as log:
+        subprocess.run([probe, os.path.join(ROOT, "dmrgcc_b200", "inputs", "hofstadter4x3.in")], env=env,
+                       stdout=log, stderr=subprocess.STDOUT, check=True, cwd=tmp)
+    for c in ZHEFF_CALLS:
+        shutil.copy(os.path.join(tmp, f"zheff_{c}.nac"), os.path.join(HERE, f"zheff_hof_c{c}.nac"))
+        shutil.copy(os.path.join(tmp, f"zlanczos_{c}.nac"), os.path.join(HERE, f"zlanczos_hof_c{c}.nac"))
+    for c in ZENV_CALLS:
+        shutil.copy(os.path.join(tmp, f"zenv_{c}.nac"), os.path.join(HERE, f"zenv_hof_c{c}.nac"))
+    shutil.copy(os.path.join(tmp, "steps.txt"), os.path.join(HERE, "steps_hofstadter4x3.txt"))
+
+
 def input_with(src: str, **values) -> str:
     """The input file text `src` with the given `key = value` lines replaced."""
     import re
@@ -336,6 +362,7 @@ def main() -> int:
                     "runs the reference up to its call: minutes of CPU)")
     ap.add_argument("--scan", action="store_true", help="only the 64-instance U/t scan reference energies")
     ap.add_argument("--spinful", action="store_true", help="only the spinful model fixtures")
+    ap.add_argument("--complex", action="store_true", help="only the complex-path (Hofstadter) fixtures")
     ap.add_argument("--reuse", action="append", default=[], metavar="LABEL=DIR",
                     help="for --spread: take run LABEL (stock, pinned, 'seed s') from DIR/log.txt")
     args = ap.parse_args()
@@ -355,6 +382,9 @@ def main() -> int:
         return 0
     if args.spinful:
         spinful_fixtures()
+        return 0
+    if args.complex:
+        complex_fixtures()
         return 0
     quicksort_cases()
     tmp = tempfile.mkdtemp(prefix="golden_")
