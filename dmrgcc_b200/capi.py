@@ -84,6 +84,9 @@ _SIGS = {
     "dmrg_zheff_set_env": (C.c_int, [_VP, _VP, _VP]),
     "dmrg_zheff_apply": (C.c_int, [_VP, _VP, _VP, C.c_int]),
     "dmrg_zlanczos": (C.c_int, [_VP, _VP, C.c_int, C.c_double, C.c_double, _D, _I]),
+    "dmrg_zenv_create": (C.c_int, [_VP, C.c_int, C.c_int, C.c_int, _I, C.POINTER(Blocks), C.c_int, C.c_int, C.c_int,
+                                   _D, C.POINTER(Blocks), C.POINTER(_VP)]),
+    "dmrg_zenv_apply": (C.c_int, [_VP, _VP, _VP, _VP]),
     "dmrg_canon_create": (C.c_int, [_VP, C.c_int, C.c_int, C.c_int, _I, _I, C.POINTER(Blocks), C.POINTER(_VP)]),
     "dmrg_canon_destroy": (C.c_int, [_VP]),
     "dmrg_canon_run": (C.c_int, [_VP, _VP, C.c_int, C.c_double, _I, _D]),
@@ -406,13 +409,22 @@ class Env:
     """Environment update (Left/RightComputeTensorContraction)."""
 
     def __init__(self, ctx: Context, side: int, site: SiteProblem, env_in: Sequence[BlockSpec],
-                 precision: int = DMRG_PREC_FP64):
+                 precision: int = DMRG_PREC_FP64, Wc: np.ndarray | None = None):
+        """Wc: a complex MPO ([lb][rb][d][d] complex128) for the complex update
+        (dmrg_zenv_create; ket and environments then hold interleaved complex)."""
         self.ctx, self.site, self.side = ctx, site, side
         self._in = _blocks_array(env_in)
+        self.complex = Wc is not None
         kb = site.ket.c()
         h = _VP()
-        check(lib().dmrg_env_create(ctx.h, side, site.nl, site.nr, _iptr(site.phys), C.byref(kb), site.d, site.lb,
-                                    site.rb, _dptr(site.W), self._in, precision, C.byref(h)), "dmrg_env_create")
+        if self.complex:
+            self._W = np.ascontiguousarray(np.asarray(Wc, dtype=np.complex128)).view(np.float64)
+            check(lib().dmrg_zenv_create(ctx.h, side, site.nl, site.nr, _iptr(site.phys), C.byref(kb), site.d,
+                                         site.lb, site.rb, _dptr(self._W), self._in, C.byref(h)), "dmrg_zenv_create")
+        else:
+            check(lib().dmrg_env_create(ctx.h, side, site.nl, site.nr, _iptr(site.phys), C.byref(kb), site.d,
+                                        site.lb, site.rb, _dptr(site.W), self._in, precision, C.byref(h)),
+                  "dmrg_env_create")
         self.h = h
         bond, size = C.c_int(), C.c_int64()
         check(lib().dmrg_env_out_info(h, C.byref(bond), C.byref(size)), "dmrg_env_out_info")
@@ -435,7 +447,10 @@ class Env:
         return a.value, e.value
 
     def apply(self, ket: DeviceArray, env_in: DeviceArray, env_out: DeviceArray) -> None:
-        check(lib().dmrg_env_apply(self.h, ket.ptr, env_in.ptr, env_out.ptr), "dmrg_env_apply")
+        if self.complex:
+            check(lib().dmrg_zenv_apply(self.h, ket.ptr, env_in.ptr, env_out.ptr), "dmrg_zenv_apply")
+        else:
+            check(lib().dmrg_env_apply(self.h, ket.ptr, env_in.ptr, env_out.ptr), "dmrg_env_apply")
 
     def close(self) -> None:
         if self.h:

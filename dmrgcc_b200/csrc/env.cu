@@ -16,6 +16,7 @@
 
 #include "blocksparse.h"
 #include "gemm.cuh"
+#include "zgemm.cuh"
 
 using namespace dmrg;
 
@@ -27,6 +28,9 @@ struct dmrg_env_s {
     EnvDesc in, out;
     GemmSchedule s1, s2;
     SplitPlan p1, p2;  // split precisions: the same two stages on the tcgen05 path
+    // the complex path (dmrg_zenv_create): the same stages on complex blocks
+    bool cplx = false;
+    ZGemmSchedule z1, z2;
     DeviceBuffer scratch;
     int64_t scratch_size = 0;
     double flops_alg = 0, flops_exec = 0;
@@ -352,6 +356,7 @@ int dmrg_env_apply(dmrg_env_t e, const double* ket_dev, const double* env_in_dev
     if (e->out.size) DMRG_CUDA_TRY(cudaMemsetAsync(env_out_dev, 0, (size_t)e->out.size * sizeof(double), st));
     // Both sides: stage 1 reads (ket, env_in) into scratch, stage 2 reads
     // (scratch, ket) into the output; the transposes live in the schedules.
+    if (e->cplx) return set_error(DMRG_E_STATE, "a complex environment update runs through dmrg_zenv_apply");
     if (e->precision != DMRG_PREC_FP64) {  // tcgen05 split products, FP64 sums and FP64 storage
         DMRG_TRY(e->p1.run(ket_dev, env_in_dev, e->scratch.as<double>(), false, e->ctx->d_status, st));
         DMRG_TRY(e->p2.run(e->scratch.as<double>(), ket_dev, env_out_dev, true, e->ctx->d_status, st));
@@ -359,6 +364,76 @@ int dmrg_env_apply(dmrg_env_t e, const double* ket_dev, const double* env_in_dev
     }
     DMRG_TRY(launch_gemm_f64(e->s1, ket_dev, env_in_dev, e->scratch.as<double>(), false, st));
     DMRG_TRY(launch_gemm_f64(e->s2, e->scratch.as<double>(), ket_dev, env_out_dev, true, st));
+    return DMRG_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// The complex path: ComplexTensorContraction::Left/RightComputeTensorContraction
+// (src/dmrg/complexdmrg/complex_tensor_contraction.cc:800-975, 977-1150) have
+// the real structure with the bra block Hermitian-conjugated
+// (HermitianConjugateMatrix, :929, :1113) and a complex MPO.  The real builder
+// runs on a surrogate MPO whose nonzero entries are the (1-based) positions of
+// the complex entries that are nonzero (|w| != 0 exactly where the complex
+// reference takes the term), so the output block maps follow the same
+// zero_flag pass; its terms then become complex terms whose scale is the
+// complex entry at that position, with the conjugation on the bra operand.
+// ---------------------------------------------------------------------------
+extern "C" {
+
+int dmrg_zenv_create(dmrg_ctx_t ctx, int side, int nl, int nr, const int* phys, const dmrg_blocks_t* ket, int d,
+                     int lb, int rb, const double* W, const dmrg_blocks_t* env_in, dmrg_env_t* out) {
+    if (!W || lb <= 0 || rb <= 0 || d <= 0 || !out) return set_error(DMRG_E_ARG, "null argument");
+    const size_t nw = (size_t)lb * rb * d * d;
+    std::vector<double> ids(nw, 0.0);
+    for (size_t i = 0; i < nw; ++i)
+        if (W[2 * i] != 0.0 || W[2 * i + 1] != 0.0) ids[i] = (double)(i + 1);
+    DMRG_TRY(dmrg_env_create(ctx, side, nl, nr, phys, ket, d, lb, rb, ids.data(), env_in, DMRG_PREC_FP64, out));
+    dmrg_env_s* e = *out;
+    auto convert = [&](const GemmSchedule& s, ZGemmSchedule& z, bool stage2, int conj) {
+        z.reset();
+        z.ta = s.ta;
+        z.tb = s.tb;
+        for (const GemmGroup& g : s.groups) {
+            z.add_group(g.c_off, g.ldc, g.m, g.n);
+            for (int t = g.t0; t < g.t1; ++t) {
+                const GemmTerm& x = s.terms[t];
+                double re = x.scale, im = 0.0;
+                if (stage2) {
+                    const size_t pos = (size_t)x.scale - 1;
+                    re = W[2 * pos];
+                    im = W[2 * pos + 1];
+                }
+                z.add_term(x.a_off, x.lda, x.b_off, x.ldb, x.k, re, im, conj);
+            }
+        }
+    };
+    // left: stage 1 B^dagger L (conjugated A), stage 2 w F K;  right: stage 1 K R, stage 2 w G B^dagger
+    convert(e->s1, e->z1, false, side == 0 ? 1 : 0);
+    convert(e->s2, e->z2, true, side == 0 ? 0 : 2);
+    int rc = e->z1.check_bounds(e->site.ket.size, e->in.size, e->scratch_size);
+    if (rc == DMRG_OK) rc = e->z2.check_bounds(e->scratch_size, e->site.ket.size, e->out.size);
+    if (rc == DMRG_OK) rc = e->z1.finalize(ctx->stream);
+    if (rc == DMRG_OK) rc = e->z2.finalize(ctx->stream);
+    if (rc == DMRG_OK) rc = e->scratch.alloc((size_t)std::max<int64_t>(e->scratch_size, 1) * 2 * sizeof(double));
+    if (rc != DMRG_OK) {
+        delete e;
+        *out = nullptr;
+        return rc;
+    }
+    e->cplx = true;
+    e->flops_alg *= 4.0;  // a complex product is four real ones
+    e->flops_exec *= 4.0;
+    return DMRG_OK;
+}
+
+int dmrg_zenv_apply(dmrg_env_t e, const double* ket_dev, const double* env_in_dev, double* env_out_dev) {
+    if (!e || !e->cplx) return set_error(DMRG_E_ARG, "not a complex environment update (dmrg_zenv_create)");
+    cudaStream_t st = e->ctx->stream;
+    if (e->out.size) DMRG_CUDA_TRY(cudaMemsetAsync(env_out_dev, 0, (size_t)e->out.size * 2 * sizeof(double), st));
+    DMRG_TRY(launch_zgemm(e->z1, ket_dev, env_in_dev, e->scratch.as<double>(), false, st));
+    DMRG_TRY(launch_zgemm(e->z2, e->scratch.as<double>(), ket_dev, env_out_dev, true, st));
     return DMRG_OK;
 }
 

@@ -226,6 +226,16 @@ int dmrg_zheff_set_env(dmrg_zheff_t h, const double* L_dev, const double* R_dev)
 int dmrg_zheff_apply(dmrg_zheff_t h, const double* psi_dev, double* out_dev, int accumulate);
 int dmrg_zlanczos(dmrg_zheff_t h, double* psi_dev, int niter, double precision, double zero_tol,
                   double* energy, int* iters);
+/* Complex environment update: ComplexTensorContraction::Left/Right
+ * ComputeTensorContraction (complex_tensor_contraction.cc:800-975, 977-1150;
+ * the bra block Hermitian-conjugated, :929, :1113).  Same arguments as
+ * dmrg_env_create with a complex MPO W; the handle answers dmrg_env_out_info /
+ * _out_blocks / _flops (real FLOPs) and is applied by dmrg_zenv_apply on
+ * complex ket and environments.  Released by dmrg_env_destroy. */
+int dmrg_zenv_create(dmrg_ctx_t ctx, int side, int num_left_sector, int num_right_sector,
+                     const int* physics_index, const dmrg_blocks_t* ket, int physics_dim, int left_bond,
+                     int right_bond, const double* W, const dmrg_blocks_t* env_in, dmrg_env_t* out);
+int dmrg_zenv_apply(dmrg_env_t e, const double* ket_dev, const double* env_in_dev, double* env_out_dev);
 
 /* ---- a2/a3: environment update ---------------------------------------------
  * side 0 replaces RealTensorContraction::LeftComputeTensorContraction
