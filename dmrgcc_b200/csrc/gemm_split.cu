@@ -38,6 +38,7 @@
 // Every wait is bounded: on a timeout a role records DMRG_E_NUMERIC in the
 // status word and stops; the CTA frees its tensor memory and returns.
 #include <algorithm>
+#include <atomic>
 #include <cstdint>
 #include <map>
 #include <tuple>
@@ -572,7 +573,10 @@ int launch_pack(const PackSchedule& p, const double* src, unsigned char* dst, cu
     return DMRG_OK;
 }
 
+int prepare_split_kernel(int fmt);  // below: the kernel's shared-memory opt-in on this device
+
 int PackedSchedule::finalize(cudaStream_t stream, int num_sms) {
+    DMRG_TRY(prepare_split_kernel(fmt));
     exec_groups.clear();
     splits.clear();
     tiles.clear();
@@ -681,21 +685,37 @@ int PackedSchedule::check_bounds(int64_t a_bytes, int64_t b_bytes, int64_t c_siz
 }
 
 namespace {
+// The kernel's dynamic shared-memory opt-in, once per device and format.  It is
+// made when a schedule is finalized (operator creation), so that no launch
+// inside a stream capture (the graph-captured Lanczos loop) has to make it.
+std::atomic<bool> g_smem_attr[2][64];
+template <int FMT>
+int ensure_smem_attr() {
+    int dev = 0;
+    DMRG_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return set_error(DMRG_E_ARG, "device ordinal %d not supported", dev);
+    if (!g_smem_attr[FMT][dev].load()) {
+        DMRG_CUDA_TRY(
+            cudaFuncSetAttribute(gemm_split_kernel<FMT>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
+        g_smem_attr[FMT][dev].store(true);
+    }
+    return DMRG_OK;
+}
+
 template <int FMT>
 int launch_fmt(const PackedSchedule& s, const unsigned char* a_imgs, const unsigned char* b_imgs, double* C,
                unsigned char* t_out, bool accumulate, int* status, int grid, cudaStream_t stream) {
-    static bool attr = false;
-    if (!attr) {
-        DMRG_CUDA_TRY(
-            cudaFuncSetAttribute(gemm_split_kernel<FMT>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
-        attr = true;
-    }
+    DMRG_TRY(ensure_smem_attr<FMT>());
     DMRG_LAUNCH gemm_split_kernel<FMT><<<grid, NT, SMEM_BYTES, stream>>>(
         a_imgs, b_imgs, C, s.aux.as<double>(), t_out, s.d_terms.as<PackedTerm>(), s.d_groups.as<PackedGroup>(),
         s.d_tiles.as<PackedTile>(), s.d_cta_first.as<int>(), accumulate ? 1 : 0, s.out_mode, status);
     return DMRG_OK;
 }
 }  // namespace
+
+int prepare_split_kernel(int fmt) {
+    return fmt == kFmtBF16 ? ensure_smem_attr<kFmtBF16>() : ensure_smem_attr<kFmtTF32>();
+}
 
 int launch_gemm_split(const PackedSchedule& s, const unsigned char* a_imgs, const unsigned char* b_imgs, double* C,
                       unsigned char* t_out, bool accumulate, int* status, cudaStream_t stream) {
