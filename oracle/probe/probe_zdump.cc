@@ -6,20 +6,22 @@
 // and outputs at the requested call indices and call the real member:
 //   ComplexTensorLanczos::LanczosMethod              complex_tensor_lanczos.cc:14
 //   ComplexTensorContraction::Left/RightCompute...   complex_tensor_contraction.cc:800,977
+//   ComplexTensorLattice::Left/RightCanonical...     complex_tensor_lattice.cc (zgesdd)
 // Complex arrays are written as interleaved (re, im) doubles.
 //
 // Usage: probe_zdump <input file>
-//   PROBE_OUT=dir, PROBE_HEFF=i,..., PROBE_ENV=i,..., PROBE_STOP=n as probe_dump.
+//   PROBE_OUT=dir, PROBE_HEFF=i,..., PROBE_ENV=i,..., PROBE_CANON=i,..., PROBE_STOP=n
+//   as probe_dump.
 // Always writes PROBE_OUT/steps.txt (call, site, niter, psi_dim, energy, seconds).
 #include "probe_common.h"
 
 using probe::NacWriter;
 
 static std::string g_out = ".";
-static std::vector<int> g_heff, g_env;
+static std::vector<int> g_heff, g_env, g_canon;
 static int g_stop = -1;
 static FILE* g_steps = nullptr;
-static int n_lanczos = 0, n_env = 0;
+static int n_lanczos = 0, n_env = 0, n_canon = 0;
 
 static std::vector<int> parse_list(const char* s) {
     std::vector<int> v;
@@ -164,6 +166,37 @@ void __wrap__ZN24ComplexTensorContraction29RightComputeTensorContractionEP20Comp
     ComplexTensorContraction* next) {
     zenv_common(false, self, lat, op, next);
 }
+
+void __real__ZN20ComplexTensorLattice26LeftCanonicalTensorLatticeEid(ComplexTensorLattice*, int, double);
+void __real__ZN20ComplexTensorLattice27RightCanonicalTensorLatticeEid(ComplexTensorLattice*, int, double);
+
+static void zcanon_common(bool left, ComplexTensorLattice* self, int max_dim, double canpre) {
+    const int call = n_canon++;
+    NacWriter* w = wanted(g_canon, call) ? new NacWriter(g_out + "/zcanon_" + std::to_string(call) + ".nac") : nullptr;
+    if (w) {
+        w->scalar_i("left", left ? 1 : 0);
+        w->scalar_i("max_dim", max_dim);
+        w->scalar_d("canpre", canpre);
+        zwrite_lattice(*w, "before", self);
+    }
+    if (left) __real__ZN20ComplexTensorLattice26LeftCanonicalTensorLatticeEid(self, max_dim, canpre);
+    else __real__ZN20ComplexTensorLattice27RightCanonicalTensorLatticeEid(self, max_dim, canpre);
+    if (w) {
+        zwrite_lattice(*w, "after", self);
+        if (self->canonical_tensor_) {
+            zwrite_block(*w, "after.canonical", self->canonical_tensor_);
+            const int n = self->canonical_tensor_->num_block_;
+            w->ints("after.match_dim", std::vector<int>(self->match_dim_, self->match_dim_ + n));
+        }
+        delete w;
+    }
+}
+void __wrap__ZN20ComplexTensorLattice26LeftCanonicalTensorLatticeEid(ComplexTensorLattice* self, int m, double c) {
+    zcanon_common(true, self, m, c);
+}
+void __wrap__ZN20ComplexTensorLattice27RightCanonicalTensorLatticeEid(ComplexTensorLattice* self, int m, double c) {
+    zcanon_common(false, self, m, c);
+}
 }  // extern "C"
 
 int main(int argc, char* argv[]) {
@@ -174,6 +207,7 @@ int main(int argc, char* argv[]) {
     if (const char* o = std::getenv("PROBE_OUT")) g_out = o;
     g_heff = parse_list(std::getenv("PROBE_HEFF"));
     g_env = parse_list(std::getenv("PROBE_ENV"));
+    g_canon = parse_list(std::getenv("PROBE_CANON"));
     if (const char* s = std::getenv("PROBE_STOP")) g_stop = std::atoi(s);
     g_steps = std::fopen((g_out + "/steps.txt").c_str(), "w");
     // model/complex_spinful_bose_square_model.cc:11-45

@@ -270,6 +270,7 @@ def spinful_fixtures() -> None:
 
 ZHEFF_CALLS = [182, 196]  # site 2 (psi_dim 54: dense branch), site 12 (psi_dim 313), half-sweep 8
 ZENV_CALLS = [219, 241]   # left update at site 12 (half-sweep 8), right update at site 12 (half-sweep 9)
+ZCANON_CALLS = [244, 266]  # expanded left / right canonicalisation at site 12 (half-sweeps 8 / 9)
 
 
 def complex_fixtures() -> None:
@@ -282,7 +283,8 @@ def complex_fixtures() -> None:
     tmp = tempfile.mkdtemp(prefix="golden_complex_")
     probe = os.path.join(ROOT, "oracle", "_ref", "probe_zdump")
     env = dict(os.environ, OMP_NUM_THREADS="1", OPENBLAS_NUM_THREADS="1", PROBE_OUT=tmp,
-               PROBE_HEFF=",".join(map(str, ZHEFF_CALLS)), PROBE_ENV=",".join(map(str, ZENV_CALLS)))
+               PROBE_HEFF=",".join(map(str, ZHEFF_CALLS)), PROBE_ENV=",".join(map(str, ZENV_CALLS)),
+               PROBE_CANON=",".join(map(str, ZCANON_CALLS)))
     with open(os.path.join(tmp, "log.txt"), "w") as log:
         subprocess.run([probe, os.path.join(ROOT, "dmrgcc_b200", "inputs", "hofstadter4x3.in")], env=env,
                        stdout=log, stderr=subprocess.STDOUT, check=True, cwd=tmp)
@@ -291,6 +293,8 @@ def complex_fixtures() -> None:
         shutil.copy(os.path.join(tmp, f"zlanczos_{c}.nac"), os.path.join(HERE, f"zlanczos_hof_c{c}.nac"))
     for c in ZENV_CALLS:
         shutil.copy(os.path.join(tmp, f"zenv_{c}.nac"), os.path.join(HERE, f"zenv_hof_c{c}.nac"))
+    for c in ZCANON_CALLS:
+        shutil.copy(os.path.join(tmp, f"zcanon_{c}.nac"), os.path.join(HERE, f"zcanon_hof_c{c}.nac"))
     shutil.copy(os.path.join(tmp, "steps.txt"), os.path.join(HERE, "steps_hofstadter4x3.txt"))
 
 
