@@ -94,6 +94,13 @@ _SIGS = {
     "dmrg_canon_out_blocks": (C.c_int, [_VP, _I, _I, _I, _I, _I]),
     "dmrg_canon_singular_values": (C.c_int, [_VP, C.c_int, C.c_int, _D, _I]),
     "dmrg_canon_write": (C.c_int, [_VP, _VP, _VP, _VP]),
+    "dmrg_zcanon_create": (C.c_int, [_VP, C.c_int, C.c_int, C.c_int, _I, _I, C.POINTER(Blocks), C.POINTER(_VP)]),
+    "dmrg_zcanon_destroy": (C.c_int, [_VP]),
+    "dmrg_zcanon_run": (C.c_int, [_VP, _VP, C.c_int, C.c_double, _I, _D]),
+    "dmrg_zcanon_out_info": (C.c_int, [_VP, _I64, _I64, _I]),
+    "dmrg_zcanon_out_blocks": (C.c_int, [_VP, _I, _I, _I, _I, _I]),
+    "dmrg_zcanon_singular_values": (C.c_int, [_VP, C.c_int, C.c_int, _D, _I]),
+    "dmrg_zcanon_write": (C.c_int, [_VP, _VP, _VP, _VP]),
     "dmrg_svd_pair_schedule": (C.c_int, [C.POINTER(C.c_ushort)]),
     "dmrg_svd_set_max_sweeps": (C.c_int, [C.c_int]),
     "dmrg_quicksort_index": (C.c_int, [_D, _I, C.c_int, C.c_int]),
@@ -465,47 +472,52 @@ class Env:
 
 
 class Canonical:
-    """Per-sector SVD canonicalisation (Left/RightCanonicalTensorLattice)."""
+    """Per-sector SVD canonicalisation (Left/RightCanonicalTensorLattice); with
+    complex=True the complex twin (dmrg_zcanon_*: interleaved complex ket)."""
 
-    def __init__(self, ctx: Context, side: int, left_dim, right_dim, ket: BlockSpec):
+    def __init__(self, ctx: Context, side: int, left_dim, right_dim, ket: BlockSpec, complex: bool = False):
         self.ctx, self.side, self.ket = ctx, side, ket
+        self._p = "dmrg_zcanon_" if complex else "dmrg_canon_"
         self.left_dim = np.ascontiguousarray(left_dim, dtype=np.int32)
         self.right_dim = np.ascontiguousarray(right_dim, dtype=np.int32)
         kb = ket.c()
         h = _VP()
-        check(lib().dmrg_canon_create(ctx.h, side, len(self.left_dim), len(self.right_dim), _iptr(self.left_dim),
-                                      _iptr(self.right_dim), C.byref(kb), C.byref(h)), "dmrg_canon_create")
+        check(self._f("create")(ctx.h, side, len(self.left_dim), len(self.right_dim), _iptr(self.left_dim),
+                                _iptr(self.right_dim), C.byref(kb), C.byref(h)), self._p + "create")
         self.h = h
         self.nsec = len(self.right_dim) if side == 0 else len(self.left_dim)
+
+    def _f(self, name: str):
+        return getattr(lib(), self._p + name)
 
     def run(self, ket_dev: DeviceArray, max_dim: int, canpre: float):
         t = np.zeros(self.nsec, dtype=np.int32)
         d = C.c_double()
-        check(lib().dmrg_canon_run(self.h, ket_dev.ptr, max_dim, canpre, _iptr(t), C.byref(d)), "dmrg_canon_run")
+        check(self._f("run")(self.h, ket_dev.ptr, max_dim, canpre, _iptr(t), C.byref(d)), self._p + "run")
         ks, cs, sw = C.c_int64(), C.c_int64(), C.c_int()
-        check(lib().dmrg_canon_out_info(self.h, C.byref(ks), C.byref(cs), C.byref(sw)), "dmrg_canon_out_info")
+        check(self._f("out_info")(self.h, C.byref(ks), C.byref(cs), C.byref(sw)), self._p + "out_info")
         n = len(self.ket.left)
         kr, kc = np.zeros(max(n, 1), np.int32), np.zeros(max(n, 1), np.int32)
         cr, cc, md = (np.zeros(self.nsec, np.int32) for _ in range(3))
-        check(lib().dmrg_canon_out_blocks(self.h, _iptr(kr), _iptr(kc), _iptr(cr), _iptr(cc), _iptr(md)),
-              "dmrg_canon_out_blocks")
+        check(self._f("out_blocks")(self.h, _iptr(kr), _iptr(kc), _iptr(cr), _iptr(cc), _iptr(md)),
+              self._p + "out_blocks")
         return {"tdim": t, "discarded": d.value, "ket_size": ks.value, "canonical_size": cs.value,
                 "sweeps": sw.value, "ket_rows": kr[:n], "ket_cols": kc[:n], "canon_rows": cr, "canon_cols": cc,
                 "match_dim": md}
 
     def singular_values(self, sector: int) -> np.ndarray:
         n = C.c_int()
-        check(lib().dmrg_canon_singular_values(self.h, sector, 0, None, C.byref(n)), "singular_values")
+        check(self._f("singular_values")(self.h, sector, 0, None, C.byref(n)), "singular_values")
         out = np.zeros(max(n.value, 1))
-        check(lib().dmrg_canon_singular_values(self.h, sector, n.value, _dptr(out), C.byref(n)), "singular_values")
+        check(self._f("singular_values")(self.h, sector, n.value, _dptr(out), C.byref(n)), "singular_values")
         return out[:n.value]
 
     def write(self, ket_dev: DeviceArray, new_ket: DeviceArray, canonical: DeviceArray) -> None:
-        check(lib().dmrg_canon_write(self.h, ket_dev.ptr, new_ket.ptr, canonical.ptr), "dmrg_canon_write")
+        check(self._f("write")(self.h, ket_dev.ptr, new_ket.ptr, canonical.ptr), self._p + "write")
 
     def close(self) -> None:
         if self.h:
-            lib().dmrg_canon_destroy(self.h)
+            self._f("destroy")(self.h)
             self.h = None
 
     def __del__(self):

@@ -236,6 +236,26 @@ int dmrg_zenv_create(dmrg_ctx_t ctx, int side, int num_left_sector, int num_righ
                      const int* physics_index, const dmrg_blocks_t* ket, int physics_dim, int left_bond,
                      int right_bond, const double* W, const dmrg_blocks_t* env_in, dmrg_env_t* out);
 int dmrg_zenv_apply(dmrg_env_t e, const double* ket_dev, const double* env_in_dev, double* env_out_dev);
+/* Complex canonicalisation: ComplexTensorLattice::Left/RightCanonicalTensorLattice
+ * (src/dmrg/complexdmrg/complex_tensor_lattice.cc; per-sector zgesdd through
+ * ComplexMatrix::SVDMatrix, src/tensor/complex_matrix.cc:601-638, and
+ * ComputeTruncateDim).  The same calls as dmrg_canon_* on complex data: each
+ * sector's SVD runs on the device as the batched Jacobi SVD of its real form
+ * [[Re A, -Im A], [Im A, Re A]], whose complex singular triplets are recovered
+ * on the host; the new ket takes U (side 0) or V^H (side 1), the canonical
+ * tensor S V^H or U S.  Singular-vector phases are free, as with zgesdd. */
+typedef struct dmrg_zcanon_s* dmrg_zcanon_t;
+int dmrg_zcanon_create(dmrg_ctx_t ctx, int side, int num_left_sector, int num_right_sector,
+                       const int* left_dim, const int* right_dim, const dmrg_blocks_t* ket,
+                       dmrg_zcanon_t* out);
+int dmrg_zcanon_destroy(dmrg_zcanon_t c);
+int dmrg_zcanon_run(dmrg_zcanon_t c, const double* ket_dev, int max_dim, double canpre, int* tdim_out,
+                    double* discarded);
+int dmrg_zcanon_out_info(dmrg_zcanon_t c, int64_t* ket_size, int64_t* canonical_size, int* sweeps);
+int dmrg_zcanon_out_blocks(dmrg_zcanon_t c, int* ket_rows, int* ket_cols, int* canon_rows,
+                           int* canon_cols, int* match_dim);
+int dmrg_zcanon_singular_values(dmrg_zcanon_t c, int sector, int cap, double* values, int* count);
+int dmrg_zcanon_write(dmrg_zcanon_t c, const double* ket_dev, double* new_ket_dev, double* canonical_dev);
 
 /* ---- a2/a3: environment update ---------------------------------------------
  * side 0 replaces RealTensorContraction::LeftComputeTensorContraction
