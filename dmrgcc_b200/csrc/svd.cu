@@ -225,7 +225,10 @@ __global__ void __launch_bounds__(kThreads) solve_kernel(const SvdProblem* __res
     // A pair whose off-diagonal measure is at or below tol needs no rotation (the
     // same test decides convergence); a step that rotates nothing skips the
     // update, and the solve ends once a sweep leaves every measure at or below tol.
-    const double tol2f = tol * tol * fro * fro;
+    // rotation test: |g_ab| above half the convergence threshold, so that every
+    // pair the measure above calls unconverged is rotated whatever the rounding
+    // of either expression
+    const double tol2f = 0.25 * tol * tol * fro * fro;
     static_assert(kThreads % 32 == 0 && (kPair / 2) * (kPair / 2) % kThreads == 0 &&
                       (kPair / 2) * kPair % kThreads == 0,
                   "even split");
@@ -402,6 +405,55 @@ __global__ void __launch_bounds__(128) rotate_kernel(const SvdProblem* __restric
         const int vc = c < kBlk ? colI + c : colJ + c - kBlk;
         if (vc < p.cols && it.r0 + k < it.r1) base[(int64_t)colmap[p.perm_off + vc] * ld + it.r0 + k] = Xt[c * kRotLd + k];
     }
+}
+
+// Scales each working matrix whose largest magnitude is below 1/2 by the power
+// of two that brings it into [0.5, 1), and records the exponent e (0: left
+// as is).  Only exponents change, so the scaling is exact; the Gram matrices,
+// thresholds and rotations then never meet underflow, however small the
+// sector's values (a sector that carries a negligible weight of the state
+// reaches 1e-100 and below, whose squares underflow).  unscale_kernel undoes
+// it on the result.
+__global__ void __launch_bounds__(1024) prescale_kernel(const SvdProblem* __restrict__ probs, double* __restrict__ W,
+                                                        int* __restrict__ expo) {
+    __shared__ double red[32];
+    __shared__ int ex;
+    const SvdProblem p = probs[blockIdx.x];
+    double* w = W + p.w_off;
+    const int64_t cnt = (int64_t)p.rows * p.cols;
+    double mx = 0.0;
+    for (int64_t i = threadIdx.x; i < cnt; i += blockDim.x) mx = fmax(mx, fabs(w[i]));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double m = 0.0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) m = fmax(m, red[k]);
+        int e = 0;
+        if (m > 0.0 && m < 0.5) frexp(m, &e);  // m = f 2^e, f in [0.5, 1), e <= -1
+        ex = e;
+        expo[blockIdx.x] = e;
+    }
+    __syncthreads();
+    const int e = ex;
+    if (e == 0) return;
+    for (int64_t i = threadIdx.x; i < cnt; i += blockDim.x) w[i] = ldexp(w[i], -e);
+}
+
+// Undoes prescale_kernel on the final working matrix and the sorted singular
+// values.  Grid (problems, slices).
+__global__ void __launch_bounds__(256) unscale_kernel(const SvdProblem* __restrict__ probs, const int* __restrict__ expo,
+                                                      double* __restrict__ W, double* __restrict__ sig) {
+    const SvdProblem p = probs[blockIdx.x];
+    const int e = expo[blockIdx.x];
+    if (e == 0) return;
+    double* w = W + p.w_off;
+    const int64_t cnt = (int64_t)p.rows * p.cols;
+    for (int64_t i = (int64_t)blockIdx.y * blockDim.x + threadIdx.x; i < cnt; i += (int64_t)gridDim.y * blockDim.x)
+        w[i] = ldexp(w[i], e);
+    if (blockIdx.y == 0)
+        for (int j = threadIdx.x; j < p.cols; j += blockDim.x) sig[p.s_off + j] = ldexp(sig[p.s_off + j], e);
 }
 
 // Squared Frobenius norm of each working matrix (fixed-order block reduction).
@@ -665,6 +717,7 @@ int BatchedSvd::plan(const std::vector<int>& m, const std::vector<int>& n, cudaS
     DMRG_TRY(d_perm.alloc((size_t)std::max<int64_t>(soff, 1) * sizeof(int)));
     DMRG_TRY(d_conv.alloc(std::max<size_t>(probs.size(), 1) * sizeof(unsigned long long)));
     DMRG_TRY(d_fro2.alloc(std::max<size_t>(probs.size(), 1) * sizeof(double)));
+    DMRG_TRY(d_expo.alloc(std::max<size_t>(probs.size(), 1) * sizeof(int)));
     DMRG_TRY(d_sign.alloc((size_t)std::max<int64_t>(soff, 1) * sizeof(double)));
     DMRG_TRY(d_colmap.alloc((size_t)std::max<int64_t>(soff, 1) * sizeof(int)));
     DMRG_TRY(d_norm.alloc((size_t)std::max<int64_t>(soff, 1) * sizeof(double)));
@@ -686,13 +739,53 @@ int BatchedSvd::plan(const std::vector<int>& m, const std::vector<int>& n, cudaS
     return DMRG_OK;
 }
 
+// Appends, for each problem whose last sweep left a measure above tol: m, n,
+// rows, cols, transposed (int32), fro2 and the measure (float64), then its
+// input and final working matrices (rows x cols float64, column-major).
+void BatchedSvd::dump_unconverged(const char* path, const DeviceBuffer& w_in,
+                                  const std::vector<unsigned long long>& conv, cudaStream_t st) {
+    std::FILE* f = std::fopen(path, "ab");
+    if (!f) return;
+    std::vector<double> fro2(probs.size());
+    cudaMemcpyAsync(fro2.data(), d_fro2.ptr, fro2.size() * sizeof(double), cudaMemcpyDeviceToHost, st);
+    cudaStreamSynchronize(st);
+    for (size_t i = 0; i < probs.size(); ++i) {
+        const SvdProblem& p = probs[i];
+        double worst;
+        std::memcpy(&worst, &conv[i], sizeof(double));
+        if (worst <= 2.0 * DBL_EPSILON * std::sqrt((double)p.rows)) continue;
+        const size_t cnt = (size_t)p.rows * p.cols;
+        std::vector<double> a(cnt), b(cnt);
+        cudaMemcpyAsync(a.data(), w_in.as<double>() + p.w_off, cnt * sizeof(double), cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(b.data(), d_w.as<double>() + p.w_off, cnt * sizeof(double), cudaMemcpyDeviceToHost, st);
+        cudaStreamSynchronize(st);
+        const int hdr[5] = {p.m, p.n, p.rows, p.cols, p.transposed};
+        const double val[2] = {fro2[i], worst};
+        std::fwrite(hdr, sizeof(int), 5, f);
+        std::fwrite(val, sizeof(double), 2, f);
+        std::fwrite(a.data(), sizeof(double), cnt, f);
+        std::fwrite(b.data(), sizeof(double), cnt, f);
+    }
+    std::fclose(f);
+}
+
 int BatchedSvd::run(cudaStream_t st, int* sweeps_out) {
     if (probs.empty()) {
         if (sweeps_out) *sweeps_out = 0;
         return DMRG_OK;
     }
     const int np = (int)probs.size();
+    // DMRG_SVD_FAIL_DUMP=path: keep the input, and if the sweeps do not converge
+    // write every unconverged sector's input and final working matrix to path
+    // (diagnostics only; see dump_unconverged)
+    static const char* fail_dump = std::getenv("DMRG_SVD_FAIL_DUMP");
+    DeviceBuffer w_in;
+    if (fail_dump) {
+        DMRG_TRY(w_in.alloc(d_w.bytes));
+        DMRG_CUDA_TRY(cudaMemcpyAsync(w_in.ptr, d_w.ptr, d_w.bytes, cudaMemcpyDeviceToDevice, st));
+    }
     DMRG_LAUNCH init_identity_kernel<<<np, 256, 0, st>>>(d_probs.as<SvdProblem>(), d_q.as<double>());
+    DMRG_LAUNCH prescale_kernel<<<np, 1024, 0, st>>>(d_probs.as<SvdProblem>(), d_w.as<double>(), d_expo.as<int>());
     DMRG_LAUNCH fro2_kernel<<<np, 256, 0, st>>>(d_probs.as<SvdProblem>(), d_w.as<double>(), d_fro2.as<double>());
     std::vector<unsigned long long> conv(np);
     static const bool debug = std::getenv("DMRG_SVD_DEBUG") != nullptr;  // per-sweep convergence to stderr
@@ -768,6 +861,7 @@ int BatchedSvd::run(cudaStream_t st, int* sweeps_out) {
         }
         if (done) break;
     }
+    if (sweep == max_sweeps && fail_dump) dump_unconverged(fail_dump, w_in, conv, st);
     if (sweep == max_sweeps)
         return set_error(DMRG_E_NUMERIC, "Jacobi SVD did not converge in %d sweeps (sector %d x %d: off-diagonal %.3e)",
                          max_sweeps, probs[worst_at].m, probs[worst_at].n, worst_left);
@@ -776,6 +870,8 @@ int BatchedSvd::run(cudaStream_t st, int* sweeps_out) {
     DMRG_LAUNCH rank_kernel<<<np, 256, 0, st>>>(d_probs.as<SvdProblem>(), d_norm.as<double>(), d_perm.as<int>(), d_s.as<double>());
     DMRG_LAUNCH sign_kernel<<<colgrid, 256, 0, st>>>(d_probs.as<SvdProblem>(), d_w.as<double>(),
                                                                d_q.as<double>(), d_perm.as<int>(), d_sign.as<double>());
+    DMRG_LAUNCH unscale_kernel<<<dim3(np, 32), 256, 0, st>>>(d_probs.as<SvdProblem>(), d_expo.as<int>(),
+                                                             d_w.as<double>(), d_s.as<double>());
     DMRG_CUDA_TRY(cudaGetLastError());
     if (sweeps_out) *sweeps_out = sweep + 1;
     return DMRG_OK;

@@ -19,7 +19,11 @@
 // (singular values to ~eps ||A||, enough for its canpre cut at 1e-12 of a
 // normalised state); columns of a rank-deficient matrix
 // whose norm falls to rounding level (4 eps sqrt(rows) ||A||_F) are left out of
-// rotations and of that test.  Singular values are the final column
+// rotations and of that test.  A matrix whose entries are all below 1/2 is
+// first scaled by a power of two (exact) so that its largest entry lies in
+// [0.5, 1), and scaled back at the end: the thresholds are relative, but their
+// squared forms and the Gram entries of a sector with values near 1e-100 would
+// underflow.  Singular values are the final column
 // norms, sorted in descending order.  The free sign of each singular pair is
 // fixed by a convention: the left singular vector's largest-magnitude component
 // is positive (ties within a relative 1e-6: the first such component).
@@ -67,8 +71,11 @@ public:
     int run(cudaStream_t st, int* sweeps_out = nullptr);
     // Sorted singular values of every active sector, copied to the host.
     int singular_values(std::vector<std::vector<double>>& out, cudaStream_t st);
+    void dump_unconverged(const char* path, const DeviceBuffer& w_in, const std::vector<unsigned long long>& conv,
+                          cudaStream_t st);
 
     DeviceBuffer d_w, d_q, d_s, d_perm, d_probs, d_tasks, d_conv, d_fro2;
+    DeviceBuffer d_expo;  // per problem: the power of two W was scaled by (prescale_kernel)
     DeviceBuffer d_sign;  // +-1 per sorted singular triplet (sign convention, set by run())
     DeviceBuffer d_gram_items, d_rot_items, d_gpart, d_rot, d_skip;
     DeviceBuffer d_colmap, d_norm;  // per sweep: columns in descending norm order

@@ -1,5 +1,7 @@
 // FP64 vector kernels (see vec.cuh).  These are HBM-bound: each reads its
 // operands once with coalesced grid-stride loops and reduces deterministically.
+#include <algorithm>
+
 #include "vec.cuh"
 
 namespace dmrg {
@@ -202,10 +204,20 @@ __global__ void __launch_bounds__(kVecThreads) lanczos_shift_it_kernel(const dou
     }
 }
 
+// Number of slices of each vector in the multidot of m vectors:
+// clamp(blocks / m, 8, max_blocks) (the host-indexed multidot's grid width).
+__host__ __device__ __forceinline__ int multidot_slices(int blocks, int max_blocks, int m) {
+    int nb = blocks / m;
+    if (nb < 8) nb = 8;
+    if (nb > max_blocks) nb = max_blocks;
+    return nb;
+}
+
 // c[k] = <V_k, w> for k < m = i+1, w = V_{i+1}.  The host-indexed multidot runs
-// a (nb, m) grid with nb = clamp(blocks / m, 8, max_blocks); here the grid is
-// max_blocks wide, blocks at or beyond this iteration's nb return, and each
-// remaining block loops over k.  Tickets: one per k, as there.
+// an (nb, m) grid; here that grid is flattened into a 1-D grid sized for the
+// largest nb * m of any iteration (multidot_it_grid): block j takes slice
+// b = j % nb of vector k = j / nb, blocks with k >= m return.  Same slices,
+// partials, tickets and reduction order as there.
 __global__ void __launch_bounds__(kVecThreads) multidot_it_kernel(const double* __restrict__ V, int64_t ldv,
                                                                   int64_t n, int blocks, int max_blocks,
                                                                   double* partial, unsigned* tickets,
@@ -215,34 +227,35 @@ __global__ void __launch_bounds__(kVecThreads) multidot_it_kernel(const double* 
     const int it = state[kIterSlot];
     if (it + 1 >= niter) return;
     const int m = it + 1;
-    int nb = blocks / m;
-    if (nb < 8) nb = 8;
-    if (nb > max_blocks) nb = max_blocks;
-    if ((int)blockIdx.x >= nb) return;
+    const int nb = multidot_slices(blocks, max_blocks, m);
+    const int k = (int)blockIdx.x / nb, b = (int)blockIdx.x % nb;
+    if (k >= m) return;
     const double* __restrict__ w = V + (int64_t)m * ldv;
+    const double* __restrict__ v = V + (int64_t)k * ldv;
+    double acc = 0.0;
+    for (int64_t i = (int64_t)b * blockDim.x + threadIdx.x; i < n; i += (int64_t)nb * blockDim.x) acc += v[i] * w[i];
+    acc = block_sum(acc);
+    if (threadIdx.x == 0) partial[(int64_t)k * nb + b] = acc;
     __shared__ bool is_last;
-    for (int k = 0; k < m; ++k) {
-        const double* v = V + (int64_t)k * ldv;
-        double acc = 0.0;
-        for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)nb * blockDim.x)
-            acc += v[i] * w[i];
-        acc = block_sum(acc);
-        if (threadIdx.x == 0) partial[(int64_t)k * nb + blockIdx.x] = acc;
-        __threadfence();
-        if (threadIdx.x == 0) is_last = (atomicAdd(tickets + k, 1u) == (unsigned)nb - 1);
-        __syncthreads();
-        if (is_last) {
-            __threadfence();
-            double r = 0.0;
-            for (int b = threadIdx.x; b < nb; b += blockDim.x) r += ((volatile double*)partial)[(int64_t)k * nb + b];
-            r = block_sum(r);
-            if (threadIdx.x == 0) {
-                c[k] = r;
-                tickets[k] = 0u;
-            }
-        }
-        __syncthreads();
+    __threadfence();
+    if (threadIdx.x == 0) is_last = (atomicAdd(tickets + k, 1u) == (unsigned)nb - 1);
+    __syncthreads();
+    if (!is_last) return;
+    __threadfence();
+    double r = 0.0;
+    for (int j = threadIdx.x; j < nb; j += blockDim.x) r += ((volatile double*)partial)[(int64_t)k * nb + j];
+    r = block_sum(r);
+    if (threadIdx.x == 0) {
+        c[k] = r;
+        tickets[k] = 0u;
     }
+}
+
+// Grid of multidot_it_kernel: the largest nb * m over the iterations m < niter.
+int multidot_it_grid(int blocks, int max_blocks, int niter) {
+    int g = 1;
+    for (int m = 1; m < niter; ++m) g = std::max(g, multidot_slices(blocks, max_blocks, m) * m);
+    return g;
 }
 
 // w = V_{i+1} (+)= sign * sum_{k<=i} c[k] V_k; with `partial` also ||w|| into *out
@@ -320,9 +333,7 @@ int vec_axpy_norm(const double* alpha, const double* x, double* y, int64_t n, do
 int vec_multidot(const double* V, int64_t ldv, int m, const double* w, int64_t n, double* c, ReduceScratch& rs,
                  int blocks, cudaStream_t st) {
     if (m <= 0) return DMRG_OK;
-    int nb = blocks / m;
-    if (nb < 8) nb = 8;
-    if (nb > rs.max_blocks) nb = rs.max_blocks;
+    const int nb = multidot_slices(blocks, rs.max_blocks, m);
     if ((size_t)nb * m * sizeof(double) > rs.partial.bytes)
         return set_error(DMRG_E_ARG, "multidot scratch too small (%d x %d)", nb, m);
     DMRG_LAUNCH multidot_kernel<<<dim3(nb, m), kVecThreads, 0, st>>>(V, ldv, w, n, rs.partial.as<double>(),
@@ -392,14 +403,15 @@ int vec_lanczos_step_it(const double* beta_base, const double* x, double* h, dou
         return set_error(DMRG_E_ARG, "multidot scratch too small (%d x %d)", rs.max_blocks, niter);
     const int cb = blocks < rs.max_blocks ? blocks : rs.max_blocks;
     unsigned* rows = rs.ticket.as<unsigned>() + kRowTickets;
+    const int mg = multidot_it_grid(blocks, rs.max_blocks, niter);
     DMRG_LAUNCH lanczos_shift_it_kernel<<<blocks, kVecThreads, 0, st>>>(beta_base, x, h, V, n, n, niter, state);
     // classical Gram-Schmidt twice; the second pass also normalises
-    DMRG_LAUNCH multidot_it_kernel<<<rs.max_blocks, kVecThreads, 0, st>>>(V, n, n, blocks, rs.max_blocks,
+    DMRG_LAUNCH multidot_it_kernel<<<mg, kVecThreads, 0, st>>>(V, n, n, blocks, rs.max_blocks,
                                                                           rs.partial.as<double>(), rows, c, niter,
                                                                           state);
     DMRG_LAUNCH combine_it_kernel<<<blocks, kVecThreads, 0, st>>>(V, n, c, -1.0, n, nullptr, nullptr, nullptr, niter,
                                                                   state);
-    DMRG_LAUNCH multidot_it_kernel<<<rs.max_blocks, kVecThreads, 0, st>>>(V, n, n, blocks, rs.max_blocks,
+    DMRG_LAUNCH multidot_it_kernel<<<mg, kVecThreads, 0, st>>>(V, n, n, blocks, rs.max_blocks,
                                                                           rs.partial.as<double>(), rows, c, niter,
                                                                           state);
     DMRG_LAUNCH combine_it_kernel<<<cb, kVecThreads, 0, st>>>(V, n, c, -1.0, n, rs.partial.as<double>(),

@@ -13,9 +13,12 @@
 // vectors of one complex value differ by a factor i.  The complex triplets are
 // recovered on the host: runs of equal singular values (to 1e-9 of the
 // largest) are one complex eigenspace, in which the real columns, taken as
-// complex vectors, are orthonormalised by Gram-Schmidt with complex
-// coefficients (the same coefficients on the right vectors keep A v = sigma u)
-// until the run's complex dimension (half its length) is reached.  Truncation is
+// complex vectors and first orthogonalised against every vector kept so far,
+// are taken in order by Gram-Schmidt with complex coefficients (the same
+// coefficients on the right vectors keep A v = sigma u) whenever more than half
+// a vector's norm remains, until the run's complex dimension (half its length)
+// is reached; a degenerate run that falls short is filled with the largest
+// remainders.  Truncation is
 // the reference's rule on the complex singular values; the new ket takes U (left)
 // or V^H (right) rows, the canonical tensor S V^H or U S, like the reference.
 // The signs (phases) of singular vectors are free, as with zgesdd; only
@@ -131,33 +134,92 @@ int recover_triplets(dmrg_zcanon_s& c, int s, cudaStream_t st) {
     int kept = 0;
     const double tol = 1e-9 * std::max(sig.empty() ? 0.0 : sig[0], 1e-300);
     std::vector<double> u, v;
+    // removes from (cu, cv) its components along the kept vectors [from, to)
+    // (complex coefficients on U; the same coefficients on V keep A v = sigma u)
+    auto project = [&](std::vector<cplx>& cu, std::vector<cplx>& cv, int from, int to) {
+        for (int q = from; q < to; ++q) {
+            const cplx* uq = &Us[(size_t)q * m];
+            const cplx* vq = &Vs[(size_t)q * n];
+            cplx a(0.0, 0.0);
+            for (int i = 0; i < m; ++i) a += std::conj(uq[i]) * cu[i];
+            for (int i = 0; i < m; ++i) cu[i] -= a * uq[i];
+            for (int i = 0; i < n; ++i) cv[i] -= a * vq[i];
+        }
+    };
     for (int j0 = 0; j0 < r2 && kept < r;) {
         int j1 = j0 + 1;
         while (j1 < r2 && sig[j1 - 1] - sig[j1] <= tol) ++j1;
         const int want = std::min(r - kept, (j1 - j0 + 1) / 2);
-        const int first = kept;
-        for (int j = j0; j < j1 && kept - first < want; ++j) {
+        // the run's real pairs as complex vectors, orthogonalised (two passes)
+        // against every vector kept so far: vectors of nearby runs are complex-
+        // orthogonal only to eps ||A|| / gap
+        std::vector<std::vector<cplx>> cu, cv;
+        std::vector<double> cs;
+        for (int j = j0; j < j1; ++j) {
             if (sig[j] <= 0.0) break;
             real_pair(j, u, v);
-            std::vector<cplx> cu(m), cvv(n);
-            for (int i = 0; i < m; ++i) cu[i] = cplx(u[i], u[m + i]);
-            for (int i = 0; i < n; ++i) cvv[i] = cplx(v[i], v[n + i]);
-            for (int pass = 0; pass < 2; ++pass)
-                for (int q = first; q < kept; ++q) {
-                    cplx a(0.0, 0.0);
-                    for (int i = 0; i < m; ++i) a += std::conj(Us[(size_t)q * m + i]) * cu[i];
-                    for (int i = 0; i < m; ++i) cu[i] -= a * Us[(size_t)q * m + i];
-                    for (int i = 0; i < n; ++i) cvv[i] -= a * Vs[(size_t)q * n + i];
-                }
-            double nrm = 0.0;
-            for (int i = 0; i < m; ++i) nrm += std::norm(cu[i]);
-            if (nrm <= 0.5) continue;  // the i-multiple of a vector already taken
-            nrm = std::sqrt(nrm);
-            for (int i = 0; i < m; ++i) Us[(size_t)kept * m + i] = cu[i] / nrm;
-            for (int i = 0; i < n; ++i) Vs[(size_t)kept * n + i] = cvv[i] / nrm;
-            out[kept] = sig[j];
-            ++kept;
+            cu.emplace_back(m);
+            cv.emplace_back(n);
+            for (int i = 0; i < m; ++i) cu.back()[i] = cplx(u[i], u[m + i]);
+            for (int i = 0; i < n; ++i) cv.back()[i] = cplx(v[i], v[n + i]);
+            cs.push_back(sig[j]);
+            for (int pass = 0; pass < 2; ++pass) project(cu.back(), cv.back(), 0, kept);
         }
+        // in descending order, a candidate whose remainder keeps more than half
+        // its norm is a new complex direction (the other real vector of a
+        // complex pair is the i-multiple of the first: remainder ~0); should a
+        // degenerate run not reach its complex dimension that way, the largest
+        // remainders fill it (pivoted Gram-Schmidt)
+        std::vector<char> taken(cu.size(), 0);
+        const int first = kept;
+        auto take = [&](int k, double nrm2) {
+            taken[k] = 1;
+            const double nrm = std::sqrt(nrm2);
+            for (int i = 0; i < m; ++i) Us[(size_t)kept * m + i] = cu[k][i] / nrm;
+            for (int i = 0; i < n; ++i) Vs[(size_t)kept * n + i] = cv[k][i] / nrm;
+            out[kept] = cs[k];
+            ++kept;
+            for (size_t k2 = 0; k2 < cu.size(); ++k2)
+                if (!taken[k2])
+                    for (int pass = 0; pass < 2; ++pass) project(cu[k2], cv[k2], kept - 1, kept);
+        };
+        auto norm2 = [&](int k) {
+            double x = 0.0;
+            for (int i = 0; i < m; ++i) x += std::norm(cu[k][i]);
+            return x;
+        };
+        for (size_t k = 0; k < cu.size() && kept - first < want; ++k) {
+            const double x = norm2((int)k);
+            if (x > 0.5) take((int)k, x);
+        }
+        while (kept - first < want) {
+            int best = -1;
+            double bn = 0.0;
+            for (size_t k = 0; k < cu.size(); ++k) {
+                if (taken[k]) continue;
+                const double x = norm2((int)k);
+                if (x > bn) {
+                    bn = x;
+                    best = (int)k;
+                }
+            }
+            if (best < 0 || bn <= 1e-6) break;  // no further independent direction in the run
+            take(best, bn);
+        }
+        // the run's triplets in descending order of their values
+        std::vector<int> ord(kept - first);
+        for (int k = 0; k < kept - first; ++k) ord[k] = first + k;
+        std::stable_sort(ord.begin(), ord.end(), [&](int x, int y) { return out[x] > out[y]; });
+        std::vector<cplx> tu((size_t)(kept - first) * m), tv((size_t)(kept - first) * n);
+        std::vector<double> to(kept - first);
+        for (int k = 0; k < kept - first; ++k) {
+            std::copy_n(&Us[(size_t)ord[k] * m], m, &tu[(size_t)k * m]);
+            std::copy_n(&Vs[(size_t)ord[k] * n], n, &tv[(size_t)k * n]);
+            to[k] = out[ord[k]];
+        }
+        std::copy(tu.begin(), tu.end(), Us.begin() + (size_t)first * m);
+        std::copy(tv.begin(), tv.end(), Vs.begin() + (size_t)first * n);
+        std::copy(to.begin(), to.end(), out.begin() + first);
         j0 = j1;
     }
     c.rank[s] = kept;

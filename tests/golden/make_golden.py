@@ -233,6 +233,31 @@ def scan_reference(jobs: int) -> None:
             f.write(f"{i} {inst['L']} {inst['U']:.17g} {e:.12f}\n")
 
 
+def converged_reference() -> None:
+    """converged_chain16.txt: the stock reference on chain16_spinless.in with its
+    D ramp continued to 256 and six noiseless D=256 half-sweep pairs, a
+    converged estimate of the ground-state energy (a variational bound for every
+    run of the same model at D <= 256 up to its own convergence)."""
+    src = open(os.path.join(ROOT, "dmrgcc_b200", "inputs", "chain16_spinless.in")).read()
+    head, _ = src.split("maxm  maxb  niter  canpre  noise")
+    rows = ([(16, 4)] * 2 + [(32, 5)] * 2 + [(64, 6)] * 2 + [(128, 7)] * 2 + [(256, 8)] * 2 + [(256, -1)] * 6)
+    head = head.replace("num_sweep = 6", f"num_sweep = {len(rows) // 2}")
+    text = head + "maxm  maxb  niter  canpre  noise\n" + "\n".join(
+        f"        {m:<5d} 100   100    1E-12   {z}" for m, z in rows) + "\n    }\n}\n"
+    tmp = tempfile.mkdtemp(prefix="golden_conv_")
+    inp = os.path.join(tmp, "chain16_D256.in")
+    with open(inp, "w") as f:
+        f.write(text)
+    model = os.path.join(ROOT, "oracle", "_ref", "real_spinless_bose_square_model")
+    env = dict(os.environ, OMP_NUM_THREADS="1", OPENBLAS_NUM_THREADS="1")
+    r = subprocess.run([model, inp], capture_output=True, text=True, env=env, cwd=tmp, check=True)
+    e = [float(ln.split("=")[1]) for ln in r.stdout.splitlines() if "energy =" in ln]
+    with open(os.path.join(HERE, "converged_chain16.txt"), "w") as f:
+        f.write("# chain16_spinless.in with the D ramp continued to 256 (16->32->64->128->256, then 6 noiseless\n"
+                "# D=256 sweeps), stock reference, 1 BLAS thread: energies of the last two half-sweeps\n")
+        f.write(f"{e[-2]:.12f}\n{e[-1]:.12f}\n")
+
+
 SPINFUL_MODELS = ("spinful4x4", "spinful3x3_periodic_y")
 
 
@@ -367,6 +392,7 @@ def main() -> int:
     ap.add_argument("--scan", action="store_true", help="only the 64-instance U/t scan reference energies")
     ap.add_argument("--spinful", action="store_true", help="only the spinful model fixtures")
     ap.add_argument("--complex", action="store_true", help="only the complex-path (Hofstadter) fixtures")
+    ap.add_argument("--converged", action="store_true", help="only the converged chain16 energy (D=256)")
     ap.add_argument("--reuse", action="append", default=[], metavar="LABEL=DIR",
                     help="for --spread: take run LABEL (stock, pinned, 'seed s') from DIR/log.txt")
     args = ap.parse_args()
@@ -389,6 +415,9 @@ def main() -> int:
         return 0
     if args.complex:
         complex_fixtures()
+        return 0
+    if args.converged:
+        converged_reference()
         return 0
     quicksort_cases()
     tmp = tempfile.mkdtemp(prefix="golden_")
