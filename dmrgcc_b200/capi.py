@@ -67,6 +67,7 @@ _SIGS = {
     "dmrg_heff_destroy": (C.c_int, [_VP]),
     "dmrg_heff_set_split_threshold": (C.c_int, [_VP, C.c_int64]),
     "dmrg_heff_split_iters": (C.c_int, [_VP, _I]),
+    "dmrg_lanczos_set_polish": (C.c_int, [C.c_int]),
     "dmrg_heff_set_graph": (C.c_int, [_VP, C.c_int]),
     "dmrg_heff_sizes": (C.c_int, [_VP, _I64, _I64, _I64]),
     "dmrg_heff_flops": (C.c_int, [_VP, _D, _D]),

@@ -18,6 +18,7 @@
 // matvecs, then the FP64 run above from its Ritz vector (FP64 for the dense
 // branch, the recurrence, reorthogonalisation, the tridiagonal problem and the
 // energy).
+#include <atomic>
 #include <algorithm>
 
 #include "eig.cuh"
@@ -58,6 +59,10 @@ namespace {
 // Convergence of the split-precision phase: |E_i - E_{i-1}| below this (the
 // matvec's relative error is ~1e-6, the Ritz value settles well before).
 constexpr double kSplitPrecision = 1e-9;
+
+// Matvecs of the FP64 run that ends a mixed-precision Lanczos (<= 0: the full
+// run to the reference's convergence; dmrg_lanczos_set_polish).
+std::atomic<int> g_polish{4};
 
 // End of one captured Lanczos iteration: advance the device's iteration
 // counter and keep the loop going while the run has not converged.  The loop is
@@ -300,6 +305,11 @@ extern "C" int dmrg_heff_set_graph(dmrg_heff_t h, int enable) {
     return DMRG_OK;
 }
 
+extern "C" int dmrg_lanczos_set_polish(int iters) {
+    g_polish.store(iters);
+    return DMRG_OK;
+}
+
 extern "C" int dmrg_heff_set_split_threshold(dmrg_heff_t h, int64_t min_psi_dim) {
     if (!h || min_psi_dim < 0) return set_error(DMRG_E_ARG, "invalid split threshold");
     h->split_min_dim = min_psi_dim;
@@ -331,8 +341,11 @@ extern "C" int dmrg_lanczos(dmrg_heff_t hp, double* psi, int niter, double preci
         return krylov(h, psi, niter, precision, zero_tol, false, energy, iters);
     }
     // Mixed precision: a Krylov run on split-precision matvecs until the Ritz
-    // value settles at the split arithmetic's resolution, then the FP64 run of
-    // the reference from that Ritz vector, which fixes the energy and the state.
+    // value settles at the split arithmetic's resolution, then an FP64 Krylov
+    // run from that Ritz vector: a short one of g_polish matvecs (its lowest
+    // Ritz value is the energy, with an error quadratic in the split vector's,
+    // and its Ritz vector the state), or with g_polish <= 0 the reference's
+    // full run to its own convergence.
     double e_split = 0.0;
     int it_split = 0;
     DMRG_TRY(krylov(h, psi, niter, kSplitPrecision, zero_tol, true, &e_split, &it_split));
@@ -340,7 +353,9 @@ extern "C" int dmrg_lanczos(dmrg_heff_t hp, double* psi, int niter, double preci
     const int blocks = (int)std::min<int64_t>((n + kVecThreads - 1) / kVecThreads, 2 * h.ctx->num_sms);
     DMRG_TRY(vec_normalize(psi, n, w.scal.as<double>() + 4 * niter, w.rs, blocks, h.ctx->stream));
     int it_fp64 = 0;
-    DMRG_TRY(krylov(h, psi, niter, precision, zero_tol, false, energy, &it_fp64));
+    const int polish = g_polish.load();
+    DMRG_TRY(krylov(h, psi, polish > 0 ? std::min(polish, niter) : niter, precision, zero_tol, false, energy,
+                    &it_fp64));
     w.split_iters = it_split;
     if (iters) *iters = it_fp64;
     return DMRG_OK;

@@ -13,14 +13,15 @@
 // vectors of one complex value differ by a factor i.  The complex triplets are
 // recovered on the host: runs of equal singular values (to 1e-9 of the
 // largest) are one complex eigenspace, in which the real columns, taken as
-// complex vectors and first orthogonalised against every vector kept so far,
-// are taken in order by Gram-Schmidt with complex coefficients (the same
-// coefficients on the right vectors keep A v = sigma u) whenever more than half
-// a vector's norm remains, until the run's complex dimension (half its length)
-// is reached; a degenerate run that falls short is filled with the largest
-// remainders.  Truncation is
-// the reference's rule on the complex singular values; the new ket takes U (left)
-// or V^H (right) rows, the canonical tensor S V^H or U S, like the reference.
+// complex vectors of the side that becomes the new ket (U for a left, V for a
+// right canonicalisation) and first orthogonalised against every vector kept
+// so far, are taken in order by Gram-Schmidt with complex coefficients whenever
+// more than half a vector's norm remains, until the run's complex dimension
+// (half its length) is reached; a degenerate run that falls short is filled
+// with the largest remainders.  Truncation is the reference's rule on the
+// complex singular values; the new ket takes U (left) or V^H (right) rows, the
+// canonical tensor the projection U^H A = S V^H or A V = U S, like the
+// reference.
 // The signs (phases) of singular vectors are free, as with zgesdd; only
 // gauge-invariant products are comparable.
 #include <algorithm>
@@ -125,77 +126,76 @@ int recover_triplets(dmrg_zcanon_s& c, int s, cudaStream_t st) {
             for (int i = 0; i < 2 * m; ++i) u[i] = Q[(size_t)k * p.cols + i];
         }
     };
-    std::vector<cplx>& Us = c.U[s];
-    std::vector<cplx>& Vs = c.V[s];
-    Us.assign((size_t)m * r, cplx(0.0, 0.0));
-    Vs.assign((size_t)n * r, cplx(0.0, 0.0));
+    // the side that becomes the new ket (U for a left, V for a right
+    // canonicalisation) is made orthonormal; the canonical factor is then the
+    // projection of the sector matrix on it (dmrg_zcanon_write)
+    const bool left = c.side == 0;
+    const int d = left ? m : n;
+    std::vector<cplx>& P = left ? c.U[s] : c.V[s];
+    (left ? c.V[s] : c.U[s]).clear();
+    P.assign((size_t)d * r, cplx(0.0, 0.0));
     std::vector<double>& out = c.sv[s];
     out.assign(r, 0.0);
     int kept = 0;
     const double tol = 1e-9 * std::max(sig.empty() ? 0.0 : sig[0], 1e-300);
     std::vector<double> u, v;
-    // removes from (cu, cv) its components along the kept vectors [from, to)
-    // (complex coefficients on U; the same coefficients on V keep A v = sigma u)
-    auto project = [&](std::vector<cplx>& cu, std::vector<cplx>& cv, int from, int to) {
+    // removes from x its components along the kept vectors [from, to)
+    auto project = [&](std::vector<cplx>& x, int from, int to) {
         for (int q = from; q < to; ++q) {
-            const cplx* uq = &Us[(size_t)q * m];
-            const cplx* vq = &Vs[(size_t)q * n];
+            const cplx* pq = &P[(size_t)q * d];
             cplx a(0.0, 0.0);
-            for (int i = 0; i < m; ++i) a += std::conj(uq[i]) * cu[i];
-            for (int i = 0; i < m; ++i) cu[i] -= a * uq[i];
-            for (int i = 0; i < n; ++i) cv[i] -= a * vq[i];
+            for (int i = 0; i < d; ++i) a += std::conj(pq[i]) * x[i];
+            for (int i = 0; i < d; ++i) x[i] -= a * pq[i];
         }
     };
     for (int j0 = 0; j0 < r2 && kept < r;) {
         int j1 = j0 + 1;
         while (j1 < r2 && sig[j1 - 1] - sig[j1] <= tol) ++j1;
         const int want = std::min(r - kept, (j1 - j0 + 1) / 2);
-        // the run's real pairs as complex vectors, orthogonalised (two passes)
-        // against every vector kept so far: vectors of nearby runs are complex-
-        // orthogonal only to eps ||A|| / gap
-        std::vector<std::vector<cplx>> cu, cv;
+        // the run's real singular vectors as complex vectors, orthogonalised (two
+        // passes) against every vector kept so far: vectors of nearby runs are
+        // complex-orthogonal only to eps ||A|| / gap
+        std::vector<std::vector<cplx>> cx;
         std::vector<double> cs;
         for (int j = j0; j < j1; ++j) {
             if (sig[j] <= 0.0) break;
             real_pair(j, u, v);
-            cu.emplace_back(m);
-            cv.emplace_back(n);
-            for (int i = 0; i < m; ++i) cu.back()[i] = cplx(u[i], u[m + i]);
-            for (int i = 0; i < n; ++i) cv.back()[i] = cplx(v[i], v[n + i]);
+            const std::vector<double>& x = left ? u : v;
+            cx.emplace_back(d);
+            for (int i = 0; i < d; ++i) cx.back()[i] = cplx(x[i], x[d + i]);
             cs.push_back(sig[j]);
-            for (int pass = 0; pass < 2; ++pass) project(cu.back(), cv.back(), 0, kept);
+            for (int pass = 0; pass < 2; ++pass) project(cx.back(), 0, kept);
         }
         // in descending order, a candidate whose remainder keeps more than half
         // its norm is a new complex direction (the other real vector of a
         // complex pair is the i-multiple of the first: remainder ~0); should a
         // degenerate run not reach its complex dimension that way, the largest
         // remainders fill it (pivoted Gram-Schmidt)
-        std::vector<char> taken(cu.size(), 0);
+        std::vector<char> taken(cx.size(), 0);
         const int first = kept;
+        auto norm2 = [&](int k) {
+            double x = 0.0;
+            for (int i = 0; i < d; ++i) x += std::norm(cx[k][i]);
+            return x;
+        };
         auto take = [&](int k, double nrm2) {
             taken[k] = 1;
             const double nrm = std::sqrt(nrm2);
-            for (int i = 0; i < m; ++i) Us[(size_t)kept * m + i] = cu[k][i] / nrm;
-            for (int i = 0; i < n; ++i) Vs[(size_t)kept * n + i] = cv[k][i] / nrm;
+            for (int i = 0; i < d; ++i) P[(size_t)kept * d + i] = cx[k][i] / nrm;
             out[kept] = cs[k];
             ++kept;
-            for (size_t k2 = 0; k2 < cu.size(); ++k2)
+            for (size_t k2 = 0; k2 < cx.size(); ++k2)
                 if (!taken[k2])
-                    for (int pass = 0; pass < 2; ++pass) project(cu[k2], cv[k2], kept - 1, kept);
+                    for (int pass = 0; pass < 2; ++pass) project(cx[k2], kept - 1, kept);
         };
-        auto norm2 = [&](int k) {
-            double x = 0.0;
-            for (int i = 0; i < m; ++i) x += std::norm(cu[k][i]);
-            return x;
-        };
-        for (size_t k = 0; k < cu.size() && kept - first < want; ++k) {
+        for (size_t k = 0; k < cx.size() && kept - first < want; ++k) {
             const double x = norm2((int)k);
             if (x > 0.5) take((int)k, x);
         }
         while (kept - first < want) {
             int best = -1;
             double bn = 0.0;
-            for (size_t k = 0; k < cu.size(); ++k) {
+            for (size_t k = 0; k < cx.size(); ++k) {
                 if (taken[k]) continue;
                 const double x = norm2((int)k);
                 if (x > bn) {
@@ -206,19 +206,17 @@ int recover_triplets(dmrg_zcanon_s& c, int s, cudaStream_t st) {
             if (best < 0 || bn <= 1e-6) break;  // no further independent direction in the run
             take(best, bn);
         }
-        // the run's triplets in descending order of their values
+        // the run's vectors in descending order of their values
         std::vector<int> ord(kept - first);
         for (int k = 0; k < kept - first; ++k) ord[k] = first + k;
         std::stable_sort(ord.begin(), ord.end(), [&](int x, int y) { return out[x] > out[y]; });
-        std::vector<cplx> tu((size_t)(kept - first) * m), tv((size_t)(kept - first) * n);
+        std::vector<cplx> tp((size_t)(kept - first) * d);
         std::vector<double> to(kept - first);
         for (int k = 0; k < kept - first; ++k) {
-            std::copy_n(&Us[(size_t)ord[k] * m], m, &tu[(size_t)k * m]);
-            std::copy_n(&Vs[(size_t)ord[k] * n], n, &tv[(size_t)k * n]);
+            std::copy_n(&P[(size_t)ord[k] * d], d, &tp[(size_t)k * d]);
             to[k] = out[ord[k]];
         }
-        std::copy(tu.begin(), tu.end(), Us.begin() + (size_t)first * m);
-        std::copy(tv.begin(), tv.end(), Vs.begin() + (size_t)first * n);
+        std::copy(tp.begin(), tp.end(), P.begin() + (size_t)first * d);
         std::copy(to.begin(), to.end(), out.begin() + first);
         j0 = j1;
     }
@@ -392,33 +390,54 @@ int dmrg_zcanon_write(dmrg_zcanon_t c, const double* ket_dev, double* new_ket_de
     for (int sct = 0; sct < c->nsec; ++sct) {
         const bool act = c->svd.active(sct);
         const int t = c->tdim[sct], m = c->sec_m[sct], n = c->sec_n[sct], rk = act ? c->rank[sct] : 0;
-        const auto& U = c->U[sct];
-        const auto& V = c->V[sct];
-        auto u = [&](int i, int k) { return k < rk ? U[(size_t)k * m + i] : cplx(0.0, 0.0); };
-        auto v = [&](int i, int k) { return k < rk ? V[(size_t)k * n + i] : cplx(0.0, 0.0); };
+        const bool left = c->side == 0;
+        const auto& P = left ? c->U[sct] : c->V[sct];  // orthonormal ket-side vectors, column k contiguous
+        const int d = left ? m : n;
+        auto pv = [&](int i, int k) { return k < rk ? P[(size_t)k * d + i] : cplx(0.0, 0.0); };
+        // the sector matrix A (m x n, row-major; blocks stacked, short blocks zero-padded)
+        std::vector<cplx> A;
+        if (act) A.assign((size_t)m * n, cplx(0.0, 0.0));
         int acc = 0;
         for (int pos : c->members[sct]) {
             const int64_t o = c->new_ket.off[pos], oo = c->ket.off[pos];
             const int rows = c->new_ket.rows[pos], cols = c->new_ket.cols[pos];
+            const int krows = c->ket.rows[pos], kcols = c->ket.cols[pos];
+            if (act)
+                for (int i = 0; i < krows; ++i)
+                    for (int j = 0; j < kcols; ++j)
+                        A[left ? (size_t)(acc + i) * n + j : (size_t)i * n + acc + j] = old[(size_t)oo + (size_t)i * kcols + j];
             for (int i = 0; i < rows; ++i)
                 for (int j = 0; j < cols; ++j) {
                     cplx x;
                     if (!act) x = old[(size_t)oo + (size_t)i * cols + j];  // untouched (empty sector)
-                    else if (c->side == 0) x = u(acc + i, j);                 // U rows of the block
-                    else x = std::conj(v(acc + j, i));                       // V^H columns of the block
+                    else if (left) x = pv(acc + i, j);                    // U rows of the block
+                    else x = std::conj(pv(acc + j, i));                   // V^H columns of the block
                     nk[(size_t)o + (size_t)i * cols + j] = x;
                 }
-            acc += c->side == 0 ? c->ket.rows[pos] : c->ket.cols[pos];
+            acc += left ? krows : kcols;
         }
         const int64_t co = c->canonical.off[sct];
         const auto& f = c->forced[sct];
         if (!act) continue;  // zero block
-        if (c->side == 0)    // diag(s) V^H : t x n
-            for (int i = 0; i < t; ++i)
-                for (int j = 0; j < n; ++j) can[(size_t)co + (size_t)i * n + j] = f[i] * std::conj(v(j, i));
-        else                 // U diag(s) : m x t
+        // canonical factor: U^H A (t x n) or A V (m x t), i.e. S V^H or U S; rows
+        // (columns) whose value the truncation forced to zero stay zero
+        if (left)
+            for (int k = 0; k < t; ++k) {
+                if (f[k] == 0.0) continue;
+                for (int j = 0; j < n; ++j) {
+                    cplx x(0.0, 0.0);
+                    for (int i = 0; i < m; ++i) x += std::conj(pv(i, k)) * A[(size_t)i * n + j];
+                    can[(size_t)co + (size_t)k * n + j] = x;
+                }
+            }
+        else
             for (int i = 0; i < m; ++i)
-                for (int j = 0; j < t; ++j) can[(size_t)co + (size_t)i * t + j] = u(i, j) * f[j];
+                for (int k = 0; k < t; ++k) {
+                    if (f[k] == 0.0) continue;
+                    cplx x(0.0, 0.0);
+                    for (int j = 0; j < n; ++j) x += A[(size_t)i * n + j] * pv(j, k);
+                    can[(size_t)co + (size_t)i * t + k] = x;
+                }
     }
     if (!nk.empty())
         DMRG_CUDA_TRY(cudaMemcpyAsync(new_ket_dev, nk.data(), nk.size() * sizeof(cplx), cudaMemcpyHostToDevice, st));

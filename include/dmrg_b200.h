@@ -182,11 +182,16 @@ int dmrg_heff_apply_noalloc(int num_left_sector, int num_right_sector, const int
 int dmrg_lanczos(dmrg_heff_t h, double* psi_dev, int niter, double precision, double zero_tol,
                  double* energy, int* iters);
 /* For a split-precision operator (DMRG_PREC_TF32X3 / BF16X3), dmrg_lanczos runs
- * a Krylov phase on split-precision matvecs and then the FP64 Lanczos from its
+ * a Krylov phase on split-precision matvecs and then an FP64 Krylov run from its
  * Ritz vector, when psi_dim >= min_psi_dim (default 200000: below it the split
  * matvec is not enough faster to pay for two phases and the FP64 run is used
  * alone).  No reference counterpart (the reference has FP64 only). */
 int dmrg_heff_set_split_threshold(dmrg_heff_t h, int64_t min_psi_dim);
+/* Length of that FP64 run, process-wide: iters > 0 (default 4) FP64 matvecs,
+ * whose lowest Ritz value is the energy (its error quadratic in the split
+ * vector's) and whose Ritz vector the state; iters <= 0: the FP64 Lanczos to the
+ * reference's own convergence. */
+int dmrg_lanczos_set_polish(int iters);
 /* Krylov dimension of the split phase of the last dmrg_lanczos call (0 when it
  * ran FP64 only). */
 int dmrg_heff_split_iters(dmrg_heff_t h, int* iters);
