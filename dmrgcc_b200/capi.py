@@ -118,6 +118,7 @@ _SIGS = {
     "dmrg_model_destroy": (C.c_int, [_VP]),
     "dmrg_model_info": (C.c_int, [_VP, _I, _I, _I]),
     "dmrg_model_mpo": (C.c_int, [_VP, C.c_int, _I, _I, C.c_int, _D]),
+    "dmrg_model_is_complex": (C.c_int, [_VP, _I]),
     "dmrg_model_quantum_table": (C.c_int, [_VP, C.c_int, C.c_int, C.c_int, _I, _I]),
     "dmrg_env_create": (C.c_int, [_VP, C.c_int, C.c_int, C.c_int, _I, C.POINTER(Blocks), C.c_int, C.c_int, C.c_int,
                                   _D, C.POINTER(Blocks), C.c_int, C.POINTER(_VP)]),
@@ -645,13 +646,19 @@ class Model:
         a, b, c = C.c_int(), C.c_int(), C.c_int()
         check(lib().dmrg_model_info(h, C.byref(a), C.byref(b), C.byref(c)), "dmrg_model_info")
         self.num_site, self.physics_dim, self.num_quantum = a.value, b.value, c.value
+        z = C.c_int()
+        check(lib().dmrg_model_is_complex(h, C.byref(z)), "dmrg_model_is_complex")
+        self.is_complex = bool(z.value)
 
     def mpo(self, site: int) -> np.ndarray:
+        """W[l][r][p1][p2] (complex128 for a complex model)."""
         lb, rb = C.c_int(), C.c_int()
         check(lib().dmrg_model_mpo(self.h, site, C.byref(lb), C.byref(rb), 0, None), "dmrg_model_mpo")
         d = self.physics_dim
-        w = np.zeros(lb.value * rb.value * d * d)
+        w = np.zeros(lb.value * rb.value * d * d * (2 if self.is_complex else 1))
         check(lib().dmrg_model_mpo(self.h, site, C.byref(lb), C.byref(rb), w.size, _dptr(w)), "dmrg_model_mpo")
+        if self.is_complex:
+            w = w.view(np.complex128)
         return w.reshape(lb.value, rb.value, d, d)
 
     def quantum_table(self, which: int, bond: int) -> np.ndarray:

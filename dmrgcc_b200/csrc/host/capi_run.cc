@@ -22,15 +22,16 @@ namespace {
 
 struct ModelSpec {
     std::unique_ptr<QuantumSpace> space;
-    std::unique_ptr<RealTensorHamiltonian> ham;
+    std::unique_ptr<MpoHamiltonian> ham;
 };
 
 // The model executables' main() (model/real_spinless_bose_square_model.cc:11-35):
 // read the model keys and build the space and the Hamiltonian.
 ModelSpec make_model(InputGroup& input, const std::string& model) {
     ModelSpec m;
-    if (model == "real_spinful_bose_square") {
-        // model/complex_spinful_bose_square_model.cc:11-45 (same keys), real tensors
+    if (model == "real_spinful_bose_square" || model == "complex_spinful_bose_square") {
+        // model/complex_spinful_bose_square_model.cc:11-45 (same keys); the real
+        // form needs flux 0, the complex one is the reference's model
         const int nx = input.getInt("num_site_x");
         const int ny = input.getInt("num_site_y");
         const int d = input.getInt("physics_dim", 2);
@@ -43,12 +44,16 @@ ModelSpec make_model(InputGroup& input, const std::string& model) {
         const double mu = input.getDouble("mu");
         const double u[3] = {input.getDouble("U_uu"), input.getDouble("U_dd"), input.getDouble("U_ud")};
         m.space.reset(new RealSpinfulBoseSquareSpace(nx, ny, nb, d));
-        m.ham.reset(new RealSpinfulBoseSquareHamiltonian(nx, ny, d, flux, jx, jy, u, mu, px, py));
+        if (model == "complex_spinful_bose_square")
+            m.ham.reset(new ComplexSpinfulBoseSquareHamiltonian(nx, ny, d, flux, jx, jy, u, mu, px, py));
+        else
+            m.ham.reset(new RealSpinfulBoseSquareHamiltonian(nx, ny, d, flux, jx, jy, u, mu, px, py));
         return m;
     }
     if (model != "real_spinless_bose_square")
         throw std::runtime_error("unknown model '" + model +
-                                 "' (supported: real_spinless_bose_square, real_spinful_bose_square)");
+                                 "' (supported: real_spinless_bose_square, real_spinful_bose_square, "
+                                 "complex_spinful_bose_square)");
     const int nx = input.getInt("num_site_x");
     const int ny = input.getInt("num_site_y");
     const int nb = input.getInt("num_boson");
@@ -230,13 +235,21 @@ int dmrg_model_info(dmrg_model_t m, int* num_site, int* physics_dim, int* num_qu
 
 int dmrg_model_mpo(dmrg_model_t m, int site, int* left_bond, int* right_bond, int cap, double* W) {
     if (!m || !left_bond || !right_bond) return set_error(DMRG_E_ARG, "null argument");
-    if (site < 0 || site >= m->spec.ham->num_site()) return set_error(DMRG_E_ARG, "site out of range");
-    const RealTensorOperator& op = m->spec.ham->get_tensor_hamiltonian(site);
-    *left_bond = op.get_left_bond();
-    *right_bond = op.get_right_bond();
-    const auto& v = op.data();
+    const MpoHamiltonian& h = *m->spec.ham;
+    if (site < 0 || site >= h.num_site()) return set_error(DMRG_E_ARG, "site out of range");
+    *left_bond = h.left_bond(site);
+    *right_bond = h.right_bond(site);
+    const int d = h.physics_dim(site);
+    const int64_t n = (int64_t)*left_bond * *right_bond * d * d * (h.is_complex() ? 2 : 1);
+    const double* v = h.values(site);
     if (W)
-        for (int i = 0; i < (int)v.size() && i < cap; ++i) W[i] = v[i];
+        for (int64_t i = 0; i < n && i < cap; ++i) W[i] = v[i];
+    return DMRG_OK;
+}
+
+int dmrg_model_is_complex(dmrg_model_t m, int* is_complex) {
+    if (!m || !is_complex) return set_error(DMRG_E_ARG, "null argument");
+    *is_complex = m->spec.ham->is_complex() ? 1 : 0;
     return DMRG_OK;
 }
 

@@ -12,6 +12,7 @@
 #include <thread>
 
 #include "gemm.cuh"
+#include "zgemm.cuh"
 
 extern "C" {
 int dmrg_canon_create(dmrg_ctx_t, int, int, int, const int*, const int*, const dmrg_blocks_t*, dmrg_canon_t*);
@@ -20,6 +21,12 @@ int dmrg_canon_run(dmrg_canon_t, const double*, int, double, int*, double*);
 int dmrg_canon_out_info(dmrg_canon_t, int64_t*, int64_t*, int*);
 int dmrg_canon_out_blocks(dmrg_canon_t, int*, int*, int*, int*, int*);
 int dmrg_canon_write(dmrg_canon_t, const double*, double*, double*);
+int dmrg_zcanon_create(dmrg_ctx_t, int, int, int, const int*, const int*, const dmrg_blocks_t*, dmrg_zcanon_t*);
+int dmrg_zcanon_destroy(dmrg_zcanon_t);
+int dmrg_zcanon_run(dmrg_zcanon_t, const double*, int, double, int*, double*);
+int dmrg_zcanon_out_info(dmrg_zcanon_t, int64_t*, int64_t*, int*);
+int dmrg_zcanon_out_blocks(dmrg_zcanon_t, int*, int*, int*, int*, int*);
+int dmrg_zcanon_write(dmrg_zcanon_t, const double*, double*, double*);
 }
 
 namespace dmrg {
@@ -45,6 +52,23 @@ void random_block(GlibcRand& rng, long long& draws, std::vector<double>& out, si
         for (int i = 0; i < rows; ++i) out[off + (size_t)i * cols + j] = 0.01 * (rng.next() % 100);
 }
 
+// ComplexMatrix::RandomMatrix (src/tensor/complex_matrix.cc:201-209): the same
+// column-major walk, each element Complex(0.01 * (rand() % 100), 0.01 *
+// (rand() % 100)); the reference's compiler (g++, x86-64) evaluates the
+// constructor's arguments right to left, so the imaginary part takes the
+// first draw.  Interleaved (re, im) into a rows x cols row-major block.
+void random_block_complex(GlibcRand& rng, long long& draws, std::vector<double>& out, size_t off, int rows,
+                          int cols) {
+    draws += 2LL * rows * cols;
+    for (int j = 0; j < cols; ++j)
+        for (int i = 0; i < rows; ++i) {
+            const double im = 0.01 * (rng.next() % 100);
+            const double re = 0.01 * (rng.next() % 100);
+            out[2 * (off + (size_t)i * cols + j)] = re;
+            out[2 * (off + (size_t)i * cols + j) + 1] = im;
+        }
+}
+
 int find_value(const std::vector<int>& v, int x) {
     for (int i = 0; i < (int)v.size(); ++i)
         if (v[i] == x) return i;
@@ -53,19 +77,23 @@ int find_value(const std::vector<int>& v, int x) {
 
 }  // namespace
 
-int DevBlocks::alloc(cudaStream_t st, bool zero) {
-    DMRG_TRY(buf.alloc((size_t)std::max<int64_t>(d.size, 1) * sizeof(double)));
-    if (zero && d.size) DMRG_CUDA_TRY(cudaMemsetAsync(buf.ptr, 0, (size_t)d.size * sizeof(double), st));
+int DevBlocks::alloc(cudaStream_t st, bool zero, int ew) {
+    DMRG_TRY(buf.alloc((size_t)std::max<int64_t>(d.size, 1) * ew * sizeof(double)));
+    if (zero && d.size) DMRG_CUDA_TRY(cudaMemsetAsync(buf.ptr, 0, (size_t)d.size * ew * sizeof(double), st));
     return DMRG_OK;
 }
 
 // ---------------------------------------------------------------------------
 // construction: RealTensorRundmrg::RealTensorRundmrg + Sweep (real_tensor_rundmrg.cc:3-113)
 // ---------------------------------------------------------------------------
-Engine::Engine(dmrg_ctx_t ctx, std::unique_ptr<QuantumSpace> space, std::unique_ptr<RealTensorHamiltonian> ham,
+Engine::Engine(dmrg_ctx_t ctx, std::unique_ptr<QuantumSpace> space, std::unique_ptr<MpoHamiltonian> ham,
                InputGroup& input, const RunOptions& opt)
     : ctx_(ctx), st_(ctx->stream), opt_(opt), space_(std::move(space)), ham_(std::move(ham)) {
     n_ = space_->num_site();
+    cplx_ = ham_->is_complex();
+    ew_ = cplx_ ? 2 : 1;
+    if (cplx_ && (opt_.two_site || opt_.precision != DMRG_PREC_FP64))
+        throw StatusError(DMRG_E_ARG, "a complex run has single-site FP64 sweeps only");
     // disk_cache (tensors swapped to files between uses) is read for compatibility
     // and ignored: every tensor stays resident.  cache_record / cache_resume
     // write and read the reference's checkpoint file (real_tensor_rundmrg.cc:16-23).
@@ -131,11 +159,11 @@ Engine::Engine(dmrg_ctx_t ctx, std::unique_ptr<QuantumSpace> space, std::unique_
     for (int i = 0; i <= n_; ++i) {
         con_[i].reset(new TensorContraction());
         if (i < n_) {
-            con_[i]->left_bond = ham_->get_tensor_hamiltonian(i).get_left_bond();
-            con_[i]->right_bond = ham_->get_tensor_hamiltonian(i).get_right_bond();
+            con_[i]->left_bond = ham_->left_bond(i);
+            con_[i]->right_bond = ham_->right_bond(i);
         } else {
-            con_[i]->left_bond = ham_->get_tensor_hamiltonian(n_ - 1).get_right_bond();
-            con_[i]->right_bond = ham_->get_tensor_hamiltonian(0).get_left_bond();
+            con_[i]->left_bond = ham_->right_bond(n_ - 1);
+            con_[i]->right_bond = ham_->left_bond(0);
         }
         con_[i]->L.desc.o.assign(con_[i]->left_bond, BlockListDesc());
         con_[i]->L.desc.rebase();
@@ -158,7 +186,7 @@ void Engine::Trace(const char* tag, int leigh, int site) {
     std::fprintf(trace_, " R:");
     for (int d : t.right_dim) std::fprintf(trace_, "%d,", d);
     auto fetch = [&](const DevBlocks& b, std::vector<double>& h) {
-        h.assign((size_t)b.d.size, 0.0);
+        h.assign((size_t)b.d.size * ew_, 0.0);
         if (!h.empty() &&
             (cudaMemcpyAsync(h.data(), b.ptr(), h.size() * sizeof(double), cudaMemcpyDeviceToHost, st_) != cudaSuccess ||
              cudaStreamSynchronize(st_) != cudaSuccess))
@@ -174,8 +202,8 @@ void Engine::Trace(const char* tag, int leigh, int site) {
         std::fprintf(trace_, " S:");
         for (int k = 0; k < t.canonical.d.count(); ++k) {
             double s2 = 0.0;
-            for (int64_t i = 0; i < (int64_t)t.canonical.d.rows[k] * t.canonical.d.cols[k]; ++i)
-                s2 += h[t.canonical.d.off[k] + i] * h[t.canonical.d.off[k] + i];
+            for (int64_t i = 0; i < (int64_t)t.canonical.d.rows[k] * t.canonical.d.cols[k] * ew_; ++i)
+                s2 += h[t.canonical.d.off[k] * ew_ + i] * h[t.canonical.d.off[k] * ew_ + i];
             std::fprintf(trace_, "%.8e,", s2);
         }
     }
@@ -239,10 +267,13 @@ int Engine::DefineLatticeBlocks(TensorLattice& t, const std::vector<int>& li, co
         t.phys[(size_t)li[k] * t.nr() + ri[k]] = pi[k];
         t.ket.d.push(li[k], ri[k], row, column);
     }
-    std::vector<double> host((size_t)std::max<int64_t>(t.ket.d.size, 0));
-    for (size_t k = 0; k < li.size(); ++k) random_block(rng_, rand_draws_, host, (size_t)t.ket.d.off[k], row, column);
+    std::vector<double> host((size_t)std::max<int64_t>(t.ket.d.size, 0) * ew_);
+    for (size_t k = 0; k < li.size(); ++k) {
+        if (cplx_) random_block_complex(rng_, rand_draws_, host, (size_t)t.ket.d.off[k], row, column);
+        else random_block(rng_, rand_draws_, host, (size_t)t.ket.d.off[k], row, column);
+    }
     if (!device) return DMRG_OK;  // the draws only advance the stream (the caller discards the values)
-    DMRG_TRY(t.ket.alloc(st_, false));
+    DMRG_TRY(t.ket.alloc(st_, false, ew_));
     if (!host.empty())
         DMRG_CUDA_TRY(cudaMemcpyAsync(t.ket.ptr(), host.data(), host.size() * sizeof(double), cudaMemcpyHostToDevice,
                                       st_));
@@ -282,31 +313,39 @@ int Engine::CanonicalTensorSpace(int leigh, int site, double* discarded) {
     TensorLattice& t = *lat_[site];
     dmrg_blocks_t kb = as_blocks(t.ket.d);
     dmrg_canon_t c = nullptr;
-    DMRG_TRY(dmrg_canon_create(ctx_, leigh, t.nl(), t.nr(), t.left_dim.data(), t.right_dim.data(), &kb, &c));
+    dmrg_zcanon_t zc = nullptr;  // complex run: ComplexTensorLattice::Left/RightCanonicalTensorLattice
+    if (cplx_) DMRG_TRY(dmrg_zcanon_create(ctx_, leigh, t.nl(), t.nr(), t.left_dim.data(), t.right_dim.data(), &kb, &zc));
+    else DMRG_TRY(dmrg_canon_create(ctx_, leigh, t.nl(), t.nr(), t.left_dim.data(), t.right_dim.data(), &kb, &c));
     const int nsec = leigh == 0 ? t.nr() : t.nl();
     std::vector<int> tdim(nsec);
     double disc = 0.0;
-    int rc = dmrg_canon_run(c, t.ket.ptr(), p_max_dim_, p_canpre_, tdim.data(), &disc);
+    int rc = cplx_ ? dmrg_zcanon_run(zc, t.ket.ptr(), p_max_dim_, p_canpre_, tdim.data(), &disc)
+                   : dmrg_canon_run(c, t.ket.ptr(), p_max_dim_, p_canpre_, tdim.data(), &disc);
     int64_t ks = 0, cs = 0;
     int sweeps = 0;
-    if (rc == DMRG_OK) rc = dmrg_canon_out_info(c, &ks, &cs, &sweeps);
+    if (rc == DMRG_OK) rc = cplx_ ? dmrg_zcanon_out_info(zc, &ks, &cs, &sweeps) : dmrg_canon_out_info(c, &ks, &cs, &sweeps);
     svd_sweeps_ += sweeps;
     const int nb = t.ket.d.count();
     std::vector<int> kr(std::max(nb, 1)), kc(std::max(nb, 1)), cr(nsec), cc(nsec), md(nsec);
-    if (rc == DMRG_OK) rc = dmrg_canon_out_blocks(c, kr.data(), kc.data(), cr.data(), cc.data(), md.data());
+    if (rc == DMRG_OK)
+        rc = cplx_ ? dmrg_zcanon_out_blocks(zc, kr.data(), kc.data(), cr.data(), cc.data(), md.data())
+                   : dmrg_canon_out_blocks(c, kr.data(), kc.data(), cr.data(), cc.data(), md.data());
     DevBlocks nk, can;
     if (rc == DMRG_OK) {
         for (int k = 0; k < nb; ++k) nk.d.push(t.ket.d.left[k], t.ket.d.right[k], kr[k], kc[k]);
         for (int s = 0; s < nsec; ++s) can.d.push(s, s, cr[s], cc[s]);
-        rc = nk.alloc(st_, false);
-        if (rc == DMRG_OK) rc = can.alloc(st_, false);
-        if (rc == DMRG_OK) rc = dmrg_canon_write(c, t.ket.ptr(), nk.ptr(), can.ptr());
+        rc = nk.alloc(st_, false, ew_);
+        if (rc == DMRG_OK) rc = can.alloc(st_, false, ew_);
+        if (rc == DMRG_OK)
+            rc = cplx_ ? dmrg_zcanon_write(zc, t.ket.ptr(), nk.ptr(), can.ptr())
+                       : dmrg_canon_write(c, t.ket.ptr(), nk.ptr(), can.ptr());
         if (rc == DMRG_OK) {
             cudaError_t e = cudaStreamSynchronize(st_);
             if (e != cudaSuccess) rc = set_error(DMRG_E_CUDA, "canonical write: %s", cudaGetErrorString(e));
         }
     }
-    dmrg_canon_destroy(c);
+    if (cplx_) dmrg_zcanon_destroy(zc);
+    else dmrg_canon_destroy(c);
     DMRG_TRY(rc);
     t.ket = std::move(nk);
     t.canonical = std::move(can);
@@ -322,8 +361,10 @@ int Engine::CanonicalTensorSpace(int leigh, int site, double* discarded) {
 int Engine::Normalize(TensorLattice& t) {
     if (t.ket.d.size == 0) return DMRG_OK;
     DMRG_TRY(norm_.alloc(8 * sizeof(double)));
-    const int blocks = (int)std::min<int64_t>((t.ket.d.size + 255) / 256, 2 * ctx_->num_sms);
-    return vec_normalize(t.ket.ptr(), t.ket.d.size, norm_.as<double>(), rs_, blocks, st_);
+    // the norm of a complex vector is that of its interleaved doubles
+    const int64_t n = t.ket.d.size * ew_;
+    const int blocks = (int)std::min<int64_t>((n + 255) / 256, 2 * ctx_->num_sms);
+    return vec_normalize(t.ket.ptr(), n, norm_.as<double>(), rs_, blocks, st_);
 }
 
 // RealTensorSpace::MergeTensorSpace -> RealTensorLattice::Left/RightMergeTensorLattice
@@ -349,10 +390,21 @@ int Engine::MergeTensorSpace(int leigh, int site) {
             nk.d.push(l, r, kr, cc);
         }
     }
-    DMRG_TRY(nk.alloc(st_, true));
+    DMRG_TRY(nk.alloc(st_, true, ew_));
+    ZGemmSchedule zs;  // complex run: ComplexMatrix::MultiplyToMatrix (zgemm)
     for (int k = 0; k < nb; ++k) {
         const int sec = leigh == 0 ? t.ket.d.left[k] : t.ket.d.right[k];
         if (nk.d.rows[k] == 0 || nk.d.cols[k] == 0) continue;
+        if (cplx_) {
+            zs.add_group(nk.d.off[k], nk.d.cols[k], nk.d.rows[k], nk.d.cols[k]);
+            if (leigh == 0)
+                zs.add_term(o.canonical.d.off[sec], o.canonical.d.cols[sec], t.ket.d.off[k], t.ket.d.cols[k],
+                            o.canonical.d.cols[sec], 1.0, 0.0);
+            else
+                zs.add_term(t.ket.d.off[k], t.ket.d.cols[k], o.canonical.d.off[sec], o.canonical.d.cols[sec],
+                            t.ket.d.cols[k], 1.0, 0.0);
+            continue;
+        }
         s.add_group(nk.d.off[k], nk.d.cols[k], nk.d.rows[k], nk.d.cols[k]);
         if (leigh == 0)
             s.add_term(o.canonical.d.off[sec], o.canonical.d.cols[sec], t.ket.d.off[k], t.ket.d.cols[k],
@@ -361,11 +413,19 @@ int Engine::MergeTensorSpace(int leigh, int site) {
             s.add_term(t.ket.d.off[k], t.ket.d.cols[k], o.canonical.d.off[sec], o.canonical.d.cols[sec],
                        t.ket.d.cols[k], 1.0);
     }
-    if (leigh == 0) DMRG_TRY(s.check_bounds(o.canonical.d.size, t.ket.d.size, nk.d.size));
-    else DMRG_TRY(s.check_bounds(t.ket.d.size, o.canonical.d.size, nk.d.size));
-    DMRG_TRY(s.finalize(64, 64, 16, st_));
-    if (leigh == 0) DMRG_TRY(launch_gemm_f64(s, o.canonical.ptr(), t.ket.ptr(), nk.ptr(), false, st_));
-    else DMRG_TRY(launch_gemm_f64(s, t.ket.ptr(), o.canonical.ptr(), nk.ptr(), false, st_));
+    if (cplx_) {
+        if (leigh == 0) DMRG_TRY(zs.check_bounds(o.canonical.d.size, t.ket.d.size, nk.d.size));
+        else DMRG_TRY(zs.check_bounds(t.ket.d.size, o.canonical.d.size, nk.d.size));
+        DMRG_TRY(zs.finalize(st_));
+        if (leigh == 0) DMRG_TRY(launch_zgemm(zs, o.canonical.ptr(), t.ket.ptr(), nk.ptr(), false, st_));
+        else DMRG_TRY(launch_zgemm(zs, t.ket.ptr(), o.canonical.ptr(), nk.ptr(), false, st_));
+    } else {
+        if (leigh == 0) DMRG_TRY(s.check_bounds(o.canonical.d.size, t.ket.d.size, nk.d.size));
+        else DMRG_TRY(s.check_bounds(t.ket.d.size, o.canonical.d.size, nk.d.size));
+        DMRG_TRY(s.finalize(64, 64, 16, st_));
+        if (leigh == 0) DMRG_TRY(launch_gemm_f64(s, o.canonical.ptr(), t.ket.ptr(), nk.ptr(), false, st_));
+        else DMRG_TRY(launch_gemm_f64(s, t.ket.ptr(), o.canonical.ptr(), nk.ptr(), false, st_));
+    }
     DMRG_CUDA_TRY(cudaStreamSynchronize(st_));
     // sector dims follow the canonical blocks
     if (leigh == 0)
@@ -459,21 +519,23 @@ int Engine::ExpanLattice(int leigh, TensorLattice& t, const TensorLattice& origi
     }
     DevBlocks nk;
     nk.d = nd;
-    DMRG_TRY(nk.alloc(st_, true));
+    DMRG_TRY(nk.alloc(st_, true, ew_));
+    // a complex block row-major is a real one of twice the columns
     std::vector<RectCopy> from_origin, from_expan;
     for (int k = 0; k < nb; ++k)
         for (const Part& p : parts[k]) {
             const TensorLattice& src = p.src == 0 ? origin : *expan;
             const int sr = src.ket.d.rows[p.q], sc = src.ket.d.cols[p.q];
-            RectCopy c{src.ket.d.off[p.q], nd.off[k] + (leigh == 0 ? p.at : (int64_t)p.at * nd.cols[k]), sc,
-                       nd.cols[k], sr, sc, 1.0};
+            RectCopy c{src.ket.d.off[p.q] * ew_, (nd.off[k] + (leigh == 0 ? p.at : (int64_t)p.at * nd.cols[k])) * ew_,
+                       sc * ew_, nd.cols[k] * ew_, sr, sc * ew_, 1.0};
             (p.src == 0 ? from_origin : from_expan).push_back(c);
         }
-    DMRG_TRY(launch_rect_copies(from_origin, origin.ket.ptr(), origin.ket.d.size, nk.ptr(), nd.size, copy_tasks_, st_));
+    DMRG_TRY(launch_rect_copies(from_origin, origin.ket.ptr(), origin.ket.d.size * ew_, nk.ptr(), nd.size * ew_,
+                                copy_tasks_, st_));
     if (!from_expan.empty()) {
         DMRG_CUDA_TRY(cudaStreamSynchronize(st_));
-        DMRG_TRY(launch_rect_copies(from_expan, expan->ket.ptr(), expan->ket.d.size, nk.ptr(), nd.size, copy_tasks_,
-                                    st_));
+        DMRG_TRY(launch_rect_copies(from_expan, expan->ket.ptr(), expan->ket.d.size * ew_, nk.ptr(), nd.size * ew_,
+                                    copy_tasks_, st_));
     }
     DMRG_CUDA_TRY(cudaStreamSynchronize(st_));
     t.ket = std::move(nk);
@@ -499,6 +561,27 @@ static void combine_sectors(const std::vector<int>& b0, const std::vector<int>& 
         j = find_value(b1, out_b[i]);
         if (j != -1) out_d[i] += d1[j];
     }
+}
+
+// One expansion random matrix (d0 x d1) appended to the plan: the reference's
+// RandomMatrix draws (real or complex), then 0.1 * W on its diagonal
+// (real_tensor_contraction.cc:396-399, complex twin :396-399).  Returns its
+// offset in elements.
+int64_t Engine::add_random(int d0, int d1, double wre, double wim) {
+    std::vector<double>& rnd = xw_.rnd;
+    const int64_t ro = (int64_t)rnd.size() / ew_;
+    rnd.resize(rnd.size() + (size_t)d0 * d1 * ew_);
+    if (cplx_) {
+        random_block_complex(rng_, rand_draws_, rnd, (size_t)ro, d0, d1);
+        for (int q = 0; q < std::min(d0, d1); ++q) {
+            rnd[2 * (ro + (size_t)q * d1 + q)] = 0.1 * wre;
+            rnd[2 * (ro + (size_t)q * d1 + q) + 1] = 0.1 * wim;
+        }
+    } else {
+        random_block(rng_, rand_draws_, rnd, (size_t)ro, d0, d1);
+        for (int q = 0; q < std::min(d0, d1); ++q) rnd[ro + (size_t)q * d1 + q] = 0.1 * wre;
+    }
+    return ro;
 }
 
 // RealTensorSpace::ExpanTensorSpace (real_tensor_space.cc:319-387)
@@ -527,7 +610,7 @@ int Engine::ExpanTensorSpace(int leigh, int site) {
     t.ket.set_shape_zero();
     if (trace_) {  // the expansion term, block by block, before it is merged
         const DevBlocks& eb = expan_->ket;
-        std::vector<double> h((size_t)eb.d.size);
+        std::vector<double> h((size_t)eb.d.size * ew_);
         if (!h.empty()) {
             DMRG_CUDA_TRY(cudaMemcpyAsync(h.data(), eb.ptr(), h.size() * sizeof(double), cudaMemcpyDeviceToHost, st_));
             DMRG_CUDA_TRY(cudaStreamSynchronize(st_));
@@ -535,7 +618,8 @@ int Engine::ExpanTensorSpace(int leigh, int site) {
         std::fprintf(trace_, "Y %d %d", leigh, site);
         for (int k = 0; k < eb.d.count(); ++k) {
             double s2 = 0.0;
-            for (int64_t i = 0; i < (int64_t)eb.d.rows[k] * eb.d.cols[k]; ++i) s2 += h[eb.d.off[k] + i] * h[eb.d.off[k] + i];
+            for (int64_t i = 0; i < (int64_t)eb.d.rows[k] * eb.d.cols[k] * ew_; ++i)
+                s2 += h[eb.d.off[k] * ew_ + i] * h[eb.d.off[k] * ew_ + i];
             std::fprintf(trace_, " %d.%d:%dx%d=%.8e", eb.d.left[k], eb.d.right[k], eb.d.rows[k], eb.d.cols[k], s2);
         }
         std::fprintf(trace_, "\n");
@@ -635,10 +719,10 @@ void Engine::ComputeExpanTensorLattice(int leigh, int site, std::vector<std::vec
 // ---------------------------------------------------------------------------
 int Engine::LeftExpanTensorContraction(int site, const std::vector<std::vector<int>>& mapping) {
     const TensorLattice& t = *lat_[site];
-    const RealTensorOperator& W = ham_->get_tensor_hamiltonian(site);
+    const MpoHamiltonian& H = *ham_;
     const TensorContraction& con = *con_[site];
     TensorLattice& e = *expan_;
-    const int lb = W.get_left_bond(), rb = W.get_right_bond();
+    const int lb = H.left_bond(site), rb = H.right_bond(site);
     auto same_left = t.ket.d.by_sector(0, t.nl());
     const bool compute = expansion_enabled(p_max_block_, p_max_dim_, p_noise_);
     xw_.active = true;
@@ -653,11 +737,11 @@ int Engine::LeftExpanTensorContraction(int site, const std::vector<std::vector<i
             for (int pos : same_left[kdx]) {
                 const int jdx = t.ket.d.right[pos];
                 const int p2 = t.p(kdx, jdx);
-                if (!W.MixedCheckZero(o1, p2)) continue;
+                if (!H.MixedCheckZero(site, o1, p2)) continue;
                 for (int o2 = 0; o2 < rb; ++o2) {
                     const int ldx = mapping[o2][jdx];
                     const int position = e.ket.d.find(idx, ldx);
-                    if (ldx != -1 && position != -1 && W.w(o1, o2, e.p(idx, ldx), p2) != 0.0) exist[ldx] = 1;
+                    if (ldx != -1 && position != -1 && H.w_nonzero(site, o1, o2, e.p(idx, ldx), p2)) exist[ldx] = 1;
                 }
             }
         }
@@ -696,7 +780,6 @@ int Engine::LeftExpanTensorContraction(int site, const std::vector<std::vector<i
     std::vector<First>& firsts = xw_.firsts;
     std::vector<std::vector<Contrib>>& contrib = xw_.contrib;
     contrib.assign(eb.count(), {});
-    std::vector<double>& rnd = xw_.rnd;
     int64_t& first_size = xw_.first_size;
     for (int o1 = 0; o1 < lb; ++o1) {
         const BlockListDesc& Lo = con.L.desc.o[o1];
@@ -706,7 +789,7 @@ int Engine::LeftExpanTensorContraction(int site, const std::vector<std::vector<i
             for (int pos : same_left[kdx]) {
                 const int jdx = t.ket.d.right[pos];
                 const int p2 = t.p(kdx, jdx);
-                if (!W.MixedCheckZero(o1, p2)) continue;
+                if (!H.MixedCheckZero(site, o1, p2)) continue;
                 const int fm = Lo.rows[i], fk = Lo.cols[i], fn = t.ket.d.cols[pos];
                 if (fk != t.ket.d.rows[pos]) return set_error(DMRG_E_ARG, "Matrix indeces do not match (expansion)");
                 int d0 = fn;
@@ -717,12 +800,9 @@ int Engine::LeftExpanTensorContraction(int site, const std::vector<std::vector<i
                     const int ldx = table[o2][jdx];
                     const int position = eb.find(idx, ldx);
                     if (ldx == -1 || position == -1) continue;
-                    const double el = W.w(o1, o2, nphys[(size_t)idx * keep.size() + ldx], p2);
-                    if (el == 0.0) continue;
-                    const int64_t ro = (int64_t)rnd.size();
-                    rnd.resize(rnd.size() + (size_t)d0 * d1);
-                    random_block(rng_, rand_draws_, rnd, ro, d0, d1);
-                    for (int q = 0; q < std::min(d0, d1); ++q) rnd[ro + (size_t)q * d1 + q] = 0.1 * el;
+                    const int pe = nphys[(size_t)idx * keep.size() + ldx];
+                    if (!H.w_nonzero(site, o1, o2, pe, p2)) continue;
+                    const int64_t ro = add_random(d0, d1, H.wre(site, o1, o2, pe, p2), H.wim(site, o1, o2, pe, p2));
                     if (fidx < 0) {
                         fidx = (int)firsts.size();
                         firsts.push_back(First{con.L.desc.base[o1] + Lo.off[i], t.ket.d.off[pos], fm, fk, fn,
@@ -747,6 +827,8 @@ int Engine::LeftExpanTensorContraction(int site, const std::vector<std::vector<i
         eb.cols[b] = cols;
     }
     // right_dim = widest block; empty blocks become zeros(left_dim[r], right_dim[r])
+    // (the real reference indexes left_dim by r; the complex one by l, and pads
+    // every other block with zero columns to right_dim, complex_tensor_contraction.cc:436-464)
     for (int r = 0; r < e.nr(); ++r) {
         e.right_dim[r] = 0;
         for (int l = 0; l < e.nl(); ++l) {
@@ -755,12 +837,16 @@ int Engine::LeftExpanTensorContraction(int site, const std::vector<std::vector<i
         }
         for (int l = 0; l < e.nl(); ++l) {
             const int b = eb.find(l, r);
-            if (b != -1 && eb.rows[b] == 0) {
-                const int rr = r < (int)e.left_dim.size() ? e.left_dim[r] : 0;  // the reference indexes left_dim by r
+            if (b == -1) continue;
+            if (eb.rows[b] == 0) {
+                const int li = cplx_ ? l : r;
+                const int rr = li < (int)e.left_dim.size() ? e.left_dim[li] : 0;
                 if ((int64_t)rr * e.right_dim[r] > 0) {
                     eb.rows[b] = rr;
                     eb.cols[b] = e.right_dim[r];
                 }
+            } else if (cplx_) {
+                eb.cols[b] = e.right_dim[r];  // zero columns after the products
             }
         }
     }
@@ -772,10 +858,10 @@ int Engine::LeftExpanTensorContraction(int site, const std::vector<std::vector<i
 
 int Engine::RightExpanTensorContraction(int site, const std::vector<std::vector<int>>& mapping) {
     const TensorLattice& t = *lat_[site];
-    const RealTensorOperator& W = ham_->get_tensor_hamiltonian(site);
+    const MpoHamiltonian& H = *ham_;
     const TensorContraction& con = *con_[site];
     TensorLattice& e = *expan_;
-    const int lb = W.get_left_bond(), rb = W.get_right_bond();
+    const int lb = H.left_bond(site), rb = H.right_bond(site);
     auto same_right = t.ket.d.by_sector(1, t.nr());
     const bool compute = expansion_enabled(p_max_block_, p_max_dim_, p_noise_);
     xw_.active = true;
@@ -789,11 +875,11 @@ int Engine::RightExpanTensorContraction(int site, const std::vector<std::vector<
             for (int pos : same_right[kdx]) {
                 const int jdx = t.ket.d.left[pos];
                 const int p2 = t.p(jdx, kdx);
-                if (!W.RightCheckZero(o2, p2)) continue;
+                if (!H.RightCheckZero(site, o2, p2)) continue;
                 for (int o1 = 0; o1 < lb; ++o1) {
                     const int ldx = mapping[o1][jdx];
                     const int position = e.ket.d.find(ldx, idx);
-                    if (ldx != -1 && position != -1 && W.w(o1, o2, e.p(ldx, idx), p2) != 0.0) exist[ldx] = 1;
+                    if (ldx != -1 && position != -1 && H.w_nonzero(site, o1, o2, e.p(ldx, idx), p2)) exist[ldx] = 1;
                 }
             }
         }
@@ -830,7 +916,6 @@ int Engine::RightExpanTensorContraction(int site, const std::vector<std::vector<
     std::vector<First>& firsts = xw_.firsts;
     std::vector<std::vector<Contrib>>& contrib = xw_.contrib;
     contrib.assign(eb.count(), {});
-    std::vector<double>& rnd = xw_.rnd;
     int64_t& first_size = xw_.first_size;
     for (int o2 = 0; o2 < rb; ++o2) {
         const BlockListDesc& Ro = con.R.desc.o[o2];
@@ -840,7 +925,7 @@ int Engine::RightExpanTensorContraction(int site, const std::vector<std::vector<
             for (int pos : same_right[kdx]) {
                 const int jdx = t.ket.d.left[pos];
                 const int p2 = t.p(jdx, kdx);
-                if (!W.RightCheckZero(o2, p2)) continue;
+                if (!H.RightCheckZero(site, o2, p2)) continue;
                 const int fm = t.ket.d.rows[pos], fk = t.ket.d.cols[pos], fn = Ro.cols[i];
                 if (fk != Ro.rows[i]) return set_error(DMRG_E_ARG, "Matrix indeces do not match (expansion)");
                 const int d1 = fm;
@@ -851,12 +936,9 @@ int Engine::RightExpanTensorContraction(int site, const std::vector<std::vector<
                     const int ldx = table[o1][jdx];
                     const int position = eb.find(ldx, idx);
                     if (ldx == -1 || position == -1) continue;
-                    const double el = W.w(o1, o2, nphys[(size_t)ldx * e.nr() + idx], p2);
-                    if (el == 0.0) continue;
-                    const int64_t ro = (int64_t)rnd.size();
-                    rnd.resize(rnd.size() + (size_t)d0 * d1);
-                    random_block(rng_, rand_draws_, rnd, ro, d0, d1);
-                    for (int q = 0; q < std::min(d0, d1); ++q) rnd[ro + (size_t)q * d1 + q] = 0.1 * el;
+                    const int pe = nphys[(size_t)ldx * e.nr() + idx];
+                    if (!H.w_nonzero(site, o1, o2, pe, p2)) continue;
+                    const int64_t ro = add_random(d0, d1, H.wre(site, o1, o2, pe, p2), H.wim(site, o1, o2, pe, p2));
                     if (fidx < 0) {
                         fidx = (int)firsts.size();
                         firsts.push_back(First{t.ket.d.off[pos], con.R.desc.base[o2] + Ro.off[i], fm, fk, fn,
@@ -887,14 +969,20 @@ int Engine::RightExpanTensorContraction(int site, const std::vector<std::vector<
         }
         for (int r = 0; r < e.nr(); ++r) {
             const int b = eb.find(l, r);
-            if (b != -1 && eb.rows[b] == 0) {
-                // the reference builds zeros(left_dim[r], right_dim[r]) here
-                const int rr = r < (int)e.left_dim.size() ? e.left_dim[r] : 0;
+            if (b == -1) continue;
+            if (eb.rows[b] == 0) {
+                // the real reference builds zeros(left_dim[r], right_dim[r]) here, the
+                // complex one zeros(left_dim[l], right_dim[r]) and pads every other
+                // block with zero rows to left_dim[l] (complex_tensor_contraction.cc:752-781)
+                const int li = cplx_ ? l : r;
+                const int rr = li < (int)e.left_dim.size() ? e.left_dim[li] : 0;
                 const int cc = e.right_dim[r];
                 if ((int64_t)rr * cc > 0) {
                     eb.rows[b] = rr;
                     eb.cols[b] = cc;
                 }
+            } else if (cplx_) {
+                eb.rows[b] = e.left_dim[l];  // zero rows after the products
             }
         }
     }
@@ -914,50 +1002,68 @@ int Engine::ExecuteExpanTensorNetwork() {
     const BlockListDesc& packed = xw_.packed;
     e.ket = DevBlocks();
     e.ket.d = packed;
-    DMRG_TRY(e.ket.alloc(st_, true));
+    DMRG_TRY(e.ket.alloc(st_, true, ew_));
     if (!xw_.compute || xw_.firsts.empty()) return DMRG_OK;  // rand() stream advanced; products unused
     const TensorLattice& t = *lat_[xw_.site];
     const TensorContraction& con = *con_[xw_.site];
     const std::vector<double>& rnd = xw_.rnd;
     const int64_t first_size = xw_.first_size;
-    DMRG_TRY(scratch_.alloc((size_t)std::max<int64_t>(first_size, 1) * sizeof(double)));
+    const int64_t rnd_size = (int64_t)rnd.size() / ew_;  // elements
+    DMRG_TRY(scratch_.alloc((size_t)std::max<int64_t>(first_size, 1) * ew_ * sizeof(double)));
     DMRG_TRY(scratch2_.alloc(std::max<size_t>(rnd.size(), 1) * sizeof(double)));
     DMRG_CUDA_TRY(cudaMemcpyAsync(scratch2_.ptr, rnd.data(), rnd.size() * sizeof(double), cudaMemcpyHostToDevice, st_));
+    // the same products in both fields: GemmSchedule (FP64) or ZGemmSchedule (complex)
     GemmSchedule sf, ss;
+    ZGemmSchedule zf, zss;
+    auto group = [&](bool second, int64_t c_off, int ldc, int m, int n) {
+        if (cplx_) (second ? zss : zf).add_group(c_off, ldc, m, n);
+        else (second ? ss : sf).add_group(c_off, ldc, m, n);
+    };
+    auto term = [&](bool second, int64_t a_off, int lda, int64_t b_off, int ldb, int k, double scale) {
+        if (cplx_) (second ? zss : zf).add_term(a_off, lda, b_off, ldb, k, scale, 0.0);
+        else (second ? ss : sf).add_term(a_off, lda, b_off, ldb, k, scale);
+    };
     for (const ExpanWork::First& f : xw_.firsts) {
-        sf.add_group(f.off, f.n, f.m, f.n);
-        sf.add_term(f.a_off, f.k, f.b_off, f.n, f.k, 1.0);
+        group(false, f.off, f.n, f.m, f.n);
+        term(false, f.a_off, f.k, f.b_off, f.n, f.k, 1.0);
     }
     for (int b = 0; b < packed.count(); ++b) {
         int at = 0;
         for (const ExpanWork::Contrib& c : xw_.contrib[b]) {
             const ExpanWork::First& f = xw_.firsts[c.first];
             if (xw_.leigh == 0) {  // columns [at, at + d1) of the block = (L K) * Rand
-                ss.add_group(packed.off[b] + at, packed.cols[b], f.m, c.d1);
-                ss.add_term(f.off, f.n, c.rnd, c.d1, c.d0, p_noise_);
+                group(true, packed.off[b] + at, packed.cols[b], f.m, c.d1);
+                term(true, f.off, f.n, c.rnd, c.d1, c.d0, p_noise_);
                 at += c.d1;
             } else {  // rows [at, at + d0) of the block = Rand * (K R)
-                ss.add_group(packed.off[b] + (int64_t)at * packed.cols[b], packed.cols[b], c.d0, f.n);
-                ss.add_term(c.rnd, c.d1, f.off, f.n, c.d1, p_noise_);
+                group(true, packed.off[b] + (int64_t)at * packed.cols[b], packed.cols[b], c.d0, f.n);
+                term(true, c.rnd, c.d1, f.off, f.n, c.d1, p_noise_);
                 at += c.d0;
             }
         }
     }
-    if (xw_.leigh == 0) {
-        DMRG_TRY(sf.check_bounds(con.L.desc.size, t.ket.d.size, first_size));
-        DMRG_TRY(ss.check_bounds(first_size, (int64_t)rnd.size(), packed.size));
+    const double* A1 = xw_.leigh == 0 ? con.L.ptr() : t.ket.ptr();
+    const double* B1 = xw_.leigh == 0 ? t.ket.ptr() : con.R.ptr();
+    const double* A2 = xw_.leigh == 0 ? scratch_.as<double>() : scratch2_.as<double>();
+    const double* B2 = xw_.leigh == 0 ? scratch2_.as<double>() : scratch_.as<double>();
+    const int64_t a1 = xw_.leigh == 0 ? con.L.desc.size : t.ket.d.size;
+    const int64_t b1 = xw_.leigh == 0 ? t.ket.d.size : con.R.desc.size;
+    const int64_t a2 = xw_.leigh == 0 ? first_size : rnd_size;
+    const int64_t b2 = xw_.leigh == 0 ? rnd_size : first_size;
+    if (cplx_) {
+        DMRG_TRY(zf.check_bounds(a1, b1, first_size));
+        DMRG_TRY(zss.check_bounds(a2, b2, packed.size));
+        DMRG_TRY(zf.finalize(st_));
+        DMRG_TRY(zss.finalize(st_));
+        DMRG_TRY(launch_zgemm(zf, A1, B1, scratch_.as<double>(), false, st_));
+        DMRG_TRY(launch_zgemm(zss, A2, B2, e.ket.ptr(), false, st_));
     } else {
-        DMRG_TRY(sf.check_bounds(t.ket.d.size, con.R.desc.size, first_size));
-        DMRG_TRY(ss.check_bounds((int64_t)rnd.size(), first_size, packed.size));
-    }
-    DMRG_TRY(sf.finalize(64, 64, 16, st_));
-    DMRG_TRY(ss.finalize(64, 64, 16, st_));
-    if (xw_.leigh == 0) {
-        DMRG_TRY(launch_gemm_f64(sf, con.L.ptr(), t.ket.ptr(), scratch_.as<double>(), false, st_));
-        DMRG_TRY(launch_gemm_f64(ss, scratch_.as<double>(), scratch2_.as<double>(), e.ket.ptr(), false, st_));
-    } else {
-        DMRG_TRY(launch_gemm_f64(sf, t.ket.ptr(), con.R.ptr(), scratch_.as<double>(), false, st_));
-        DMRG_TRY(launch_gemm_f64(ss, scratch2_.as<double>(), scratch_.as<double>(), e.ket.ptr(), false, st_));
+        DMRG_TRY(sf.check_bounds(a1, b1, first_size));
+        DMRG_TRY(ss.check_bounds(a2, b2, packed.size));
+        DMRG_TRY(sf.finalize(64, 64, 16, st_));
+        DMRG_TRY(ss.finalize(64, 64, 16, st_));
+        DMRG_TRY(launch_gemm_f64(sf, A1, B1, scratch_.as<double>(), false, st_));
+        DMRG_TRY(launch_gemm_f64(ss, A2, B2, e.ket.ptr(), false, st_));
     }
     DMRG_CUDA_TRY(cudaStreamSynchronize(st_));
     return DMRG_OK;
@@ -997,6 +1103,14 @@ int dmrg_heff_create(dmrg_ctx_t, int, int, const int*, const dmrg_blocks_t*, int
 int dmrg_heff_destroy(dmrg_heff_t);
 int dmrg_heff_set_env(dmrg_heff_t, const double*, const double*);
 int dmrg_lanczos(dmrg_heff_t, double*, int, double, double, double*, int*);
+int dmrg_zenv_create(dmrg_ctx_t, int, int, int, const int*, const dmrg_blocks_t*, int, int, int, const double*,
+                     const dmrg_blocks_t*, dmrg_env_t*);
+int dmrg_zenv_apply(dmrg_env_t, const double*, const double*, double*);
+int dmrg_zheff_create(dmrg_ctx_t, int, int, const int*, const dmrg_blocks_t*, int, int, int, const double*,
+                      const dmrg_blocks_t*, const dmrg_blocks_t*, dmrg_zheff_t*);
+int dmrg_zheff_destroy(dmrg_zheff_t);
+int dmrg_zheff_set_env(dmrg_zheff_t, const double*, const double*);
+int dmrg_zlanczos(dmrg_zheff_t, double*, int, double, double, double*, int*);
 }
 
 namespace dmrg {
@@ -1015,8 +1129,10 @@ void Engine::DefineTensorNetwork() {
         env.desc.o.assign(bond, BlockListDesc());
         for (int o = 0; o < bond; ++o) env.desc.o[o].push(0, 0, 1, 1);
         env.desc.rebase();
-        env.buf.alloc((size_t)std::max<int64_t>(env.desc.size, 1) * sizeof(double));
-        std::vector<double> ones((size_t)env.desc.size, 1.0);
+        env.buf.alloc((size_t)std::max<int64_t>(env.desc.size, 1) * ew_ * sizeof(double));
+        std::vector<double> ones((size_t)env.desc.size * ew_, 1.0);
+        if (cplx_)  // Complex(1, 0)
+            for (size_t i = 1; i < ones.size(); i += 2) ones[i] = 0.0;
         if (!ones.empty())
             cudaMemcpyAsync(env.buf.ptr, ones.data(), ones.size() * sizeof(double), cudaMemcpyHostToDevice, st_);
         cudaStreamSynchronize(st_);
@@ -1042,7 +1158,7 @@ int Engine::ResetEnv(int leigh, int site) {
 // RealTensorNetwork::ComputeTensorNetwork (real_tensor_network.cc:142-154)
 int Engine::ComputeTensorNetwork(int leigh, int site) {
     TensorLattice& t = *lat_[site];
-    const RealTensorOperator& W = ham_->get_tensor_hamiltonian(site);
+    const MpoHamiltonian& H = *ham_;
     const TensorContraction& src = *con_[site];
     TensorContraction& dst = *con_[leigh == 0 ? site + 1 : (site - 1 + n_ + 1) % (n_ + 1)];
     const EnvData& in = leigh == 0 ? src.L : src.R;
@@ -1050,9 +1166,13 @@ int Engine::ComputeTensorNetwork(int leigh, int site) {
     std::vector<dmrg_blocks_t> ib = env_blocks(in.desc);
     dmrg_blocks_t kb = as_blocks(t.ket.d);
     dmrg_env_t e = nullptr;
-    DMRG_TRY(dmrg_env_create(ctx_, leigh, t.nl(), t.nr(), t.phys.data(), &kb, W.get_physics_dim(), W.get_left_bond(),
-                             W.get_right_bond(), W.data().data(), ib.data(), DMRG_PREC_FP64,
-                             &e));
+    if (cplx_)  // ComplexTensorContraction::Left/RightComputeTensorContraction
+        DMRG_TRY(dmrg_zenv_create(ctx_, leigh, t.nl(), t.nr(), t.phys.data(), &kb, H.physics_dim(site),
+                                  H.left_bond(site), H.right_bond(site), H.values(site), ib.data(), &e));
+    else
+        DMRG_TRY(dmrg_env_create(ctx_, leigh, t.nl(), t.nr(), t.phys.data(), &kb, H.physics_dim(site),
+                                 H.left_bond(site), H.right_bond(site), H.values(site), ib.data(), DMRG_PREC_FP64,
+                                 &e));
     int bond = 0;
     int64_t size = 0;
     int rc = dmrg_env_out_info(e, &bond, &size);
@@ -1067,8 +1187,10 @@ int Engine::ComputeTensorNetwork(int leigh, int site) {
     }
     od.rebase();
     DeviceBuffer buf;
-    if (rc == DMRG_OK) rc = buf.alloc((size_t)std::max<int64_t>(od.size, 1) * sizeof(double));
-    if (rc == DMRG_OK) rc = dmrg_env_apply(e, t.ket.ptr(), in.ptr(), buf.as<double>());
+    if (rc == DMRG_OK) rc = buf.alloc((size_t)std::max<int64_t>(od.size, 1) * ew_ * sizeof(double));
+    if (rc == DMRG_OK)
+        rc = cplx_ ? dmrg_zenv_apply(e, t.ket.ptr(), in.ptr(), buf.as<double>())
+                   : dmrg_env_apply(e, t.ket.ptr(), in.ptr(), buf.as<double>());
     if (rc == DMRG_OK) {
         cudaError_t err = cudaStreamSynchronize(st_);
         if (err != cudaSuccess) rc = set_error(DMRG_E_CUDA, "env update: %s", cudaGetErrorString(err));
@@ -1084,14 +1206,24 @@ int Engine::ComputeTensorNetwork(int leigh, int site) {
 // RealTensorLanczos::LanczosMethod through the device solver.
 int Engine::LanczosMethod(int niter, int site, double& energy, int& dim) {
     TensorLattice& t = *lat_[site];
-    const RealTensorOperator& W = ham_->get_tensor_hamiltonian(site);
+    const MpoHamiltonian& H = *ham_;
     const TensorContraction& c = *con_[site];
     std::vector<dmrg_blocks_t> lb = env_blocks(c.L.desc), rb = env_blocks(c.R.desc);
     dmrg_blocks_t kb = as_blocks(t.ket.d);
+    if (cplx_) {  // ComplexTensorLanczos::LanczosMethod
+        dmrg_zheff_t zh = nullptr;
+        DMRG_TRY(dmrg_zheff_create(ctx_, t.nl(), t.nr(), t.phys.data(), &kb, H.physics_dim(site), H.left_bond(site),
+                                   H.right_bond(site), H.values(site), lb.data(), rb.data(), &zh));
+        int rc = dmrg_zheff_set_env(zh, c.L.ptr(), c.R.ptr());
+        if (rc == DMRG_OK)
+            rc = dmrg_zlanczos(zh, t.ket.ptr(), niter, opt_.lanczos_precision, opt_.zero_tolerance, &energy, &dim);
+        dmrg_zheff_destroy(zh);
+        return rc;
+    }
     dmrg_heff_t h = nullptr;
     const double t0 = wall_time();
-    DMRG_TRY(dmrg_heff_create(ctx_, t.nl(), t.nr(), t.phys.data(), &kb, W.get_physics_dim(), W.get_left_bond(),
-                              W.get_right_bond(), W.data().data(), lb.data(), rb.data(), opt_.precision, &h));
+    DMRG_TRY(dmrg_heff_create(ctx_, t.nl(), t.nr(), t.phys.data(), &kb, H.physics_dim(site), H.left_bond(site),
+                              H.right_bond(site), H.values(site), lb.data(), rb.data(), opt_.precision, &h));
     int rc = dmrg_heff_set_env(h, c.L.ptr(), c.R.ptr());
     const double t1 = wall_time();
     if (rc == DMRG_OK)
@@ -1239,6 +1371,7 @@ struct BinIn {
 }  // namespace
 
 int Engine::WriteTensorSpace(const std::string& path) {
+    if (cplx_) return set_error(DMRG_E_ARG, "checkpoints of complex runs are not supported");
     std::FILE* f = std::fopen(path.c_str(), "wb");
     if (!f) return set_error(DMRG_E_IO, "cannot open %s for writing", path.c_str());
     BinOut o{f};
@@ -1297,6 +1430,7 @@ int Engine::WriteTensorSpace(const std::string& path) {
 }
 
 int Engine::ReadTensorSpace(const std::string& path) {
+    if (cplx_) return set_error(DMRG_E_ARG, "checkpoints of complex runs are not supported");
     std::FILE* f = std::fopen(path.c_str(), "rb");
     if (!f) return set_error(DMRG_E_IO, "cannot open %s", path.c_str());
     BinIn in{f};

@@ -30,12 +30,13 @@ struct StatusError : std::runtime_error {
     StatusError(int st, const std::string& what) : std::runtime_error(what), status(st) {}
 };
 
-// RealMatrixBlock with its values on the device (packed, list order).
+// RealMatrixBlock (ComplexMatrixBlock) with its values on the device (packed,
+// list order; a complex value is two doubles, offsets count elements).
 struct DevBlocks {
     BlockListDesc d;
     DeviceBuffer buf;
     double* ptr() const { return buf.as<double>(); }
-    int alloc(cudaStream_t st, bool zero);
+    int alloc(cudaStream_t st, bool zero, int ew = 1);  // ew: doubles per element
     void set_shape_zero() {  // ResetMatrixBlock: every block 0 x 0
         for (int k = 0; k < d.count(); ++k) d.rows[k] = d.cols[k] = 0;
         d.size = 0;
@@ -92,7 +93,10 @@ struct RunOptions {
 
 class Engine {
 public:
-    Engine(dmrg_ctx_t ctx, std::unique_ptr<QuantumSpace> space, std::unique_ptr<RealTensorHamiltonian> ham,
+    // A complex Hamiltonian (ham->is_complex()) runs the complexdmrg twin of
+    // every step (ComplexTensorRundmrg, src/dmrg/complexdmrg/*): complex site
+    // tensors and environments, complex kernels.
+    Engine(dmrg_ctx_t ctx, std::unique_ptr<QuantumSpace> space, std::unique_ptr<MpoHamiltonian> ham,
            InputGroup& input, const RunOptions& opt);
     ~Engine();
     // RealTensorRundmrg::Run (real_tensor_rundmrg.cc:115-245), or RunTwoSite
@@ -112,6 +116,7 @@ public:
     TensorLattice& lattice(int i) { return *lat_[i]; }
     TensorContraction& contraction(int i) { return *con_[i]; }
     int num_site() const { return n_; }
+    bool is_complex() const { return cplx_; }
     cudaStream_t stream() const { return st_; }
     int device() const { return ctx_->device; }
 
@@ -151,6 +156,7 @@ private:
     int LeftExpanTensorContraction(int site, const std::vector<std::vector<int>>& mapping);
     int RightExpanTensorContraction(int site, const std::vector<std::vector<int>>& mapping);
     int ExpanLattice(int leigh, TensorLattice& t, const TensorLattice& origin, const TensorLattice* expan);
+    int64_t add_random(int d0, int d1, double wre, double wim);
     int Normalize(TensorLattice& t);
     void Trace(const char* tag, int leigh, int site);
     void DefineTensorNetwork();
@@ -160,7 +166,9 @@ private:
     cudaStream_t st_;
     RunOptions opt_;
     std::unique_ptr<QuantumSpace> space_;
-    std::unique_ptr<RealTensorHamiltonian> ham_;
+    std::unique_ptr<MpoHamiltonian> ham_;
+    bool cplx_ = false;  // complex run
+    int ew_ = 1;         // doubles per tensor element (2 when complex)
     int n_ = 0;
     std::vector<std::unique_ptr<TensorLattice>> lat_;
     std::vector<std::unique_ptr<TensorContraction>> con_;

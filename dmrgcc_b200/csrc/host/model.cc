@@ -11,7 +11,9 @@ namespace dmrg {
 // ---------------------------------------------------------------------------
 // RealTensorOperator
 // ---------------------------------------------------------------------------
-void RealTensorOperator::ExpanTensorOperator(const std::vector<HostMatrix>& basic, int leigh, int op, double coeff) {
+template <class T>
+void TensorOperatorT<T>::ExpanTensorOperator(const std::vector<HostMatrixT<T>>& basic, int leigh, int op,
+                                             const T& coeff) {
     int e0 = 1, e1 = 1;
     if (leigh == 0) e0 = 0;
     if (leigh == 1) e1 = 0;
@@ -23,7 +25,7 @@ void RealTensorOperator::ExpanTensorOperator(const std::vector<HostMatrix>& basi
         nlb = lb_ + e0;
         nrb = rb_ + e1;
     }
-    std::vector<double> old = W_;
+    std::vector<T> old = W_;
     const int olb = lb_, orb = rb_;
     resize(nlb, nrb);
     for (int l = 0; l < olb; ++l)
@@ -59,22 +61,45 @@ void parallel_element(double e0, double e1, int position, int& info, double& pre
     }
 }
 
+
+// The complex form (the Complex overload of isParallelElement, util/general.h):
+// Norm in place of fabs, the reference's complex quotient.
+void parallel_element(const Cplx& e0, const Cplx& e1, int position, int& info, Cplx& prefactor, bool& zero) {
+    if (norm_of(e1) <= 1e-10) {
+        if (norm_of(e0) > 1e-10) {
+            info = -1;
+            prefactor = Cplx(1.0);
+        }
+    } else {
+        const Cplx factor = e0 / e1;
+        if (zero) {
+            info = position;
+            prefactor = factor;
+            zero = false;
+        } else if (norm_of(factor - prefactor) > 1e-8) {
+            info = -1;
+            prefactor = Cplx(1.0);
+        }
+    }
+}
+
 }  // namespace
 
-void parallel_matrix(const HostMatrix& M, int leigh, int& nu, std::vector<int>& pos, HostMatrix& T) {
+template <class S>
+void parallel_matrix(const HostMatrixT<S>& M, int leigh, int& nu, std::vector<int>& pos, HostMatrixT<S>& T) {
     int info = 0;
-    double prefactor = 0.0;
+    S prefactor = S(0.0);
     bool zero = true;
     if (leigh == 0) {
         pos.assign(M.cols, -1);
         pos[0] = 0;
-        T = HostMatrix(M.cols, M.cols);
-        T.at(0, 0) = 1.0;
+        T = HostMatrixT<S>(M.cols, M.cols);
+        T.at(0, 0) = S(1.0);
         nu = 1;
         for (int r = 0; r < M.cols; ++r) {
             for (int k = 0; k < nu; ++k) {
                 info = nu;
-                prefactor = 0.0;
+                prefactor = S(0.0);
                 zero = true;
                 for (int l = 0; l < M.rows; ++l) {
                     parallel_element(M.at(l, r), M.at(l, pos[k]), pos[k], info, prefactor, zero);
@@ -87,20 +112,20 @@ void parallel_matrix(const HostMatrix& M, int leigh, int& nu, std::vector<int>& 
             }
             if (info == -1) {
                 pos[nu] = r;
-                T.at(nu, r) = 1.0;
+                T.at(nu, r) = S(1.0);
                 ++nu;
             }
         }
     } else {
         pos.assign(M.rows, -1);
         pos[0] = 0;
-        T = HostMatrix(M.rows, M.rows);
-        T.at(0, 0) = 1.0;
+        T = HostMatrixT<S>(M.rows, M.rows);
+        T.at(0, 0) = S(1.0);
         nu = 1;
         for (int l = 0; l < M.rows; ++l) {
             for (int k = 0; k < nu; ++k) {
                 info = nu;
-                prefactor = 0.0;
+                prefactor = S(0.0);
                 zero = true;
                 for (int r = 0; r < M.cols; ++r) {
                     parallel_element(M.at(l, r), M.at(pos[k], r), pos[k], info, prefactor, zero);
@@ -113,20 +138,21 @@ void parallel_matrix(const HostMatrix& M, int leigh, int& nu, std::vector<int>& 
             }
             if (info == -1) {
                 pos[nu] = l;
-                T.at(l, nu) = 1.0;
+                T.at(l, nu) = S(1.0);
                 ++nu;
             }
         }
     }
 }
 
-void RealTensorOperator::LeftParallelTensorOperator(int& nu, std::vector<int>& pos, HostMatrix& T) {
-    HostMatrix R(lb_ * d_ * d_, rb_);
+template <class T>
+void TensorOperatorT<T>::LeftParallelTensorOperator(int& nu, std::vector<int>& pos, HostMatrixT<T>& Tm) {
+    HostMatrixT<T> R(lb_ * d_ * d_, rb_);
     for (int l = 0; l < lb_; ++l)
         for (int r = 0; r < rb_; ++r)
             for (int p1 = 0; p1 < d_; ++p1)
                 for (int p2 = 0; p2 < d_; ++p2) R.at(p2 + (p1 + l * d_) * d_, r) = w(l, r, p1, p2);
-    parallel_matrix(R, 0, nu, pos, T);
+    parallel_matrix(R, 0, nu, pos, Tm);
     resize(lb_, nu);
     for (int l = 0; l < lb_; ++l)
         for (int r = 0; r < rb_; ++r)
@@ -134,13 +160,14 @@ void RealTensorOperator::LeftParallelTensorOperator(int& nu, std::vector<int>& p
                 for (int p2 = 0; p2 < d_; ++p2) w(l, r, p1, p2) = R.at(p2 + (p1 + l * d_) * d_, pos[r]);
 }
 
-void RealTensorOperator::RightParallelTensorOperator(int& nu, std::vector<int>& pos, HostMatrix& T) {
-    HostMatrix R(lb_, rb_ * d_ * d_);
+template <class T>
+void TensorOperatorT<T>::RightParallelTensorOperator(int& nu, std::vector<int>& pos, HostMatrixT<T>& Tm) {
+    HostMatrixT<T> R(lb_, rb_ * d_ * d_);
     for (int l = 0; l < lb_; ++l)
         for (int r = 0; r < rb_; ++r)
             for (int p1 = 0; p1 < d_; ++p1)
                 for (int p2 = 0; p2 < d_; ++p2) R.at(l, p2 + (p1 + r * d_) * d_) = w(l, r, p1, p2);
-    parallel_matrix(R, 1, nu, pos, T);
+    parallel_matrix(R, 1, nu, pos, Tm);
     resize(nu, rb_);
     for (int l = 0; l < lb_; ++l)
         for (int r = 0; r < rb_; ++r)
@@ -148,70 +175,86 @@ void RealTensorOperator::RightParallelTensorOperator(int& nu, std::vector<int>& 
                 for (int p2 = 0; p2 < d_; ++p2) w(l, r, p1, p2) = R.at(pos[l], p2 + (p1 + r * d_) * d_);
 }
 
-void RealTensorOperator::LeftMergeTensorOperator(int nu, const HostMatrix& T) {
-    const int merge = T.cols;
+template <class T>
+void TensorOperatorT<T>::LeftMergeTensorOperator(int nu, const HostMatrixT<T>& Tm) {
+    const int merge = Tm.cols;
     if (merge != lb_) throw std::runtime_error("merge dimension is not match in LeftMergeTensorOperator");
-    std::vector<double> old = W_;
+    std::vector<T> old = W_;
     const int orb = rb_;
     resize(nu, orb);
     for (int l = 0; l < nu; ++l)
         for (int r = 0; r < orb; ++r)
             for (int p1 = 0; p1 < d_; ++p1)
                 for (int p2 = 0; p2 < d_; ++p2) {
-                    double e = 0.0;
+                    T e = T(0.0);
                     for (int m = 0; m < merge; ++m)
-                        e += T.at(l, m) * old[(((size_t)m * orb + r) * d_ + p1) * d_ + p2];
+                        e += Tm.at(l, m) * old[(((size_t)m * orb + r) * d_ + p1) * d_ + p2];
                     w(l, r, p1, p2) = e;
                 }
 }
 
-void RealTensorOperator::RightMergeTensorOperator(int nu, const HostMatrix& T) {
-    const int merge = T.rows;
+template <class T>
+void TensorOperatorT<T>::RightMergeTensorOperator(int nu, const HostMatrixT<T>& Tm) {
+    const int merge = Tm.rows;
     if (merge != rb_) throw std::runtime_error("merge dimension is not match in RightMergeTensorOperator");
-    std::vector<double> old = W_;
+    std::vector<T> old = W_;
     const int olb = lb_, orb = rb_;
     resize(olb, nu);
     for (int l = 0; l < olb; ++l)
         for (int r = 0; r < nu; ++r)
             for (int p1 = 0; p1 < d_; ++p1)
                 for (int p2 = 0; p2 < d_; ++p2) {
-                    double e = 0.0;
+                    T e = T(0.0);
                     for (int m = 0; m < merge; ++m)
-                        e += T.at(m, r) * old[(((size_t)l * orb + m) * d_ + p1) * d_ + p2];
+                        e += Tm.at(m, r) * old[(((size_t)l * orb + m) * d_ + p1) * d_ + p2];
                     w(l, r, p1, p2) = e;
                 }
 }
 
-bool RealTensorOperator::LeftCheckZero(int l, int p1) const {
+template <class T>
+bool TensorOperatorT<T>::LeftCheckZero(int l, int p1) const {
     for (int r = 0; r < rb_; ++r)
         for (int p2 = 0; p2 < d_; ++p2)
-            if (std::fabs(w(l, r, p1, p2)) > 1e-15) return true;
+            if (norm_of(w(l, r, p1, p2)) > 1e-15) return true;
     return false;
 }
-bool RealTensorOperator::RightCheckZero(int r, int p2) const {
+template <class T>
+bool TensorOperatorT<T>::RightCheckZero(int r, int p2) const {
     for (int l = 0; l < lb_; ++l)
         for (int p1 = 0; p1 < d_; ++p1)
-            if (std::fabs(w(l, r, p1, p2)) > 1e-15) return true;
+            if (norm_of(w(l, r, p1, p2)) > 1e-15) return true;
     return false;
 }
-bool RealTensorOperator::MixedCheckZero(int l, int p2) const {
+template <class T>
+bool TensorOperatorT<T>::MixedCheckZero(int l, int p2) const {
     for (int r = 0; r < rb_; ++r)
         for (int p1 = 0; p1 < d_; ++p1)
-            if (std::fabs(w(l, r, p1, p2)) > 1e-15) return true;
+            if (norm_of(w(l, r, p1, p2)) > 1e-15) return true;
     return false;
 }
 
 // ---------------------------------------------------------------------------
 // RealTensorHamiltonian
 // ---------------------------------------------------------------------------
-void RealTensorHamiltonian::init(int num_site, int d, int num_quantum) {
+template <>
+bool TensorHamiltonianT<double>::is_complex() const {
+    return false;
+}
+template <>
+bool TensorHamiltonianT<Cplx>::is_complex() const {
+    return true;
+}
+
+template <class T>
+void TensorHamiltonianT<T>::init(int num_site, int d, int num_quantum) {
     num_site_ = num_site;
     num_quantum_ = num_quantum;
     qtab_.assign(num_site + 1, {});
-    ops_.assign(num_site, RealTensorOperator(d));
+    ops_.assign(num_site, TensorOperatorT<T>(d));
 }
 
-void RealTensorHamiltonian::ExpanTensorHamiltonian(int site, int op, double coeff, const std::vector<int>& table) {
+template <class T>
+void TensorHamiltonianT<T>::ExpanTensorHamiltonian(int site, int op, const T& coeff, const std::vector<int>& table) {
     int leigh = -1;
     if (site == 0) leigh = 0;
     if (site == num_site_ - 1) leigh = 1;
@@ -219,27 +262,34 @@ void RealTensorHamiltonian::ExpanTensorHamiltonian(int site, int op, double coef
     if (site < num_site_ - 1) qtab_[site + 1].push_back(table);
 }
 
-void RealTensorHamiltonian::ParallelQuantumTable(int site, int nu, const std::vector<int>& pos) {
+template <class T>
+void TensorHamiltonianT<T>::ParallelQuantumTable(int site, int nu, const std::vector<int>& pos) {
     std::vector<std::vector<int>> t(nu);
     for (int i = 0; i < nu; ++i) t[i] = qtab_[site][pos[i]];
     qtab_[site] = t;
 }
 
-void RealTensorHamiltonian::ParallelTensorHamiltonian() {
+template <class T>
+void TensorHamiltonianT<T>::ParallelTensorHamiltonian() {
     int nu;
     std::vector<int> pos;
-    HostMatrix T;
+    HostMatrixT<T> Tm;
     for (int i = 0; i < num_site_ - 1; ++i) {
-        ops_[i].LeftParallelTensorOperator(nu, pos, T);
-        ops_[i + 1].LeftMergeTensorOperator(nu, T);
+        ops_[i].LeftParallelTensorOperator(nu, pos, Tm);
+        ops_[i + 1].LeftMergeTensorOperator(nu, Tm);
         ParallelQuantumTable(i + 1, nu, pos);
     }
     for (int i = num_site_ - 1; i > 0; --i) {
-        ops_[i].RightParallelTensorOperator(nu, pos, T);
-        ops_[i - 1].RightMergeTensorOperator(nu, T);
+        ops_[i].RightParallelTensorOperator(nu, pos, Tm);
+        ops_[i - 1].RightMergeTensorOperator(nu, Tm);
         ParallelQuantumTable(i, nu, pos);
     }
 }
+
+template class TensorOperatorT<double>;
+template class TensorOperatorT<Cplx>;
+template class TensorHamiltonianT<double>;
+template class TensorHamiltonianT<Cplx>;
 
 RealSpinlessBoseSquareHamiltonian::RealSpinlessBoseSquareHamiltonian(int nx, int ny, int d, double flux_value,
                                                                      double hop_x, double hop_y, double inter,
@@ -404,37 +454,54 @@ namespace dmrg {
 // ---------------------------------------------------------------------------
 // Spinful bosons on interleaved species sites
 // ---------------------------------------------------------------------------
-RealSpinfulBoseSquareHamiltonian::RealSpinfulBoseSquareHamiltonian(int nx, int ny, int d, double flux, double hop_x,
-                                                                   double hop_y, const double inter[3], double chem,
-                                                                   bool px, bool py)
-    : nx_(nx), ny_(ny), d_(d), hop_x_(hop_x), hop_y_(hop_y), chem_(chem), px_(px), py_(py) {
-    if (flux != 0.0)
+template <class T>
+SpinfulBoseSquareHamiltonianT<T>::SpinfulBoseSquareHamiltonianT(int nx, int ny, int d, double flux, double hop_x,
+                                                                double hop_y, const double inter[3], double chem,
+                                                                bool px, bool py)
+    : nx_(nx), ny_(ny), d_(d), flux_(flux), hop_x_(hop_x), hop_y_(hop_y), chem_(chem), px_(px), py_(py) {
+    if (flux != 0.0 && !this->is_complex())
         throw std::runtime_error("the spinful model's Peierls phases (flux != 0) need complex tensors");
     for (int t = 0; t < 3; ++t) inter_[t] = inter[t];
-    init(2 * nx * ny, d, 2);
+    this->init(2 * nx * ny, d, 2);
     // 0 = I, 1 = a+, 2 = a, 3 = n, 4 = mu n + U_0/2 n(n-1), 5 = mu n + U_1/2 n(n-1)
     // (one chemical potential for both species, as the reference's operator 5
     // takes the first species' value, complex_spinful_bose_square_hamiltonian.cc:61)
-    basic_.assign(6, HostMatrix(d, d));
+    auto& basic = this->basic_;
+    basic.assign(6, HostMatrixT<T>(d, d));
     for (int i = 0; i < d; ++i) {
-        basic_[0].at(i, i) = 1.0;
-        basic_[3].at(i, i) = i;
-        basic_[4].at(i, i) = chem * i + 0.5 * inter_[0] * i * (i - 1);
-        basic_[5].at(i, i) = chem * i + 0.5 * inter_[1] * i * (i - 1);
+        basic[0].at(i, i) = T(1.0);
+        basic[3].at(i, i) = T((double)i);
+        basic[4].at(i, i) = T(chem * i + 0.5 * inter_[0] * i * (i - 1));
+        basic[5].at(i, i) = T(chem * i + 0.5 * inter_[1] * i * (i - 1));
     }
     for (int i = 1; i < d; ++i) {
-        basic_[1].at(i, i - 1) = std::sqrt((double)i);
-        basic_[2].at(i - 1, i) = std::sqrt((double)i);
+        basic[1].at(i, i - 1) = T(std::sqrt((double)i));
+        basic[2].at(i - 1, i) = T(std::sqrt((double)i));
     }
+}
+
+template <>
+void SpinfulBoseSquareHamiltonianT<double>::y_coeff(int, double& first, double& second) const {
+    first = second = hop_y_;
+}
+
+// phase = Phase(2 pi (x+1) flux); the first term of a bond takes Conj(phase) J_y,
+// the second phase J_y (complex_spinful_bose_square_hamiltonian.cc:297-311)
+template <>
+void SpinfulBoseSquareHamiltonianT<Cplx>::y_coeff(int x, Cplx& first, Cplx& second) const {
+    const Cplx phase = phase_of(2 * M_PI * (x + 1) * flux_);
+    first = conj_of(phase) * hop_y_;
+    second = phase * hop_y_;
 }
 
 // The operator's quantum number between p1 and p2 is carried by the species of p1.
-void RealSpinfulBoseSquareHamiltonian::DefineHamiltonian1(int p1, int p2, double coeff) {
+template <class T>
+void SpinfulBoseSquareHamiltonianT<T>::DefineHamiltonian1(int p1, int p2, const T& coeff) {
     if (p1 >= p2) throw std::runtime_error("position1 >= position2 in DefineHamiltonian1");
     const std::vector<int> q = p1 % 2 == 0 ? std::vector<int>{1, 0} : std::vector<int>{0, 1};
-    for (int i = 0; i < num_site_; ++i) {
+    for (int i = 0; i < this->num_site_; ++i) {
         int op = 0;
-        double c = 1.0;
+        T c = T(1.0);
         std::vector<int> t{0, 0};
         if (i == p1) {
             op = 1;
@@ -446,16 +513,17 @@ void RealSpinfulBoseSquareHamiltonian::DefineHamiltonian1(int p1, int p2, double
             c = coeff;
             t = {0, 0};
         }
-        ExpanTensorHamiltonian(i, op, c, t);
+        this->ExpanTensorHamiltonian(i, op, c, t);
     }
 }
 
-void RealSpinfulBoseSquareHamiltonian::DefineHamiltonian2(int p1, int p2, double coeff) {
+template <class T>
+void SpinfulBoseSquareHamiltonianT<T>::DefineHamiltonian2(int p1, int p2, const T& coeff) {
     if (p1 >= p2) throw std::runtime_error("position1 >= position2 in DefineHamiltonian2");
     const std::vector<int> q = p1 % 2 == 0 ? std::vector<int>{-1, 0} : std::vector<int>{0, -1};
-    for (int i = 0; i < num_site_; ++i) {
+    for (int i = 0; i < this->num_site_; ++i) {
         int op = 0;
-        double c = 1.0;
+        T c = T(1.0);
         std::vector<int> t{0, 0};
         if (i == p1) {
             op = 2;
@@ -467,69 +535,78 @@ void RealSpinfulBoseSquareHamiltonian::DefineHamiltonian2(int p1, int p2, double
             c = coeff;
             t = {0, 0};
         }
-        ExpanTensorHamiltonian(i, op, c, t);
+        this->ExpanTensorHamiltonian(i, op, c, t);
     }
 }
 
-void RealSpinfulBoseSquareHamiltonian::DefineHamiltonian3(int p, double coeff) {
-    for (int i = 0; i < num_site_; ++i) {
+template <class T>
+void SpinfulBoseSquareHamiltonianT<T>::DefineHamiltonian3(int p, const T& coeff) {
+    for (int i = 0; i < this->num_site_; ++i) {
         int op = 0;
-        double c = 1.0;
+        T c = T(1.0);
         if (i == p) {
             op = p % 2 == 0 ? 4 : 5;
             c = coeff;
         }
-        ExpanTensorHamiltonian(i, op, c, {0, 0});
+        this->ExpanTensorHamiltonian(i, op, c, {0, 0});
     }
 }
 
-void RealSpinfulBoseSquareHamiltonian::DefineHamiltonian4(int p1, int p2, double coeff) {
-    for (int i = 0; i < num_site_; ++i) {
+template <class T>
+void SpinfulBoseSquareHamiltonianT<T>::DefineHamiltonian4(int p1, int p2, const T& coeff) {
+    for (int i = 0; i < this->num_site_; ++i) {
         int op = 0;
-        double c = 1.0;
+        T c = T(1.0);
         if (i == p1) op = 3;
         if (i == p2) {
             op = 3;
             c = coeff;
         }
-        ExpanTensorHamiltonian(i, op, c, {0, 0});
+        this->ExpanTensorHamiltonian(i, op, c, {0, 0});
     }
 }
 
 // ComplexSpinfulBoseSquareHamiltonian::DefineTensorHamiltonian (:249-350): the
-// same term order (it decides the MPO bond indices), flux 0.
-void RealSpinfulBoseSquareHamiltonian::DefineTensorHamiltonian() {
-    qtab_[0] = {{0, 0}};
-    qtab_[num_site_] = {{0, 0}};
+// same term order (it decides the MPO bond indices).
+template <class T>
+void SpinfulBoseSquareHamiltonianT<T>::DefineTensorHamiltonian() {
+    const int n = this->num_site_;
+    this->qtab_[0] = {{0, 0}};
+    this->qtab_[n] = {{0, 0}};
     for (int i = 0; i < nx_; ++i)
         for (int j = 0; j < ny_; ++j) {
             const int p0 = j + i * ny_;
             for (int s = 0; s < 2 && hop_x_ != 0; ++s) {
                 const int p1 = j + ((i + 1) % nx_) * ny_;
                 if (i + 1 < nx_) {
-                    DefineHamiltonian1(2 * p0 + s, 2 * p1 + s, hop_x_);
-                    DefineHamiltonian2(2 * p0 + s, 2 * p1 + s, hop_x_);
+                    DefineHamiltonian1(2 * p0 + s, 2 * p1 + s, T(hop_x_));
+                    DefineHamiltonian2(2 * p0 + s, 2 * p1 + s, T(hop_x_));
                 } else if (nx_ > 2 && px_) {
-                    DefineHamiltonian1(2 * p1 + s, 2 * p0 + s, hop_x_);
-                    DefineHamiltonian2(2 * p1 + s, 2 * p0 + s, hop_x_);
+                    DefineHamiltonian1(2 * p1 + s, 2 * p0 + s, T(hop_x_));
+                    DefineHamiltonian2(2 * p1 + s, 2 * p0 + s, T(hop_x_));
                 }
             }
             for (int s = 0; s < 2 && hop_y_ != 0; ++s) {
                 const int p1 = (j + 1) % ny_ + i * ny_;
+                T first, second;
+                y_coeff(i, first, second);
                 if (j + 1 < ny_) {
-                    DefineHamiltonian1(2 * p0 + s, 2 * p1 + s, hop_y_);
-                    DefineHamiltonian2(2 * p0 + s, 2 * p1 + s, hop_y_);
+                    DefineHamiltonian1(2 * p0 + s, 2 * p1 + s, first);
+                    DefineHamiltonian2(2 * p0 + s, 2 * p1 + s, second);
                 } else if (ny_ > 2 && py_) {  // the wrap adds its two terms in the other order
-                    DefineHamiltonian2(2 * p1 + s, 2 * p0 + s, hop_y_);
-                    DefineHamiltonian1(2 * p1 + s, 2 * p0 + s, hop_y_);
+                    DefineHamiltonian2(2 * p1 + s, 2 * p0 + s, first);
+                    DefineHamiltonian1(2 * p1 + s, 2 * p0 + s, second);
                 }
             }
-            if (chem_ != 0.0 || inter_[0] != 0.0) DefineHamiltonian3(2 * p0, 1.0);
-            if (chem_ != 0.0 || inter_[1] != 0.0) DefineHamiltonian3(2 * p0 + 1, 1.0);
-            if (inter_[2] != 0.0) DefineHamiltonian4(2 * p0, 2 * p0 + 1, inter_[2]);
-            ParallelTensorHamiltonian();
+            if (chem_ != 0.0 || inter_[0] != 0.0) DefineHamiltonian3(2 * p0, T(1.0));
+            if (chem_ != 0.0 || inter_[1] != 0.0) DefineHamiltonian3(2 * p0 + 1, T(1.0));
+            if (inter_[2] != 0.0) DefineHamiltonian4(2 * p0, 2 * p0 + 1, T(inter_[2]));
+            this->ParallelTensorHamiltonian();
         }
 }
+
+template class SpinfulBoseSquareHamiltonianT<double>;
+template class SpinfulBoseSquareHamiltonianT<Cplx>;
 
 // ComplexSpinfulBoseSquareSpace::DefineQuantumTable (:28-97): per bond, the
 // admissible (N0, N1) with species 0 counted over the first (i+1)/2 MPS sites

@@ -7,40 +7,47 @@
 #include <string>
 #include <vector>
 
+#include "host/cplx.h"
+
 namespace dmrg {
 
-// Dense row-major host matrix used for the small one-time MPO algebra.
-struct HostMatrix {
+// Dense row-major host matrix used for the small one-time MPO algebra (T =
+// double for the real models, Cplx for the complex ones).
+template <class T>
+struct HostMatrixT {
     int rows = 0, cols = 0;
-    std::vector<double> v;
-    HostMatrix() = default;
-    HostMatrix(int r, int c) : rows(r), cols(c), v((size_t)r * c, 0.0) {}
-    double& at(int i, int j) { return v[(size_t)i * cols + j]; }
-    double at(int i, int j) const { return v[(size_t)i * cols + j]; }
+    std::vector<T> v;
+    HostMatrixT() = default;
+    HostMatrixT(int r, int c) : rows(r), cols(c), v((size_t)r * c, T(0.0)) {}
+    T& at(int i, int j) { return v[(size_t)i * cols + j]; }
+    const T& at(int i, int j) const { return v[(size_t)i * cols + j]; }
 };
+using HostMatrix = HostMatrixT<double>;
 
-// RealTensorOperator (src/dmrg/realdmrg/real_tensor_operator.{h,cc}): an MPO
-// site tensor W[l][r](p1, p2).
-class RealTensorOperator {
+// RealTensorOperator / ComplexTensorOperator (src/dmrg/realdmrg/
+// real_tensor_operator.{h,cc}, complexdmrg/complex_tensor_operator.cc: the same
+// code on complex values, zero tests by Norm): an MPO site tensor W[l][r](p1, p2).
+template <class T>
+class TensorOperatorT {
 public:
-    explicit RealTensorOperator(int physics_dim = 0) : d_(physics_dim) {}
+    explicit TensorOperatorT(int physics_dim = 0) : d_(physics_dim) {}
     int get_physics_dim() const { return d_; }
     int get_left_bond() const { return lb_; }
     int get_right_bond() const { return rb_; }
-    double w(int l, int r, int p1, int p2) const { return W_[idx(l, r, p1, p2)]; }
-    double& w(int l, int r, int p1, int p2) { return W_[idx(l, r, p1, p2)]; }
-    const std::vector<double>& data() const { return W_; }
+    const T& w(int l, int r, int p1, int p2) const { return W_[idx(l, r, p1, p2)]; }
+    T& w(int l, int r, int p1, int p2) { return W_[idx(l, r, p1, p2)]; }
+    const std::vector<T>& data() const { return W_; }
 
     // Appends one term: leigh 0 (first site) grows the right bond, 1 (last site)
     // the left bond, otherwise both; the new corner is coeff * basic[op]
     // (ExpanTensorOperator, real_tensor_operator.cc:141-197).
-    void ExpanTensorOperator(const std::vector<HostMatrix>& basic, int leigh, int op, double coeff);
+    void ExpanTensorOperator(const std::vector<HostMatrixT<T>>& basic, int leigh, int op, const T& coeff);
     // Deparallelisation of the right bond (:199-237) / left bond (:239-275).
-    void LeftParallelTensorOperator(int& num_unparallel, std::vector<int>& position, HostMatrix& transfer);
-    void RightParallelTensorOperator(int& num_unparallel, std::vector<int>& position, HostMatrix& transfer);
+    void LeftParallelTensorOperator(int& num_unparallel, std::vector<int>& position, HostMatrixT<T>& transfer);
+    void RightParallelTensorOperator(int& num_unparallel, std::vector<int>& position, HostMatrixT<T>& transfer);
     // Absorbs a neighbour's transfer matrix into the left (:277-319) / right (:321-361) bond.
-    void LeftMergeTensorOperator(int num_unparallel, const HostMatrix& transfer);
-    void RightMergeTensorOperator(int num_unparallel, const HostMatrix& transfer);
+    void LeftMergeTensorOperator(int num_unparallel, const HostMatrixT<T>& transfer);
+    void RightMergeTensorOperator(int num_unparallel, const HostMatrixT<T>& transfer);
     // Any |W| > 1e-15 in the given row/column slice (:363-409).
     bool LeftCheckZero(int l, int p1) const;
     bool RightCheckZero(int r, int p2) const;
@@ -51,41 +58,82 @@ private:
     void resize(int lb, int rb) {
         lb_ = lb;
         rb_ = rb;
-        W_.assign((size_t)lb * rb * d_ * d_, 0.0);
+        W_.assign((size_t)lb * rb * d_ * d_, T(0.0));
     }
     int d_ = 0, lb_ = 0, rb_ = 0;
-    std::vector<double> W_;
+    std::vector<T> W_;
 };
+using RealTensorOperator = TensorOperatorT<double>;
+using ComplexTensorOperator = TensorOperatorT<Cplx>;
 
-// RealMatrix::ParallelMatrix (src/tensor/real_matrix.cc:438-531): removes
-// columns (leigh 0) or rows (leigh 1) parallel to an earlier one.
-void parallel_matrix(const HostMatrix& M, int leigh, int& num_unparallel, std::vector<int>& position,
-                     HostMatrix& transfer);
+// RealMatrix::ParallelMatrix (src/tensor/real_matrix.cc:438-531) and its
+// complex twin (complex_matrix.cc:451): removes columns (leigh 0) or rows
+// (leigh 1) parallel to an earlier one.
+template <class T>
+void parallel_matrix(const HostMatrixT<T>& M, int leigh, int& num_unparallel, std::vector<int>& position,
+                     HostMatrixT<T>& transfer);
 
-// RealTensorHamiltonian (+ the spin-less Bose-Hubbard square-lattice model,
-// model/hamiltonian/real_spinless_bose_square_hamiltonian.cc).
-class RealTensorHamiltonian {
+// What the sweep engine reads of a Hamiltonian, real or complex: the MPO site
+// tensors (values as doubles, complex ones interleaved (re, im)), their zero
+// tests, and the operator quantum numbers of the MPO bonds.
+class MpoHamiltonian {
 public:
-    virtual ~RealTensorHamiltonian() = default;
+    virtual ~MpoHamiltonian() = default;
+    virtual void DefineTensorHamiltonian() = 0;
+    virtual bool is_complex() const = 0;
     int num_site() const { return num_site_; }
-    RealTensorOperator& get_tensor_hamiltonian(int site) { return ops_[site]; }
-    const RealTensorOperator& get_tensor_hamiltonian(int site) const { return ops_[site]; }
     // operator quantum numbers of MPO bond b (b = 0..num_site): rows x num_quantum
     const std::vector<std::vector<int>>& quantum_table(int b) const { return qtab_[b]; }
     int num_quantum() const { return num_quantum_; }
-    virtual void DefineTensorHamiltonian() = 0;
+    virtual int physics_dim(int site) const = 0;
+    virtual int left_bond(int site) const = 0;
+    virtual int right_bond(int site) const = 0;
+    virtual const double* values(int site) const = 0;
+    virtual double wre(int site, int l, int r, int p1, int p2) const = 0;
+    virtual double wim(int site, int l, int r, int p1, int p2) const = 0;
+    virtual bool LeftCheckZero(int site, int l, int p1) const = 0;
+    virtual bool RightCheckZero(int site, int r, int p2) const = 0;
+    virtual bool MixedCheckZero(int site, int l, int p2) const = 0;
+    bool w_nonzero(int site, int l, int r, int p1, int p2) const {
+        return wre(site, l, r, p1, p2) != 0.0 || wim(site, l, r, p1, p2) != 0.0;
+    }
+
+protected:
+    int num_site_ = 0, num_quantum_ = 1;
+    std::vector<std::vector<std::vector<int>>> qtab_;
+};
+
+// RealTensorHamiltonian / ComplexTensorHamiltonian (real_tensor_hamiltonian.cc,
+// complex_tensor_hamiltonian.cc): the MPO built term by term and deparallelised.
+template <class T>
+class TensorHamiltonianT : public MpoHamiltonian {
+public:
+    TensorOperatorT<T>& get_tensor_hamiltonian(int site) { return ops_[site]; }
+    const TensorOperatorT<T>& get_tensor_hamiltonian(int site) const { return ops_[site]; }
+    bool is_complex() const override;
+    int physics_dim(int site) const override { return ops_[site].get_physics_dim(); }
+    int left_bond(int site) const override { return ops_[site].get_left_bond(); }
+    int right_bond(int site) const override { return ops_[site].get_right_bond(); }
+    const double* values(int site) const override {
+        return reinterpret_cast<const double*>(ops_[site].data().data());
+    }
+    double wre(int site, int l, int r, int p1, int p2) const override { return real_of(ops_[site].w(l, r, p1, p2)); }
+    double wim(int site, int l, int r, int p1, int p2) const override { return imag_of(ops_[site].w(l, r, p1, p2)); }
+    bool LeftCheckZero(int site, int l, int p1) const override { return ops_[site].LeftCheckZero(l, p1); }
+    bool RightCheckZero(int site, int r, int p2) const override { return ops_[site].RightCheckZero(r, p2); }
+    bool MixedCheckZero(int site, int l, int p2) const override { return ops_[site].MixedCheckZero(l, p2); }
 
 protected:
     void init(int num_site, int physics_dim, int num_quantum);
-    void ExpanTensorHamiltonian(int site, int op, double coeff, const std::vector<int>& expan_table);
+    void ExpanTensorHamiltonian(int site, int op, const T& coeff, const std::vector<int>& expan_table);
     void ParallelTensorHamiltonian();
     void ParallelQuantumTable(int site, int num_unparallel, const std::vector<int>& position);
 
-    int num_site_ = 0, num_quantum_ = 1;
-    std::vector<HostMatrix> basic_;
-    std::vector<std::vector<std::vector<int>>> qtab_;
-    std::vector<RealTensorOperator> ops_;
+    std::vector<HostMatrixT<T>> basic_;
+    std::vector<TensorOperatorT<T>> ops_;
 };
+using RealTensorHamiltonian = TensorHamiltonianT<double>;
+using ComplexTensorHamiltonian = TensorHamiltonianT<Cplx>;
 
 class RealSpinlessBoseSquareHamiltonian : public RealTensorHamiltonian {
 public:
@@ -151,23 +199,29 @@ private:
 
 // H = sum over bonds of J_s (a+_s a_s' + h.c.) per species + sum_i [mu n + U_s/2
 // n(n-1)] per species + U_ud n0 n1: ComplexSpinfulBoseSquareHamiltonian
-// (model/hamiltonian/complex_spinful_bose_square_hamiltonian.cc:3-350) with
-// real coefficients.  Its Peierls phases exp(i 2 pi (x+1) flux) on y-bonds
-// need complex tensors: a nonzero flux is rejected.
-class RealSpinfulBoseSquareHamiltonian : public RealTensorHamiltonian {
+// (model/hamiltonian/complex_spinful_bose_square_hamiltonian.cc:3-350), with
+// the Peierls phase exp(i 2 pi (x+1) flux) on the y-bonds of column x (:297-331).
+// T = double (RealSpinfulBoseSquareHamiltonian) needs flux 0 and rejects any
+// other; T = Cplx (ComplexSpinfulBoseSquareHamiltonian) is the reference's class.
+template <class T>
+class SpinfulBoseSquareHamiltonianT : public TensorHamiltonianT<T> {
 public:
-    RealSpinfulBoseSquareHamiltonian(int nx, int ny, int physics_dim, double flux, double hop_x, double hop_y,
-                                     const double inter[3], double chemical, bool period_x, bool period_y);
+    SpinfulBoseSquareHamiltonianT(int nx, int ny, int physics_dim, double flux, double hop_x, double hop_y,
+                                  const double inter[3], double chemical, bool period_x, bool period_y);
     void DefineTensorHamiltonian() override;
 
 private:
-    void DefineHamiltonian1(int p1, int p2, double coeff);  // a+_p1 a_p2
-    void DefineHamiltonian2(int p1, int p2, double coeff);  // a_p1 a+_p2
-    void DefineHamiltonian3(int p, double coeff);           // mu n + U/2 n(n-1) of the site's species
-    void DefineHamiltonian4(int p1, int p2, double coeff);  // n_p1 n_p2
+    void DefineHamiltonian1(int p1, int p2, const T& coeff);  // a+_p1 a_p2
+    void DefineHamiltonian2(int p1, int p2, const T& coeff);  // a_p1 a+_p2
+    void DefineHamiltonian3(int p, const T& coeff);           // mu n + U/2 n(n-1) of the site's species
+    void DefineHamiltonian4(int p1, int p2, const T& coeff);  // n_p1 n_p2
+    // the y-bond coefficients of column x: (conj(phase) J_y, phase J_y)
+    void y_coeff(int x, T& first, T& second) const;
     int nx_, ny_, d_;
-    double hop_x_, hop_y_, inter_[3], chem_;
+    double flux_, hop_x_, hop_y_, inter_[3], chem_;
     bool px_, py_;
 };
+using RealSpinfulBoseSquareHamiltonian = SpinfulBoseSquareHamiltonianT<double>;
+using ComplexSpinfulBoseSquareHamiltonian = SpinfulBoseSquareHamiltonianT<Cplx>;
 
 }  // namespace dmrg

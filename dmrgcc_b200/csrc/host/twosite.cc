@@ -140,8 +140,9 @@ int Engine::TwoSiteStep(bool l2r, int j, int niter, double& energy, int& dim, do
                         int64_t& theta_dim, std::array<double, kPhases>& ph) {
     TensorLattice& A = *lat_[j];
     TensorLattice& B = *lat_[j + 1];
-    const RealTensorOperator& Wa = ham_->get_tensor_hamiltonian(j);
-    const RealTensorOperator& Wb = ham_->get_tensor_hamiltonian(j + 1);
+    const RealTensorHamiltonian& rh = static_cast<const RealTensorHamiltonian&>(*ham_);  // two-site runs are real
+    const RealTensorOperator& Wa = rh.get_tensor_hamiltonian(j);
+    const RealTensorOperator& Wb = rh.get_tensor_hamiltonian(j + 1);
     const int d = Wa.get_physics_dim();
     const auto& lq = space_->table(j);
     const auto& mq = space_->table(j + 1);

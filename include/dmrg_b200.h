@@ -388,6 +388,12 @@ int dmrg_model_create(const char* input_path, const char* model, dmrg_model_t* o
 int dmrg_model_destroy(dmrg_model_t m);
 int dmrg_model_info(dmrg_model_t m, int* num_site, int* physics_dim, int* num_quantum);
 int dmrg_model_mpo(dmrg_model_t m, int site, int* left_bond, int* right_bond, int cap, double* W);
+/* model "complex_spinful_bose_square" (the reference's
+ * ComplexSpinfulBoseSquareHamiltonian, Peierls phases included) builds a complex
+ * MPO: *is_complex = 1 and dmrg_model_mpo writes interleaved (re, im) values
+ * (cap counts doubles).  A run of such a model sweeps with complex tensors
+ * (ComplexTensorRundmrg), single-site FP64. */
+int dmrg_model_is_complex(dmrg_model_t m, int* is_complex);
 int dmrg_model_quantum_table(dmrg_model_t m, int which, int bond, int cap, int* values, int* rows);
 
 /* ---- host bookkeeping helpers (no device work) ----------------------------

@@ -65,12 +65,15 @@ def ground_energy(nx: int, ny: int, nboson: int, d: int, jx: float, jy: float, u
 
 
 def ground_energy_spinful(nx: int, ny: int, nup: int, ndown: int, d: int, jx: float, jy: float, u_uu: float,
-                          u_dd: float, u_ud: float, mu: float, px: bool = False, py: bool = False) -> float:
+                          u_dd: float, u_ud: float, mu: float, px: bool = False, py: bool = False,
+                          flux: float = 0.0) -> float:
     """Two-component bosons in the (N_up, N_down) sector, the reference's
-    spinful model (model/hamiltonian/complex_spinful_bose_square_hamiltonian.cc)
-    at zero flux: per species s, J (a+ a + h.c.) on the bonds of bonds(), mu n +
-    U_s/2 n(n-1) on site; U_ud n_up n_down.  A state lists (n_up, n_down) per
-    lattice site."""
+    spinful model (model/hamiltonian/complex_spinful_bose_square_hamiltonian.cc):
+    per species s, J (a+ a + h.c.) on the bonds of bonds(), mu n + U_s/2 n(n-1)
+    on site; U_ud n_up n_down.  With a flux, a boson hopping along y from row j
+    to row j+1 (mod Ny) of column x picks up phi = exp(i 2 pi (x+1) flux) and the
+    reverse hop conj(phi) (the reference's Peierls phase, :297-331).  A state
+    lists (n_up, n_down) per lattice site."""
     L = nx * ny
     occ = [s for s in itertools.product(range(d), repeat=L)]
     ups = [s for s in occ if sum(s) == nup]
@@ -91,6 +94,11 @@ def ground_energy_spinful(nx: int, ny: int, nup: int, ndown: int, d: int, jx: fl
             J = jx if kind == "x" else jy
             if J == 0:
                 continue
+            phase = {(p0, p1): 1.0, (p1, p0): 1.0}
+            if kind == "y" and flux != 0.0:
+                phi = np.exp(2j * np.pi * (p0 // ny + 1) * flux)
+                lo, hi = (p0, p1) if (p0 % ny + 1) % ny == p1 % ny else (p1, p0)  # hi = row j + 1 of lo
+                phase = {(lo, hi): phi, (hi, lo): np.conj(phi)}
             for sp_ in range(2):
                 s = (a, b)[sp_]
                 for src, dst in ((p0, p1), (p1, p0)):
@@ -103,9 +111,9 @@ def ground_energy_spinful(nx: int, ny: int, nup: int, ndown: int, d: int, jx: fl
                     new = (tuple(t), b) if sp_ == 0 else (a, tuple(t))
                     rows.append(index[new])
                     cols.append(k)
-                    vals.append(J * amp)
+                    vals.append(J * amp * phase[(src, dst)])
     n = len(states)
-    H = sp.csr_matrix((vals, (rows, cols)), shape=(n, n))
+    H = sp.csr_matrix((np.asarray(vals, dtype=complex if flux != 0.0 else float), (rows, cols)), shape=(n, n))
     if n < 400:
         return float(np.linalg.eigvalsh(H.toarray())[0])
-    return float(sla.eigsh(H, k=1, which="SA")[0][0])
+    return float(sla.eigsh(H, k=1, which="SA")[0][0].real)

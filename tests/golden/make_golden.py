@@ -259,12 +259,14 @@ def converged_reference() -> None:
 
 
 SPINFUL_MODELS = ("spinful4x4", "spinful3x3_periodic_y")
+COMPLEX_MODELS = ("hofstadter4x3",)
 
 
 def spinful_fixtures() -> None:
     """model_<input>.nac: the reference's spinful MPO and quantum tables
     (oracle/_ref/probe_model; the imaginary parts, zero at flux 0, are checked
-    and dropped), and spinful_reference.txt: the reference's final energy on
+    and dropped; kept for the Hofstadter input, whose flux makes them nonzero),
+    and spinful_reference.txt: the reference's final energy on
     spinful3x2.in (complex_spinful_bose_square_model, 1 BLAS thread)."""
     import numpy as np
 
@@ -282,6 +284,12 @@ def spinful_fixtures() -> None:
             assert not np.any(d[k]), k
             del d[k]
         write_nac(os.path.join(HERE, f"model_{name}.nac"), d)
+    for name in COMPLEX_MODELS:  # Peierls phases: the imaginary parts are kept
+        tmp = tempfile.mkdtemp(prefix="golden_model_")
+        out = os.path.join(tmp, "model.nac")
+        subprocess.run([probe, os.path.join(ROOT, "dmrgcc_b200", "inputs", f"{name}.in"), out], check=True,
+                       stdout=subprocess.DEVNULL)
+        write_nac(os.path.join(HERE, f"model_{name}.nac"), read_nac(out))
     tmp = tempfile.mkdtemp(prefix="golden_spinful_")
     env = dict(os.environ, OMP_NUM_THREADS="1", OPENBLAS_NUM_THREADS="1")
     model = os.path.join(ROOT, "oracle", "_ref", "complex_spinful_bose_square_model")

@@ -79,3 +79,39 @@ def test_spinful_exact_diagonalisation_matches_reference():
         e_ref = float([ln.split()[1] for ln in f if ln.startswith("spinful3x2")][0])
     e = ground_energy_spinful(3, 2, 3, 3, 3, -1.0, -1.0, 6.0, 6.0, 3.0, 0.0)
     assert abs(e - e_ref) / 12 <= 1e-12
+
+
+def test_complex_spinful_mpo_with_flux_bit_exact():
+    """The complex spinful model with the Peierls phases exp(i 2 pi (x+1) flux)
+    on the y-bonds (hofstadter4x3.in: flux 1/6, periodic in y, one species
+    filled): every complex MPO entry and both quantum tables bit-identical to
+    the reference's ComplexSpinfulBoseSquare classes (oracle/_ref/probe_model)."""
+    ref = read_nac(os.path.join(GOLD, "model_hofstadter4x3.nac"))
+    m = capi.Model(os.path.join(ROOT, "dmrgcc_b200", "inputs", "hofstadter4x3.in"), "complex_spinful_bose_square")
+    assert m.is_complex
+    n = int(ref["num_site"][0])
+    assert m.num_site == n and m.num_quantum == 2
+    assert any(np.any(ref[f"op{i}.Wi"]) for i in range(n))
+    for i in range(n):
+        W = m.mpo(i)
+        d, lb, rb = (int(x) for x in ref[f"op{i}.dims"])
+        assert W.shape == (lb, rb, d, d)
+        assert np.array_equal(W.real.ravel(), ref[f"op{i}.W"])
+        assert np.array_equal(W.imag.ravel(), ref[f"op{i}.Wi"])
+    for b in range(n + 1):
+        assert np.array_equal(m.quantum_table(0, b).ravel(), ref[f"sq{b}"])
+        assert np.array_equal(m.quantum_table(1, b).ravel(), ref[f"hq{b}"])
+
+
+def test_hofstadter_exact_diagonalisation_matches_reference():
+    """oracle/ed.py with the Peierls phase equals the reference's converged complex
+    run of hofstadter4x3.in (its last Lanczos energy, tests/golden/
+    steps_hofstadter4x3.txt; D = 64 spans the 3-boson space): pins the complex ED."""
+    from oracle.ed import ground_energy_spinful
+
+    with open(os.path.join(GOLD, "steps_hofstadter4x3.txt")) as f:
+        e_ref = float([ln.split() for ln in f if ln.strip() and not ln.startswith("#")][-1][4])
+    e = ground_energy_spinful(4, 3, 3, 0, 3, -1.0, -1.0, 10.0, 0.0, 0.0, 0.0, False, True, flux=0.16666666666666666)
+    assert abs(e - e_ref) / 12 <= 1e-12
+    e0 = ground_energy_spinful(4, 3, 3, 0, 3, -1.0, -1.0, 10.0, 0.0, 0.0, 0.0, False, True)
+    assert e0 < e - 1.0  # the flux matters
