@@ -133,6 +133,9 @@ int dmrg_run_execute_many(dmrg_run_t* runs, int n, int threads, int* status) {
         for (int j = i + 1; j < n; ++j)
             if (runs[i]->engine->stream() == runs[j]->engine->stream())
                 return set_error(DMRG_E_ARG, "runs %d and %d share a stream (give each its own context)", i, j);
+    // side by side, a run's Lanczos calls go launch by launch unless it asked for graphs
+    for (int i = 0; i < n; ++i)
+        if (runs[i]->engine->lanczos_graph() < 0) runs[i]->engine->set_lanczos_graph(0);
     if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
     threads = std::min(threads, n);
     std::atomic<int> next{0};

@@ -1103,6 +1103,7 @@ int dmrg_heff_create(dmrg_ctx_t, int, int, const int*, const dmrg_blocks_t*, int
 int dmrg_heff_destroy(dmrg_heff_t);
 int dmrg_heff_set_env(dmrg_heff_t, const double*, const double*);
 int dmrg_lanczos(dmrg_heff_t, double*, int, double, double, double*, int*);
+int dmrg_heff_set_graph(dmrg_heff_t, int);
 int dmrg_zenv_create(dmrg_ctx_t, int, int, int, const int*, const dmrg_blocks_t*, int, int, int, const double*,
                      const dmrg_blocks_t*, dmrg_env_t*);
 int dmrg_zenv_apply(dmrg_env_t, const double*, const double*, double*);
@@ -1224,6 +1225,7 @@ int Engine::LanczosMethod(int niter, int site, double& energy, int& dim) {
     const double t0 = wall_time();
     DMRG_TRY(dmrg_heff_create(ctx_, t.nl(), t.nr(), t.phys.data(), &kb, H.physics_dim(site), H.left_bond(site),
                               H.right_bond(site), H.values(site), lb.data(), rb.data(), opt_.precision, &h));
+    if (opt_.lanczos_graph >= 0) dmrg_heff_set_graph(h, opt_.lanczos_graph);
     int rc = dmrg_heff_set_env(h, c.L.ptr(), c.R.ptr());
     const double t1 = wall_time();
     if (rc == DMRG_OK)

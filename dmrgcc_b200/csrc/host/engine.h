@@ -89,6 +89,11 @@ struct RunOptions {
     unsigned seed = 1;                  // glibc rand() seed; 1 = the reference's implicit seed
     int stop_after_half_sweeps = -1;    // run only this many half-sweeps (-1: all)
     int two_site = 0;                   // 1: two-site sweeps (RunTwoSite) instead of the reference's single-site ones
+    // Lanczos loop as one CUDA-graph launch per call (dmrg_heff_set_graph): 1 on,
+    // 0 off, -1 the operator's default.  Runs executed side by side turn it off:
+    // every site step captures and instantiates a new graph, and those host calls
+    // serialise across threads on one device.
+    int lanczos_graph = -1;
 };
 
 class Engine {
@@ -117,6 +122,8 @@ public:
     TensorContraction& contraction(int i) { return *con_[i]; }
     int num_site() const { return n_; }
     bool is_complex() const { return cplx_; }
+    void set_lanczos_graph(int enable) { opt_.lanczos_graph = enable; }
+    int lanczos_graph() const { return opt_.lanczos_graph; }
     cudaStream_t stream() const { return st_; }
     int device() const { return ctx_->device; }
 
