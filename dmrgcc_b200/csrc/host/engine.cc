@@ -1213,12 +1213,18 @@ int Engine::LanczosMethod(int niter, int site, double& energy, int& dim) {
     dmrg_blocks_t kb = as_blocks(t.ket.d);
     if (cplx_) {  // ComplexTensorLanczos::LanczosMethod
         dmrg_zheff_t zh = nullptr;
+        const double z0 = wall_time();
         DMRG_TRY(dmrg_zheff_create(ctx_, t.nl(), t.nr(), t.phys.data(), &kb, H.physics_dim(site), H.left_bond(site),
                                    H.right_bond(site), H.values(site), lb.data(), rb.data(), &zh));
         int rc = dmrg_zheff_set_env(zh, c.L.ptr(), c.R.ptr());
+        const double z1 = wall_time();
         if (rc == DMRG_OK)
             rc = dmrg_zlanczos(zh, t.ket.ptr(), niter, opt_.lanczos_precision, opt_.zero_tolerance, &energy, &dim);
+        const double z2 = wall_time();
         dmrg_zheff_destroy(zh);
+        if (trace_)
+            std::fprintf(trace_, "L %d %.3f %.3f %.3f %d %lld\n", site, 1e3 * (z1 - z0), 1e3 * (z2 - z1),
+                         1e3 * (wall_time() - z2), dim, (long long)t.psi_dim());
         return rc;
     }
     dmrg_heff_t h = nullptr;

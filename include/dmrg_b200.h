@@ -361,7 +361,7 @@ int dmrg_run_execute(dmrg_run_t r);
  * order, each on its own context's stream, so the kernels of different runs
  * overlap on the GPU.  Every run must have a context (stream) of its own.
  * Their Lanczos calls run launch by launch (the per-call graph capture and
- * instantiation serialise across host threads on one device). */
+ * instantiation serialise across host threads on one device).
  * status[i] receives run i's return code; the call returns the first failure.
  * The reference runs one instance per process
  * (model/real_spinless_bose_square_model.cc:11-42). */
