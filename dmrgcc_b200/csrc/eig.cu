@@ -359,6 +359,8 @@ static size_t jacobi_smem(int n) {
     return (jacobi_table_doubles(n) + (jacobi_in_smem(n) ? 2 * (size_t)n * n : 0)) * sizeof(double);
 }
 
+bool sym_jacobi_in_shared(int n) { return jacobi_in_smem(n); }
+
 int launch_sym_jacobi(double* A, int n, double* w, double* Z, double* ws, int* status, cudaStream_t st) {
     if (n <= 0) return DMRG_OK;
     const size_t smem = jacobi_smem(n);

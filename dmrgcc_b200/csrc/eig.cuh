@@ -22,6 +22,9 @@ int launch_tridiag_lowest_it(const double* alpha, const double* beta, const int*
 // columns (Z[i*n + k] = component i of eigenvector k).  `ws` needs
 // 2*n*n + 4*n doubles.  status[0] = DMRG_E_NUMERIC if 60 sweeps did not converge.
 int launch_sym_jacobi(double* A, int n, double* w, double* Z, double* ws, int* status, cudaStream_t st);
+// True when launch_sym_jacobi keeps an n x n problem in shared memory (its fast
+// form); larger ones work in global memory, orders of magnitude slower.
+bool sym_jacobi_in_shared(int n);
 
 // Eigenvector y[0..m) of the tridiagonal (alpha, beta) of size *m_dev (read on
 // the device: the Lanczos dimension is only known there) for its lowest

@@ -140,13 +140,35 @@ int recover_triplets(dmrg_zcanon_s& c, int s, cudaStream_t st) {
     const double tol = 1e-9 * std::max(sig.empty() ? 0.0 : sig[0], 1e-300);
     std::vector<double> u, v;
     // removes from x its components along the kept vectors [from, to)
+    // (plain real arithmetic: std::complex's product guards against NaN/inf
+    // operands at a large cost in this inner loop)
     auto project = [&](std::vector<cplx>& x, int from, int to) {
+        double* xv = reinterpret_cast<double*>(x.data());
         for (int q = from; q < to; ++q) {
-            const cplx* pq = &P[(size_t)q * d];
-            cplx a(0.0, 0.0);
-            for (int i = 0; i < d; ++i) a += std::conj(pq[i]) * x[i];
-            for (int i = 0; i < d; ++i) x[i] -= a * pq[i];
+            const double* pv = reinterpret_cast<const double*>(&P[(size_t)q * d]);
+            double ar = 0.0, ai = 0.0;  // a = <p_q, x> = sum conj(p) x
+            for (int i = 0; i < d; ++i) {
+                ar += pv[2 * i] * xv[2 * i] + pv[2 * i + 1] * xv[2 * i + 1];
+                ai += pv[2 * i] * xv[2 * i + 1] - pv[2 * i + 1] * xv[2 * i];
+            }
+            for (int i = 0; i < d; ++i) {  // x -= a p_q
+                const double pr = pv[2 * i], pi = pv[2 * i + 1];
+                xv[2 * i] -= ar * pr - ai * pi;
+                xv[2 * i + 1] -= ar * pi + ai * pr;
+            }
         }
+    };
+    // kept vectors far in value from a candidate are complex-orthogonal to it
+    // to eps ||A|| / gap already: a candidate is projected only against the
+    // kept vectors within kWindow * sigma_max of its value
+    constexpr double kWindow = 1e-3;
+    auto project_near = [&](std::vector<cplx>& x, double value) {
+        const double w = kWindow * (sig.empty() ? 0.0 : sig[0]);
+        int q0 = 0;
+        while (q0 < kept && out[q0] > value + w) ++q0;  // out descending
+        int q1 = q0;
+        while (q1 < kept && out[q1] >= value - w) ++q1;
+        project(x, q0, q1);
     };
     for (int j0 = 0; j0 < r2 && kept < r;) {
         int j1 = j0 + 1;
@@ -164,7 +186,7 @@ int recover_triplets(dmrg_zcanon_s& c, int s, cudaStream_t st) {
             cx.emplace_back(d);
             for (int i = 0; i < d; ++i) cx.back()[i] = cplx(x[i], x[d + i]);
             cs.push_back(sig[j]);
-            for (int pass = 0; pass < 2; ++pass) project(cx.back(), 0, kept);
+            for (int pass = 0; pass < 2; ++pass) project_near(cx.back(), sig[j]);
         }
         // in descending order, a candidate whose remainder keeps more than half
         // its norm is a new complex direction (the other real vector of a

@@ -360,7 +360,13 @@ int dmrg_zlanczos(dmrg_zheff_t h, double* psi, int niter, double precision, doub
     if (!h || !psi || !energy || niter <= 0) return set_error(DMRG_E_ARG, "invalid Lanczos arguments");
     if (niter > kMaxVec) return set_error(DMRG_E_ARG, "niter %d above %d", niter, kMaxVec);
     DMRG_TRY(ensure_zwork(*h, niter));
-    if (h->site.ket.size < 100) {  // the dense branch (complex_tensor_lanczos.cc:34-56)
+    // The dense branch (complex_tensor_lanczos.cc:34-56) diagonalises the real
+    // form (2 psi_dim) with the one-CTA Jacobi while that fits in shared memory
+    // (psi_dim <= 56); above, up to psi_dim 99, its global-memory form takes
+    // 50-300 ms a call, so the Krylov run of the same operator takes over: its
+    // space is the whole one after psi_dim steps at most, and it stops at the
+    // same ground state (any vector of it, if degenerate).
+    if (h->site.ket.size < 100 && sym_jacobi_in_shared(2 * (int)h->site.ket.size)) {
         if (iters) *iters = 0;
         return zexact(*h, psi, energy);
     }
