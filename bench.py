@@ -13,7 +13,10 @@ synthetic values.  A step = one matvec.
 The line also carries `split`: the same matvec through a DMRG_PREC_TF32X3
 operator (tcgen05 tensor cores), its time and its error against the FP64 result;
 and `sweep`: the wall time of one whole DMRG run of the same cylinder input (8
-sweeps, D up to 1024) through dmrg_run_execute (N=1 only).
+sweeps, D up to 1024) through dmrg_run_execute (N=1 only), in FP64 and with
+TF32X3 matvecs; `two_site`: the same run with two-site sweeps; `complex`: a
+whole complex run (Hofstadter 6x6); `scan`: the 64-instance U/t scan side by
+side.
 
 Multi-GPU: replicas only (each rank runs its own matvec; no collective on the
 data path); value = all ranks' FLOPs / max-over-ranks time.
@@ -342,6 +345,85 @@ def sweep_pair(ctx) -> dict:
     return fp64
 
 
+def two_site_form(ctx) -> dict:
+    """Two-site sweeps (dmrg_run_options_t.two_site) over the same cylinder input
+    and sweep table, in FP64 and with TF32X3 matvecs: whole-run and per-sweep wall
+    times (the last sweeps run at D=1024), phases, final energies and the split
+    run's |dE/site| against the FP64 run (32 sites)."""
+    from dmrgcc_b200 import capi
+
+    res = {}
+    for name, prec in (("fp64", capi.DMRG_PREC_FP64), ("tf32x3", capi.DMRG_PREC_TF32X3)):
+        run = capi.Run(ctx, CYL_INPUT, verbose=0, precision=prec, two_site=True)
+        t0 = time.perf_counter()
+        run.execute()
+        total = time.perf_counter() - t0
+        e, s = run.half_sweeps()
+        ph, sw = run.phases()
+        res[name] = {"total_s": total, "per_sweep_s": [float(s[2 * i] + s[2 * i + 1]) for i in range(len(s) // 2)],
+                     "phase_s": {k: float(v) for k, v in zip(capi.Run.PHASES, ph.sum(axis=0))},
+                     "svd_sweeps": int(sw.sum()), "final_energy": float(e[-1])}
+        run.close()
+    out = {"workload": "two-site DMRG, 8x4 Bose-Hubbard cylinder (d=5, N=16, U=8), D 128->1024, 8 sweeps"}
+    out.update(res)
+    out["speedup_vs_fp64"] = res["fp64"]["total_s"] / res["tf32x3"]["total_s"]
+    out["last_sweep_speedup_vs_fp64"] = res["fp64"]["per_sweep_s"][-1] / res["tf32x3"]["per_sweep_s"][-1]
+    out["abs_dE_per_site_tf32x3_vs_fp64"] = abs(res["tf32x3"]["final_energy"] - res["fp64"]["final_energy"]) / 32.0
+    return out
+
+
+CPLX_INPUT = os.path.join(ROOT, "dmrgcc_b200", "inputs", "hofstadter6x6.in")
+CPLX_MODEL = os.path.join(ROOT, "oracle", "_ref", "complex_spinful_bose_square_model")
+CPLX_REFERENCE = os.path.join(ROOT, "tests", "golden", "hofstadter6x6_reference.txt")
+
+
+def complex_form(ctx, threads: int) -> dict:
+    """The complex path on the Hofstadter geometry of configuration 3 (6x6,
+    periodic in y, flux 1/6, U=10, d=3; 4 bosons, D ramp 32 -> 256, 5 sweeps;
+    hofstadter6x6.in): the whole complex run (dmrg_run_execute, every tensor
+    complex), its final energy against the reference's on the same input
+    (tests/golden/hofstadter6x6_reference.txt, 1 BLAS thread), and the
+    reference's initialisation + first sweep timed on this host beside the
+    library's (`threads` BLAS threads)."""
+    import tempfile
+
+    from dmrgcc_b200 import capi
+
+    run = capi.Run(ctx, CPLX_INPUT, verbose=0, model="complex_spinful_bose_square")
+    t0 = time.perf_counter()
+    run.execute()
+    total = time.perf_counter() - t0
+    e, s = run.half_sweeps()
+    ph, _ = run.phases()
+    run.close()
+    out = {"workload": "complex Hofstadter 6x6 (flux 1/6, 4 bosons, d=3), D 32->256, 5 sweeps",
+           "total_s": total, "phase_s": {k: float(v) for k, v in zip(capi.Run.PHASES, ph.sum(axis=0))},
+           "final_energy": float(e[-1])}
+    if os.path.exists(CPLX_REFERENCE):
+        with open(CPLX_REFERENCE) as f:
+            e_ref = float([ln.split()[1] for ln in f if ln.startswith("hofstadter6x6")][0])
+        out["reference_final_energy"] = e_ref
+        out["abs_dE_per_site_vs_reference"] = abs(float(e[-1]) - e_ref) / 36.0
+    if os.path.exists(CPLX_MODEL):
+        with tempfile.TemporaryDirectory() as tmp:
+            inp = os.path.join(tmp, "h66_first_sweep.in")
+            first_sweep_input(CPLX_INPUT, inp)
+            env = dict(os.environ, OMP_NUM_THREADS=str(threads), OPENBLAS_NUM_THREADS=str(threads))
+            t0 = time.perf_counter()
+            r = subprocess.run([CPLX_MODEL, inp], capture_output=True, text=True, env=env, cwd=tmp, timeout=900)
+            ref_wall = time.perf_counter() - t0
+            lib = capi.Run(ctx, inp, verbose=0, model="complex_spinful_bose_square")
+            t0 = time.perf_counter()
+            lib.execute()
+            lib_wall = time.perf_counter() - t0
+            lib.close()
+        if r.returncode == 0:
+            out["reference_cpu_sample"] = {"sample": "initialisation + first sweep (D=32) of the same input",
+                                           "cores": threads, "reference_s": ref_wall, "library_s": lib_wall,
+                                           "speedup": ref_wall / lib_wall}
+    return out
+
+
 def run_b200(args) -> None:
     import numpy as np
     import torch
@@ -480,6 +562,9 @@ def run_b200(args) -> None:
                 sp["speedup_vs_fp64"] = ms_per_step / sp["ms_per_step"]
         if world == 1 and not args.no_sweep:
             line["sweep"] = sweep_pair(ctx)
+        if world == 1 and not args.no_sweep:
+            line["two_site"] = two_site_form(ctx)
+            line["complex"] = complex_form(ctx, os.cpu_count() or 1)
         if world == 1 and not args.no_scan:
             line["scan"] = scan_form(min(os.cpu_count() or 1, 64))
         cpu = cpu_reference(args.cpu_reps, 1, os.cpu_count() or 1) if not args.no_cpu else {"unavailable": "skipped"}

@@ -258,6 +258,22 @@ def converged_reference() -> None:
         f.write(f"{e[-2]:.12f}\n{e[-1]:.12f}\n")
 
 
+def complex_run_reference() -> None:
+    """hofstadter6x6_reference.txt: the reference's final energy on
+    hofstadter6x6.in (complex_spinful_bose_square_model, 1 BLAS thread): the
+    Hofstadter geometry of configuration 3 with 4 bosons (the reference's model
+    crashes on this lattice with 5 or 6 bosons)."""
+    tmp = tempfile.mkdtemp(prefix="golden_h66_")
+    env = dict(os.environ, OMP_NUM_THREADS="1", OPENBLAS_NUM_THREADS="1")
+    model = os.path.join(ROOT, "oracle", "_ref", "complex_spinful_bose_square_model")
+    r = subprocess.run([model, os.path.join(ROOT, "dmrgcc_b200", "inputs", "hofstadter6x6.in")], capture_output=True,
+                       text=True, env=env, cwd=tmp, check=True)
+    e = [float(ln.split("=")[1]) for ln in r.stdout.splitlines() if "energy =" in ln][-1]
+    with open(os.path.join(HERE, "hofstadter6x6_reference.txt"), "w") as f:
+        f.write("# final energy of complex_spinful_bose_square_model on hofstadter6x6.in (1 BLAS thread)\n")
+        f.write(f"hofstadter6x6 {e:.14f}\n")
+
+
 SPINFUL_MODELS = ("spinful4x4", "spinful3x3_periodic_y")
 COMPLEX_MODELS = ("hofstadter4x3",)
 
@@ -401,6 +417,7 @@ def main() -> int:
     ap.add_argument("--spinful", action="store_true", help="only the spinful model fixtures")
     ap.add_argument("--complex", action="store_true", help="only the complex-path (Hofstadter) fixtures")
     ap.add_argument("--converged", action="store_true", help="only the converged chain16 energy (D=256)")
+    ap.add_argument("--complex-run", action="store_true", help="only the reference energy of hofstadter6x6.in")
     ap.add_argument("--reuse", action="append", default=[], metavar="LABEL=DIR",
                     help="for --spread: take run LABEL (stock, pinned, 'seed s') from DIR/log.txt")
     args = ap.parse_args()
@@ -426,6 +443,9 @@ def main() -> int:
         return 0
     if args.converged:
         converged_reference()
+        return 0
+    if args.complex_run:
+        complex_run_reference()
         return 0
     quicksort_cases()
     tmp = tempfile.mkdtemp(prefix="golden_")

@@ -47,3 +47,17 @@ def test_complex_path_on_a_real_model_matches_the_real_path(ctx, tmp_path):
     e_ed = ground_energy_spinful(4, 3, 3, 0, 3, -1.0, -1.0, 10.0, 0.0, 0.0, 0.0, False, True)
     assert abs(ez.half_sweeps()[0][-1] - e_ed) / 12 <= 1e-10
     assert abs(er.half_sweeps()[0][-1] - e_ed) / 12 <= 1e-10
+
+
+def test_hofstadter_6x6_matches_the_reference_run(ctx):
+    """The Hofstadter geometry of configuration 3 (6x6, periodic in y, flux
+    1/6, 4 bosons, D <= 256; hofstadter6x6.in): the final energy within 1e-10
+    per lattice site of the reference's run of the same input
+    (tests/golden/hofstadter6x6_reference.txt)."""
+    run = capi.Run(ctx, os.path.join(ROOT, "dmrgcc_b200", "inputs", "hofstadter6x6.in"),
+                   model="complex_spinful_bose_square")
+    run.execute()
+    with open(os.path.join(GOLD, "hofstadter6x6_reference.txt")) as f:
+        e_ref = float([ln.split()[1] for ln in f if ln.startswith("hofstadter6x6")][0])
+    e = run.half_sweeps()[0][-1]
+    assert abs(e - e_ref) / 36 <= 1e-10, (e, e_ref)
