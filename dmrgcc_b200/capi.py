@@ -564,7 +564,8 @@ class RunOptions(C.Structure):
     """dmrg_run_options_t."""
 
     _fields_ = [("precision", C.c_int), ("verbose", C.c_int), ("seed", C.c_uint),
-                ("stop_after_half_sweeps", C.c_int), ("lanczos_precision", C.c_double), ("two_site", C.c_int)]
+                ("stop_after_half_sweeps", C.c_int), ("lanczos_precision", C.c_double), ("two_site", C.c_int),
+                ("lanczos_graph", C.c_int)]
 
 
 class Run:
@@ -572,9 +573,10 @@ class Run:
 
     def __init__(self, ctx: Context, input_path: str, model: str = "real_spinless_bose_square", verbose: int = 0,
                  seed: int = 1, stop_after_half_sweeps: int = -1, precision: int = DMRG_PREC_FP64,
-                 two_site: bool = False):
+                 two_site: bool = False, lanczos_graph: int = 0):
         self.ctx = ctx
-        self._opt = RunOptions(precision, verbose, seed, stop_after_half_sweeps, 0.0, int(bool(two_site)))
+        self._opt = RunOptions(precision, verbose, seed, stop_after_half_sweeps, 0.0, int(bool(two_site)),
+                               int(lanczos_graph))
         h = _VP()
         check(lib().dmrg_run_create(ctx.h, input_path.encode(), model.encode(), C.byref(self._opt), C.byref(h)),
               "dmrg_run_create")

@@ -99,6 +99,7 @@ int dmrg_run_create(dmrg_ctx_t ctx, const char* input_path, const char* model, c
             o.stop_after_half_sweeps = opt->stop_after_half_sweeps;
             if (opt->lanczos_precision > 0) o.lanczos_precision = opt->lanczos_precision;
             o.two_site = opt->two_site != 0;
+            o.lanczos_graph = opt->lanczos_graph == 0 ? -1 : (opt->lanczos_graph > 0 ? 1 : 0);
         }
         InputGroup input(input_path, "input", o.verbose != 0);
         ModelSpec m = make_model(input, model ? model : "real_spinless_bose_square");

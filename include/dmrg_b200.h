@@ -352,6 +352,10 @@ typedef struct {
                                    (dmrg_heff_create_blocks), a per-middle-sector
                                    SVD truncated to maxm, the environment update.
                                    No reference counterpart. */
+    int lanczos_graph;          /* 0: the default (each Lanczos call one CUDA
+                                   graph launch in a single run, launch by
+                                   launch in dmrg_run_execute_many); 1: graphs
+                                   always; -1: never */
 } dmrg_run_options_t;
 int dmrg_run_create(dmrg_ctx_t ctx, const char* input_path, const char* model,
                     const dmrg_run_options_t* opt, dmrg_run_t* out);
