@@ -102,7 +102,7 @@ _SIGS = {
     "dmrg_zcanon_out_blocks": (C.c_int, [_VP, _I, _I, _I, _I, _I]),
     "dmrg_zcanon_singular_values": (C.c_int, [_VP, C.c_int, C.c_int, _D, _I]),
     "dmrg_zcanon_write": (C.c_int, [_VP, _VP, _VP, _VP]),
-    "dmrg_svd_pair_schedule": (C.c_int, [C.POINTER(C.c_ushort)]),
+    "dmrg_svd_pair_schedule": (C.c_int, [C.POINTER(C.c_uint)]),
     "dmrg_svd_set_max_sweeps": (C.c_int, [C.c_int]),
     "dmrg_quicksort_index": (C.c_int, [_D, _I, C.c_int, C.c_int]),
     "dmrg_truncate_dims": (C.c_int, [C.c_int, _I, _D, C.c_int, C.c_double, _I]),
@@ -554,9 +554,10 @@ def truncate_dims(svals, max_dim: int, canpre: float):
 
 def svd_pair_schedule() -> np.ndarray:
     """The Jacobi pair solve's rotation schedule, [63 steps, 32 lanes] of
-    a | b << 6 | flip << 12 (host data; no GPU needed)."""
-    out = np.zeros(63 * 32, dtype=np.uint16)
-    check(lib().dmrg_svd_pair_schedule(out.ctypes.data_as(C.POINTER(C.c_ushort))), "dmrg_svd_pair_schedule")
+    a | b << 6 | flip << 12 | seat lane << 13 | seat flip << 18 (host data; no
+    GPU needed)."""
+    out = np.zeros(63 * 32, dtype=np.uint32)
+    check(lib().dmrg_svd_pair_schedule(out.ctypes.data_as(C.POINTER(C.c_uint))), "dmrg_svd_pair_schedule")
     return out.reshape(63, 32)
 
 

@@ -40,16 +40,32 @@ constexpr int kGramMinRows = DMRG_SVD_GRAM_MIN_ROWS;  // rows of a Gram item, at
 // meaningful in FP64; rotating them only stirs rounding noise).
 constexpr double kZeroRel = 4.0 * DBL_EPSILON;
 
+constexpr int kSteps = kPair - 1;                 // steps of one cyclic sweep of a pair
+constexpr int kMaxSteps = kInnerSweeps * kSteps;  // rotation log capacity
+
 struct SvdSmem {
-    double G[kPair * kLd];
-    double Q[kPair * kLd];
-    double2 cs[kPair / 2];   // (c, s) of the step's rotation k
-    int2 pq[kPair / 2];      // the columns (first, second) that rotation k mixes
+    // the Gram matrix, double-buffered: a step reads one copy and writes the
+    // other, so that one barrier per step orders every read before the writes
+    double G[2][kPair * kLd];
+    // rotation log: step t, seat lane j -> (c, s) of the rotation of the two
+    // columns seated at lane j (see seat_column), oriented (first, second)
+    double2 log[kMaxSteps * (kPair / 2)];
+    double2 cs[kPair / 2];   // (c, s) of the step's rotation k, oriented as schedule entry k addresses it
+    int active[2];           // by step parity: the step rotates something
     double red[kThreads / 32];
     double flag;
-    int active;   // the current step rotates something
-    uint16_t sched[(kPair - 1) * (kPair / 2)];   // the pair schedule (pair_schedule())
+    uint32_t sched[kSteps * (kPair / 2)];   // the pair schedule (pair_schedule())
 };
+
+// Seating of the pair solve's columns (the circle method of a round-robin
+// tournament): at step r, seat 0 holds column 0 and seat s >= 1 holds column
+// ((s - 1 - r) mod 63) + 1; seat lane j owns seats j and 63 - j, whose columns
+// are the pair rotated at that step.  From one step to the next the column in
+// seat s moves to seat s + 1 (seat 63 to seat 1; seat 0 stays), so a lane's two
+// columns reach their next seats by one shuffle each way.
+__host__ __device__ __forceinline__ int seat_column(int seat, int r) {
+    return seat == 0 ? 0 : ((seat - 1 - r) % kSteps + kSteps) % kSteps + 1;
+}
 
 __host__ __device__ __forceinline__ void rr_pair(int r, int i, int N, int& p, int& q) {
     if (i == 0) {
@@ -172,7 +188,7 @@ __global__ void __launch_bounds__(kThreads) solve_kernel(const SvdProblem* __res
                                                          const double* __restrict__ gpart,
                                                          const double* __restrict__ fro2, double* __restrict__ rot,
                                                          int* __restrict__ skip, unsigned long long* __restrict__ conv,
-                                                         const uint16_t* __restrict__ sched, int inner_sweeps) {
+                                                         const uint32_t* __restrict__ sched, int inner_sweeps) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     SvdSmem& S = *reinterpret_cast<SvdSmem*>(smem_raw);
     const int t = first + blockIdx.x;
@@ -195,11 +211,10 @@ __global__ void __launch_bounds__(kThreads) solve_kernel(const SvdProblem* __res
 #pragma unroll
         for (int u = 0; u < kElems; ++u) {
             const int idx = threadIdx.x + u * kThreads;
-            S.G[(idx / kPair) * kLd + idx % kPair] = v[u];
-            S.Q[(idx / kPair) * kLd + idx % kPair] = (idx / kPair == idx % kPair) ? 1.0 : 0.0;
+            S.G[0][(idx / kPair) * kLd + idx % kPair] = v[u];
         }
     }
-    for (int idx = threadIdx.x; idx < (kPair - 1) * (kPair / 2); idx += kThreads) S.sched[idx] = sched[idx];
+    for (int idx = threadIdx.x; idx < kSteps * (kPair / 2); idx += kThreads) S.sched[idx] = sched[idx];
     __syncthreads();
 
     // ---- convergence measure over the pair: |g_ij| / (||A||_F max(|x_i|, |x_j|)),
@@ -212,8 +227,8 @@ __global__ void __launch_bounds__(kThreads) solve_kernel(const SvdProblem* __res
     for (int idx = threadIdx.x; idx < kPair * kPair; idx += kThreads) {
         const int a = idx / kPair, b = idx % kPair;
         if (a >= b) continue;
-        const double ga = S.G[a * kLd + a], gb = S.G[b * kLd + b];
-        if (ga > zero2 && gb > zero2) worst = fmax(worst, fabs(S.G[a * kLd + b]) / (fro * sqrt(fmax(ga, gb))));
+        const double ga = S.G[0][a * kLd + a], gb = S.G[0][b * kLd + b];
+        if (ga > zero2 && gb > zero2) worst = fmax(worst, fabs(S.G[0][a * kLd + b]) / (fro * sqrt(fmax(ga, gb))));
     }
     worst = block_max(worst, S);
     if (threadIdx.x == 0) {
@@ -229,98 +244,80 @@ __global__ void __launch_bounds__(kThreads) solve_kernel(const SvdProblem* __res
     // pair the measure above calls unconverged is rotated whatever the rounding
     // of either expression
     const double tol2f = 0.25 * tol * tol * fro * fro;
-    static_assert(kThreads % 32 == 0 && (kPair / 2) * (kPair / 2) % kThreads == 0 &&
-                      (kPair / 2) * kPair % kThreads == 0,
-                  "even split");
+    constexpr int kWarps = kThreads / 32;
+    constexpr int kItems = (kPair / 2) * (kPair / 2) / kThreads;  // 2x2 Gram blocks per thread
+    constexpr int kQRows = kPair / kWarps;                         // rows of Q per warp
+    static_assert(kThreads % 32 == 0 && kItems * kThreads == (kPair / 2) * (kPair / 2) && kQRows * kWarps == kPair,
+                  "even split of the Gram blocks and of the rows of Q");
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int steps = 0;  // rotation log entries written
+    int cur = 0;    // the copy of G holding the current matrix
     for (int sweep = 0; sweep < inner_sweeps; ++sweep) {
-        int rotated = 0;
-        for (int r = 0; r < kPair - 1; ++r) {
-            if (threadIdx.x < kPair / 2) {
-                const unsigned e = S.sched[r * (kPair / 2) + threadIdx.x];
+        bool rotated = false;
+        for (int r = 0; r < kSteps; ++r, ++steps) {
+            // Warp 0 computes the step's 32 rotations (lane k: the pair of schedule
+            // entry k) while the other warps load the entries they update (the
+            // addresses come from the static schedule); a barrier publishes the
+            // rotations, and a step that rotates nothing ends there.
+            const unsigned e = S.sched[r * (kPair / 2) + lane];
+            const int pc = (e >> 12) & 1 ? (e >> 6) & 63 : e & 63;  // the lane's columns in the order it addresses them
+            const int qc = (e >> 12) & 1 ? e & 63 : (e >> 6) & 63;
+            const double* Gc = S.G[cur];
+            int pi[kItems], qi[kItems];
+            double x[kItems][4];
+#pragma unroll
+            for (int u = 0; u < kItems; ++u) {
+                const unsigned ei = S.sched[r * (kPair / 2) + warp + kWarps * u];  // the row pair's entry
+                pi[u] = (ei >> 12) & 1 ? (ei >> 6) & 63 : ei & 63;
+                qi[u] = (ei >> 12) & 1 ? ei & 63 : (ei >> 6) & 63;
+                x[u][0] = Gc[pi[u] * kLd + pc];
+                x[u][1] = Gc[pi[u] * kLd + qc];
+                x[u][2] = Gc[qi[u] * kLd + pc];
+                x[u][3] = Gc[qi[u] * kLd + qc];
+            }
+            if (warp == 0) {
                 const int a = e & 63, b = (e >> 6) & 63;  // a < b
-                const bool flip = (e >> 12) & 1;
-                const double apq = S.G[a * kLd + b];
+                const double apq = Gc[a * kLd + b];
+                const double daa = Gc[a * kLd + a], dbb = Gc[b * kLd + b];
                 double c = 1.0, s = 0.0;
-                const double daa = S.G[a * kLd + a], dbb = S.G[b * kLd + b];
                 if (daa > zero2 && dbb > zero2 && apq * apq > tol2f * fmax(daa, dbb)) {
                     // The rotation with tan = sign(x) y / (|x| + sqrt(x^2 + y^2)),
                     // x = dbb - daa, y = 2 apq (the smaller root of the Jacobi
                     // equation), as c = u / sqrt(u^2 + y^2), s = sign(x) y / sqrt(u^2 + y^2)
                     // with u = |x| + sqrt(x^2 + y^2): no division.
-                    const double x = dbb - daa, y = 2.0 * apq;
-                    const double u = fabs(x) + sqrt(x * x + y * y);
+                    const double xd = dbb - daa, y = 2.0 * apq;
+                    const double u = fabs(xd) + sqrt(xd * xd + y * y);
                     const double rn = rsqrt(u * u + y * y);
                     c = u * rn;
-                    s = (x >= 0.0 ? y : -y) * rn;
+                    s = (xd >= 0.0 ? y : -y) * rn;
                 }
-                // rotating (b, a) by (c, -s) is rotating (a, b) by (c, s)
-                S.cs[threadIdx.x] = make_double2(c, flip ? -s : s);
-                S.pq[threadIdx.x] = flip ? make_int2(b, a) : make_int2(a, b);
+                // the lane addresses p first: rotating (b, a) by (c, -s) is rotating (a, b) by (c, s)
+                const double se = (e >> 12) & 1 ? -s : s;
+                S.cs[lane] = make_double2(c, se);
+                S.log[steps * (kPair / 2) + ((e >> 13) & 31)] = make_double2(c, ((e >> 18) & 1) ? -se : se);
                 const bool any = __any_sync(0xffffffffu, s != 0.0);
-                if (threadIdx.x == 0) S.active = any ? 1 : 0;
+                if (lane == 0) S.active[steps & 1] = any ? 1 : 0;
             }
             __syncthreads();
-            if (!S.active) {
-                __syncthreads();  // every thread has read the flag before the next step rewrites it
-                continue;
-            }
-            rotated = 1;
-            // G <- J^T G J: thread (i, j = lane) takes the 2x2 block of rows (a_i, b_i)
-            // and columns (a_j, b_j), both rotations at once; Q <- Q J: thread
-            // (row, j = lane).  The step's rotations touch disjoint entries, so every
-            // thread first loads all it updates and then stores.
-            constexpr int kGItems = (kPair / 2) * (kPair / 2) / kThreads;
-            constexpr int kQItems = kPair * (kPair / 2) / kThreads;
-            const int lane = threadIdx.x & 31;
+            if (!S.active[steps & 1]) continue;  // the same verdict for every thread
+            rotated = true;
+            // G <- J^T G J into the other copy: thread (i, j = lane) takes the 2x2
+            // block of rows (p_i, q_i) and columns (p_j, q_j), both rotations at
+            // once (an untouched block is copied), for i = warp + kWarps u
+            double* Gn = S.G[cur ^ 1];
             const double2 csj = S.cs[lane];
-            const int2 pqj = S.pq[lane];
-            double2 csi[kGItems];
-            int2 pqi[kGItems];
-            double x[kGItems][4];
-            bool gon[kGItems];
 #pragma unroll
-            for (int u = 0; u < kGItems; ++u) {
-                const int i = (threadIdx.x + u * kThreads) >> 5;
-                csi[u] = S.cs[i];
-                pqi[u] = S.pq[i];
-                gon[u] = csi[u].y != 0.0 || csj.y != 0.0;
-                if (gon[u]) {
-                    x[u][0] = S.G[pqi[u].x * kLd + pqj.x];
-                    x[u][1] = S.G[pqi[u].x * kLd + pqj.y];
-                    x[u][2] = S.G[pqi[u].y * kLd + pqj.x];
-                    x[u][3] = S.G[pqi[u].y * kLd + pqj.y];
-                }
+            for (int u = 0; u < kItems; ++u) {
+                const double2 csi = S.cs[warp + kWarps * u];
+                const double ci = csi.x, si = csi.y, c = csj.x, se = csj.y;
+                const double y11 = ci * x[u][0] - si * x[u][2], y12 = ci * x[u][1] - si * x[u][3];
+                const double y21 = si * x[u][0] + ci * x[u][2], y22 = si * x[u][1] + ci * x[u][3];
+                Gn[pi[u] * kLd + pc] = c * y11 - se * y12;
+                Gn[pi[u] * kLd + qc] = se * y11 + c * y12;
+                Gn[qi[u] * kLd + pc] = c * y21 - se * y22;
+                Gn[qi[u] * kLd + qc] = se * y21 + c * y22;
             }
-            double q[kQItems][2];
-            const bool qon = csj.y != 0.0;
-            if (qon) {
-#pragma unroll
-                for (int u = 0; u < kQItems; ++u) {
-                    const int row = (threadIdx.x + u * kThreads) >> 5;
-                    q[u][0] = S.Q[row * kLd + pqj.x];
-                    q[u][1] = S.Q[row * kLd + pqj.y];
-                }
-            }
-#pragma unroll
-            for (int u = 0; u < kGItems; ++u) {
-                if (gon[u]) {
-                    const double ci = csi[u].x, si = csi[u].y, cj = csj.x, sj = csj.y;
-                    const double y11 = ci * x[u][0] - si * x[u][2], y12 = ci * x[u][1] - si * x[u][3];  // rows
-                    const double y21 = si * x[u][0] + ci * x[u][2], y22 = si * x[u][1] + ci * x[u][3];
-                    S.G[pqi[u].x * kLd + pqj.x] = cj * y11 - sj * y12;                                  // columns
-                    S.G[pqi[u].x * kLd + pqj.y] = sj * y11 + cj * y12;
-                    S.G[pqi[u].y * kLd + pqj.x] = cj * y21 - sj * y22;
-                    S.G[pqi[u].y * kLd + pqj.y] = sj * y21 + cj * y22;
-                }
-            }
-            if (qon) {
-#pragma unroll
-                for (int u = 0; u < kQItems; ++u) {
-                    const int row = (threadIdx.x + u * kThreads) >> 5;
-                    S.Q[row * kLd + pqj.x] = csj.x * q[u][0] - csj.y * q[u][1];
-                    S.Q[row * kLd + pqj.y] = csj.y * q[u][0] + csj.x * q[u][1];
-                }
-            }
+            cur ^= 1;
             __syncthreads();
         }
         if (!rotated || sweep + 1 == inner_sweeps) break;  // uniform: every thread saw the same flags
@@ -329,13 +326,43 @@ __global__ void __launch_bounds__(kThreads) solve_kernel(const SvdProblem* __res
         for (int idx = threadIdx.x; idx < kPair * kPair; idx += kThreads) {
             const int a = idx / kPair, b = idx % kPair;
             if (a >= b) continue;
-            const double ga = S.G[a * kLd + a], gb = S.G[b * kLd + b], g = S.G[a * kLd + b];
+            const double ga = S.G[cur][a * kLd + a], gb = S.G[cur][b * kLd + b], g = S.G[cur][a * kLd + b];
             if (ga > zero2 && gb > zero2 && g * g > tol2f * fmax(ga, gb)) off = 1.0;
         }
         if (block_max(off, S) == 0.0) break;
     }
+    __syncthreads();  // the log is complete
+
+    // The accumulated rotation Q = J_0 J_1 ... from the log, in registers: warp w
+    // takes rows kQRows w ... of Q, lane j the two entries of each row in the
+    // columns seated at lane j.  After each step's rotation the entries move to their next
+    // seats (seat_column): seat s -> s + 1 for 1 <= s <= 62, seat 63 -> seat 1.
+    double q1[kQRows], q2[kQRows];
+#pragma unroll
+    for (int k = 0; k < kQRows; ++k) {
+        const int row = kQRows * warp + k;
+        q1[k] = row == lane ? 1.0 : 0.0;               // seat lane (column lane at step 0)
+        q2[k] = row == kPair - 1 - lane ? 1.0 : 0.0;   // seat 63 - lane
+    }
+    for (int t = 0; t < steps; ++t) {
+        const double2 cs = S.log[t * (kPair / 2) + lane];
+#pragma unroll
+        for (int k = 0; k < kQRows; ++k) {
+            const double f = cs.x * q1[k] - cs.y * q2[k], g = cs.y * q1[k] + cs.x * q2[k];
+            const double up = __shfl_up_sync(0xffffffffu, lane == 0 ? g : f, 1);  // seat j - 1 (lane 0: seat 63)
+            const double dn = __shfl_down_sync(0xffffffffu, g, 1);               // seat 62 - j
+            q1[k] = lane == 0 ? f : up;
+            q2[k] = lane == 31 ? f : dn;
+        }
+    }
     double* R = rot + (int64_t)blockIdx.x * kPair * kPair;
-    for (int idx = threadIdx.x; idx < kPair * kPair; idx += kThreads) R[idx] = S.Q[(idx / kPair) * kLd + idx % kPair];
+    const int c1 = seat_column(lane, steps), c2 = seat_column(kPair - 1 - lane, steps);
+#pragma unroll
+    for (int k = 0; k < kQRows; ++k) {
+        const int row = kQRows * warp + k;
+        R[row * kPair + c1] = q1[k];
+        R[row * kPair + c2] = q2[k];
+    }
 }
 
 // Stage 3: item = (pair task, segment, row range): the pair's 64 columns of W
@@ -544,9 +571,11 @@ __global__ void __launch_bounds__(256) sign_kernel(const SvdProblem* __restrict_
 }
 
 // Lane order of the pair solve's rotations.  Step r rotates the 32 column pairs
-// of the round-robin schedule rr_pair(r, k); chosen here is which lane takes
-// which pair and which of its two columns the lane addresses first.  Entry
-// (r, lane) = a | b << 6 | flip << 12, a < b, flip = the lane addresses b first.
+// seated at the 32 seat lanes (seat_column); chosen here is which lane of the
+// Gram update takes which pair and which of its two columns the lane addresses
+// first.  Entry (r, lane) = a | b << 6 | flip << 12 | j << 13 | jflip << 18:
+// a < b the pair's columns, flip = the lane addresses b first, j = the pair's
+// seat lane, jflip = the column in seat j is not the one addressed first.
 // In each half-warp the 16 first columns lie in 16 distinct 8-byte shared-memory
 // banks (column mod 16), and so do the 16 second columns, so that every 8-byte
 // access of a step's update takes the minimum of two wavefronts.  Such an order
@@ -555,8 +584,8 @@ __global__ void __launch_bounds__(256) sign_kernel(const SvdProblem* __restrict_
 // out-degree 2, and the oriented edges split into two perfect matchings (tail
 // residue -> head residue), one per half-warp.  Returns DMRG_OK or, if a check
 // of the result fails, DMRG_E_STATE.
-int build_pair_schedule(std::vector<uint16_t>& tab) {
-    constexpr int kP = kPair / 2, kR = 16, kSteps = kPair - 1;
+int build_pair_schedule(std::vector<uint32_t>& tab) {
+    constexpr int kP = kPair / 2, kR = 16;
     tab.assign(kSteps * kP, 0);
     std::vector<int> met(kPair * kPair, 0);
     for (int r = 0; r < kSteps; ++r) {
@@ -564,7 +593,9 @@ int build_pair_schedule(std::vector<uint16_t>& tab) {
         bool used[kP];
         std::vector<int> adj[kR];
         for (int k = 0; k < kP; ++k) {
-            rr_pair(r, k, kPair, pa[k], pb[k]);
+            const int c0 = seat_column(k, r), c1 = seat_column(kPair - 1 - k, r);
+            pa[k] = std::min(c0, c1);
+            pb[k] = std::max(c0, c1);
             adj[pa[k] % kR].push_back(k);
             adj[pb[k] % kR].push_back(k);
             used[k] = false;
@@ -614,7 +645,9 @@ int build_pair_schedule(std::vector<uint16_t>& tab) {
         for (int k = 0; k < kP; ++k) {
             if (side[k] < 0 || n[side[k]] >= kP / 2) return set_error(DMRG_E_STATE, "pair schedule: unbalanced split");
             const int slot = side[k] * (kP / 2) + n[side[k]]++;
-            tab[r * kP + slot] = (uint16_t)(pa[k] | pb[k] << 6 | (first[k] != pa[k] ? 1 : 0) << 12);
+            const int seated_first = seat_column(k, r);  // the column in seat k (seat lane k)
+            tab[r * kP + slot] = (uint32_t)(pa[k] | pb[k] << 6 | (first[k] != pa[k] ? 1 : 0) << 12 | k << 13 |
+                                            (seated_first != first[k] ? 1 : 0) << 18);
         }
         for (int h = 0; h < 2; ++h) {
             unsigned fm = 0, sm = 0;
@@ -634,8 +667,8 @@ int build_pair_schedule(std::vector<uint16_t>& tab) {
     return DMRG_OK;
 }
 
-const std::vector<uint16_t>* pair_schedule() {
-    static std::vector<uint16_t> tab;
+const std::vector<uint32_t>* pair_schedule() {
+    static std::vector<uint32_t> tab;
     static const int rc = build_pair_schedule(tab);
     return rc == DMRG_OK ? &tab : nullptr;
 }
@@ -722,7 +755,7 @@ int BatchedSvd::plan(const std::vector<int>& m, const std::vector<int>& n, cudaS
     DMRG_TRY(d_colmap.alloc((size_t)std::max<int64_t>(soff, 1) * sizeof(int)));
     DMRG_TRY(d_norm.alloc((size_t)std::max<int64_t>(soff, 1) * sizeof(double)));
     if (!d_sched.ptr) {
-        const std::vector<uint16_t>* sched = pair_schedule();
+        const std::vector<uint32_t>* sched = pair_schedule();
         if (!sched) return set_error(DMRG_E_STATE, "no pair schedule");
         DMRG_TRY(upload(d_sched, *sched, st));
     }
@@ -814,7 +847,7 @@ int BatchedSvd::run(cudaStream_t st, int* sweeps_out) {
             DMRG_LAUNCH solve_kernel<<<nt, kThreads, sizeof(SvdSmem), st>>>(
                 d_probs.as<SvdProblem>(), d_tasks.as<SvdTask>(), round_first[r], d_gpart.as<double>(),
                 d_fro2.as<double>(), d_rot.as<double>(), d_skip.as<int>(), d_conv.as<unsigned long long>(),
-                d_sched.as<uint16_t>(), kInnerSweeps);
+                d_sched.as<uint32_t>(), kInnerSweeps);
             DMRG_LAUNCH rotate_kernel<<<nr, 128, kRotSmem, st>>>(d_probs.as<SvdProblem>(), d_tasks.as<SvdTask>(),
                                                      d_rot_items.as<SvdItem>() + round_rot_first[r], r,
                                                      round_first[r], d_rot.as<double>(), d_skip.as<int>(),
@@ -900,10 +933,10 @@ extern "C" int dmrg_svd_set_max_sweeps(int sweeps) {
     return DMRG_OK;
 }
 
-extern "C" int dmrg_svd_pair_schedule(unsigned short* out) {
+extern "C" int dmrg_svd_pair_schedule(unsigned int* out) {
     if (!out) return dmrg::set_error(DMRG_E_ARG, "null argument");
-    const std::vector<uint16_t>* tab = dmrg::pair_schedule();
+    const std::vector<uint32_t>* tab = dmrg::pair_schedule();
     if (!tab) return DMRG_E_STATE;
-    std::memcpy(out, tab->data(), tab->size() * sizeof(uint16_t));
+    std::memcpy(out, tab->data(), tab->size() * sizeof(uint32_t));
     return DMRG_OK;
 }

@@ -314,11 +314,14 @@ int dmrg_canon_out_blocks(dmrg_canon_t c, int* ket_rows, int* ket_cols, int* can
 int dmrg_canon_singular_values(dmrg_canon_t c, int sector, int cap, double* values, int* count);
 int dmrg_canon_write(dmrg_canon_t c, const double* ket_dev, double* new_ket_dev, double* canonical_dev);
 /* The Jacobi pair solve's rotation schedule (diagnostic; no reference
- * counterpart): out[63 * 32], entry (step r, lane) = a | b << 6 | flip << 12 with
- * (a, b), a < b, the pair of the pair's 64 columns that the lane rotates in step
- * r and flip = the lane addresses b first.  Every two columns share one step;
+ * counterpart): out[63 * 32], entry (step r, lane) = a | b << 6 | flip << 12 |
+ * j << 13 | jflip << 18 with (a, b), a < b, the pair of the pair's 64 columns
+ * that the lane rotates in step r, flip = the lane addresses b first, j = the
+ * seat lane holding the pair (seats j and 63 - j; at step r seat 0 holds column
+ * 0 and seat s >= 1 column ((s - 1 - r) mod 63) + 1) and jflip = the column in
+ * seat j is not the one addressed first.  Every two columns share one step;
  * within each half-warp the first (and the second) columns are distinct mod 16. */
-int dmrg_svd_pair_schedule(unsigned short* out);
+int dmrg_svd_pair_schedule(unsigned int* out);
 /* Cap on the Jacobi sweeps of every later canonicalisation in this process
  * (sweeps <= 0: the default, 40).  A canonicalisation that does not converge
  * within the cap returns DMRG_E_NUMERIC, as the reference treats a failed
