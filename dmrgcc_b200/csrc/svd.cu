@@ -111,16 +111,14 @@ __device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, dou
 constexpr int kGramLd = kChunk + 4;
 __global__ void __launch_bounds__(128) gram_kernel(const SvdProblem* __restrict__ probs,
                                                    const SvdTask* __restrict__ tasks,
-                                                   const SvdItem* __restrict__ items, int round,
+                                                   const SvdItem* __restrict__ items,
                                                    const int* __restrict__ colmap, const double* __restrict__ W,
                                                    double* __restrict__ gpart) {
     __shared__ double Xt[kPair * kGramLd];  // Xt[c][k]
     const SvdItem it = items[blockIdx.x];
     const SvdTask task = tasks[it.task];
     const SvdProblem p = probs[task.problem];
-    int I, J;
-    rr_pair(round, task.pair, p.nbe, I, J);
-    const int colI = I * kBlk, colJ = J * kBlk;
+    const int colI = task.bi * kBlk, colJ = task.bj * kBlk;
     const double* Wp = W + p.w_off;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int wm = warp >> 1, wn = warp & 1, fr = lane >> 2, fc = lane & 3;
@@ -179,6 +177,87 @@ __global__ void __launch_bounds__(128) gram_kernel(const SvdProblem* __restrict_
         }
 }
 
+// Convergence measure of a sweep: one CTA per tile (problem, bi <= bj), the
+// 32x32 block X_bi^T X_bj of the sector's Gram matrix over all rows (DMMA, 2x2
+// warps of 16x16), reduced to the largest pair measure
+// |g_ab| / (||A||_F max(|x_a|, |x_b|)) over its column pairs a < b (norms from
+// the sweep's column norms), skipping columns at rounding level.
+__global__ void __launch_bounds__(128) measure_kernel(const SvdProblem* __restrict__ probs,
+                                                      const SvdTile* __restrict__ tiles,
+                                                      const int* __restrict__ colmap, const double* __restrict__ W,
+                                                      const double* __restrict__ norm, const double* __restrict__ fro2,
+                                                      double* __restrict__ bm) {
+    __shared__ double Xt[kPair * kGramLd];  // Xt[c][k]: c < 32 block bi, c >= 32 block bj
+    __shared__ double red[4];
+    const SvdTile tile = tiles[blockIdx.x];
+    const SvdProblem p = probs[tile.problem];
+    const int colI = tile.bi * kBlk, colJ = tile.bj * kBlk;
+    const double* Wp = W + p.w_off;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int wm = warp >> 1, wn = warp & 1, fr = lane >> 2, fc = lane & 3;
+    double acc[2][2][2];
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 2; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+    constexpr int kCols = kChunk * kPair / 128;
+    const int k = lane;
+    int64_t coff[kCols];
+#pragma unroll
+    for (int e = 0; e < kCols; ++e) {
+        const int c = warp + 4 * e;
+        const int vc = c < kBlk ? colI + c : colJ + c - kBlk;
+        coff[e] = vc < p.cols ? (int64_t)colmap[p.perm_off + vc] * p.rows : -1;
+    }
+    double nxt[kCols];
+#pragma unroll
+    for (int e = 0; e < kCols; ++e) nxt[e] = (coff[e] >= 0 && k < p.rows) ? Wp[coff[e] + k] : 0.0;
+    for (int k0 = 0; k0 < p.rows; k0 += kChunk) {
+#pragma unroll
+        for (int e = 0; e < kCols; ++e) Xt[(warp + 4 * e) * kGramLd + k] = nxt[e];
+        __syncthreads();
+        const int k1 = k0 + kChunk;
+        if (k1 < p.rows) {
+#pragma unroll
+            for (int e = 0; e < kCols; ++e) nxt[e] = (coff[e] >= 0 && k1 + k < p.rows) ? Wp[coff[e] + k1 + k] : 0.0;
+        }
+#pragma unroll
+        for (int kk = 0; kk < kChunk; kk += 4) {
+            double a[2], b[2];
+#pragma unroll
+            for (int i = 0; i < 2; ++i) a[i] = Xt[(wm * 16 + i * 8 + fr) * kGramLd + kk + fc];
+#pragma unroll
+            for (int j = 0; j < 2; ++j) b[j] = Xt[(kBlk + wn * 16 + j * 8 + fr) * kGramLd + kk + fc];
+#pragma unroll
+            for (int i = 0; i < 2; ++i)
+#pragma unroll
+                for (int j = 0; j < 2; ++j) dmma_8x8x4(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+        }
+        __syncthreads();
+    }
+    const double f2 = fro2[tile.problem];
+    const double fro = sqrt(f2);
+    const double zero2 = kZeroRel * kZeroRel * (double)p.rows * f2;
+    double worst = 0.0;
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 2; ++j)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int a = colI + wm * 16 + i * 8 + fr, b = colJ + wn * 16 + j * 8 + 2 * fc + h;
+                if (a >= p.cols || b >= p.cols || a >= b) continue;
+                const double na = norm[p.s_off + colmap[p.perm_off + a]], nb = norm[p.s_off + colmap[p.perm_off + b]];
+                if (na * na <= zero2 || nb * nb <= zero2) continue;
+                worst = fmax(worst, fabs(acc[i][j][h]) / (fro * fmax(na, nb)));
+            }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) worst = fmax(worst, __shfl_xor_sync(0xffffffffu, worst, o));
+    if (lane == 0) red[warp] = worst;
+    __syncthreads();
+    if (threadIdx.x == 0) bm[blockIdx.x] = fmax(fmax(red[0], red[1]), fmax(red[2], red[3]));
+}
+
 // Stage 2: one CTA per pair task.  Sums the task's partial Gram matrices (fixed
 // order), measures the pair's convergence, and (unless converged) runs a few
 // cyclic Jacobi sweeps on the 64x64 Gram matrix, writing the accumulated 64x64
@@ -187,8 +266,8 @@ __global__ void __launch_bounds__(kThreads) solve_kernel(const SvdProblem* __res
                                                          const SvdTask* __restrict__ tasks, int first,
                                                          const double* __restrict__ gpart,
                                                          const double* __restrict__ fro2, double* __restrict__ rot,
-                                                         int* __restrict__ skip, unsigned long long* __restrict__ conv,
-                                                         const uint32_t* __restrict__ sched, int inner_sweeps) {
+                                                         int* __restrict__ skip, const uint32_t* __restrict__ sched,
+                                                         int inner_sweeps) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     SvdSmem& S = *reinterpret_cast<SvdSmem*>(smem_raw);
     const int t = first + blockIdx.x;
@@ -231,10 +310,7 @@ __global__ void __launch_bounds__(kThreads) solve_kernel(const SvdProblem* __res
         if (ga > zero2 && gb > zero2) worst = fmax(worst, fabs(S.G[0][a * kLd + b]) / (fro * sqrt(fmax(ga, gb))));
     }
     worst = block_max(worst, S);
-    if (threadIdx.x == 0) {
-        atomicMax(conv + task.problem, (unsigned long long)__double_as_longlong(worst));
-        skip[blockIdx.x] = worst <= tol ? 1 : 0;
-    }
+    if (threadIdx.x == 0) skip[blockIdx.x] = worst <= tol ? 1 : 0;
     if (worst <= tol) return;  // pair already orthogonal: nothing to rotate
 
     // A pair whose off-diagonal measure is at or below tol needs no rotation (the
@@ -373,7 +449,7 @@ constexpr int kRotLd = kPair + 4;
 constexpr size_t kRotSmem = 2 * sizeof(double) * kPair * kRotLd;
 __global__ void __launch_bounds__(128) rotate_kernel(const SvdProblem* __restrict__ probs,
                                                      const SvdTask* __restrict__ tasks,
-                                                     const SvdItem* __restrict__ items, int round, int first,
+                                                     const SvdItem* __restrict__ items, int first,
                                                      const double* __restrict__ rot, const int* __restrict__ skip,
                                                      const int* __restrict__ colmap, double* __restrict__ W,
                                                      double* __restrict__ Qacc) {
@@ -384,9 +460,7 @@ __global__ void __launch_bounds__(128) rotate_kernel(const SvdProblem* __restric
     if (skip[it.task - first]) return;
     const SvdTask task = tasks[it.task];
     const SvdProblem p = probs[task.problem];
-    int I, J;
-    rr_pair(round, task.pair, p.nbe, I, J);
-    const int colI = I * kBlk, colJ = J * kBlk;
+    const int colI = task.bi * kBlk, colJ = task.bj * kBlk;
     double* base = it.seg == 0 ? W + p.w_off : Qacc + p.q_off;
     const int ld = it.seg == 0 ? p.rows : p.cols;
     const double* Rg = rot + (int64_t)(it.task - first) * kPair * kPair;
@@ -677,11 +751,10 @@ const std::vector<uint32_t>* pair_schedule() {
 
 int BatchedSvd::plan(const std::vector<int>& m, const std::vector<int>& n, cudaStream_t st) {
     probs.clear();
-    tasks.clear();
-    round_first.clear();
+    tiles.clear();
+    tile_first.clear();
     index.assign(m.size(), -1);
     int64_t woff = 0, qoff = 0, soff = 0;
-    max_rounds = 0;
     for (size_t i = 0; i < m.size(); ++i) {
         if ((int64_t)m[i] * n[i] <= 0) continue;
         SvdProblem p{};
@@ -700,83 +773,195 @@ int BatchedSvd::plan(const std::vector<int>& m, const std::vector<int>& n, cudaS
         qoff += (int64_t)p.cols * p.cols;
         soff += p.cols;
         index[i] = (int)probs.size();
+        tile_first.push_back((int)tiles.size());
+        for (int bi = 0; bi < nb; ++bi)
+            for (int bj = bi; bj < nb; ++bj) tiles.push_back(SvdTile{(int)probs.size(), bi, bj, 0});
         probs.push_back(p);
-        max_rounds = std::max(max_rounds, p.nbe - 1);
     }
-    // Row ranges of the Gram items: at least kGramMinRows rows each, fewer items
-    // than ~4 per SM in the widest round (bounds the partial-Gram buffer).
-    int64_t widest = 0;
-    for (int r = 0; r < max_rounds; ++r) {
-        int64_t rows = 0;
-        for (const SvdProblem& p : probs)
-            if (r < p.nbe - 1) rows += (int64_t)p.rows * (p.nbe / 2);
-        widest = std::max(widest, rows);
+    tile_first.push_back((int)tiles.size());
+    // Capacities.  A sweep holds at most every block pair of a problem plus one
+    // pair per block for blocks unconverged only within themselves; a round at
+    // most nbe / 2 pairs per problem.  Row ranges of the Gram items: at least
+    // kGramMinRows rows each, fewer items than ~4 per SM in the widest round
+    // (bounds the partial-Gram buffer).
+    int64_t widest = 0, sweep_tasks = 0, sweep_gram = 0, sweep_rot = 0, round_tasks = 0;
+    for (const SvdProblem& p : probs) {
+        widest += (int64_t)p.rows * (p.nbe / 2);
+        round_tasks += p.nbe / 2;
     }
-    const int gram_rows = (int)std::max<int64_t>(kGramMinRows, ((widest / 600 + 31) / 32) * 32);
-    gram_items.clear();
-    rot_items.clear();
-    round_gram_first.clear();
-    round_rot_first.clear();
-    max_round_tasks = max_round_gram = 0;
-    for (int r = 0; r < max_rounds; ++r) {
-        round_first.push_back((int)tasks.size());
-        round_gram_first.push_back((int)gram_items.size());
-        round_rot_first.push_back((int)rot_items.size());
-        for (int pi = 0; pi < (int)probs.size(); ++pi) {
-            const SvdProblem& p = probs[pi];
-            if (r >= p.nbe - 1) continue;
-            for (int k = 0; k < p.nbe / 2; ++k) {
-                const int t = (int)tasks.size();
-                SvdTask task{pi, k, (int)gram_items.size() - round_gram_first.back(), 0};
-                for (int r0 = 0; r0 < p.rows; r0 += gram_rows)
-                    gram_items.push_back(SvdItem{t, 0, r0, std::min(p.rows, r0 + gram_rows)});
-                task.g_count = (int)gram_items.size() - round_gram_first.back() - task.g_first;
-                tasks.push_back(task);
-                for (int r0 = 0; r0 < p.rows; r0 += kPair)
-                    rot_items.push_back(SvdItem{t, 0, r0, std::min(p.rows, r0 + kPair)});
-                for (int r0 = 0; r0 < p.cols; r0 += kPair)
-                    rot_items.push_back(SvdItem{t, 1, r0, std::min(p.cols, r0 + kPair)});
-            }
-        }
-        max_round_tasks = std::max(max_round_tasks, (int)tasks.size() - round_first.back());
-        max_round_gram = std::max(max_round_gram, (int)gram_items.size() - round_gram_first.back());
+    gram_rows = (int)std::max<int64_t>(kGramMinRows, ((widest / 600 + 31) / 32) * 32);
+    int64_t round_gram = 0;
+    for (const SvdProblem& p : probs) {
+        const int64_t pairs = (int64_t)p.nbe * (p.nbe - 1) / 2 + p.nbe;
+        const int64_t gi = (p.rows + gram_rows - 1) / gram_rows;
+        const int64_t ri = (p.rows + kPair - 1) / kPair + (p.cols + kPair - 1) / kPair;
+        sweep_tasks += pairs;
+        sweep_gram += pairs * gi;
+        sweep_rot += pairs * ri;
+        round_gram += (int64_t)(p.nbe / 2) * gi;
     }
-    round_first.push_back((int)tasks.size());
-    round_gram_first.push_back((int)gram_items.size());
-    round_rot_first.push_back((int)rot_items.size());
+    max_tasks = (int)sweep_tasks;
+    max_gram = (int)sweep_gram;
+    max_rot = (int)sweep_rot;
+    max_round_tasks = (int)round_tasks;
+    max_round_gram = (int)round_gram;
     DMRG_TRY(d_w.alloc((size_t)std::max<int64_t>(woff, 1) * sizeof(double)));
     DMRG_TRY(d_q.alloc((size_t)std::max<int64_t>(qoff, 1) * sizeof(double)));
     DMRG_TRY(d_s.alloc((size_t)std::max<int64_t>(2 * soff, 1) * sizeof(double)));
     DMRG_TRY(d_perm.alloc((size_t)std::max<int64_t>(soff, 1) * sizeof(int)));
-    DMRG_TRY(d_conv.alloc(std::max<size_t>(probs.size(), 1) * sizeof(unsigned long long)));
     DMRG_TRY(d_fro2.alloc(std::max<size_t>(probs.size(), 1) * sizeof(double)));
     DMRG_TRY(d_expo.alloc(std::max<size_t>(probs.size(), 1) * sizeof(int)));
     DMRG_TRY(d_sign.alloc((size_t)std::max<int64_t>(soff, 1) * sizeof(double)));
     DMRG_TRY(d_colmap.alloc((size_t)std::max<int64_t>(soff, 1) * sizeof(int)));
     DMRG_TRY(d_norm.alloc((size_t)std::max<int64_t>(soff, 1) * sizeof(double)));
+    DMRG_TRY(d_bm.alloc(std::max<size_t>(tiles.size(), 1) * sizeof(double)));
     if (!d_sched.ptr) {
         const std::vector<uint32_t>* sched = pair_schedule();
         if (!sched) return set_error(DMRG_E_STATE, "no pair schedule");
         DMRG_TRY(upload(d_sched, *sched, st));
     }
     DMRG_TRY(upload(d_probs, probs, st));
-    DMRG_TRY(upload(d_tasks, tasks, st));
-    DMRG_TRY(upload(d_gram_items, gram_items, st));
-    DMRG_TRY(upload(d_rot_items, rot_items, st));
+    DMRG_TRY(upload(d_tiles, tiles, st));
+    DMRG_TRY(d_tasks.alloc(std::max<size_t>(max_tasks, 1) * sizeof(SvdTask)));
+    DMRG_TRY(d_gram_items.alloc(std::max<size_t>(max_gram, 1) * sizeof(SvdItem)));
+    DMRG_TRY(d_rot_items.alloc(std::max<size_t>(max_rot, 1) * sizeof(SvdItem)));
     DMRG_TRY(d_gpart.alloc((size_t)std::max(max_round_gram, 1) * kPair * kPair * sizeof(double)));
     DMRG_TRY(d_rot.alloc((size_t)std::max(max_round_tasks, 1) * kPair * kPair * sizeof(double)));
     DMRG_TRY(d_skip.alloc((size_t)std::max(max_round_tasks, 1) * sizeof(int)));
     DMRG_CUDA_TRY(cudaFuncSetAttribute(solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)sizeof(SvdSmem)));
+    static_assert(sizeof(SvdSmem) <= 227 * 1024, "pair solve shared memory");
     DMRG_CUDA_TRY(cudaFuncSetAttribute(rotate_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRotSmem));
     return DMRG_OK;
 }
 
-// Appends, for each problem whose last sweep left a measure above tol: m, n,
-// rows, cols, transposed (int32), fro2 and the measure (float64), then its
-// input and final working matrices (rows x cols float64, column-major).
-void BatchedSvd::dump_unconverged(const char* path, const DeviceBuffer& w_in,
-                                  const std::vector<unsigned long long>& conv, cudaStream_t st) {
+void BatchedSvd::add_task(int problem, int bi, int bj) {
+    const SvdProblem& p = probs[problem];
+    const int t = (int)tasks.size();
+    SvdTask task{problem, bi, bj, (int)gram_items.size() - round_gram_first.back(), 0};
+    for (int r0 = 0; r0 < p.rows; r0 += gram_rows)
+        gram_items.push_back(SvdItem{t, 0, r0, std::min(p.rows, r0 + gram_rows)});
+    task.g_count = (int)gram_items.size() - round_gram_first.back() - task.g_first;
+    tasks.push_back(task);
+    for (int r0 = 0; r0 < p.rows; r0 += kPair) rot_items.push_back(SvdItem{t, 0, r0, std::min(p.rows, r0 + kPair)});
+    for (int r0 = 0; r0 < p.cols; r0 += kPair) rot_items.push_back(SvdItem{t, 1, r0, std::min(p.cols, r0 + kPair)});
+}
+
+// Rounds of one problem's sweep: its unconverged block pairs (measure > tol) as
+// a sequence of matchings, and every block unconverged within itself in some
+// pair.  Two candidates, the fewer rounds kept: the round-robin order over nbe
+// blocks restricted to those pairs, and a greedy matching by decreasing measure.
+static std::vector<std::vector<std::pair<int, int>>> problem_rounds(const SvdProblem& p, const double* bm,
+                                                                     double tol) {
+    const int nb = (p.cols + kBlk - 1) / kBlk;
+    auto at = [&](int i, int j) {  // tiles of a problem: bi <= bj, row-major over bi
+        if (i > j) std::swap(i, j);
+        return bm[i * nb - i * (i - 1) / 2 + (j - i)];
+    };
+    std::vector<std::pair<double, std::pair<int, int>>> cross;
+    std::vector<int> internal;
+    for (int i = 0; i < nb; ++i) {
+        if (at(i, i) > tol) internal.push_back(i);
+        for (int j = i + 1; j < nb; ++j)
+            if (at(i, j) > tol) cross.push_back({at(i, j), {i, j}});
+    }
+    using Rounds = std::vector<std::vector<std::pair<int, int>>>;
+    auto cover = [&](Rounds& rounds) {  // every internally unconverged block in some pair
+        std::vector<char> seen(p.nbe, 0);
+        for (const auto& rd : rounds)
+            for (const auto& pr : rd) seen[pr.first] = seen[pr.second] = 1;
+        for (int i : internal) {
+            if (seen[i]) continue;
+            bool placed = false;
+            for (auto& rd : rounds) {
+                std::vector<char> used(p.nbe, 0);
+                for (const auto& pr : rd) used[pr.first] = used[pr.second] = 1;
+                if (used[i]) continue;
+                for (int j = 0; j < p.nbe && !placed; ++j)
+                    if (j != i && !used[j]) {
+                        rd.push_back({std::min(i, j), std::max(i, j)});
+                        seen[j] = 1;
+                        placed = true;
+                    }
+                if (placed) break;
+            }
+            if (!placed) {
+                const int j = (i + 1) % p.nbe;
+                rounds.push_back({{std::min(i, j), std::max(i, j)}});
+                seen[j] = 1;
+            }
+            seen[i] = 1;
+        }
+    };
+    Rounds rr;
+    {
+        std::vector<char> need((size_t)p.nbe * p.nbe, 0);
+        for (const auto& c : cross) need[c.second.first * p.nbe + c.second.second] = 1;
+        for (int r = 0; r < p.nbe - 1; ++r) {
+            std::vector<std::pair<int, int>> rd;
+            for (int k = 0; k < p.nbe / 2; ++k) {
+                int i, j;
+                rr_pair(r, k, p.nbe, i, j);
+                if (need[i * p.nbe + j]) rd.push_back({i, j});
+            }
+            if (!rd.empty()) rr.push_back(rd);
+        }
+        cover(rr);
+    }
+    Rounds gr;
+    {
+        std::sort(cross.begin(), cross.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
+        std::vector<std::vector<char>> used;
+        for (const auto& c : cross) {
+            const int i = c.second.first, j = c.second.second;
+            size_t r = 0;
+            for (; r < gr.size(); ++r)
+                if (!used[r][i] && !used[r][j]) break;
+            if (r == gr.size()) {
+                gr.emplace_back();
+                used.emplace_back(p.nbe, 0);
+            }
+            gr[r].push_back({i, j});
+            used[r][i] = used[r][j] = 1;
+        }
+        cover(gr);
+    }
+    return gr.size() < rr.size() ? gr : rr;
+}
+
+int BatchedSvd::schedule(const std::vector<double>& bm) {
+    tasks.clear();
+    gram_items.clear();
+    rot_items.clear();
+    round_first.clear();
+    round_gram_first.clear();
+    round_rot_first.clear();
+    std::vector<std::vector<std::vector<std::pair<int, int>>>> per(probs.size());
+    size_t rounds = 0;
+    for (size_t pi = 0; pi < probs.size(); ++pi) {
+        const double tol = 2.0 * DBL_EPSILON * std::sqrt((double)probs[pi].rows);
+        per[pi] = problem_rounds(probs[pi], bm.data() + tile_first[pi], tol);
+        rounds = std::max(rounds, per[pi].size());
+    }
+    for (size_t r = 0; r < rounds; ++r) {
+        round_first.push_back((int)tasks.size());
+        round_gram_first.push_back((int)gram_items.size());
+        round_rot_first.push_back((int)rot_items.size());
+        for (size_t pi = 0; pi < probs.size(); ++pi)
+            if (r < per[pi].size())
+                for (const auto& pr : per[pi][r]) add_task((int)pi, pr.first, pr.second);
+    }
+    round_first.push_back((int)tasks.size());
+    round_gram_first.push_back((int)gram_items.size());
+    round_rot_first.push_back((int)rot_items.size());
+    return (int)rounds;
+}
+
+// Appends, for each problem whose last measure was above tol: m, n, rows,
+// cols, transposed (int32), fro2 and the measure (float64), then its input and
+// final working matrices (rows x cols float64, column-major).
+void BatchedSvd::dump_unconverged(const char* path, const DeviceBuffer& w_in, const std::vector<double>& worst,
+                                  cudaStream_t st) {
     std::FILE* f = std::fopen(path, "ab");
     if (!f) return;
     std::vector<double> fro2(probs.size());
@@ -784,16 +969,14 @@ void BatchedSvd::dump_unconverged(const char* path, const DeviceBuffer& w_in,
     cudaStreamSynchronize(st);
     for (size_t i = 0; i < probs.size(); ++i) {
         const SvdProblem& p = probs[i];
-        double worst;
-        std::memcpy(&worst, &conv[i], sizeof(double));
-        if (worst <= 2.0 * DBL_EPSILON * std::sqrt((double)p.rows)) continue;
+        if (worst[i] <= 2.0 * DBL_EPSILON * std::sqrt((double)p.rows)) continue;
         const size_t cnt = (size_t)p.rows * p.cols;
         std::vector<double> a(cnt), b(cnt);
         cudaMemcpyAsync(a.data(), w_in.as<double>() + p.w_off, cnt * sizeof(double), cudaMemcpyDeviceToHost, st);
         cudaMemcpyAsync(b.data(), d_w.as<double>() + p.w_off, cnt * sizeof(double), cudaMemcpyDeviceToHost, st);
         cudaStreamSynchronize(st);
         const int hdr[5] = {p.m, p.n, p.rows, p.cols, p.transposed};
-        const double val[2] = {fro2[i], worst};
+        const double val[2] = {fro2[i], worst[i]};
         std::fwrite(hdr, sizeof(int), 5, f);
         std::fwrite(val, sizeof(double), 2, f);
         std::fwrite(a.data(), sizeof(double), cnt, f);
@@ -820,84 +1003,87 @@ int BatchedSvd::run(cudaStream_t st, int* sweeps_out) {
     DMRG_LAUNCH init_identity_kernel<<<np, 256, 0, st>>>(d_probs.as<SvdProblem>(), d_q.as<double>());
     DMRG_LAUNCH prescale_kernel<<<np, 1024, 0, st>>>(d_probs.as<SvdProblem>(), d_w.as<double>(), d_expo.as<int>());
     DMRG_LAUNCH fro2_kernel<<<np, 256, 0, st>>>(d_probs.as<SvdProblem>(), d_w.as<double>(), d_fro2.as<double>());
-    std::vector<unsigned long long> conv(np);
     static const bool debug = std::getenv("DMRG_SVD_DEBUG") != nullptr;  // per-sweep convergence to stderr
     int max_cols = 0;
     for (const SvdProblem& p : probs) max_cols = std::max(max_cols, p.cols);
     const dim3 colgrid(np, (max_cols + 7) / 8);
-    int sweep = 0, worst_at = 0;
-    double worst_left = 0.0;
-    auto t_sweep = std::chrono::steady_clock::now();
+    std::vector<double> bm(tiles.size()), worst(np);
     const int max_sweeps = g_max_sweeps.load();
-    for (; sweep < max_sweeps; ++sweep) {
-        DMRG_CUDA_TRY(cudaMemsetAsync(d_conv.ptr, 0, np * sizeof(unsigned long long), st));
+    auto t_sweep = std::chrono::steady_clock::now();
+    int sweep = 0;
+    bool converged = false;
+    for (;; ++sweep) {
         // the sweep visits columns in descending norm order: blocks hold columns of
         // similar size, which keeps the many tiny singular values of a noise-expanded
-        // tensor from converging only linearly
+        // tensor from converging only linearly; then every block pair is measured
         DMRG_LAUNCH colnorm_kernel<<<colgrid, 256, 0, st>>>(d_probs.as<SvdProblem>(), d_w.as<double>(), d_norm.as<double>());
-        DMRG_LAUNCH rank_kernel<<<np, 256, 0, st>>>(d_probs.as<SvdProblem>(), d_norm.as<double>(), d_colmap.as<int>(), nullptr);
-        for (int r = 0; r < max_rounds; ++r) {
+        DMRG_LAUNCH rank_kernel<<<np, 256, 0, st>>>(d_probs.as<SvdProblem>(), d_norm.as<double>(), d_colmap.as<int>(),
+                                                    nullptr);
+        DMRG_LAUNCH measure_kernel<<<(int)tiles.size(), 128, 0, st>>>(
+            d_probs.as<SvdProblem>(), d_tiles.as<SvdTile>(), d_colmap.as<int>(), d_w.as<double>(),
+            d_norm.as<double>(), d_fro2.as<double>(), d_bm.as<double>());
+        DMRG_CUDA_TRY(cudaGetLastError());
+        DMRG_CUDA_TRY(cudaMemcpyAsync(bm.data(), d_bm.ptr, bm.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+        DMRG_CUDA_TRY(cudaStreamSynchronize(st));
+        for (int i = 0; i < np; ++i) {
+            worst[i] = 0.0;
+            for (int k = tile_first[i]; k < tile_first[i + 1]; ++k) worst[i] = std::max(worst[i], bm[k]);
+        }
+        const int rounds = schedule(bm);
+        if (debug) {
+            int wi = 0;
+            for (int i = 1; i < np; ++i)
+                if (worst[i] > worst[wi]) wi = i;
+            const auto now = std::chrono::steady_clock::now();
+            std::fprintf(stderr, "svd sweep %d: %.2f ms, worst %.3e (sector %d x %d), %d rounds\n", sweep,
+                         std::chrono::duration<double, std::milli>(now - t_sweep).count(), worst[wi], probs[wi].m,
+                         probs[wi].n, rounds);
+            t_sweep = now;
+        }
+        if (rounds == 0) {
+            converged = true;
+            break;
+        }
+        if (sweep >= max_sweeps) break;
+        int widest_round = 0, widest_gram = 0;
+        for (int r = 0; r < rounds; ++r) {
+            widest_round = std::max(widest_round, round_first[r + 1] - round_first[r]);
+            widest_gram = std::max(widest_gram, round_gram_first[r + 1] - round_gram_first[r]);
+        }
+        if ((int)tasks.size() > max_tasks || (int)gram_items.size() > max_gram || (int)rot_items.size() > max_rot ||
+            widest_round > max_round_tasks || widest_gram > max_round_gram)
+            return set_error(DMRG_E_STATE, "Jacobi SVD schedule exceeds its plan");
+        DMRG_CUDA_TRY(cudaMemcpyAsync(d_tasks.ptr, tasks.data(), tasks.size() * sizeof(SvdTask), cudaMemcpyHostToDevice, st));
+        DMRG_CUDA_TRY(cudaMemcpyAsync(d_gram_items.ptr, gram_items.data(), gram_items.size() * sizeof(SvdItem),
+                                      cudaMemcpyHostToDevice, st));
+        DMRG_CUDA_TRY(cudaMemcpyAsync(d_rot_items.ptr, rot_items.data(), rot_items.size() * sizeof(SvdItem),
+                                      cudaMemcpyHostToDevice, st));
+        for (int r = 0; r < rounds; ++r) {
             const int nt = round_first[r + 1] - round_first[r];
             const int ng = round_gram_first[r + 1] - round_gram_first[r];
             const int nr = round_rot_first[r + 1] - round_rot_first[r];
             if (nt == 0) continue;
             DMRG_LAUNCH gram_kernel<<<ng, 128, 0, st>>>(d_probs.as<SvdProblem>(), d_tasks.as<SvdTask>(),
-                                            d_gram_items.as<SvdItem>() + round_gram_first[r], r,
-                                            d_colmap.as<int>(), d_w.as<double>(), d_gpart.as<double>());
+                                                        d_gram_items.as<SvdItem>() + round_gram_first[r],
+                                                        d_colmap.as<int>(), d_w.as<double>(), d_gpart.as<double>());
             DMRG_LAUNCH solve_kernel<<<nt, kThreads, sizeof(SvdSmem), st>>>(
                 d_probs.as<SvdProblem>(), d_tasks.as<SvdTask>(), round_first[r], d_gpart.as<double>(),
-                d_fro2.as<double>(), d_rot.as<double>(), d_skip.as<int>(), d_conv.as<unsigned long long>(),
-                d_sched.as<uint32_t>(), kInnerSweeps);
+                d_fro2.as<double>(), d_rot.as<double>(), d_skip.as<int>(), d_sched.as<uint32_t>(), kInnerSweeps);
             DMRG_LAUNCH rotate_kernel<<<nr, 128, kRotSmem, st>>>(d_probs.as<SvdProblem>(), d_tasks.as<SvdTask>(),
-                                                     d_rot_items.as<SvdItem>() + round_rot_first[r], r,
-                                                     round_first[r], d_rot.as<double>(), d_skip.as<int>(),
-                                                     d_colmap.as<int>(), d_w.as<double>(), d_q.as<double>());
+                                                                 d_rot_items.as<SvdItem>() + round_rot_first[r],
+                                                                 round_first[r], d_rot.as<double>(), d_skip.as<int>(),
+                                                                 d_colmap.as<int>(), d_w.as<double>(), d_q.as<double>());
         }
         DMRG_CUDA_TRY(cudaGetLastError());
-        DMRG_CUDA_TRY(cudaMemcpyAsync(conv.data(), d_conv.ptr, np * sizeof(unsigned long long),
-                                      cudaMemcpyDeviceToHost, st));
-        DMRG_CUDA_TRY(cudaStreamSynchronize(st));
-        bool done = true;
-        if (debug) {
-            double w = 0.0;
-            int wi = 0;
-            for (int i = 0; i < np; ++i) {
-                double x;
-                std::memcpy(&x, &conv[i], sizeof(double));
-                if (x > w) {
-                    w = x;
-                    wi = i;
-                }
-            }
-            int nconv = 0;
-            for (int i = 0; i < np; ++i) {
-                double x;
-                std::memcpy(&x, &conv[i], sizeof(double));
-                if (x <= 2.0 * DBL_EPSILON * std::sqrt((double)probs[i].rows)) ++nconv;
-            }
-            const auto now = std::chrono::steady_clock::now();
-            std::fprintf(stderr, "svd sweep %d: %.2f ms, worst %.3e (sector %d x %d), %d of %d sectors converged\n",
-                         sweep, std::chrono::duration<double, std::milli>(now - t_sweep).count(), w, probs[wi].m,
-                         probs[wi].n, nconv, np);
-            t_sweep = now;
-        }
-        for (int i = 0; i < np; ++i) {
-            double worst;
-            std::memcpy(&worst, &conv[i], sizeof(double));
-            if (worst > 2.0 * DBL_EPSILON * std::sqrt((double)probs[i].rows)) {
-                done = false;
-                if (sweep == max_sweeps - 1 && worst > worst_left) {
-                    worst_left = worst;
-                    worst_at = i;
-                }
-            }
-        }
-        if (done) break;
     }
-    if (sweep == max_sweeps && fail_dump) dump_unconverged(fail_dump, w_in, conv, st);
-    if (sweep == max_sweeps)
+    if (!converged) {
+        if (fail_dump) dump_unconverged(fail_dump, w_in, worst, st);
+        int wi = 0;
+        for (int i = 1; i < np; ++i)
+            if (worst[i] > worst[wi]) wi = i;
         return set_error(DMRG_E_NUMERIC, "Jacobi SVD did not converge in %d sweeps (sector %d x %d: off-diagonal %.3e)",
-                         max_sweeps, probs[worst_at].m, probs[worst_at].n, worst_left);
+                         max_sweeps, probs[wi].m, probs[wi].n, worst[wi]);
+    }
     // singular values = final column norms, sorted
     DMRG_LAUNCH colnorm_kernel<<<colgrid, 256, 0, st>>>(d_probs.as<SvdProblem>(), d_w.as<double>(), d_norm.as<double>());
     DMRG_LAUNCH rank_kernel<<<np, 256, 0, st>>>(d_probs.as<SvdProblem>(), d_norm.as<double>(), d_perm.as<int>(), d_s.as<double>());
@@ -906,7 +1092,7 @@ int BatchedSvd::run(cudaStream_t st, int* sweeps_out) {
     DMRG_LAUNCH unscale_kernel<<<dim3(np, 32), 256, 0, st>>>(d_probs.as<SvdProblem>(), d_expo.as<int>(),
                                                              d_w.as<double>(), d_s.as<double>());
     DMRG_CUDA_TRY(cudaGetLastError());
-    if (sweeps_out) *sweeps_out = sweep + 1;
+    if (sweeps_out) *sweeps_out = sweep;  // sweeps that rotated
     return DMRG_OK;
 }
 

@@ -6,14 +6,17 @@
 // (they accumulate U).  A sweep first orders the columns by descending norm
 // (de Rijk's pivoting, applied block-wise: blocks then hold columns of similar
 // size, which halves the sweeps on noise-expanded tensors whose spectra are
-// mostly tiny), then visits every pair of column blocks once in the
-// round-robin order; in a round all pairs of all sectors are independent and
+// mostly tiny), then measures every pair of column blocks at once (the 32x32
+// cross-Gram blocks of W, DMMA) and visits only the block pairs found
+// unconverged, in as few rounds as a matching of them allows (the round-robin
+// order restricted to them, or a greedy matching by measure if that needs
+// fewer rounds).  In a round all pairs of all sectors are independent and each
 // is split over CTAs by rows: (1) partial 64x64 Gram matrices of the pair over
 // row ranges (DMMA), (2) one CTA per pair sums them and runs a few cyclic
 // Jacobi sweeps on the Gram matrix in shared memory, (3) 64-row slices of the
 // pair's columns of W and of the accumulated rotation are multiplied by the
-// resulting 64x64 rotation (DMMA).  Converged when no
-// pair has |g_ij| > tol ||A||_F max(|x_i|, |x_j|), tol = 2 eps sqrt(rows): the
+// resulting 64x64 rotation (DMMA).  Converged when no pair has
+// |g_ij| > tol ||A||_F max(|x_i|, |x_j|), tol = 2 eps sqrt(rows): the
 // remaining non-orthogonality is a backward perturbation of A below rounding
 // level, the accuracy of a backward-stable SVD such as the reference's dgesvd
 // (singular values to ~eps ||A||, enough for its canpre cut at 1e-12 of a
@@ -48,9 +51,16 @@ struct SvdProblem {
 
 struct SvdTask {
     int problem;
-    int pair;
+    int bi, bj;            // the pair's column blocks (sorted order), bi < bj; bj may be an empty block
     int g_first, g_count;  // its Gram items, as indices into the round's item list
 };
+
+struct SvdTile {           // a 32x32 block of a sector's cross-Gram matrix (convergence measure)
+    int problem;
+    int bi, bj;            // bi <= bj
+    int pad;
+};
+
 
 struct SvdItem {   // a row range of one pair task's columns
     int task;      // index into the task list
@@ -71,22 +81,34 @@ public:
     int run(cudaStream_t st, int* sweeps_out = nullptr);
     // Sorted singular values of every active sector, copied to the host.
     int singular_values(std::vector<std::vector<double>>& out, cudaStream_t st);
-    void dump_unconverged(const char* path, const DeviceBuffer& w_in, const std::vector<unsigned long long>& conv,
+    void dump_unconverged(const char* path, const DeviceBuffer& w_in, const std::vector<double>& worst,
                           cudaStream_t st);
 
-    DeviceBuffer d_w, d_q, d_s, d_perm, d_probs, d_tasks, d_conv, d_fro2;
+    DeviceBuffer d_w, d_q, d_s, d_perm, d_probs, d_tasks, d_fro2;
     DeviceBuffer d_expo;  // per problem: the power of two W was scaled by (prescale_kernel)
     DeviceBuffer d_sign;  // +-1 per sorted singular triplet (sign convention, set by run())
     DeviceBuffer d_gram_items, d_rot_items, d_gpart, d_rot, d_skip;
     DeviceBuffer d_colmap, d_norm;  // per sweep: columns in descending norm order
+    DeviceBuffer d_tiles, d_bm;     // the convergence measure's tiles and their values
     DeviceBuffer d_sched;           // lane order of the pair solve's rotations (uploaded once)
     std::vector<SvdProblem> probs;
     std::vector<int> index;             // sector -> problem (-1 when empty)
+    std::vector<SvdTile> tiles;         // all block pairs bi <= bj of every problem
+    std::vector<int> tile_first;        // per problem: its first tile
+    int gram_rows = 64;                 // rows of a Gram item
+    // the current sweep's rounds (rebuilt every sweep from the measure)
     std::vector<int> round_first;       // task offset of each round
     std::vector<SvdTask> tasks;
     std::vector<SvdItem> gram_items, rot_items;    // per round, contiguous
     std::vector<int> round_gram_first, round_rot_first;
-    int max_rounds = 0, max_round_tasks = 0, max_round_gram = 0;
+    int max_tasks = 0, max_gram = 0, max_rot = 0;  // capacities (per sweep)
+    int max_round_tasks = 0, max_round_gram = 0;   // capacities (per round)
+
+private:
+    // Builds the sweep's rounds from the block measures bm (tiles order);
+    // returns the number of rounds (0: converged).
+    int schedule(const std::vector<double>& bm);
+    void add_task(int problem, int bi, int bj);
 };
 
 }  // namespace dmrg
