@@ -11,10 +11,26 @@
 // canonical[l] = U[:, :t_l] diag(S[:t_l]); left_dim[l] <- t_l.
 // Sectors without rows (left) / columns (right) keep the reference's special
 // case: one singular value 0, a zero canonical block, the ket untouched.
+//
+// The kept columns on the ket's side are orthonormal to FP64 rounding, as the
+// reference's dgesvd gives them.  Where the ket side is the one the Jacobi SVD
+// accumulates (U of a wide A, V of a tall A) it already is.  Where it is the
+// side whose vectors are the working matrix's columns divided by their norms,
+// the Jacobi convergence test (a backward error of eps ||A||) leaves vectors of
+// singular values near eps ||A|| / |x| non-orthogonal by up to ~1e-2, so they
+// are orthonormalised in descending order (Gram-Schmidt in effect: K <- K (I -
+// strictly upper part of K^T K), columns renormalised, four passes, each
+// squaring the departure from orthonormality), and the canonical block is the
+// projection of the sector matrix on them (K^T A left, A K right), zero in the
+// rows / columns whose singular value the truncation forced to 0.  Since
+// K = K0 R with R upper triangular and near the identity, row i of K^T A is
+// s_i v_i^T plus terms of size eps ||A||: the same factors as diag(S) V^T to
+// rounding, now with an orthonormal ket.
 #include <algorithm>
 #include <numeric>
 
 #include "blocksparse.h"
+#include "gemm.cuh"
 #include "svd.cuh"
 #include "truncate.h"
 
@@ -34,6 +50,7 @@ struct WriteTask {
     int rows, cols;   // new ket block shape
     int problem;
     int off;          // row0 / col0
+    int64_t k_off;    // the sector's orthonormalised kept columns in the K buffer (-1: none)
 };
 
 struct CanonTask {
@@ -41,6 +58,19 @@ struct CanonTask {
     int rows, cols;   // canonical block shape
     int problem;      // -1: zero block
     int64_t sig_off;  // offset of the forced singular values of this sector
+    int projected;    // 1: written as a projection (GEMM), only the forced zeros here
+    int pad_;
+};
+
+// A sector whose kept ket columns are orthonormalised: its working-matrix
+// columns U = W / s (left, W = A) or V = W / s (right, W = A^T), t of them,
+// rows r (= the working matrix's rows), at k_off (column-major, ld r) of the
+// K buffer; its Gram matrix (t x t, row-major) at g_off.
+struct OrthoTask {
+    int problem;
+    int t, r;
+    int pad_;
+    int64_t k_off, g_off;
 };
 
 // gather: stacked A (m x n) into W (column-major; W = A or W = A^T)
@@ -65,12 +95,21 @@ __global__ void gather_kernel(const double* __restrict__ ket, const CopyTask* __
 __global__ void write_ket_kernel(const WriteTask* __restrict__ tasks, const SvdProblem* __restrict__ probs,
                                  const double* __restrict__ W, const double* __restrict__ Q,
                                  const double* __restrict__ sig, const int* __restrict__ perm,
-                                 const double* __restrict__ sgn, double* __restrict__ out, int side) {
+                                 const double* __restrict__ sgn, const double* __restrict__ K,
+                                 double* __restrict__ out, int side) {
     const WriteTask t = tasks[blockIdx.x];
     const SvdProblem p = probs[t.problem];
     const double* w = W + p.w_off;
     const double* q = Q + p.q_off;
     const int64_t total = (int64_t)t.rows * t.cols;
+    if (t.k_off >= 0) {  // orthonormalised columns: U[row0 + i][j] (left) or V^T[i][col0 + j] (right)
+        const double* k = K + t.k_off;
+        for (int64_t e = threadIdx.x; e < total; e += blockDim.x) {
+            const int i = (int)(e / t.cols), j = (int)(e % t.cols);
+            out[t.out_off + e] = side == 0 ? k[(int64_t)j * p.rows + t.off + i] : k[(int64_t)i * p.rows + t.off + j];
+        }
+        return;
+    }
     for (int64_t e = threadIdx.x; e < total; e += blockDim.x) {
         const int i = (int)(e / t.cols), j = (int)(e % t.cols);
         double v;
@@ -111,6 +150,13 @@ __global__ void write_canonical_kernel(const CanonTask* __restrict__ tasks, cons
         for (int64_t e = threadIdx.x; e < total; e += blockDim.x) out[t.out_off + e] = 0.0;
         return;
     }
+    if (t.projected) {  // the block is K^T A / A K already: zero the rows / columns forced to 0
+        for (int64_t e = threadIdx.x; e < total; e += blockDim.x) {
+            const int i = (int)(e / t.cols), j = (int)(e % t.cols);
+            if (forced[t.sig_off + (side == 0 ? i : j)] == 0.0) out[t.out_off + e] = 0.0;
+        }
+        return;
+    }
     const SvdProblem p = probs[t.problem];
     const double* w = W + p.w_off;
     const double* q = Q + p.q_off;
@@ -142,6 +188,47 @@ __global__ void write_canonical_kernel(const CanonTask* __restrict__ tasks, cons
     }
 }
 
+// K0 of every orthonormalised sector: column j = sign_j W[:, perm_j] / s_j
+// (0 where s_j = 0).  Grid (tasks, column groups of 8), one warp per column.
+__global__ void __launch_bounds__(256) kform_kernel(const OrthoTask* __restrict__ tasks,
+                                                    const SvdProblem* __restrict__ probs, const double* __restrict__ W,
+                                                    const double* __restrict__ sig, const int* __restrict__ perm,
+                                                    const double* __restrict__ sgn, double* __restrict__ K) {
+    const OrthoTask t = tasks[blockIdx.x];
+    const int j = blockIdx.y * 8 + (threadIdx.x >> 5);
+    if (j >= t.t) return;
+    const SvdProblem p = probs[t.problem];
+    const double s = sig[p.s_off + j];
+    const double f = s > 0.0 ? sgn[p.s_off + j] / s : 0.0;
+    const double* w = W + p.w_off + (int64_t)perm[p.perm_off + j] * p.rows;
+    double* k = K + t.k_off + (int64_t)j * t.r;
+    for (int i = threadIdx.x & 31; i < t.r; i += 32) k[i] = f * w[i];
+}
+
+// G (t x t, row-major, symmetric) <- its strictly lower part.
+__global__ void __launch_bounds__(256) strict_lower_kernel(const OrthoTask* __restrict__ tasks, double* __restrict__ G) {
+    const OrthoTask t = tasks[blockIdx.x];
+    double* g = G + t.g_off;
+    for (int64_t e = threadIdx.x; e < (int64_t)t.t * t.t; e += blockDim.x)
+        if (e % t.t >= e / t.t) g[e] = 0.0;
+}
+
+// Every nonzero column of K scaled to unit norm.  Grid (tasks, column groups of
+// 8), one warp per column (fixed reduction order).
+__global__ void __launch_bounds__(256) normalize_kernel(const OrthoTask* __restrict__ tasks, double* __restrict__ K) {
+    const OrthoTask t = tasks[blockIdx.x];
+    const int j = blockIdx.y * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (j >= t.t) return;
+    double* k = K + t.k_off + (int64_t)j * t.r;
+    double s = 0.0;
+    for (int i = lane; i < t.r; i += 32) s += k[i] * k[i];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (s <= 0.0) return;
+    const double f = 1.0 / sqrt(s);
+    for (int i = lane; i < t.r; i += 32) k[i] *= f;
+}
+
 }  // namespace
 
 struct dmrg_canon_s {
@@ -156,6 +243,11 @@ struct dmrg_canon_s {
     BatchedSvd svd;
     std::vector<CopyTask> copies;
     DeviceBuffer d_copies, d_writes, d_canons, d_forced;
+    // orthonormalisation of the kept ket columns taken from the working matrix
+    std::vector<OrthoTask> otasks;
+    int ortho_cols = 0;                     // largest t of the tasks
+    DeviceBuffer d_otasks, d_k, d_k2, d_g, d_a;
+    GemmSchedule sg, su, sc;                // K^T K; K2 -= L K; the projected canonical blocks
     // results
     bool ran = false;
     std::vector<std::vector<double>> sv;  // singular values per sector (reference semantics)
@@ -165,6 +257,116 @@ struct dmrg_canon_s {
     double discarded = 0.0;
     int sweeps = 0;
 };
+
+namespace {
+
+// The orthonormalisation tasks of a run (sectors whose ket side is the working
+// matrix's columns) and the three GEMM schedules over them.
+int plan_ortho(dmrg_canon_s* c, cudaStream_t st) {
+    BatchedSvd& svd = c->svd;
+    c->otasks.clear();
+    c->ortho_cols = 0;
+    int64_t ksz = 0, gsz = 0, wsz = 0;
+    for (const SvdProblem& p : svd.probs) wsz += (int64_t)p.rows * p.cols;
+    for (int sct = 0; sct < c->nsec; ++sct) {
+        if (!svd.active(sct)) continue;
+        const SvdProblem& p = svd.problem(sct);
+        const bool wside = c->side == 0 ? !p.transposed : p.transposed != 0;
+        const int t = c->tdim[sct];
+        if (!wside || t <= 0) continue;
+        c->otasks.push_back(OrthoTask{svd.index[sct], t, p.rows, 0, ksz, gsz});
+        c->ortho_cols = std::max(c->ortho_cols, t);
+        ksz += (int64_t)p.rows * t;
+        gsz += (int64_t)t * t;
+    }
+    if (c->otasks.empty()) return DMRG_OK;
+    DMRG_TRY(c->d_k.alloc(ksz * sizeof(double)));
+    DMRG_TRY(c->d_k2.alloc(ksz * sizeof(double)));
+    DMRG_TRY(c->d_g.alloc(gsz * sizeof(double)));
+    DMRG_TRY(c->d_a.alloc(std::max<int64_t>(wsz, 1) * sizeof(double)));
+    DMRG_TRY(upload(c->d_otasks, c->otasks, st));
+    GemmSchedule &sg = c->sg, &su = c->su, &sc = c->sc;
+    sg.reset();
+    su.reset();
+    sc.reset();
+    sg.tb = true;  // G = K^T K: K^T is K column-major read row-major (t x r), K the transposed B
+    sc.tb = true;
+    for (const OrthoTask& o : c->otasks) {
+        sg.add_group(o.g_off, o.t, o.t, o.t);
+        sg.add_term(o.k_off, o.r, o.k_off, o.r, o.r, 1.0);
+        // K2^T (row-major t x r) -= L (t x t) K^T: L = the strictly lower part of G
+        su.add_group(o.k_off, o.r, o.t, o.r);
+        su.add_term(o.g_off, o.t, o.k_off, o.r, o.t, -1.0);
+    }
+    for (int sct = 0; sct < c->nsec; ++sct) {
+        if (!svd.active(sct)) continue;
+        const int pi = svd.index[sct];
+        const SvdProblem& p = svd.probs[pi];
+        const OrthoTask* o = nullptr;
+        for (const OrthoTask& x : c->otasks)
+            if (x.problem == pi) o = &x;
+        if (!o) continue;
+        if (c->side == 0) {
+            // C (t x n) = K^T A; A (m x n) is held column-major (W layout), i.e. the transposed B
+            sc.add_group(c->canonical.off[sct], p.n, o->t, p.n);
+            sc.add_term(o->k_off, p.rows, p.w_off, p.rows, p.rows, 1.0);
+        } else {
+            // C (m x t) = A K; A is held as A^T column-major = A row-major (ld n); K the transposed B
+            sc.add_group(c->canonical.off[sct], o->t, p.m, o->t);
+            sc.add_term(p.w_off, p.rows, o->k_off, p.rows, p.rows, 1.0);
+        }
+    }
+    DMRG_TRY(sg.check_bounds(ksz, ksz, gsz));
+    DMRG_TRY(su.check_bounds(gsz, ksz, ksz));
+    if (c->side == 0)
+        DMRG_TRY(sc.check_bounds(ksz, wsz, c->canonical.size));
+    else
+        DMRG_TRY(sc.check_bounds(wsz, ksz, c->canonical.size));
+    const int sms = c->ctx->num_sms;
+    DMRG_TRY(sg.finalize(64, 64, 16, st, sms));
+    DMRG_TRY(su.finalize(64, 64, 16, st, sms));
+    DMRG_TRY(sc.finalize(64, 64, 16, st, sms));
+    return DMRG_OK;
+}
+
+// Orthonormalised ket columns (K, in c->d_k on return) and the projected
+// canonical blocks of the tasks' sectors.
+int run_ortho(dmrg_canon_s* c, const double* ket_dev, double* canonical_dev, cudaStream_t st) {
+    if (c->otasks.empty()) return DMRG_OK;
+    BatchedSvd& svd = c->svd;
+    const int nt = (int)c->otasks.size();
+    const dim3 grid(nt, (c->ortho_cols + 7) / 8);
+    const OrthoTask* ot = c->d_otasks.as<OrthoTask>();
+    DMRG_CUDA_TRY(cudaMemsetAsync(c->d_a.ptr, 0, c->d_a.bytes, st));
+    if (!c->copies.empty())
+        DMRG_LAUNCH gather_kernel<<<(int)c->copies.size(), 256, 0, st>>>(ket_dev, c->d_copies.as<CopyTask>(),
+                                                                          svd.d_probs.as<SvdProblem>(),
+                                                                          c->d_a.as<double>(), c->side);
+    DMRG_LAUNCH kform_kernel<<<grid, 256, 0, st>>>(ot, svd.d_probs.as<SvdProblem>(), svd.d_w.as<double>(),
+                                                   svd.d_s.as<double>(), svd.d_perm.as<int>(),
+                                                   svd.d_sign.as<double>(), c->d_k.as<double>());
+    DMRG_CUDA_TRY(cudaGetLastError());
+    // each pass squares the departure from orthonormality (~1e-2 at most for
+    // kept values near canpre): four take it to rounding level
+    for (int pass = 0; pass < 4; ++pass) {
+        DeviceBuffer& k = pass % 2 == 0 ? c->d_k : c->d_k2;
+        DeviceBuffer& k2 = pass % 2 == 0 ? c->d_k2 : c->d_k;
+        DMRG_TRY(launch_gemm_f64(c->sg, k.as<double>(), k.as<double>(), c->d_g.as<double>(), false, st));
+        DMRG_LAUNCH strict_lower_kernel<<<nt, 256, 0, st>>>(ot, c->d_g.as<double>());
+        DMRG_CUDA_TRY(cudaMemcpyAsync(k2.ptr, k.ptr, k.bytes, cudaMemcpyDeviceToDevice, st));
+        DMRG_TRY(launch_gemm_f64(c->su, c->d_g.as<double>(), k.as<double>(), k2.as<double>(), true, st));
+        DMRG_LAUNCH normalize_kernel<<<grid, 256, 0, st>>>(ot, k2.as<double>());
+        DMRG_CUDA_TRY(cudaGetLastError());
+    }
+    // four passes: the result is back in d_k
+    if (c->side == 0)
+        DMRG_TRY(launch_gemm_f64(c->sc, c->d_k.as<double>(), c->d_a.as<double>(), canonical_dev, false, st));
+    else
+        DMRG_TRY(launch_gemm_f64(c->sc, c->d_a.as<double>(), c->d_k.as<double>(), canonical_dev, false, st));
+    return DMRG_OK;
+}
+
+}  // namespace
 
 extern "C" {
 
@@ -293,16 +495,22 @@ int dmrg_canon_run(dmrg_canon_t c, const double* ket_dev, int max_dim, double ca
     std::vector<CanonTask> ctasks;
     for (int sct = 0; sct < c->nsec; ++sct) {
         CanonTask t{c->canonical.off[sct], c->canonical.rows[sct], c->canonical.cols[sct],
-                    svd.active(sct) ? svd.index[sct] : -1, (int64_t)forced.size()};
+                    svd.active(sct) ? svd.index[sct] : -1, (int64_t)forced.size(), 0, 0};
         for (int i = 0; i < c->tdim[sct]; ++i) forced.push_back(i < (int)s[sct].size() ? s[sct][i] : 0.0);
         ctasks.push_back(t);
     }
+    DMRG_TRY(plan_ortho(c, st));
+    std::vector<int64_t> k_of(c->nsec, -1);
+    for (const OrthoTask& o : c->otasks) k_of[o.problem] = o.k_off;  // by problem index
+    for (CanonTask& t : ctasks)
+        if (t.problem >= 0 && k_of[t.problem] >= 0) t.projected = 1;
     std::vector<WriteTask> wtasks;
     for (int sct = 0; sct < c->nsec; ++sct) {
         if (!svd.active(sct)) continue;
         int acc = 0;
         for (int p : c->members[sct]) {
-            wtasks.push_back(WriteTask{c->new_ket.off[p], c->new_ket.rows[p], c->new_ket.cols[p], svd.index[sct], acc});
+            wtasks.push_back(WriteTask{c->new_ket.off[p], c->new_ket.rows[p], c->new_ket.cols[p], svd.index[sct], acc,
+                                       k_of[svd.index[sct]]});
             acc += c->side == 0 ? c->ket.rows[p] : c->ket.cols[p];
         }
     }
@@ -366,10 +574,12 @@ int dmrg_canon_write(dmrg_canon_t c, const double* ket_dev, double* new_ket_dev,
         if (svd.active(s)) n_writes += (int)c->members[s].size();
     (void)nw;
     const double* sig = svd.d_s.as<double>();
+    DMRG_TRY(run_ortho(c, ket_dev, canonical_dev, st));
     if (n_writes)
         DMRG_LAUNCH write_ket_kernel<<<n_writes, 256, 0, st>>>(c->d_writes.as<WriteTask>(), svd.d_probs.as<SvdProblem>(),
                                                    svd.d_w.as<double>(), svd.d_q.as<double>(), sig,
-                                                   svd.d_perm.as<int>(), svd.d_sign.as<double>(), new_ket_dev, c->side);
+                                                   svd.d_perm.as<int>(), svd.d_sign.as<double>(),
+                                                   c->d_k.as<double>(), new_ket_dev, c->side);
     DMRG_LAUNCH write_canonical_kernel<<<c->nsec, 256, 0, st>>>(c->d_canons.as<CanonTask>(), svd.d_probs.as<SvdProblem>(),
                                                     svd.d_w.as<double>(), svd.d_q.as<double>(), sig,
                                                     svd.d_perm.as<int>(), c->d_forced.as<double>(),

@@ -97,3 +97,55 @@ def test_svd_sweep_cap_returns_numeric_error(ctx):
     c = capi.Canonical(ctx, 0, d["before.left_dim"], d["before.right_dim"], ket)
     res = c.run(kdev, int(d["max_dim"][0]), float(d["canpre"][0]))
     assert np.array_equal(res["tdim"], d["after.right_dim"])
+
+
+@pytest.mark.parametrize("side", [0, 1])
+def test_graded_spectrum_ket_is_orthonormal(ctx, side):
+    """Sector matrices with singular values spread from 1 down to 1e-13 (the
+    kept ones reach the canpre cut): the Jacobi convergence test leaves the
+    working matrix's columns of such tiny values non-orthogonal by up to
+    eps ||A|| / s, so the new ket is orthonormalised and the canonical block is
+    the projection of A on it.  Checked against numpy's SVD: the ket
+    orthonormal within 1e-12, the kept singular values (canonical row / column
+    norms) and the truncated product (ket x canonical) within 1e-12 of
+    ||A||, the truncation dimensions equal."""
+    rng = np.random.default_rng(11)
+    shapes = [(300, 120), (250, 64), (90, 40)] if side == 0 else [(120, 300), (64, 250), (40, 90)]
+    A = []
+    for m, n in shapes:
+        k = min(m, n)
+        U, _ = np.linalg.qr(rng.standard_normal((m, k)))
+        V, _ = np.linalg.qr(rng.standard_normal((n, k)))
+        s = np.logspace(0, -13, k) * rng.uniform(0.5, 1.0)
+        A.append((U * s) @ V.T)
+    ns = len(A)
+    m = np.array([a.shape[0] for a in A])
+    n = np.array([a.shape[1] for a in A])
+    ket = capi.BlockSpec(np.arange(ns), np.arange(ns), m, n)
+    c = capi.Canonical(ctx, side, m, n, ket)
+    kdev = capi.DeviceArray.from_host(ctx, np.concatenate([a.ravel() for a in A]))
+    canpre = 1e-12
+    res = c.run(kdev, 10000, canpre)
+    newk = capi.DeviceArray(ctx, res["ket_size"])
+    can = capi.DeviceArray(ctx, res["canonical_size"])
+    c.write(kdev, newk, can)
+    ctx.sync()
+    K, Cn = newk.download(), can.download()
+    kp = cp = 0
+    for i, a in enumerate(A):
+        Ur, sr, Vtr = np.linalg.svd(a, full_matrices=False)
+        t = int((sr > canpre).sum())
+        assert res["tdim"][i] == t
+        kr, kc = res["ket_rows"][i], res["ket_cols"][i]
+        Kb = K[kp:kp + kr * kc].reshape(kr, kc)
+        kp += kr * kc
+        cr, cc = res["canon_rows"][i], res["canon_cols"][i]
+        Cb = Cn[cp:cp + cr * cc].reshape(cr, cc)
+        cp += cr * cc
+        gram = Kb.T @ Kb if side == 0 else Kb @ Kb.T
+        assert np.abs(gram - np.eye(t)).max() < 1e-12
+        norms = np.linalg.norm(Cb, axis=1 if side == 0 else 0)
+        assert np.abs(norms - sr[:t]).max() < 1e-12
+        prod = Kb @ Cb if side == 0 else Cb @ Kb
+        ref = (Ur[:, :t] * sr[:t]) @ Vtr[:t]
+        assert np.abs(prod - ref).max() < 1e-12
