@@ -19,14 +19,18 @@
 // the Jacobi convergence test (a backward error of eps ||A||) leaves vectors of
 // singular values near eps ||A|| / |x| non-orthogonal by up to ~1e-2, so they
 // are orthonormalised in descending order (Gram-Schmidt in effect: K <- K (I -
-// strictly upper part of K^T K), columns renormalised, four passes, each
-// squaring the departure from orthonormality), and the canonical block is the
+// strictly upper part of K^T K), columns renormalised, each pass squaring the
+// departure from orthonormality; as many passes as take the largest departure
+// the convergence test allows, tol ||A||_F / s_t with s_t the smallest kept
+// value, below 1e-16, plus one), and the canonical block is the
 // projection of the sector matrix on them (K^T A left, A K right), zero in the
 // rows / columns whose singular value the truncation forced to 0.  Since
 // K = K0 R with R upper triangular and near the identity, row i of K^T A is
 // s_i v_i^T plus terms of size eps ||A||: the same factors as diag(S) V^T to
 // rounding, now with an orthonormal ket.
 #include <algorithm>
+#include <cfloat>
+#include <cmath>
 #include <numeric>
 
 #include "blocksparse.h"
@@ -73,119 +77,179 @@ struct OrthoTask {
     int64_t k_off, g_off;
 };
 
-// gather: stacked A (m x n) into W (column-major; W = A or W = A^T)
-__global__ void gather_kernel(const double* __restrict__ ket, const CopyTask* __restrict__ tasks,
-                              const SvdProblem* __restrict__ probs, double* __restrict__ W, int side) {
+// The kernels below move blocks in 32x32 tiles, one tile per CTA of 256
+// threads (grid y = the block's tile, CTAs beyond a block's tiles return), so
+// that both the row-major ket / canonical blocks and the column-major working
+// matrices are read and written along their contiguous direction (a transpose
+// goes through shared memory).
+constexpr int kTile = 32;
+__host__ __device__ inline int tiles_of(int rows, int cols) {
+    return ((rows + kTile - 1) / kTile) * ((cols + kTile - 1) / kTile);
+}
+
+// Writes tile blockIdx.y of the row-major rows x cols block at out (ld cols):
+// element (i, j) = value(i, j).  With `down` the source is contiguous along i
+// (a column-major matrix): lanes read along i into shared memory and write
+// along j.
+template <class F>
+__device__ __forceinline__ void write_tile(double* __restrict__ out, int rows, int cols, bool down, F value) {
+    __shared__ double tile[kTile][kTile + 1];
+    const int tc = (cols + kTile - 1) / kTile;
+    const int i0 = (blockIdx.y / tc) * kTile, j0 = (blockIdx.y % tc) * kTile;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    if (down) {
+        for (int c = ty; c < kTile; c += 8) {
+            const int i = i0 + tx, j = j0 + c;
+            tile[tx][c] = (i < rows && j < cols) ? value(i, j) : 0.0;
+        }
+        __syncthreads();
+        for (int r = ty; r < kTile; r += 8) {
+            const int i = i0 + r, j = j0 + tx;
+            if (i < rows && j < cols) out[(int64_t)i * cols + j] = tile[r][tx];
+        }
+    } else {
+        for (int r = ty; r < kTile; r += 8) {
+            const int i = i0 + r, j = j0 + tx;
+            if (i < rows && j < cols) out[(int64_t)i * cols + j] = value(i, j);
+        }
+    }
+}
+
+// gather: stacked A (m x n) into W (column-major; W = A or W = A^T).  Tile
+// blockIdx.y of ket block blockIdx.x; block element (i, j) is A(ai, aj) with
+// ai = off + i, aj = j (left) or ai = i, aj = off + j (right).
+__global__ void __launch_bounds__(256) gather_kernel(const double* __restrict__ ket, const CopyTask* __restrict__ tasks,
+                                                     const SvdProblem* __restrict__ probs, double* __restrict__ W,
+                                                     int side) {
+    __shared__ double tile[kTile][kTile + 1];
     const CopyTask t = tasks[blockIdx.x];
+    if ((int)blockIdx.y >= tiles_of(t.rows, t.cols)) return;
     const SvdProblem p = probs[t.problem];
     const double* src = ket + t.blk_off;
     double* w = W + p.w_off;
-    const int64_t total = (int64_t)t.rows * t.cols;
-    for (int64_t e = threadIdx.x; e < total; e += blockDim.x) {
-        const int i = (int)(e / t.cols), j = (int)(e % t.cols);
-        const int ai = side == 0 ? t.off + i : i;  // row in A
-        const int aj = side == 0 ? j : t.off + j;  // column in A
-        if (ai >= p.m || aj >= p.n) continue;
-        const int64_t dst = p.transposed ? (int64_t)ai * p.n + aj : (int64_t)aj * p.m + ai;
-        w[dst] = src[e];
+    const int tc = (t.cols + kTile - 1) / kTile;
+    const int i0 = (blockIdx.y / tc) * kTile, j0 = (blockIdx.y % tc) * kTile;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    for (int r = ty; r < kTile; r += 8) {
+        const int i = i0 + r, j = j0 + tx;
+        tile[r][tx] = (i < t.rows && j < t.cols) ? src[(int64_t)i * t.cols + j] : 0.0;
+    }
+    __syncthreads();
+    if (p.transposed) {  // W = A^T: w[ai * n + aj], contiguous along the block's columns
+        for (int r = ty; r < kTile; r += 8) {
+            const int i = i0 + r, j = j0 + tx;
+            const int ai = side == 0 ? t.off + i : i, aj = side == 0 ? j : t.off + j;
+            if (i < t.rows && j < t.cols && ai < p.m && aj < p.n) w[(int64_t)ai * p.n + aj] = tile[r][tx];
+        }
+    } else {  // W = A: w[aj * m + ai], contiguous along the block's rows
+        for (int c = ty; c < kTile; c += 8) {
+            const int i = i0 + tx, j = j0 + c;
+            const int ai = side == 0 ? t.off + i : i, aj = side == 0 ? j : t.off + j;
+            if (i < t.rows && j < t.cols && ai < p.m && aj < p.n) w[(int64_t)aj * p.m + ai] = tile[tx][c];
+        }
     }
 }
 
 // new ket blocks: left -> rows of U[:, :t]; right -> columns of V^T[:t, :]
-__global__ void write_ket_kernel(const WriteTask* __restrict__ tasks, const SvdProblem* __restrict__ probs,
-                                 const double* __restrict__ W, const double* __restrict__ Q,
-                                 const double* __restrict__ sig, const int* __restrict__ perm,
-                                 const double* __restrict__ sgn, const double* __restrict__ K,
-                                 double* __restrict__ out, int side) {
+__global__ void __launch_bounds__(256) write_ket_kernel(const WriteTask* __restrict__ tasks,
+                                                        const SvdProblem* __restrict__ probs,
+                                                        const double* __restrict__ W, const double* __restrict__ Q,
+                                                        const double* __restrict__ sig, const int* __restrict__ perm,
+                                                        const double* __restrict__ sgn, const double* __restrict__ K,
+                                                        double* __restrict__ out, int side) {
     const WriteTask t = tasks[blockIdx.x];
+    if ((int)blockIdx.y >= tiles_of(t.rows, t.cols)) return;
     const SvdProblem p = probs[t.problem];
     const double* w = W + p.w_off;
     const double* q = Q + p.q_off;
-    const int64_t total = (int64_t)t.rows * t.cols;
+    double* o = out + t.out_off;
+    // left: U columns are contiguous along the block's rows; right: V columns along its columns
+    const bool down = side == 0;
     if (t.k_off >= 0) {  // orthonormalised columns: U[row0 + i][j] (left) or V^T[i][col0 + j] (right)
         const double* k = K + t.k_off;
-        for (int64_t e = threadIdx.x; e < total; e += blockDim.x) {
-            const int i = (int)(e / t.cols), j = (int)(e % t.cols);
-            out[t.out_off + e] = side == 0 ? k[(int64_t)j * p.rows + t.off + i] : k[(int64_t)i * p.rows + t.off + j];
-        }
+        write_tile(o, t.rows, t.cols, down, [&](int i, int j) {
+            return side == 0 ? k[(int64_t)j * p.rows + t.off + i] : k[(int64_t)i * p.rows + t.off + j];
+        });
         return;
     }
-    for (int64_t e = threadIdx.x; e < total; e += blockDim.x) {
-        const int i = (int)(e / t.cols), j = (int)(e % t.cols);
+    write_tile(o, t.rows, t.cols, down, [&](int i, int j) {
         double v;
         if (side == 0) {  // U[row0 + i][j]
-            const int k = perm[p.perm_off + j];
+            const int kc = perm[p.perm_off + j];
             const int row = t.off + i;
             if (!p.transposed) {
                 const double s = sig[p.s_off + j];
-                v = s > 0.0 ? w[(int64_t)k * p.m + row] / s : 0.0;
+                v = s > 0.0 ? w[(int64_t)kc * p.m + row] / s : 0.0;
             } else {
-                v = q[(int64_t)k * p.m + row];
+                v = q[(int64_t)kc * p.m + row];
             }
             v *= sgn[p.s_off + j];
         } else {  // V^T[i][col0 + j] = v_i[col0 + j]
-            const int k = perm[p.perm_off + i];
+            const int kc = perm[p.perm_off + i];
             const int col = t.off + j;
             if (!p.transposed) {
-                v = q[(int64_t)k * p.n + col];
+                v = q[(int64_t)kc * p.n + col];
             } else {
                 const double s = sig[p.s_off + i];
-                v = s > 0.0 ? w[(int64_t)k * p.n + col] / s : 0.0;
+                v = s > 0.0 ? w[(int64_t)kc * p.n + col] / s : 0.0;
             }
             v *= sgn[p.s_off + i];
         }
-        out[t.out_off + e] = v;
-    }
+        return v;
+    });
 }
 
 // canonical blocks: left -> diag(s_forced) V^T[:t, :] (t x n); right -> U[:, :t] diag(s_forced) (m x t)
-__global__ void write_canonical_kernel(const CanonTask* __restrict__ tasks, const SvdProblem* __restrict__ probs,
-                                       const double* __restrict__ W, const double* __restrict__ Q,
-                                       const double* __restrict__ sig, const int* __restrict__ perm,
-                                       const double* __restrict__ forced, const double* __restrict__ sgn,
-                                       double* __restrict__ out, int side) {
+__global__ void __launch_bounds__(256) write_canonical_kernel(const CanonTask* __restrict__ tasks,
+                                                              const SvdProblem* __restrict__ probs,
+                                                              const double* __restrict__ W, const double* __restrict__ Q,
+                                                              const double* __restrict__ sig, const int* __restrict__ perm,
+                                                              const double* __restrict__ forced,
+                                                              const double* __restrict__ sgn, double* __restrict__ out,
+                                                              int side) {
     const CanonTask t = tasks[blockIdx.x];
-    const int64_t total = (int64_t)t.rows * t.cols;
-    if (t.problem < 0) {
-        for (int64_t e = threadIdx.x; e < total; e += blockDim.x) out[t.out_off + e] = 0.0;
-        return;
-    }
-    if (t.projected) {  // the block is K^T A / A K already: zero the rows / columns forced to 0
-        for (int64_t e = threadIdx.x; e < total; e += blockDim.x) {
-            const int i = (int)(e / t.cols), j = (int)(e % t.cols);
-            if (forced[t.sig_off + (side == 0 ? i : j)] == 0.0) out[t.out_off + e] = 0.0;
+    if ((int)blockIdx.y >= tiles_of(t.rows, t.cols)) return;
+    double* o = out + t.out_off;
+    const int tc = (t.cols + kTile - 1) / kTile;
+    const int i0 = (blockIdx.y / tc) * kTile, j0 = (blockIdx.y % tc) * kTile;
+    if (t.problem < 0 || t.projected) {
+        // a zero block; or one that is K^T A / A K already: zero the rows / columns forced to 0
+        for (int e = threadIdx.x; e < kTile * kTile; e += blockDim.x) {
+            const int i = i0 + e / kTile, j = j0 + e % kTile;
+            if (i >= t.rows || j >= t.cols) continue;
+            if (t.problem < 0 || forced[t.sig_off + (side == 0 ? i : j)] == 0.0) o[(int64_t)i * t.cols + j] = 0.0;
         }
         return;
     }
     const SvdProblem p = probs[t.problem];
     const double* w = W + p.w_off;
     const double* q = Q + p.q_off;
-    for (int64_t e = threadIdx.x; e < total; e += blockDim.x) {
-        const int i = (int)(e / t.cols), j = (int)(e % t.cols);
+    // left: rows of V^T are contiguous along the block's columns; right: U columns along its rows
+    write_tile(o, t.rows, t.cols, side == 1, [&](int i, int j) {
         double v;
         if (side == 0) {  // s_i * v_i[j]
-            const int k = perm[p.perm_off + i];
+            const int kc = perm[p.perm_off + i];
             const double sf = forced[t.sig_off + i];
             if (!p.transposed) {
-                v = sf * q[(int64_t)k * p.n + j];
+                v = sf * q[(int64_t)kc * p.n + j];
             } else {
                 const double s = sig[p.s_off + i];
-                v = s > 0.0 ? sf * w[(int64_t)k * p.n + j] / s : 0.0;
+                v = s > 0.0 ? sf * w[(int64_t)kc * p.n + j] / s : 0.0;
             }
             v *= sgn[p.s_off + i];
         } else {  // u_j[i] * s_j
-            const int k = perm[p.perm_off + j];
+            const int kc = perm[p.perm_off + j];
             const double sf = forced[t.sig_off + j];
             if (!p.transposed) {
                 const double s = sig[p.s_off + j];
-                v = s > 0.0 ? sf * w[(int64_t)k * p.m + i] / s : 0.0;
+                v = s > 0.0 ? sf * w[(int64_t)kc * p.m + i] / s : 0.0;
             } else {
-                v = sf * q[(int64_t)k * p.m + i];
+                v = sf * q[(int64_t)kc * p.m + i];
             }
             v *= sgn[p.s_off + j];
         }
-        out[t.out_off + e] = v;
-    }
+        return v;
+    });
 }
 
 // K0 of every orthonormalised sector: column j = sign_j W[:, perm_j] / s_j
@@ -243,9 +307,11 @@ struct dmrg_canon_s {
     BatchedSvd svd;
     std::vector<CopyTask> copies;
     DeviceBuffer d_copies, d_writes, d_canons, d_forced;
+    int gather_tiles = 1, write_tiles = 1, canon_tiles = 1;  // grid y of the tile kernels
     // orthonormalisation of the kept ket columns taken from the working matrix
     std::vector<OrthoTask> otasks;
     int ortho_cols = 0;                     // largest t of the tasks
+    int ortho_passes = 0;                   // correction passes (the worst sector's need)
     DeviceBuffer d_otasks, d_k, d_k2, d_g, d_a;
     GemmSchedule sg, su, sc;                // K^T K; K2 -= L K; the projected canonical blocks
     // results
@@ -266,6 +332,7 @@ int plan_ortho(dmrg_canon_s* c, cudaStream_t st) {
     BatchedSvd& svd = c->svd;
     c->otasks.clear();
     c->ortho_cols = 0;
+    c->ortho_passes = 0;
     int64_t ksz = 0, gsz = 0, wsz = 0;
     for (const SvdProblem& p : svd.probs) wsz += (int64_t)p.rows * p.cols;
     for (int sct = 0; sct < c->nsec; ++sct) {
@@ -274,6 +341,17 @@ int plan_ortho(dmrg_canon_s* c, cudaStream_t st) {
         const bool wside = c->side == 0 ? !p.transposed : p.transposed != 0;
         const int t = c->tdim[sct];
         if (!wside || t <= 0) continue;
+        // the Jacobi test leaves |u_i . u_j| <= tol ||A||_F / min(s_i, s_j)
+        const std::vector<double>& sv = c->sv[sct];
+        double fro2 = 0.0;
+        for (double v : sv) fro2 += v * v;
+        const double smin = t - 1 < (int)sv.size() ? sv[t - 1] : 0.0;
+        const double tol = 2.0 * DBL_EPSILON * std::sqrt((double)p.rows);
+        const double e = smin > 0.0 ? tol * std::sqrt(fro2) / smin : 1.0;
+        int passes = 1;
+        for (double x = e; x > 1e-16 && passes < 6; x *= x) ++passes;
+        if (e >= 0.5) passes = 6;
+        c->ortho_passes = std::max(c->ortho_passes, passes);
         c->otasks.push_back(OrthoTask{svd.index[sct], t, p.rows, 0, ksz, gsz});
         c->ortho_cols = std::max(c->ortho_cols, t);
         ksz += (int64_t)p.rows * t;
@@ -329,7 +407,12 @@ int plan_ortho(dmrg_canon_s* c, cudaStream_t st) {
     return DMRG_OK;
 }
 
-// Orthonormalised ket columns (K, in c->d_k on return) and the projected
+// The buffer holding the orthonormalised columns after the passes.
+const double* ortho_result(const dmrg_canon_s* c) {
+    return (c->ortho_passes % 2 == 0 ? c->d_k : c->d_k2).as<double>();
+}
+
+// Orthonormalised ket columns (ortho_result) and the projected
 // canonical blocks of the tasks' sectors.
 int run_ortho(dmrg_canon_s* c, const double* ket_dev, double* canonical_dev, cudaStream_t st) {
     if (c->otasks.empty()) return DMRG_OK;
@@ -339,16 +422,15 @@ int run_ortho(dmrg_canon_s* c, const double* ket_dev, double* canonical_dev, cud
     const OrthoTask* ot = c->d_otasks.as<OrthoTask>();
     DMRG_CUDA_TRY(cudaMemsetAsync(c->d_a.ptr, 0, c->d_a.bytes, st));
     if (!c->copies.empty())
-        DMRG_LAUNCH gather_kernel<<<(int)c->copies.size(), 256, 0, st>>>(ket_dev, c->d_copies.as<CopyTask>(),
+        DMRG_LAUNCH gather_kernel<<<dim3((int)c->copies.size(), c->gather_tiles), 256, 0, st>>>(ket_dev, c->d_copies.as<CopyTask>(),
                                                                           svd.d_probs.as<SvdProblem>(),
                                                                           c->d_a.as<double>(), c->side);
     DMRG_LAUNCH kform_kernel<<<grid, 256, 0, st>>>(ot, svd.d_probs.as<SvdProblem>(), svd.d_w.as<double>(),
                                                    svd.d_s.as<double>(), svd.d_perm.as<int>(),
                                                    svd.d_sign.as<double>(), c->d_k.as<double>());
     DMRG_CUDA_TRY(cudaGetLastError());
-    // each pass squares the departure from orthonormality (~1e-2 at most for
-    // kept values near canpre): four take it to rounding level
-    for (int pass = 0; pass < 4; ++pass) {
+    // each pass squares the departure from orthonormality
+    for (int pass = 0; pass < c->ortho_passes; ++pass) {
         DeviceBuffer& k = pass % 2 == 0 ? c->d_k : c->d_k2;
         DeviceBuffer& k2 = pass % 2 == 0 ? c->d_k2 : c->d_k;
         DMRG_TRY(launch_gemm_f64(c->sg, k.as<double>(), k.as<double>(), c->d_g.as<double>(), false, st));
@@ -358,11 +440,11 @@ int run_ortho(dmrg_canon_s* c, const double* ket_dev, double* canonical_dev, cud
         DMRG_LAUNCH normalize_kernel<<<grid, 256, 0, st>>>(ot, k2.as<double>());
         DMRG_CUDA_TRY(cudaGetLastError());
     }
-    // four passes: the result is back in d_k
+    const double* k = ortho_result(c);
     if (c->side == 0)
-        DMRG_TRY(launch_gemm_f64(c->sc, c->d_k.as<double>(), c->d_a.as<double>(), canonical_dev, false, st));
+        DMRG_TRY(launch_gemm_f64(c->sc, k, c->d_a.as<double>(), canonical_dev, false, st));
     else
-        DMRG_TRY(launch_gemm_f64(c->sc, c->d_a.as<double>(), c->d_k.as<double>(), canonical_dev, false, st));
+        DMRG_TRY(launch_gemm_f64(c->sc, c->d_a.as<double>(), k, canonical_dev, false, st));
     return DMRG_OK;
 }
 
@@ -416,6 +498,7 @@ int dmrg_canon_create(dmrg_ctx_t ctx, int side, int nl, int nr, const int* left_
             int acc = 0;
             for (int p : c->members[s]) {
                 c->copies.push_back(CopyTask{c->ket.off[p], c->ket.rows[p], c->ket.cols[p], c->svd.index[s], acc});
+                c->gather_tiles = std::max(c->gather_tiles, tiles_of(c->ket.rows[p], c->ket.cols[p]));
                 acc += side == 0 ? c->ket.rows[p] : c->ket.cols[p];
             }
         }
@@ -444,7 +527,7 @@ int dmrg_canon_run(dmrg_canon_t c, const double* ket_dev, int max_dim, double ca
         for (const auto& p : svd.probs) wsize += (int64_t)p.rows * p.cols;
         DMRG_CUDA_TRY(cudaMemsetAsync(svd.d_w.ptr, 0, wsize * sizeof(double), st));
         if (!c->copies.empty())
-            DMRG_LAUNCH gather_kernel<<<(int)c->copies.size(), 256, 0, st>>>(ket_dev, c->d_copies.as<CopyTask>(),
+            DMRG_LAUNCH gather_kernel<<<dim3((int)c->copies.size(), c->gather_tiles), 256, 0, st>>>(ket_dev, c->d_copies.as<CopyTask>(),
                                                                  svd.d_probs.as<SvdProblem>(), svd.d_w.as<double>(),
                                                                  c->side);
         DMRG_CUDA_TRY(cudaGetLastError());
@@ -514,6 +597,9 @@ int dmrg_canon_run(dmrg_canon_t c, const double* ket_dev, int max_dim, double ca
             acc += c->side == 0 ? c->ket.rows[p] : c->ket.cols[p];
         }
     }
+    c->write_tiles = c->canon_tiles = 1;
+    for (const WriteTask& w : wtasks) c->write_tiles = std::max(c->write_tiles, tiles_of(w.rows, w.cols));
+    for (const CanonTask& t : ctasks) c->canon_tiles = std::max(c->canon_tiles, tiles_of(t.rows, t.cols));
     DMRG_TRY(upload(c->d_forced, forced, st));
     DMRG_TRY(upload(c->d_canons, ctasks, st));
     DMRG_TRY(upload(c->d_writes, wtasks, st));
@@ -576,11 +662,11 @@ int dmrg_canon_write(dmrg_canon_t c, const double* ket_dev, double* new_ket_dev,
     const double* sig = svd.d_s.as<double>();
     DMRG_TRY(run_ortho(c, ket_dev, canonical_dev, st));
     if (n_writes)
-        DMRG_LAUNCH write_ket_kernel<<<n_writes, 256, 0, st>>>(c->d_writes.as<WriteTask>(), svd.d_probs.as<SvdProblem>(),
+        DMRG_LAUNCH write_ket_kernel<<<dim3(n_writes, c->write_tiles), 256, 0, st>>>(c->d_writes.as<WriteTask>(), svd.d_probs.as<SvdProblem>(),
                                                    svd.d_w.as<double>(), svd.d_q.as<double>(), sig,
                                                    svd.d_perm.as<int>(), svd.d_sign.as<double>(),
-                                                   c->d_k.as<double>(), new_ket_dev, c->side);
-    DMRG_LAUNCH write_canonical_kernel<<<c->nsec, 256, 0, st>>>(c->d_canons.as<CanonTask>(), svd.d_probs.as<SvdProblem>(),
+                                                   ortho_result(c), new_ket_dev, c->side);
+    DMRG_LAUNCH write_canonical_kernel<<<dim3(c->nsec, c->canon_tiles), 256, 0, st>>>(c->d_canons.as<CanonTask>(), svd.d_probs.as<SvdProblem>(),
                                                     svd.d_w.as<double>(), svd.d_q.as<double>(), sig,
                                                     svd.d_perm.as<int>(), c->d_forced.as<double>(),
                                                     svd.d_sign.as<double>(), canonical_dev, c->side);

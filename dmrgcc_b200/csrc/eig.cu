@@ -6,6 +6,7 @@
 // Dense symmetric eigenproblem: two-sided cyclic Jacobi with the round-robin
 // (Brent-Luk) ordering, n/2 disjoint rotations applied per round.
 #include <cfloat>
+#include <mutex>
 
 #include "eig.cuh"
 
@@ -364,8 +365,21 @@ bool sym_jacobi_in_shared(int n) { return jacobi_in_smem(n); }
 int launch_sym_jacobi(double* A, int n, double* w, double* Z, double* ws, int* status, cudaStream_t st) {
     if (n <= 0) return DMRG_OK;
     const size_t smem = jacobi_smem(n);
-    if (smem > 48 * 1024)
-        DMRG_CUDA_TRY(cudaFuncSetAttribute(sym_jacobi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (smem > 48 * 1024) {
+        // The kernel's shared-memory allowance is process-wide: raise it under a
+        // lock and never lower it, so that runs side by side (one per host
+        // thread, each with its own n) cannot undercut each other's launch.
+        static std::mutex mu;
+        static size_t allowed[64] = {};  // per device
+        int dev = 0;
+        DMRG_CUDA_TRY(cudaGetDevice(&dev));
+        if (dev < 0 || dev >= 64) return set_error(DMRG_E_ARG, "device ordinal %d not supported", dev);
+        std::lock_guard<std::mutex> lock(mu);
+        if (smem > allowed[dev]) {
+            DMRG_CUDA_TRY(cudaFuncSetAttribute(sym_jacobi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            allowed[dev] = smem;
+        }
+    }
     DMRG_LAUNCH sym_jacobi_kernel<<<1, kJacobiThreads, smem, st>>>(A, n, w, Z, ws, status);
     DMRG_CUDA_TRY(cudaGetLastError());
     return DMRG_OK;

@@ -514,32 +514,62 @@ __global__ void __launch_bounds__(128) rotate_kernel(const SvdProblem* __restric
 // thresholds and rotations then never meet underflow, however small the
 // sector's values (a sector that carries a negligible weight of the state
 // reaches 1e-100 and below, whose squares underflow).  unscale_kernel undoes
-// it on the result.
-__global__ void __launch_bounds__(1024) prescale_kernel(const SvdProblem* __restrict__ probs, double* __restrict__ W,
-                                                        int* __restrict__ expo) {
-    __shared__ double red[32];
-    __shared__ int ex;
-    const SvdProblem p = probs[blockIdx.x];
-    double* w = W + p.w_off;
-    const int64_t cnt = (int64_t)p.rows * p.cols;
-    double mx = 0.0;
-    for (int64_t i = threadIdx.x; i < cnt; i += blockDim.x) mx = fmax(mx, fabs(w[i]));
+// it on the result.  Three kernels over grid (problems, kSlices): the slices'
+// largest magnitudes; the scaling (each slice takes the problem's maximum over
+// the slice maxima) with the slices' sums of squares; the squared Frobenius
+// norms, summing the slices in a fixed order.
+constexpr int kSlices = 32;
+__device__ __forceinline__ void slice_range(int64_t cnt, int slice, int64_t& b, int64_t& e) {
+    b = cnt * slice / kSlices;
+    e = cnt * (slice + 1) / kSlices;
+}
+
+__device__ __forceinline__ double block_reduce(double v, bool take_max) {
+    __shared__ double red[8];
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double m = 0.0;
-        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) m = fmax(m, red[k]);
-        int e = 0;
-        if (m > 0.0 && m < 0.5) frexp(m, &e);  // m = f 2^e, f in [0.5, 1), e <= -1
-        ex = e;
-        expo[blockIdx.x] = e;
+    for (int o = 16; o > 0; o >>= 1) {
+        const double u = __shfl_xor_sync(0xffffffffu, v, o);
+        v = take_max ? fmax(v, u) : v + u;
     }
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
     __syncthreads();
-    const int e = ex;
-    if (e == 0) return;
-    for (int64_t i = threadIdx.x; i < cnt; i += blockDim.x) w[i] = ldexp(w[i], -e);
+    double r = 0.0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) r = take_max ? fmax(r, red[k]) : r + red[k];
+    return r;
+}
+
+__global__ void __launch_bounds__(256) slice_max_kernel(const SvdProblem* __restrict__ probs,
+                                                        const double* __restrict__ W, double* __restrict__ part) {
+    const SvdProblem p = probs[blockIdx.x];
+    const double* w = W + p.w_off;
+    int64_t b, e;
+    slice_range((int64_t)p.rows * p.cols, blockIdx.y, b, e);
+    double mx = 0.0;
+    for (int64_t i = b + threadIdx.x; i < e; i += blockDim.x) mx = fmax(mx, fabs(w[i]));
+    mx = block_reduce(mx, true);
+    if (threadIdx.x == 0) part[blockIdx.x * kSlices + blockIdx.y] = mx;
+}
+
+__global__ void __launch_bounds__(256) prescale_kernel(const SvdProblem* __restrict__ probs, double* __restrict__ W,
+                                                       const double* __restrict__ part_max, int* __restrict__ expo,
+                                                       double* __restrict__ part_ss) {
+    const SvdProblem p = probs[blockIdx.x];
+    double m = 0.0;
+    for (int k = 0; k < kSlices; ++k) m = fmax(m, part_max[blockIdx.x * kSlices + k]);
+    int ex = 0;
+    if (m > 0.0 && m < 0.5) frexp(m, &ex);  // m = f 2^e, f in [0.5, 1), e <= -1
+    if (blockIdx.y == 0 && threadIdx.x == 0) expo[blockIdx.x] = ex;
+    double* w = W + p.w_off;
+    int64_t b, e;
+    slice_range((int64_t)p.rows * p.cols, blockIdx.y, b, e);
+    double ss = 0.0;
+    for (int64_t i = b + threadIdx.x; i < e; i += blockDim.x) {
+        const double v = ex ? ldexp(w[i], -ex) : w[i];
+        if (ex) w[i] = v;
+        ss += v * v;
+    }
+    ss = block_reduce(ss, false);
+    if (threadIdx.x == 0) part_ss[blockIdx.x * kSlices + blockIdx.y] = ss;
 }
 
 // Undoes prescale_kernel on the final working matrix and the sorted singular
@@ -557,28 +587,22 @@ __global__ void __launch_bounds__(256) unscale_kernel(const SvdProblem* __restri
         for (int j = threadIdx.x; j < p.cols; j += blockDim.x) sig[p.s_off + j] = ldexp(sig[p.s_off + j], e);
 }
 
-// Squared Frobenius norm of each working matrix (fixed-order block reduction).
-__global__ void __launch_bounds__(256) fro2_kernel(const SvdProblem* __restrict__ probs, const double* __restrict__ W,
-                                                   double* __restrict__ fro2) {
-    __shared__ double red[256];
-    const SvdProblem p = probs[blockIdx.x];
-    const double* w = W + p.w_off;
+// Squared Frobenius norm of each working matrix: its slices' sums in order.
+__global__ void fro2_kernel(const double* __restrict__ part_ss, int np, double* __restrict__ fro2) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= np) return;
     double s = 0.0;
-    for (int64_t i = threadIdx.x; i < (int64_t)p.rows * p.cols; i += blockDim.x) s += w[i] * w[i];
-    red[threadIdx.x] = s;
-    __syncthreads();
-    for (int o = 128; o > 0; o >>= 1) {
-        if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) fro2[blockIdx.x] = red[0];
+    for (int k = 0; k < kSlices; ++k) s += part_ss[i * kSlices + k];
+    fro2[i] = s;
 }
 
-__global__ void init_identity_kernel(const SvdProblem* __restrict__ probs, double* __restrict__ Q) {
+// Q <- I for every problem.  Grid (problems, kSlices).
+__global__ void __launch_bounds__(256) init_identity_kernel(const SvdProblem* __restrict__ probs, double* __restrict__ Q) {
     const SvdProblem p = probs[blockIdx.x];
     double* q = Q + p.q_off;
-    for (int64_t idx = threadIdx.x; idx < (int64_t)p.cols * p.cols; idx += blockDim.x)
-        q[idx] = (idx / p.cols == idx % p.cols) ? 1.0 : 0.0;
+    int64_t b, e;
+    slice_range((int64_t)p.cols * p.cols, blockIdx.y, b, e);
+    for (int64_t idx = b + threadIdx.x; idx < e; idx += blockDim.x) q[idx] = (idx / p.cols == idx % p.cols) ? 1.0 : 0.0;
 }
 
 // Column norms of every working matrix, one warp per column (fixed reduction order).
@@ -597,13 +621,13 @@ __global__ void __launch_bounds__(256) colnorm_kernel(const SvdProblem* __restri
 }
 
 // Descending order of the column norms (ties by column index): order[rank] = column;
-// with `sig`, also the sorted values.
+// with `sig`, also the sorted values.  Grid (problems, column slices of 256).
 __global__ void __launch_bounds__(256) rank_kernel(const SvdProblem* __restrict__ probs,
                                                    const double* __restrict__ norm, int* __restrict__ order,
                                                    double* __restrict__ sig) {
     const SvdProblem p = probs[blockIdx.x];
     const double* t = norm + p.s_off;
-    for (int j = threadIdx.x; j < p.cols; j += blockDim.x) {
+    for (int j = blockIdx.y * blockDim.x + threadIdx.x; j < p.cols; j += gridDim.y * blockDim.x) {
         const double v = t[j];
         int rank = 0;
         for (int o = 0; o < p.cols; ++o) {
@@ -811,6 +835,7 @@ int BatchedSvd::plan(const std::vector<int>& m, const std::vector<int>& n, cudaS
     DMRG_TRY(d_perm.alloc((size_t)std::max<int64_t>(soff, 1) * sizeof(int)));
     DMRG_TRY(d_fro2.alloc(std::max<size_t>(probs.size(), 1) * sizeof(double)));
     DMRG_TRY(d_expo.alloc(std::max<size_t>(probs.size(), 1) * sizeof(int)));
+    DMRG_TRY(d_part.alloc(std::max<size_t>(probs.size(), 1) * 2 * kSlices * sizeof(double)));
     DMRG_TRY(d_sign.alloc((size_t)std::max<int64_t>(soff, 1) * sizeof(double)));
     DMRG_TRY(d_colmap.alloc((size_t)std::max<int64_t>(soff, 1) * sizeof(int)));
     DMRG_TRY(d_norm.alloc((size_t)std::max<int64_t>(soff, 1) * sizeof(double)));
@@ -1000,13 +1025,18 @@ int BatchedSvd::run(cudaStream_t st, int* sweeps_out) {
         DMRG_TRY(w_in.alloc(d_w.bytes));
         DMRG_CUDA_TRY(cudaMemcpyAsync(w_in.ptr, d_w.ptr, d_w.bytes, cudaMemcpyDeviceToDevice, st));
     }
-    DMRG_LAUNCH init_identity_kernel<<<np, 256, 0, st>>>(d_probs.as<SvdProblem>(), d_q.as<double>());
-    DMRG_LAUNCH prescale_kernel<<<np, 1024, 0, st>>>(d_probs.as<SvdProblem>(), d_w.as<double>(), d_expo.as<int>());
-    DMRG_LAUNCH fro2_kernel<<<np, 256, 0, st>>>(d_probs.as<SvdProblem>(), d_w.as<double>(), d_fro2.as<double>());
+    const dim3 sliced(np, kSlices);
+    DMRG_LAUNCH init_identity_kernel<<<sliced, 256, 0, st>>>(d_probs.as<SvdProblem>(), d_q.as<double>());
+    DMRG_LAUNCH slice_max_kernel<<<sliced, 256, 0, st>>>(d_probs.as<SvdProblem>(), d_w.as<double>(), d_part.as<double>());
+    DMRG_LAUNCH prescale_kernel<<<sliced, 256, 0, st>>>(d_probs.as<SvdProblem>(), d_w.as<double>(), d_part.as<double>(),
+                                                        d_expo.as<int>(), d_part.as<double>() + (int64_t)np * kSlices);
+    DMRG_LAUNCH fro2_kernel<<<(np + 127) / 128, 128, 0, st>>>(d_part.as<double>() + (int64_t)np * kSlices, np,
+                                                              d_fro2.as<double>());
     static const bool debug = std::getenv("DMRG_SVD_DEBUG") != nullptr;  // per-sweep convergence to stderr
     int max_cols = 0;
     for (const SvdProblem& p : probs) max_cols = std::max(max_cols, p.cols);
     const dim3 colgrid(np, (max_cols + 7) / 8);
+    const dim3 rankgrid(np, (max_cols + 255) / 256);
     std::vector<double> bm(tiles.size()), worst(np);
     const int max_sweeps = g_max_sweeps.load();
     auto t_sweep = std::chrono::steady_clock::now();
@@ -1017,7 +1047,7 @@ int BatchedSvd::run(cudaStream_t st, int* sweeps_out) {
         // similar size, which keeps the many tiny singular values of a noise-expanded
         // tensor from converging only linearly; then every block pair is measured
         DMRG_LAUNCH colnorm_kernel<<<colgrid, 256, 0, st>>>(d_probs.as<SvdProblem>(), d_w.as<double>(), d_norm.as<double>());
-        DMRG_LAUNCH rank_kernel<<<np, 256, 0, st>>>(d_probs.as<SvdProblem>(), d_norm.as<double>(), d_colmap.as<int>(),
+        DMRG_LAUNCH rank_kernel<<<rankgrid, 256, 0, st>>>(d_probs.as<SvdProblem>(), d_norm.as<double>(), d_colmap.as<int>(),
                                                     nullptr);
         DMRG_LAUNCH measure_kernel<<<(int)tiles.size(), 128, 0, st>>>(
             d_probs.as<SvdProblem>(), d_tiles.as<SvdTile>(), d_colmap.as<int>(), d_w.as<double>(),
@@ -1086,7 +1116,7 @@ int BatchedSvd::run(cudaStream_t st, int* sweeps_out) {
     }
     // singular values = final column norms, sorted
     DMRG_LAUNCH colnorm_kernel<<<colgrid, 256, 0, st>>>(d_probs.as<SvdProblem>(), d_w.as<double>(), d_norm.as<double>());
-    DMRG_LAUNCH rank_kernel<<<np, 256, 0, st>>>(d_probs.as<SvdProblem>(), d_norm.as<double>(), d_perm.as<int>(), d_s.as<double>());
+    DMRG_LAUNCH rank_kernel<<<rankgrid, 256, 0, st>>>(d_probs.as<SvdProblem>(), d_norm.as<double>(), d_perm.as<int>(), d_s.as<double>());
     DMRG_LAUNCH sign_kernel<<<colgrid, 256, 0, st>>>(d_probs.as<SvdProblem>(), d_w.as<double>(),
                                                                d_q.as<double>(), d_perm.as<int>(), d_sign.as<double>());
     DMRG_LAUNCH unscale_kernel<<<dim3(np, 32), 256, 0, st>>>(d_probs.as<SvdProblem>(), d_expo.as<int>(),

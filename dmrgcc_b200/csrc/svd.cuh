@@ -86,6 +86,7 @@ public:
 
     DeviceBuffer d_w, d_q, d_s, d_perm, d_probs, d_tasks, d_fro2;
     DeviceBuffer d_expo;  // per problem: the power of two W was scaled by (prescale_kernel)
+    DeviceBuffer d_part;  // per problem and slice: largest magnitude, then sum of squares
     DeviceBuffer d_sign;  // +-1 per sorted singular triplet (sign convention, set by run())
     DeviceBuffer d_gram_items, d_rot_items, d_gpart, d_rot, d_skip;
     DeviceBuffer d_colmap, d_norm;  // per sweep: columns in descending norm order
