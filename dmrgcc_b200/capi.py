@@ -103,6 +103,8 @@ _SIGS = {
     "dmrg_zcanon_singular_values": (C.c_int, [_VP, C.c_int, C.c_int, _D, _I]),
     "dmrg_zcanon_write": (C.c_int, [_VP, _VP, _VP, _VP]),
     "dmrg_svd_pair_schedule": (C.c_int, [C.POINTER(C.c_uint)]),
+    "dmrg_svd_plan_rounds": (C.c_int, [C.c_int, C.POINTER(C.c_double), C.c_double, C.c_int, C.POINTER(C.c_int),
+                                       C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "dmrg_svd_set_max_sweeps": (C.c_int, [C.c_int]),
     "dmrg_quicksort_index": (C.c_int, [_D, _I, C.c_int, C.c_int]),
     "dmrg_truncate_dims": (C.c_int, [C.c_int, _I, _D, C.c_int, C.c_double, _I]),
@@ -550,6 +552,21 @@ def truncate_dims(svals, max_dim: int, canpre: float):
         out.append(flat[pos:pos + c].copy())
         pos += c
     return t[:len(svals)], out
+
+
+def svd_plan_rounds(cols: int, bm, tol: float):
+    """The Jacobi sweep's rounds for one sector (host data; no GPU needed):
+    a list of rounds, each a list of (bi, bj) block pairs."""
+    bm = np.ascontiguousarray(bm, dtype=np.float64)
+    cap = 4096
+    out = np.zeros(cap, dtype=np.int32)
+    n_pairs, n_rounds = C.c_int(), C.c_int()
+    check(lib().dmrg_svd_plan_rounds(cols, _dptr(bm), tol, cap, _iptr(out), C.byref(n_pairs), C.byref(n_rounds)),
+          "dmrg_svd_plan_rounds")
+    rounds = [[] for _ in range(n_rounds.value)]
+    for v in out[:n_pairs.value]:
+        rounds[int(v) >> 16].append(((int(v) >> 8) & 255, int(v) & 255))
+    return rounds
 
 
 def svd_pair_schedule() -> np.ndarray:

@@ -1149,6 +1149,26 @@ extern "C" int dmrg_svd_set_max_sweeps(int sweeps) {
     return DMRG_OK;
 }
 
+extern "C" int dmrg_svd_plan_rounds(int cols, const double* bm, double tol, int cap, int* pairs, int* n_pairs,
+                                    int* n_rounds) {
+    if (cols <= 0 || !bm || !n_pairs || !n_rounds || (cap > 0 && !pairs))
+        return dmrg::set_error(DMRG_E_ARG, "invalid argument");
+    dmrg::SvdProblem p{};
+    p.rows = p.cols = p.m = p.n = cols;
+    const int nb = (cols + dmrg::kBlk - 1) / dmrg::kBlk;
+    p.nbe = std::max(2, nb + (nb & 1));
+    const auto rounds = dmrg::problem_rounds(p, bm, tol);
+    int k = 0;
+    for (size_t r = 0; r < rounds.size(); ++r)
+        for (const auto& pr : rounds[r]) {
+            if (k < cap) pairs[k] = (int)r << 16 | pr.first << 8 | pr.second;
+            ++k;
+        }
+    *n_pairs = k;
+    *n_rounds = (int)rounds.size();
+    return k <= cap ? DMRG_OK : dmrg::set_error(DMRG_E_ARG, "%d pairs, room for %d", k, cap);
+}
+
 extern "C" int dmrg_svd_pair_schedule(unsigned int* out) {
     if (!out) return dmrg::set_error(DMRG_E_ARG, "null argument");
     const std::vector<uint32_t>* tab = dmrg::pair_schedule();

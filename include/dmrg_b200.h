@@ -322,6 +322,14 @@ int dmrg_canon_write(dmrg_canon_t c, const double* ket_dev, double* new_ket_dev,
  * seat j is not the one addressed first.  Every two columns share one step;
  * within each half-warp the first (and the second) columns are distinct mod 16. */
 int dmrg_svd_pair_schedule(unsigned int* out);
+/* The rounds a Jacobi sweep visits for one sector of `cols` columns (diagnostic;
+ * no reference counterpart): bm holds the block-pair measures of its 32-column
+ * blocks (bi <= bj, row-major over bi: nb (nb + 1) / 2 values), tol the
+ * convergence threshold.  pairs[k] = round << 16 | bi << 8 | bj for the block
+ * pairs the sweep solves (bj may be the empty block that pads an odd count);
+ * *n_pairs and *n_rounds are set, DMRG_E_ARG when more than cap pairs. */
+int dmrg_svd_plan_rounds(int cols, const double* bm, double tol, int cap, int* pairs, int* n_pairs,
+                         int* n_rounds);
 /* Cap on the Jacobi sweeps of every later canonicalisation in this process
  * (sweeps <= 0: the default, 40).  A canonicalisation that does not converge
  * within the cap returns DMRG_E_NUMERIC, as the reference treats a failed

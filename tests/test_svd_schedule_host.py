@@ -84,3 +84,45 @@ def test_seat_shift_accumulates_the_rotation_product():
         reg[:, seat_column(lane, steps)] = q1[:, lane]
         reg[:, seat_column(63 - lane, steps)] = q2[:, lane]
     assert np.allclose(reg, direct, atol=1e-13)
+
+
+def _tiles(nb, meas):
+    """measure matrix (nb x nb, symmetric) -> the planner's tile order (bi <= bj, row-major)"""
+    return np.array([meas[i, j] for i in range(nb) for j in range(i, nb)])
+
+
+def test_guided_rounds_cover_every_unconverged_pair_once():
+    """The measure-guided sweep (svd.cu, problem_rounds): every round is a
+    matching of column blocks, every block pair whose measure is above tol is
+    solved exactly once, every block unconverged only within itself takes part
+    in some pair, and a sweep never needs more rounds than the full round-robin
+    order plus one round per such block.  Random measure patterns, from a few
+    unconverged pairs (the late sweeps) to all of them (the first)."""
+    rng = np.random.default_rng(5)
+    tol = 1e-14
+    for cols in (20, 64, 100, 384, 550, 668):
+        nb = (cols + 31) // 32
+        nbe = max(2, nb + (nb & 1))
+        for frac in (0.0, 0.05, 0.3, 1.0):
+            meas = np.where(rng.random((nb, nb)) < frac, rng.uniform(2, 1e6, (nb, nb)) * tol,
+                            rng.uniform(0, 0.9, (nb, nb)) * tol)
+            meas = np.triu(meas) + np.triu(meas, 1).T
+            rounds = capi.svd_plan_rounds(cols, _tiles(nb, meas), tol)
+            seen = {}
+            in_pair = set()
+            for rd in rounds:
+                used = [b for pr in rd for b in pr]
+                assert len(used) == len(set(used)), "a block twice in one round"
+                for bi, bj in rd:
+                    assert 0 <= bi < bj < nbe
+                    seen[(bi, bj)] = seen.get((bi, bj), 0) + 1
+                    in_pair.update((bi, bj))
+            need = {(i, j) for i in range(nb) for j in range(i + 1, nb) if meas[i, j] > tol}
+            for pr in need:
+                assert seen.get(pr) == 1, (cols, frac, pr)
+            internal = [i for i in range(nb) if meas[i, i] > tol]
+            for i in internal:
+                assert i in in_pair
+            if not need and not internal:
+                assert rounds == []
+            assert len(rounds) <= (nbe - 1) + len(internal)
