@@ -13,21 +13,11 @@
 // case: one singular value 0, a zero canonical block, the ket untouched.
 //
 // The kept columns on the ket's side are orthonormal to FP64 rounding, as the
-// reference's dgesvd gives them.  Where the ket side is the one the Jacobi SVD
-// accumulates (U of a wide A, V of a tall A) it already is.  Where it is the
-// side whose vectors are the working matrix's columns divided by their norms,
-// the Jacobi convergence test (a backward error of eps ||A||) leaves vectors of
-// singular values near eps ||A|| / |x| non-orthogonal by up to ~1e-2, so they
-// are orthonormalised in descending order (Gram-Schmidt in effect: K <- K (I -
-// strictly upper part of K^T K), columns renormalised, each pass squaring the
-// departure from orthonormality; as many passes as take the largest departure
-// the convergence test allows, tol ||A||_F / s_t with s_t the smallest kept
-// value, below 1e-16, plus one), and the canonical block is the
-// projection of the sector matrix on them (K^T A left, A K right), zero in the
-// rows / columns whose singular value the truncation forced to 0.  Since
-// K = K0 R with R upper triangular and near the identity, row i of K^T A is
-// s_i v_i^T plus terms of size eps ||A||: the same factors as diag(S) V^T to
-// rounding, now with an orthonormal ket.
+// reference's dgesvd gives them: where the ket side is the one the Jacobi SVD
+// leaves as the working matrix's normalised columns, they are orthonormalised
+// (KetOrtho, ortho.cuh) and the canonical block is the projection of the sector
+// matrix on them (K^T A left, A K right), zero in the rows / columns whose
+// singular value the truncation forced to 0.
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
@@ -35,6 +25,7 @@
 
 #include "blocksparse.h"
 #include "gemm.cuh"
+#include "ortho.cuh"
 #include "svd.cuh"
 #include "truncate.h"
 
@@ -64,17 +55,6 @@ struct CanonTask {
     int64_t sig_off;  // offset of the forced singular values of this sector
     int projected;    // 1: written as a projection (GEMM), only the forced zeros here
     int pad_;
-};
-
-// A sector whose kept ket columns are orthonormalised: its working-matrix
-// columns U = W / s (left, W = A) or V = W / s (right, W = A^T), t of them,
-// rows r (= the working matrix's rows), at k_off (column-major, ld r) of the
-// K buffer; its Gram matrix (t x t, row-major) at g_off.
-struct OrthoTask {
-    int problem;
-    int t, r;
-    int pad_;
-    int64_t k_off, g_off;
 };
 
 // The kernels below move blocks in 32x32 tiles, one tile per CTA of 256
@@ -252,47 +232,6 @@ __global__ void __launch_bounds__(256) write_canonical_kernel(const CanonTask* _
     });
 }
 
-// K0 of every orthonormalised sector: column j = sign_j W[:, perm_j] / s_j
-// (0 where s_j = 0).  Grid (tasks, column groups of 8), one warp per column.
-__global__ void __launch_bounds__(256) kform_kernel(const OrthoTask* __restrict__ tasks,
-                                                    const SvdProblem* __restrict__ probs, const double* __restrict__ W,
-                                                    const double* __restrict__ sig, const int* __restrict__ perm,
-                                                    const double* __restrict__ sgn, double* __restrict__ K) {
-    const OrthoTask t = tasks[blockIdx.x];
-    const int j = blockIdx.y * 8 + (threadIdx.x >> 5);
-    if (j >= t.t) return;
-    const SvdProblem p = probs[t.problem];
-    const double s = sig[p.s_off + j];
-    const double f = s > 0.0 ? sgn[p.s_off + j] / s : 0.0;
-    const double* w = W + p.w_off + (int64_t)perm[p.perm_off + j] * p.rows;
-    double* k = K + t.k_off + (int64_t)j * t.r;
-    for (int i = threadIdx.x & 31; i < t.r; i += 32) k[i] = f * w[i];
-}
-
-// G (t x t, row-major, symmetric) <- its strictly lower part.
-__global__ void __launch_bounds__(256) strict_lower_kernel(const OrthoTask* __restrict__ tasks, double* __restrict__ G) {
-    const OrthoTask t = tasks[blockIdx.x];
-    double* g = G + t.g_off;
-    for (int64_t e = threadIdx.x; e < (int64_t)t.t * t.t; e += blockDim.x)
-        if (e % t.t >= e / t.t) g[e] = 0.0;
-}
-
-// Every nonzero column of K scaled to unit norm.  Grid (tasks, column groups of
-// 8), one warp per column (fixed reduction order).
-__global__ void __launch_bounds__(256) normalize_kernel(const OrthoTask* __restrict__ tasks, double* __restrict__ K) {
-    const OrthoTask t = tasks[blockIdx.x];
-    const int j = blockIdx.y * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
-    if (j >= t.t) return;
-    double* k = K + t.k_off + (int64_t)j * t.r;
-    double s = 0.0;
-    for (int i = lane; i < t.r; i += 32) s += k[i] * k[i];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if (s <= 0.0) return;
-    const double f = 1.0 / sqrt(s);
-    for (int i = lane; i < t.r; i += 32) k[i] *= f;
-}
-
 }  // namespace
 
 struct dmrg_canon_s {
@@ -309,11 +248,9 @@ struct dmrg_canon_s {
     DeviceBuffer d_copies, d_writes, d_canons, d_forced;
     int gather_tiles = 1, write_tiles = 1, canon_tiles = 1;  // grid y of the tile kernels
     // orthonormalisation of the kept ket columns taken from the working matrix
-    std::vector<OrthoTask> otasks;
-    int ortho_cols = 0;                     // largest t of the tasks
-    int ortho_passes = 0;                   // correction passes (the worst sector's need)
-    DeviceBuffer d_otasks, d_k, d_k2, d_g, d_a;
-    GemmSchedule sg, su, sc;                // K^T K; K2 -= L K; the projected canonical blocks
+    KetOrtho ortho;
+    DeviceBuffer d_a;                       // the sector matrices again (working-matrix layout)
+    GemmSchedule sc;                        // the projected canonical blocks
     // results
     bool ran = false;
     std::vector<std::vector<double>> sv;  // singular values per sector (reference semantics)
@@ -326,125 +263,68 @@ struct dmrg_canon_s {
 
 namespace {
 
-// The orthonormalisation tasks of a run (sectors whose ket side is the working
-// matrix's columns) and the three GEMM schedules over them.
+// The orthonormalisation of a run (sectors whose ket side is the working
+// matrix's columns) and the GEMM schedule of the projected canonical blocks.
 int plan_ortho(dmrg_canon_s* c, cudaStream_t st) {
     BatchedSvd& svd = c->svd;
-    c->otasks.clear();
-    c->ortho_cols = 0;
-    c->ortho_passes = 0;
-    int64_t ksz = 0, gsz = 0, wsz = 0;
+    std::vector<int> kept(svd.probs.size(), 0);
+    std::vector<std::vector<double>> sv(svd.probs.size());
+    int64_t wsz = 0;
     for (const SvdProblem& p : svd.probs) wsz += (int64_t)p.rows * p.cols;
     for (int sct = 0; sct < c->nsec; ++sct) {
         if (!svd.active(sct)) continue;
         const SvdProblem& p = svd.problem(sct);
         const bool wside = c->side == 0 ? !p.transposed : p.transposed != 0;
-        const int t = c->tdim[sct];
-        if (!wside || t <= 0) continue;
-        // the Jacobi test leaves |u_i . u_j| <= tol ||A||_F / min(s_i, s_j)
-        const std::vector<double>& sv = c->sv[sct];
-        double fro2 = 0.0;
-        for (double v : sv) fro2 += v * v;
-        const double smin = t - 1 < (int)sv.size() ? sv[t - 1] : 0.0;
-        const double tol = 2.0 * DBL_EPSILON * std::sqrt((double)p.rows);
-        const double e = smin > 0.0 ? tol * std::sqrt(fro2) / smin : 1.0;
-        int passes = 1;
-        for (double x = e; x > 1e-16 && passes < 6; x *= x) ++passes;
-        if (e >= 0.5) passes = 6;
-        c->ortho_passes = std::max(c->ortho_passes, passes);
-        c->otasks.push_back(OrthoTask{svd.index[sct], t, p.rows, 0, ksz, gsz});
-        c->ortho_cols = std::max(c->ortho_cols, t);
-        ksz += (int64_t)p.rows * t;
-        gsz += (int64_t)t * t;
+        if (!wside || c->tdim[sct] <= 0) continue;
+        kept[svd.index[sct]] = c->tdim[sct];
+        sv[svd.index[sct]] = c->sv[sct];
     }
-    if (c->otasks.empty()) return DMRG_OK;
-    DMRG_TRY(c->d_k.alloc(ksz * sizeof(double)));
-    DMRG_TRY(c->d_k2.alloc(ksz * sizeof(double)));
-    DMRG_TRY(c->d_g.alloc(gsz * sizeof(double)));
+    DMRG_TRY(c->ortho.plan(svd, kept, sv, st, c->ctx->num_sms));
+    if (c->ortho.empty()) return DMRG_OK;
     DMRG_TRY(c->d_a.alloc(std::max<int64_t>(wsz, 1) * sizeof(double)));
-    DMRG_TRY(upload(c->d_otasks, c->otasks, st));
-    GemmSchedule &sg = c->sg, &su = c->su, &sc = c->sc;
-    sg.reset();
-    su.reset();
+    GemmSchedule& sc = c->sc;
     sc.reset();
-    sg.tb = true;  // G = K^T K: K^T is K column-major read row-major (t x r), K the transposed B
     sc.tb = true;
-    for (const OrthoTask& o : c->otasks) {
-        sg.add_group(o.g_off, o.t, o.t, o.t);
-        sg.add_term(o.k_off, o.r, o.k_off, o.r, o.r, 1.0);
-        // K2^T (row-major t x r) -= L (t x t) K^T: L = the strictly lower part of G
-        su.add_group(o.k_off, o.r, o.t, o.r);
-        su.add_term(o.g_off, o.t, o.k_off, o.r, o.t, -1.0);
-    }
     for (int sct = 0; sct < c->nsec; ++sct) {
         if (!svd.active(sct)) continue;
         const int pi = svd.index[sct];
+        const int64_t ko = c->ortho.k_off(pi);
+        if (ko < 0) continue;
         const SvdProblem& p = svd.probs[pi];
-        const OrthoTask* o = nullptr;
-        for (const OrthoTask& x : c->otasks)
-            if (x.problem == pi) o = &x;
-        if (!o) continue;
+        const int t = c->tdim[sct];
         if (c->side == 0) {
             // C (t x n) = K^T A; A (m x n) is held column-major (W layout), i.e. the transposed B
-            sc.add_group(c->canonical.off[sct], p.n, o->t, p.n);
-            sc.add_term(o->k_off, p.rows, p.w_off, p.rows, p.rows, 1.0);
+            sc.add_group(c->canonical.off[sct], p.n, t, p.n);
+            sc.add_term(ko, p.rows, p.w_off, p.rows, p.rows, 1.0);
         } else {
             // C (m x t) = A K; A is held as A^T column-major = A row-major (ld n); K the transposed B
-            sc.add_group(c->canonical.off[sct], o->t, p.m, o->t);
-            sc.add_term(p.w_off, p.rows, o->k_off, p.rows, p.rows, 1.0);
+            sc.add_group(c->canonical.off[sct], t, p.m, t);
+            sc.add_term(p.w_off, p.rows, ko, p.rows, p.rows, 1.0);
         }
     }
-    DMRG_TRY(sg.check_bounds(ksz, ksz, gsz));
-    DMRG_TRY(su.check_bounds(gsz, ksz, ksz));
+    const int64_t ksz = c->ortho.k_size();
     if (c->side == 0)
         DMRG_TRY(sc.check_bounds(ksz, wsz, c->canonical.size));
     else
         DMRG_TRY(sc.check_bounds(wsz, ksz, c->canonical.size));
-    const int sms = c->ctx->num_sms;
-    DMRG_TRY(sg.finalize(64, 64, 16, st, sms));
-    DMRG_TRY(su.finalize(64, 64, 16, st, sms));
-    DMRG_TRY(sc.finalize(64, 64, 16, st, sms));
+    DMRG_TRY(sc.finalize(64, 64, 16, st, c->ctx->num_sms));
     return DMRG_OK;
 }
 
-// The buffer holding the orthonormalised columns after the passes.
-const double* ortho_result(const dmrg_canon_s* c) {
-    return (c->ortho_passes % 2 == 0 ? c->d_k : c->d_k2).as<double>();
-}
-
-// Orthonormalised ket columns (ortho_result) and the projected
-// canonical blocks of the tasks' sectors.
+// Orthonormalised ket columns and the projected canonical blocks.
 int run_ortho(dmrg_canon_s* c, const double* ket_dev, double* canonical_dev, cudaStream_t st) {
-    if (c->otasks.empty()) return DMRG_OK;
+    if (c->ortho.empty()) return DMRG_OK;
     BatchedSvd& svd = c->svd;
-    const int nt = (int)c->otasks.size();
-    const dim3 grid(nt, (c->ortho_cols + 7) / 8);
-    const OrthoTask* ot = c->d_otasks.as<OrthoTask>();
     DMRG_CUDA_TRY(cudaMemsetAsync(c->d_a.ptr, 0, c->d_a.bytes, st));
     if (!c->copies.empty())
-        DMRG_LAUNCH gather_kernel<<<dim3((int)c->copies.size(), c->gather_tiles), 256, 0, st>>>(ket_dev, c->d_copies.as<CopyTask>(),
-                                                                          svd.d_probs.as<SvdProblem>(),
-                                                                          c->d_a.as<double>(), c->side);
-    DMRG_LAUNCH kform_kernel<<<grid, 256, 0, st>>>(ot, svd.d_probs.as<SvdProblem>(), svd.d_w.as<double>(),
-                                                   svd.d_s.as<double>(), svd.d_perm.as<int>(),
-                                                   svd.d_sign.as<double>(), c->d_k.as<double>());
+        DMRG_LAUNCH gather_kernel<<<dim3((int)c->copies.size(), c->gather_tiles), 256, 0, st>>>(
+            ket_dev, c->d_copies.as<CopyTask>(), svd.d_probs.as<SvdProblem>(), c->d_a.as<double>(), c->side);
     DMRG_CUDA_TRY(cudaGetLastError());
-    // each pass squares the departure from orthonormality
-    for (int pass = 0; pass < c->ortho_passes; ++pass) {
-        DeviceBuffer& k = pass % 2 == 0 ? c->d_k : c->d_k2;
-        DeviceBuffer& k2 = pass % 2 == 0 ? c->d_k2 : c->d_k;
-        DMRG_TRY(launch_gemm_f64(c->sg, k.as<double>(), k.as<double>(), c->d_g.as<double>(), false, st));
-        DMRG_LAUNCH strict_lower_kernel<<<nt, 256, 0, st>>>(ot, c->d_g.as<double>());
-        DMRG_CUDA_TRY(cudaMemcpyAsync(k2.ptr, k.ptr, k.bytes, cudaMemcpyDeviceToDevice, st));
-        DMRG_TRY(launch_gemm_f64(c->su, c->d_g.as<double>(), k.as<double>(), k2.as<double>(), true, st));
-        DMRG_LAUNCH normalize_kernel<<<grid, 256, 0, st>>>(ot, k2.as<double>());
-        DMRG_CUDA_TRY(cudaGetLastError());
-    }
-    const double* k = ortho_result(c);
+    DMRG_TRY(c->ortho.run(svd, st));
     if (c->side == 0)
-        DMRG_TRY(launch_gemm_f64(c->sc, k, c->d_a.as<double>(), canonical_dev, false, st));
+        DMRG_TRY(launch_gemm_f64(c->sc, c->ortho.k(), c->d_a.as<double>(), canonical_dev, false, st));
     else
-        DMRG_TRY(launch_gemm_f64(c->sc, c->d_a.as<double>(), k, canonical_dev, false, st));
+        DMRG_TRY(launch_gemm_f64(c->sc, c->d_a.as<double>(), c->ortho.k(), canonical_dev, false, st));
     return DMRG_OK;
 }
 
@@ -583,17 +463,15 @@ int dmrg_canon_run(dmrg_canon_t c, const double* ket_dev, int max_dim, double ca
         ctasks.push_back(t);
     }
     DMRG_TRY(plan_ortho(c, st));
-    std::vector<int64_t> k_of(c->nsec, -1);
-    for (const OrthoTask& o : c->otasks) k_of[o.problem] = o.k_off;  // by problem index
     for (CanonTask& t : ctasks)
-        if (t.problem >= 0 && k_of[t.problem] >= 0) t.projected = 1;
+        if (t.problem >= 0 && c->ortho.k_off(t.problem) >= 0) t.projected = 1;
     std::vector<WriteTask> wtasks;
     for (int sct = 0; sct < c->nsec; ++sct) {
         if (!svd.active(sct)) continue;
         int acc = 0;
         for (int p : c->members[sct]) {
             wtasks.push_back(WriteTask{c->new_ket.off[p], c->new_ket.rows[p], c->new_ket.cols[p], svd.index[sct], acc,
-                                       k_of[svd.index[sct]]});
+                                       c->ortho.k_off(svd.index[sct])});
             acc += c->side == 0 ? c->ket.rows[p] : c->ket.cols[p];
         }
     }
@@ -665,7 +543,7 @@ int dmrg_canon_write(dmrg_canon_t c, const double* ket_dev, double* new_ket_dev,
         DMRG_LAUNCH write_ket_kernel<<<dim3(n_writes, c->write_tiles), 256, 0, st>>>(c->d_writes.as<WriteTask>(), svd.d_probs.as<SvdProblem>(),
                                                    svd.d_w.as<double>(), svd.d_q.as<double>(), sig,
                                                    svd.d_perm.as<int>(), svd.d_sign.as<double>(),
-                                                   ortho_result(c), new_ket_dev, c->side);
+                                                   c->ortho.k(), new_ket_dev, c->side);
     DMRG_LAUNCH write_canonical_kernel<<<dim3(c->nsec, c->canon_tiles), 256, 0, st>>>(c->d_canons.as<CanonTask>(), svd.d_probs.as<SvdProblem>(),
                                                     svd.d_w.as<double>(), svd.d_q.as<double>(), sig,
                                                     svd.d_perm.as<int>(), c->d_forced.as<double>(),

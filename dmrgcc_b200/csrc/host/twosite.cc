@@ -31,6 +31,7 @@
 
 #include "gemm.cuh"
 #include "host/engine.h"
+#include "ortho.cuh"
 #include "twosite.cuh"
 
 extern "C" {
@@ -294,7 +295,7 @@ int Engine::TwoSiteStep(bool l2r, int j, int niter, double& energy, int& dim, do
             aphys[(size_t)k * nk + q] = M.p1[a];
             na.d.push(k, q, A.left_dim[k], t[keep[q]]);
             const int pos = na.d.count() - 1;
-            writes.push_back(SplitWrite{na.d.off[pos], na.d.rows[pos], na.d.cols[pos], keep[q], M.row0[a], 0});
+            writes.push_back(SplitWrite{na.d.off[pos], na.d.rows[pos], na.d.cols[pos], keep[q], M.row0[a], 0, -1, -1});
         }
     std::vector<SplitWrite> writes_b;
     for (int q = 0; q < nk; ++q) {
@@ -306,13 +307,78 @@ int Engine::TwoSiteStep(bool l2r, int j, int niter, double& energy, int& dim, do
             bphys2[(size_t)q * B.nr() + l] = M.p2[b];
             nb.d.push(q, l, t[keep[q]], B.right_dim[l]);
             const int pos = nb.d.count() - 1;
-            writes_b.push_back(SplitWrite{nb.d.off[pos], nb.d.rows[pos], nb.d.cols[pos], keep[q], M.col0[b], 1});
+            writes_b.push_back(SplitWrite{nb.d.off[pos], nb.d.rows[pos], nb.d.cols[pos], keep[q], M.col0[b], 1, -1, -1});
         }
     }
     writes.insert(writes.end(), writes_b.begin(), writes_b.end());
+    // the canonical factor (U left to right, V^T right to left) orthonormal: where
+    // it is the working matrix's normalised columns, orthonormalise them and take
+    // the other factor as the projection of M_c on them
+    KetOrtho ortho;
+    DeviceBuffer d_a, d_p;
+    std::vector<int64_t> p_of(svd.probs.size(), -1);
+    {
+        std::vector<int> kept(svd.probs.size(), 0);
+        std::vector<std::vector<double>> svp(svd.probs.size());
+        for (int s : keep) {
+            const int pi = svd.index[s];
+            if (pi < 0) continue;
+            const SvdProblem& p = svd.probs[pi];
+            const bool wside = l2r ? !p.transposed : p.transposed != 0;
+            if (!wside) continue;
+            kept[pi] = t[s];
+            svp[pi] = sv[s];
+        }
+        DMRG_TRY(ortho.plan(svd, kept, svp, st_, ctx_->num_sms));
+        if (!ortho.empty()) {
+            int64_t wsz = 0, psz = 0;
+            for (const SvdProblem& p : svd.probs) wsz += (int64_t)p.rows * p.cols;
+            GemmSchedule sp;
+            sp.tb = true;
+            for (int pi = 0; pi < (int)svd.probs.size(); ++pi) {
+                const int64_t ko = ortho.k_off(pi);
+                if (ko < 0) continue;
+                const SvdProblem& p = svd.probs[pi];
+                const int tk = kept[pi];
+                p_of[pi] = psz;
+                if (l2r) {  // S V^T = K^T M (t x n); M column-major (W layout) is the transposed B
+                    sp.add_group(psz, p.n, tk, p.n);
+                    sp.add_term(ko, p.rows, p.w_off, p.rows, p.rows, 1.0);
+                    psz += (int64_t)tk * p.n;
+                } else {    // U S = M K (m x t); M^T column-major = M row-major (ld n); K the transposed B
+                    sp.add_group(psz, tk, p.m, tk);
+                    sp.add_term(p.w_off, p.rows, ko, p.rows, p.rows, 1.0);
+                    psz += (int64_t)p.m * tk;
+                }
+            }
+            DMRG_TRY(d_a.alloc(std::max<int64_t>(wsz, 1) * sizeof(double)));
+            DMRG_TRY(d_p.alloc(std::max<int64_t>(psz, 1) * sizeof(double)));
+            if (l2r)
+                DMRG_TRY(sp.check_bounds(ortho.k_size(), wsz, psz));
+            else
+                DMRG_TRY(sp.check_bounds(wsz, ortho.k_size(), psz));
+            DMRG_TRY(sp.finalize(64, 64, 16, st_, ctx_->num_sms));
+            DeviceBuffer d_split2;
+            DMRG_TRY(twosite_gather(svd, svd.index, th.ptr(), split, d_split2, st_, d_a.as<double>()));
+            DMRG_TRY(ortho.run(svd, st_));
+            if (l2r)
+                DMRG_TRY(launch_gemm_f64(sp, ortho.k(), d_a.as<double>(), d_p.as<double>(), false, st_));
+            else
+                DMRG_TRY(launch_gemm_f64(sp, d_a.as<double>(), ortho.k(), d_p.as<double>(), false, st_));
+            const int canonical_part = l2r ? 0 : 1;
+            for (SplitWrite& w : writes) {
+                const int pi = svd.index[w.sector];
+                if (pi < 0 || ortho.k_off(pi) < 0) continue;
+                if (w.part == canonical_part)
+                    w.k_off = ortho.k_off(pi);
+                else
+                    w.p_off = p_of[pi];
+            }
+        }
+    }
     DMRG_TRY(na.alloc(st_, false));
     DMRG_TRY(nb.alloc(st_, false));
-    DMRG_TRY(twosite_write(svd, svd.index, writes, d_writes, na.ptr(), nb.ptr(), !l2r, st_));
+    DMRG_TRY(twosite_write(svd, svd.index, writes, d_writes, na.ptr(), nb.ptr(), !l2r, st_, ortho.k(), d_p.as<double>()));
     A.ket = std::move(na);
     A.right_block = mid_block;
     A.right_dim = mid_dim;

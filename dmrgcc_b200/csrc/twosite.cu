@@ -33,13 +33,30 @@ __global__ void twosite_write_kernel(const SplitWrite* __restrict__ writes, cons
                                      const SvdProblem* __restrict__ probs, const double* __restrict__ W,
                                      const double* __restrict__ Q, const double* __restrict__ sig,
                                      const int* __restrict__ perm, const double* __restrict__ sgn,
-                                     double* __restrict__ left, double* __restrict__ right, int s_left) {
+                                     double* __restrict__ left, double* __restrict__ right, int s_left,
+                                     const double* __restrict__ K, const double* __restrict__ P) {
     const SplitWrite t = writes[blockIdx.x];
     const SvdProblem p = probs[batch[t.sector]];
     const double* w = W + p.w_off;
     const double* q = Q + p.q_off;
     double* out = t.part == 0 ? left : right;
     const int64_t total = (int64_t)t.rows * t.cols;
+    if (t.k_off >= 0) {  // orthonormalised columns: U[row][j] (part 0) or V^T[i][col] (part 1)
+        const double* k = K + t.k_off;
+        for (int64_t e = threadIdx.x; e < total; e += blockDim.x) {
+            const int i = (int)(e / t.cols), j = (int)(e % t.cols);
+            out[t.out_off + e] = t.part == 0 ? k[(int64_t)j * p.rows + t.off + i] : k[(int64_t)i * p.rows + t.off + j];
+        }
+        return;
+    }
+    if (t.p_off >= 0) {  // projected factor: S V^T columns (part 1, t x n) or U S rows (part 0, m x t)
+        const double* pr = P + t.p_off;
+        for (int64_t e = threadIdx.x; e < total; e += blockDim.x) {
+            const int i = (int)(e / t.cols), j = (int)(e % t.cols);
+            out[t.out_off + e] = t.part == 1 ? pr[(int64_t)i * p.n + t.off + j] : pr[(int64_t)(t.off + i) * t.cols + j];
+        }
+        return;
+    }
     for (int64_t e = threadIdx.x; e < total; e += blockDim.x) {
         const int i = (int)(e / t.cols), j = (int)(e % t.cols);
         double v;
@@ -75,10 +92,11 @@ __global__ void twosite_write_kernel(const SplitWrite* __restrict__ writes, cons
 }  // namespace
 
 int twosite_gather(BatchedSvd& svd, const std::vector<int>& sector_batch, const double* theta,
-                   const std::vector<SplitBlock>& blocks, DeviceBuffer& d_blocks, cudaStream_t st) {
+                   const std::vector<SplitBlock>& blocks, DeviceBuffer& d_blocks, cudaStream_t st, double* dst) {
     int64_t wsize = 0;
     for (const auto& p : svd.probs) wsize += (int64_t)p.rows * p.cols;
-    if (wsize) DMRG_CUDA_TRY(cudaMemsetAsync(svd.d_w.ptr, 0, wsize * sizeof(double), st));
+    double* W = dst ? dst : svd.d_w.as<double>();
+    if (wsize) DMRG_CUDA_TRY(cudaMemsetAsync(W, 0, wsize * sizeof(double), st));
     std::vector<SplitBlock> active;
     for (const SplitBlock& b : blocks)
         if (sector_batch[b.sector] >= 0 && b.rows > 0 && b.cols > 0) active.push_back(b);
@@ -92,14 +110,15 @@ int twosite_gather(BatchedSvd& svd, const std::vector<int>& sector_batch, const 
     DMRG_TRY(upload(d_batch, sector_batch, st));
     DMRG_TRY(upload(d_blocks, active, st));
     DMRG_LAUNCH twosite_gather_kernel<<<(int)active.size(), 256, 0, st>>>(
-        theta, d_blocks.as<SplitBlock>(), d_batch.as<int>(), svd.d_probs.as<SvdProblem>(), svd.d_w.as<double>());
+        theta, d_blocks.as<SplitBlock>(), d_batch.as<int>(), svd.d_probs.as<SvdProblem>(), W);
     DMRG_CUDA_TRY(cudaGetLastError());
     DMRG_CUDA_TRY(cudaStreamSynchronize(st));  // d_batch is released on return
     return DMRG_OK;
 }
 
 int twosite_write(BatchedSvd& svd, const std::vector<int>& sector_batch, const std::vector<SplitWrite>& writes,
-                  DeviceBuffer& d_writes, double* left, double* right, bool s_left, cudaStream_t st) {
+                  DeviceBuffer& d_writes, double* left, double* right, bool s_left, cudaStream_t st,
+                  const double* K, const double* P) {
     std::vector<SplitWrite> active;
     for (const SplitWrite& t : writes)
         if (t.rows > 0 && t.cols > 0) {
@@ -109,6 +128,8 @@ int twosite_write(BatchedSvd& svd, const std::vector<int>& sector_batch, const s
             const int span = t.part == 0 ? t.off + t.rows : t.off + t.cols;
             if (kept > std::min(p.m, p.n) || span > (t.part == 0 ? p.m : p.n))
                 return set_error(DMRG_E_ARG, "two-site write outside its sector's factors");
+            if ((t.k_off >= 0 && !K) || (t.p_off >= 0 && !P))
+                return set_error(DMRG_E_ARG, "two-site write from a missing orthonormalised factor");
             active.push_back(t);
         }
     if (active.empty()) return DMRG_OK;
@@ -118,7 +139,7 @@ int twosite_write(BatchedSvd& svd, const std::vector<int>& sector_batch, const s
     DMRG_LAUNCH twosite_write_kernel<<<(int)active.size(), 256, 0, st>>>(
         d_writes.as<SplitWrite>(), d_batch.as<int>(), svd.d_probs.as<SvdProblem>(), svd.d_w.as<double>(),
         svd.d_q.as<double>(), svd.d_s.as<double>(), svd.d_perm.as<int>(), svd.d_sign.as<double>(), left, right,
-        s_left ? 1 : 0);
+        s_left ? 1 : 0, K, P);
     DMRG_CUDA_TRY(cudaGetLastError());
     DMRG_CUDA_TRY(cudaStreamSynchronize(st));
     return DMRG_OK;

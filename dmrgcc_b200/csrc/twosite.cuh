@@ -11,6 +11,10 @@
 //   right to left:  K_j(k, c) = U S rows of k,      K_{j+1}(c, l) = V^T columns of l.
 // The reference has no two-site mode (its sweep is single-site with subspace
 // expansion, real_tensor_rundmrg.cc:145-214); this is the engine's own.
+// The factor that stays canonical (U left to right, V^T right to left) is
+// orthonormal to rounding: where the Jacobi SVD leaves it as normalised
+// working-matrix columns it is orthonormalised (KetOrtho) and the other factor
+// is the projection of M_c on it (K^T M_c, or M_c K).
 #pragma once
 
 #include <vector>
@@ -32,17 +36,24 @@ struct SplitWrite {   // a block of a new site tensor
     int sector;
     int off;          // part 0: first row of the block in M_c; part 1: first column
     int part;         // 0: left factor (rows of U), 1: right factor (columns of V^T)
+    int64_t k_off;    // >= 0: the canonical factor's orthonormalised columns (column-major, ld = W rows)
+    int64_t p_off;    // >= 0: the other factor as a projection, row-major (t x n_c, or m_c x t)
 };
 
-// Fills the batch's working matrices from Theta (zeroing them first).
+// Fills the batch's working matrices from Theta (zeroing them first); with
+// `dst`, a buffer of the same layout instead.
 int twosite_gather(BatchedSvd& svd, const std::vector<int>& sector_batch, const double* theta,
-                   const std::vector<SplitBlock>& blocks, DeviceBuffer& d_blocks, cudaStream_t st);
+                   const std::vector<SplitBlock>& blocks, DeviceBuffer& d_blocks, cudaStream_t st,
+                   double* dst = nullptr);
 
 // Writes the new site tensors: left factor blocks into `left`, right factor
 // blocks into `right`; `s_left` puts the singular values into the left factor
 // (right-to-left sweep) instead of the right one.
+// K: the orthonormalised columns (writes with k_off >= 0), P: the projected
+// factors (writes with p_off >= 0).
 int twosite_write(BatchedSvd& svd, const std::vector<int>& sector_batch, const std::vector<SplitWrite>& writes,
-                  DeviceBuffer& d_writes, double* left, double* right, bool s_left, cudaStream_t st);
+                  DeviceBuffer& d_writes, double* left, double* right, bool s_left, cudaStream_t st,
+                  const double* K = nullptr, const double* P = nullptr);
 
 // Global truncation of the two-site split: every singular value above canpre
 // (canpre > 1: none), and of those the max_dim largest when max_dim > 0
