@@ -66,6 +66,25 @@ def profiled_traffic() -> dict | None:
     return None
 
 
+def max_over_ranks(x: float, dist=None, device: str = "cuda") -> float:
+    """The maximum of `x` over every rank of the default process group (`dist`
+    is torch.distributed, or None for a single process, which returns `x`).
+    Every rank must call it at the same point: it is one all-reduce."""
+    if dist is None:
+        return float(x)
+    import torch
+
+    t = torch.tensor([float(x)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_tflops(world: int, flop_per_step: float, steps: int, max_ms: float) -> float:
+    """Whole-job throughput of `world` replicas that each ran `steps` steps of
+    `flop_per_step`, timed as the slowest rank's `max_ms`."""
+    return world * flop_per_step * steps / (max_ms * 1e-3) * 1e-12
+
+
 def peaks() -> dict:
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -485,13 +504,9 @@ def run_b200(args) -> None:
     if dist:
         dist.barrier()
     step_ms = [e0.elapsed_time(e1) for e0, e1 in evs]
-    total_ms = sum(step_ms)
-    if dist:
-        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(sum(step_ms), dist)
     ms_per_step = total_ms / args.steps
-    value = world * alg_flops * args.steps / (total_ms * 1e-3) * 1e-12
+    value = whole_job_tflops(world, alg_flops, args.steps, total_ms)
 
     # per-launch durations (stage A: K*R products, stage B: L*(KR) sums), L2 flushed
     prof = []
@@ -517,12 +532,8 @@ def run_b200(args) -> None:
         capi.check(lib.dmrg_heff_apply_host(heff.h, h_psi.data_ptr(), h_out.data_ptr(), 0), "apply_host")
     e1.record(stream)
     torch.cuda.synchronize()
-    e2e_ms = e0.elapsed_time(e1)
-    if dist:
-        t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e_value = world * alg_flops * args.steps / (e2e_ms * 1e-3) * 1e-12
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1), dist)
+    e2e_value = whole_job_tflops(world, alg_flops, args.steps, e2e_ms)
 
     if rank == 0:
         traffic = profiled_traffic()

@@ -12,9 +12,11 @@
 // The device array exists once per GPU that loads the library and stays until
 // the process exits.  Every call reuses it and leaves the previous call's
 // contents behind (nothing in it needs to start at zero: the intermediate is
-// overwritten by the first launch).  Calls that overlap on the GPU (another
-// stream, another host thread) race on that array; the host staging area is
-// guarded by a mutex, so concurrent host threads serialise their set-up only.
+// overwritten by the first launch).  Calls that overlap on the GPU race on that
+// array.  This function itself keeps its calls apart: a mutex guards the host
+// staging area and is held until the call's own stream has finished the call's
+// work, so calls from different host threads run one after the other, device
+// work included; only work that reaches the array by other means can overlap.
 // The first call on a device looks up the array's device address
 // (cudaGetSymbolAddress) with that device current; make that first call before
 // any stream capture.  The address is kept for the life of the process, so the

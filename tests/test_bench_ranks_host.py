@@ -1,0 +1,77 @@
+"""The multi-rank path of bench.py on CPU: two `gloo` ranks on 127.0.0.1.
+
+`bench.py --gpus N` runs N replicas (one process per GPU, no collective on the
+data path); its only collectives are the barriers and the max-over-ranks of the
+timed totals, after which `value` is all ranks' work over the slowest rank's
+time.  These tests run that reduction and the throughput formula in two
+processes, and check that the reference arm does no work on ranks other than 0."""
+import contextlib
+import io
+import os
+import socket
+import sys
+
+import pytest
+import torch.multiprocessing as mp
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _free_port() -> int:
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank_main(rank: int, world: int, port: int) -> None:
+    import datetime
+
+    import torch.distributed as dist
+
+    sys.path.insert(0, ROOT)
+    import bench
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        local_ms = [120.0, 80.0][rank]  # rank 0 is the slower replica
+        dist.barrier()
+        total = bench.max_over_ranks(local_ms, dist, "cpu")
+        assert total == 120.0, total
+        e2e = bench.max_over_ranks([3.0, 5.0][rank], dist, "cpu")
+        assert e2e == 5.0, e2e
+        # 2 replicas x 10 steps x 3.6e9 FLOP in 120 ms
+        v = bench.whole_job_tflops(world, 3.6e9, 10, total)
+        assert abs(v - 2 * 10 * 3.6e9 / 0.120 * 1e-12) < 1e-12, v
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_max_over_ranks_and_whole_job_value_two_gloo_ranks():
+    mp.start_processes(_rank_main, args=(2, _free_port()), nprocs=2, join=True, start_method="spawn")
+
+
+def test_single_process_reduction_is_identity():
+    sys.path.insert(0, ROOT)
+    import bench
+
+    assert bench.max_over_ranks(7.5) == 7.5
+    assert bench.whole_job_tflops(1, 1e12, 1, 1000.0) == pytest.approx(1.0)
+
+
+def test_reference_arm_does_nothing_on_other_ranks(monkeypatch):
+    """Under torchrun only rank 0 times the reference's CPU path and prints its
+    line; every other rank returns at once, printing nothing."""
+    import argparse
+
+    sys.path.insert(0, ROOT)
+    import bench
+
+    monkeypatch.setenv("RANK", "1")
+    called = []
+    monkeypatch.setattr(bench, "cpu_reference", lambda *a, **k: called.append(a) or {})
+    buf = io.StringIO()
+    with contextlib.redirect_stdout(buf):
+        bench.run_reference(argparse.Namespace(steps=3, warmup=3, gpus=2))
+    assert buf.getvalue() == "" and not called
