@@ -294,7 +294,7 @@ def reference_sweep_sample(ctx, threads: int) -> dict:
 
 
 def scan_form(threads: int) -> dict:
-    """The batched U/t scan (BASELINE configuration 5: 64 seeded open chains, L in
+    """The batched U/t scan (64 seeded open chains, L in
     {12..32}, U/t in [1, 20], d=4, unit filling, D<=128, 6 sweeps): all 64 runs
     side by side on this GPU (dmrg_run_execute_many, one context and stream per
     instance), in FP64 and with TF32X3 matvecs; aggregate sweeps per second,
@@ -397,8 +397,8 @@ CPLX_REFERENCE = os.path.join(ROOT, "tests", "golden", "hofstadter6x6_reference.
 
 
 def complex_form(ctx, threads: int) -> dict:
-    """The complex path on the Hofstadter geometry of configuration 3 (6x6,
-    periodic in y, flux 1/6, U=10, d=3; 4 bosons, D ramp 32 -> 256, 5 sweeps;
+    """The complex path on the 6x6 Hofstadter geometry (periodic in y, flux
+    1/6, U=10, d=3; 4 bosons, D ramp 32 -> 256, 5 sweeps;
     hofstadter6x6.in): the whole complex run (dmrg_run_execute, every tensor
     complex), its final energy against the reference's on the same input
     (tests/golden/hofstadter6x6_reference.txt, 1 BLAS thread), and the

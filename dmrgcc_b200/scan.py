@@ -1,6 +1,6 @@
 """The batched U/t scan: many independent Bose-Hubbard chains run side by side.
 
-The workload (BASELINE configuration 5) is 64 open chains of the reference's
+The workload is 64 open chains of the reference's
 real spinless Bose-Hubbard model, drawn with numpy's default_rng(0): length L
 uniform in {12, 16, 20, 24, 28, 32}, U/t uniform in [1, 20], n_max = 3 (d = 4),
 unit filling (N = L), bond dimension up to 128, 6 sweeps.  Each instance is an

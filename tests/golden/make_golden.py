@@ -261,7 +261,7 @@ def converged_reference() -> None:
 def complex_run_reference() -> None:
     """hofstadter6x6_reference.txt: the reference's final energy on
     hofstadter6x6.in (complex_spinful_bose_square_model, 1 BLAS thread): the
-    Hofstadter geometry of configuration 3 with 4 bosons (the reference's model
+    6x6 Hofstadter geometry (flux 1/6, periodic in y) with 4 bosons (the reference's model
     crashes on this lattice with 5 or 6 bosons)."""
     tmp = tempfile.mkdtemp(prefix="golden_h66_")
     env = dict(os.environ, OMP_NUM_THREADS="1", OPENBLAS_NUM_THREADS="1")

@@ -50,7 +50,7 @@ def test_complex_path_on_a_real_model_matches_the_real_path(ctx, tmp_path):
 
 
 def test_hofstadter_6x6_matches_the_reference_run(ctx):
-    """The Hofstadter geometry of configuration 3 (6x6, periodic in y, flux
+    """The 6x6 Hofstadter geometry (periodic in y, flux
     1/6, 4 bosons, D <= 256; hofstadter6x6.in): the final energy within 1e-10
     per lattice site of the reference's run of the same input
     (tests/golden/hofstadter6x6_reference.txt)."""

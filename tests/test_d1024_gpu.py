@@ -1,5 +1,5 @@
 """Config-scale parity: environment updates, canonicalisations and a Lanczos
-solve at bond dimension 1024 on the 8x4 cylinder,
+solve at bond dimension 1024 on the 8x4 cylinder (d=5, N=16, U=8),
 against the reference's own outputs (tests/golden/make_golden.py --d1024).
 
 * Environment updates (left at site 4, right at site 27) and canonicalisations

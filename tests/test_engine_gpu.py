@@ -169,7 +169,7 @@ def test_gauge_spread_check_rejects_an_energy_outside_it(tmp_path):
 
 @pytest.mark.gpu
 def test_cylinder8x4_D1024_final_energy_within_reference_spread(ctx):
-    """Config 2 (8x4 cylinder, D 128 -> 1024, 8 sweeps) end to end on the device:
+    """The 8x4 cylinder (D 128 -> 1024, 8 sweeps) end to end on the device:
     the final energy lies within the reference's own gauge spread (stock,
     pinned and random-sign runs of the reference on the same input), widened by
     1e-10 per site, and the sites visited match the stock run's."""

@@ -45,8 +45,8 @@ def test_mpo_and_quantum_tables_bit_exact(inp, gold):
 def test_spinful_mpo_and_quantum_tables_bit_exact(name):
     """The spinful U(1) x U(1) model (species on alternating MPS sites): MPO and
     quantum tables bit-identical to the reference's ComplexSpinfulBoseSquare
-    classes at zero flux (oracle/_ref/probe_model); 4x4 open is BASELINE
-    configuration 4, 3x3 periodic in y exercises the wrap-around terms."""
+    classes at zero flux (oracle/_ref/probe_model); the 4x4 open lattice is
+    the spinful benchmark geometry, 3x3 periodic in y exercises the wrap-around terms."""
     ref = read_nac(os.path.join(GOLD, f"model_{name}.nac"))
     m = capi.Model(os.path.join(ROOT, "dmrgcc_b200", "inputs", f"{name}.in"), "real_spinful_bose_square")
     n = int(ref["num_site"][0])
