@@ -4,6 +4,7 @@
 #include <atomic>
 #include <cmath>
 #include <cstring>
+#include <initializer_list>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -25,6 +26,19 @@ struct ModelSpec {
     std::unique_ptr<MpoHamiltonian> ham;
 };
 
+// The lattice and filling a model can be built for.  The reference takes these
+// keys as given; outside these ranges its quantum-number tables come out empty
+// or inconsistent, so the library rejects them before building anything.
+void check_sizes(int nx, int ny, int d, std::initializer_list<int> bosons) {
+    if (nx < 1 || ny < 1) throw std::runtime_error("num_site_x and num_site_y must be at least 1");
+    if (d < 2) throw std::runtime_error("physics_dim must be at least 2 (n_max = physics_dim - 1 >= 1)");
+    const long long cap = (long long)(d - 1) * nx * ny;
+    for (int n : bosons)
+        if (n < 0 || n > cap)
+            throw std::runtime_error("boson number " + std::to_string(n) + " outside [0, (physics_dim - 1) * sites = " +
+                                     std::to_string(cap) + "]");
+}
+
 // The model executables' main() (model/real_spinless_bose_square_model.cc:11-35):
 // read the model keys and build the space and the Hamiltonian.
 ModelSpec make_model(InputGroup& input, const std::string& model) {
@@ -43,6 +57,7 @@ ModelSpec make_model(InputGroup& input, const std::string& model) {
         const double jy = input.getDouble("Jy");
         const double mu = input.getDouble("mu");
         const double u[3] = {input.getDouble("U_uu"), input.getDouble("U_dd"), input.getDouble("U_ud")};
+        check_sizes(nx, ny, d, {nb[0], nb[1]});
         m.space.reset(new RealSpinfulBoseSquareSpace(nx, ny, nb, d));
         if (model == "complex_spinful_bose_square")
             m.ham.reset(new ComplexSpinfulBoseSquareHamiltonian(nx, ny, d, flux, jx, jy, u, mu, px, py));
@@ -65,6 +80,7 @@ ModelSpec make_model(InputGroup& input, const std::string& model) {
     const double mu = input.getDouble("mu");
     const bool px = input.getBool("period_x");
     const bool py = input.getBool("period_y");
+    check_sizes(nx, ny, d, {nb});
     m.space.reset(new RealSpinlessBoseSquareSpace(nx, ny, nb, d));
     m.ham.reset(new RealSpinlessBoseSquareHamiltonian(nx, ny, d, flux * 3.14159265358979323846, jx, jy, u, mu, px, py));
     return m;
@@ -259,6 +275,7 @@ int dmrg_model_is_complex(dmrg_model_t m, int* is_complex) {
 
 int dmrg_model_quantum_table(dmrg_model_t m, int which, int bond, int cap, int* values, int* rows) {
     if (!m || !rows) return set_error(DMRG_E_ARG, "null argument");
+    if (which != 0 && which != 1) return set_error(DMRG_E_ARG, "which must be 0 (MPS bonds) or 1 (MPO bonds)");
     if (bond < 0 || bond > m->spec.space->num_site()) return set_error(DMRG_E_ARG, "bond out of range");
     const auto& t = which == 0 ? m->spec.space->table(bond) : m->spec.ham->quantum_table(bond);
     *rows = (int)t.size();

@@ -400,7 +400,14 @@ int dmrg_run_phases(dmrg_run_t r, int cap, double* seconds, int* svd_sweeps, int
  * The MPO of RealSpinlessBoseSquareHamiltonian::DefineTensorHamiltonian
  * (model/hamiltonian/real_spinless_bose_square_hamiltonian.cc:171-228) and the
  * quantum tables (which 0: MPS bonds, RealTensorSpace; 1: MPO bonds,
- * RealTensorHamiltonian), built from an input file without a GPU. */
+ * RealTensorHamiltonian), built from an input file without a GPU.
+ * dmrg_model_create returns DMRG_E_ARG, with the reason, for a missing or
+ * malformed input file (the reference prints and exits), an unknown model, and
+ * sizes no model can be built for: num_site_x or num_site_y below 1,
+ * physics_dim below 2, or a boson number outside [0, (physics_dim - 1) * sites].
+ * The array outputs take a capacity `cap` and receive at most cap values; the
+ * sizes (*left_bond, *right_bond, *rows) are always set, so a call with cap 0
+ * returns them.  which: 0 or 1. */
 int dmrg_model_create(const char* input_path, const char* model, dmrg_model_t* out);
 int dmrg_model_destroy(dmrg_model_t m);
 int dmrg_model_info(dmrg_model_t m, int* num_site, int* physics_dim, int* num_quantum);
