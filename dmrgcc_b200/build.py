@@ -3,7 +3,8 @@
     python -m dmrgcc_b200.build [--force] [--jobs N]
 
 Every translation unit under csrc/ is compiled in-tree into dmrgcc_b200/lib/
-(object files in dmrgcc_b200/lib/obj/), then linked into one shared library.
+(object files in dmrgcc_b200/lib/obj/), then linked into one shared library;
+the reference's model executables (csrc/apps/) are linked against it beside it.
 A unit is recompiled when it, or any header under csrc/ or include/, is newer
 than its object file.
 """
@@ -88,7 +89,32 @@ def build(force: bool = False, jobs: int | None = None, verbose: bool = False) -
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
+    build_apps(force)
     return LIB
+
+
+# The reference's model executables (csrc/apps/model_main.cc), one per model,
+# linked against the library next to them.
+APPS = {"real_spinless_bose_square_model": "real_spinless_bose_square",
+        "complex_spinful_bose_square_model": "complex_spinful_bose_square",
+        "real_spinful_bose_square_model": "real_spinful_bose_square"}
+
+
+def build_apps(force: bool = False) -> list[str]:
+    src = os.path.join(CSRC, "apps", "model_main.cc")
+    deps = [src, LIB, os.path.join(INCLUDE, "dmrg_b200.h"), os.path.join(INCLUDE, "dmrg_b200.hpp")]
+    newest = max(os.path.getmtime(d) for d in deps)
+    out = []
+    for exe, model in APPS.items():
+        path = os.path.join(LIBDIR, exe)
+        if force or not os.path.exists(path) or os.path.getmtime(path) < newest:
+            cmd = [cxx(), "-std=c++17", "-O2", "-Wall", "-Wextra", f'-DDMRG_MODEL="{model}"', "-I", INCLUDE, src,
+                   "-L", LIBDIR, "-ldmrg_b200", "-Wl,-rpath,$ORIGIN", "-o", path]
+            r = subprocess.run(cmd, capture_output=True, text=True)
+            if r.returncode != 0:
+                raise RuntimeError(f"build of {exe} failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
+        out.append(path)
+    return out
 
 
 def main() -> int:

@@ -110,6 +110,7 @@ _SIGS = {
     "dmrg_truncate_dims": (C.c_int, [C.c_int, _I, _D, C.c_int, C.c_double, _I]),
     "dmrg_rand_stream": (C.c_int, [C.c_uint, C.c_int, _I]),
     "dmrg_run_create": (C.c_int, [_VP, C.c_char_p, C.c_char_p, _VP, C.POINTER(_VP)]),
+    "dmrg_run_options_from_input": (C.c_int, [C.c_char_p, _VP]),
     "dmrg_run_execute": (C.c_int, [_VP]),
     "dmrg_run_execute_many": (C.c_int, [C.POINTER(_VP), C.c_int, C.c_int, _I]),
     "dmrg_run_destroy": (C.c_int, [_VP]),
@@ -584,6 +585,14 @@ class RunOptions(C.Structure):
     _fields_ = [("precision", C.c_int), ("verbose", C.c_int), ("seed", C.c_uint),
                 ("stop_after_half_sweeps", C.c_int), ("lanczos_precision", C.c_double), ("two_site", C.c_int),
                 ("lanczos_graph", C.c_int)]
+
+
+def run_options_from_input(input_path: str) -> RunOptions:
+    """The options an input file's optional keys ask for (precision, mode, seed,
+    lanczos_tol, lanczos_graph); host only."""
+    o = RunOptions()
+    check(lib().dmrg_run_options_from_input(input_path.encode(), C.byref(o)), "dmrg_run_options_from_input")
+    return o
 
 
 class Run:

@@ -225,6 +225,42 @@ int dmrg_run_phases(dmrg_run_t r, int cap, double* seconds, int* svd_sweeps, int
     return DMRG_OK;
 }
 
+int dmrg_run_options_from_input(const char* input_path, dmrg_run_options_t* opt) {
+    if (!input_path || !opt) return set_error(DMRG_E_ARG, "null argument");
+    try {
+        InputGroup input(input_path, "input", false);
+        dmrg_run_options_t o{};
+        o.precision = DMRG_PREC_FP64;
+        o.verbose = 1;
+        o.seed = 1;
+        o.stop_after_half_sweeps = -1;
+        o.lanczos_precision = 0.0;
+        o.two_site = 0;
+        o.lanczos_graph = 0;
+        const std::string prec = input.getString("precision", "");
+        if (prec == "tf32x3") o.precision = DMRG_PREC_TF32X3;
+        else if (prec == "bf16x3") o.precision = DMRG_PREC_BF16X3;
+        else if (!prec.empty() && prec != "fp64")
+            throw std::runtime_error("precision = " + prec + ": fp64, tf32x3 or bf16x3");
+        const std::string mode = input.getString("mode", "");
+        if (mode == "twosite") o.two_site = 1;
+        else if (!mode.empty() && mode != "onesite") throw std::runtime_error("mode = " + mode + ": onesite or twosite");
+        const int seed = input.getInt("seed", 1);
+        if (seed < 0) throw std::runtime_error("seed = " + std::to_string(seed) + ": must be >= 0");
+        o.seed = (unsigned)seed;
+        const double tol = input.getDouble("lanczos_tol", 0.0);
+        if (!(tol >= 0.0) || !std::isfinite(tol)) throw std::runtime_error("lanczos_tol must be >= 0");
+        o.lanczos_precision = tol;
+        const int graph = input.getInt("lanczos_graph", 0);
+        if (graph < -1 || graph > 1) throw std::runtime_error("lanczos_graph must be -1, 0 or 1");
+        o.lanczos_graph = graph;
+        *opt = o;
+        return DMRG_OK;
+    } catch (const std::exception& e) {
+        return set_error(DMRG_E_ARG, "%s", e.what());
+    }
+}
+
 int dmrg_model_create(const char* input_path, const char* model, dmrg_model_t* out) {
     if (!input_path || !out) return set_error(DMRG_E_ARG, "null argument");
     *out = nullptr;

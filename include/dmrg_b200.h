@@ -368,6 +368,15 @@ typedef struct {
                                    launch in dmrg_run_execute_many); 1: graphs
                                    always; -1: never */
 } dmrg_run_options_t;
+/* The run options an input file asks for (host only, no GPU needed): the
+ * defaults (FP64, verbose 1, seed 1, every half-sweep, the reference's Lanczos
+ * tolerance, single-site, default graph use), changed by the optional keys of
+ * the file's input group: precision = fp64 | tf32x3 | bf16x3, mode = onesite |
+ * twosite, seed = <int >= 0>, lanczos_tol = <double >= 0, 0 = 1e-15>,
+ * lanczos_graph = -1 | 0 | 1.  The reference reads none of these keys, so its
+ * own input files give its behaviour.  DMRG_E_ARG for an unreadable file or a
+ * value outside these sets. */
+int dmrg_run_options_from_input(const char* input_path, dmrg_run_options_t* opt);
 int dmrg_run_create(dmrg_ctx_t ctx, const char* input_path, const char* model,
                     const dmrg_run_options_t* opt, dmrg_run_t* out);
 int dmrg_run_execute(dmrg_run_t r);
