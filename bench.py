@@ -211,6 +211,19 @@ def split_form(ctx, step, psi, L, R, out_ref, steps: int, flush, stream, prec: i
                       % ("f16 on bf16" if name == "bf16x3" else "tf32")}
 
 
+def truncation_summary(run) -> dict:
+    """The discarded weight (sum of dropped sigma^2) summed over a run's
+    truncations, and over those of its last sweep, from dmrg_run_steps."""
+    try:
+        st = run.steps()
+        hs = st["half_sweep"]
+        last = hs >= (hs.max() - 1) if len(hs) else hs
+        return {"discarded_weight_total": float(st["discarded"].sum()),
+                "discarded_weight_last_sweep": float(st["discarded"][last].sum())}
+    except Exception as e:  # a summary must not cost the bench line
+        return {"discarded_weight_total": None, "error": str(e)[:200]}
+
+
 def sweep_time(ctx, precision: int = 0, name: str = "fp64") -> dict:
     """One whole run of the 8x4 cylinder input (D ramp 128 -> 1024, 8 sweeps =
     16 half-sweeps, niter 100, noise on for the first 12 half-sweeps), wall
@@ -231,6 +244,7 @@ def sweep_time(ctx, precision: int = 0, name: str = "fp64") -> dict:
         "per_sweep_s": [float(s[2 * i] + s[2 * i + 1]) for i in range(len(s) // 2)],
         "phase_s": {k: float(v) for k, v in zip(capi.Run.PHASES, ph.sum(axis=0))},
         "svd_sweeps": int(sw.sum()), "final_energy": float(e[-1]),
+        "truncation": truncation_summary(run),
     }
     run.close()
     return out
@@ -360,7 +374,10 @@ def sweep_pair(ctx) -> dict:
     fp64["split"] = {"precision": "tf32x3", "total_s": split["total_s"], "per_sweep_s": split["per_sweep_s"],
                      "phase_s": split["phase_s"], "final_energy": split["final_energy"],
                      "speedup_vs_fp64": fp64["total_s"] / split["total_s"],
-                     "abs_dE_per_site_vs_fp64": abs(split["final_energy"] - fp64["final_energy"]) / 32.0}
+                     "abs_dE_per_site_vs_fp64": abs(split["final_energy"] - fp64["final_energy"]) / 32.0,
+                     "truncation": split["truncation"]}
+    a, b = fp64["truncation"].get("discarded_weight_total"), split["truncation"].get("discarded_weight_total")
+    fp64["split"]["discarded_weight_delta_vs_fp64"] = (b - a) if a is not None and b is not None else None
     return fp64
 
 
@@ -381,7 +398,8 @@ def two_site_form(ctx) -> dict:
         ph, sw = run.phases()
         res[name] = {"total_s": total, "per_sweep_s": [float(s[2 * i] + s[2 * i + 1]) for i in range(len(s) // 2)],
                      "phase_s": {k: float(v) for k, v in zip(capi.Run.PHASES, ph.sum(axis=0))},
-                     "svd_sweeps": int(sw.sum()), "final_energy": float(e[-1])}
+                     "svd_sweeps": int(sw.sum()), "final_energy": float(e[-1]),
+                     "truncation": truncation_summary(run)}
         run.close()
     out = {"workload": "two-site DMRG, 8x4 Bose-Hubbard cylinder (d=5, N=16, U=8), D 128->1024, 8 sweeps"}
     out.update(res)

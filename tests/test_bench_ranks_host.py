@@ -4,7 +4,8 @@
 data path); its only collectives are the barriers and the max-over-ranks of the
 timed totals, after which `value` is all ranks' work over the slowest rank's
 time.  These tests run that reduction and the throughput formula in two
-processes, and check that the reference arm does no work on ranks other than 0."""
+processes, and check that the reference arm does no work on ranks other than 0.
+The last test covers the bench's truncation summary of a run's step records."""
 import contextlib
 import io
 import os
@@ -75,3 +76,28 @@ def test_reference_arm_does_nothing_on_other_ranks(monkeypatch):
     with contextlib.redirect_stdout(buf):
         bench.run_reference(argparse.Namespace(steps=3, warmup=3, gpus=2))
     assert buf.getvalue() == "" and not called
+
+
+def test_truncation_summary_of_a_run_record():
+    """The bench's truncation figures from a run's step records (the arrays that
+    dmrg_run_steps returns): the total discarded weight and that of the last
+    sweep (its two half-sweeps)."""
+    import numpy as np
+
+    sys.path.insert(0, ROOT)
+    import bench
+
+    class _Run:
+        def steps(self):
+            return {"half_sweep": np.array([0, 0, 1, 1, 2, 2, 3, 3], np.int32),
+                    "discarded": np.array([1e-3, 2e-3, 1e-4, 1e-4, 1e-6, 2e-6, 3e-7, 4e-7])}
+
+    t = bench.truncation_summary(_Run())
+    assert t["discarded_weight_total"] == pytest.approx(3.2037e-3)
+    assert t["discarded_weight_last_sweep"] == pytest.approx(3.7e-6)
+
+    class _Broken:
+        def steps(self):
+            raise RuntimeError("no records")
+
+    assert bench.truncation_summary(_Broken())["discarded_weight_total"] is None
