@@ -96,6 +96,7 @@ def build(force: bool = False, jobs: int | None = None, verbose: bool = False) -
 # The reference's model executables (csrc/apps/model_main.cc), one per model,
 # linked against the library next to them.
 APPS = {"real_spinless_bose_square_model": "real_spinless_bose_square",
+        "complex_spinless_bose_square_model": "complex_spinless_bose_square",
         "complex_spinful_bose_square_model": "complex_spinful_bose_square",
         "real_spinful_bose_square_model": "real_spinful_bose_square"}
 

@@ -1,5 +1,6 @@
 // The reference's model executables, run on the GPU:
 //   real_spinless_bose_square_model <input file>   (model/real_spinless_bose_square_model.cc)
+//   complex_spinless_bose_square_model <input file> (model/complex_spinless_bose_square_model.cc)
 //   complex_spinful_bose_square_model <input file> (model/complex_spinful_bose_square_model.cc)
 //   real_spinful_bose_square_model <input file>    (the spinful model on real tensors; flux 0)
 // Same argument, same input file, the same printed lines (the Got/Def echo of

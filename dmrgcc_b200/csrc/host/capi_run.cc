@@ -65,10 +65,13 @@ ModelSpec make_model(InputGroup& input, const std::string& model) {
             m.ham.reset(new RealSpinfulBoseSquareHamiltonian(nx, ny, d, flux, jx, jy, u, mu, px, py));
         return m;
     }
-    if (model != "real_spinless_bose_square")
+    if (model != "real_spinless_bose_square" && model != "complex_spinless_bose_square")
         throw std::runtime_error("unknown model '" + model +
-                                 "' (supported: real_spinless_bose_square, real_spinful_bose_square, "
-                                 "complex_spinful_bose_square)");
+                                 "' (supported: real_spinless_bose_square, complex_spinless_bose_square, "
+                                 "real_spinful_bose_square, complex_spinful_bose_square)");
+    // model/real_spinless_bose_square_model.cc:11-42, or its complex twin
+    // model/complex_spinless_bose_square_model.cc (same keys, same space; the
+    // Hamiltonian's operators complex, so the run is ComplexTensorRundmrg's)
     const int nx = input.getInt("num_site_x");
     const int ny = input.getInt("num_site_y");
     const int nb = input.getInt("num_boson");
@@ -82,7 +85,11 @@ ModelSpec make_model(InputGroup& input, const std::string& model) {
     const bool py = input.getBool("period_y");
     check_sizes(nx, ny, d, {nb});
     m.space.reset(new RealSpinlessBoseSquareSpace(nx, ny, nb, d));
-    m.ham.reset(new RealSpinlessBoseSquareHamiltonian(nx, ny, d, flux * 3.14159265358979323846, jx, jy, u, mu, px, py));
+    const double flux_value = flux * 3.14159265358979323846;
+    if (model == "complex_spinless_bose_square")
+        m.ham.reset(new ComplexSpinlessBoseSquareHamiltonian(nx, ny, d, flux_value, jx, jy, u, mu, px, py));
+    else
+        m.ham.reset(new RealSpinlessBoseSquareHamiltonian(nx, ny, d, flux_value, jx, jy, u, mu, px, py));
     return m;
 }
 

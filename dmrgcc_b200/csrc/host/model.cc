@@ -291,28 +291,31 @@ template class TensorOperatorT<Cplx>;
 template class TensorHamiltonianT<double>;
 template class TensorHamiltonianT<Cplx>;
 
-RealSpinlessBoseSquareHamiltonian::RealSpinlessBoseSquareHamiltonian(int nx, int ny, int d, double flux_value,
-                                                                     double hop_x, double hop_y, double inter,
-                                                                     double chem, bool px, bool py)
+template <class T>
+SpinlessBoseSquareHamiltonianT<T>::SpinlessBoseSquareHamiltonianT(int nx, int ny, int d, double flux_value,
+                                                                  double hop_x, double hop_y, double inter,
+                                                                  double chem, bool px, bool py)
     : nx_(nx), ny_(ny), d_(d), hop_x_(hop_x), hop_y_(hop_y), inter_(inter), chem_(chem), px_(px), py_(py) {
-    (void)flux_value;  // stored but unused by the real spinless model (as in the reference)
-    init(nx * ny, d, 1);
+    (void)flux_value;  // stored but unused by both spinless models (as in the reference)
+    this->init(nx * ny, d, 1);
     // 0 = I, 1 = b+, 2 = b, 3 = n, 4 = mu n + U n(n-1)
-    basic_.assign(5, HostMatrix(d, d));
+    auto& basic = this->basic_;
+    basic.assign(5, HostMatrixT<T>(d, d));
     for (int i = 0; i < d; ++i) {
-        basic_[0].at(i, i) = 1.0;
-        basic_[3].at(i, i) = i;
-        basic_[4].at(i, i) = chem * i + inter * i * (i - 1);
+        basic[0].at(i, i) = T(1.0);
+        basic[3].at(i, i) = T((double)i);
+        basic[4].at(i, i) = T(chem * i + inter * i * (i - 1));
     }
     for (int i = 1; i < d; ++i) {
-        basic_[1].at(i, i - 1) = std::sqrt((double)i);
-        basic_[2].at(i - 1, i) = std::sqrt((double)i);
+        basic[1].at(i, i - 1) = T(std::sqrt((double)i));
+        basic[2].at(i - 1, i) = T(std::sqrt((double)i));
     }
 }
 
-void RealSpinlessBoseSquareHamiltonian::DefineHamiltonian1(int p1, int p2, double coeff) {
+template <class T>
+void SpinlessBoseSquareHamiltonianT<T>::DefineHamiltonian1(int p1, int p2, double coeff) {
     if (p1 >= p2) throw std::runtime_error("position1 >= position2 in DefineHamiltonian1");
-    for (int i = 0; i < num_site_; ++i) {
+    for (int i = 0; i < this->num_site_; ++i) {
         int op = 0, q = 0;
         double c = 1.0;
         if (i == p1) {
@@ -325,13 +328,14 @@ void RealSpinlessBoseSquareHamiltonian::DefineHamiltonian1(int p1, int p2, doubl
             c = coeff;
             q = 0;
         }
-        ExpanTensorHamiltonian(i, op, c, {q});
+        this->ExpanTensorHamiltonian(i, op, T(c), {q});
     }
 }
 
-void RealSpinlessBoseSquareHamiltonian::DefineHamiltonian2(int p1, int p2, double coeff) {
+template <class T>
+void SpinlessBoseSquareHamiltonianT<T>::DefineHamiltonian2(int p1, int p2, double coeff) {
     if (p1 >= p2) throw std::runtime_error("position1 >= position2 in DefineHamiltonian2");
-    for (int i = 0; i < num_site_; ++i) {
+    for (int i = 0; i < this->num_site_; ++i) {
         int op = 0, q = 0;
         double c = 1.0;
         if (i == p1) {
@@ -344,25 +348,29 @@ void RealSpinlessBoseSquareHamiltonian::DefineHamiltonian2(int p1, int p2, doubl
             c = coeff;
             q = 0;
         }
-        ExpanTensorHamiltonian(i, op, c, {q});
+        this->ExpanTensorHamiltonian(i, op, T(c), {q});
     }
 }
 
-void RealSpinlessBoseSquareHamiltonian::DefineHamiltonian3(int p, double coeff) {
-    for (int i = 0; i < num_site_; ++i) {
+template <class T>
+void SpinlessBoseSquareHamiltonianT<T>::DefineHamiltonian3(int p, double coeff) {
+    for (int i = 0; i < this->num_site_; ++i) {
         int op = 0;
         double c = 1.0;
         if (i == p) {
             op = 4;
             c = coeff;
         }
-        ExpanTensorHamiltonian(i, op, c, {0});
+        this->ExpanTensorHamiltonian(i, op, T(c), {0});
     }
 }
 
-void RealSpinlessBoseSquareHamiltonian::DefineTensorHamiltonian() {
-    qtab_[0] = {{0}};
-    qtab_[num_site_] = {{0}};
+template <class T>
+void SpinlessBoseSquareHamiltonianT<T>::DefineTensorHamiltonian() {
+    auto& qtab = this->qtab_;
+    const int ns = this->num_site_;
+    qtab[0] = {{0}};
+    qtab[ns] = {{0}};
     for (int i = 0; i < nx_; ++i)
         for (int j = 0; j < ny_; ++j) {
             const int p0 = j + i * ny_;  // column-major site order (p = j + i * Ny)
@@ -387,9 +395,12 @@ void RealSpinlessBoseSquareHamiltonian::DefineTensorHamiltonian() {
                 }
             }
             if (chem_ != 0 || inter_ != 0) DefineHamiltonian3(p0, 1.0);
-            ParallelTensorHamiltonian();
+            this->ParallelTensorHamiltonian();
         }
 }
+
+template class SpinlessBoseSquareHamiltonianT<double>;
+template class SpinlessBoseSquareHamiltonianT<Cplx>;
 
 // ---------------------------------------------------------------------------
 // Quantum tables of the MPS bonds

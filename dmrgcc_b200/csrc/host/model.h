@@ -135,10 +135,17 @@ protected:
 using RealTensorHamiltonian = TensorHamiltonianT<double>;
 using ComplexTensorHamiltonian = TensorHamiltonianT<Cplx>;
 
-class RealSpinlessBoseSquareHamiltonian : public RealTensorHamiltonian {
+// H = sum over bonds of J (b+_p b_p' + h.c.) + sum_i [mu n + U n(n-1)]:
+// RealSpinlessBoseSquareHamiltonian
+// (model/hamiltonian/real_spinless_bose_square_hamiltonian.cc) for T = double,
+// and ComplexSpinlessBoseSquareHamiltonian
+// (model/hamiltonian/complex_spinless_bose_square_hamiltonian.cc), the same
+// terms on complex operators, for T = Cplx.  Both store the flux and use none.
+template <class T>
+class SpinlessBoseSquareHamiltonianT : public TensorHamiltonianT<T> {
 public:
-    RealSpinlessBoseSquareHamiltonian(int nx, int ny, int physics_dim, double flux_value, double hop_x, double hop_y,
-                                      double inter_value, double chemical_value, bool period_x, bool period_y);
+    SpinlessBoseSquareHamiltonianT(int nx, int ny, int physics_dim, double flux_value, double hop_x, double hop_y,
+                                   double inter_value, double chemical_value, bool period_x, bool period_y);
     void DefineTensorHamiltonian() override;
 
 private:
@@ -149,6 +156,8 @@ private:
     double hop_x_, hop_y_, inter_, chem_;
     bool px_, py_;
 };
+using RealSpinlessBoseSquareHamiltonian = SpinlessBoseSquareHamiltonianT<double>;
+using ComplexSpinlessBoseSquareHamiltonian = SpinlessBoseSquareHamiltonianT<Cplx>;
 
 // Quantum-number tables of the MPS bonds (RealTensorSpace's quantum_table_ and
 // its model hooks, real_tensor_space.cc:716-736 and

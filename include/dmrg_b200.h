@@ -346,7 +346,9 @@ int dmrg_svd_set_max_sweeps(int sweeps);
  * the reference's implicit seed).  dmrg_run_execute replaces
  * RealTensorRundmrg::Run (:115-245): every site step (Lanczos, subspace
  * expansion, SVD truncation, environment update, merge) runs on the device.
- * model: "real_spinless_bose_square" (NULL = that). */
+ * model: "real_spinless_bose_square" (NULL = that), "complex_spinless_bose_square"
+ * (its complex twin, model/complex_spinless_bose_square_model.cc),
+ * "real_spinful_bose_square" or "complex_spinful_bose_square". */
 typedef struct {
     int precision;              /* DMRG_PREC_FP64, or DMRG_PREC_TF32X3: Lanczos
                                    matvecs first in split precision, then the

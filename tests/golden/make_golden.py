@@ -278,6 +278,26 @@ SPINFUL_MODELS = ("spinful4x4", "spinful3x3_periodic_y")
 COMPLEX_MODELS = ("hofstadter4x3",)
 
 
+COMPLEX_SPINLESS_MODELS = ("chain16_spinless", "cylinder3x3_spinless")
+
+
+def complex_spinless_fixtures() -> None:
+    """model_complex_<input>.nac: the MPO (real and imaginary parts) and the
+    quantum tables of the reference's complex spinless model
+    (ComplexSpinlessBoseSquareSpace / ComplexSpinlessBoseSquareHamiltonian,
+    oracle/_ref/probe_model ... spinless) on the spinless inputs."""
+    sys.path.insert(0, ROOT)
+    from oracle.nac import read_nac, write_nac
+
+    probe = os.path.join(ROOT, "oracle", "_ref", "probe_model")
+    for name in COMPLEX_SPINLESS_MODELS:
+        tmp = tempfile.mkdtemp(prefix="golden_zmodel_")
+        out = os.path.join(tmp, "model.nac")
+        subprocess.run([probe, os.path.join(ROOT, "dmrgcc_b200", "inputs", f"{name}.in"), out, "spinless"],
+                       check=True, stdout=subprocess.DEVNULL)
+        write_nac(os.path.join(HERE, f"model_complex_{name}.nac"), read_nac(out))
+
+
 def spinful_fixtures() -> None:
     """model_<input>.nac: the reference's spinful MPO and quantum tables
     (oracle/_ref/probe_model; the imaginary parts, zero at flux 0, are checked
@@ -415,6 +435,7 @@ def main() -> int:
                     "runs the reference up to its call: minutes of CPU)")
     ap.add_argument("--scan", action="store_true", help="only the 64-instance U/t scan reference energies")
     ap.add_argument("--spinful", action="store_true", help="only the spinful model fixtures")
+    ap.add_argument("--complex-spinless", action="store_true", help="only the complex spinless model fixtures")
     ap.add_argument("--complex", action="store_true", help="only the complex-path (Hofstadter) fixtures")
     ap.add_argument("--converged", action="store_true", help="only the converged chain16 energy (D=256)")
     ap.add_argument("--complex-run", action="store_true", help="only the reference energy of hofstadter6x6.in")
@@ -437,6 +458,9 @@ def main() -> int:
         return 0
     if args.spinful:
         spinful_fixtures()
+        return 0
+    if args.complex_spinless:
+        complex_spinless_fixtures()
         return 0
     if args.complex:
         complex_fixtures()

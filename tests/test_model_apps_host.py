@@ -1,6 +1,7 @@
 """The reference's model executables rebuilt on the library
 (dmrgcc_b200/csrc/apps/model_main.cc: real_spinless_bose_square_model,
-complex_spinful_bose_square_model, real_spinful_bose_square_model) and the
+complex_spinless_bose_square_model, complex_spinful_bose_square_model,
+real_spinful_bose_square_model) and the
 optional input keys that choose the run options (dmrg_run_options_from_input),
 host side: usage and error behaviour as the reference's main()
 (model/real_spinless_bose_square_model.cc:3-9), the keys' defaults and values,

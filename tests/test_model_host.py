@@ -115,3 +115,32 @@ def test_hofstadter_exact_diagonalisation_matches_reference():
     assert abs(e - e_ref) / 12 <= 1e-12
     e0 = ground_energy_spinful(4, 3, 3, 0, 3, -1.0, -1.0, 10.0, 0.0, 0.0, 0.0, False, True)
     assert e0 < e - 1.0  # the flux matters
+
+
+@pytest.mark.parametrize("name", ["chain16_spinless", "cylinder3x3_spinless"])
+def test_complex_spinless_mpo_bit_exact(name):
+    """The complex spinless model (model/complex_spinless_bose_square_model.cc:
+    the real spinless terms on complex operators, run by the complex engine):
+    every complex MPO entry and both quantum tables bit-identical to the
+    reference's ComplexSpinlessBoseSquare classes (oracle/_ref/probe_model ...
+    spinless), and its real parts equal to the real spinless model's MPO."""
+    ref = read_nac(os.path.join(GOLD, f"model_complex_{name}.nac"))
+    inp = os.path.join(ROOT, "dmrgcc_b200", "inputs", f"{name}.in")
+    m = capi.Model(inp, "complex_spinless_bose_square")
+    real = capi.Model(inp)
+    assert m.is_complex and not real.is_complex
+    n = int(ref["num_site"][0])
+    assert m.num_site == n and m.num_quantum == 1
+    for i in range(n):
+        W = m.mpo(i)
+        d, lb, rb = (int(x) for x in ref[f"op{i}.dims"])
+        assert W.shape == (lb, rb, d, d)
+        assert np.array_equal(W.real.ravel(), ref[f"op{i}.W"])
+        assert np.array_equal(W.imag.ravel(), ref[f"op{i}.Wi"])
+        Wr = real.mpo(i)
+        assert Wr.shape == W.shape and np.array_equal(Wr, W.real)
+    for b in range(n + 1):
+        assert np.array_equal(m.quantum_table(0, b).ravel(), ref[f"sq{b}"])
+        assert np.array_equal(m.quantum_table(1, b).ravel(), ref[f"hq{b}"])
+    m.close()
+    real.close()
