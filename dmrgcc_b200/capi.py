@@ -653,6 +653,22 @@ class Run:
         return {"half_sweep": hs[:m], "site": st[:m], "energy": en[:m], "lanczos_dim": dims[:m],
                 "discarded": dis[:m], "psi_dim": psi[:m], "seconds": sec[:m]}
 
+    def log_records(self) -> list[dict]:
+        """The run as log records: one per site step ("step": half-sweep, site,
+        Lanczos energy and Krylov dimension, discarded weight of the truncation,
+        psi_dim, seconds), then one per half-sweep ("half_sweep": its energy,
+        the reference's "right/left energy =", seconds, per-phase seconds,
+        Jacobi SVD sweeps).  The reference prints only the energies."""
+        return run_log_records(self.steps(), *self.half_sweeps(), *self.phases())
+
+    def write_log(self, path: str) -> None:
+        """The records of log_records() as JSON lines."""
+        import json
+
+        with open(path, "w") as f:
+            for r in self.log_records():
+                f.write(json.dumps(r) + "\n")
+
     def close(self) -> None:
         if self.h:
             lib().dmrg_run_destroy(self.h)
@@ -663,6 +679,25 @@ class Run:
             self.close()
         except Exception:
             pass
+
+
+def run_log_records(steps: dict, energies, seconds, phase_seconds, svd_sweeps) -> list[dict]:
+    """Log records of a run from its step records (Run.steps()), half-sweep
+    energies and times (Run.half_sweeps()) and phases (Run.phases())."""
+    out = []
+    for k in range(len(steps["site"])):
+        out.append({"record": "step", "half_sweep": int(steps["half_sweep"][k]), "site": int(steps["site"][k]),
+                    "energy": float(steps["energy"][k]), "lanczos_dim": int(steps["lanczos_dim"][k]),
+                    "discarded": float(steps["discarded"][k]), "psi_dim": int(steps["psi_dim"][k]),
+                    "seconds": float(steps["seconds"][k])})
+    for h in range(len(energies)):
+        rec = {"record": "half_sweep", "half_sweep": h, "direction": "right" if h % 2 == 0 else "left",
+               "energy": float(energies[h]), "seconds": float(seconds[h])}
+        if h < len(phase_seconds):
+            rec["phase_seconds"] = {name: float(v) for name, v in zip(Run.PHASES, phase_seconds[h])}
+            rec["svd_sweeps"] = int(svd_sweeps[h])
+        out.append(rec)
+    return out
 
 
 class Model:
