@@ -562,7 +562,10 @@ def run_b200(args) -> None:
             "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else args.precision + " (f32 accumulate per term, f64 sums)",
             "data": "synthetic (seeded splitmix64 values on the reference's own D=1024 block structure)",
             "config": bench_config(step.psi_dim, alg_flops * 1e-9),
-            "detail": {"precision": args.precision, "gflop_per_step_executed": exec_flops * 1e-9,
+            # exec_flops counts the products the schedule runs (each K*R product
+            # once), not the padding of the 64x64x16 DMMA tiles around them
+            "detail": {"precision": args.precision, "gflop_per_step_scheduled": exec_flops * 1e-9,
+                       "gflop_note": "scheduled products without the tile padding of the DMMA tiles",
                        "l2": "256 MiB write between timed steps (outside the per-step CUDA-event pair)",
                        "parallelism": f"replicas x{world}"},
             # counted by the library (dmrg_launch_count) around the timed loop: per
