@@ -544,6 +544,39 @@ def right_canonical(lat: Lattice, max_dim: int, canpre: float) -> dict:
     return {"svals": svals_full, "tdim": tdim, "discarded": _discarded(svals_full, tdim)}
 
 
+def merge_lattice(lat: Lattice, source: Lattice, side: int) -> Lattice:
+    """Left/RightMergeTensorLattice (real_tensor_lattice.cc:914-977): every ket
+    block of `lat` whose left (side 0) / right (side 1) sector is s is replaced
+    by canonical[s] @ block (side 0) or block @ canonical[s] (side 1), with
+    canonical the per-sector blocks of `source`; that sector's dimension becomes
+    the canonical block's rows (cols); then NormalizeTensorLattice
+    (:491-494 -> real_matrix_block.cc:164-171) scales the whole ket by
+    sqrt(1 / sum of squares)."""
+    C = source.canonical.mats
+    mats = [m.copy() for m in lat.ket.mats]
+    left_dim, right_dim = list(lat.left_dim), list(lat.right_dim)
+    if side == 0:
+        for sec in range(len(left_dim)):
+            for k, li in enumerate(lat.ket.left):
+                if li == sec:
+                    mats[k] = C[sec] @ mats[k]
+            left_dim[sec] = C[sec].shape[0]
+    else:
+        for sec in range(len(right_dim)):
+            for k, ri in enumerate(lat.ket.right):
+                if ri == sec:
+                    mats[k] = mats[k] @ C[sec]
+            right_dim[sec] = C[sec].shape[1]
+    total = 0.0
+    for m in mats:
+        total += float(np.sum(m * m))
+    f = np.sqrt(1.0 / total)
+    out = Lattice(physics_dim=lat.physics_dim, left_block=list(lat.left_block), left_dim=left_dim,
+                  right_block=list(lat.right_block), right_dim=right_dim, physics_index=lat.physics_index.copy(),
+                  ket=BlockList(list(lat.ket.left), list(lat.ket.right), [m * f for m in mats]))
+    return out
+
+
 def _discarded(svals: list, tdim: list) -> float:
     tot = 0.0
     for s, t in zip(svals, tdim):

@@ -15,6 +15,7 @@
 //   PROBE_STRUCT_ONLY=1    H_eff dumps carry block structure only (no values)
 //   PROBE_ENV=i,j,...      environment-update call indices to dump
 //   PROBE_CANON=i,j,...    canonicalisation call indices to dump
+//   PROBE_MERGE=i,j,...    merge call indices to dump (Left/RightMergeTensorLattice)
 //   PROBE_STOP=n           exit(0) right after Lanczos call n
 // cache_resume in the input reads the checkpoint through a corrected copy of
 // the reference's reader (see __wrap__ZN15RealTensorSpace15ReadTensorSpaceEPKc).
@@ -262,13 +263,37 @@ void __wrap__ZN15RealTensorSpace15ReadTensorSpaceEPKc(RealTensorSpace* self, con
         std::exit(2);
     }
 }
+// PROBE_MERGE=i,j: merge call i writes merge_<i>.nac with the site it merges
+// into before and after (lattices "before" / "after") and the lattice whose
+// canonical tensor it multiplies in ("source", with its canonical blocks).
+static std::vector<int> g_merge;
+static int n_merge = 0;
+static NacWriter* merge_begin(int side, RealTensorLattice* self, RealTensorLattice* o) {
+    const int call = n_merge++;
+    if (!wanted(g_merge, call)) return nullptr;
+    auto* w = new NacWriter(g_out + "/merge_" + std::to_string(call) + ".nac");
+    w->scalar_i("side", side);
+    w->scalar_i("site", site_of(self));
+    probe::write_lattice(*w, "before", self);
+    probe::write_lattice(*w, "source", o);
+    return w;
+}
+static void merge_end(NacWriter* w, RealTensorLattice* self) {
+    if (!w) return;
+    probe::write_lattice(*w, "after", self);
+    delete w;
+}
 void __wrap__ZN17RealTensorLattice22LeftMergeTensorLatticeEPS_(RealTensorLattice* self, RealTensorLattice* o) {
+    NacWriter* w = merge_begin(0, self, o);
     __real__ZN17RealTensorLattice22LeftMergeTensorLatticeEPS_(self, o);
     trace("M", 0, self);
+    merge_end(w, self);
 }
 void __wrap__ZN17RealTensorLattice23RightMergeTensorLatticeEPS_(RealTensorLattice* self, RealTensorLattice* o) {
+    NacWriter* w = merge_begin(1, self, o);
     __real__ZN17RealTensorLattice23RightMergeTensorLatticeEPS_(self, o);
     trace("M", 1, self);
+    merge_end(w, self);
 }
 void __real__ZN17RealTensorLattice20CombineTensorLatticeEiRiRPiS2_PS_(RealTensorLattice*, int, int&, int*&, int*&,
                                                                       RealTensorLattice*);
@@ -522,6 +547,7 @@ int main(int argc, char* argv[]) {
     g_heff = parse_list(std::getenv("PROBE_HEFF"));
     g_env = parse_list(std::getenv("PROBE_ENV"));
     g_canon = parse_list(std::getenv("PROBE_CANON"));
+    g_merge = parse_list(std::getenv("PROBE_MERGE"));
     g_struct_only = std::getenv("PROBE_STRUCT_ONLY") != nullptr;
     if (const char* s = std::getenv("PROBE_STOP")) g_stop = std::atoi(s);
     g_gauge = std::getenv("PROBE_GAUGE") != nullptr && std::atoi(std::getenv("PROBE_GAUGE")) != 0;

@@ -278,6 +278,21 @@ SPINFUL_MODELS = ("spinful4x4", "spinful3x3_periodic_y")
 COMPLEX_MODELS = ("hofstadter4x3",)
 
 
+MERGE_CALLS = (38, 50)  # a left and a right merge (site 9, second sweep) of the 16-site chain run
+
+
+def merge_fixtures() -> None:
+    """merge_c<i>.nac: the inputs and output of the reference's
+    Left/RightMergeTensorLattice at merge calls MERGE_CALLS of the 16-site chain
+    run (1 BLAS thread): the site merged into, before and after, and the
+    lattice whose canonical tensor is multiplied in."""
+    tmp = tempfile.mkdtemp(prefix="golden_merge_")
+    run_probe(os.path.join(ROOT, "dmrgcc_b200", "inputs", "chain16_spinless.in"), tmp,
+              {"PROBE_MERGE": ",".join(map(str, MERGE_CALLS))})
+    for c in MERGE_CALLS:
+        shutil.copy(os.path.join(tmp, f"merge_{c}.nac"), os.path.join(HERE, f"merge_c{c}.nac"))
+
+
 COMPLEX_SPINLESS_MODELS = ("chain16_spinless", "cylinder3x3_spinless")
 
 
@@ -436,6 +451,7 @@ def main() -> int:
     ap.add_argument("--scan", action="store_true", help="only the 64-instance U/t scan reference energies")
     ap.add_argument("--spinful", action="store_true", help="only the spinful model fixtures")
     ap.add_argument("--complex-spinless", action="store_true", help="only the complex spinless model fixtures")
+    ap.add_argument("--merge", action="store_true", help="only the merge fixtures of the 16-site chain")
     ap.add_argument("--complex", action="store_true", help="only the complex-path (Hofstadter) fixtures")
     ap.add_argument("--converged", action="store_true", help="only the converged chain16 energy (D=256)")
     ap.add_argument("--complex-run", action="store_true", help="only the reference energy of hofstadter6x6.in")
@@ -461,6 +477,9 @@ def main() -> int:
         return 0
     if args.complex_spinless:
         complex_spinless_fixtures()
+        return 0
+    if args.merge:
+        merge_fixtures()
         return 0
     if args.complex:
         complex_fixtures()

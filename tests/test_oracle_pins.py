@@ -132,3 +132,29 @@ def test_reference_energy_trajectory_monotone_at_end():
     assert rows.shape[1] == 6 and len(rows) == 180
     final = rows[-1, 4]
     assert abs(final - (-13.539043419078)) < 1e-9
+
+
+@pytest.mark.parametrize("call", [38, 50])
+def test_merge_matches_reference(call):
+    """a8: the oracle's Left/RightMergeTensorLattice + NormalizeTensorLattice
+    against the reference's own merge on the 16-site chain (merge call 38: left,
+    50: right; site 9 of the second sweep): sector dimensions and block shapes
+    exact, values to 1e-13 of the largest (the reference's products are
+    OpenBLAS dgemm calls, the oracle's numpy's)."""
+    d = read_nac(os.path.join(GOLD, f"merge_c{call}.nac"))
+    side = int(d["side"][0])
+    before = O.lattice_from_nac(d, "before")
+    source = O.lattice_from_nac(d, "source")
+    after = O.lattice_from_nac(d, "after")
+    got = O.merge_lattice(before, source, side)
+    assert got.left_dim == after.left_dim and got.right_dim == after.right_dim
+    assert got.ket.left == after.ket.left and got.ket.right == after.ket.right
+    scale = max(float(np.max(np.abs(m))) for m in after.ket.mats if m.size)
+    for g, w in zip(got.ket.mats, after.ket.mats):
+        assert g.shape == w.shape
+        if w.size:
+            assert np.max(np.abs(g - w)) <= 1e-13 * scale
+    # the merge changes the merged side's dimensions where the truncation did
+    changed = (before.left_dim != after.left_dim) if side == 0 else (before.right_dim != after.right_dim)
+    assert changed
+    assert abs(sum(float(np.sum(m * m)) for m in got.ket.mats) - 1.0) < 1e-13
