@@ -11,6 +11,8 @@
 #include <system_error>
 #include <thread>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "gemm.cuh"
 #include "zgemm.cuh"
 
@@ -1273,13 +1275,19 @@ int Engine::Run() {
         const bool l2r = (h % 2) == 0;
         std::array<double, kPhases> ph{};
         svd_sweeps_ = 0;
-        // phase clock: every phase ends with its stream drained
+        // phase clock: every phase ends with its stream drained.  Each phase is
+        // also an NVTX range (the names of dmrg_run_phases) for CUDA tools that
+        // read them (ncu --nvtx); without such a tool the calls do nothing.
+        static const char* const kPhaseName[kPhases] = {"lanczos", "expansion", "canonicalisation",
+                                                         "environment", "match_merge"};
         double tp = wall_time();
         auto lap = [&](int k) -> int {
             DMRG_CUDA_TRY(cudaStreamSynchronize(st_));
+            nvtxRangePop();
             const double now = wall_time();
             ph[k] += now - tp;
             tp = now;
+            if (k + 1 < kPhases) nvtxRangePushA(kPhaseName[k + 1]);
             return DMRG_OK;
         };
         if (l2r && opt_.verbose) std::printf("------------------------ sweep=%d ------------------------\n", h / 2);
@@ -1289,6 +1297,7 @@ int Engine::Run() {
             int dim = 0;
             const int64_t psi_dim = lat_[j]->psi_dim();  // at the Lanczos call, like the reference's log
             tp = wall_time();
+            nvtxRangePushA(kPhaseName[0]);
             // The expansion's host half (its lattice, its products and their
             // rand() matrices) depends only on block structures that the Lanczos
             // leaves as they are, so a second host thread plans it while the
