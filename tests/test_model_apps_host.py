@@ -6,6 +6,7 @@ optional input keys that choose the run options (dmrg_run_options_from_input),
 host side: usage and error behaviour as the reference's main()
 (model/real_spinless_bose_square_model.cc:3-9), the keys' defaults and values,
 and, without a GPU, a clean CUDA error instead of a crash."""
+import ctypes as C
 import os
 import subprocess
 
@@ -87,3 +88,10 @@ def test_invalid_option_values(tmp_path, bad):
         capi.run_options_from_input(_with_keys(tmp_path, [bad]))
     assert err.value.code == capi.E_ARG
     assert bad.split("=")[0].strip() in str(err.value)
+
+
+def test_null_arguments():
+    lib = capi.lib()
+    o = capi.RunOptions()
+    assert lib.dmrg_run_options_from_input(None, C.byref(o)) == capi.E_ARG
+    assert lib.dmrg_run_options_from_input(CHAIN.encode(), None) == capi.E_ARG
