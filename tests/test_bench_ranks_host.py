@@ -101,3 +101,57 @@ def test_truncation_summary_of_a_run_record():
             raise RuntimeError("no records")
 
     assert bench.truncation_summary(_Broken())["discarded_weight_total"] is None
+
+
+class _FakeRun:
+    """Stands in for capi.Run (the calls sweep_time and two_site_form make)."""
+
+    PHASES = ("lanczos", "expansion", "canonicalisation", "environment", "match_merge")
+
+    def __init__(self, ctx, path, verbose=0, precision=0, two_site=False, **kw):
+        import numpy as np
+
+        self.np = np
+        self.scale = 1.0 + 0.1 * precision + 0.2 * bool(two_site)
+
+    def execute(self):
+        pass
+
+    def half_sweeps(self):
+        e = self.np.array([-45.0, -45.6, -45.65, -45.653])
+        return e - 1e-9 * self.scale, self.np.array([0.5, 0.6, 0.7, 0.8]) * self.scale
+
+    def phases(self):
+        return self.np.ones((4, 5)) * 0.1 * self.scale, self.np.array([3, 4, 5, 6], self.np.int32)
+
+    def steps(self):
+        return {"half_sweep": self.np.array([0, 1, 2, 3], self.np.int32),
+                "discarded": self.np.array([1e-6, 1e-7, 1e-8, 1e-9]) * self.scale}
+
+    def close(self):
+        pass
+
+
+def test_sweep_sections_of_the_bench_line(monkeypatch):
+    """sweep_pair and two_site_form assemble their JSON objects (times, phases,
+    energies, truncation summaries, split deltas) from the run records; here
+    the runs are stand-ins, so only the host logic of the bench is exercised."""
+    import json
+
+    sys.path.insert(0, ROOT)
+    import bench
+    from dmrgcc_b200 import capi
+
+    monkeypatch.setattr(capi, "Run", _FakeRun)
+    monkeypatch.setattr(bench, "reference_sweep_sample", lambda ctx, threads: {"unavailable": "stand-in"})
+    sp = bench.sweep_pair(None)
+    json.dumps(sp)
+    assert sp["per_sweep_s"] == pytest.approx([1.1, 1.5])
+    assert sp["truncation"]["discarded_weight_total"] == pytest.approx(1.111e-6)
+    assert sp["split"]["discarded_weight_delta_vs_fp64"] == pytest.approx(0.2 * 1.111e-6)
+    assert sp["split"]["abs_dE_per_site_vs_fp64"] == pytest.approx(0.2e-9 / 32.0)
+    ts = bench.two_site_form(None)
+    json.dumps(ts)
+    # the last sweep is half-sweeps 2 and 3
+    assert ts["fp64"]["truncation"]["discarded_weight_last_sweep"] == pytest.approx(1.2 * 1.1e-8)
+    assert ts["last_sweep_speedup_vs_fp64"] == pytest.approx(1.2 / 1.4)
