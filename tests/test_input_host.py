@@ -91,3 +91,24 @@ def test_nonphysical_sizes_are_rejected(tmp_path, bad):
     p.write_text("\n".join(out))
     rc, _, msg = _create(str(p))
     assert rc == capi.E_ARG and msg
+
+
+def test_every_shipped_input_builds_its_model():
+    """Every input file under dmrgcc_b200/inputs passes the model layer's size
+    checks: spinless files as the real and the complex spinless model, spinful
+    ones as the complex spinful model, and as the real one where the flux is 0."""
+    for name in sorted(os.listdir(INPUTS)):
+        path = os.path.join(INPUTS, name)
+        with open(path) as f:
+            text = f.read()
+        if "Nup" in text:
+            models = ["complex_spinful_bose_square"]
+            flux = [ln for ln in text.splitlines() if ln.strip().startswith("flux")][0]
+            if float(flux.split("=")[1]) == 0.0:
+                models.append("real_spinful_bose_square")
+        else:
+            models = ["real_spinless_bose_square", "complex_spinless_bose_square"]
+        for model in models:
+            rc, h, msg = _create(path, model)
+            assert rc == 0, (name, model, msg)
+            capi.lib().dmrg_model_destroy(h)
