@@ -155,3 +155,45 @@ def test_sweep_sections_of_the_bench_line(monkeypatch):
     # the last sweep is half-sweeps 2 and 3
     assert ts["fp64"]["truncation"]["discarded_weight_last_sweep"] == pytest.approx(1.2 * 1.1e-8)
     assert ts["last_sweep_speedup_vs_fp64"] == pytest.approx(1.2 / 1.4)
+
+
+def test_scan_and_complex_sections_of_the_bench_line(monkeypatch, tmp_path):
+    """scan_form and complex_form assemble their objects from stand-in runs and
+    contexts (the reference binaries pointed at a missing path, so neither
+    runs): the host logic only."""
+    import json
+
+    sys.path.insert(0, ROOT)
+    import bench
+    from dmrgcc_b200 import capi
+
+    class _Ctx:
+        def __init__(self, dev=0):
+            pass
+
+        def close(self):
+            pass
+
+    class _ScanRun(_FakeRun):
+        def __init__(self, ctx, path, precision=0, **kw):
+            super().__init__(ctx, path, precision=precision)
+
+        @staticmethod
+        def execute_many(runs, threads=0):
+            import time
+
+            time.sleep(0.001)
+
+    monkeypatch.setattr(capi, "Context", _Ctx)
+    monkeypatch.setattr(capi, "Run", _ScanRun)
+    missing = str(tmp_path / "missing")
+    monkeypatch.setattr(bench, "REF_MODEL", missing)
+    monkeypatch.setattr(bench, "CPLX_MODEL", missing)
+    sc = bench.scan_form(2)
+    json.dumps(sc)
+    assert sc["instances"] == 64 and sc["sweeps_total"] == 384
+    assert sc["max_abs_dE_per_site_tf32x3_vs_fp64"] > 0 and "reference_cpu" not in sc
+    cx = bench.complex_form(None, 2)
+    json.dumps(cx)
+    assert cx["final_energy"] == pytest.approx(-45.653 - 1e-9)
+    assert "reference_final_energy" in cx and "reference_cpu_sample" not in cx
