@@ -42,6 +42,20 @@ static void quicksort_cases(const char* path) {
     }
 }
 
+// QuickSort's edge cases: a flag other than 0 or 1 and an empty or one-element
+// range leave both arrays as they are; a sub-range sorts only that range.
+static void quicksort_edges() {
+    double v[5] = {0.3, 0.9, 0.1, 0.9, 0.5};
+    int idx[5] = {0, 1, 2, 3, 4};
+    QuickSort(v, idx, 0, 4, 2);
+    QuickSort(v, idx, 3, 3, 0);
+    QuickSort(v, idx, 4, 3, 0);
+    QuickSort(v, idx, 1, 3, 1);  // ascending on v[1..3]
+    std::printf("quicksort_edges");
+    for (int i = 0; i < 5; ++i) std::printf(" %d:%.17g", idx[i], v[i]);
+    std::printf("\n");
+}
+
 // Each line: nsec max_dim canpre, then per sector its count and its values.
 static void truncate_cases(const char* path) {
     std::ifstream f(path);
@@ -140,6 +154,7 @@ int main(int argc, char** argv) {
     try {
         if (argc > 5 && std::strcmp(argv[5], "--device") == 0) return device_classes(argv[3], argv[4]);
         quicksort_cases(argv[1]);
+        quicksort_edges();
         truncate_cases(argv[2]);
         model(argv[3], argv[4]);
         try {

@@ -77,6 +77,10 @@ def test_quicksort_and_truncation_through_the_cxx_classes(program, tmp_path):
     assert len(got) == len(gold) == 40
     for g, want in zip(got, gold):
         assert [int(x) for x in g] == [int(x) for x in want.split()]
+    # flag 2, empty and one-element ranges change nothing; v[1..3] sorted ascending
+    edges = _by_tag(lines, "quicksort_edges")[0]
+    assert edges == ["0:0.29999999999999999", "2:0.10000000000000001", "1:0.90000000000000002",
+                     "3:0.90000000000000002", "4:0.5"]
     got = [" ".join(t).split("|") for t in _by_tag(lines, "truncate")]
     assert len(got) == len(cases)
     for (dims, vals), (sv, max_dim, canpre) in zip(got, cases):
